@@ -1,0 +1,293 @@
+"""Benchmark: rigid TIP4P/2005 water timesteps/s and ns/day on B200.
+
+Workload (default): 4,096 molecules (16,384 sites incl. M), cubic lattice at
+0.997 g/cm^3 with seeded random orientations, LJ + Coulomb 9 A cutoff, skin
+1 A, Ewald real space + P3M 64^3 order 5, SETTLE, dt 2 fs, Nose-Hoover NVT at
+298 K, FP32 with FP64 reductions and FP64 SETTLE, neighbour check every 10
+steps.  A "step" is one MD timestep of that system.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload water|water_e3b|lj]
+  python bench.py --impl reference ...   # the reference's CPU arm (the oracle)
+
+Under torchrun every rank steps its own independent replica (the path does
+not shard: replicas only); value = sum over ranks of steps / max rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "water timesteps/s & ns/day on 1 B200, plain vs surrogate/batched at force RMSE"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="water", choices=["water", "water_e3b", "lj"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def init_pg(world, backend):
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def reduce_max(dist, value, device=None):
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist, device=None):
+    if dist is None:
+        return
+    import torch
+    t = torch.zeros(1, device=device)
+    dist.all_reduce(t)
+
+
+def workload(name, seed=20261203):
+    from md_engine_b200 import systems
+    if name == "lj":
+        sysd = systems.lj_fcc(ncell=20, seed=seed)
+        st, _ = systems.build_lj_state(sysd, rcut=2.5, skin=0.3, dt=0.005, interval=10, T=1.2, tau=0.5)
+        cfg = {"workload": "LJ fluid 32,000 atoms FCC rho*=0.8442 T*=1.2, rc 2.5 skin 0.3, dt 0.005, NH",
+               "atoms": len(sysd.pos)}
+        return sysd, st, cfg, 0.005
+    e3b = name == "water_e3b"
+    sysd = systems.water_tip4p2005(nside=16, seed=seed)
+    st, _ = systems.build_water_state(sysd, rcut=9.0, skin=1.0, dt=2.0, interval=10, grid=64, e3b=e3b,
+                                      T=298.0, tau=100.0)
+    cfg = {"workload": ("TIP4P/2005" + ("+E3B3" if e3b else "") +
+                        " 4,096 molecules (16,384 sites), LJ+Coulomb 9 A, skin 1 A, P3M 64^3 order 5, "
+                        "SETTLE, dt 2 fs, Nose-Hoover 298 K"),
+           "molecules": int(len(sysd.molecules)), "sites": int(len(sysd.pos))}
+    return sysd, st, cfg, 2.0
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.15)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=2)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return None
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4)
+                          if len(s) > 5 + k and s[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(key):
+    """dram bytes per launch of the dominant kernel from the committed ncu summary"""
+    p = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f).get(key)
+    return None
+
+
+def cpu_baseline(sysd, name, dt_fs, nsample=1):
+    """The oracle's FP64 water step on the host cores (the reference has no CPU
+    force path; its CPU restatement is the baseline).  Bounded sample."""
+    from oracle import cpu_step
+    return cpu_step.time_steps(sysd, name, nsample=nsample)
+
+
+def run_reference_arm(args, rank, world):
+    """--impl reference: the oracle's CPU step (OpenMP, all host threads),
+    rank 0 only; other ranks exit without work."""
+    if rank != 0:
+        return
+    from md_engine_b200 import systems
+    from oracle import cpu_step
+    if args.workload == "lj":
+        sysd = systems.lj_fcc(ncell=20)
+        dt = 0.005
+    else:
+        sysd = systems.water_tip4p2005(nside=16)
+        dt = 2.0
+    steps = max(1, min(args.steps, 3))
+    warm = 1 if args.warmup > 0 else 0
+    res = cpu_step.time_steps(sysd, args.workload, nsample=steps, warmup=warm)
+    v = res["steps_per_s"]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "timesteps/s", "n_gpus": world,
+            "steps": steps, "warmup": warm, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+            "config": {"workload": res["workload"]},
+            "ns_per_day": v * dt * 86400 / 1e6 if args.workload != "lj" else None,
+            "cpu_baseline": {"value": v, "unit": "timesteps/s", "cores": res["cores"], "kind": "port",
+                             "sample": res["sample"]},
+            "e2e": {"value": v, "unit": "timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+    import torch
+    from md_engine_b200 import IntegratorVerlet, kernel_launches
+    from md_engine_b200._lib import lib
+    torch.cuda.set_device(local)
+    lib().mdx_set_device(local)
+    dist = init_pg(world, "nccl")
+    dev = torch.device("cuda", local)
+    sysd, st, cfg, dt = workload(args.workload, seed=20261203 + rank)
+    it = IntegratorVerlet(st)
+    # warm-up: prepare, capture graphs, settle clocks (untimed)
+    it.run(max(args.warmup, 3))
+    K = args.steps
+    P = 10
+    barrier(dist, dev)
+    torch.cuda.synchronize()
+    k0 = kernel_launches()
+    with ClockSampler(local) as clk:
+        ms = it.runTimed(K, P, L2_FLUSH_BYTES)
+    k1 = kernel_launches()
+    torch.cuda.synchronize()
+    barrier(dist, dev)
+    ms_max = reduce_max(dist, ms, dev)
+    value = world * K / (ms_max * 1e-3)
+    # end to end through the C ABI with host buffers: H2D positions+velocities,
+    # P steps, D2H positions+velocities+forces, per call
+    x, v, _ = st.getAtoms()
+    n = len(x)
+    e2e_calls = max(1, K // P)
+    barrier(dist, dev)
+    t0 = time.perf_counter()
+    for _ in range(e2e_calls):
+        out = it.runHost(P, positions=x, velocities=v)
+        x, v = out["pos"], out["vel"]
+    t_e2e = time.perf_counter() - t0
+    t_e2e = reduce_max(dist, t_e2e, dev)
+    e2e = world * e2e_calls * P / t_e2e
+    # roofline of the dominant kernel (pair forces): algorithmic bytes per
+    # launch = 16N (x) + 4N (q) + 16N (f) + 4 N nbar (directed list entries)
+    counts, _, _ = st.getNeighborList()
+    nbar = float(np.mean(counts))
+    charged = args.workload != "lj"
+    alg_bytes = n * (16 + (4 if charged else 0) + 16) + 4.0 * n * nbar
+    pair_ms = st.timeStage("pair", iters=20, flushBytes=L2_FLUSH_BYTES)
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (pair_ms * 1e-3) / 1e9
+    stages = {}
+    for sname in ("pair", "p3m", "e3b", "nlist"):
+        try:
+            stages[sname] = round(st.timeStage(sname, iters=10, flushBytes=L2_FLUSH_BYTES) * 1000.0, 2)
+        except Exception:
+            pass
+    line = None
+    if rank == 0:
+        ns_day = value / world * dt * 86400 / 1e6 if args.workload != "lj" else None
+        line = {
+            "metric": METRIC, "value": value, "unit": "timesteps/s", "n_gpus": world, "steps": K,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms_max / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 reductions, f64 SETTLE)",
+            "data": "synthetic (seeded lattice + random orientations + Maxwell-Boltzmann)",
+            "config": dict(cfg, l2="flushed between timed 10-step chunks (256 MiB write)",
+                           parallelism="replicas only" if world > 1 else "single system"),
+            "ns_per_day": ns_day,
+            "e2e": {"value": e2e, "unit": "timesteps/s",
+                    "h2d_bytes_per_step": int(2 * 16 * n / P), "d2h_bytes_per_step": int(3 * 16 * n / P)},
+            "gpu_launches": int(k1 - k0),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": profile_traffic(args.workload + "_pair"),
+                         "kernel": "k_pair (LJ + Ewald real space)", "kernel_ms": pair_ms,
+                         "alg_bytes_per_launch": alg_bytes, "nbar": nbar, "peak_source": peak_kind},
+            "stage_us": stages,
+            "clocks": clk.summary(),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                from oracle import cpu_step
+                res = cpu_step.time_steps(sysd, args.workload, nsample=1, warmup=0)
+                line["cpu_baseline"] = {"value": res["steps_per_s"], "unit": "timesteps/s", "cores": res["cores"],
+                                        "kind": "port", "sample": res["sample"]}
+            except Exception as ex:  # the baseline is reported, never required
+                line["cpu_baseline"] = {"value": None, "unit": "timesteps/s", "cores": os.cpu_count(),
+                                        "kind": "port", "sample": f"failed: {ex}"}
+        print(json.dumps(line))
+    if dist is not None:
+        barrier(dist, dev)
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

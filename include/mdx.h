@@ -1,0 +1,195 @@
+/*
+ * mdx.h -- C ABI of the B200-native DASH force hot path (libmdx.so).
+ *
+ * Plain C types only: opaque handles, pointers and sizes, int status codes
+ * (0 = MDX_OK).  No C++ exceptions cross this boundary; the message of the
+ * last failure on the calling thread is returned by mdx_last_error().
+ *
+ * Each entry point names the reference (dreid1991/md_engine, "DASH")
+ * interface it replaces, by file:line within that project.  Handles are not
+ * thread safe; one state per host thread / CUDA stream.  Device memory is
+ * owned by the library handle and released by its destroy call.
+ */
+#ifndef MDX_H
+#define MDX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MDX_OK 0
+#define MDX_ERR_ARG 1         /* invalid argument / unknown handle or key   */
+#define MDX_ERR_CUDA 2        /* CUDA runtime or cuFFT failure              */
+#define MDX_ERR_STATE 3       /* call not valid in the current state        */
+#define MDX_ERR_OVERFLOW 4    /* neighbour-list capacity exceeded           */
+#define MDX_ERR_UNSUPPORTED 5 /* configuration outside the implemented path */
+#define MDX_ERR_NUMERIC 6     /* NaN force / SETTLE failure / constraint    */
+
+#define MDX_UNITS_REAL 0
+#define MDX_UNITS_LJ 1
+
+typedef struct mdx_state mdx_state;
+typedef struct mdx_fix mdx_fix;
+typedef struct mdx_integrator mdx_integrator;
+
+/* ---- library ------------------------------------------------------------ */
+const char *mdx_last_error(void);
+int mdx_version(void);
+/* select the CUDA device for subsequent state creation on this host thread
+ * (DeviceManager::setDevice, src/DeviceManager.cpp) */
+int mdx_set_device(int device);
+/* number of CUDA kernels this library has launched since load (for the
+ * benchmark's launch count; cuFFT's own kernels are not included) */
+uint64_t mdx_kernel_launch_count(void);
+
+/* ---- State (src/State.h:63-146, src/State.cpp:28-68) --------------------- */
+int mdx_state_create(mdx_state **out);
+int mdx_state_destroy(mdx_state *st);
+/* Units::setReal / Units::setLJ (src/Units.cpp:5-32) */
+int mdx_state_set_units(mdx_state *st, int unit_type);
+/* state.bounds = Bounds(state, lo=..., hi=...) (src/Bounds.cpp) */
+int mdx_state_set_bounds(mdx_state *st, const double lo[3], const double hi[3]);
+/* State attributes exported at src/State.cpp:1220-1247: keys "rCut",
+ * "padding", "dt" (double); "periodicInterval", "nThreadPerAtom",
+ * "nThreadPerBlock", "turn" (int) */
+int mdx_state_set_double(mdx_state *st, const char *key, double value);
+int mdx_state_get_double(mdx_state *st, const char *key, double *value);
+int mdx_state_set_int(mdx_state *st, const char *key, int64_t value);
+int mdx_state_get_int(mdx_state *st, const char *key, int64_t *value);
+/* State::setSpecialNeighborCoefs (src/State.cpp:406-410) */
+int mdx_state_set_special_neighbor_coefs(mdx_state *st, double onetwo, double onethree, double onefour);
+/* AtomParams::addSpecies (src/AtomParams.cpp); returns the type index */
+int mdx_state_add_species(mdx_state *st, const char *handle, double mass, int atomic_num, int *type_out);
+/* State::addAtom (src/State.cpp) for n atoms; ids are assigned 0..N-1 in
+ * call order and the first new id is returned.  pos/q may not be NULL. */
+int mdx_state_add_atoms(mdx_state *st, int n, const char *const *species_handles, const double *pos,
+                        const double *q, int *first_id_out);
+int mdx_state_n_atoms(mdx_state *st, int *n_out);
+/* atom.vel = ... for ids[i] (vel is 3 doubles per id) */
+int mdx_state_set_velocities(mdx_state *st, int n, const int *ids, const double *vel);
+/* host copies by atom id (each pointer may be NULL): positions, velocities,
+ * forces as 3 doubles per atom.  Syncs the device copy back first. */
+int mdx_state_get_atoms(mdx_state *st, double *pos, double *vel, double *force);
+/* overwrite device positions/velocities by atom id from host buffers
+ * (3 doubles per atom; either may be NULL) after a prepared run */
+int mdx_state_put_atoms(mdx_state *st, const double *pos, const double *vel);
+/* State::activateFix / deactivateFix (src/State.cpp:445-500) */
+int mdx_state_activate_fix(mdx_state *st, mdx_fix *fix);
+int mdx_state_deactivate_fix(mdx_state *st, mdx_fix *fix);
+/* device status bits (see common.cuh StatusBits) and the largest neighbour
+ * count seen at the last build */
+int mdx_state_status(mdx_state *st, uint32_t *bits, uint32_t *max_neighbors, uint64_t *n_builds);
+/* use a caller-owned cudaStream_t (NULL = the library's own stream) */
+int mdx_state_set_stream(mdx_state *st, void *cuda_stream);
+int mdx_state_synchronize(mdx_state *st);
+
+/* ---- fixes (src/Fixes/Fix.h:79-281) ------------------------------------- */
+/* FixLJCut(state, handle, mixingRules) (src/Fixes/FixLJCut.cu:14-28) */
+int mdx_fix_lj_cut_create(mdx_state *st, const char *handle, const char *mixing, mdx_fix **out);
+/* FixWCA(state, handle, mixingRules) (src/Fixes/FixWCA.cu) */
+int mdx_fix_wca_create(mdx_state *st, const char *handle, const char *mixing, mdx_fix **out);
+/* FixPair::setParameter(param, handleA, handleB, val) (src/Fixes/FixPair.cpp:143-168);
+ * param is "eps", "sig" or "rCut" */
+int mdx_fix_pair_set_parameter(mdx_fix *fix, const char *param, const char *handle_a, const char *handle_b,
+                               double value);
+/* FixChargeEwald(state, handle, group) (src/Fixes/FixChargeEwald.cu:828-839) */
+int mdx_fix_charge_ewald_create(mdx_state *st, const char *handle, const char *group, mdx_fix **out);
+/* FixChargeEwald::setParameters(sz, rcut, order) (src/Fixes/FixChargeEwald.cu:969-1021);
+ * rcut < 0 means state rCut.  Grid sizes 32..1024 powers of two, order 5. */
+int mdx_fix_charge_ewald_set_parameters(mdx_fix *fix, int nx, int ny, int nz, double rcut, int order);
+/* explicit splitting parameter (the reference solves it by secant in
+ * find_optimal_parameters, src/Fixes/FixChargeEwald.cu:918-967; <= 0 restores that) */
+int mdx_fix_charge_ewald_set_alpha(mdx_fix *fix, double alpha);
+int mdx_fix_charge_ewald_get_alpha(mdx_fix *fix, double *alpha);
+/* FixE3B(state, handle, style) (src/Fixes/FixE3B.cu:16-36), style "E3B3" or "E3B2" */
+int mdx_fix_e3b_create(mdx_state *st, const char *handle, const char *style, mdx_fix **out);
+/* FixE3B::addMolecule(O, H1, H2, M) (src/Fixes/FixE3B.cu:753-792) */
+int mdx_fix_e3b_add_molecule(mdx_fix *fix, int id_o, int id_h1, int id_h2, int id_m);
+/* FixRigid(state, handle, style) (src/Fixes/FixRigid.cu:18-37) */
+int mdx_fix_rigid_create(mdx_state *st, const char *handle, const char *style, mdx_fix **out);
+/* FixRigid::createRigid(O, H1, H2, M) (src/Fixes/FixRigid.cu:1560-1610); id_m < 0 for 3-site */
+int mdx_fix_rigid_create_rigid(mdx_fix *fix, int id_o, int id_h1, int id_h2, int id_m);
+/* FixNoseHoover(state, handle, group) + setTemperature(T, timeConstant)
+ * (src/Fixes/FixNoseHoover.cu:97-130, 221-226) */
+int mdx_fix_nose_hoover_create(mdx_state *st, const char *handle, const char *group, mdx_fix **out);
+int mdx_fix_nose_hoover_set_temperature(mdx_fix *fix, double temperature, double time_constant);
+int mdx_fix_destroy(mdx_fix *fix);
+
+/* ---- integrator (src/Integrators/IntegratorVerlet.cu:649-770) ----------- */
+int mdx_integrator_verlet_create(mdx_state *st, mdx_integrator **out);
+/* IntegratorVerlet::run(numTurns); returns particle-timesteps per second
+ * measured with CUDA events around the stepping loop */
+int mdx_integrator_run(mdx_integrator *it, int num_turns, double *ptsps_out);
+/* 0: fused, CUDA-graph captured timestep (default); 1: one kernel per
+ * reference hook, no graph (the reference's launch structure) */
+int mdx_integrator_set_mode(mdx_integrator *it, int mode);
+int mdx_integrator_destroy(mdx_integrator *it);
+/* IntegratorVerlet::run with host buffers (the State's atoms are the host
+ * buffers in the reference, State.cpp:529-610): positions/velocities (3
+ * doubles per atom, by id; NULL keeps the resident copy) are copied in,
+ * num_turns steps run on the fused graph path, and positions / velocities /
+ * forces (NULL to skip) are copied back, all within this call. */
+int mdx_integrator_run_host(mdx_integrator *it, int num_turns, const double *pos_in, const double *vel_in,
+                            double *pos_out, double *vel_out, double *force_out);
+/* Benchmark support (no reference counterpart): run num_turns in chunks of
+ * `chunk` timesteps on the fused graph path; each chunk is bracketed by CUDA
+ * events on the library stream and preceded, outside the timed window, by a
+ * flush_bytes device write that evicts L2.  *device_ms = summed chunk time. */
+int mdx_integrator_run_timed(mdx_integrator *it, int num_turns, int chunk, size_t flush_bytes, double *device_ms);
+/* Benchmark support (no reference counterpart): average device time of one
+ * launch of a hot-path stage over `iters` launches, L2 flushed between them.
+ * stage 0 pair forces, 1 P3M reciprocal (spread+FFT+field+gather), 2 E3B,
+ * 3 neighbour-list rebuild (forced), 4 fused first half, 5 fused second half */
+int mdx_time_stage(mdx_state *st, int stage, int iters, size_t flush_bytes, double *avg_ms);
+
+/* ---- stage-level hot path ------------------------------------------------ */
+/* Integrator::basicPrepare + prepareFixes + forceInitial + prepareFinal
+ * (src/Integrators/Integrator.cu:142-219): upload, build, prepare, forces. */
+int mdx_prepare(mdx_state *st);
+/* GridGPU::periodicBoundaryConditions(-1, forceBuild) (src/GridGPU.cu:824-1103) */
+int mdx_nlist_build(mdx_state *st, int force_build);
+/* Grid.getNeighborList (src/GridGPU.cu:1520-1648): per-id neighbour ids,
+ * sorted ascending.  counts[id]; nbr[id*max_per_atom + k] (atom ids);
+ * tags[id*max_per_atom + k] = exclusion depth (0..3), may be NULL. */
+int mdx_nlist_get(mdx_state *st, int max_per_atom, int *counts, int *nbr, int *tags);
+/* IntegratorUtil::force(virialMode) (src/Integrators/IntegratorUtil.cpp:15-30):
+ * zero forces, run every fix's compute() */
+int mdx_compute_forces(mdx_state *st, int virial_mode);
+/* Fix::singlePointEng summed per term: out[0] pair (LJ/WCA + Ewald real),
+ * out[1] Ewald reciprocal, out[2] E3B two-body, out[3] E3B three-body;
+ * FP64 device reductions */
+int mdx_potential_energy(mdx_state *st, double out[4]);
+/* sum over atoms of m v^2 (FP64) and the degrees of freedom */
+int mdx_kinetic(mdx_state *st, double *sum_mv2, double *ndf);
+/* per-atom virials (6 per atom, xx yy zz xy xz yz) by id, FP64 total in sum6 */
+int mdx_get_virials(mdx_state *st, double *per_atom, double sum6[6]);
+/* single hooks, for stage-level parity (src/Fixes/FixRigid.cu:1234-1279, 1916-1984) */
+int mdx_rigid_settle_positions(mdx_state *st, mdx_fix *rigid);   /* save_prev_val before x move is the caller's */
+int mdx_rigid_save_prev(mdx_state *st, mdx_fix *rigid);
+int mdx_rigid_settle_velocities(mdx_state *st, mdx_fix *rigid);
+int mdx_rigid_distribute_msite(mdx_state *st, mdx_fix *rigid);
+int mdx_verlet_first_half(mdx_state *st);   /* nve_v + nve_x (IntegratorVerlet.cu:23-61) */
+int mdx_verlet_second_half(mdx_state *st);  /* postForce_cu (IntegratorVerlet.cu:610-627) */
+
+/* ---- raw device-pointer entry point (EvaluatorWrapper::compute,
+ *      src/Evaluators/EvaluatorWrapper.h:10-16 / PairEvaluateIso.h:8-207) --
+ * Pair forces over a neighbour list in this library's layout: atom i is in
+ * warp group g = i / (32/team), slot a = i % (32/team); its k-th entry is at
+ * nlist[g*cap*(32/team) + (k/team)*32 + a*team + k%team]; entries are atom
+ * indices with the exclusion depth in bits 30-31.  params = {rc2, 24*eps,
+ * sig^6} per type pair (3 * ntypes^2 floats, row-major, the reference's
+ * paramsCoalesced order).  lj_kind 0 none / 1 LJ / 2 WCA; qrc <= 0 disables
+ * the Ewald real-space term.  virials (6 floats per atom) may be NULL.
+ * accumulate != 0 adds to fs instead of overwriting.  All pointers device. */
+int mdx_pair_force_raw(int n, const float *xs4, float *fs4, const float *qs, const uint32_t *counts,
+                       const uint32_t *nlist, int team, int cap, const float *params, int ntypes,
+                       const double lo[3], const double hi[3], const float coef[3], int lj_kind, float qrc,
+                       float alpha, float qqr_to_eng, float *virials, int accumulate, void *cuda_stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MDX_H */

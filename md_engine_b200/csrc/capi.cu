@@ -1,0 +1,689 @@
+// extern "C" entry points of include/mdx.h.  Every call returns an int
+// status; no C++ exception crosses this boundary.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "engine.hpp"
+
+namespace mdx {
+const char *last_error();
+int ewald_recip_energy(State &s, FixChargeEwald &f, double *out);
+}  // namespace mdx
+
+using namespace mdx;
+
+#define ARG_CHECK(cond, msg)                \
+    do {                                    \
+        if (!(cond)) {                      \
+            set_error(MDX_ERR_ARG, "%s", msg); \
+            return MDX_ERR_ARG;             \
+        }                                   \
+    } while (0)
+
+#define GUARD(body)                                           \
+    try {                                                     \
+        body                                                  \
+    } catch (const std::exception &ex) {                      \
+        set_error(MDX_ERR_STATE, "exception: %s", ex.what()); \
+        return MDX_ERR_STATE;                                 \
+    } catch (...) {                                           \
+        set_error(MDX_ERR_STATE, "unknown exception");        \
+        return MDX_ERR_STATE;                                 \
+    }
+
+extern "C" {
+
+const char *mdx_last_error(void) { return last_error(); }
+int mdx_version(void) { return 100; }
+
+int mdx_set_device(int device) {
+    MDX_CUDA_TRY(cudaSetDevice(device));
+    return 0;
+}
+uint64_t mdx_kernel_launch_count(void) { return g_launches; }
+
+int mdx_state_create(mdx_state **out) {
+    ARG_CHECK(out, "null out");
+    GUARD(*out = new mdx_state{new State()}; return 0;)
+}
+
+int mdx_state_destroy(mdx_state *st) {
+    if (!st) return 0;
+    if (st->s->stream) cudaStreamSynchronize(st->s->stream);
+    delete st->s;
+    delete st;
+    return 0;
+}
+
+int mdx_state_set_units(mdx_state *st, int unit_type) {
+    ARG_CHECK(st, "null state");
+    if (unit_type == MDX_UNITS_REAL) st->s->units.setReal();
+    else if (unit_type == MDX_UNITS_LJ) st->s->units.setLJ();
+    else ARG_CHECK(false, "unit_type must be MDX_UNITS_REAL or MDX_UNITS_LJ");
+    st->s->prepared = false;
+    return 0;
+}
+
+int mdx_state_set_bounds(mdx_state *st, const double lo[3], const double hi[3]) {
+    ARG_CHECK(st && lo && hi, "null argument");
+    for (int d = 0; d < 3; d++) ARG_CHECK(hi[d] > lo[d], "bounds: hi must exceed lo");
+    State &s = *st->s;
+    for (int d = 0; d < 3; d++) {
+        s.lo[d] = lo[d];
+        s.hi[d] = hi[d];
+    }
+    s.bounds_set = true;
+    s.setBox();
+    s.prepared = false;
+    return 0;
+}
+
+int mdx_state_set_double(mdx_state *st, const char *key, double v) {
+    ARG_CHECK(st && key, "null argument");
+    State &s = *st->s;
+    std::string k(key);
+    if (k == "rCut") s.rCut = v;
+    else if (k == "padding") s.padding = v;
+    else if (k == "dt") s.dt = v;
+    else {
+        set_error(MDX_ERR_ARG, "unknown double key '%s'", key);
+        return MDX_ERR_ARG;
+    }
+    s.prepared = false;
+    return 0;
+}
+
+int mdx_state_get_double(mdx_state *st, const char *key, double *v) {
+    ARG_CHECK(st && key && v, "null argument");
+    State &s = *st->s;
+    std::string k(key);
+    if (k == "rCut") *v = s.rCut;
+    else if (k == "padding") *v = s.padding;
+    else if (k == "dt") *v = s.dt;
+    else {
+        set_error(MDX_ERR_ARG, "unknown double key '%s'", key);
+        return MDX_ERR_ARG;
+    }
+    return 0;
+}
+
+int mdx_state_set_int(mdx_state *st, const char *key, int64_t v) {
+    ARG_CHECK(st && key, "null argument");
+    State &s = *st->s;
+    std::string k(key);
+    if (k == "periodicInterval") s.periodicInterval = (int)v;
+    else if (k == "nThreadPerAtom") s.nThreadPerAtom = (int)v;
+    else if (k == "nThreadPerBlock") s.nThreadPerBlock = (int)v;
+    else if (k == "turn") s.turn = v;
+    else {
+        set_error(MDX_ERR_ARG, "unknown int key '%s'", key);
+        return MDX_ERR_ARG;
+    }
+    s.prepared = false;
+    return 0;
+}
+
+int mdx_state_get_int(mdx_state *st, const char *key, int64_t *v) {
+    ARG_CHECK(st && key && v, "null argument");
+    State &s = *st->s;
+    std::string k(key);
+    if (k == "periodicInterval") *v = s.periodicInterval;
+    else if (k == "nThreadPerAtom") *v = s.grid.team;
+    else if (k == "nThreadPerBlock") *v = s.nThreadPerBlock;
+    else if (k == "turn") *v = s.turn;
+    else if (k == "nlistCapacity") *v = s.grid.cap;
+    else if (k == "cellsPerSide") *v = s.grid.ns.x;
+    else {
+        set_error(MDX_ERR_ARG, "unknown int key '%s'", key);
+        return MDX_ERR_ARG;
+    }
+    return 0;
+}
+
+int mdx_state_set_special_neighbor_coefs(mdx_state *st, double c12, double c13, double c14) {
+    ARG_CHECK(st, "null state");
+    st->s->specialNeighborCoefs[0] = (float)c12;
+    st->s->specialNeighborCoefs[1] = (float)c13;
+    st->s->specialNeighborCoefs[2] = (float)c14;
+    st->s->prepared = false;
+    return 0;
+}
+
+int mdx_state_add_species(mdx_state *st, const char *handle, double mass, int atomic_num, int *type_out) {
+    ARG_CHECK(st && handle, "null argument");
+    ARG_CHECK(mass >= 0, "mass must be >= 0");
+    State &s = *st->s;
+    ARG_CHECK(s.typeFromHandle(handle) < 0, "species handle already exists");
+    s.species.push_back({handle, mass, atomic_num});
+    if (type_out) *type_out = (int)s.species.size() - 1;
+    s.prepared = false;
+    return 0;
+}
+
+int mdx_state_add_atoms(mdx_state *st, int n, const char *const *handles, const double *pos, const double *q,
+                        int *first_id_out) {
+    ARG_CHECK(st && handles && pos && n >= 0, "null argument");
+    State &s = *st->s;
+    const int first = (int)s.atoms.size();
+    for (int i = 0; i < n; i++) {
+        int t = s.typeFromHandle(handles[i]);
+        if (t < 0) {
+            set_error(MDX_ERR_ARG, "unknown species '%s'", handles[i]);
+            return MDX_ERR_ARG;
+        }
+        HostAtom a{};
+        for (int d = 0; d < 3; d++) a.pos[d] = pos[3 * i + d];
+        a.mass = s.species[t].mass;
+        a.q = q ? q[i] : 0.0;
+        a.type = t;
+        a.ndf = 3;
+        a.groupTag = 1u;
+        s.atoms.push_back(a);
+    }
+    if (first_id_out) *first_id_out = first;
+    s.prepared = false;
+    s.uploaded = false;
+    return 0;
+}
+
+int mdx_state_n_atoms(mdx_state *st, int *n) {
+    ARG_CHECK(st && n, "null argument");
+    *n = (int)st->s->atoms.size();
+    return 0;
+}
+
+int mdx_state_set_velocities(mdx_state *st, int n, const int *ids, const double *vel) {
+    ARG_CHECK(st && ids && vel, "null argument");
+    State &s = *st->s;
+    for (int i = 0; i < n; i++) {
+        ARG_CHECK(ids[i] >= 0 && ids[i] < (int)s.atoms.size(), "atom id out of range");
+        for (int d = 0; d < 3; d++) s.atoms[ids[i]].vel[d] = vel[3 * i + d];
+    }
+    s.prepared = false;
+    return 0;
+}
+
+int mdx_state_get_atoms(mdx_state *st, double *pos, double *vel, double *force) {
+    ARG_CHECK(st, "null state");
+    State &s = *st->s;
+    GUARD(if (int e = s.download()) return e;)
+    for (size_t i = 0; i < s.atoms.size(); i++)
+        for (int d = 0; d < 3; d++) {
+            if (pos) pos[3 * i + d] = s.atoms[i].pos[d];
+            if (vel) vel[3 * i + d] = s.atoms[i].vel[d];
+            if (force) force[3 * i + d] = s.atoms[i].force[d];
+        }
+    return 0;
+}
+
+int mdx_state_put_atoms(mdx_state *st, const double *pos, const double *vel) {
+    ARG_CHECK(st, "null state");
+    State &s = *st->s;
+    if (!s.uploaded) {
+        set_error(MDX_ERR_STATE, "state has no device copy yet (call mdx_prepare or run first)");
+        return MDX_ERR_STATE;
+    }
+    const int n = s.gpd.n;
+    std::vector<uint32_t> ids(n);
+    std::vector<float4> xs(n), vs(n);
+    MDX_CUDA_TRY(cudaStreamSynchronize(s.stream));
+    MDX_CUDA_TRY(cudaMemcpy(ids.data(), s.gpd.ids.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    MDX_CUDA_TRY(cudaMemcpy(xs.data(), s.gpd.xs.p, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    MDX_CUDA_TRY(cudaMemcpy(vs.data(), s.gpd.vs.p, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; i++) {
+        const uint32_t id = ids[i];
+        if (pos) {
+            xs[i].x = (float)pos[3 * id];
+            xs[i].y = (float)pos[3 * id + 1];
+            xs[i].z = (float)pos[3 * id + 2];
+            for (int d = 0; d < 3; d++) s.atoms[id].pos[d] = pos[3 * id + d];
+        }
+        if (vel) {
+            vs[i].x = (float)vel[3 * id];
+            vs[i].y = (float)vel[3 * id + 1];
+            vs[i].z = (float)vel[3 * id + 2];
+            for (int d = 0; d < 3; d++) s.atoms[id].vel[d] = vel[3 * id + d];
+        }
+    }
+    MDX_CUDA_TRY(cudaMemcpy(s.gpd.xs.p, xs.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+    MDX_CUDA_TRY(cudaMemcpy(s.gpd.vs.p, vs.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+    return 0;
+}
+
+int mdx_state_activate_fix(mdx_state *st, mdx_fix *fix) {
+    ARG_CHECK(st && fix, "null argument");
+    State &s = *st->s;
+    ARG_CHECK(fix->owner == st, "fix belongs to another state");
+    if (std::find(s.fixes.begin(), s.fixes.end(), fix->f) != s.fixes.end()) return 0;
+    for (Fix *f : s.fixes)
+        if (f->kind == fix->f->kind) {
+            set_error(MDX_ERR_UNSUPPORTED, "only one fix of kind '%s' is supported per state", fix->f->type.c_str());
+            return MDX_ERR_UNSUPPORTED;
+        }
+    s.fixes.push_back(fix->f);
+    fix->f->active = true;
+    s.prepared = false;
+    return 0;
+}
+
+int mdx_state_deactivate_fix(mdx_state *st, mdx_fix *fix) {
+    ARG_CHECK(st && fix, "null argument");
+    State &s = *st->s;
+    auto it = std::find(s.fixes.begin(), s.fixes.end(), fix->f);
+    if (it != s.fixes.end()) s.fixes.erase(it);
+    fix->f->active = false;
+    s.prepared = false;
+    return 0;
+}
+
+int mdx_state_status(mdx_state *st, uint32_t *bits, uint32_t *max_neighbors, uint64_t *n_builds) {
+    ARG_CHECK(st, "null state");
+    State &s = *st->s;
+    if (!s.d_status.p) {
+        if (bits) *bits = 0;
+        if (max_neighbors) *max_neighbors = 0;
+        if (n_builds) *n_builds = 0;
+        return 0;
+    }
+    DeviceStatus h;
+    MDX_CUDA_TRY(cudaStreamSynchronize(s.stream));
+    MDX_CUDA_TRY(cudaMemcpy(&h, s.d_status.p, sizeof(h), cudaMemcpyDeviceToHost));
+    if (bits) *bits = h.bits;
+    if (max_neighbors) *max_neighbors = h.max_neighbors;
+    if (n_builds) *n_builds = h.n_builds;
+    return 0;
+}
+
+int mdx_state_set_stream(mdx_state *st, void *stream) {
+    ARG_CHECK(st, "null state");
+    State &s = *st->s;
+    if (s.stream && s.own_stream) cudaStreamDestroy(s.stream);
+    s.stream = (cudaStream_t)stream;
+    s.own_stream = stream == nullptr;
+    if (!s.stream) {
+        MDX_CUDA_TRY(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+        s.own_stream = true;
+    }
+    s.prepared = false;
+    return 0;
+}
+
+int mdx_state_synchronize(mdx_state *st) {
+    ARG_CHECK(st, "null state");
+    if (st->s->stream) MDX_CUDA_TRY(cudaStreamSynchronize(st->s->stream));
+    return 0;
+}
+
+// ---- fixes ---------------------------------------------------------------
+static int new_fix(mdx_state *st, Fix *f, mdx_fix **out) {
+    *out = new mdx_fix{f, st};
+    return 0;
+}
+
+int mdx_fix_lj_cut_create(mdx_state *st, const char *handle, const char *mixing, mdx_fix **out) {
+    ARG_CHECK(st && handle && out, "null argument");
+    std::string mix = mixing ? mixing : "geometric";
+    ARG_CHECK(mix == "geometric" || mix == "arithmetic", "mixing must be 'geometric' or 'arithmetic'");
+    return new_fix(st, new FixPair(st->s, handle, 1, mix), out);
+}
+
+int mdx_fix_wca_create(mdx_state *st, const char *handle, const char *mixing, mdx_fix **out) {
+    ARG_CHECK(st && handle && out, "null argument");
+    std::string mix = mixing ? mixing : "geometric";
+    ARG_CHECK(mix == "geometric" || mix == "arithmetic", "mixing must be 'geometric' or 'arithmetic'");
+    return new_fix(st, new FixPair(st->s, handle, 2, mix), out);
+}
+
+int mdx_fix_pair_set_parameter(mdx_fix *fix, const char *param, const char *ha, const char *hb, double value) {
+    ARG_CHECK(fix && param && ha && hb, "null argument");
+    ARG_CHECK(fix->f->kind == FixKind::Pair, "not a pair fix");
+    State &s = *fix->f->state;
+    int a = s.typeFromHandle(ha), b = s.typeFromHandle(hb);
+    if (a < 0 || b < 0) {
+        set_error(MDX_ERR_ARG, "unknown species handle '%s' or '%s'", ha, hb);
+        return MDX_ERR_ARG;
+    }
+    s.prepared = false;
+    return static_cast<FixPair *>(fix->f)->setParameter(param, a, b, value);
+}
+
+int mdx_fix_charge_ewald_create(mdx_state *st, const char *handle, const char *group, mdx_fix **out) {
+    ARG_CHECK(st && handle && out, "null argument");
+    return new_fix(st, new FixChargeEwald(st->s, handle, group ? group : "all"), out);
+}
+
+int mdx_fix_charge_ewald_set_parameters(mdx_fix *fix, int nx, int ny, int nz, double rcut, int order) {
+    ARG_CHECK(fix && fix->f->kind == FixKind::ChargeEwald, "not a FixChargeEwald");
+    fix->f->state->prepared = false;
+    return static_cast<FixChargeEwald *>(fix->f)->setParameters(nx, ny, nz, rcut, order);
+}
+
+int mdx_fix_charge_ewald_set_alpha(mdx_fix *fix, double alpha) {
+    ARG_CHECK(fix && fix->f->kind == FixKind::ChargeEwald, "not a FixChargeEwald");
+    static_cast<FixChargeEwald *>(fix->f)->alpha_user = alpha;
+    fix->f->state->prepared = false;
+    return 0;
+}
+
+int mdx_fix_charge_ewald_get_alpha(mdx_fix *fix, double *alpha) {
+    ARG_CHECK(fix && alpha && fix->f->kind == FixKind::ChargeEwald, "not a FixChargeEwald");
+    FixChargeEwald *f = static_cast<FixChargeEwald *>(fix->f);
+    if (!f->prepared) {
+        State &s = *f->state;
+        s.setBox();
+        if (f->r_cut < 0) f->r_cut = s.rCut;
+        *alpha = f->alpha_user > 0 ? f->alpha_user : f->findAlpha();
+        return 0;
+    }
+    *alpha = f->alpha;
+    return 0;
+}
+
+int mdx_fix_e3b_create(mdx_state *st, const char *handle, const char *style, mdx_fix **out) {
+    ARG_CHECK(st && handle && out, "null argument");
+    std::string sty = style ? style : "E3B3";
+    ARG_CHECK(sty == "E3B3" || sty == "E3B2", "FixE3B requires the style argument to be either 'E3B3' or 'E3B2'");
+    return new_fix(st, new FixE3B(st->s, handle, sty), out);
+}
+
+int mdx_fix_e3b_add_molecule(mdx_fix *fix, int o, int h1, int h2, int m) {
+    ARG_CHECK(fix && fix->f->kind == FixKind::E3B, "not a FixE3B");
+    State &s = *fix->f->state;
+    const int n = (int)s.atoms.size();
+    ARG_CHECK(o >= 0 && h1 >= 0 && h2 >= 0 && m >= 0 && o < n && h1 < n && h2 < n && m < n, "atom id out of range");
+    const double mo = s.atoms[o].mass, m1 = s.atoms[h1].mass, m2 = s.atoms[h2].mass, mm = s.atoms[m].mass;
+    ARG_CHECK(mo > m1 && mo > m2 && m1 == m2 && m1 > mm, "Ids in FixE3B::addMolecule must be as O, H1, H2, M");
+    static_cast<FixE3B *>(fix->f)->mol_ids.push_back(make_int4(o, h1, h2, m));
+    s.prepared = false;
+    return 0;
+}
+
+int mdx_fix_rigid_create(mdx_state *st, const char *handle, const char *style, mdx_fix **out) {
+    ARG_CHECK(st && handle && style && out, "null argument");
+    std::string sty(style);
+    ARG_CHECK(sty == "TIP4P/2005" || sty == "TIP4P" || sty == "TIP3P" || sty == "SPC" || sty == "SPC/E",
+              "Unsupported style argument passed to the Rigid fix");
+    return new_fix(st, new FixRigid(st->s, handle, sty), out);
+}
+
+int mdx_fix_rigid_create_rigid(mdx_fix *fix, int o, int h1, int h2, int m) {
+    ARG_CHECK(fix && fix->f->kind == FixKind::Rigid, "not a FixRigid");
+    fix->f->state->prepared = false;
+    return static_cast<FixRigid *>(fix->f)->createRigid(o, h1, h2, m);
+}
+
+int mdx_fix_nose_hoover_create(mdx_state *st, const char *handle, const char *group, mdx_fix **out) {
+    ARG_CHECK(st && handle && out, "null argument");
+    std::string g = group ? group : "all";
+    if (g != "all") {
+        set_error(MDX_ERR_UNSUPPORTED, "FixNoseHoover groups other than 'all' are not implemented");
+        return MDX_ERR_UNSUPPORTED;
+    }
+    return new_fix(st, new FixNoseHoover(st->s, handle, g), out);
+}
+
+int mdx_fix_nose_hoover_set_temperature(mdx_fix *fix, double T, double tau) {
+    ARG_CHECK(fix && fix->f->kind == FixKind::NoseHoover, "not a FixNoseHoover");
+    fix->f->state->prepared = false;
+    return static_cast<FixNoseHoover *>(fix->f)->setTemperature(T, tau);
+}
+
+int mdx_fix_destroy(mdx_fix *fix) {
+    if (!fix) return 0;
+    State &s = *fix->f->state;
+    auto it = std::find(s.fixes.begin(), s.fixes.end(), fix->f);
+    if (it != s.fixes.end()) s.fixes.erase(it);
+    s.prepared = false;
+    delete fix->f;
+    delete fix;
+    return 0;
+}
+
+// ---- stage level ---------------------------------------------------------
+int mdx_prepare(mdx_state *st) {
+    ARG_CHECK(st, "null state");
+    GUARD(return st->s->prepare();)
+}
+
+static int need_prepared(State &s) {
+    if (!s.prepared) {
+        set_error(MDX_ERR_STATE, "call mdx_prepare (or run) first");
+        return MDX_ERR_STATE;
+    }
+    return 0;
+}
+
+int mdx_nlist_build(mdx_state *st, int force_build) {
+    ARG_CHECK(st, "null state");
+    State &s = *st->s;
+    if (int e = need_prepared(s)) return e;
+    GUARD(if (int e = nlist_rebuild(s, force_build != 0, false)) return e;
+          MDX_CUDA_TRY(cudaStreamSynchronize(s.stream)); return s.checkStatus();)
+}
+
+int mdx_nlist_get(mdx_state *st, int max_per_atom, int *counts, int *nbr, int *tags) {
+    ARG_CHECK(st && counts && nbr && max_per_atom > 0, "null argument");
+    State &s = *st->s;
+    if (int e = need_prepared(s)) return e;
+    const int n = s.gpd.n;
+    GridGPU &g = s.grid;
+    const int G = 32 / g.team;
+    const size_t groups = (size_t)(n + G - 1) / G;
+    std::vector<uint32_t> cnt(n), list(groups * g.cap * G), ids(n);
+    MDX_CUDA_TRY(cudaStreamSynchronize(s.stream));
+    MDX_CUDA_TRY(cudaMemcpy(cnt.data(), g.counts.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    MDX_CUDA_TRY(cudaMemcpy(list.data(), g.nlist.p, list.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    MDX_CUDA_TRY(cudaMemcpy(ids.data(), s.gpd.ids.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; i++) {
+        const uint32_t id = ids[i];
+        const int c = (int)std::min<uint32_t>(cnt[i], (uint32_t)g.cap);
+        if (c > max_per_atom || (int)cnt[i] > g.cap) {
+            set_error(MDX_ERR_OVERFLOW, "atom %u has %u neighbours (> %d)", id, cnt[i], std::min(max_per_atom, g.cap));
+            return MDX_ERR_OVERFLOW;
+        }
+        std::vector<std::pair<int, int>> row(c);
+        const size_t base = (size_t)(i / G) * g.cap * G + (i % G) * g.team;
+        for (int k = 0; k < c; k++) {
+            const uint32_t e = list[base + (size_t)(k / g.team) * 32 + (k % g.team)];
+            row[k] = {(int)ids[e & kExclMask], (int)(e >> 30)};
+        }
+        std::sort(row.begin(), row.end());
+        counts[id] = c;
+        for (int k = 0; k < c; k++) {
+            nbr[(size_t)id * max_per_atom + k] = row[k].first;
+            if (tags) tags[(size_t)id * max_per_atom + k] = row[k].second;
+        }
+    }
+    return 0;
+}
+
+int mdx_compute_forces(mdx_state *st, int virial_mode) {
+    ARG_CHECK(st, "null state");
+    State &s = *st->s;
+    if (int e = need_prepared(s)) return e;
+    GUARD(if (int e = s.computeForces(virial_mode)) return e; MDX_CUDA_TRY(cudaStreamSynchronize(s.stream));
+          return s.checkStatus();)
+}
+
+int mdx_potential_energy(mdx_state *st, double out[4]) {
+    ARG_CHECK(st && out, "null argument");
+    State &s = *st->s;
+    if (int e = need_prepared(s)) return e;
+    out[0] = out[1] = out[2] = out[3] = 0.0;
+    GUARD(if (FixPair *p = s.pairFix()) {
+        if (int e = pair_energy(s, *p, &out[0])) return e;
+    } if (FixChargeEwald *ew = s.ewaldFix()) {
+        if (int e = ewald_recip_energy(s, *ew, &out[1])) return e;
+    } if (FixE3B *e3 = s.e3bFix()) {
+        double e23[2];
+        if (int e = e3b_energy(s, *e3, e23)) return e;
+        out[2] = e23[0];
+        out[3] = e23[1];
+    } return 0;)
+}
+
+int mdx_kinetic(mdx_state *st, double *sum_mv2, double *ndf) {
+    ARG_CHECK(st, "null state");
+    State &s = *st->s;
+    if (int e = need_prepared(s)) return e;
+    if (sum_mv2)
+        if (int e = kinetic_sum(s, sum_mv2)) return e;
+    if (ndf) {
+        double n = 0;
+        for (auto &a : s.atoms) n += a.ndf;
+        *ndf = n;
+    }
+    return 0;
+}
+
+int mdx_get_virials(mdx_state *st, double *per_atom, double sum6[6]) {
+    ARG_CHECK(st, "null state");
+    State &s = *st->s;
+    if (int e = need_prepared(s)) return e;
+    if (sum6)
+        if (int e = virial_sum(s, sum6)) return e;
+    if (per_atom) {
+        const int n = s.gpd.n;
+        std::vector<float> v(6 * (size_t)n);
+        std::vector<uint32_t> ids(n);
+        MDX_CUDA_TRY(cudaStreamSynchronize(s.stream));
+        MDX_CUDA_TRY(cudaMemcpy(v.data(), s.gpd.virials.p, v.size() * sizeof(float), cudaMemcpyDeviceToHost));
+        MDX_CUDA_TRY(cudaMemcpy(ids.data(), s.gpd.ids.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < n; i++)
+            for (int c = 0; c < 6; c++) per_atom[6 * (size_t)ids[i] + c] = v[6 * (size_t)i + c];
+    }
+    return 0;
+}
+
+static FixRigid *rigid_of(mdx_state *st, mdx_fix *fix) {
+    if (!st || !fix || fix->f->kind != FixKind::Rigid) return nullptr;
+    return static_cast<FixRigid *>(fix->f);
+}
+
+#define RIGID_HOOK(name, which)                                                    \
+    int name(mdx_state *st, mdx_fix *fix) {                                        \
+        FixRigid *r = rigid_of(st, fix);                                           \
+        ARG_CHECK(r, "not a FixRigid");                                            \
+        if (int e = need_prepared(*st->s)) return e;                               \
+        if (int e = rigid_hook(*st->s, *r, which)) return e;                       \
+        MDX_CUDA_TRY(cudaStreamSynchronize(st->s->stream));                        \
+        return st->s->checkStatus();                                               \
+    }
+RIGID_HOOK(mdx_rigid_save_prev, 0)
+RIGID_HOOK(mdx_rigid_settle_positions, 1)
+RIGID_HOOK(mdx_rigid_distribute_msite, 2)
+RIGID_HOOK(mdx_rigid_settle_velocities, 3)
+
+int mdx_verlet_first_half(mdx_state *st) {
+    ARG_CHECK(st, "null state");
+    if (int e = need_prepared(*st->s)) return e;
+    State &s = *st->s;
+    // nve_v + nve_x on every atom, the reference's unfused kernels
+    FixRigid *r = s.rigidFix();
+    FixNoseHoover *nh = s.nhFix();
+    std::vector<Fix *> saved = s.fixes;
+    // run the hook-mode first half without NH/rigid extras
+    s.fixes.erase(std::remove_if(s.fixes.begin(), s.fixes.end(),
+                                 [&](Fix *f) { return f == r || f == nh; }),
+                  s.fixes.end());
+    int e = step_first_half(s, false);
+    s.fixes = saved;
+    if (e) return e;
+    MDX_CUDA_TRY(cudaStreamSynchronize(s.stream));
+    return 0;
+}
+
+int mdx_verlet_second_half(mdx_state *st) {
+    ARG_CHECK(st, "null state");
+    if (int e = need_prepared(*st->s)) return e;
+    State &s = *st->s;
+    FixRigid *r = s.rigidFix();
+    FixNoseHoover *nh = s.nhFix();
+    std::vector<Fix *> saved = s.fixes;
+    s.fixes.erase(std::remove_if(s.fixes.begin(), s.fixes.end(),
+                                 [&](Fix *f) { return f == r || f == nh; }),
+                  s.fixes.end());
+    int e = step_second_half(s, false);
+    s.fixes = saved;
+    if (e) return e;
+    MDX_CUDA_TRY(cudaStreamSynchronize(s.stream));
+    return 0;
+}
+
+int mdx_time_stage(mdx_state *st, int stage, int iters, size_t flush_bytes, double *avg_ms) {
+    ARG_CHECK(st && avg_ms && iters > 0, "bad argument");
+    State &s = *st->s;
+    if (int e = need_prepared(s)) return e;
+    DBuf<char> flush;
+    if (flush_bytes)
+        if (int e = flush.alloc(flush_bytes)) return e;
+    std::vector<cudaEvent_t> ev(2 * iters);
+    for (auto &e : ev) MDX_CUDA_TRY(cudaEventCreate(&e));
+    for (int k = 0; k < iters; k++) {
+        if (flush_bytes) MDX_CUDA_TRY(cudaMemsetAsync(flush.p, k & 0xff, flush_bytes, s.stream));
+        MDX_CUDA_TRY(cudaEventRecord(ev[2 * k], s.stream));
+        int e = 0;
+        switch (stage) {
+            case 0: {
+                FixPair *p = s.pairFix();
+                ARG_CHECK(p, "no pair fix");
+                e = pair_launch(s, *p, 0, false);
+                break;
+            }
+            case 1: {
+                FixChargeEwald *w = s.ewaldFix();
+                ARG_CHECK(w, "no FixChargeEwald");
+                e = w->compute(0);
+                break;
+            }
+            case 2: {
+                FixE3B *f = s.e3bFix();
+                ARG_CHECK(f, "no FixE3B");
+                e = e3b_forces(s, *f);
+                break;
+            }
+            case 3: e = nlist_rebuild(s, true, false); break;
+            case 4: e = step_first_half(s, true); break;
+            case 5: e = step_second_half(s, true); break;
+            default: ARG_CHECK(false, "unknown stage");
+        }
+        if (e) return e;
+        MDX_CUDA_TRY(cudaEventRecord(ev[2 * k + 1], s.stream));
+    }
+    MDX_CUDA_TRY(cudaStreamSynchronize(s.stream));
+    double tot = 0.0;
+    for (int k = 0; k < iters; k++) {
+        float ms = 0.f;
+        MDX_CUDA_TRY(cudaEventElapsedTime(&ms, ev[2 * k], ev[2 * k + 1]));
+        tot += ms;
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    *avg_ms = tot / iters;
+    return s.checkStatus();
+}
+
+int mdx_pair_force_raw(int n, const float *xs4, float *fs4, const float *qs, const uint32_t *counts,
+                       const uint32_t *nlist, int team, int cap, const float *params, int ntypes, const double lo[3],
+                       const double hi[3], const float coef[3], int lj_kind, float qrc, float alpha, float qqr_to_eng,
+                       float *virials, int accumulate, void *stream) {
+    ARG_CHECK(n >= 0 && xs4 && fs4 && counts && nlist && lo && hi && coef, "null argument");
+    ARG_CHECK(lj_kind == 0 || params, "params required for LJ/WCA");
+    ARG_CHECK(qrc <= 0.f || qs, "charges required for the Ewald term");
+    ARG_CHECK(team == 1 || team == 2 || team == 4 || team == 8 || team == 16 || team == 32, "team must be a power of two <= 32");
+    ARG_CHECK(cap > 0 && cap % team == 0, "cap must be a positive multiple of team");
+    Box b;
+    b.lod = make_double3(lo[0], lo[1], lo[2]);
+    b.Ld = make_double3(hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]);
+    b.invLd = make_double3(1.0 / b.Ld.x, 1.0 / b.Ld.y, 1.0 / b.Ld.z);
+    b.lo = make_float3((float)lo[0], (float)lo[1], (float)lo[2]);
+    b.L = make_float3((float)b.Ld.x, (float)b.Ld.y, (float)b.Ld.z);
+    b.invL = make_float3(1.0f / b.L.x, 1.0f / b.L.y, 1.0f / b.L.z);
+    GUARD(return pair_force_raw(n, (const float4 *)xs4, (float4 *)fs4, qs, counts, nlist, team, cap, params, ntypes, b,
+                                coef, lj_kind, qrc, alpha, qqr_to_eng, virials, accumulate != 0,
+                                (cudaStream_t)stream);)
+}
+
+}  // extern "C"

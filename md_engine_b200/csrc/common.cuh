@@ -1,0 +1,101 @@
+// Shared device/host helpers for the B200 force hot path.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <math.h>
+
+#include "mdx.h"
+
+namespace mdx {
+
+// Exclusion tag bits of a neighbour entry (bits 30-31 = depth 1..3), the
+// same packing as the reference's EXCL_MASK (globalDefs.h:40).
+constexpr uint32_t kExclMask = ~(3u << 30);
+// Inverse-mass sentinel for massless sites and its threshold
+// (globalDefs.h:37-38: INVMASSLESS 1e30, INVMASSBOOL 1e18).
+constexpr float kInvMassless = 1.0e30f;
+constexpr float kInvMassBool = 1.0e18f;
+
+// Device status word bits (written with atomicOr, read by the host between
+// runs; nothing here traps or waits on the device).
+enum StatusBits : uint32_t {
+    kStatusNlistOverflow = 1u << 0,   // an atom had more neighbours than the list capacity
+    kStatusMolOverflow   = 1u << 1,   // molecule (E3B) list overflow
+    kStatusNanForce      = 1u << 2,   // non-finite force seen
+    kStatusSettleFail    = 1u << 3,   // SETTLE cos^2 <= 0 (degenerate triangle)
+    kStatusConstraint    = 1u << 4,   // bond length drift beyond tolerance
+    kStatusBoxTooSmall   = 1u << 5,   // cut + skin >= half box
+    kStatusP3MMiss       = 1u << 6,   // charge assignment stencil out of grid
+};
+
+struct DeviceStatus {
+    uint32_t bits;
+    uint32_t max_neighbors;      // largest per-atom count seen at the last build
+    uint32_t max_mol_neighbors;  // largest per-molecule count seen
+    uint32_t rebuild;            // 1 when the current step rebuilds the list
+    uint64_t n_builds;           // number of list builds executed on device
+    int64_t turn;                // device-side turn counter
+};
+
+// Box, the analogue of BoundsGPU (BoundsGPU.h) for a fully periodic
+// orthorhombic box.  Float and double copies so that the SETTLE kernels can
+// take minimum images in FP64 (BoundsGPU.h:102-108).
+struct Box {
+    float3 lo, L, invL;
+    double3 lod, Ld, invLd;
+};
+
+__host__ __device__ inline float3 f3(float4 a) { return make_float3(a.x, a.y, a.z); }
+__host__ __device__ inline float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__host__ __device__ inline float3 operator-(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__host__ __device__ inline float3 operator*(float3 a, float s) { return make_float3(a.x * s, a.y * s, a.z * s); }
+__host__ __device__ inline float3 operator*(float s, float3 a) { return make_float3(a.x * s, a.y * s, a.z * s); }
+__host__ __device__ inline void operator+=(float3 &a, float3 b) { a.x += b.x; a.y += b.y; a.z += b.z; }
+__host__ __device__ inline void operator-=(float3 &a, float3 b) { a.x -= b.x; a.y -= b.y; a.z -= b.z; }
+__host__ __device__ inline float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+__host__ __device__ inline double3 d3(float4 a) { return make_double3(a.x, a.y, a.z); }
+__host__ __device__ inline double3 operator+(double3 a, double3 b) { return make_double3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__host__ __device__ inline double3 operator-(double3 a, double3 b) { return make_double3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__host__ __device__ inline double3 operator*(double3 a, double s) { return make_double3(a.x * s, a.y * s, a.z * s); }
+__host__ __device__ inline double3 operator*(double s, double3 a) { return make_double3(a.x * s, a.y * s, a.z * s); }
+__host__ __device__ inline void operator+=(double3 &a, double3 b) { a.x += b.x; a.y += b.y; a.z += b.z; }
+__host__ __device__ inline void operator-=(double3 &a, double3 b) { a.x -= b.x; a.y -= b.y; a.z -= b.z; }
+__host__ __device__ inline void operator/=(double3 &a, double s) { a.x /= s; a.y /= s; a.z /= s; }
+__host__ __device__ inline double dotd(double3 a, double3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__host__ __device__ inline double lend(double3 a) { return sqrt(dotd(a, a)); }
+__host__ __device__ inline double3 crossd(double3 a, double3 b) {
+    return make_double3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+
+// minimum image (BoundsGPU::minImage, BoundsGPU.h:91-108)
+__device__ inline float3 min_image(const Box &b, float3 v) {
+    v.x -= b.L.x * rintf(v.x * b.invL.x);
+    v.y -= b.L.y * rintf(v.y * b.invL.y);
+    v.z -= b.L.z * rintf(v.z * b.invL.z);
+    return v;
+}
+__device__ inline double3 min_image(const Box &b, double3 v) {
+    v.x -= b.Ld.x * rint(v.x * b.invLd.x);
+    v.y -= b.Ld.y * rint(v.y * b.invLd.y);
+    v.z -= b.Ld.z * rint(v.z * b.invLd.z);
+    return v;
+}
+
+__device__ inline int type_of(float4 x) { return __float_as_int(x.w); }
+
+}  // namespace mdx
+
+#define MDX_CUDA_TRY(expr)                                                     \
+    do {                                                                       \
+        cudaError_t _e = (expr);                                               \
+        if (_e != cudaSuccess) {                                               \
+            ::mdx::set_error(MDX_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, \
+                             #expr, cudaGetErrorString(_e));                   \
+            return MDX_ERR_CUDA;                                               \
+        }                                                                      \
+    } while (0)
+
+namespace mdx {
+void set_error(int code, const char *fmt, ...);
+}

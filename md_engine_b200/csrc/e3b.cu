@@ -1,0 +1,463 @@
+// E3B three-body water term (FixE3B, src/Fixes/FixE3B.cu; kernels
+// src/Evaluators/ThreeBodyE3B.h:18-549; maths src/Evaluators/EvaluatorE3B.h).
+//
+// The reference rebuilds a private molecule grid + neighbour list every step
+// (FixE3B::handleLocalData, FixE3B.cu:349-406: 3 host syncs + 7 memsets),
+// writes five per-pair scratch arrays in a two-body kernel and combines them
+// with 18 float atomics per pair in a three-body kernel.  Here:
+//  * the molecule list (O-O within rf + 1 A + skin) is cut from the atom list
+//    whenever the atom list is rebuilt (same skin criterion, so it holds every
+//    pair within the reference's 6.2 A list radius at every step);
+//  * pass 1 (k_e3b_totals): each molecule sums its own e3bTotals over its FULL
+//    list -- no atomics -- and adds the O-O two-body force;
+//  * pass 2 (k_e3b_forces): each molecule re-evaluates the four switched
+//    O-H exponentials of every pair within RMAX_E3B and keeps the forces that
+//    land on its own three atoms, evaluating EvaluatorE3B::threeBodyPairForce
+//    with the lower index as molecule "1" exactly as the reference's i<j
+//    ordering; no scratch arrays, no atomics, deterministic.
+#include <cstdio>
+
+#include "engine.hpp"
+
+namespace mdx {
+
+namespace {
+
+template <int T>
+__device__ __forceinline__ float tsum(float v) {
+#pragma unroll
+    for (int o = T / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// switching(r), dswitchdr(r) (EvaluatorE3B.h:91-115)
+__device__ __forceinline__ float e3b_sw(const E3BParams &p, float r) {
+    if (r <= p.rs) return 1.0f;
+    if (r > p.rf) return 0.0f;
+    float v = (p.rf - r);
+    v *= v;
+    v *= ((p.rf + (2.0f * r) - p.rstimes3) * p.rfminusrs_cubed_inv);
+    return v;
+}
+__device__ __forceinline__ float e3b_dsw(const E3BParams &p, float r) {
+    if (r <= p.rs || r > p.rf) return 0.0f;
+    return 6.0f * (p.rf - r) * (p.rs - r) * p.rfminusrs_cubed_inv;
+}
+// threeBodyPairEnergy(r) and threeBodyForce(dr, r) (EvaluatorE3B.h:117-141)
+__device__ __forceinline__ void e3b_ef(const E3BParams &p, float3 dr, float &e, float3 &f) {
+    const float r = sqrtf(dot3(dr, dr));
+    const float es = expf(-p.k3 * r);
+    const float sw = e3b_sw(p, r);
+    e = sw * es;
+    f = make_float3(0.f, 0.f, 0.f);
+    if (r <= p.rf) {
+        float s = p.k3 * es / r;
+        if (r > p.rs) {
+            s *= sw;
+            s -= (es * e3b_dsw(p, r) / r);
+        }
+        f = dr * s;
+    }
+}
+
+struct MolPos {
+    float3 a, b, c;  // O, H1, H2
+};
+
+__device__ __forceinline__ MolPos load_mol(const float4 *__restrict__ xs, int4 ix) {
+    MolPos m;
+    m.a = f3(__ldg(xs + ix.x));
+    m.b = f3(__ldg(xs + ix.y));
+    m.c = f3(__ldg(xs + ix.z));
+    return m;
+}
+
+// geometry of the pair with molecule 1 = m1 and 2 = m2 (ThreeBodyE3B.h:128-176)
+struct PairGeom {
+    float es[4];     // e_b2a1, e_c2a1, e_b1a2, e_c1a2
+    float3 fv[4];    // forces_b2a1, c2a1, b1a2, c1a2
+};
+__device__ __forceinline__ void pair_geom(const E3BParams &p, const Box &box, const MolPos &m1, const MolPos &m2,
+                                          PairGeom &g) {
+    e3b_ef(p, min_image(box, m2.b - m1.a), g.es[0], g.fv[0]);
+    e3b_ef(p, min_image(box, m2.c - m1.a), g.es[1], g.fv[1]);
+    e3b_ef(p, min_image(box, m1.b - m2.a), g.es[2], g.fv[2]);
+    e3b_ef(p, min_image(box, m1.c - m2.a), g.es[3], g.fv[3]);
+}
+
+// EvaluatorE3B::threeBodyPairForce (EvaluatorE3B.h:145-249); returns the
+// forces on molecule 1's atoms (first) or molecule 2's atoms (!first)
+__device__ __forceinline__ void pair_force(const E3BParams &p, const PairGeom &g, float4 T1, float4 T2, bool first,
+                                           float3 &fa, float3 &fb, float3 &fc) {
+    const float *e = g.es;
+    float3 a1 = make_float3(0.f, 0.f, 0.f), b1 = a1, c1 = a1, a2 = a1, b2 = a1, c2 = a1;
+    float3 fj;
+    float sc;
+    // type A
+    sc = p.Ea * (T2.y - e[0]);
+    fj = sc * g.fv[1]; a1 -= fj; c2 += fj;
+    sc = p.Ea * (T1.y - e[2]);
+    fj = sc * g.fv[3]; a2 -= fj; c1 += fj;
+    sc = p.Ea * (T2.z - e[1]);
+    fj = sc * g.fv[0]; a1 -= fj; b2 += fj;
+    sc = p.Ea * (T1.z - e[3]);
+    fj = sc * g.fv[2]; a2 -= fj; b1 += fj;
+    // type B
+    sc = p.Eb * (T2.x + T1.y + T1.z - 2.0f * (e[2] + e[3]));
+    fj = sc * g.fv[0]; a1 -= fj; b2 += fj;
+    fj = sc * g.fv[1]; a1 -= fj; c2 += fj;
+    sc = p.Eb * (T1.x + T2.y + T2.z - 2.0f * (e[0] + e[1]));
+    fj = sc * g.fv[2]; a2 -= fj; b1 += fj;
+    fj = sc * g.fv[3]; a2 -= fj; c1 += fj;
+    // type C
+    sc = p.Ec * (T1.x - e[1] - e[0]);
+    fj = sc * g.fv[0]; a1 -= fj; b2 += fj;
+    fj = sc * g.fv[1]; a1 -= fj; c2 += fj;
+    sc = p.Ec * (T2.x - e[2] - e[3]);
+    fj = sc * g.fv[2]; a2 -= fj; b1 += fj;
+    fj = sc * g.fv[3]; a2 -= fj; c1 += fj;
+    if (first) { fa = a1; fb = b1; fc = c1; }
+    else { fa = a2; fb = b2; fc = c2; }
+}
+
+// total three-body energy of one unordered pair (EvaluatorE3B.h:251-345)
+__device__ __forceinline__ float pair_energy(const E3BParams &p, const float *e, float4 T1, float4 T2) {
+    float s = 0.f, sc;
+    sc = p.Ea * (T2.y - e[0]); s += 0.5f * sc * e[1];
+    sc = p.Ea * (T1.y - e[2]); s += 0.5f * sc * e[3];
+    sc = p.Ea * (T2.z - e[1]); s += 0.5f * sc * e[0];
+    sc = p.Ea * (T1.z - e[3]); s += 0.5f * sc * e[2];
+    sc = p.Eb * (T2.x + T1.y + T1.z - 2.0f * (e[2] + e[3])); s += 0.5f * sc * (e[0] + e[1]);
+    sc = p.Eb * (T1.x + T2.y + T2.z - 2.0f * (e[0] + e[1])); s += 0.5f * sc * (e[2] + e[3]);
+    sc = p.Ec * (T1.x - e[1] - e[0]); s += 0.5f * sc * (e[0] + e[1]);
+    sc = p.Ec * (T2.x - e[2] - e[3]); s += 0.5f * sc * (e[2] + e[3]);
+    return s;
+}
+
+// updateMoleculeIdxsMap (FixE3B.cu:41-65) + molecule list cut from the atom
+// list: O-O pairs with r^2 < (rf + 1 + skin)^2.  Team of T lanes per molecule.
+template <int T>
+__global__ void k_e3b_list(int nmol, const int4 *__restrict__ mol_ids, int4 *__restrict__ mol_idx,
+                           const int *__restrict__ idToIdx, const int *__restrict__ mol_of_id,
+                           const uint32_t *__restrict__ ids, const float4 *__restrict__ xs,
+                           const uint32_t *__restrict__ counts, const uint32_t *__restrict__ nlist, int team_atom,
+                           int cap_atom, Box box, float cut2, uint32_t *__restrict__ mcounts,
+                           uint32_t *__restrict__ mlist, int mcap, DeviceStatus *st, int conditional) {
+    if (conditional && !st->rebuild) return;
+    constexpr int G = 32 / T;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int a = lane / T, t = lane % T;
+    const int m = warp * G + a;
+    if (m >= nmol) return;
+    const unsigned team_mask = (T == 32) ? 0xffffffffu : (((1u << T) - 1u) << (a * T));
+    const int4 id4 = mol_ids[m];
+    const int4 ix = make_int4(idToIdx[id4.x], idToIdx[id4.y], idToIdx[id4.z], id4.w >= 0 ? idToIdx[id4.w] : -1);
+    if (t == 0) mol_idx[m] = ix;
+    const int oi = ix.x;
+    const float3 po = f3(xs[oi]);
+    int cnt = (int)counts[oi];
+    cnt = cnt < cap_atom ? cnt : cap_atom;
+    const int Ga = 32 / team_atom;
+    const uint32_t *row = nlist + (size_t)(oi / Ga) * cap_atom * Ga + (oi % Ga) * team_atom;
+    uint32_t *mrow = mlist + (size_t)(m / G) * mcap * G + a * T;
+    int mc = 0;
+    for (int k0 = 0; k0 < cnt; k0 += T) {
+        const int k = k0 + t;
+        bool hit = false;
+        int mj = -1;
+        if (k < cnt) {
+            const uint32_t e = row[(size_t)(k / team_atom) * 32 + (k % team_atom)];
+            const int j = (int)(e & kExclMask);
+            mj = mol_of_id[ids[j]];
+            if (mj >= 0 && mj != m) {
+                const float3 d = min_image(box, po - f3(xs[j]));
+                hit = dot3(d, d) < cut2;
+            }
+        }
+        const unsigned b = __ballot_sync(team_mask, hit);
+        if (hit) {
+            const unsigned mine = (T == 32) ? b : (b >> (a * T));
+            const int pos = mc + __popc(mine & ((1u << t) - 1u));
+            if (pos < mcap) mrow[(size_t)(pos / T) * 32 + (pos % T)] = (uint32_t)mj;
+        }
+        mc += __popc(b);
+    }
+    if (t == 0) {
+        mcounts[m] = (uint32_t)mc;
+        if (mc > mcap) atomicOr(&st->bits, kStatusMolOverflow);
+        atomicMax(&st->max_mol_neighbors, (uint32_t)mc);
+    }
+}
+
+// pass 1: e3bTotals of molecule i (ThreeBodyE3B.h:170-211 summed from i's own
+// full list) and the O-O two-body force (EvaluatorE3B::twoBodyForce, :67-78)
+template <int T, bool ENERGY>
+__global__ void k_e3b_totals(int nmol, const int4 *__restrict__ mol_idx, const float4 *__restrict__ xs,
+                             float4 *__restrict__ fs, const uint32_t *__restrict__ mcounts,
+                             const uint32_t *__restrict__ mlist, int mcap, Box box, E3BParams p,
+                             float4 *__restrict__ totals, double *__restrict__ e2_out) {
+    constexpr int G = 32 / T;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int a = lane / T, t = lane % T;
+    const int m = warp * G + a;
+    const bool valid = m < nmol;
+    float fx = 0.f, fy = 0.f, fz = 0.f, tx = 0.f, ty = 0.f, tz = 0.f, e2 = 0.f;
+    int4 ix = make_int4(0, 0, 0, 0);
+    if (valid) {
+        ix = mol_idx[m];
+        const MolPos mi = load_mol(xs, ix);
+        int cnt = (int)mcounts[m];
+        cnt = cnt < mcap ? cnt : mcap;
+        const uint32_t *row = mlist + (size_t)(m / G) * mcap * G + a * T + t;
+        for (int k = t; k < cnt; k += T) {
+            const int mj = (int)row[(size_t)(k / T) * 32];
+            const int4 jx = __ldg(mol_idx + mj);
+            const float3 oj = f3(__ldg(xs + jx.x));
+            const float3 dr = min_image(box, mi.a - oj);
+            const float r2 = dot3(dr, dr);
+            if (r2 >= p.list_cut2) continue;
+            const float r = sqrtf(r2);
+            const float ex = expf(-p.k2 * r);
+            const float s = p.k2 * p.E2 * ex / r;
+            fx += dr.x * s;
+            fy += dr.y * s;
+            fz += dr.z * s;
+            if (ENERGY) e2 += 0.5f * p.E2 * ex;
+            if (r <= p.rmax) {
+                MolPos mj_;
+                mj_.a = oj;
+                mj_.b = f3(__ldg(xs + jx.y));
+                mj_.c = f3(__ldg(xs + jx.z));
+                float e;
+                float3 f;
+                e3b_ef(p, min_image(box, mj_.b - mi.a), e, f);
+                tx += e;
+                e3b_ef(p, min_image(box, mj_.c - mi.a), e, f);
+                tx += e;
+                e3b_ef(p, min_image(box, mi.b - mj_.a), e, f);
+                ty += e;
+                e3b_ef(p, min_image(box, mi.c - mj_.a), e, f);
+                tz += e;
+            }
+        }
+    }
+    if (ENERGY) {
+        e2 = tsum<T>(e2);
+        if (valid && t == 0) atomicAdd(e2_out, (double)e2);
+        return;
+    }
+    fx = tsum<T>(fx);
+    fy = tsum<T>(fy);
+    fz = tsum<T>(fz);
+    tx = tsum<T>(tx);
+    ty = tsum<T>(ty);
+    tz = tsum<T>(tz);
+    if (valid && t == 0) {
+        totals[m] = make_float4(tx, ty, tz, 0.f);
+        float4 f = fs[ix.x];
+        f.x += fx;
+        f.y += fy;
+        f.z += fz;
+        fs[ix.x] = f;
+    }
+}
+
+// pass 2: three-body forces on molecule i's O, H1, H2 (ThreeBodyE3B.h:255-549)
+template <int T, bool ENERGY>
+__global__ void k_e3b_forces(int nmol, const int4 *__restrict__ mol_idx, const float4 *__restrict__ xs,
+                             float4 *__restrict__ fs, const uint32_t *__restrict__ mcounts,
+                             const uint32_t *__restrict__ mlist, int mcap, Box box, E3BParams p,
+                             const float4 *__restrict__ totals, double *__restrict__ e3_out) {
+    constexpr int G = 32 / T;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int a = lane / T, t = lane % T;
+    const int m = warp * G + a;
+    const bool valid = m < nmol;
+    float3 fa = make_float3(0.f, 0.f, 0.f), fb = fa, fc = fa;
+    float e3 = 0.f;
+    int4 ix = make_int4(0, 0, 0, 0);
+    if (valid) {
+        ix = mol_idx[m];
+        const MolPos mi = load_mol(xs, ix);
+        const float4 Ti = totals[m];
+        int cnt = (int)mcounts[m];
+        cnt = cnt < mcap ? cnt : mcap;
+        const uint32_t *row = mlist + (size_t)(m / G) * mcap * G + a * T + t;
+        for (int k = t; k < cnt; k += T) {
+            const int mj = (int)row[(size_t)(k / T) * 32];
+            const int4 jx = __ldg(mol_idx + mj);
+            MolPos mjp;
+            mjp.a = f3(__ldg(xs + jx.x));
+            const float3 dr = min_image(box, mi.a - mjp.a);
+            const float r2 = dot3(dr, dr);
+            if (r2 >= p.list_cut2) continue;
+            if (sqrtf(r2) > p.rmax) continue;
+            mjp.b = f3(__ldg(xs + jx.y));
+            mjp.c = f3(__ldg(xs + jx.z));
+            const float4 Tj = __ldg(totals + mj);
+            const bool first = m < mj;
+            PairGeom g;
+            if (first) pair_geom(p, box, mi, mjp, g);
+            else pair_geom(p, box, mjp, mi, g);
+            if (ENERGY) {
+                e3 += 0.5f * (first ? pair_energy(p, g.es, Ti, Tj) : pair_energy(p, g.es, Tj, Ti));
+                continue;
+            }
+            float3 da, db, dc;
+            if (first) pair_force(p, g, Ti, Tj, true, da, db, dc);
+            else pair_force(p, g, Tj, Ti, false, da, db, dc);
+            fa += da;
+            fb += db;
+            fc += dc;
+        }
+    }
+    if (ENERGY) {
+        e3 = tsum<T>(e3);
+        if (valid && t == 0) atomicAdd(e3_out, (double)e3);
+        return;
+    }
+    fa.x = tsum<T>(fa.x); fa.y = tsum<T>(fa.y); fa.z = tsum<T>(fa.z);
+    fb.x = tsum<T>(fb.x); fb.y = tsum<T>(fb.y); fb.z = tsum<T>(fb.z);
+    fc.x = tsum<T>(fc.x); fc.y = tsum<T>(fc.y); fc.z = tsum<T>(fc.z);
+    if (valid && t == 0) {
+        float4 f = fs[ix.x];
+        f.x += fa.x; f.y += fa.y; f.z += fa.z;
+        fs[ix.x] = f;
+        f = fs[ix.y];
+        f.x += fb.x; f.y += fb.y; f.z += fb.z;
+        fs[ix.y] = f;
+        f = fs[ix.z];
+        f.x += fc.x; f.y += fc.y; f.z += fc.z;
+        fs[ix.z] = f;
+    }
+}
+
+constexpr int kMolTeam = 8;
+
+}  // namespace
+
+FixE3B::FixE3B(State *s, std::string h, std::string st) : Fix(s, h, "all", "E3B", FixKind::E3B), style(st) {}
+
+int FixE3B::prepareForRun() {
+    State &s = *state;
+    if (style != "E3B3" && style != "E3B2") {
+        set_error(MDX_ERR_ARG, "FixE3B style must be 'E3B3' or 'E3B2'");
+        return MDX_ERR_ARG;
+    }
+    if (s.units.type != MDX_UNITS_REAL) {
+        set_error(MDX_ERR_UNSUPPORTED, "Units for E3B potential are not yet as LJ (FixE3B.cu:541)");
+        return MDX_ERR_UNSUPPORTED;
+    }
+    const double kj = 0.23900573614;
+    double E2, Ea, Eb, Ec;
+    if (style == "E3B3") { E2 = 453000.0; Ea = 150.0; Eb = -1005.0; Ec = 1880.0; }
+    else { E2 = 2349000.0; Ea = 1745.7; Eb = -4565.0; Ec = 7606.8; }
+    // EvaluatorE3B ctor (EvaluatorE3B.h:46-64): float parameters
+    prm.rs = 5.0f;
+    prm.rf = 5.2f;
+    prm.E2 = (float)(E2 * kj);
+    prm.Ea = (float)(Ea * kj);
+    prm.Eb = (float)(Eb * kj);
+    prm.Ec = (float)(Ec * kj);
+    prm.k2 = 4.872f;
+    prm.k3 = 1.907f;
+    float d = prm.rf - prm.rs;
+    prm.rfminusrs_cubed_inv = 1.0f / (d * d * d);
+    prm.rstimes3 = 3.0f * prm.rs;
+    float lc = (float)((double)prm.rf + 1.0);  // molecule-list radius rf + padding(1.0) (FixE3B.cu:29, 657)
+    prm.list_cut2 = lc * lc;
+    prm.rmax = 6.157200f;
+    if ((double)s.grid.cut < (double)lc + s.padding) {
+        set_error(MDX_ERR_UNSUPPORTED,
+                  "FixE3B needs the atom neighbour cutoff (rCut + padding = %g) >= %g (E3B list radius + padding)",
+                  (double)s.grid.cut, (double)lc + s.padding);
+        return MDX_ERR_UNSUPPORTED;
+    }
+    const int nmol = (int)mol_ids.size();
+    if (int e = d_mol_ids.alloc(nmol)) return e;
+    if (int e = d_mol_idx.alloc(nmol)) return e;
+    if (int e = totals.alloc(nmol)) return e;
+    if (int e = mcounts.alloc(nmol)) return e;
+    MDX_CUDA_TRY(cudaMemcpy(d_mol_ids.p, mol_ids.data(), nmol * sizeof(int4), cudaMemcpyHostToDevice));
+    std::vector<int> mof(s.atoms.size(), -1);
+    for (int m = 0; m < nmol; m++) mof[mol_ids[m].x] = m;
+    if (int e = d_mol_of_atom.alloc(mof.size())) return e;
+    MDX_CUDA_TRY(cudaMemcpy(d_mol_of_atom.p, mof.data(), mof.size() * sizeof(int), cudaMemcpyHostToDevice));
+    mteam = kMolTeam;
+    const double vol = s.box.Ld.x * s.box.Ld.y * s.box.Ld.z;
+    const double rl = (double)lc + s.padding;
+    const double est = nmol / vol * 4.18879 * rl * rl * rl;
+    mcap = ((int)(2.0 * est + 32) + mteam - 1) / mteam * mteam;
+    const size_t groups = (size_t)(nmol + 32 / mteam - 1) / (32 / mteam);
+    if (int e = mlist.alloc(groups * mcap * (32 / mteam))) return e;
+    prepared = true;
+    return 0;
+}
+
+int e3b_build_list(State &s, FixE3B &f, bool conditional) {
+    const int nmol = (int)f.mol_ids.size();
+    if (nmol == 0 || !f.prepared) return 0;
+    const float lc = (float)((double)f.prm.rf + 1.0 + s.padding);
+    const int warps = (nmol + (32 / kMolTeam) - 1) / (32 / kMolTeam);
+    k_e3b_list<kMolTeam><<<(warps * 32 + 255) / 256, 256, 0, s.stream>>>(
+        nmol, f.d_mol_ids.p, f.d_mol_idx.p, s.gpd.idToIdx.p, f.d_mol_of_atom.p, s.gpd.ids.p, s.gpd.xs.p,
+        s.grid.counts.p, s.grid.nlist.p, s.grid.team, s.grid.cap, s.box, lc * lc, f.mcounts.p, f.mlist.p, f.mcap,
+        s.d_status.p, conditional ? 1 : 0);
+    MDX_LAUNCHED();
+    return 0;
+}
+
+int e3b_forces(State &s, FixE3B &f) {
+    const int nmol = (int)f.mol_ids.size();
+    if (nmol == 0) return 0;
+    const int warps = (nmol + (32 / kMolTeam) - 1) / (32 / kMolTeam);
+    const int blocks = (warps * 32 + 255) / 256;
+    k_e3b_totals<kMolTeam, false><<<blocks, 256, 0, s.stream>>>(nmol, f.d_mol_idx.p, s.gpd.xs.p, s.gpd.fs.p,
+                                                               f.mcounts.p, f.mlist.p, f.mcap, s.box, f.prm,
+                                                               f.totals.p, nullptr);
+    MDX_LAUNCHED();
+    k_e3b_forces<kMolTeam, false><<<blocks, 256, 0, s.stream>>>(nmol, f.d_mol_idx.p, s.gpd.xs.p, s.gpd.fs.p,
+                                                               f.mcounts.p, f.mlist.p, f.mcap, s.box, f.prm,
+                                                               f.totals.p, nullptr);
+    MDX_LAUNCHED();
+    return 0;
+}
+
+int e3b_energy(State &s, FixE3B &f, double out[2]) {
+    const int nmol = (int)f.mol_ids.size();
+    out[0] = out[1] = 0.0;
+    if (nmol == 0) return 0;
+    DBuf<double> acc;
+    if (int e = acc.alloc(2)) return e;
+    MDX_CUDA_TRY(cudaMemsetAsync(acc.p, 0, 2 * sizeof(double), s.stream));
+    const int warps = (nmol + (32 / kMolTeam) - 1) / (32 / kMolTeam);
+    const int blocks = (warps * 32 + 255) / 256;
+    // totals are needed by the energy pass: run the force-less totals first
+    DBuf<float4> ftmp;
+    if (int e = ftmp.alloc(s.gpd.n)) return e;
+    MDX_CUDA_TRY(cudaMemcpyAsync(ftmp.p, s.gpd.fs.p, s.gpd.n * sizeof(float4), cudaMemcpyDeviceToDevice, s.stream));
+    k_e3b_totals<kMolTeam, false><<<blocks, 256, 0, s.stream>>>(nmol, f.d_mol_idx.p, s.gpd.xs.p, ftmp.p, f.mcounts.p,
+                                                               f.mlist.p, f.mcap, s.box, f.prm, f.totals.p, nullptr);
+    MDX_LAUNCHED();
+    k_e3b_totals<kMolTeam, true><<<blocks, 256, 0, s.stream>>>(nmol, f.d_mol_idx.p, s.gpd.xs.p, ftmp.p, f.mcounts.p,
+                                                              f.mlist.p, f.mcap, s.box, f.prm, f.totals.p, acc.p);
+    MDX_LAUNCHED();
+    k_e3b_forces<kMolTeam, true><<<blocks, 256, 0, s.stream>>>(nmol, f.d_mol_idx.p, s.gpd.xs.p, ftmp.p, f.mcounts.p,
+                                                              f.mlist.p, f.mcap, s.box, f.prm, f.totals.p, acc.p + 1);
+    MDX_LAUNCHED();
+    MDX_CUDA_TRY(cudaMemcpyAsync(out, acc.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+    MDX_CUDA_TRY(cudaStreamSynchronize(s.stream));
+    return 0;
+}
+
+int FixE3B::compute(int virialMode) {
+    (void)virialMode;
+    return e3b_forces(*state, *this);
+}
+
+int FixE3B::handleLocalData() { return 0; }
+
+}  // namespace mdx

@@ -1,0 +1,350 @@
+// C++ host side of the hot path: State / GPUData / GridGPU / Fix / Integrator,
+// mirroring the reference's operator API (src/State.h, src/GPUData.h,
+// src/GridGPU.h, src/Fixes/Fix.h, src/Integrators/IntegratorVerlet.h).
+#pragma once
+#include <cufft.h>
+
+#include <map>
+#include <memory>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "common.cuh"
+
+namespace mdx {
+
+extern uint64_t g_launches;  // kernels launched by this library
+#define MDX_LAUNCHED() (++::mdx::g_launches)
+
+template <class T>
+struct DBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    int alloc(size_t count) {
+        if (count <= n && p) return 0;
+        release();
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            n = 0;
+            set_error(MDX_ERR_CUDA, "cudaMalloc(%zu bytes): %s", count * sizeof(T), cudaGetErrorString(e));
+            return MDX_ERR_CUDA;
+        }
+        n = count;
+        return 0;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    ~DBuf() { release(); }
+    DBuf() = default;
+    DBuf(const DBuf &) = delete;
+    DBuf &operator=(const DBuf &) = delete;
+};
+
+struct Units {  // src/Units.cpp:5-32
+    int type = MDX_UNITS_LJ;
+    double boltz = 1, hbar = 1, mvv_to_eng = 1, qqr_to_eng = 1, nktv_to_press = 1, ftm_to_v = 1;
+    void setLJ() {
+        type = MDX_UNITS_LJ;
+        boltz = hbar = mvv_to_eng = qqr_to_eng = nktv_to_press = ftm_to_v = 1.0;
+    }
+    void setReal() {
+        type = MDX_UNITS_REAL;
+        boltz = 0.0019872067;
+        hbar = 15.178728314015;
+        mvv_to_eng = 48.88821291 * 48.88821291;
+        nktv_to_press = 68568.415;
+        qqr_to_eng = 332.06371;
+        ftm_to_v = (double)(1.0f / (48.88821291 * 48.88821291));
+    }
+};
+
+struct Species {
+    std::string handle;
+    double mass;
+    int atomic_num;
+};
+
+struct HostAtom {
+    double pos[3], vel[3], force[3];
+    double mass, q;
+    int type, ndf;
+    uint32_t groupTag;
+};
+
+class State;
+
+// ---------------------------------------------------------------- GPUData
+// Per-atom device streams (src/GPUData.h:18-28): xs (type bits in .w),
+// vs (1/m in .w), fs (group tag bits in .w), ids, qs, idToIdx, virials.
+// Streams are sorted by cell at each list rebuild; the *_alt buffers are
+// the scatter targets, copied back so that captured graphs see fixed
+// pointers.
+struct GPUData {
+    DBuf<float4> xs, vs, fs, xs_alt, vs_alt, fs_alt, xs_last_build;
+    DBuf<float> qs, qs_alt;
+    DBuf<uint32_t> ids, ids_alt;
+    DBuf<int> idToIdx;
+    DBuf<float> virials;  // 6 per atom
+    int n = 0;
+};
+
+// ---------------------------------------------------------------- GridGPU
+// Cell-binned neighbour list (src/GridGPU.h).  Layout: "team-interleaved
+// ELL": atoms are grouped 32/team per warp; an atom's k-th entry lives at
+// group*cap*(32/team) + (k/team)*32 + slot*team + k%team, so a warp's team
+// lanes read 128 contiguous bytes per row.
+struct GridGPU {
+    int team = 8;        // threads per atom in build and force kernels
+    int cap = 0;         // per-atom capacity (multiple of team)
+    int3 ns{0, 0, 0};    // cells per dimension
+    int m = 2;           // stencil half width in cells (cells >= cut/m)
+    float cut = 0.f;     // neighCut = rCut + padding (float, as GridGPU)
+    float skin = 0.f;    // padding
+    DBuf<uint32_t> cell_start, cell_count, cell_fill, block_sums;
+    DBuf<int> cell_of;     // per atom (unsorted order)
+    DBuf<int> perm_tmp, perm;  // sort scratch
+    DBuf<uint32_t> counts; // per atom neighbour count
+    DBuf<uint32_t> nlist;  // entries
+    DBuf<int> excl_start;  // by id
+    DBuf<uint32_t> excl_ids;
+    int max_excl = 0;
+    bool have_excl = false;
+    bool built = false;
+};
+
+// ---------------------------------------------------------------- Fixes
+enum class FixKind { Pair, ChargeEwald, E3B, Rigid, NoseHoover };
+
+class Fix {
+   public:
+    State *state;
+    std::string handle, group, type;
+    FixKind kind;
+    int orderPreference = 0;
+    bool prepared = false;
+    bool active = false;
+    bool requiresCharges = false;
+    Fix(State *s, std::string h, std::string g, std::string t, FixKind k) : state(s), handle(h), group(g), type(t), kind(k) {}
+    virtual ~Fix() {}
+    // hooks of src/Fixes/Fix.h:79-281 (return 0 on success, MDX_ERR_* otherwise)
+    virtual int prepareForRun() { prepared = true; return 0; }
+    virtual int stepInit() { return 0; }
+    virtual int postNVE_X() { return 0; }
+    virtual int compute(int virialMode) { (void)virialMode; return 0; }
+    virtual int preStepFinal() { return 0; }
+    virtual int stepFinal() { return 0; }
+    virtual int handleLocalData() { return 0; }
+    virtual std::vector<double> getRCuts() { return {}; }
+    virtual void getBonds(std::vector<std::pair<int, int>> &out) { (void)out; }
+};
+
+class FixChargeEwald;
+
+// FixPair / FixLJCut / FixWCA (src/Fixes/FixPair.cpp, FixLJCut.cu, FixWCA.cu)
+class FixPair : public Fix {
+   public:
+    int lj_kind;  // 1 LJ/cut, 2 WCA
+    std::string mixing;
+    // unprocessed per-type tables; NaN = unset (DEFAULT_FILL)
+    std::map<std::string, std::vector<double>> params;
+    DBuf<float> d_params;  // rc2, eps24, sig6 (3*T*T)
+    std::vector<float> h_params;
+    FixChargeEwald *chargeFix = nullptr;  // offloaded real-space Ewald (State.cpp:648-660)
+    double chargeRCut = 0;
+    FixPair(State *s, std::string h, int kind, std::string mix);
+    int setParameter(const std::string &param, int a, int b, double v);
+    int prepareForRun() override;
+    int compute(int virialMode) override;
+    std::vector<double> getRCuts() override;
+    void ensureSize();
+};
+
+class FixChargeEwald : public Fix {
+   public:
+    int3 sz{64, 64, 64};
+    int order = 5;
+    double r_cut = -1;
+    double alpha = 0;
+    double alpha_user = 0;
+    bool offloaded = false;
+    cufftHandle plan_r2c = 0, plan_c2r = 0;
+    bool plans = false;
+    DBuf<float> rho;        // real grid
+    DBuf<float2> rho_k;     // half spectrum
+    DBuf<float2> e_k;       // 3 half spectra
+    DBuf<float> e_r;        // 3 real grids
+    DBuf<float> green;      // half spectrum Green function
+    DBuf<double> energy_acc;
+    FixChargeEwald(State *s, std::string h, std::string g);
+    ~FixChargeEwald() override;
+    int setParameters(int nx, int ny, int nz, double rcut, int ord);
+    int prepareForRun() override;
+    int compute(int virialMode) override;
+    std::vector<double> getRCuts() override { return {r_cut}; }
+    double findAlpha();
+    int spread();   // zero + spread
+    int solve();    // FFT, E-field, inverse FFTs
+    int gather(bool accumulate);
+};
+
+struct E3BParams {  // EvaluatorE3B (EvaluatorE3B.h:9-65), FixE3B.cu:515-593
+    float rs, rf, E2, Ea, Eb, Ec, k2, k3;
+    float rfminusrs_cubed_inv, rstimes3;
+    float list_cut2;  // (rf + padding)^2, the reference's molecule-list radius
+    float rmax;       // RMAX_E3B (ThreeBodyE3B.h:16)
+};
+
+class FixE3B : public Fix {
+   public:
+    std::string style;
+    std::vector<int4> mol_ids;
+    E3BParams prm{};
+    DBuf<int4> d_mol_ids, d_mol_idx;
+    DBuf<int> d_mol_of_atom;  // by atom index, -1 if none (rebuilt with the list)
+    DBuf<uint32_t> mcounts, mlist;  // molecule neighbour list (full, team layout)
+    DBuf<float4> totals;
+    int mteam = 8, mcap = 0;
+    FixE3B(State *s, std::string h, std::string st);
+    int prepareForRun() override;
+    int compute(int virialMode) override;
+    int handleLocalData() override;
+};
+
+struct RigidConsts {  // FixRigidData (FixRigid.h:23-77)
+    double ra, rb, rc, inv2Rc;
+    double wO, wH, mO, mH, invmO, invmH;
+    double r_OH, r_HH, r_OM, gamma;
+    double invOH, invHH;
+    double Minv[9];
+    int foursite;
+};
+
+class FixRigid : public Fix {
+   public:
+    std::string style;
+    std::vector<int4> mol_ids;
+    RigidConsts rc{};
+    DBuf<int4> d_mol_ids, d_mol_idx;
+    DBuf<float4> xs0;  // previous constrained O,H1,H2 (stand-alone hook path)
+    bool foursite = false, threesite = false;
+    FixRigid(State *s, std::string h, std::string st);
+    int createRigid(int o, int h1, int h2, int m);
+    int prepareForRun() override;
+    void getBonds(std::vector<std::pair<int, int>> &out) override;
+    int setConsts();
+};
+
+struct NHChain {  // FixNoseHoover chain state (FixNoseHoover.h), FP64
+    double vel[10], force[10], mass[10];
+    double ke;       // sum m v^2 * mvv_to_eng
+    double T, freq, ndf, kB, dt;
+    double mvv_to_eng;
+    int n;
+    double scale;    // pending velocity scale for the next stepInit
+    double last_ke;
+};
+
+class FixNoseHoover : public Fix {
+   public:
+    double T = 0, tau = 0;
+    NHChain h{};
+    DBuf<NHChain> d_chain;
+    DBuf<double> partials;
+    DBuf<unsigned int> counter;
+    bool chain_on_device = false;
+    FixNoseHoover(State *s, std::string h, std::string g);
+    int setTemperature(double T_, double tau_);
+    int prepareFinal();
+};
+
+// ---------------------------------------------------------------- State
+class State {
+   public:
+    Units units;
+    double rCut = -1, padding = 0.5, dt = 0.005;
+    int64_t turn = 0;
+    int periodicInterval = 50;
+    int nThreadPerAtom = 0, nThreadPerBlock = 256;  // 0 = automatic team size
+    float specialNeighborCoefs[3] = {0.f, 0.f, 0.5f};
+    double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    bool bounds_set = false;
+    std::vector<Species> species;
+    std::vector<HostAtom> atoms;  // index == id
+    std::vector<Fix *> fixes;     // active fixes in order
+    Box box{};
+    GPUData gpd;
+    GridGPU grid;
+    DBuf<DeviceStatus> d_status;
+    DeviceStatus *h_status = nullptr;  // pinned
+    DBuf<double> red_partials;
+    DBuf<double> red_out;
+    DBuf<unsigned int> red_counter;
+    cudaStream_t stream = nullptr;
+    bool own_stream = true;
+    bool uploaded = false;   // device copy is authoritative
+    bool prepared = false;
+    bool requiresCharges = false;
+    State();
+    ~State();
+    int typeFromHandle(const std::string &h) const;
+    void setBox();
+    int upload();
+    int download();
+    int prepare();
+    int buildNeighborList(bool force);
+    int computeForces(int virialMode);
+    int checkStatus();
+    FixPair *pairFix();
+    FixChargeEwald *ewaldFix();
+    FixE3B *e3bFix();
+    FixRigid *rigidFix();
+    FixNoseHoover *nhFix();
+    double maxRCut();
+};
+
+// ---------------------------------------------------------------- kernels
+// neighbour list (nlist.cu)
+int nlist_rebuild(State &s, bool force, bool conditional);
+int nlist_init(State &s);
+int nlist_exclusions(State &s);
+// pair (pair.cu)
+int pair_launch(State &s, FixPair &f, int virialMode, bool accumulate);
+int pair_energy(State &s, FixPair &f, double *out);
+int pair_force_raw(int n, const float4 *xs, float4 *fs, const float *qs, const uint32_t *counts,
+                   const uint32_t *nlist, int team, int cap, const float *params, int ntypes, const Box &box,
+                   const float coef[3], int lj_kind, float qrc, float alpha, float qqr, float *virials,
+                   bool accumulate, cudaStream_t stream);
+// e3b (e3b.cu)
+int e3b_build_list(State &s, FixE3B &f, bool conditional);
+int e3b_forces(State &s, FixE3B &f);
+int e3b_energy(State &s, FixE3B &f, double out[2]);
+// rigid + integration (integrate.cu)
+int rigid_update_maps(State &s, FixRigid &r, bool conditional);
+int step_first_half(State &s, bool fused);
+int step_second_half(State &s, bool fused);
+int rigid_prepare(State &s, FixRigid &r);
+int rigid_hook(State &s, FixRigid &r, int which);
+int kinetic_sum(State &s, double *out);
+int nh_prepare(State &s, FixNoseHoover &nh);
+int zero_forces(State &s);
+int device_sum(State &s, const double *src, int n, double *out_host);
+int virial_sum(State &s, double out[6]);
+int remove_com_velocity(State &s);
+int nh_end_of_run(State &s);
+int rigid_flags_prepare(State &s);
+
+}  // namespace mdx
+
+struct mdx_state {
+    mdx::State *s;
+};
+struct mdx_fix {
+    mdx::Fix *f;
+    mdx_state *owner;
+};

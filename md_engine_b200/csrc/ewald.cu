@@ -1,0 +1,414 @@
+// P3M reciprocal-space Ewald (FixChargeEwald, src/Fixes/FixChargeEwald.cu).
+//
+//  spread   map_charge_to_grid_order_5_cu (:174-217): order-5 charge
+//           assignment W_p_5 (:163-172), float atomics into a REAL grid
+//  FFT      cuFFT R2C (the reference runs C2C on a complex grid with a zero
+//           imaginary part, :1307-1309; R2C computes the same half spectrum)
+//  E(k)     E_field_cu (:386-434): E_d(k) = i k_d G(k) rho(k).  The reference
+//           keeps only the real part after its C2C inverse, which drops the
+//           anti-Hermitian Nyquist-plane term of each component; that term is
+//           zeroed here so the C2R inverse gives the identical real field.
+//  inverse  one batched cuFFT C2R for the three components (:1340-1346)
+//  gather   Ewald_long_range_forces_order_5_cu (:561-630): F = Q q sum W E,
+//           E = -ifft / V
+//  G(k)     Green_function_cu (:314-366), evaluated once per box in FP64.
+//  alpha    find_optimal_parameters (:848-967), secant on the RMS errors.
+//
+// Deviation (documented): the reference's nearest grid point is
+// make_int3((x-lo+h/2)/h), a truncation toward zero, which mis-assigns the
+// stencil of an atom more than h/2 below lo (atoms drift out of the box
+// between list rebuilds); floorf is used here.
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "engine.hpp"
+
+namespace mdx {
+
+namespace {
+
+__device__ __forceinline__ void w5(float x, float w[5]) {
+    const float x2 = x * x, x4 = x2 * x2;
+    w[0] = (1.0f / 384.0f) * (1.0f - 8.0f * x + 24.0f * x2 - 32.0f * x * x2 + 16.0f * x4);
+    w[1] = (1.0f / 96.0f) * (19.0f - 44.0f * x + 24.0f * x2 + 16.0f * x * x2 - 16.0f * x4);
+    w[2] = (1.0f / 192.0f) * (115.0f - 120.0f * x2 + 48.0f * x4);
+    w[3] = (1.0f / 96.0f) * (19.0f + 44.0f * x + 24.0f * x2 - 16.0f * x * x2 - 16.0f * x4);
+    w[4] = (1.0f / 384.0f) * (1.0f + 8.0f * x + 24.0f * x2 + 32.0f * x * x2 + 16.0f * x4);
+}
+
+__device__ __forceinline__ int wrapi(int p, int n) {
+    p %= n;
+    return p < 0 ? p + n : p;
+}
+
+struct P3MGeom {
+    int3 sz;
+    float3 lo, h, invh;
+    float qunit;
+};
+
+__device__ __forceinline__ void stencil(const P3MGeom &g, float4 x, int3 &ng, float3 &d) {
+    const float px = x.x - g.lo.x, py = x.y - g.lo.y, pz = x.z - g.lo.z;
+    ng.x = (int)floorf((px + 0.5f * g.h.x) / g.h.x);
+    ng.y = (int)floorf((py + 0.5f * g.h.y) / g.h.y);
+    ng.z = (int)floorf((pz + 0.5f * g.h.z) / g.h.z);
+    d.x = px / g.h.x - (float)ng.x;
+    d.y = py / g.h.y - (float)ng.y;
+    d.z = pz / g.h.z - (float)ng.z;
+}
+
+__global__ void k_spread(int n, const float4 *__restrict__ xs, const float *__restrict__ qs, P3MGeom g,
+                         float *__restrict__ rho) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float q = qs[i];
+    if (q == 0.f) return;
+    const float qi = g.qunit * q;
+    int3 ng;
+    float3 d;
+    stencil(g, xs[i], ng, d);
+    float wx[5], wy[5], wz[5];
+    w5(d.x, wx);
+    w5(d.y, wy);
+    w5(d.z, wz);
+    int pz[5];
+#pragma unroll
+    for (int c = 0; c < 5; c++) pz[c] = wrapi(ng.z + c - 2, g.sz.z);
+#pragma unroll
+    for (int a = 0; a < 5; a++) {
+        const int px = wrapi(ng.x + a - 2, g.sz.x);
+        const float cyz = qi * wx[a];
+#pragma unroll
+        for (int b = 0; b < 5; b++) {
+            const int py = wrapi(ng.y + b - 2, g.sz.y);
+            const float cz = cyz * wy[b];
+            float *row = rho + ((size_t)px * g.sz.y + py) * g.sz.z;
+#pragma unroll
+            for (int c = 0; c < 5; c++) atomicAdd(row + pz[c], cz * wz[c]);
+        }
+    }
+}
+
+// E_d(k) = i k_d G rho on the half spectrum (z halved), batched output
+__global__ void k_efield(int3 sz, float3 twopi_over_L, const float2 *__restrict__ rho_k,
+                         const float *__restrict__ green, float2 *__restrict__ ek, size_t nk) {
+    size_t id = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= nk) return;
+    const int nzh = sz.z / 2 + 1;
+    const int iz = (int)(id % nzh);
+    const int iy = (int)((id / nzh) % sz.y);
+    const int ix = (int)(id / ((size_t)nzh * sz.y));
+    const float kx = twopi_over_L.x * (float)(ix > sz.x / 2 ? ix - sz.x : ix);
+    const float ky = twopi_over_L.y * (float)(iy > sz.y / 2 ? iy - sz.y : iy);
+    const float kz = twopi_over_L.z * (float)iz;
+    const float G = green[id];
+    const float2 q = rho_k[id];
+    // i k G (q.x + i q.y) = (-k G q.y) + i (k G q.x); Nyquist planes dropped per component
+    const float gx = (2 * ix == sz.x) ? 0.f : kx * G;
+    const float gy = (2 * iy == sz.y) ? 0.f : ky * G;
+    const float gz = (2 * iz == sz.z) ? 0.f : kz * G;
+    ek[id] = make_float2(-gx * q.y, gx * q.x);
+    ek[nk + id] = make_float2(-gy * q.y, gy * q.x);
+    ek[2 * nk + id] = make_float2(-gz * q.y, gz * q.x);
+}
+
+template <bool ACC>
+__global__ void k_gather(int n, const float4 *__restrict__ xs, const float *__restrict__ qs, P3MGeom g,
+                         const float *__restrict__ er, size_t ngrid, float neg_inv_vol, float4 *__restrict__ fs) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float q = qs[i];
+    if (q == 0.f) {
+        if (!ACC) {
+            float4 f = fs[i];
+            fs[i] = make_float4(0.f, 0.f, 0.f, f.w);
+        }
+        return;
+    }
+    int3 ng;
+    float3 d;
+    stencil(g, xs[i], ng, d);
+    float wx[5], wy[5], wz[5];
+    w5(d.x, wx);
+    w5(d.y, wy);
+    w5(d.z, wz);
+    int pz[5];
+#pragma unroll
+    for (int c = 0; c < 5; c++) pz[c] = wrapi(ng.z + c - 2, g.sz.z);
+    float ex = 0.f, ey = 0.f, ez = 0.f;
+#pragma unroll
+    for (int a = 0; a < 5; a++) {
+        const int px = wrapi(ng.x + a - 2, g.sz.x);
+#pragma unroll
+        for (int b = 0; b < 5; b++) {
+            const int py = wrapi(ng.y + b - 2, g.sz.y);
+            const size_t row = ((size_t)px * g.sz.y + py) * g.sz.z;
+            const float wab = wx[a] * wy[b];
+#pragma unroll
+            for (int c = 0; c < 5; c++) {
+                const float w = wab * wz[c];
+                const size_t o = row + pz[c];
+                ex += w * __ldg(er + o);
+                ey += w * __ldg(er + ngrid + o);
+                ez += w * __ldg(er + 2 * ngrid + o);
+            }
+        }
+    }
+    const float s = g.qunit * q * neg_inv_vol;
+    float4 f = fs[i];
+    if (ACC) {
+        f.x += s * ex;
+        f.y += s * ey;
+        f.z += s * ez;
+    } else {
+        f.x = s * ex;
+        f.y = s * ey;
+        f.z = s * ez;
+    }
+    fs[i] = f;
+}
+
+// sum_k G |rho_k|^2 over the full spectrum from the half spectrum (FP64)
+__global__ void k_recip_energy(int3 sz, const float2 *__restrict__ rho_k, const float *__restrict__ green, size_t nk,
+                               double *out) {
+    double acc = 0.0;
+    const int nzh = sz.z / 2 + 1;
+    for (size_t id = (size_t)blockIdx.x * blockDim.x + threadIdx.x; id < nk; id += (size_t)gridDim.x * blockDim.x) {
+        const int iz = (int)(id % nzh);
+        const double w = (iz == 0 || 2 * iz == sz.z) ? 1.0 : 2.0;
+        const float2 q = rho_k[id];
+        acc += w * (double)green[id] * ((double)q.x * q.x + (double)q.y * q.y);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
+}
+
+double sinc(double x) {
+    if (x < 0.1 && x > -0.1) {
+        double x2 = x * x;
+        return 1.0 - x2 * 0.16666666667 + x2 * x2 * 0.008333333333333333 - x2 * x2 * x2 * 0.00019841269841269841;
+    }
+    return std::sin(x) / x;
+}
+
+const double kAmp[5][5] = {
+    {2.0 / 3.0, 0, 0, 0, 0},
+    {1.0 / 50.0, 5.0 / 294.0, 0, 0, 0},
+    {1.0 / 588.0, 7.0 / 1440.0, 21.0 / 3872.0, 0, 0},
+    {1.0 / 4320.0, 3.0 / 1936.0, 7601.0 / 2271360.0, 143.0 / 28800.0, 0},
+    {1.0 / 23232.0, 7601.0 / 12628160.0, 143.0 / 69120.0, 517231.0 / 106536960.0, 106640677.0 / 11737571328.0},
+};
+
+P3MGeom geom(State &s, FixChargeEwald &f) {
+    P3MGeom g;
+    g.sz = f.sz;
+    g.lo = s.box.lo;
+    g.h = make_float3(s.box.L.x / (float)f.sz.x, s.box.L.y / (float)f.sz.y, s.box.L.z / (float)f.sz.z);
+    g.invh = make_float3(1.f / g.h.x, 1.f / g.h.y, 1.f / g.h.z);
+    g.qunit = (float)std::sqrt(s.units.qqr_to_eng);
+    return g;
+}
+
+}  // namespace
+
+FixChargeEwald::FixChargeEwald(State *s, std::string h, std::string g)
+    : Fix(s, h, g, "ChargeEwald", FixKind::ChargeEwald) {
+    requiresCharges = true;
+}
+
+FixChargeEwald::~FixChargeEwald() {
+    if (plans) {
+        cufftDestroy(plan_r2c);
+        cufftDestroy(plan_c2r);
+    }
+}
+
+int FixChargeEwald::setParameters(int nx, int ny, int nz, double rcut, int ord) {
+    auto ok = [](int v) { return v == 32 || v == 64 || v == 128 || v == 256 || v == 512 || v == 1024; };
+    if (!ok(nx) || !ok(ny) || !ok(nz)) {
+        set_error(MDX_ERR_ARG, "P3M grid %d %d %d: only 2^N sizes 32..1024 are supported (FixChargeEwald.cu:976-987)",
+                  nx, ny, nz);
+        return MDX_ERR_ARG;
+    }
+    if (ord != 5) {
+        set_error(MDX_ERR_UNSUPPORTED, "P3M interpolation order %d: this build implements order 5", ord);
+        return MDX_ERR_UNSUPPORTED;
+    }
+    sz = make_int3(nx, ny, nz);
+    r_cut = rcut;
+    order = ord;
+    return 0;
+}
+
+// total_Q2 (setTotalQ2, :883-914) in FP64 and the secant of :918-967
+double FixChargeEwald::findAlpha() {
+    State &s = *state;
+    double Q2 = 0.0;
+    for (auto &a : s.atoms) Q2 += a.q * a.q;
+    Q2 *= s.units.qqr_to_eng;
+    const double L[3] = {s.box.Ld.x, s.box.Ld.y, s.box.Ld.z};
+    const double h[3] = {L[0] / sz.x, L[1] / sz.y, L[2] / sz.z};
+    const double nAtoms = (double)s.atoms.size();
+    const double rc = r_cut;
+    auto dk = [&](double a) {
+        double tot = 0.0;
+        for (int d = 0; d < 3; d++) {
+            double sum = 0.0;
+            for (int m = 0; m < order; m++) sum += kAmp[order - 1][m] * std::pow(h[d] * a, 2 * m);
+            tot += 1.0 / (L[d] * L[d]) * std::pow(a * h[d], order) * std::sqrt(a * L[d] / nAtoms * std::sqrt(2.0 * M_PI) * sum);
+        }
+        return Q2 / 3.0 * tot;
+    };
+    auto dr = [&](double a) { return 2 * Q2 / std::sqrt(nAtoms * rc * L[0] * L[1] * L[2]) * std::exp(-a * a * rc * rc); };
+    double xa = 0.0, xb = 4.79853 / rc;
+    double ya = dk(xa) - dr(xa), yb = dk(xb) - dr(xb);
+    for (int it = 0; it < 100 && std::fabs(yb) / dr(xb) > 1e-5; it++) {
+        double kinv = (xb - xa) / (yb - ya);
+        ya = yb;
+        xa = xb;
+        xb = xa - ya * kinv;
+        yb = dk(xb) - dr(xb);
+    }
+    return xb;
+}
+
+int FixChargeEwald::prepareForRun() {
+    State &s = *state;
+    if (r_cut < 0) r_cut = s.rCut;
+    alpha = alpha_user > 0 ? alpha_user : findAlpha();
+    const size_t ng = (size_t)sz.x * sz.y * sz.z;
+    const size_t nk = (size_t)sz.x * sz.y * (sz.z / 2 + 1);
+    if (int e = rho.alloc(ng)) return e;
+    if (int e = rho_k.alloc(nk)) return e;
+    if (int e = e_k.alloc(3 * nk)) return e;
+    if (int e = e_r.alloc(3 * ng)) return e;
+    if (int e = green.alloc(nk)) return e;
+    if (int e = energy_acc.alloc(1)) return e;
+    if (!plans) {
+        if (cufftPlan3d(&plan_r2c, sz.x, sz.y, sz.z, CUFFT_R2C) != CUFFT_SUCCESS) {
+            set_error(MDX_ERR_CUDA, "cufftPlan3d R2C failed");
+            return MDX_ERR_CUDA;
+        }
+        int dims[3] = {sz.x, sz.y, sz.z};
+        if (cufftPlanMany(&plan_c2r, 3, dims, nullptr, 1, (int)nk, nullptr, 1, (int)ng, CUFFT_C2R, 3) !=
+            CUFFT_SUCCESS) {
+            set_error(MDX_ERR_CUDA, "cufftPlanMany C2R failed");
+            return MDX_ERR_CUDA;
+        }
+        plans = true;
+    }
+    cufftSetStream(plan_r2c, s.stream);
+    cufftSetStream(plan_c2r, s.stream);
+    // Green function on the half spectrum (Green_function_cu, FP64 here)
+    std::vector<float> G(nk);
+    const double L[3] = {s.box.Ld.x, s.box.Ld.y, s.box.Ld.z};
+    const double h[3] = {L[0] / sz.x, L[1] / sz.y, L[2] / sz.z};
+    const int lim = (int)(alpha * std::pow(h[0] * h[1] * h[2], 1.0 / 3.0) / 3.14159 * std::sqrt(-std::log(10E-7))) + 1;
+    const double f4a = 0.25 / alpha / alpha;
+    const double tp = 6.28318530717958647693;
+    const int nzh = sz.z / 2 + 1;
+    for (int ix = 0; ix < sz.x; ix++) {
+        double kx = tp * (ix > sz.x / 2 ? ix - sz.x : ix) / L[0];
+        for (int iy = 0; iy < sz.y; iy++) {
+            double ky = tp * (iy > sz.y / 2 ? iy - sz.y : iy) / L[1];
+            for (int iz = 0; iz < nzh; iz++) {
+                double kz = tp * iz / L[2];
+                double k2 = kx * kx + ky * ky + kz * kz;
+                double val = 0.0;
+                if (k2 != 0.0) {
+                    double s1 = 0.0, s2 = 0.0;
+                    for (int mx = -lim; mx <= lim; mx++)
+                        for (int my = -lim; my <= lim; my++)
+                            for (int mz = -lim; mz <= lim; mz++) {
+                                double px = kx + tp * mx / h[0], py = ky + tp * my / h[1], pz = kz + tp * mz / h[2];
+                                double pp = px * px + py * py + pz * pz;
+                                double W = sinc(px * h[0] * 0.5) * sinc(py * h[1] * 0.5) * sinc(pz * h[2] * 0.5);
+                                double W2 = std::pow(W, order * 2);
+                                s1 += 12.56637061435917295385 * std::exp(-pp * f4a) * (kx * px + ky * py + kz * pz) / pp * W2;
+                                s2 += W2;
+                            }
+                    val = s1 / (s2 * s2) / k2;
+                }
+                G[((size_t)ix * sz.y + iy) * nzh + iz] = (float)val;
+            }
+        }
+    }
+    MDX_CUDA_TRY(cudaMemcpy(green.p, G.data(), nk * sizeof(float), cudaMemcpyHostToDevice));
+    prepared = true;
+    return 0;
+}
+
+int FixChargeEwald::spread() {
+    State &s = *state;
+    const size_t ng = (size_t)sz.x * sz.y * sz.z;
+    MDX_CUDA_TRY(cudaMemsetAsync(rho.p, 0, ng * sizeof(float), s.stream));
+    P3MGeom g = geom(s, *this);
+    k_spread<<<(s.gpd.n + 127) / 128, 128, 0, s.stream>>>(s.gpd.n, s.gpd.xs.p, s.gpd.qs.p, g, rho.p);
+    MDX_LAUNCHED();
+    return 0;
+}
+
+int FixChargeEwald::solve() {
+    State &s = *state;
+    const size_t nk = (size_t)sz.x * sz.y * (sz.z / 2 + 1);
+    if (cufftExecR2C(plan_r2c, rho.p, (cufftComplex *)rho_k.p) != CUFFT_SUCCESS) {
+        set_error(MDX_ERR_CUDA, "cufftExecR2C failed");
+        return MDX_ERR_CUDA;
+    }
+    const float3 tpl = make_float3((float)(6.28318530717958647693 / s.box.Ld.x),
+                                   (float)(6.28318530717958647693 / s.box.Ld.y),
+                                   (float)(6.28318530717958647693 / s.box.Ld.z));
+    k_efield<<<(unsigned)((nk + 255) / 256), 256, 0, s.stream>>>(sz, tpl, rho_k.p, green.p, e_k.p, nk);
+    MDX_LAUNCHED();
+    if (cufftExecC2R(plan_c2r, (cufftComplex *)e_k.p, e_r.p) != CUFFT_SUCCESS) {
+        set_error(MDX_ERR_CUDA, "cufftExecC2R failed");
+        return MDX_ERR_CUDA;
+    }
+    return 0;
+}
+
+int FixChargeEwald::gather(bool accumulate) {
+    State &s = *state;
+    P3MGeom g = geom(s, *this);
+    const size_t ng = (size_t)sz.x * sz.y * sz.z;
+    const float niv = (float)(-1.0 / (s.box.Ld.x * s.box.Ld.y * s.box.Ld.z));
+    if (accumulate)
+        k_gather<true><<<(s.gpd.n + 127) / 128, 128, 0, s.stream>>>(s.gpd.n, s.gpd.xs.p, s.gpd.qs.p, g, e_r.p, ng, niv,
+                                                                   s.gpd.fs.p);
+    else
+        k_gather<false><<<(s.gpd.n + 127) / 128, 128, 0, s.stream>>>(s.gpd.n, s.gpd.xs.p, s.gpd.qs.p, g, e_r.p, ng, niv,
+                                                                    s.gpd.fs.p);
+    MDX_LAUNCHED();
+    return 0;
+}
+
+int FixChargeEwald::compute(int virialMode) {
+    (void)virialMode;
+    if (int e = spread()) return e;
+    if (int e = solve()) return e;
+    return gather(true);
+}
+
+int ewald_recip_energy(State &s, FixChargeEwald &f, double *out) {
+    if (int e = f.spread()) return e;
+    if (cufftExecR2C(f.plan_r2c, f.rho.p, (cufftComplex *)f.rho_k.p) != CUFFT_SUCCESS) {
+        set_error(MDX_ERR_CUDA, "cufftExecR2C failed");
+        return MDX_ERR_CUDA;
+    }
+    const size_t nk = (size_t)f.sz.x * f.sz.y * (f.sz.z / 2 + 1);
+    MDX_CUDA_TRY(cudaMemsetAsync(f.energy_acc.p, 0, sizeof(double), s.stream));
+    k_recip_energy<<<148, 256, 0, s.stream>>>(f.sz, f.rho_k.p, f.green.p, nk, f.energy_acc.p);
+    MDX_LAUNCHED();
+    double sumG = 0.0;
+    MDX_CUDA_TRY(cudaMemcpyAsync(&sumG, f.energy_acc.p, sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+    MDX_CUDA_TRY(cudaStreamSynchronize(s.stream));
+    double Q2 = 0.0;
+    for (auto &a : s.atoms) Q2 += a.q * a.q;
+    Q2 *= s.units.qqr_to_eng;
+    const double V = s.box.Ld.x * s.box.Ld.y * s.box.Ld.z;
+    *out = 0.5 * sumG / V - f.alpha / std::sqrt(M_PI) * Q2;
+    return 0;
+}
+
+}  // namespace mdx

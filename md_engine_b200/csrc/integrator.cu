@@ -1,0 +1,362 @@
+// IntegratorVerlet (src/Integrators/IntegratorVerlet.cu:649-770).
+//
+// The run loop keeps the reference's per-step hook order (§ stepInit ->
+// nve_v/nve_x -> postNVE_X -> force -> postForce -> preStepFinal ->
+// stepFinal) but, in the default fused mode, a chunk of periodicInterval
+// steps is captured once into a CUDA graph: [neighbour-list check + rebuild
+// group, each kernel returning at once unless the device decided to rebuild]
+// followed by the steps.  Nothing in a step waits on the host.
+#include <chrono>
+#include <cstdio>
+#include <algorithm>
+#include <map>
+#include <vector>
+
+#include "engine.hpp"
+
+namespace mdx {
+
+namespace {
+// host-buffer run support: scatter by id into the sorted device streams and
+// gather them back in id order
+__global__ void k_put_by_id(int n, const float4 *__restrict__ in, const int *__restrict__ idToIdx,
+                            float4 *__restrict__ dst) {
+    int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= n) return;
+    const int i = idToIdx[id];
+    float4 d = dst[i];
+    const float4 v = in[id];
+    dst[i] = make_float4(v.x, v.y, v.z, d.w);
+}
+__global__ void k_get_by_id(int n, const float4 *__restrict__ src, const uint32_t *__restrict__ ids,
+                            float4 *__restrict__ out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[ids[i]] = src[i];
+}
+}  // namespace
+
+class IntegratorVerlet {
+   public:
+    State *s;
+    int mode = 0;  // 0 fused + graphs, 1 hook-by-hook without graphs
+    std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
+    std::map<std::pair<int, int>, uint64_t> graph_kernels;  // our kernels per graph
+    explicit IntegratorVerlet(State *st) : s(st) {}
+    ~IntegratorVerlet() {
+        clearGraphs();
+        if (h_stage) cudaFreeHost(h_stage);
+    }
+    void clearGraphs() {
+        for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+        graphs.clear();
+        graph_kernels.clear();
+    }
+    int forces() {
+        // IntegratorUtil::force: pair fixes first (orderPreference -1)
+        if (FixPair *p = s->pairFix())
+            if (int e = p->compute(0)) return e;
+        for (Fix *f : s->fixes) {
+            if (f->kind == FixKind::Pair) continue;
+            if (int e = f->compute(0)) return e;
+        }
+        return 0;
+    }
+    int stepBody() {
+        const bool fused = mode == 0;
+        if (int e = step_first_half(*s, fused)) return e;
+        if (int e = forces()) return e;
+        if (int e = step_second_half(*s, fused)) return e;
+        return 0;
+    }
+    int enqueue(int nsteps, bool with_group) {
+        if (with_group)
+            if (int e = nlist_rebuild(*s, false, true)) return e;
+        for (int k = 0; k < nsteps; k++)
+            if (int e = stepBody()) return e;
+        return 0;
+    }
+    int getGraph(int nsteps, bool with_group, cudaGraphExec_t *out) {
+        auto key = std::make_pair(nsteps, with_group ? 1 : 0);
+        auto it = graphs.find(key);
+        if (it != graphs.end()) {
+            *out = it->second;
+            return 0;
+        }
+        cudaGraph_t g;
+        MDX_CUDA_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+        const uint64_t before = g_launches;
+        int e = enqueue(nsteps, with_group);
+        const uint64_t captured = g_launches - before;
+        g_launches = before;  // counted again at every replay
+        cudaError_t ce = cudaStreamEndCapture(s->stream, &g);
+        if (e) return e;
+        if (ce != cudaSuccess) {
+            set_error(MDX_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+            return MDX_ERR_CUDA;
+        }
+        cudaGraphExec_t ex;
+        MDX_CUDA_TRY(cudaGraphInstantiate(&ex, g, 0));
+        cudaGraphDestroy(g);
+        graphs[key] = ex;
+        graph_kernels[key] = captured;
+        *out = ex;
+        return 0;
+    }
+    int launchGraph(int nsteps, bool with_group) {
+        cudaGraphExec_t ex;
+        if (int e = getGraph(nsteps, with_group, &ex)) return e;
+        MDX_CUDA_TRY(cudaGraphLaunch(ex, s->stream));
+        g_launches += graph_kernels[std::make_pair(nsteps, with_group ? 1 : 0)];
+        return 0;
+    }
+    // bench support: nturns in chunks of `chunk`, each chunk bracketed by
+    // CUDA events on the library stream, L2 flushed (a write larger than L2)
+    // before every chunk outside the timed windows; returns summed device ms
+    int runTimed(int nturns, int chunk, size_t flush_bytes, double *ms_total) {
+        if (!s->prepared) {
+            clearGraphs();
+            if (int e = s->prepare()) return e;
+        }
+        DBuf<char> flush;
+        if (flush_bytes)
+            if (int e = flush.alloc(flush_bytes)) return e;
+        std::vector<cudaEvent_t> ev;
+        const int P = s->periodicInterval > 0 ? s->periodicInterval : 1;
+        int done = 0;
+        while (done < nturns) {
+            if (flush_bytes) MDX_CUDA_TRY(cudaMemsetAsync(flush.p, (int)(done & 0xff), flush_bytes, s->stream));
+            cudaEvent_t a, b;
+            MDX_CUDA_TRY(cudaEventCreate(&a));
+            MDX_CUDA_TRY(cudaEventCreate(&b));
+            MDX_CUDA_TRY(cudaEventRecord(a, s->stream));
+            int todo = std::min(chunk, nturns - done);
+            while (todo > 0) {
+                const int64_t t = s->turn;
+                const bool check = (t % P) == 0;
+                int c = check ? P : (int)(P - (t % P));
+                c = std::min(c, todo);
+                if (int e = launchGraph(c, check)) return e;
+                s->turn += c;
+                todo -= c;
+                done += c;
+            }
+            MDX_CUDA_TRY(cudaEventRecord(b, s->stream));
+            ev.push_back(a);
+            ev.push_back(b);
+        }
+        MDX_CUDA_TRY(cudaStreamSynchronize(s->stream));
+        double tot = 0.0;
+        for (size_t k = 0; k < ev.size(); k += 2) {
+            float ms = 0.f;
+            MDX_CUDA_TRY(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+            tot += ms;
+            cudaEventDestroy(ev[k]);
+            cudaEventDestroy(ev[k + 1]);
+        }
+        *ms_total = tot;
+        return s->checkStatus();
+    }
+
+    // run with host buffers in/out (the call a host program makes): inputs are
+    // copied from pinned staging and scattered by id, outputs gathered by id
+    // and copied back, all inside the call
+    float4 *h_stage = nullptr;
+    size_t h_stage_n = 0;
+    DBuf<float4> d_stage;
+    int runHost(int nturns, const double *pin, const double *vin, double *pout, double *vout, double *fout) {
+        if (!s->prepared) {
+            clearGraphs();
+            if (int e = s->prepare()) return e;
+        }
+        const int n = s->gpd.n;
+        if (h_stage_n < (size_t)3 * n) {
+            if (h_stage) cudaFreeHost(h_stage);
+            MDX_CUDA_TRY(cudaMallocHost(&h_stage, 3 * (size_t)n * sizeof(float4)));
+            h_stage_n = 3 * (size_t)n;
+        }
+        if (int e = d_stage.alloc(3 * (size_t)n)) return e;
+        const double *ins[2] = {pin, vin};
+        float4 *dsts[2] = {s->gpd.xs.p, s->gpd.vs.p};
+        for (int k = 0; k < 2; k++) {
+            if (!ins[k]) continue;
+            float4 *h = h_stage + (size_t)k * n;
+            for (int i = 0; i < n; i++)
+                h[i] = make_float4((float)ins[k][3 * i], (float)ins[k][3 * i + 1], (float)ins[k][3 * i + 2], 0.f);
+            MDX_CUDA_TRY(cudaMemcpyAsync(d_stage.p + (size_t)k * n, h, n * sizeof(float4), cudaMemcpyHostToDevice,
+                                         s->stream));
+            k_put_by_id<<<(n + 255) / 256, 256, 0, s->stream>>>(n, d_stage.p + (size_t)k * n, s->gpd.idToIdx.p,
+                                                              dsts[k]);
+            MDX_LAUNCHED();
+        }
+        const int P = s->periodicInterval > 0 ? s->periodicInterval : 1;
+        int done = 0;
+        while (done < nturns) {
+            const int64_t t = s->turn;
+            const bool check = (t % P) == 0;
+            int c = check ? P : (int)(P - (t % P));
+            c = std::min(c, nturns - done);
+            if (int e = launchGraph(c, check)) return e;
+            s->turn += c;
+            done += c;
+        }
+        if (nturns > 0)
+            if (int e = nh_end_of_run(*s)) return e;
+        double *outs[3] = {pout, vout, fout};
+        const float4 *srcs[3] = {s->gpd.xs.p, s->gpd.vs.p, s->gpd.fs.p};
+        for (int k = 0; k < 3; k++) {
+            if (!outs[k]) continue;
+            k_get_by_id<<<(n + 255) / 256, 256, 0, s->stream>>>(n, srcs[k], s->gpd.ids.p, d_stage.p + (size_t)k * n);
+            MDX_LAUNCHED();
+            MDX_CUDA_TRY(cudaMemcpyAsync(h_stage + (size_t)k * n, d_stage.p + (size_t)k * n, n * sizeof(float4),
+                                         cudaMemcpyDeviceToHost, s->stream));
+        }
+        MDX_CUDA_TRY(cudaMemcpyAsync(s->h_status, s->d_status.p, sizeof(DeviceStatus), cudaMemcpyDeviceToHost,
+                                     s->stream));
+        MDX_CUDA_TRY(cudaStreamSynchronize(s->stream));
+        for (int k = 0; k < 3; k++) {
+            if (!outs[k]) continue;
+            const float4 *h = h_stage + (size_t)k * n;
+            for (int i = 0; i < n; i++) {
+                outs[k][3 * i] = h[i].x;
+                outs[k][3 * i + 1] = h[i].y;
+                outs[k][3 * i + 2] = h[i].z;
+            }
+        }
+        if (s->h_status->bits) return s->checkStatus();
+        return 0;
+    }
+
+    int run(int nturns, double *ptsps) {
+        if (nturns < 0) {
+            set_error(MDX_ERR_ARG, "numTurns must be >= 0");
+            return MDX_ERR_ARG;
+        }
+        if (!s->prepared) {
+            clearGraphs();
+            if (int e = s->prepare()) return e;
+        }
+        const int P = s->periodicInterval > 0 ? s->periodicInterval : 1;
+        cudaEvent_t e0, e1;
+        MDX_CUDA_TRY(cudaEventCreate(&e0));
+        MDX_CUDA_TRY(cudaEventCreate(&e1));
+        MDX_CUDA_TRY(cudaEventRecord(e0, s->stream));
+        int done = 0;
+        while (done < nturns) {
+            const int64_t t = s->turn;
+            const bool check = (t % P) == 0;
+            int chunk = check ? P : (int)(P - (t % P));
+            if (chunk > nturns - done) chunk = nturns - done;
+            if (mode == 0) {
+                if (int e = launchGraph(chunk, check)) return e;
+            } else {
+                if (int e = enqueue(chunk, check)) return e;
+            }
+            s->turn += chunk;
+            done += chunk;
+        }
+        MDX_CUDA_TRY(cudaEventRecord(e1, s->stream));
+        if (nturns > 0)
+            if (int e = nh_end_of_run(*s)) return e;
+        MDX_CUDA_TRY(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        MDX_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        MDX_CUDA_TRY(cudaGetLastError());
+        if (int e = s->checkStatus()) return e;
+        if (ptsps) *ptsps = ms > 0 ? (double)s->atoms.size() * nturns / (ms * 1e-3) : 0.0;
+        if (FixNoseHoover *nh = s->nhFix()) {
+            NHChain c[2];
+            MDX_CUDA_TRY(cudaMemcpy(c, nh->d_chain.p, sizeof(c), cudaMemcpyDeviceToHost));
+            nh->h = c[0];
+        }
+        return s->download();
+    }
+};
+
+}  // namespace mdx
+
+struct mdx_integrator {
+    mdx::IntegratorVerlet *it;
+};
+
+using namespace mdx;
+
+extern "C" {
+
+int mdx_integrator_verlet_create(mdx_state *st, mdx_integrator **out) {
+    if (!st || !out) {
+        set_error(MDX_ERR_ARG, "null argument");
+        return MDX_ERR_ARG;
+    }
+    *out = new mdx_integrator{new IntegratorVerlet(st->s)};
+    return 0;
+}
+
+int mdx_integrator_run(mdx_integrator *it, int num_turns, double *ptsps_out) {
+    if (!it) {
+        set_error(MDX_ERR_ARG, "null integrator");
+        return MDX_ERR_ARG;
+    }
+    try {
+        return it->it->run(num_turns, ptsps_out);
+    } catch (...) {
+        set_error(MDX_ERR_STATE, "exception in run");
+        return MDX_ERR_STATE;
+    }
+}
+
+int mdx_integrator_run_timed(mdx_integrator *it, int num_turns, int chunk, size_t flush_bytes, double *device_ms) {
+    if (!it || !device_ms || num_turns < 0 || chunk <= 0) {
+        set_error(MDX_ERR_ARG, "bad argument");
+        return MDX_ERR_ARG;
+    }
+    if (it->it->mode != 0) {
+        set_error(MDX_ERR_STATE, "timed runs use the fused graph mode");
+        return MDX_ERR_STATE;
+    }
+    try {
+        return it->it->runTimed(num_turns, chunk, flush_bytes, device_ms);
+    } catch (...) {
+        set_error(MDX_ERR_STATE, "exception in run");
+        return MDX_ERR_STATE;
+    }
+}
+
+int mdx_integrator_run_host(mdx_integrator *it, int num_turns, const double *pos_in, const double *vel_in,
+                            double *pos_out, double *vel_out, double *force_out) {
+    if (!it || num_turns < 0) {
+        set_error(MDX_ERR_ARG, "bad argument");
+        return MDX_ERR_ARG;
+    }
+    if (it->it->mode != 0) {
+        set_error(MDX_ERR_STATE, "host-buffer runs use the fused graph mode");
+        return MDX_ERR_STATE;
+    }
+    try {
+        return it->it->runHost(num_turns, pos_in, vel_in, pos_out, vel_out, force_out);
+    } catch (...) {
+        set_error(MDX_ERR_STATE, "exception in run");
+        return MDX_ERR_STATE;
+    }
+}
+
+int mdx_integrator_set_mode(mdx_integrator *it, int mode) {
+    if (!it || (mode != 0 && mode != 1)) {
+        set_error(MDX_ERR_ARG, "mode must be 0 (fused graph) or 1 (hook by hook)");
+        return MDX_ERR_ARG;
+    }
+    it->it->mode = mode;
+    it->it->clearGraphs();
+    return 0;
+}
+
+int mdx_integrator_destroy(mdx_integrator *it) {
+    if (!it) return 0;
+    delete it->it;
+    delete it;
+    return 0;
+}
+
+}  // extern "C"

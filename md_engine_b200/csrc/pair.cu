@@ -1,0 +1,319 @@
+// Short-range pair forces: LJ/cut or WCA plus the Ewald real-space term
+// offloaded into the same kernel (compute_force_iso, PairEvaluateIso.h:8-207,
+// with EvaluatorLJ PairEvaluatorLJ.h:17-60, EvaluatorWCA PairEvaluatorWCA.h:13-38,
+// ChargeEvaluatorEwald ChargeEvaluatorEwald.h:11-64; charge offload
+// State.cpp:648-660).
+//
+// Layout: a team of T lanes per atom i walks i's neighbour row; a warp covers
+// 32/T atoms, so every list load is one 128-byte row.  Per-type-pair
+// parameters {rc^2, 24 eps, sig^6} sit in shared memory (the reference's
+// paramsCoalesced order).  The team's partial forces (and the optional
+// per-atom virial, x0.5 as helpers.h:34-41 / PairEvaluateIso.h:180-195) are
+// reduced with register shuffles, not shared memory.
+#include <cstdio>
+
+#include "engine.hpp"
+
+namespace mdx {
+
+namespace {
+
+template <int T>
+__device__ __forceinline__ float team_sum(float v) {
+#pragma unroll
+    for (int o = T / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+struct PairArgs {
+    int n;
+    const float4 *__restrict__ xs;
+    float4 *__restrict__ fs;
+    const float *__restrict__ qs;
+    const uint32_t *__restrict__ counts;
+    const uint32_t *__restrict__ nlist;
+    int cap;
+    const float *__restrict__ params;
+    int ntypes;
+    Box box;
+    float coef1, coef2, coef3;
+    float qrc2, alpha, qqr;
+    float *__restrict__ virials;
+    float *__restrict__ energy;  // per-atom (energy kernel)
+};
+
+// one neighbour: returns the scalar force factor (F = dr * s) and energy
+template <int LJ, bool EW, bool ENERGY>
+__device__ __forceinline__ bool pair_term(const PairArgs &A, const float *sp, int nt2, int ti, float qi, float4 xj,
+                                          float qj, float3 dr, float r2, float mult, float &s, float &e) {
+    bool any = false;
+    s = 0.f;
+    e = 0.f;
+    if (LJ) {
+        const int tj = type_of(xj);
+        const int ix = ti * A.ntypes + tj;
+        const float rc2 = sp[ix];
+        if (r2 < rc2) {
+            any = true;
+            if (mult != 0.f) {
+                const float eps24 = sp[nt2 + ix];
+                const float sig6 = sp[2 * nt2 + ix];
+                const float p1 = eps24 * 2.f * sig6 * sig6;
+                const float p2 = eps24 * sig6;
+                const float r2inv = 1.0f / r2;
+                const float r6inv = r2inv * r2inv * r2inv;
+                s += r6inv * r2inv * (p1 * r6inv - p2) * mult;
+                if (ENERGY) {
+                    const float eps = eps24 / 24.0f;
+                    const float s6r6 = sig6 * r6inv;
+                    if (LJ == 1) {
+                        const float rc6 = rc2 * rc2 * rc2;
+                        const float s6rc6 = sig6 / rc6;
+                        const float off = s6rc6 * (s6rc6 - 1.0f);
+                        e += 0.5f * 4.0f * eps * (s6r6 * (s6r6 - 1.0f) - off) * mult;
+                    } else {
+                        e += 0.5f * (4.0f * eps * s6r6 * (s6r6 - 1.0f) + eps) * mult;
+                    }
+                }
+            }
+        }
+    }
+    if (EW) {
+        if (r2 < A.qrc2) {
+            any = true;
+            const float r2c = r2 < 1e-10f ? 1e-10f : r2;
+            const float r2inv = 1.0f / r2c;
+            const float rinv = sqrtf(r2inv);
+            const float len = sqrtf(r2c);
+            const float qq = A.qqr * qi * qj;
+            const float erfcv = erfcf(A.alpha * len);
+            float fsc = qq * (erfcv * rinv + (2.0f * 0.5641895835477563f * A.alpha) * expf(-A.alpha * A.alpha * r2c));
+            if (mult < 1.0f) fsc -= (1.0f - mult) * qq * rinv;
+            s += fsc * r2inv;
+            if (ENERGY) {
+                float eng = qq * rinv * erfcv;
+                if (mult < 1.0f) eng -= (1.0f - mult) * qq * rinv;
+                e += 0.5f * eng;
+            }
+        }
+    }
+    return any;
+}
+
+template <int T, int LJ, bool EW, bool VIR, bool ENERGY>
+__global__ void __launch_bounds__(256) k_pair(PairArgs A, int accumulate) {
+    extern __shared__ float sp[];
+    const int nt2 = A.ntypes * A.ntypes;
+    if (LJ) {
+        for (int k = threadIdx.x; k < 3 * nt2; k += blockDim.x) sp[k] = A.params[k];
+        __syncthreads();
+    }
+    constexpr int G = 32 / T;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int a = lane / T, t = lane % T;
+    const int i = warp * G + a;
+    const bool valid = i < A.n;
+    float fx = 0.f, fy = 0.f, fz = 0.f, en = 0.f;
+    float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f, v4 = 0.f, v5 = 0.f;
+    float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (valid) {
+        xi = A.xs[i];
+        const int ti = type_of(xi);
+        const float qi = EW ? A.qs[i] : 0.f;
+        int cnt = (int)A.counts[i];
+        cnt = cnt < A.cap ? cnt : A.cap;
+        const uint32_t *row = A.nlist + (size_t)(i / G) * A.cap * G + a * T + t;
+        const float mults[4] = {1.0f, A.coef1, A.coef2, A.coef3};
+        for (int k = t; k < cnt; k += T) {
+            const uint32_t e = __ldg(row + (size_t)(k / T) * 32);
+            const int j = (int)(e & kExclMask);
+            const float mult = mults[e >> 30];
+            const float4 xj = __ldg(A.xs + j);
+            const float3 dr = min_image(A.box, make_float3(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z));
+            const float r2 = dot3(dr, dr);
+            const float qj = EW ? __ldg(A.qs + j) : 0.f;
+            float s, eng;
+            if (pair_term<LJ, EW, ENERGY>(A, sp, nt2, ti, qi, xj, qj, dr, r2, mult, s, eng)) {
+                const float Fx = dr.x * s, Fy = dr.y * s, Fz = dr.z * s;
+                fx += Fx;
+                fy += Fy;
+                fz += Fz;
+                if (ENERGY) en += eng;
+                if (VIR) {
+                    v0 += Fx * dr.x;
+                    v1 += Fy * dr.y;
+                    v2 += Fz * dr.z;
+                    v3 += Fx * dr.y;
+                    v4 += Fx * dr.z;
+                    v5 += Fy * dr.z;
+                }
+            }
+        }
+    }
+    // invalid lanes carry zeros; whole warp takes part in the shuffles
+    if (ENERGY) {
+        en = team_sum<T>(en);
+        if (valid && t == 0) A.energy[i] = en;
+        return;
+    }
+    fx = team_sum<T>(fx);
+    fy = team_sum<T>(fy);
+    fz = team_sum<T>(fz);
+    if (VIR) {
+        v0 = team_sum<T>(v0);
+        v1 = team_sum<T>(v1);
+        v2 = team_sum<T>(v2);
+        v3 = team_sum<T>(v3);
+        v4 = team_sum<T>(v4);
+        v5 = team_sum<T>(v5);
+    }
+    if (valid && t == 0) {
+        float4 f = A.fs[i];
+        if (accumulate) {
+            f.x += fx;
+            f.y += fy;
+            f.z += fz;
+        } else {
+            f.x = fx;
+            f.y = fy;
+            f.z = fz;
+        }
+        A.fs[i] = f;
+        if (VIR) {
+            float *v = A.virials + 6 * (size_t)i;
+            v[0] += 0.5f * v0;
+            v[1] += 0.5f * v1;
+            v[2] += 0.5f * v2;
+            v[3] += 0.5f * v3;
+            v[4] += 0.5f * v4;
+            v[5] += 0.5f * v5;
+        }
+    }
+}
+
+template <int T, int LJ, bool EW>
+void launch_t(const PairArgs &A, bool vir, bool energy, bool accumulate, cudaStream_t st) {
+    const int G = 32 / T;
+    const int warps = (A.n + G - 1) / G;
+    const int blocks = (warps * 32 + 255) / 256;
+    const size_t smem = LJ ? 3 * A.ntypes * A.ntypes * sizeof(float) : 0;
+    if (energy)
+        k_pair<T, LJ, EW, false, true><<<blocks, 256, smem, st>>>(A, 0);
+    else if (vir)
+        k_pair<T, LJ, EW, true, false><<<blocks, 256, smem, st>>>(A, accumulate ? 1 : 0);
+    else
+        k_pair<T, LJ, EW, false, false><<<blocks, 256, smem, st>>>(A, accumulate ? 1 : 0);
+    MDX_LAUNCHED();
+}
+
+template <int T>
+int launch_kind(const PairArgs &A, int lj, bool ew, bool vir, bool energy, bool acc, cudaStream_t st) {
+    if (lj == 0 && ew) launch_t<T, 0, true>(A, vir, energy, acc, st);
+    else if (lj == 1 && ew) launch_t<T, 1, true>(A, vir, energy, acc, st);
+    else if (lj == 1) launch_t<T, 1, false>(A, vir, energy, acc, st);
+    else if (lj == 2 && ew) launch_t<T, 2, true>(A, vir, energy, acc, st);
+    else if (lj == 2) launch_t<T, 2, false>(A, vir, energy, acc, st);
+    else return MDX_ERR_ARG;
+    return 0;
+}
+
+int launch_any(const PairArgs &A, int team, int lj, bool ew, bool vir, bool energy, bool acc, cudaStream_t st) {
+    switch (team) {
+        case 1: return launch_kind<1>(A, lj, ew, vir, energy, acc, st);
+        case 2: return launch_kind<2>(A, lj, ew, vir, energy, acc, st);
+        case 4: return launch_kind<4>(A, lj, ew, vir, energy, acc, st);
+        case 8: return launch_kind<8>(A, lj, ew, vir, energy, acc, st);
+        case 16: return launch_kind<16>(A, lj, ew, vir, energy, acc, st);
+        case 32: return launch_kind<32>(A, lj, ew, vir, energy, acc, st);
+    }
+    set_error(MDX_ERR_ARG, "team size %d not in {1,2,4,8,16,32}", team);
+    return MDX_ERR_ARG;
+}
+
+PairArgs make_args(State &s, FixPair &f) {
+    PairArgs A;
+    A.n = s.gpd.n;
+    A.xs = s.gpd.xs.p;
+    A.fs = s.gpd.fs.p;
+    A.qs = s.gpd.qs.p;
+    A.counts = s.grid.counts.p;
+    A.nlist = s.grid.nlist.p;
+    A.cap = s.grid.cap;
+    A.params = f.d_params.p;
+    A.ntypes = (int)s.species.size();
+    A.box = s.box;
+    A.coef1 = s.specialNeighborCoefs[0];
+    A.coef2 = s.specialNeighborCoefs[1];
+    A.coef3 = s.specialNeighborCoefs[2];
+    A.qrc2 = 0.f;
+    A.alpha = 0.f;
+    A.qqr = (float)s.units.qqr_to_eng;
+    if (f.chargeFix) {
+        float qrc = (float)f.chargeRCut;
+        A.qrc2 = qrc * qrc;
+        A.alpha = (float)f.chargeFix->alpha;
+    }
+    A.virials = s.gpd.virials.p;
+    A.energy = nullptr;
+    return A;
+}
+
+}  // namespace
+
+int pair_launch(State &s, FixPair &f, int virialMode, bool accumulate) {
+    PairArgs A = make_args(s, f);
+    bool vir = virialMode == 1 || virialMode == 2;
+    return launch_any(A, s.grid.team, f.lj_kind, f.chargeFix != nullptr, vir, false, accumulate, s.stream);
+}
+
+int pair_energy(State &s, FixPair &f, double *out) {
+    PairArgs A = make_args(s, f);
+    DBuf<float> e;
+    if (int r = e.alloc(A.n)) return r;
+    A.energy = e.p;
+    if (int r = launch_any(A, s.grid.team, f.lj_kind, f.chargeFix != nullptr, false, true, false, s.stream)) return r;
+    // widen to double for the FP64 reduction
+    DBuf<double> ed;
+    if (int r = ed.alloc(A.n)) return r;
+    std::vector<float> h(A.n);
+    MDX_CUDA_TRY(cudaMemcpyAsync(h.data(), e.p, A.n * sizeof(float), cudaMemcpyDeviceToHost, s.stream));
+    MDX_CUDA_TRY(cudaStreamSynchronize(s.stream));
+    double sum = 0.0;
+    for (int i = 0; i < A.n; i++) sum += (double)h[i];
+    *out = sum;
+    return 0;
+}
+
+int pair_force_raw(int n, const float4 *xs, float4 *fs, const float *qs, const uint32_t *counts,
+                   const uint32_t *nlist, int team, int cap, const float *params, int ntypes, const Box &box,
+                   const float coef[3], int lj_kind, float qrc, float alpha, float qqr, float *virials,
+                   bool accumulate, cudaStream_t stream) {
+    PairArgs A;
+    A.n = n;
+    A.xs = xs;
+    A.fs = fs;
+    A.qs = qs;
+    A.counts = counts;
+    A.nlist = nlist;
+    A.cap = cap;
+    A.params = params;
+    A.ntypes = ntypes;
+    A.box = box;
+    A.coef1 = coef[0];
+    A.coef2 = coef[1];
+    A.coef3 = coef[2];
+    A.qrc2 = qrc > 0.f ? qrc * qrc : 0.f;
+    A.alpha = alpha;
+    A.qqr = qqr;
+    A.virials = virials;
+    A.energy = nullptr;
+    bool ew = qrc > 0.f;
+    if (lj_kind == 0 && !ew) return 0;
+    int r = launch_any(A, team, lj_kind, ew, virials != nullptr, false, accumulate, stream);
+    if (r) return r;
+    MDX_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+}  // namespace mdx

@@ -1,0 +1,442 @@
+"""Python front end mirroring DASH's Python API (python/DASH.cpp:34-131) for
+the hot path: State, Bounds, Vector, units, atomParams, FixLJCut, FixWCA,
+FixChargeEwald, FixE3B, FixRigid, FixNoseHoover, IntegratorVerlet.
+
+Every call goes through the C ABI of libmdx.so (include/mdx.h); argument
+names and meanings follow the reference, e.g.
+
+    state = State()
+    state.units.setReal()
+    state.bounds = Bounds(state, lo=Vector(0, 0, 0), hi=Vector(L, L, L))
+    state.rCut = 9.0; state.padding = 1.0; state.dt = 2.0
+    state.atomParams.addSpecies(handle='OW', mass=15.9994, atomicNum=8)
+    lj = FixLJCut(state, 'cut'); lj.setParameter('sig', 'OW', 'OW', 3.1589)
+    state.activateFix(lj)
+    IntegratorVerlet(state).run(1000)
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from ._lib import P, c_dbl, c_i64, c_int, c_u32, c_u64, c_void_p, check, lib
+
+UNITS_REAL = 0
+UNITS_LJ = 1
+
+
+class Vector:
+    """3-vector with the arithmetic scripts use (src/Vector.h)."""
+
+    def __init__(self, x=0.0, y=0.0, z=0.0):
+        self.v = np.array([float(x), float(y), float(z)])
+
+    def __getitem__(self, i):
+        return self.v[i]
+
+    def __add__(self, o):
+        return Vector(*(self.v + np.asarray(o.v if isinstance(o, Vector) else o)))
+
+    def __sub__(self, o):
+        return Vector(*(self.v - np.asarray(o.v if isinstance(o, Vector) else o)))
+
+    def __mul__(self, s):
+        return Vector(*(self.v * s))
+
+    def len(self):
+        return float(np.linalg.norm(self.v))
+
+    def __repr__(self):
+        return f"Vector({self.v[0]}, {self.v[1]}, {self.v[2]})"
+
+
+class Bounds:
+    def __init__(self, state, lo, hi):
+        self.lo = lo if isinstance(lo, Vector) else Vector(*lo)
+        self.hi = hi if isinstance(hi, Vector) else Vector(*hi)
+
+
+class _Units:
+    def __init__(self, st):
+        self._st = st
+
+    def setReal(self):
+        check(lib().mdx_state_set_units(self._st._h, UNITS_REAL))
+        self._st._units = UNITS_REAL
+
+    def setLJ(self):
+        check(lib().mdx_state_set_units(self._st._h, UNITS_LJ))
+        self._st._units = UNITS_LJ
+
+
+class _AtomParams:
+    def __init__(self, st):
+        self._st = st
+        self.handles = []
+        self.masses = []
+
+    def addSpecies(self, handle, mass, atomicNum=0):
+        t = c_int()
+        check(lib().mdx_state_add_species(self._st._h, handle.encode(), float(mass), int(atomicNum), ctypes.byref(t)))
+        self.handles.append(handle)
+        self.masses.append(float(mass))
+        return t.value
+
+    def typeFromHandle(self, handle):
+        return self.handles.index(handle)
+
+    @property
+    def numTypes(self):
+        return len(self.handles)
+
+
+def _darr(a, n=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a, a.ctypes.data_as(P(c_dbl))
+
+
+class State:
+    """src/State.h:63-146 -- owns the atoms and the device copy."""
+
+    _DOUBLE_KEYS = ("rCut", "padding", "dt")
+    _INT_KEYS = ("periodicInterval", "nThreadPerAtom", "nThreadPerBlock", "turn")
+
+    def __init__(self):
+        h = c_void_p()
+        check(lib().mdx_state_create(ctypes.byref(h)))
+        object.__setattr__(self, "_h", h)
+        object.__setattr__(self, "units", _Units(self))
+        object.__setattr__(self, "atomParams", _AtomParams(self))
+        object.__setattr__(self, "_bounds", None)
+        object.__setattr__(self, "_fixes", [])
+        object.__setattr__(self, "_units", UNITS_LJ)
+        object.__setattr__(self, "_charges", [])
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                lib().mdx_state_destroy(h)
+            except Exception:
+                pass
+
+    def __setattr__(self, k, v):
+        if k in self._DOUBLE_KEYS:
+            check(lib().mdx_state_set_double(self._h, k.encode(), float(v)))
+        elif k in self._INT_KEYS:
+            check(lib().mdx_state_set_int(self._h, k.encode(), int(v)))
+        elif k == "bounds":
+            lo = (ctypes.c_double * 3)(*v.lo.v)
+            hi = (ctypes.c_double * 3)(*v.hi.v)
+            check(lib().mdx_state_set_bounds(self._h, lo, hi))
+            object.__setattr__(self, "_bounds", v)
+        else:
+            object.__setattr__(self, k, v)
+
+    def __getattr__(self, k):
+        if k in State._DOUBLE_KEYS:
+            out = c_dbl()
+            check(lib().mdx_state_get_double(self._h, k.encode(), ctypes.byref(out)))
+            return out.value
+        if k in State._INT_KEYS or k in ("nlistCapacity", "cellsPerSide"):
+            out = c_i64()
+            check(lib().mdx_state_get_int(self._h, k.encode(), ctypes.byref(out)))
+            return out.value
+        if k == "bounds":
+            return object.__getattribute__(self, "_bounds")
+        raise AttributeError(k)
+
+    def setSpecialNeighborCoefs(self, onetwo, onethree, onefour):
+        check(lib().mdx_state_set_special_neighbor_coefs(self._h, onetwo, onethree, onefour))
+
+    # -- atoms ------------------------------------------------------------
+    def addAtom(self, handle, pos, q=0.0):
+        p = pos.v if isinstance(pos, Vector) else pos
+        return self.addAtoms([handle], np.asarray([p], np.float64), np.asarray([q], np.float64))
+
+    def addAtoms(self, handles, positions, charges=None):
+        """Bulk State::addAtom; returns the first new id (ids are consecutive)."""
+        n = len(handles)
+        pos, pp = _darr(np.asarray(positions, np.float64).reshape(n, 3))
+        q = np.zeros(n) if charges is None else np.asarray(charges, np.float64)
+        q, qp = _darr(q)
+        enc = [h.encode() for h in handles]
+        arr = (ctypes.c_char_p * n)(*enc)
+        first = c_int()
+        check(lib().mdx_state_add_atoms(self._h, n, arr, pp, qp, ctypes.byref(first)))
+        self._charges.extend(q.tolist())
+        return first.value
+
+    @property
+    def nAtoms(self):
+        n = c_int()
+        check(lib().mdx_state_n_atoms(self._h, ctypes.byref(n)))
+        return n.value
+
+    def setVelocities(self, ids, vels):
+        ids = np.ascontiguousarray(ids, np.int32)
+        v, vp = _darr(np.asarray(vels).reshape(len(ids), 3))
+        check(lib().mdx_state_set_velocities(self._h, len(ids), ids.ctypes.data_as(P(c_int)), vp))
+
+    def getAtoms(self):
+        """(positions, velocities, forces) by atom id, (n,3) float64."""
+        n = self.nAtoms
+        x = np.zeros((n, 3))
+        v = np.zeros((n, 3))
+        f = np.zeros((n, 3))
+        check(lib().mdx_state_get_atoms(self._h, x.ctypes.data_as(P(c_dbl)), v.ctypes.data_as(P(c_dbl)),
+                                        f.ctypes.data_as(P(c_dbl))))
+        return x, v, f
+
+    def putAtoms(self, positions=None, velocities=None):
+        px = vx = None
+        if positions is not None:
+            xa, px = _darr(positions)
+        if velocities is not None:
+            va, vx = _darr(velocities)
+        check(lib().mdx_state_put_atoms(self._h, px, vx))
+
+    def activateFix(self, fix):
+        check(lib().mdx_state_activate_fix(self._h, fix._h))
+        self._fixes.append(fix)
+
+    def deactivateFix(self, fix):
+        check(lib().mdx_state_deactivate_fix(self._h, fix._h))
+        if fix in self._fixes:
+            self._fixes.remove(fix)
+
+    # -- stage-level access (tests, observables) ----------------------------
+    def prepare(self):
+        check(lib().mdx_prepare(self._h))
+
+    def buildNeighborlists(self, force=True):
+        check(lib().mdx_nlist_build(self._h, 1 if force else 0))
+
+    def getNeighborList(self, maxPerAtom=None):
+        """Grid.getNeighborList: (counts[id], ids[id, k], tags[id, k]) sorted per id."""
+        n = self.nAtoms
+        if maxPerAtom is None:
+            maxPerAtom = max(int(self.nlistCapacity), 1)
+        c = np.zeros(n, np.int32)
+        nb = np.zeros((n, maxPerAtom), np.int32)
+        tg = np.zeros((n, maxPerAtom), np.int32)
+        check(lib().mdx_nlist_get(self._h, maxPerAtom, c.ctypes.data_as(P(c_int)), nb.ctypes.data_as(P(c_int)),
+                                  tg.ctypes.data_as(P(c_int))))
+        return c, nb, tg
+
+    def computeForces(self, virialMode=0):
+        check(lib().mdx_compute_forces(self._h, int(virialMode)))
+
+    def potentialEnergy(self):
+        """[pair (LJ/WCA + Ewald real), Ewald reciprocal (incl. self), E3B 2-body, E3B 3-body]"""
+        out = (ctypes.c_double * 4)()
+        check(lib().mdx_potential_energy(self._h, out))
+        return np.array(list(out))
+
+    def kinetic(self):
+        s = c_dbl()
+        n = c_dbl()
+        check(lib().mdx_kinetic(self._h, ctypes.byref(s), ctypes.byref(n)))
+        return s.value, n.value
+
+    def virials(self):
+        n = self.nAtoms
+        per = np.zeros((n, 6))
+        tot = (ctypes.c_double * 6)()
+        check(lib().mdx_get_virials(self._h, per.ctypes.data_as(P(c_dbl)), tot))
+        return per, np.array(list(tot))
+
+    def status(self):
+        b = c_u32()
+        m = c_u32()
+        nb = c_u64()
+        check(lib().mdx_state_status(self._h, ctypes.byref(b), ctypes.byref(m), ctypes.byref(nb)))
+        return b.value, m.value, nb.value
+
+    def synchronize(self):
+        check(lib().mdx_state_synchronize(self._h))
+
+    STAGES = {"pair": 0, "p3m": 1, "e3b": 2, "nlist": 3, "first_half": 4, "second_half": 5}
+
+    def timeStage(self, stage, iters=20, flushBytes=0):
+        """average device ms of one launch of a hot-path stage"""
+        out = c_dbl()
+        check(lib().mdx_time_stage(self._h, self.STAGES[stage], int(iters), int(flushBytes), ctypes.byref(out)))
+        return out.value
+
+
+class _Fix:
+    _h = None
+
+    def __del__(self):
+        pass  # fixes live as long as their state (the state owns the device data)
+
+
+class FixPair(_Fix):
+    def setParameter(self, param, handleA, handleB, val):
+        check(lib().mdx_fix_pair_set_parameter(self._h, param.encode(), handleA.encode(), handleB.encode(), float(val)))
+
+
+class FixLJCut(FixPair):
+    """FixLJCut(state, handle, mixingRules='geometric') (src/Fixes/FixLJCut.cu:14-28)"""
+
+    def __init__(self, state, handle, mixingRules="geometric"):
+        h = c_void_p()
+        check(lib().mdx_fix_lj_cut_create(state._h, handle.encode(), mixingRules.encode(), ctypes.byref(h)))
+        self._h = h
+        self.state = state
+        self.handle = handle
+
+
+class FixWCA(FixPair):
+    """FixWCA(state, handle, mixingRules='geometric') (src/Fixes/FixWCA.cu)"""
+
+    def __init__(self, state, handle, mixingRules="geometric"):
+        h = c_void_p()
+        check(lib().mdx_fix_wca_create(state._h, handle.encode(), mixingRules.encode(), ctypes.byref(h)))
+        self._h = h
+        self.state = state
+        self.handle = handle
+
+
+class FixChargeEwald(_Fix):
+    """FixChargeEwald(state, handle, groupHandle) (src/Fixes/FixChargeEwald.cu:828-839)"""
+
+    def __init__(self, state, handle, groupHandle="all"):
+        h = c_void_p()
+        check(lib().mdx_fix_charge_ewald_create(state._h, handle.encode(), groupHandle.encode(), ctypes.byref(h)))
+        self._h = h
+        self.state = state
+
+    def setParameters(self, szx, szy=None, szz=None, rcut=-1.0, interpolation_order=5):
+        """setParameters(sz, rcut, order) or (szx, szy, szz, rcut, order)."""
+        if szy is not None and szz is None:
+            rcut, interpolation_order, szy, szz = szy, (rcut if rcut != -1.0 else 5), szx, szx
+        if szy is None:
+            szy = szz = szx
+        check(lib().mdx_fix_charge_ewald_set_parameters(self._h, int(szx), int(szy), int(szz), float(rcut),
+                                                        int(interpolation_order)))
+
+    def setAlpha(self, alpha):
+        check(lib().mdx_fix_charge_ewald_set_alpha(self._h, float(alpha)))
+
+    @property
+    def alpha(self):
+        a = c_dbl()
+        check(lib().mdx_fix_charge_ewald_get_alpha(self._h, ctypes.byref(a)))
+        return a.value
+
+
+class FixE3B(_Fix):
+    """FixE3B(state, handle, style) (src/Fixes/FixE3B.cu:16-36)"""
+
+    def __init__(self, state, handle, style="E3B3"):
+        h = c_void_p()
+        check(lib().mdx_fix_e3b_create(state._h, handle.encode(), style.encode(), ctypes.byref(h)))
+        self._h = h
+        self.state = state
+
+    def addMolecule(self, id_O, id_H1, id_H2, id_M):
+        check(lib().mdx_fix_e3b_add_molecule(self._h, int(id_O), int(id_H1), int(id_H2), int(id_M)))
+
+
+class FixRigid(_Fix):
+    """FixRigid(state, handle, style) (src/Fixes/FixRigid.cu:18-37)"""
+
+    def __init__(self, state, handle, style="TIP4P/2005"):
+        h = c_void_p()
+        check(lib().mdx_fix_rigid_create(state._h, handle.encode(), style.encode(), ctypes.byref(h)))
+        self._h = h
+        self.state = state
+
+    def createRigid(self, id_a, id_b, id_c, id_d=-1):
+        check(lib().mdx_fix_rigid_create_rigid(self._h, int(id_a), int(id_b), int(id_c), int(id_d)))
+
+    # single hooks (stage-level parity)
+    def savePrev(self):
+        check(lib().mdx_rigid_save_prev(self.state._h, self._h))
+
+    def settlePositions(self):
+        check(lib().mdx_rigid_settle_positions(self.state._h, self._h))
+
+    def settleVelocities(self):
+        check(lib().mdx_rigid_settle_velocities(self.state._h, self._h))
+
+    def distributeMSite(self):
+        check(lib().mdx_rigid_distribute_msite(self.state._h, self._h))
+
+
+class FixNoseHoover(_Fix):
+    """FixNoseHoover(state, handle, groupHandle) (src/Fixes/FixNoseHoover.cu:97-130)"""
+
+    def __init__(self, state, handle, groupHandle="all"):
+        h = c_void_p()
+        check(lib().mdx_fix_nose_hoover_create(state._h, handle.encode(), groupHandle.encode(), ctypes.byref(h)))
+        self._h = h
+        self.state = state
+
+    def setTemperature(self, temperature, timeConstant):
+        check(lib().mdx_fix_nose_hoover_set_temperature(self._h, float(temperature), float(timeConstant)))
+
+
+class IntegratorVerlet:
+    """IntegratorVerlet(state).run(numTurns) (src/Integrators/IntegratorVerlet.cu:649-770)."""
+
+    def __init__(self, state):
+        h = c_void_p()
+        check(lib().mdx_integrator_verlet_create(state._h, ctypes.byref(h)))
+        self._h = h
+        self.state = state
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                lib().mdx_integrator_destroy(h)
+            except Exception:
+                pass
+
+    def setMode(self, mode):
+        """0: fused, CUDA-graph captured (default); 1: one kernel per reference hook."""
+        check(lib().mdx_integrator_set_mode(self._h, int(mode)))
+
+    def run(self, numTurns):
+        out = c_dbl()
+        check(lib().mdx_integrator_run(self._h, int(numTurns), ctypes.byref(out)))
+        return out.value
+
+    def runHost(self, numTurns, positions=None, velocities=None, want=("pos", "vel", "force")):
+        """run with host buffers: copy positions/velocities (by id) in, step,
+        copy positions/velocities/forces out -- all inside one C-ABI call."""
+        n = self.state.nAtoms
+
+        def inp(a):
+            if a is None:
+                return None, None
+            a = np.ascontiguousarray(a, np.float64).reshape(n, 3)
+            return a, a.ctypes.data_as(P(c_dbl))
+
+        pa, pp = inp(positions)
+        va, vp = inp(velocities)
+        outs = {k: np.zeros((n, 3)) for k in want}
+        op = [outs[k].ctypes.data_as(P(c_dbl)) if k in outs else None for k in ("pos", "vel", "force")]
+        check(lib().mdx_integrator_run_host(self._h, int(numTurns), pp, vp, op[0], op[1], op[2]))
+        return outs
+
+    def runTimed(self, numTurns, chunk, flushBytes):
+        """device milliseconds summed over chunks (L2 flushed between chunks)"""
+        out = c_dbl()
+        check(lib().mdx_integrator_run_timed(self._h, int(numTurns), int(chunk), int(flushBytes), ctypes.byref(out)))
+        return out.value
+
+    # stage-level halves
+    def firstHalf(self):
+        check(lib().mdx_verlet_first_half(self.state._h))
+
+    def secondHalf(self):
+        check(lib().mdx_verlet_second_half(self.state._h))
+
+
+def kernel_launches():
+    return int(lib().mdx_kernel_launch_count())

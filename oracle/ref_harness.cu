@@ -1,0 +1,185 @@
+// Harness around the REFERENCE's own force kernels -- TEST INFRASTRUCTURE ONLY.
+//
+// Compiled by oracle/ref.mk straight from the reference sources where they lie
+// (src/Evaluators/PairEvaluateIso.h, PairEvaluatorLJ.h, PairEvaluatorWCA.h,
+// ChargeEvaluatorEwald.h, ThreeBodyE3B.h, EvaluatorE3B.h and the headers they
+// include) for sm_100a, with the reference's nvcc flags (CMakeLists.txt:53).
+// Nothing here is part of the product; tests load oracle/_ref/librefkernels.so
+// (when present) to compare the B200 kernels with the reference kernels run
+// on the same GPU and the same inputs.
+//
+// The only code written here: C entry points that lay a given neighbour list
+// out in the reference's per-block padded format (GridGPU.cu:777-821,
+// cutils_func.h:23-45), launch the reference kernels exactly as
+// EvaluatorWrapper.h:49-109 / FixE3B.cu:85-347 do, and copy results back.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "ChargeEvaluatorEwald.h"
+#include "ChargeEvaluatorNone.h"
+#include "PairEvaluateIso.h"
+#include "PairEvaluatorLJ.h"
+#include "PairEvaluatorWCA.h"
+#include "ThreeBodyE3B.h"
+
+// declared (not defined) by PairEvaluatorLJ.h; its definition lives in a file
+// that needs Boost.Python
+EvaluatorLJ::EvaluatorLJ() {}
+
+namespace {
+
+template <class T>
+T *dev(const std::vector<T> &h) {
+    T *p = nullptr;
+    cudaMalloc(&p, std::max<size_t>(1, h.size()) * sizeof(T));
+    if (!h.empty()) cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+    return p;
+}
+
+// reference neighbour-list layout for atoms 0..n-1 (NTPA threads per atom,
+// NTPB threads per block): per-block max count, padded per warp
+struct RefLayout {
+    std::vector<uint16_t> counts;
+    std::vector<uint32_t> cum;
+    std::vector<uint32_t> list;
+};
+
+RefLayout make_layout(int n, const int *counts, const uint32_t *nbr, int maxn, int ntpb, int ntpa) {
+    RefLayout L;
+    const int perBlock = ntpb / ntpa;
+    const int nblocks = (n + perBlock - 1) / perBlock;
+    L.counts.resize(n);
+    L.cum.assign(nblocks + 1, 0);
+    for (int b = 0; b < nblocks; b++) {
+        int mx = 0;
+        for (int a = b * perBlock; a < std::min(n, (b + 1) * perBlock); a++) mx = std::max(mx, counts[a]);
+        L.cum[b + 1] = L.cum[b] + (uint32_t)(std::ceil((float)mx / ntpa) * 32);
+    }
+    const int warpsPerBlock = ntpb / 32;
+    L.list.assign((size_t)L.cum[nblocks] * warpsPerBlock + 1, 0u);
+    for (int a = 0; a < n; a++) {
+        L.counts[a] = (uint16_t)counts[a];
+        const int blk = a / perBlock;
+        const uint32_t memPerWarp = L.cum[blk + 1] - L.cum[blk];
+        const int nth = a % perBlock;
+        const int perWarp = 32 / ntpa;
+        const size_t base = (size_t)warpsPerBlock * L.cum[blk] + memPerWarp * (nth / perWarp) + (nth % perWarp) * ntpa;
+        for (int k = 0; k < counts[a]; k++) L.list[base + (k % ntpa) + 32 * (k / ntpa)] = nbr[(size_t)a * maxn + k];
+    }
+    return L;
+}
+
+}  // namespace
+
+extern "C" {
+
+// compute_force_iso<EvaluatorLJ|EvaluatorWCA, ..., ChargeEvaluatorEwald|None>
+// on atoms in the given order.  lj_kind 1 LJ, 2 WCA; qcut <= 0: no charges.
+int ref_pair_forces(int n, const float *xs4, const float *qs, const int *counts, const uint32_t *nbr, int maxn,
+                    const float *params, int ntypes, const float lo[3], const float L[3], float c12, float c13,
+                    float c14, int lj_kind, float qcut, float alpha, float qqr, int ntpb, int ntpa, float *fs4_out) {
+    RefLayout lay = make_layout(n, counts, nbr, maxn, ntpb, ntpa);
+    std::vector<float4> hx(n), hf(n);
+    std::memcpy(hx.data(), xs4, n * sizeof(float4));
+    for (int i = 0; i < n; i++) hf[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    std::vector<float> hq(qs, qs + n), hp(params, params + 3 * ntypes * ntypes);
+    float4 *dx = dev(hx), *df = dev(hf);
+    float *dq = dev(hq), *dp = dev(hp);
+    uint16_t *dc = dev(lay.counts);
+    uint32_t *dl = dev(lay.list), *dcum = dev(lay.cum);
+    BoundsGPU b(make_float3(lo[0], lo[1], lo[2]), make_float3(L[0], L[1], L[2]), make_float3(1.f, 1.f, 1.f));
+    const int blocks = NBLOCKTEAM(n, ntpb, ntpa);
+    const size_t smem = 3 * ntypes * ntypes * sizeof(float) + ntpb * sizeof(float3);
+    ChargeEvaluatorEwald ew(alpha, qqr);
+    ChargeEvaluatorNone none;
+    if (ntpa < 2) return -2;
+    if (lj_kind == 1 && qcut > 0)
+        compute_force_iso<EvaluatorLJ, true, 3, false, ChargeEvaluatorEwald, true, 1><<<blocks, ntpb, smem>>>(
+            n, 1, dx, df, dc, dl, dcum, 32, dp, ntypes, b, c12, c13, c14, nullptr, dq, qcut * qcut, ntpa,
+            EvaluatorLJ(), ew);
+    else if (lj_kind == 1)
+        compute_force_iso<EvaluatorLJ, true, 3, false, ChargeEvaluatorNone, false, 1><<<blocks, ntpb, smem>>>(
+            n, 1, dx, df, dc, dl, dcum, 32, dp, ntypes, b, c12, c13, c14, nullptr, dq, 0.f, ntpa, EvaluatorLJ(), none);
+    else if (lj_kind == 2)
+        compute_force_iso<EvaluatorWCA, true, 3, false, ChargeEvaluatorNone, false, 1><<<blocks, ntpb, smem>>>(
+            n, 1, dx, df, dc, dl, dcum, 32, dp, ntypes, b, c12, c13, c14, nullptr, dq, 0.f, ntpa, EvaluatorWCA(),
+            none);
+    else
+        return -1;
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(hf.data(), df, n * sizeof(float4), cudaMemcpyDeviceToHost);
+    std::memcpy(fs4_out, hf.data(), n * sizeof(float4));
+    cudaFree(dx); cudaFree(df); cudaFree(dq); cudaFree(dp); cudaFree(dc); cudaFree(dl); cudaFree(dcum);
+    return e == cudaSuccess ? 0 : (int)e;
+}
+
+// compute_E3B_force_twobody + compute_E3B_force_threebody (FixE3B::compute,
+// FixE3B.cu:85-347) with the molecule list given (molecule indices), atoms
+// in the given order, E3B3 or E3B2 parameters as FixE3B::createEvaluator.
+int ref_e3b_forces(int natoms, const float *xs4, int nmol, const int *mol4, const int *mcounts, const uint32_t *mnbr,
+                   int maxn, const float lo[3], const float L[3], int style3, int ntpb, int ntpa, float *fs4_out) {
+    RefLayout lay = make_layout(nmol, mcounts, mnbr, maxn, ntpb, ntpa);
+    std::vector<float4> hx(natoms), hf(natoms, make_float4(0.f, 0.f, 0.f, 0.f));
+    std::memcpy(hx.data(), xs4, natoms * sizeof(float4));
+    std::vector<int4> hm(nmol);
+    std::memcpy(hm.data(), mol4, nmol * sizeof(int4));
+    float4 *dx = dev(hx), *df = dev(hf);
+    int4 *dm = dev(hm);
+    uint16_t *dc = dev(lay.counts);
+    uint32_t *dl = dev(lay.list), *dcum = dev(lay.cum);
+    const size_t nl = lay.list.size();
+    std::vector<float4> z4(nl, make_float4(0.f, 0.f, 0.f, 0.f));
+    std::vector<float4> zt(nmol, make_float4(0.f, 0.f, 0.f, 0.f));
+    std::vector<uint32_t> zu(nl, 0u);
+    float4 *tot = dev(zt), *es = dev(z4), *f1 = dev(z4), *f2 = dev(z4), *f3 = dev(z4), *f4 = dev(z4);
+    uint32_t *ct = dev(zu);
+    const float kj = 0.23900573614f;
+    float E2, Ea, Eb, Ec;
+    if (style3) { E2 = 453000.0f; Ea = 150.0f; Eb = -1005.0f; Ec = 1880.0f; }
+    else { E2 = 2349000.0f; Ea = 1745.7f; Eb = -4565.0f; Ec = 7606.8f; }
+    EvaluatorE3B ev(5.0f, 5.2f, E2 * kj, Ea * kj, Eb * kj, Ec * kj, 4.872f, 1.907f);
+    BoundsGPU b(make_float3(lo[0], lo[1], lo[2]), make_float3(L[0], L[1], L[2]), make_float3(1.f, 1.f, 1.f));
+    const int blocks = NBLOCKTEAM(nmol, ntpb, ntpa);
+    const size_t smem = ntpb * 3 * (sizeof(float3) + sizeof(Virial));
+    if (ntpa < 2) return -2;
+    compute_E3B_force_twobody<false, true><<<blocks, ntpb, smem>>>(nmol, 1, dm, dx, df, dc, dl, dcum, 32, tot, es, f1,
+                                                                  f2, f3, f4, ct, ntpa, b, nullptr, ev);
+    compute_E3B_force_threebody<false, true><<<blocks, ntpb, smem>>>(nmol, 1, dm, dx, df, dc, dl, dcum, 32, b, tot,
+                                                                    es, f1, f2, f3, f4, ct, nullptr, ntpa, ev);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(hf.data(), df, natoms * sizeof(float4), cudaMemcpyDeviceToHost);
+    std::memcpy(fs4_out, hf.data(), natoms * sizeof(float4));
+    cudaFree(dx); cudaFree(df); cudaFree(dm); cudaFree(dc); cudaFree(dl); cudaFree(dcum);
+    cudaFree(tot); cudaFree(es); cudaFree(f1); cudaFree(f2); cudaFree(f3); cudaFree(f4); cudaFree(ct);
+    return e == cudaSuccess ? 0 : (int)e;
+}
+
+// the reference's host-callable LJ functor (PairEvaluatorLJ.h:17-30) in the
+// build's precision, for pinning the oracle's per-pair arithmetic on the CPU
+void ref_lj_force_host(float sigma, float eps, float rcut, const float dr[3], float out[3]) {
+    EvaluatorLJ lj;
+    float sig2 = sigma * sigma;
+    float params[3] = {rcut * rcut, eps * 24.0f, sig2 * sig2 * sig2};
+    float3 d = make_float3(dr[0], dr[1], dr[2]);
+    float3 f = lj.force(d, params, d.x * d.x + d.y * d.y + d.z * d.z, 1.0f);
+    out[0] = f.x;
+    out[1] = f.y;
+    out[2] = f.z;
+}
+
+// EvaluatorE3B host/device scalar functions (EvaluatorE3B.h:91-141)
+void ref_e3b_single_host(float r, float out[4]) {
+    const float kj = 0.23900573614f;
+    EvaluatorE3B ev(5.0f, 5.2f, 453000.0f * kj, 150.0f * kj, -1005.0f * kj, 1880.0f * kj, 4.872f, 1.907f);
+    out[0] = ev.switching(r);
+    out[1] = ev.dswitchdr(r);
+    out[2] = ev.threeBodyPairEnergy(r);
+    float3 f = ev.threeBodyForce(make_float3(r, 0.f, 0.f), r);
+    out[3] = f.x;
+}
+
+}  // extern "C"

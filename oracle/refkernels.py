@@ -1,0 +1,85 @@
+"""ctypes access to the reference's own kernels compiled from source
+(oracle/ref.mk -> oracle/_ref/librefkernels.so) -- TEST INFRASTRUCTURE ONLY.
+Used by the GPU parity tests to run the reference kernels on the same GPU and
+inputs as the B200 kernels.  Absent when the reference sources were not
+mounted at build time; callers skip then."""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+PATH = os.path.join(_HERE, "_ref", "librefkernels.so")
+_L = None
+
+
+def available():
+    return os.path.exists(PATH)
+
+
+def lib():
+    global _L
+    if _L is None:
+        _L = ctypes.CDLL(PATH)
+        V = ctypes.c_void_p
+        I = ctypes.c_int
+        F = ctypes.c_float
+        _L.ref_pair_forces.argtypes = [I, V, V, V, V, I, V, I, V, V, F, F, F, I, F, F, F, I, I, V]
+        _L.ref_pair_forces.restype = I
+        _L.ref_e3b_forces.argtypes = [I, V, I, V, V, V, I, V, V, I, I, I, V]
+        _L.ref_e3b_forces.restype = I
+        _L.ref_lj_force_host.argtypes = [F, F, F, V, V]
+        _L.ref_e3b_single_host.argtypes = [F, V]
+    return _L
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def pair_forces(xs4, q, counts, nbr, params_flat, ntypes, lo, L, coef, lj_kind, qcut, alpha, qqr,
+                ntpb=256, ntpa=8):
+    xs4 = np.ascontiguousarray(xs4, np.float32)
+    n = len(xs4)
+    q = np.ascontiguousarray(q if q is not None else np.zeros(n), np.float32)
+    counts = np.ascontiguousarray(counts, np.int32)
+    nbr = np.ascontiguousarray(nbr, np.uint32)
+    pf = np.ascontiguousarray(params_flat, np.float32)
+    lo = np.ascontiguousarray(lo, np.float32)
+    L = np.ascontiguousarray(L, np.float32)
+    out = np.zeros((n, 4), np.float32)
+    rc = lib().ref_pair_forces(n, _p(xs4), _p(q), _p(counts), _p(nbr), nbr.shape[1], _p(pf), ntypes, _p(lo), _p(L),
+                               coef[0], coef[1], coef[2], lj_kind, qcut, alpha, qqr, ntpb, ntpa, _p(out))
+    if rc != 0:
+        raise RuntimeError(f"reference pair kernel failed: {rc}")
+    return out[:, :3].astype(np.float64)
+
+
+def e3b_forces(xs4, mol, mcounts, mnbr, lo, L, style3=True, ntpb=256, ntpa=8):
+    xs4 = np.ascontiguousarray(xs4, np.float32)
+    mol = np.ascontiguousarray(mol, np.int32)
+    mcounts = np.ascontiguousarray(mcounts, np.int32)
+    mnbr = np.ascontiguousarray(mnbr, np.uint32)
+    lo = np.ascontiguousarray(lo, np.float32)
+    L = np.ascontiguousarray(L, np.float32)
+    out = np.zeros((len(xs4), 4), np.float32)
+    rc = lib().ref_e3b_forces(len(xs4), _p(xs4), len(mol), _p(mol), _p(mcounts), _p(mnbr), mnbr.shape[1], _p(lo),
+                              _p(L), 1 if style3 else 0, ntpb, ntpa, _p(out))
+    if rc != 0:
+        raise RuntimeError(f"reference E3B kernels failed: {rc}")
+    return out[:, :3].astype(np.float64)
+
+
+def lj_force_host(sigma, eps, rcut, dr):
+    d = np.ascontiguousarray(dr, np.float32)
+    o = np.zeros(3, np.float32)
+    lib().ref_lj_force_host(sigma, eps, rcut, _p(d), _p(o))
+    return o
+
+
+def e3b_single_host(r):
+    o = np.zeros(4, np.float32)
+    lib().ref_e3b_single_host(float(r), _p(o))
+    return o
