@@ -42,6 +42,18 @@ struct PairArgs {
     float *__restrict__ energy;  // per-atom (energy kernel)
 };
 
+// erfc(x) for x >= 0 by Abramowitz & Stegun, Handbook of Mathematical
+// Functions, eq. 7.1.26 (|error| <= 1.5e-7): erfc(x) = t P5(t) exp(-x^2) with
+// t = 1 / (1 + p x).  exp(-x^2) is passed in: the Ewald force needs it anyway.
+__device__ __forceinline__ float erfc_as(float x, float expmx2) {
+    const float t = __frcp_rn(fmaf(0.3275911f, x, 1.0f));
+    float poly = fmaf(t, 1.061405429f, -1.453152027f);
+    poly = fmaf(t, poly, 1.421413741f);
+    poly = fmaf(t, poly, -0.284496736f);
+    poly = fmaf(t, poly, 0.254829592f);
+    return t * poly * expmx2;
+}
+
 // one neighbour: returns the scalar force factor (F = dr * s) and energy
 template <int LJ, bool EW, bool ENERGY>
 __device__ __forceinline__ bool pair_term(const PairArgs &A, const float *sp, int nt2, int ti, float qi, float4 xj,
@@ -55,8 +67,9 @@ __device__ __forceinline__ bool pair_term(const PairArgs &A, const float *sp, in
         const float rc2 = sp[ix];
         if (r2 < rc2) {
             any = true;
-            if (mult != 0.f) {
-                const float eps24 = sp[nt2 + ix];
+            const float eps24 = sp[nt2 + ix];
+            // eps = 0 (e.g. TIP4P/2005 H and M sites) contributes exactly zero
+            if (mult != 0.f && eps24 != 0.f) {
                 const float sig6 = sp[2 * nt2 + ix];
                 const float p1 = eps24 * 2.f * sig6 * sig6;
                 const float p2 = eps24 * sig6;
@@ -79,15 +92,17 @@ __device__ __forceinline__ bool pair_term(const PairArgs &A, const float *sp, in
         }
     }
     if (EW) {
-        if (r2 < A.qrc2) {
+        // q_i q_j = 0 (e.g. the TIP4P/2005 oxygen) contributes exactly zero
+        if (r2 < A.qrc2 && qi * qj != 0.f) {
             any = true;
             const float r2c = r2 < 1e-10f ? 1e-10f : r2;
-            const float r2inv = 1.0f / r2c;
-            const float rinv = sqrtf(r2inv);
-            const float len = sqrtf(r2c);
+            const float rinv = rsqrtf(r2c);
+            const float r2inv = rinv * rinv;
+            const float x = A.alpha * (r2c * rinv);  // alpha r
+            const float expm = __expf(-x * x);       // exp(-alpha^2 r^2), as the reference's __expf
             const float qq = A.qqr * qi * qj;
-            const float erfcv = erfcf(A.alpha * len);
-            float fsc = qq * (erfcv * rinv + (2.0f * 0.5641895835477563f * A.alpha) * expf(-A.alpha * A.alpha * r2c));
+            const float erfcv = erfc_as(x, expm);
+            float fsc = qq * (erfcv * rinv + (2.0f * 0.5641895835477563f * A.alpha) * expm);
             if (mult < 1.0f) fsc -= (1.0f - mult) * qq * rinv;
             s += fsc * r2inv;
             if (ENERGY) {
@@ -124,29 +139,49 @@ __global__ void __launch_bounds__(256) k_pair(PairArgs A, int accumulate) {
         int cnt = (int)A.counts[i];
         cnt = cnt < A.cap ? cnt : A.cap;
         const uint32_t *row = A.nlist + (size_t)(i / G) * A.cap * G + a * T + t;
-        const float mults[4] = {1.0f, A.coef1, A.coef2, A.coef3};
-        for (int k = t; k < cnt; k += T) {
-            const uint32_t e = __ldg(row + (size_t)(k / T) * 32);
-            const int j = (int)(e & kExclMask);
-            const float mult = mults[e >> 30];
-            const float4 xj = __ldg(A.xs + j);
-            const float3 dr = min_image(A.box, make_float3(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z));
-            const float r2 = dot3(dr, dr);
-            const float qj = EW ? __ldg(A.qs + j) : 0.f;
-            float s, eng;
-            if (pair_term<LJ, EW, ENERGY>(A, sp, nt2, ti, qi, xj, qj, dr, r2, mult, s, eng)) {
-                const float Fx = dr.x * s, Fy = dr.y * s, Fz = dr.z * s;
-                fx += Fx;
-                fy += Fy;
-                fz += Fz;
-                if (ENERGY) en += eng;
-                if (VIR) {
-                    v0 += Fx * dr.x;
-                    v1 += Fy * dr.y;
-                    v2 += Fz * dr.z;
-                    v3 += Fx * dr.y;
-                    v4 += Fx * dr.z;
-                    v5 += Fy * dr.z;
+        // U entries per lane per trip: all list loads, then all position and
+        // charge gathers, then the arithmetic -- U independent memory chains
+        // in flight per lane instead of one dependent list->position chain
+        constexpr int U = 4;
+        constexpr uint32_t kNone = 0xffffffffu;
+        for (int k0 = t; k0 < cnt; k0 += U * T) {
+            uint32_t ent[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int k = k0 + u * T;
+                ent[u] = k < cnt ? __ldg(row + (size_t)(k / T) * 32) : kNone;
+            }
+            float4 xj[U];
+            float qj[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int j = ent[u] == kNone ? i : (int)(ent[u] & kExclMask);
+                xj[u] = __ldg(A.xs + j);
+                qj[u] = EW ? __ldg(A.qs + j) : 0.f;
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                if (ent[u] == kNone) continue;
+                const uint32_t tag = ent[u] >> 30;
+                float mult = 1.0f;
+                if (tag) mult = tag == 1u ? A.coef1 : (tag == 2u ? A.coef2 : A.coef3);
+                const float3 dr = min_image(A.box, make_float3(xi.x - xj[u].x, xi.y - xj[u].y, xi.z - xj[u].z));
+                const float r2 = dot3(dr, dr);
+                float s, eng;
+                if (pair_term<LJ, EW, ENERGY>(A, sp, nt2, ti, qi, xj[u], qj[u], dr, r2, mult, s, eng)) {
+                    const float Fx = dr.x * s, Fy = dr.y * s, Fz = dr.z * s;
+                    fx += Fx;
+                    fy += Fy;
+                    fz += Fz;
+                    if (ENERGY) en += eng;
+                    if (VIR) {
+                        v0 += Fx * dr.x;
+                        v1 += Fy * dr.y;
+                        v2 += Fz * dr.z;
+                        v3 += Fx * dr.y;
+                        v4 += Fx * dr.z;
+                        v5 += Fy * dr.z;
+                    }
                 }
             }
         }

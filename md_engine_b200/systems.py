@@ -60,14 +60,17 @@ def _mb_velocities(rng, mass, T, kB, mvv):
     return v
 
 
-def lj_fcc(ncell=20, rho=0.8442, T=1.2, seed=DEFAULT_SEED):
-    """LJ fluid: 4*ncell^3 atoms on an FCC lattice at reduced density rho."""
+def lj_fcc(ncell=20, rho=0.8442, T=1.2, seed=DEFAULT_SEED, jitter=0.0):
+    """LJ fluid: 4*ncell^3 atoms on an FCC lattice at reduced density rho
+    (optionally displaced by a seeded normal jitter of `jitter` sigma)."""
     a = (4.0 / rho) ** (1.0 / 3.0)
     base = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])
     g = np.stack(np.meshgrid(np.arange(ncell), np.arange(ncell), np.arange(ncell), indexing="ij"), -1).reshape(-1, 3)
     pos = ((g[:, None, :] + base[None, :, :]).reshape(-1, 3) + 0.25) * a
     n = len(pos)
     rng = np.random.default_rng(seed)
+    if jitter:
+        pos = pos + rng.normal(0.0, jitter, pos.shape)
     mass = np.ones(n)
     vel = _mb_velocities(rng, mass, T, 1.0, 1.0)
     L = np.full(3, ncell * a)

@@ -41,10 +41,27 @@ class WaterCPU:
         self.G = O.p3m_green(sysd.L, (grid,) * 3, self.alpha)
         self.ftm = O.REAL_UNITS["ftm_to_v"]
         ndf = 6 * len(self.mol)
-        self.nh = O.NoseHooverChain(T, tau, ndf, O.REAL_UNITS["boltz"], dt)
-        self.f = self.forces()
-        self.nh.prepare(O.kinetic_sum(self.v, self.invm) * O.REAL_UNITS["mvv_to_eng"])
+        self.nh = O.NoseHooverChain(T, tau, ndf, O.REAL_UNITS["boltz"], dt) if T is not None else None
+        self.f = self.forces()  # forceInitial, before FixRigid::prepareForRun
+        self.initial_constraints()
+        if self.nh is not None:
+            self.nh.prepare(O.kinetic_sum(self.v, self.invm) * O.REAL_UNITS["mvv_to_eng"])
         self.pending = 1.0
+
+    def initial_constraints(self):
+        """FixRigid::prepareForRun with solveInitialConstraints
+        (FixRigid.cu:1740-1880): SETTLE onto itself, M sites, velocity
+        constraints, centre-of-mass velocity removal over all atoms."""
+        s, mol = self.s, self.mol
+        x0 = self.x[mol[:, :3]].copy()
+        xn, vn = O.settle_positions(x0, x0.copy(), self.v[mol[:, :3]], s.L, self.rd, self.dt)
+        self.x[mol[:, :3]] = xn
+        self.v[mol[:, :3]] = vn
+        self.x[mol[:, 3]] = O.msite_positions(xn[:, 0], xn[:, 1], xn[:, 2], s.L, self.rd.r_OM)
+        self.v[mol[:, :3]] = O.settle_velocities(self.x[mol[:, :3]], self.v[mol[:, :3]], s.L, self.rd)
+        m = np.where(self.m > 0, self.m, 1e-30)
+        vcom = np.sum(self.v * m[:, None], 0) / np.sum(m)
+        self.v -= vcom
 
     def forces(self):
         s = self.s
@@ -63,8 +80,9 @@ class WaterCPU:
     def step(self):
         s, mol, dt = self.s, self.mol, self.dt
         dtf = 0.5 * dt * self.ftm
-        self.pending *= self.nh.integrate(True)
-        self.v *= self.pending
+        if self.nh is not None:
+            self.pending *= self.nh.integrate(True)
+            self.v *= self.pending
         real = self.m > 0
         x0 = self.x[mol[:, :3]].copy()
         self.v[real] += dtf * self.f[real] * self.invm[real][:, None]
@@ -84,8 +102,14 @@ class WaterCPU:
         self.f[mol[:, 3]] = 0.0
         self.v[mol[:, 0]], self.v[mol[:, 1]], self.v[mol[:, 2]] = vO, vH1, vH2
         self.v[mol[:, :3]] = O.settle_velocities(self.x[mol[:, :3]], self.v[mol[:, :3]], s.L, self.rd)
-        self.nh.ke = O.kinetic_sum(self.v, self.invm) * O.REAL_UNITS["mvv_to_eng"]
-        self.pending = self.nh.integrate(False)
+        if self.nh is not None:
+            self.nh.ke = O.kinetic_sum(self.v, self.invm) * O.REAL_UNITS["mvv_to_eng"]
+            self.pending = self.nh.integrate(False)
+
+    def end_of_run(self):
+        """FixNoseHoover::postRun applies the scale left by the last stepFinal"""
+        self.v *= self.pending
+        self.pending = 1.0
 
 
 class LJCPU:

@@ -25,7 +25,7 @@ def _oracle_pair(O, st, sysd, params, rcut, padding, lj_kind=1, qrc=0.0, alpha=0
 
 @pytest.mark.parametrize("wca", [False, True])
 def test_lj_wca_forces_32k(oracle, wca):
-    sysd = systems.lj_fcc(ncell=20)
+    sysd = systems.lj_fcc(ncell=20, jitter=0.05)
     st, _ = systems.build_lj_state(sysd, rcut=2.5, skin=0.3, wca=wca)
     st.prepare()
     st.computeForces(virialMode=1)

@@ -12,10 +12,14 @@ pytestmark = pytest.mark.gpu
 
 def _compare(O, st, sysd, rcut, padding, excl=None):
     st.prepare()
+    # prepare may move atoms after its first build (the initial SETTLE of
+    # FixRigid); rebuild on the current positions and compare with those
+    x_pre, _, _ = st.getAtoms()
+    st.buildNeighborlists(force=True)
     x, _, _ = st.getAtoms()
     # the device wrapped the float32 positions in place: same as the oracle's wrap
-    xs4 = np.zeros((len(sysd.pos), 4), np.float32)
-    xs4[:, :3] = np.asarray(sysd.pos, np.float32)
+    xs4 = np.zeros((len(x_pre), 4), np.float32)
+    xs4[:, :3] = np.asarray(x_pre, np.float32)
     O.wrap_f32(xs4, sysd.lo, sysd.L)
     assert np.array_equal(xs4[:, :3].astype(np.float64), x), "periodic wrap differs"
     cut = neighbor_cut(rcut, padding)

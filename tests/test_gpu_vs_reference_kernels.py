@@ -27,7 +27,7 @@ def _xs4(x, types):
 
 
 def test_pair_kernel_matches_reference_kernel_lj(oracle):
-    sysd = systems.lj_fcc(ncell=20)
+    sysd = systems.lj_fcc(ncell=20, jitter=0.05)
     st, _ = systems.build_lj_state(sysd, rcut=2.5, skin=0.3)
     st.prepare()
     st.computeForces()
