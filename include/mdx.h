@@ -164,6 +164,17 @@ int mdx_compute_forces(mdx_state *st, int virial_mode);
 int mdx_potential_energy(mdx_state *st, double out[4]);
 /* sum over atoms of m v^2 (FP64) and the degrees of freedom */
 int mdx_kinetic(mdx_state *st, double *sum_mv2, double *ndf);
+/* The same FP64 sum of m v^2 as mdx_kinetic, for host programs that cannot
+ * allocate device memory while they run (e.g. a host that serves all device
+ * memory from its own pre-reserved pool, or a loop that must avoid the
+ * implicit device synchronisation of cudaMalloc/cudaFree).  No counterpart
+ * in the reference.  It allocates nothing: its block partials live in a fixed
+ * 64 KiB file-scope device array (held on every GPU that loads the library
+ * until exit), so states of more than 2,097,152 atoms are rejected with
+ * MDX_ERR_ARG.  The first call on a device looks the array up (set-up, once
+ * per device) and should come before any stream capture; all calls share the
+ * array, so calls whose kernels overlap on the GPU race. */
+int mdx_kinetic_noalloc(mdx_state *st, double *sum_mv2);
 /* per-atom virials (6 per atom, xx yy zz xy xz yz) by id, FP64 total in sum6 */
 int mdx_get_virials(mdx_state *st, double *per_atom, double sum6[6]);
 /* single hooks, for stage-level parity (src/Fixes/FixRigid.cu:1234-1279, 1916-1984) */
