@@ -157,7 +157,8 @@ def profile_traffic(key):
     p = os.path.join(ROOT, "profiles", "roofline_traffic.json")
     if os.path.exists(p):
         with open(p) as f:
-            return json.load(f).get(key)
+            e = json.load(f).get(key)
+        return None if e is None else float(e["traffic_bytes"])
     return None
 
 

@@ -472,9 +472,11 @@ int mdx_nlist_get(mdx_state *st, int max_per_atom, int *counts, int *nbr, int *t
     GridGPU &g = s.grid;
     const int G = 32 / g.team;
     const size_t groups = (size_t)(n + G - 1) / G;
-    std::vector<uint32_t> cnt(n), list(groups * g.cap * G), ids(n);
+    std::vector<uint32_t> cnt(n), cint(n), list(groups * g.cap * G), ids(n);
     MDX_CUDA_TRY(cudaStreamSynchronize(s.stream));
     MDX_CUDA_TRY(cudaMemcpy(cnt.data(), g.counts.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (g.partition) MDX_CUDA_TRY(cudaMemcpy(cint.data(), g.counts_int.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    else cint = cnt;
     MDX_CUDA_TRY(cudaMemcpy(list.data(), g.nlist.p, list.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
     MDX_CUDA_TRY(cudaMemcpy(ids.data(), s.gpd.ids.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
     for (int i = 0; i < n; i++) {
@@ -486,8 +488,10 @@ int mdx_nlist_get(mdx_state *st, int max_per_atom, int *counts, int *nbr, int *t
         }
         std::vector<std::pair<int, int>> row(c);
         const size_t base = (size_t)(i / G) * g.cap * G + (i % G) * g.team;
+        const int cf = (int)std::min<uint32_t>(cint[i], (uint32_t)c);
         for (int k = 0; k < c; k++) {
-            const uint32_t e = list[base + (size_t)(k / g.team) * 32 + (k % g.team)];
+            const int kk = k < cf ? k : g.cap - 1 - (k - cf);  // front: interacting, back: the rest
+            const uint32_t e = list[base + (size_t)(kk / g.team) * 32 + (kk % g.team)];
             row[k] = {(int)ids[e & kExclMask], (int)(e >> 30)};
         }
         std::sort(row.begin(), row.end());

@@ -140,7 +140,8 @@ template <int T>
 __global__ void k_e3b_list(int nmol, const int4 *__restrict__ mol_ids, int4 *__restrict__ mol_idx,
                            const int *__restrict__ idToIdx, const int *__restrict__ mol_of_id,
                            const uint32_t *__restrict__ ids, const float4 *__restrict__ xs,
-                           const uint32_t *__restrict__ counts, const uint32_t *__restrict__ nlist, int team_atom,
+                           const uint32_t *__restrict__ counts, const uint32_t *__restrict__ counts_int,
+                           const uint32_t *__restrict__ nlist, int team_atom,
                            int cap_atom, Box box, float cut2, uint32_t *__restrict__ mcounts,
                            uint32_t *__restrict__ mlist, int mcap, DeviceStatus *st, int conditional) {
     if (conditional && !st->rebuild) return;
@@ -158,6 +159,8 @@ __global__ void k_e3b_list(int nmol, const int4 *__restrict__ mol_ids, int4 *__r
     const float3 po = f3(xs[oi]);
     int cnt = (int)counts[oi];
     cnt = cnt < cap_atom ? cnt : cap_atom;
+    // rows hold interacting pairs from the front and the rest from the back
+    const int cfront = counts_int ? (int)counts_int[oi] : cnt;
     const int Ga = 32 / team_atom;
     const uint32_t *row = nlist + (size_t)(oi / Ga) * cap_atom * Ga + (oi % Ga) * team_atom;
     uint32_t *mrow = mlist + (size_t)(m / G) * mcap * G + a * T;
@@ -167,7 +170,8 @@ __global__ void k_e3b_list(int nmol, const int4 *__restrict__ mol_ids, int4 *__r
         bool hit = false;
         int mj = -1;
         if (k < cnt) {
-            const uint32_t e = row[(size_t)(k / team_atom) * 32 + (k % team_atom)];
+            const int kk = k < cfront ? k : cap_atom - 1 - (k - cfront);
+            const uint32_t e = row[(size_t)(kk / team_atom) * 32 + (kk % team_atom)];
             const int j = (int)(e & kExclMask);
             mj = mol_of_id[ids[j]];
             if (mj >= 0 && mj != m) {
@@ -192,7 +196,9 @@ __global__ void k_e3b_list(int nmol, const int4 *__restrict__ mol_ids, int4 *__r
 
 // pass 1: e3bTotals of molecule i (ThreeBodyE3B.h:170-211 summed from i's own
 // full list) and the O-O two-body force (EvaluatorE3B::twoBodyForce, :67-78)
-template <int T, bool ENERGY>
+// STORE: write into a per-step side buffer instead of adding to the forces
+// (lets E3B run concurrently with the pair kernel; the second half merges it)
+template <int T, bool ENERGY, bool STORE = false>
 __global__ void k_e3b_totals(int nmol, const int4 *__restrict__ mol_idx, const float4 *__restrict__ xs,
                              float4 *__restrict__ fs, const uint32_t *__restrict__ mcounts,
                              const uint32_t *__restrict__ mlist, int mcap, Box box, E3BParams p,
@@ -256,16 +262,20 @@ __global__ void k_e3b_totals(int nmol, const int4 *__restrict__ mol_idx, const f
     tz = tsum<T>(tz);
     if (valid && t == 0) {
         totals[m] = make_float4(tx, ty, tz, 0.f);
-        float4 f = fs[ix.x];
-        f.x += fx;
-        f.y += fy;
-        f.z += fz;
-        fs[ix.x] = f;
+        if (STORE) {
+            fs[ix.x] = make_float4(fx, fy, fz, 0.f);
+        } else {
+            float4 f = fs[ix.x];
+            f.x += fx;
+            f.y += fy;
+            f.z += fz;
+            fs[ix.x] = f;
+        }
     }
 }
 
 // pass 2: three-body forces on molecule i's O, H1, H2 (ThreeBodyE3B.h:255-549)
-template <int T, bool ENERGY>
+template <int T, bool ENERGY, bool STORE = false>
 __global__ void k_e3b_forces(int nmol, const int4 *__restrict__ mol_idx, const float4 *__restrict__ xs,
                              float4 *__restrict__ fs, const uint32_t *__restrict__ mcounts,
                              const uint32_t *__restrict__ mlist, int mcap, Box box, E3BParams p,
@@ -326,12 +336,17 @@ __global__ void k_e3b_forces(int nmol, const int4 *__restrict__ mol_idx, const f
         float4 f = fs[ix.x];
         f.x += fa.x; f.y += fa.y; f.z += fa.z;
         fs[ix.x] = f;
-        f = fs[ix.y];
-        f.x += fb.x; f.y += fb.y; f.z += fb.z;
-        fs[ix.y] = f;
-        f = fs[ix.z];
-        f.x += fc.x; f.y += fc.y; f.z += fc.z;
-        fs[ix.z] = f;
+        if (STORE) {
+            fs[ix.y] = make_float4(fb.x, fb.y, fb.z, 0.f);
+            fs[ix.z] = make_float4(fc.x, fc.y, fc.z, 0.f);
+        } else {
+            f = fs[ix.y];
+            f.x += fb.x; f.y += fb.y; f.z += fb.z;
+            fs[ix.y] = f;
+            f = fs[ix.z];
+            f.x += fc.x; f.y += fc.y; f.z += fc.z;
+            fs[ix.z] = f;
+        }
     }
 }
 
@@ -386,6 +401,20 @@ int FixE3B::prepareForRun() {
     for (int m = 0; m < nmol; m++) mof[mol_ids[m].x] = m;
     if (int e = d_mol_of_atom.alloc(mof.size())) return e;
     MDX_CUDA_TRY(cudaMemcpy(d_mol_of_atom.p, mof.data(), mof.size() * sizeof(int), cudaMemcpyHostToDevice));
+    // the fused step can run E3B beside the pair kernel when its molecules
+    // are FixRigid's, in the same order (the second half merges the forces)
+    side_ok = false;
+    if (FixRigid *r = s.rigidFix()) {
+        if (r->mol_ids.size() == mol_ids.size()) {
+            side_ok = true;
+            for (size_t k = 0; k < mol_ids.size(); k++) {
+                const int4 a = mol_ids[k], b = r->mol_ids[k];
+                if (a.x != b.x || a.y != b.y || a.z != b.z) side_ok = false;
+            }
+        }
+    }
+    if (side_ok)
+        if (int e = f_side.alloc(s.atoms.size())) return e;
     mteam = kMolTeam;
     const double vol = s.box.Ld.x * s.box.Ld.y * s.box.Ld.z;
     const double rl = (double)lc + s.padding;
@@ -404,24 +433,36 @@ int e3b_build_list(State &s, FixE3B &f, bool conditional) {
     const int warps = (nmol + (32 / kMolTeam) - 1) / (32 / kMolTeam);
     k_e3b_list<kMolTeam><<<(warps * 32 + 255) / 256, 256, 0, s.stream>>>(
         nmol, f.d_mol_ids.p, f.d_mol_idx.p, s.gpd.idToIdx.p, f.d_mol_of_atom.p, s.gpd.ids.p, s.gpd.xs.p,
-        s.grid.counts.p, s.grid.nlist.p, s.grid.team, s.grid.cap, s.box, lc * lc, f.mcounts.p, f.mlist.p, f.mcap,
+        s.grid.counts.p, s.grid.partition ? s.grid.counts_int.p : nullptr, s.grid.nlist.p, s.grid.team, s.grid.cap,
+        s.box, lc * lc, f.mcounts.p, f.mlist.p, f.mcap,
         s.d_status.p, conditional ? 1 : 0);
     MDX_LAUNCHED();
     return 0;
 }
 
-int e3b_forces(State &s, FixE3B &f) {
+int e3b_forces(State &s, FixE3B &f) { return e3b_forces_to(s, f, s.gpd.fs.p, false, s.stream); }
+
+// side = true: store into `out` (a per-step E3B force buffer of O/H1/H2),
+// otherwise add to `out` (the atom forces)
+int e3b_forces_to(State &s, FixE3B &f, float4 *out, bool side, cudaStream_t stream) {
     const int nmol = (int)f.mol_ids.size();
     if (nmol == 0) return 0;
     const int warps = (nmol + (32 / kMolTeam) - 1) / (32 / kMolTeam);
     const int blocks = (warps * 32 + 255) / 256;
-    k_e3b_totals<kMolTeam, false><<<blocks, 256, 0, s.stream>>>(nmol, f.d_mol_idx.p, s.gpd.xs.p, s.gpd.fs.p,
-                                                               f.mcounts.p, f.mlist.p, f.mcap, s.box, f.prm,
-                                                               f.totals.p, nullptr);
+    if (side) {
+        k_e3b_totals<kMolTeam, false, true><<<blocks, 256, 0, stream>>>(
+            nmol, f.d_mol_idx.p, s.gpd.xs.p, out, f.mcounts.p, f.mlist.p, f.mcap, s.box, f.prm, f.totals.p, nullptr);
+        MDX_LAUNCHED();
+        k_e3b_forces<kMolTeam, false, true><<<blocks, 256, 0, stream>>>(
+            nmol, f.d_mol_idx.p, s.gpd.xs.p, out, f.mcounts.p, f.mlist.p, f.mcap, s.box, f.prm, f.totals.p, nullptr);
+        MDX_LAUNCHED();
+        return 0;
+    }
+    k_e3b_totals<kMolTeam, false><<<blocks, 256, 0, stream>>>(nmol, f.d_mol_idx.p, s.gpd.xs.p, out, f.mcounts.p,
+                                                             f.mlist.p, f.mcap, s.box, f.prm, f.totals.p, nullptr);
     MDX_LAUNCHED();
-    k_e3b_forces<kMolTeam, false><<<blocks, 256, 0, s.stream>>>(nmol, f.d_mol_idx.p, s.gpd.xs.p, s.gpd.fs.p,
-                                                               f.mcounts.p, f.mlist.p, f.mcap, s.box, f.prm,
-                                                               f.totals.p, nullptr);
+    k_e3b_forces<kMolTeam, false><<<blocks, 256, 0, stream>>>(nmol, f.d_mol_idx.p, s.gpd.xs.p, out, f.mcounts.p,
+                                                             f.mlist.p, f.mcap, s.box, f.prm, f.totals.p, nullptr);
     MDX_LAUNCHED();
     return 0;
 }

@@ -109,10 +109,20 @@ struct GridGPU {
     DBuf<uint32_t> cell_start, cell_count, cell_fill, block_sums;
     DBuf<int> cell_of;     // per atom (unsorted order)
     DBuf<int> perm_tmp, perm;  // sort scratch
-    DBuf<uint32_t> counts; // per atom neighbour count
-    DBuf<uint32_t> nlist;  // entries
+    DBuf<uint32_t> counts; // per atom neighbour count (all pairs within cut)
+    DBuf<uint32_t> counts_int;  // per atom count of pairs that can interact
+    DBuf<uint32_t> nlist;  // entries: interacting ones from the front of the
+                           // row, provably zero ones (no LJ, q_i q_j = 0) from the back
+    DBuf<uint32_t> ljmask;  // per type: bit tj set when LJ/WCA eps(ti,tj) != 0
+    bool partition = false; // rows are split as above
+    bool part_q = false;    // charges take part in the split (Ewald active)
     DBuf<int> excl_start;  // by id
     DBuf<uint32_t> excl_ids;
+    // per id: exclusion depth of the ids id-32 .. id+31 as two bit planes
+    // (bit d of .x: depth bit 0 of id-32+d, .y: depth bit 1); excl_far[id]
+    // is set when some exclusion of id lies outside that window
+    DBuf<ulonglong2> excl_win;
+    DBuf<uint8_t> excl_far;
     int max_excl = 0;
     bool have_excl = false;
     bool built = false;
@@ -188,9 +198,9 @@ class FixChargeEwald : public Fix {
     int compute(int virialMode) override;
     std::vector<double> getRCuts() override { return {r_cut}; }
     double findAlpha();
-    int spread();   // zero + spread
-    int solve();    // FFT, E-field, inverse FFTs
-    int gather(bool accumulate);
+    int spread(cudaStream_t st);   // zero + spread
+    int solve(cudaStream_t st);    // FFT, E-field, inverse FFTs
+    int gather(bool accumulate, cudaStream_t st);
 };
 
 struct E3BParams {  // EvaluatorE3B (EvaluatorE3B.h:9-65), FixE3B.cu:515-593
@@ -209,6 +219,8 @@ class FixE3B : public Fix {
     DBuf<int> d_mol_of_atom;  // by atom index, -1 if none (rebuilt with the list)
     DBuf<uint32_t> mcounts, mlist;  // molecule neighbour list (full, team layout)
     DBuf<float4> totals;
+    DBuf<float4> f_side;  // per-step E3B forces when run beside the pair kernel
+    bool side_ok = false; // molecules identical to FixRigid's, in the same order
     int mteam = 8, mcap = 0;
     FixE3B(State *s, std::string h, std::string st);
     int prepareForRun() override;
@@ -287,6 +299,8 @@ class State {
     DBuf<unsigned int> red_counter;
     cudaStream_t stream = nullptr;
     bool own_stream = true;
+    cudaStream_t side[2] = {nullptr, nullptr};  // concurrent branches of the fused step
+    cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
     bool uploaded = false;   // device copy is authoritative
     bool prepared = false;
     bool requiresCharges = false;
@@ -313,6 +327,7 @@ class State {
 int nlist_rebuild(State &s, bool force, bool conditional);
 int nlist_init(State &s);
 int nlist_exclusions(State &s);
+int nlist_set_interactions(State &s);
 // pair (pair.cu)
 int pair_launch(State &s, FixPair &f, int virialMode, bool accumulate);
 int pair_energy(State &s, FixPair &f, double *out);
@@ -323,11 +338,12 @@ int pair_force_raw(int n, const float4 *xs, float4 *fs, const float *qs, const u
 // e3b (e3b.cu)
 int e3b_build_list(State &s, FixE3B &f, bool conditional);
 int e3b_forces(State &s, FixE3B &f);
+int e3b_forces_to(State &s, FixE3B &f, float4 *out, bool side, cudaStream_t stream);
 int e3b_energy(State &s, FixE3B &f, double out[2]);
 // rigid + integration (integrate.cu)
 int rigid_update_maps(State &s, FixRigid &r, bool conditional);
 int step_first_half(State &s, bool fused);
-int step_second_half(State &s, bool fused);
+int step_second_half(State &s, bool fused, const float4 *fextra = nullptr);
 int rigid_prepare(State &s, FixRigid &r);
 int rigid_hook(State &s, FixRigid &r, int which);
 int kinetic_sum(State &s, double *out);

@@ -339,19 +339,21 @@ int FixChargeEwald::prepareForRun() {
     return 0;
 }
 
-int FixChargeEwald::spread() {
+int FixChargeEwald::spread(cudaStream_t st) {
     State &s = *state;
     const size_t ng = (size_t)sz.x * sz.y * sz.z;
-    MDX_CUDA_TRY(cudaMemsetAsync(rho.p, 0, ng * sizeof(float), s.stream));
+    MDX_CUDA_TRY(cudaMemsetAsync(rho.p, 0, ng * sizeof(float), st));
     P3MGeom g = geom(s, *this);
-    k_spread<<<(s.gpd.n + 127) / 128, 128, 0, s.stream>>>(s.gpd.n, s.gpd.xs.p, s.gpd.qs.p, g, rho.p);
+    k_spread<<<(s.gpd.n + 127) / 128, 128, 0, st>>>(s.gpd.n, s.gpd.xs.p, s.gpd.qs.p, g, rho.p);
     MDX_LAUNCHED();
     return 0;
 }
 
-int FixChargeEwald::solve() {
+int FixChargeEwald::solve(cudaStream_t st) {
     State &s = *state;
     const size_t nk = (size_t)sz.x * sz.y * (sz.z / 2 + 1);
+    cufftSetStream(plan_r2c, st);
+    cufftSetStream(plan_c2r, st);
     if (cufftExecR2C(plan_r2c, rho.p, (cufftComplex *)rho_k.p) != CUFFT_SUCCESS) {
         set_error(MDX_ERR_CUDA, "cufftExecR2C failed");
         return MDX_ERR_CUDA;
@@ -359,7 +361,7 @@ int FixChargeEwald::solve() {
     const float3 tpl = make_float3((float)(6.28318530717958647693 / s.box.Ld.x),
                                    (float)(6.28318530717958647693 / s.box.Ld.y),
                                    (float)(6.28318530717958647693 / s.box.Ld.z));
-    k_efield<<<(unsigned)((nk + 255) / 256), 256, 0, s.stream>>>(sz, tpl, rho_k.p, green.p, e_k.p, nk);
+    k_efield<<<(unsigned)((nk + 255) / 256), 256, 0, st>>>(sz, tpl, rho_k.p, green.p, e_k.p, nk);
     MDX_LAUNCHED();
     if (cufftExecC2R(plan_c2r, (cufftComplex *)e_k.p, e_r.p) != CUFFT_SUCCESS) {
         set_error(MDX_ERR_CUDA, "cufftExecC2R failed");
@@ -368,30 +370,33 @@ int FixChargeEwald::solve() {
     return 0;
 }
 
-int FixChargeEwald::gather(bool accumulate) {
+int FixChargeEwald::gather(bool accumulate, cudaStream_t st) {
     State &s = *state;
     P3MGeom g = geom(s, *this);
     const size_t ng = (size_t)sz.x * sz.y * sz.z;
     const float niv = (float)(-1.0 / (s.box.Ld.x * s.box.Ld.y * s.box.Ld.z));
-    if (accumulate)
-        k_gather<true><<<(s.gpd.n + 127) / 128, 128, 0, s.stream>>>(s.gpd.n, s.gpd.xs.p, s.gpd.qs.p, g, e_r.p, ng, niv,
-                                                                   s.gpd.fs.p);
-    else
-        k_gather<false><<<(s.gpd.n + 127) / 128, 128, 0, s.stream>>>(s.gpd.n, s.gpd.xs.p, s.gpd.qs.p, g, e_r.p, ng, niv,
-                                                                    s.gpd.fs.p);
+    if (accumulate) {
+        k_gather<true><<<(s.gpd.n + 127) / 128, 128, 0, st>>>(s.gpd.n, s.gpd.xs.p, s.gpd.qs.p, g, e_r.p, ng, niv,
+                                                              s.gpd.fs.p);
+    } else {
+        k_gather<false><<<(s.gpd.n + 127) / 128, 128, 0, st>>>(s.gpd.n, s.gpd.xs.p, s.gpd.qs.p, g, e_r.p, ng, niv,
+                                                               s.gpd.fs.p);
+    }
     MDX_LAUNCHED();
     return 0;
 }
 
 int FixChargeEwald::compute(int virialMode) {
     (void)virialMode;
-    if (int e = spread()) return e;
-    if (int e = solve()) return e;
-    return gather(true);
+    State &s = *state;
+    if (int e = spread(s.stream)) return e;
+    if (int e = solve(s.stream)) return e;
+    return gather(true, s.stream);
 }
 
 int ewald_recip_energy(State &s, FixChargeEwald &f, double *out) {
-    if (int e = f.spread()) return e;
+    if (int e = f.spread(s.stream)) return e;
+    cufftSetStream(f.plan_r2c, s.stream);
     if (cufftExecR2C(f.plan_r2c, f.rho.p, (cufftComplex *)f.rho_k.p) != CUFFT_SUCCESS) {
         set_error(MDX_ERR_CUDA, "cufftExecR2C failed");
         return MDX_ERR_CUDA;

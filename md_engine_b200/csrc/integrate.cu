@@ -330,10 +330,13 @@ __global__ void k_second_atoms(int n, float4 *__restrict__ vs, const float4 *__r
 
 // per-molecule fused: postForce + distributeMSite + settleVelocities +
 // validateConstraints + m v^2 partials (+ last-block NH / turn)
+// fextra (may be null): per-molecule-atom forces computed beside the pair
+// kernel (E3B), indexed like fs, merged into O/H1/H2 here
 __global__ void k_second_mol(int nmol, const int4 *__restrict__ mol_idx, const float4 *__restrict__ xs,
                              float4 *__restrict__ vs, float4 *__restrict__ fs, RigidConsts rc, Box box, float dtf,
                              double *__restrict__ partials, int part_off, int nparts, unsigned int *counter,
-                             NHChain *chain, int nh, DeviceStatus *st, double *ke_out) {
+                             NHChain *chain, int nh, DeviceStatus *st, double *ke_out,
+                             const float4 *__restrict__ fextra) {
     __shared__ double sh[32];
     int m = blockIdx.x * blockDim.x + threadIdx.x;
     double mv2 = 0.0;
@@ -345,6 +348,12 @@ __global__ void k_second_mol(int nmol, const int4 *__restrict__ mol_idx, const f
         for (int k = 0; k < 3; k++) {
             x[k] = xs[id3[k]];
             f[k] = fs[id3[k]];
+            if (fextra) {
+                const float4 fe = fextra[id3[k]];
+                f[k].x += fe.x;
+                f[k].y += fe.y;
+                f[k].z += fe.z;
+            }
             v[k] = kick(vs[id3[k]], f[k], dtf);
         }
         if (rc.foursite) {
@@ -363,6 +372,8 @@ __global__ void k_second_mol(int nmol, const int4 *__restrict__ mol_idx, const f
             f[2].x += fHd.x; f[2].y += fHd.y; f[2].z += fHd.z;
             vs[ix.w] = make_float4(0.f, 0.f, 0.f, vm.w);
             fs[ix.w] = make_float4(0.f, 0.f, 0.f, fm.w);
+        }
+        if (rc.foursite || fextra) {
 #pragma unroll
             for (int k = 0; k < 3; k++) fs[id3[k]] = f[k];
         }
@@ -677,7 +688,7 @@ int step_first_half(State &s, bool fused) {
     return 0;
 }
 
-int step_second_half(State &s, bool fused) {
+int step_second_half(State &s, bool fused, const float4 *fextra) {
     const int n = s.gpd.n;
     const float dtf = (float)(0.5 * s.dt * s.units.ftm_to_v);
     FixNoseHoover *nh = s.nhFix();
@@ -718,7 +729,7 @@ int step_second_half(State &s, bool fused) {
         const int nmol = (int)r->mol_ids.size();
         k_second_mol<<<mb, 128, 0, s.stream>>>(nmol, r->d_mol_idx.p, s.gpd.xs.p, s.gpd.vs.p, s.gpd.fs.p, r->rc,
                                                s.box, dtf, s.red_partials.p, free_atoms ? ab : 0, nparts,
-                                               s.red_counter.p, chain, nh ? 1 : 0, s.d_status.p, s.red_out.p);
+                                               s.red_counter.p, chain, nh ? 1 : 0, s.d_status.p, s.red_out.p, fextra);
         MDX_LAUNCHED();
     }
     return 0;

@@ -62,11 +62,43 @@ class IntegratorVerlet {
         }
         return 0;
     }
+    // fused step: the P3M chain (spread, R2C, E(k), C2R) and E3B run on two
+    // side streams beside the pair kernel; they join before the P3M gather
+    // and the second half (which merges the E3B forces)
+    int stepFused() {
+        FixPair *pf = s->pairFix();
+        FixChargeEwald *ew = s->ewaldFix();
+        FixE3B *e3 = s->e3bFix();
+        const bool e3side = e3 && e3->side_ok && s->rigidFix();
+        if (int e = step_first_half(*s, true)) return e;
+        if (ew || e3side) MDX_CUDA_TRY(cudaEventRecord(s->ev_fork, s->stream));
+        if (ew) {
+            MDX_CUDA_TRY(cudaStreamWaitEvent(s->side[0], s->ev_fork, 0));
+            if (int e = ew->spread(s->side[0])) return e;
+            if (int e = ew->solve(s->side[0])) return e;
+            MDX_CUDA_TRY(cudaEventRecord(s->ev_join[0], s->side[0]));
+        }
+        if (e3side) {
+            MDX_CUDA_TRY(cudaStreamWaitEvent(s->side[1], s->ev_fork, 0));
+            if (int e = e3b_forces_to(*s, *e3, e3->f_side.p, true, s->side[1])) return e;
+            MDX_CUDA_TRY(cudaEventRecord(s->ev_join[1], s->side[1]));
+        }
+        if (pf)
+            if (int e = pair_launch(*s, *pf, 0, false)) return e;
+        if (e3 && !e3side)
+            if (int e = e3b_forces(*s, *e3)) return e;
+        if (ew) {
+            MDX_CUDA_TRY(cudaStreamWaitEvent(s->stream, s->ev_join[0], 0));
+            if (int e = ew->gather(true, s->stream)) return e;
+        }
+        if (e3side) MDX_CUDA_TRY(cudaStreamWaitEvent(s->stream, s->ev_join[1], 0));
+        return step_second_half(*s, true, e3side ? e3->f_side.p : nullptr);
+    }
     int stepBody() {
-        const bool fused = mode == 0;
-        if (int e = step_first_half(*s, fused)) return e;
+        if (mode == 0) return stepFused();
+        if (int e = step_first_half(*s, false)) return e;
         if (int e = forces()) return e;
-        if (int e = step_second_half(*s, fused)) return e;
+        if (int e = step_second_half(*s, false)) return e;
         return 0;
     }
     int enqueue(int nsteps, bool with_group) {

@@ -184,113 +184,233 @@ __global__ void k_gather(const int *__restrict__ perm, int n, const float4 *__re
 }
 
 // assignNeighbors / assignFromCell (GridGPU.cu:482-734) with the exclusion
-// lookup of addExclusion (GridGPU.cu:466-478).  Team of T lanes per atom;
-// also copies the sorted streams back to the primary buffers.
-template <int T>
-__global__ void __launch_bounds__(256) k_build(
-    int n, const float4 *__restrict__ xs2, const float4 *__restrict__ vs2, const float4 *__restrict__ fs2,
-    const float *__restrict__ qs2, const uint32_t *__restrict__ ids2, float4 *__restrict__ xs,
-    float4 *__restrict__ vs, float4 *__restrict__ fs, float *__restrict__ qs, uint32_t *__restrict__ ids,
-    float4 *__restrict__ xs_last, const uint32_t *__restrict__ cell_start, CellGrid g, Box box, int m,
-    float cutsq, const int *__restrict__ excl_start, const uint32_t *__restrict__ excl_ids, int use_excl,
-    uint32_t *__restrict__ counts, uint32_t *__restrict__ nlist, int cap, DeviceStatus *st) {
-    if (!st->rebuild) return;
-    constexpr int G = 32 / T;
+// lookup of addExclusion (GridGPU.cu:466-478), one block of kBuildWarps warps
+// per home cell.  Lane l of every warp owns home atom l of the cell (chunks of
+// 32 for fuller cells); the 25 stencil rows are dealt round-robin to the
+// warps.  For each of its rows a warp stages 32 candidates at a time in shared
+// memory, already shifted by the periodic image (x_j + shift, the reference's
+// first rounding), and each lane tests all of them against its atom with the
+// reference's predicate.  Rows and z ranges are trimmed to the cells that can
+// hold a point within cut of the chunk's bounding box (conservative margin of
+// 1e-3 cell), so the pair set equals the full stencil's.  Two passes keep the
+// row deterministic: pass 1 counts per (warp, atom), a prefix over the warps
+// gives each warp its slice, pass 2 writes.  Pairs that can interact fill the
+// row from the front, provably zero ones from the back.  Exclusion depths come
+// from the id-window bit planes (the id list only for atoms with far
+// exclusions).  COUNT runs pass 1 alone to size the first build.  Also copies
+// the sorted streams back to the primary buffers.
+constexpr int kBuildWarps = 8;
+
+struct BuildArgs {
+    const float4 *xs2, *vs2, *fs2;
+    const float *qs2;
+    const uint32_t *ids2;
+    float4 *xs, *vs, *fs;
+    float *qs;
+    uint32_t *ids;
+    float4 *xs_last;
+    const uint32_t *cell_start;
+    const int *excl_start;
+    const uint32_t *excl_ids;
+    const ulonglong2 *excl_win;
+    const uint8_t *excl_far;
+    const uint32_t *ljmask;
+    uint32_t *counts, *counts_int, *nlist;
+    DeviceStatus *st;
+    CellGrid g;
+    Box box;
+    int ncell, m, use_excl, part_q, cap;
+    float cutsq;
+};
+
+template <int TP, bool COUNT>
+__global__ void __launch_bounds__(kBuildWarps * 32, 3) k_build_cells(const BuildArgs A) {
+    if (!COUNT && !A.st->rebuild) return;
+    constexpr int GP = 32 / TP;
+    __shared__ float4 sh_x[kBuildWarps][32];
+    __shared__ uint2 sh_it[kBuildWarps][32];
+    __shared__ uint32_t sh_ci[kBuildWarps][32], sh_cn[kBuildWarps][32];
+    const CellGrid &g = A.g;
     const int lane = threadIdx.x & 31;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int a = lane / T, t = lane % T;
-    const int i = warp * G + a;
-    if (i >= n) return;  // whole team leaves together
-    const unsigned team_mask = (T == 32) ? 0xffffffffu : (((1u << T) - 1u) << (a * T));
-    const float4 pi4 = xs2[i];
-    if (t == 0) {
-        xs[i] = pi4;
-        xs_last[i] = pi4;
-        vs[i] = vs2[i];
-        fs[i] = fs2[i];
-        qs[i] = qs2[i];
-        ids[i] = ids2[i];
-    }
-    const float3 pi = f3(pi4);
-    const int cx = cell_coord(pi.x, g.lo.x, g.inv_ds.x, g.ns.x);
-    const int cy = cell_coord(pi.y, g.lo.y, g.inv_ds.y, g.ns.y);
-    const int cz = cell_coord(pi.z, g.lo.z, g.inv_ds.z, g.ns.z);
-    int e0 = 0, e1 = 0;
-    if (use_excl) {
-        uint32_t myid = ids2[i];
-        e0 = excl_start[myid];
-        e1 = excl_start[myid + 1];
-    }
-    uint32_t *mylist = nlist + (size_t)(i / G) * cap * G + a * T + t;
-    int cnt = 0;
-    for (int dx = -m; dx <= m; dx++) {
-        int kx = cx + dx;
-        float sx = 0.f;
-        if (kx < 0) { kx += g.ns.x; sx = -box.L.x; }
-        else if (kx >= g.ns.x) { kx -= g.ns.x; sx = box.L.x; }
-        for (int dy = -m; dy <= m; dy++) {
-            int ky = cy + dy;
-            float sy = 0.f;
-            if (ky < 0) { ky += g.ns.y; sy = -box.L.y; }
-            else if (ky >= g.ns.y) { ky -= g.ns.y; sy = box.L.y; }
-            const int rowbase = (kx * g.ns.y + ky) * g.ns.z;
-            // up to three z segments: [main, wrapped low, wrapped high]
-            for (int seg = 0; seg < 3; seg++) {
-                int z0, z1;
-                float sz = 0.f;
-                if (seg == 0) {
-                    z0 = cz - m < 0 ? 0 : cz - m;
-                    z1 = cz + m >= g.ns.z ? g.ns.z - 1 : cz + m;
-                } else if (seg == 1) {
-                    if (cz - m >= 0) continue;
-                    z0 = cz - m + g.ns.z;
-                    z1 = g.ns.z - 1;
-                    sz = -box.L.z;
-                } else {
-                    if (cz + m < g.ns.z) continue;
-                    z0 = 0;
-                    z1 = cz + m - g.ns.z;
-                    sz = box.L.z;
-                }
-                const int pbeg = cell_start[rowbase + z0];
-                const int pend = cell_start[rowbase + z1 + 1];
-                for (int p0 = pbeg; p0 < pend; p0 += T) {
-                    const int p = p0 + t;
-                    bool hit = false;
-                    if (p < pend && p != i) {
-                        const float4 pj = xs2[p];
-                        const float ddx = __fsub_rn(__fadd_rn(pj.x, sx), pi.x);
-                        const float ddy = __fsub_rn(__fadd_rn(pj.y, sy), pi.y);
-                        const float ddz = __fsub_rn(__fadd_rn(pj.z, sz), pi.z);
-                        const float r2 = __fmaf_rn(ddz, ddz, __fmaf_rn(ddy, ddy, __fmul_rn(ddx, ddx)));
-                        hit = r2 < cutsq;
+    const int wib = threadIdx.x >> 5;
+    const int c = blockIdx.x;
+    const int cs = (int)A.cell_start[c], ce = (int)A.cell_start[c + 1];
+    const int cz = c % g.ns.z, cy = (c / g.ns.z) % g.ns.y, cx = c / (g.ns.z * g.ns.y);
+    const int m = A.m, side = 2 * m + 1;
+    const float cutsq = A.cutsq;
+    const float dsx = 1.0f / g.inv_ds.x, dsy = 1.0f / g.inv_ds.y, dsz = 1.0f / g.inv_ds.z;
+    float4 *const shx = sh_x[wib];
+    uint2 *const shi = sh_it[wib];
+    for (int h0 = cs; h0 < ce; h0 += 32) {
+        const int i = h0 + lane;
+        const bool valid = i < ce;
+        float xi = 0.f, yi = 0.f, zi = 0.f, qi = 0.f;
+        uint32_t amask = 0xffffffffu, myid = 0u;
+        unsigned long long w1 = 0ull, w2 = 0ull;
+        bool far = false;
+        if (valid) {
+            const float4 p4 = A.xs2[i];
+            xi = p4.x;
+            yi = p4.y;
+            zi = p4.z;
+            if (A.ljmask) amask = A.ljmask[type_of(p4)];
+            if (A.part_q) qi = A.qs2[i];
+            if (A.use_excl) {
+                myid = A.ids2[i];
+                const ulonglong2 w = A.excl_win[myid];
+                w1 = w.x;
+                w2 = w.y;
+                far = A.excl_far[myid] != 0;
+            }
+            if (!COUNT && wib == 0) {
+                A.xs[i] = p4;
+                A.xs_last[i] = p4;
+                A.vs[i] = A.vs2[i];
+                A.fs[i] = A.fs2[i];
+                A.qs[i] = A.qs2[i];
+                A.ids[i] = A.ids2[i];
+            }
+        }
+        // chunk bounding box (warp-uniform, identical in every warp)
+        float bxl = valid ? xi : 3.0e38f, bxh = valid ? xi : -3.0e38f;
+        float byl = valid ? yi : 3.0e38f, byh = valid ? yi : -3.0e38f;
+        float bzl = valid ? zi : 3.0e38f, bzh = valid ? zi : -3.0e38f;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            bxl = fminf(bxl, __shfl_xor_sync(0xffffffffu, bxl, o));
+            bxh = fmaxf(bxh, __shfl_xor_sync(0xffffffffu, bxh, o));
+            byl = fminf(byl, __shfl_xor_sync(0xffffffffu, byl, o));
+            byh = fmaxf(byh, __shfl_xor_sync(0xffffffffu, byh, o));
+            bzl = fminf(bzl, __shfl_xor_sync(0xffffffffu, bzl, o));
+            bzh = fmaxf(bzh, __shfl_xor_sync(0xffffffffu, bzh, o));
+        }
+        uint32_t *const row_i = A.nlist + (size_t)(i / GP) * A.cap * GP + (i % GP) * TP;
+        int base_i = 0, base_n = 0;  // this warp's slice of the row (pass 2)
+        for (int pass = 0; pass < (COUNT ? 1 : 2); pass++) {
+            const bool write = pass == 1;
+            int ci = 0, cn = 0;
+            for (int r = wib; r < side * side; r += kBuildWarps) {
+                const int kx = cx - m + r / side, ky = cy - m + r % side;
+                const int kxw = kx < 0 ? kx + g.ns.x : (kx >= g.ns.x ? kx - g.ns.x : kx);
+                const float sx = kx < 0 ? -A.box.L.x : (kx >= g.ns.x ? A.box.L.x : 0.f);
+                const int kyw = ky < 0 ? ky + g.ns.y : (ky >= g.ns.y ? ky - g.ns.y : ky);
+                const float sy = ky < 0 ? -A.box.L.y : (ky >= g.ns.y ? A.box.L.y : 0.f);
+                // distance from the chunk's box to this row of cells (image
+                // frame), shrunk by the margin
+                const float clx = g.lo.x + (float)kx * dsx;
+                const float cly = g.lo.y + (float)ky * dsy;
+                float dxm = fmaxf(fmaxf(clx - bxh, bxl - (clx + dsx)), 0.f);
+                float dym = fmaxf(fmaxf(cly - byh, byl - (cly + dsy)), 0.f);
+                dxm = fmaxf(dxm - 1e-3f * dsx, 0.f);
+                dym = fmaxf(dym - 1e-3f * dsy, 0.f);
+                const float rz2 = cutsq - dxm * dxm - dym * dym;
+                if (rz2 <= 0.f) continue;
+                const float rz = sqrtf(rz2) + 1e-3f * dsz;
+                const int zlo = max(cz - m, (int)floorf((bzl - rz - g.lo.z) * g.inv_ds.z));
+                const int zhi = min(cz + m, (int)floorf((bzh + rz - g.lo.z) * g.inv_ds.z));
+                const int rowbase = (kxw * g.ns.y + kyw) * g.ns.z;
+                // up to two contiguous z segments (the stencil wraps at most once)
+                for (int kz = zlo; kz <= zhi;) {
+                    int kzw, kend;
+                    float sz;
+                    if (kz < 0) {
+                        kzw = kz + g.ns.z;
+                        kend = min(zhi, -1);
+                        sz = -A.box.L.z;
+                    } else if (kz >= g.ns.z) {
+                        kzw = kz - g.ns.z;
+                        kend = zhi;
+                        sz = A.box.L.z;
+                    } else {
+                        kzw = kz;
+                        kend = min(zhi, g.ns.z - 1);
+                        sz = 0.f;
                     }
-                    const unsigned b = __ballot_sync(team_mask, hit);
-                    if (hit) {
-                        const unsigned mine = (T == 32) ? b : (b >> (a * T));
-                        const int pos = cnt + __popc(mine & ((1u << t) - 1u));
-                        if (pos < cap) {
-                            uint32_t entry = (uint32_t)p;
-                            if (use_excl) {
-                                const uint32_t oid = ids2[p];
-                                for (int e = e0; e < e1; e++) {
-                                    const uint32_t x = excl_ids[e];
-                                    if ((x & kExclMask) == oid) { entry |= x & ~kExclMask; break; }
+                    const int pbeg = (int)A.cell_start[rowbase + kzw];
+                    const int pend = (int)A.cell_start[rowbase + kzw + (kend - kz) + 1];
+                    kz = kend + 1;
+                    for (int p0 = pbeg; p0 < pend; p0 += 32) {
+                        const int nc = min(32, pend - p0);
+                        __syncwarp();
+                        if (lane < nc) {
+                            const int p = p0 + lane;
+                            const float4 pj = A.xs2[p];
+                            shx[lane] = make_float4(__fadd_rn(pj.x, sx), __fadd_rn(pj.y, sy), __fadd_rn(pj.z, sz),
+                                                    (A.part_q && A.ljmask) ? A.qs2[p] : 0.f);
+                            shi[lane] = make_uint2(A.use_excl ? A.ids2[p] : 0u, (uint32_t)type_of(pj));
+                        }
+                        __syncwarp();
+                        if (!valid) continue;
+#pragma unroll 4
+                        for (int k = 0; k < nc; k++) {
+                            const float4 cj = shx[k];
+                            const float ddx = __fsub_rn(cj.x, xi);
+                            const float ddy = __fsub_rn(cj.y, yi);
+                            const float ddz = __fsub_rn(cj.z, zi);
+                            const float r2 = __fmaf_rn(ddz, ddz, __fmaf_rn(ddy, ddy, __fmul_rn(ddx, ddx)));
+                            const int p = p0 + k;
+                            if (!(r2 < cutsq) || p == i) continue;
+                            bool act = true;
+                            uint2 it;
+                            if (A.ljmask || write) it = shi[k];
+                            if (A.ljmask) {
+                                act = ((amask >> it.y) & 1u) != 0u;
+                                if (!act && A.part_q) act = qi * cj.w != 0.f;
+                            }
+                            if (write) {
+                                const int pos = act ? base_i + ci : A.cap - 1 - (base_n + cn);
+                                if (base_i + ci + base_n + cn < A.cap) {
+                                    uint32_t entry = (uint32_t)p;
+                                    if (A.use_excl) {
+                                        const uint32_t dd = it.x - myid + 32u;
+                                        uint32_t depth = 0u;
+                                        if (dd < 64u)
+                                            depth = (uint32_t)((w1 >> dd) & 1ull) | ((uint32_t)((w2 >> dd) & 1ull) << 1);
+                                        if (far && depth == 0u) {
+                                            for (int e = A.excl_start[myid]; e < A.excl_start[myid + 1]; e++) {
+                                                const uint32_t x = A.excl_ids[e];
+                                                if ((x & kExclMask) == it.x) { depth = x >> 30; break; }
+                                            }
+                                        }
+                                        entry |= depth << 30;
+                                    }
+                                    row_i[(size_t)(pos / TP) * 32 + (pos % TP)] = entry;
                                 }
                             }
-                            // k-th entry: row k/T, column within team k%T
-                            mylist[(size_t)(pos / T) * 32 + (pos % T) - t] = entry;
+                            ci += act ? 1 : 0;
+                            cn += act ? 0 : 1;
                         }
                     }
-                    cnt += __popc(b);
+                }
+            }
+            if (pass == 0) {
+                sh_ci[wib][lane] = (uint32_t)ci;
+                sh_cn[wib][lane] = (uint32_t)cn;
+                __syncthreads();
+                uint32_t ti = 0u, tn = 0u;
+                for (int w = 0; w < kBuildWarps; w++) {
+                    const uint32_t a = sh_ci[w][lane], b = sh_cn[w][lane];
+                    if (w < wib) {
+                        base_i += (int)a;
+                        base_n += (int)b;
+                    }
+                    ti += a;
+                    tn += b;
+                }
+                if (valid && wib == 0) {
+                    const uint32_t cnt = ti + tn;
+                    if (COUNT) {
+                        atomicMax(&A.st->max_neighbors, cnt);
+                    } else {
+                        A.counts[i] = cnt;
+                        A.counts_int[i] = ti;
+                        if (cnt > (uint32_t)A.cap) atomicOr(&A.st->bits, kStatusNlistOverflow);
+                        atomicMax(&A.st->max_neighbors, cnt);
+                    }
                 }
             }
         }
-    }
-    if (t == 0) {
-        counts[i] = (uint32_t)cnt;
-        if (cnt > cap) atomicOr(&st->bits, kStatusNlistOverflow);
-        atomicMax(&st->max_neighbors, (uint32_t)cnt);
+        __syncthreads();  // sh_ci / sh_cn are reused by the next chunk
     }
 }
 
@@ -305,58 +425,6 @@ __global__ void k_finish(uint32_t *__restrict__ cell_count, int ncell, DeviceSta
     }
 }
 
-// count-only sweep used to size the list before the first build
-template <int T>
-__global__ void k_count_only(int n, const float4 *__restrict__ xs2, const uint32_t *__restrict__ cell_start,
-                             CellGrid g, Box box, int m, float cutsq, DeviceStatus *st) {
-    constexpr int G = 32 / T;
-    const int lane = threadIdx.x & 31;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int a = lane / T, t = lane % T;
-    const int i = warp * G + a;
-    if (i >= n) return;
-    const unsigned team_mask = (T == 32) ? 0xffffffffu : (((1u << T) - 1u) << (a * T));
-    const float3 pi = f3(xs2[i]);
-    const int cx = cell_coord(pi.x, g.lo.x, g.inv_ds.x, g.ns.x);
-    const int cy = cell_coord(pi.y, g.lo.y, g.inv_ds.y, g.ns.y);
-    const int cz = cell_coord(pi.z, g.lo.z, g.inv_ds.z, g.ns.z);
-    int cnt = 0;
-    for (int dx = -m; dx <= m; dx++) {
-        int kx = cx + dx;
-        float sx = 0.f;
-        if (kx < 0) { kx += g.ns.x; sx = -box.L.x; }
-        else if (kx >= g.ns.x) { kx -= g.ns.x; sx = box.L.x; }
-        for (int dy = -m; dy <= m; dy++) {
-            int ky = cy + dy;
-            float sy = 0.f;
-            if (ky < 0) { ky += g.ns.y; sy = -box.L.y; }
-            else if (ky >= g.ns.y) { ky -= g.ns.y; sy = box.L.y; }
-            const int rowbase = (kx * g.ns.y + ky) * g.ns.z;
-            for (int dz = -m; dz <= m; dz++) {
-                int kz = cz + dz;
-                float sz = 0.f;
-                if (kz < 0) { kz += g.ns.z; sz = -box.L.z; }
-                else if (kz >= g.ns.z) { kz -= g.ns.z; sz = box.L.z; }
-                const int pbeg = cell_start[rowbase + kz], pend = cell_start[rowbase + kz + 1];
-                for (int p0 = pbeg; p0 < pend; p0 += T) {
-                    const int p = p0 + t;
-                    bool hit = false;
-                    if (p < pend && p != i) {
-                        const float4 pj = xs2[p];
-                        const float ddx = __fsub_rn(__fadd_rn(pj.x, sx), pi.x);
-                        const float ddy = __fsub_rn(__fadd_rn(pj.y, sy), pi.y);
-                        const float ddz = __fsub_rn(__fadd_rn(pj.z, sz), pi.z);
-                        const float r2 = __fmaf_rn(ddz, ddz, __fmaf_rn(ddy, ddy, __fmul_rn(ddx, ddx)));
-                        hit = r2 < cutsq;
-                    }
-                    cnt += __popc(__ballot_sync(team_mask, hit));
-                }
-            }
-        }
-    }
-    if (t == 0) atomicMax(&st->max_neighbors, (uint32_t)cnt);
-}
-
 CellGrid make_grid(const State &s) {
     CellGrid g;
     g.lo = s.box.lo;
@@ -366,38 +434,58 @@ CellGrid make_grid(const State &s) {
     return g;
 }
 
-template <int T>
-void launch_build(State &s, const CellGrid &g, float cutsq) {
+BuildArgs build_args(State &s, const CellGrid &g, float cutsq) {
     GridGPU &gr = s.grid;
     GPUData &d = s.gpd;
-    int warps = (d.n + (32 / T) - 1) / (32 / T);
-    int blocks = (warps * 32 + 255) / 256;
-    k_build<T><<<blocks, 256, 0, s.stream>>>(
-        d.n, d.xs_alt.p, d.vs_alt.p, d.fs_alt.p, d.qs_alt.p, d.ids_alt.p, d.xs.p, d.vs.p, d.fs.p, d.qs.p, d.ids.p,
-        d.xs_last_build.p, gr.cell_start.p, g, s.box, gr.m, cutsq, gr.excl_start.p, gr.excl_ids.p,
-        gr.have_excl ? 1 : 0, gr.counts.p, gr.nlist.p, gr.cap, s.d_status.p);
+    BuildArgs A{};
+    A.xs2 = d.xs_alt.p;
+    A.vs2 = d.vs_alt.p;
+    A.fs2 = d.fs_alt.p;
+    A.qs2 = d.qs_alt.p;
+    A.ids2 = d.ids_alt.p;
+    A.xs = d.xs.p;
+    A.vs = d.vs.p;
+    A.fs = d.fs.p;
+    A.qs = d.qs.p;
+    A.ids = d.ids.p;
+    A.xs_last = d.xs_last_build.p;
+    A.cell_start = gr.cell_start.p;
+    A.excl_start = gr.excl_start.p;
+    A.excl_ids = gr.excl_ids.p;
+    A.excl_win = gr.excl_win.p;
+    A.excl_far = gr.excl_far.p;
+    A.ljmask = gr.partition ? gr.ljmask.p : nullptr;
+    A.counts = gr.counts.p;
+    A.counts_int = gr.counts_int.p;
+    A.nlist = gr.nlist.p;
+    A.st = s.d_status.p;
+    A.g = g;
+    A.box = s.box;
+    A.ncell = g.ns.x * g.ns.y * g.ns.z;
+    A.m = gr.m;
+    A.use_excl = gr.have_excl ? 1 : 0;
+    A.part_q = gr.part_q ? 1 : 0;
+    A.cap = gr.cap;
+    A.cutsq = cutsq;
+    return A;
+}
+
+template <int T>
+void launch_build(State &s, const CellGrid &g, float cutsq) {
+    const BuildArgs A = build_args(s, g, cutsq);
+    k_build_cells<T, false><<<A.ncell, kBuildWarps * 32, 0, s.stream>>>(A);
     MDX_LAUNCHED();
 }
 
 template <int T>
 void launch_count(State &s, const CellGrid &g, float cutsq) {
-    int warps = (s.gpd.n + (32 / T) - 1) / (32 / T);
-    int blocks = (warps * 32 + 255) / 256;
-    k_count_only<T><<<blocks, 256, 0, s.stream>>>(s.gpd.n, s.gpd.xs_alt.p, s.grid.cell_start.p, g, s.box, s.grid.m,
-                                                  cutsq, s.d_status.p);
+    BuildArgs A = build_args(s, g, cutsq);
+    A.use_excl = 0;
+    A.ljmask = nullptr;
+    A.part_q = 0;
+    A.cap = 0;
+    k_build_cells<T, true><<<A.ncell, kBuildWarps * 32, 0, s.stream>>>(A);
     MDX_LAUNCHED();
-}
-
-int dispatch_team(int team, void (*f1)(), void (*f2)(), void (*f4)(), void (*f8)(), void (*f16)(), void (*f32)()) {
-    switch (team) {
-        case 1: f1(); return 0;
-        case 2: f2(); return 0;
-        case 4: f4(); return 0;
-        case 8: f8(); return 0;
-        case 16: f16(); return 0;
-        case 32: f32(); return 0;
-    }
-    return MDX_ERR_ARG;
 }
 
 }  // namespace
@@ -444,10 +532,50 @@ int nlist_exclusions(State &s) {
         start[i + 1] = (int)ent.size();
         gr.max_excl = std::max(gr.max_excl, start[i + 1] - start[i]);
     }
+    std::vector<ulonglong2> win(nid, make_ulonglong2(0ull, 0ull));
+    std::vector<uint8_t> far(nid, 0);
+    for (int i = 0; i < nid; i++)
+        for (int e = start[i]; e < start[i + 1]; e++) {
+            const long long d = (long long)(ent[e] & kExclMask) - i + 32;
+            const uint32_t depth = ent[e] >> 30;
+            if (d < 0 || d >= 64) {
+                far[i] = 1;
+                continue;
+            }
+            if (depth & 1u) win[i].x |= 1ull << d;
+            if (depth & 2u) win[i].y |= 1ull << d;
+        }
+    if (int e = gr.excl_win.alloc(nid)) return e;
+    if (int e = gr.excl_far.alloc(nid)) return e;
+    MDX_CUDA_TRY(cudaMemcpy(gr.excl_win.p, win.data(), nid * sizeof(ulonglong2), cudaMemcpyHostToDevice));
+    MDX_CUDA_TRY(cudaMemcpy(gr.excl_far.p, far.data(), nid * sizeof(uint8_t), cudaMemcpyHostToDevice));
     if (int e = gr.excl_start.alloc(start.size())) return e;
     if (int e = gr.excl_ids.alloc(ent.size())) return e;
     MDX_CUDA_TRY(cudaMemcpy(gr.excl_start.p, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
     MDX_CUDA_TRY(cudaMemcpy(gr.excl_ids.p, ent.data(), ent.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    return 0;
+}
+
+// Which listed pairs can interact: bit tj of ljmask[ti] is set when the pair
+// fix's eps(ti, tj) != 0; with an Ewald fix, pairs with q_i q_j != 0 also
+// interact.  Everything else contributes exactly zero force, energy and
+// virial in compute_force_iso (PairEvaluatorLJ.h:17-30 scales by eps,
+// ChargeEvaluatorEwald.h:11-40 by q_i q_j) and is kept at the back of the row.
+int nlist_set_interactions(State &s) {
+    GridGPU &gr = s.grid;
+    FixPair *pf = s.pairFix();
+    const int nt = (int)s.species.size();
+    gr.partition = false;
+    gr.part_q = false;
+    if (!pf || nt > 32 || pf->h_params.size() != (size_t)3 * nt * nt) return 0;
+    std::vector<uint32_t> mask(nt, 0u);
+    for (int a = 0; a < nt; a++)
+        for (int b = 0; b < nt; b++)
+            if (pf->h_params[nt * nt + a * nt + b] != 0.f) mask[a] |= 1u << b;
+    if (int e = gr.ljmask.alloc(nt)) return e;
+    MDX_CUDA_TRY(cudaMemcpy(gr.ljmask.p, mask.data(), nt * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    gr.partition = true;
+    gr.part_q = pf->chargeFix != nullptr;
     return 0;
 }
 
@@ -481,6 +609,7 @@ int nlist_init(State &s) {
     if (int e = gr.perm_tmp.alloc(n)) return e;
     if (int e = gr.perm.alloc(n)) return e;
     if (int e = gr.counts.alloc(n)) return e;
+    if (int e = gr.counts_int.alloc(n)) return e;
     if (s.nThreadPerAtom > 0) {
         gr.team = s.nThreadPerAtom;
     } else {

@@ -272,7 +272,7 @@ PairArgs make_args(State &s, FixPair &f) {
     A.xs = s.gpd.xs.p;
     A.fs = s.gpd.fs.p;
     A.qs = s.gpd.qs.p;
-    A.counts = s.grid.counts.p;
+    A.counts = s.grid.partition ? s.grid.counts_int.p : s.grid.counts.p;
     A.nlist = s.grid.nlist.p;
     A.cap = s.grid.cap;
     A.params = f.d_params.p;

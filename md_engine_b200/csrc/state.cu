@@ -31,6 +31,11 @@ State::State() {
 
 State::~State() {
     if (h_status) cudaFreeHost(h_status);
+    for (int k = 0; k < 2; k++) {
+        if (side[k]) cudaStreamDestroy(side[k]);
+        if (ev_join[k]) cudaEventDestroy(ev_join[k]);
+    }
+    if (ev_fork) cudaEventDestroy(ev_fork);
     if (stream && own_stream) cudaStreamDestroy(stream);
 }
 
@@ -91,6 +96,11 @@ int State::upload() {
         MDX_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         own_stream = true;
     }
+    for (int k = 0; k < 2; k++) {
+        if (!side[k]) MDX_CUDA_TRY(cudaStreamCreateWithFlags(&side[k], cudaStreamNonBlocking));
+        if (!ev_join[k]) MDX_CUDA_TRY(cudaEventCreateWithFlags(&ev_join[k], cudaEventDisableTiming));
+    }
+    if (!ev_fork) MDX_CUDA_TRY(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
     if (!h_status) MDX_CUDA_TRY(cudaMallocHost(&h_status, sizeof(DeviceStatus)));
     if (int e = d_status.alloc(1)) return e;
     MDX_CUDA_TRY(cudaMemset(d_status.p, 0, sizeof(DeviceStatus)));
@@ -257,6 +267,7 @@ int State::prepare() {
     if (FixRigid *r = rigidFix()) {
         if (int e = r->prepareForRun()) return e;  // device molecule arrays
     }
+    if (int e = nlist_set_interactions(*this)) return e;
     // first build (GridGPU::periodicBoundaryConditions(-1, true), Integrator.cu:216)
     if (int e = nlist_rebuild(*this, true, false)) return e;
     if (int e = computeForces(0)) return e;  // forceInitial

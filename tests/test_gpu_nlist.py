@@ -105,3 +105,23 @@ def test_small_box_edge_cases(oracle):
         assert np.array_equal(counts_g, counts_o)
         for i in range(len(x)):
             assert np.array_equal(nbr_g[i, :counts_g[i]], np.sort(nbr_o[i, :counts_o[i]]).astype(np.int32))
+
+
+def test_water_far_exclusions_bit_exact(oracle):
+    """ids numbered site-major (all O, then all H1, H2, M): every exclusion
+    partner lies thousands of ids away, outside the id window the build reads
+    its exclusion depths from, so the tags come from the id list instead."""
+    base = systems.water_tip4p2005(nside=8, seed=21)
+    M = len(base.molecules)
+    new_id = np.empty(4 * M, np.int64)
+    for j, mol in enumerate(base.molecules):
+        for k, old in enumerate(mol):
+            new_id[old] = k * M + j
+    order = np.argsort(new_id)
+    sysd = systems.System(base.pos[order], base.vel[order], base.types[order], base.q[order],
+                          base.mass[order], base.L, base.lo, base.species,
+                          new_id[np.asarray(base.molecules)])
+    st, _ = systems.build_water_state(sysd, rcut=6.5, skin=1.0, grid=32)
+    excl = oracle.exclusions_from_bonds(len(sysd.pos), water_bonds(sysd.molecules))
+    counts = _compare(oracle, st, sysd, 6.5, 1.0, excl=excl)
+    assert counts.mean() > 150
