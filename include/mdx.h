@@ -200,6 +200,59 @@ int mdx_pair_force_raw(int n, const float *xs4, float *fs4, const float *qs, con
                        const double lo[3], const double hi[3], const float coef[3], int lj_kind, float qrc,
                        float alpha, float qqr_to_eng, float *virials, int accumulate, void *cuda_stream);
 
+/* ---- learned E3B three-body surrogate (no reference counterpart; the exact
+ *      term is src/Fixes/ThreeBodyE3B.h:255-549, which stays the fallback) --
+ * Per molecule: a frame (e1 along the H-O-H bisector, e2 toward H1, e3 =
+ * e1 x e2) and 128 invariant features (O->O, O->H, H1->O, H2->O channels x 8
+ * Gaussian shells x {weight sum, weighted unit vector in the frame}); an MLP
+ * 128-64-64-64-9 (SiLU; BF16 operands, FP32 accumulation) gives the
+ * three-body forces on O, H1, H2 in the frame.  collect appends the current
+ * frame's features and exact three-body forces to a device dataset; train
+ * standardises (first call) and runs Adam; enable switches the fix's force
+ * evaluations (fused step and compute) between exact (0) and surrogate (1);
+ * eval compares surrogate and exact three-body forces on the current frame.
+ * The exact O-O two-body term is always evaluated exactly.  Parameters are
+ * kParams = 17,552 floats: W1[128x64] b1 W2[64x64] b2 W3[64x64] b3 W4[64x16]
+ * b4[16] (outputs 9..15 unused). */
+int mdx_e3b_surrogate_collect(mdx_state *st, mdx_fix *e3b);
+int mdx_e3b_surrogate_dataset_size(mdx_fix *e3b, int64_t *n);
+int mdx_e3b_surrogate_train(mdx_state *st, mdx_fix *e3b, int iters, int batch, float lr, uint64_t seed,
+                            double *loss_first, double *loss_last);
+int mdx_e3b_surrogate_enable(mdx_fix *e3b, int on);
+int mdx_e3b_surrogate_eval(mdx_state *st, mdx_fix *e3b, double *rmse, double *rms);
+int mdx_e3b_surrogate_get_params(mdx_fix *e3b, float *w, float *mean, float *inv_std, float *scale);
+int mdx_e3b_surrogate_set_params(mdx_state *st, mdx_fix *e3b, const float *w, const float *mean,
+                                 const float *inv_std, float scale);
+/* raw features (nmol x 128) and frames (nmol x 9) of the current positions */
+int mdx_e3b_surrogate_features(mdx_state *st, mdx_fix *e3b, float *raw, float *frames);
+/* model outputs (n x 16) for n standardised feature rows (n x 128) */
+int mdx_e3b_surrogate_infer(mdx_state *st, mdx_fix *e3b, const float *x, int n, float *y);
+/* mean-squared-error loss and its gradient (17,552 floats) for n rows of
+ * standardised features x (n x 128) and scaled targets t (n x 16); n % 64 == 0 */
+int mdx_e3b_surrogate_grad(mdx_state *st, mdx_fix *e3b, const float *x, const float *t, int n, float *grad,
+                           double *loss);
+
+/* ---- batched replicas (no reference counterpart: DASH runs one State per
+ *      process, src/Integrators/IntegratorVerlet.cu:649-770) --------------
+ * Many independent rigid-water systems, each a configured mdx_state with its
+ * own box, size and FixNoseHoover temperature, advanced together: every phase
+ * of the step is one launch covering all replicas and each chunk of steps is
+ * one CUDA graph.  Every replica needs a pair fix, FixChargeEwald, FixRigid
+ * (all atoms in molecules) and FixNoseHoover, the same fix set (E3B in all or
+ * none), periodicInterval and species count.  The batch does not own the
+ * states; destroy the batch before its states.  run returns the device time
+ * of the whole call in device_ms (may be NULL); run_timed brackets chunks of
+ * `chunk` turns with CUDA events after an L2 flush of flush_bytes and returns
+ * their summed device time. */
+typedef struct mdx_batch mdx_batch;
+int mdx_batch_create(mdx_batch **out);
+int mdx_batch_add(mdx_batch *b, mdx_state *st);
+int mdx_batch_size(mdx_batch *b, int *n);
+int mdx_batch_prepare(mdx_batch *b);
+int mdx_batch_run(mdx_batch *b, int num_turns, double *device_ms);
+int mdx_batch_run_timed(mdx_batch *b, int num_turns, int chunk, size_t flush_bytes, double *device_ms);
+int mdx_batch_destroy(mdx_batch *b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -86,6 +86,23 @@ SIGNATURES = [
     ("mdx_pair_force_raw", c_int, [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int,
                                    c_void_p, c_int, P(c_dbl), P(c_dbl), P(c_flt), c_int, c_flt, c_flt, c_flt,
                                    c_void_p, c_int, c_void_p]),
+    ("mdx_e3b_surrogate_collect", c_int, [c_void_p, c_void_p]),
+    ("mdx_e3b_surrogate_dataset_size", c_int, [c_void_p, P(ctypes.c_int64)]),
+    ("mdx_e3b_surrogate_train", c_int, [c_void_p, c_void_p, c_int, c_int, c_flt, ctypes.c_uint64, P(c_dbl), P(c_dbl)]),
+    ("mdx_e3b_surrogate_enable", c_int, [c_void_p, c_int]),
+    ("mdx_e3b_surrogate_eval", c_int, [c_void_p, c_void_p, P(c_dbl), P(c_dbl)]),
+    ("mdx_e3b_surrogate_get_params", c_int, [c_void_p, P(c_flt), P(c_flt), P(c_flt), P(c_flt)]),
+    ("mdx_e3b_surrogate_set_params", c_int, [c_void_p, c_void_p, P(c_flt), P(c_flt), P(c_flt), c_flt]),
+    ("mdx_e3b_surrogate_features", c_int, [c_void_p, c_void_p, P(c_flt), P(c_flt)]),
+    ("mdx_e3b_surrogate_infer", c_int, [c_void_p, c_void_p, P(c_flt), c_int, P(c_flt)]),
+    ("mdx_e3b_surrogate_grad", c_int, [c_void_p, c_void_p, P(c_flt), P(c_flt), c_int, P(c_flt), P(c_dbl)]),
+    ("mdx_batch_create", c_int, [P(c_void_p)]),
+    ("mdx_batch_add", c_int, [c_void_p, c_void_p]),
+    ("mdx_batch_size", c_int, [c_void_p, P(c_int)]),
+    ("mdx_batch_prepare", c_int, [c_void_p]),
+    ("mdx_batch_run", c_int, [c_void_p, c_int, P(c_dbl)]),
+    ("mdx_batch_run_timed", c_int, [c_void_p, c_int, c_int, ctypes.c_size_t, P(c_dbl)]),
+    ("mdx_batch_destroy", c_int, [c_void_p]),
 ]
 
 

@@ -134,16 +134,52 @@ __device__ __forceinline__ float pair_energy(const E3BParams &p, const float *e,
     return s;
 }
 
+// Arguments of the E3B kernels for one system: a0 (single system) or
+// tab[blockIdx.y] (batched replicas; a0 then only sizes the grid).
+struct E3BArgs {
+    int nmol;
+    const int4 *mol_ids;
+    int4 *mol_idx;
+    const int *idToIdx, *mol_of_id;
+    const uint32_t *ids;
+    const float4 *xs;
+    const uint32_t *counts, *counts_int, *nlist;
+    int team_atom, cap_atom;
+    Box box;
+    float cut2;
+    uint32_t *mcounts, *mlist;
+    int mcap;
+    DeviceStatus *st;
+    float4 *out;      // forces (added) or the per-step side buffer (STORE)
+    E3BParams p;
+    float4 *totals;
+    double *e_out;    // energy passes
+    int twobody;      // 0: the totals pass leaves out the O-O two-body force
+};
+#define MDX_E3B_ARGS const E3BArgs A = tab ? tab[blockIdx.y] : a0
+
 // updateMoleculeIdxsMap (FixE3B.cu:41-65) + molecule list cut from the atom
 // list: O-O pairs with r^2 < (rf + 1 + skin)^2.  Team of T lanes per molecule.
 template <int T>
-__global__ void k_e3b_list(int nmol, const int4 *__restrict__ mol_ids, int4 *__restrict__ mol_idx,
-                           const int *__restrict__ idToIdx, const int *__restrict__ mol_of_id,
-                           const uint32_t *__restrict__ ids, const float4 *__restrict__ xs,
-                           const uint32_t *__restrict__ counts, const uint32_t *__restrict__ counts_int,
-                           const uint32_t *__restrict__ nlist, int team_atom,
-                           int cap_atom, Box box, float cut2, uint32_t *__restrict__ mcounts,
-                           uint32_t *__restrict__ mlist, int mcap, DeviceStatus *st, int conditional) {
+__global__ void k_e3b_list(const E3BArgs a0, const E3BArgs *__restrict__ tab, int conditional) {
+    MDX_E3B_ARGS;
+    DeviceStatus *st = A.st;
+    const int nmol = A.nmol;
+    const int4 *__restrict__ mol_ids = A.mol_ids;
+    int4 *__restrict__ mol_idx = A.mol_idx;
+    const int *__restrict__ idToIdx = A.idToIdx;
+    const int *__restrict__ mol_of_id = A.mol_of_id;
+    const uint32_t *__restrict__ ids = A.ids;
+    const float4 *__restrict__ xs = A.xs;
+    const uint32_t *__restrict__ counts = A.counts;
+    const uint32_t *__restrict__ counts_int = A.counts_int;
+    const uint32_t *__restrict__ nlist = A.nlist;
+    const int team_atom = A.team_atom, cap_atom = A.cap_atom;
+    const Box &box = A.box;
+    const float cut2 = A.cut2;
+    uint32_t *__restrict__ mcounts = A.mcounts;
+    uint32_t *__restrict__ mlist = A.mlist;
+    const int mcap = A.mcap;
     if (conditional && !st->rebuild) return;
     constexpr int G = 32 / T;
     const int lane = threadIdx.x & 31;
@@ -199,10 +235,19 @@ __global__ void k_e3b_list(int nmol, const int4 *__restrict__ mol_ids, int4 *__r
 // STORE: write into a per-step side buffer instead of adding to the forces
 // (lets E3B run concurrently with the pair kernel; the second half merges it)
 template <int T, bool ENERGY, bool STORE = false>
-__global__ void k_e3b_totals(int nmol, const int4 *__restrict__ mol_idx, const float4 *__restrict__ xs,
-                             float4 *__restrict__ fs, const uint32_t *__restrict__ mcounts,
-                             const uint32_t *__restrict__ mlist, int mcap, Box box, E3BParams p,
-                             float4 *__restrict__ totals, double *__restrict__ e2_out) {
+__global__ void k_e3b_totals(const E3BArgs a0, const E3BArgs *__restrict__ tab) {
+    MDX_E3B_ARGS;
+    const int nmol = A.nmol;
+    const int4 *__restrict__ mol_idx = A.mol_idx;
+    const float4 *__restrict__ xs = A.xs;
+    float4 *__restrict__ fs = A.out;
+    const uint32_t *__restrict__ mcounts = A.mcounts;
+    const uint32_t *__restrict__ mlist = A.mlist;
+    const int mcap = A.mcap;
+    const Box &box = A.box;
+    const E3BParams &p = A.p;
+    float4 *__restrict__ totals = A.totals;
+    double *__restrict__ e2_out = A.e_out;
     constexpr int G = 32 / T;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -260,6 +305,7 @@ __global__ void k_e3b_totals(int nmol, const int4 *__restrict__ mol_idx, const f
     tx = tsum<T>(tx);
     ty = tsum<T>(ty);
     tz = tsum<T>(tz);
+    if (!A.twobody) fx = fy = fz = 0.f;
     if (valid && t == 0) {
         totals[m] = make_float4(tx, ty, tz, 0.f);
         if (STORE) {
@@ -276,10 +322,19 @@ __global__ void k_e3b_totals(int nmol, const int4 *__restrict__ mol_idx, const f
 
 // pass 2: three-body forces on molecule i's O, H1, H2 (ThreeBodyE3B.h:255-549)
 template <int T, bool ENERGY, bool STORE = false>
-__global__ void k_e3b_forces(int nmol, const int4 *__restrict__ mol_idx, const float4 *__restrict__ xs,
-                             float4 *__restrict__ fs, const uint32_t *__restrict__ mcounts,
-                             const uint32_t *__restrict__ mlist, int mcap, Box box, E3BParams p,
-                             const float4 *__restrict__ totals, double *__restrict__ e3_out) {
+__global__ void k_e3b_forces(const E3BArgs a0, const E3BArgs *__restrict__ tab) {
+    MDX_E3B_ARGS;
+    const int nmol = A.nmol;
+    const int4 *__restrict__ mol_idx = A.mol_idx;
+    const float4 *__restrict__ xs = A.xs;
+    float4 *__restrict__ fs = A.out;
+    const uint32_t *__restrict__ mcounts = A.mcounts;
+    const uint32_t *__restrict__ mlist = A.mlist;
+    const int mcap = A.mcap;
+    const Box &box = A.box;
+    const E3BParams &p = A.p;
+    const float4 *__restrict__ totals = A.totals;
+    double *__restrict__ e3_out = A.e_out;
     constexpr int G = 32 / T;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -426,16 +481,45 @@ int FixE3B::prepareForRun() {
     return 0;
 }
 
+static E3BArgs e3b_args(State &s, FixE3B &f, float4 *out) {
+    E3BArgs A{};
+    const float lc = (float)((double)f.prm.rf + 1.0 + s.padding);
+    A.nmol = (int)f.mol_ids.size();
+    A.mol_ids = f.d_mol_ids.p;
+    A.mol_idx = f.d_mol_idx.p;
+    A.idToIdx = s.gpd.idToIdx.p;
+    A.mol_of_id = f.d_mol_of_atom.p;
+    A.ids = s.gpd.ids.p;
+    A.xs = s.gpd.xs.p;
+    A.counts = s.grid.counts.p;
+    A.counts_int = s.grid.partition ? s.grid.counts_int.p : nullptr;
+    A.nlist = s.grid.nlist.p;
+    A.team_atom = s.grid.team;
+    A.cap_atom = s.grid.cap;
+    A.box = s.box;
+    A.cut2 = lc * lc;
+    A.mcounts = f.mcounts.p;
+    A.mlist = f.mlist.p;
+    A.mcap = f.mcap;
+    A.st = s.d_status.p;
+    A.out = out;
+    A.p = f.prm;
+    A.totals = f.totals.p;
+    A.e_out = nullptr;
+    A.twobody = 1;
+    return A;
+}
+
+static dim3 e3b_blocks(int nmol, unsigned nrep = 1) {
+    const int warps = (nmol + (32 / kMolTeam) - 1) / (32 / kMolTeam);
+    return dim3((warps * 32 + 255) / 256, nrep);
+}
+
 int e3b_build_list(State &s, FixE3B &f, bool conditional) {
     const int nmol = (int)f.mol_ids.size();
     if (nmol == 0 || !f.prepared) return 0;
-    const float lc = (float)((double)f.prm.rf + 1.0 + s.padding);
-    const int warps = (nmol + (32 / kMolTeam) - 1) / (32 / kMolTeam);
-    k_e3b_list<kMolTeam><<<(warps * 32 + 255) / 256, 256, 0, s.stream>>>(
-        nmol, f.d_mol_ids.p, f.d_mol_idx.p, s.gpd.idToIdx.p, f.d_mol_of_atom.p, s.gpd.ids.p, s.gpd.xs.p,
-        s.grid.counts.p, s.grid.partition ? s.grid.counts_int.p : nullptr, s.grid.nlist.p, s.grid.team, s.grid.cap,
-        s.box, lc * lc, f.mcounts.p, f.mlist.p, f.mcap,
-        s.d_status.p, conditional ? 1 : 0);
+    k_e3b_list<kMolTeam><<<e3b_blocks(nmol), 256, 0, s.stream>>>(e3b_args(s, f, nullptr), nullptr,
+                                                                 conditional ? 1 : 0);
     MDX_LAUNCHED();
     return 0;
 }
@@ -447,22 +531,45 @@ int e3b_forces(State &s, FixE3B &f) { return e3b_forces_to(s, f, s.gpd.fs.p, fal
 int e3b_forces_to(State &s, FixE3B &f, float4 *out, bool side, cudaStream_t stream) {
     const int nmol = (int)f.mol_ids.size();
     if (nmol == 0) return 0;
-    const int warps = (nmol + (32 / kMolTeam) - 1) / (32 / kMolTeam);
-    const int blocks = (warps * 32 + 255) / 256;
+    const E3BArgs A = e3b_args(s, f, out);
+    const dim3 blocks = e3b_blocks(nmol);
     if (side) {
-        k_e3b_totals<kMolTeam, false, true><<<blocks, 256, 0, stream>>>(
-            nmol, f.d_mol_idx.p, s.gpd.xs.p, out, f.mcounts.p, f.mlist.p, f.mcap, s.box, f.prm, f.totals.p, nullptr);
+        k_e3b_totals<kMolTeam, false, true><<<blocks, 256, 0, stream>>>(A, nullptr);
         MDX_LAUNCHED();
-        k_e3b_forces<kMolTeam, false, true><<<blocks, 256, 0, stream>>>(
-            nmol, f.d_mol_idx.p, s.gpd.xs.p, out, f.mcounts.p, f.mlist.p, f.mcap, s.box, f.prm, f.totals.p, nullptr);
+        k_e3b_forces<kMolTeam, false, true><<<blocks, 256, 0, stream>>>(A, nullptr);
         MDX_LAUNCHED();
         return 0;
     }
-    k_e3b_totals<kMolTeam, false><<<blocks, 256, 0, stream>>>(nmol, f.d_mol_idx.p, s.gpd.xs.p, out, f.mcounts.p,
-                                                             f.mlist.p, f.mcap, s.box, f.prm, f.totals.p, nullptr);
+    k_e3b_totals<kMolTeam, false><<<blocks, 256, 0, stream>>>(A, nullptr);
     MDX_LAUNCHED();
-    k_e3b_forces<kMolTeam, false><<<blocks, 256, 0, stream>>>(nmol, f.d_mol_idx.p, s.gpd.xs.p, out, f.mcounts.p,
-                                                             f.mlist.p, f.mcap, s.box, f.prm, f.totals.p, nullptr);
+    k_e3b_forces<kMolTeam, false><<<blocks, 256, 0, stream>>>(A, nullptr);
+    MDX_LAUNCHED();
+    return 0;
+}
+
+// exact E3B forces stored into out[O], out[H1], out[H2]; twobody = 0 leaves
+// out the O-O two-body term (the three-body forces alone: the surrogate's
+// training target and judge)
+int e3b_exact_to(State &s, FixE3B &f, float4 *out, int twobody, cudaStream_t stream) {
+    const int nmol = (int)f.mol_ids.size();
+    if (nmol == 0) return 0;
+    E3BArgs A = e3b_args(s, f, out);
+    A.twobody = twobody;
+    const dim3 blocks = e3b_blocks(nmol);
+    k_e3b_totals<kMolTeam, false, true><<<blocks, 256, 0, stream>>>(A, nullptr);
+    MDX_LAUNCHED();
+    k_e3b_forces<kMolTeam, false, true><<<blocks, 256, 0, stream>>>(A, nullptr);
+    MDX_LAUNCHED();
+    return 0;
+}
+
+// the O-O two-body force alone, stored into out[O] (the exact part of the
+// surrogate step)
+int e3b_twobody_to(State &s, FixE3B &f, float4 *out, cudaStream_t stream) {
+    const int nmol = (int)f.mol_ids.size();
+    if (nmol == 0) return 0;
+    E3BArgs A = e3b_args(s, f, out);
+    k_e3b_totals<kMolTeam, false, true><<<e3b_blocks(nmol), 256, 0, stream>>>(A, nullptr);
     MDX_LAUNCHED();
     return 0;
 }
@@ -474,28 +581,79 @@ int e3b_energy(State &s, FixE3B &f, double out[2]) {
     DBuf<double> acc;
     if (int e = acc.alloc(2)) return e;
     MDX_CUDA_TRY(cudaMemsetAsync(acc.p, 0, 2 * sizeof(double), s.stream));
-    const int warps = (nmol + (32 / kMolTeam) - 1) / (32 / kMolTeam);
-    const int blocks = (warps * 32 + 255) / 256;
+    const dim3 blocks = e3b_blocks(nmol);
     // totals are needed by the energy pass: run the force-less totals first
     DBuf<float4> ftmp;
     if (int e = ftmp.alloc(s.gpd.n)) return e;
     MDX_CUDA_TRY(cudaMemcpyAsync(ftmp.p, s.gpd.fs.p, s.gpd.n * sizeof(float4), cudaMemcpyDeviceToDevice, s.stream));
-    k_e3b_totals<kMolTeam, false><<<blocks, 256, 0, s.stream>>>(nmol, f.d_mol_idx.p, s.gpd.xs.p, ftmp.p, f.mcounts.p,
-                                                               f.mlist.p, f.mcap, s.box, f.prm, f.totals.p, nullptr);
+    E3BArgs A = e3b_args(s, f, ftmp.p);
+    k_e3b_totals<kMolTeam, false><<<blocks, 256, 0, s.stream>>>(A, nullptr);
     MDX_LAUNCHED();
-    k_e3b_totals<kMolTeam, true><<<blocks, 256, 0, s.stream>>>(nmol, f.d_mol_idx.p, s.gpd.xs.p, ftmp.p, f.mcounts.p,
-                                                              f.mlist.p, f.mcap, s.box, f.prm, f.totals.p, acc.p);
+    A.e_out = acc.p;
+    k_e3b_totals<kMolTeam, true><<<blocks, 256, 0, s.stream>>>(A, nullptr);
     MDX_LAUNCHED();
-    k_e3b_forces<kMolTeam, true><<<blocks, 256, 0, s.stream>>>(nmol, f.d_mol_idx.p, s.gpd.xs.p, ftmp.p, f.mcounts.p,
-                                                              f.mlist.p, f.mcap, s.box, f.prm, f.totals.p, acc.p + 1);
+    A.e_out = acc.p + 1;
+    k_e3b_forces<kMolTeam, true><<<blocks, 256, 0, s.stream>>>(A, nullptr);
     MDX_LAUNCHED();
     MDX_CUDA_TRY(cudaMemcpyAsync(out, acc.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
     MDX_CUDA_TRY(cudaStreamSynchronize(s.stream));
     return 0;
 }
 
+// ---- batched replicas: one launch per pass, blockIdx.y = replica ----------
+int batch_e3b_tables(Batch &b) {
+    const int R = (int)b.reps.size();
+    std::vector<E3BArgs> h(R);
+    for (int r = 0; r < R; r++) {
+        State &s = *b.reps[r];
+        FixE3B &f = *s.e3bFix();
+        if (!f.side_ok || !f.f_side.p) {
+            set_error(MDX_ERR_UNSUPPORTED, "batched E3B needs FixRigid molecules matching the E3B molecules");
+            return MDX_ERR_UNSUPPORTED;
+        }
+        h[r] = e3b_args(s, f, f.f_side.p);
+    }
+    if (int e = b.tab_e3b.alloc(R * sizeof(E3BArgs))) return e;
+    MDX_CUDA_TRY(cudaMemcpy(b.tab_e3b.p, h.data(), R * sizeof(E3BArgs), cudaMemcpyHostToDevice));
+    return 0;
+}
+
+static int batch_e3b_sizing(Batch &b, E3BArgs *out) {
+    if (!b.tab_e3b.p) {
+        set_error(MDX_ERR_STATE, "batch tables not built (prepare the batch)");
+        return MDX_ERR_STATE;
+    }
+    State &s0 = *b.reps[0];
+    E3BArgs A = e3b_args(s0, *s0.e3bFix(), nullptr);
+    A.nmol = b.max_mol;
+    *out = A;
+    return 0;
+}
+
+int batch_e3b_list(Batch &b) {
+    E3BArgs A;
+    if (int e = batch_e3b_sizing(b, &A)) return e;
+    k_e3b_list<kMolTeam><<<e3b_blocks(b.max_mol, (unsigned)b.reps.size()), 256, 0, b.stream>>>(
+        A, reinterpret_cast<const E3BArgs *>(b.tab_e3b.p), 1);
+    MDX_LAUNCHED();
+    return 0;
+}
+
+int batch_e3b_forces(Batch &b, cudaStream_t stream) {
+    E3BArgs A;
+    if (int e = batch_e3b_sizing(b, &A)) return e;
+    const E3BArgs *tab = reinterpret_cast<const E3BArgs *>(b.tab_e3b.p);
+    const dim3 blocks = e3b_blocks(b.max_mol, (unsigned)b.reps.size());
+    k_e3b_totals<kMolTeam, false, true><<<blocks, 256, 0, stream>>>(A, tab);
+    MDX_LAUNCHED();
+    k_e3b_forces<kMolTeam, false, true><<<blocks, 256, 0, stream>>>(A, tab);
+    MDX_LAUNCHED();
+    return 0;
+}
+
 int FixE3B::compute(int virialMode) {
     (void)virialMode;
+    if (sur && sur->enabled) return surrogate_compute(*state, *this);
     return e3b_forces(*state, *this);
 }
 

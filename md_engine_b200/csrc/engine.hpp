@@ -2,6 +2,7 @@
 // mirroring the reference's operator API (src/State.h, src/GPUData.h,
 // src/GridGPU.h, src/Fixes/Fix.h, src/Integrators/IntegratorVerlet.h).
 #pragma once
+#include <cuda_bf16.h>
 #include <cufft.h>
 
 #include <map>
@@ -21,8 +22,13 @@ template <class T>
 struct DBuf {
     T *p = nullptr;
     size_t n = 0;
+    bool own = true;  // false: a view into memory owned elsewhere (a pool)
     int alloc(size_t count) {
         if (count <= n && p) return 0;
+        if (!own) {
+            set_error(MDX_ERR_STATE, "buffer is a pool view of %zu elements; %zu requested", n, count);
+            return MDX_ERR_STATE;
+        }
         release();
         if (count == 0) count = 1;
         cudaError_t e = cudaMalloc(&p, count * sizeof(T));
@@ -36,9 +42,16 @@ struct DBuf {
         return 0;
     }
     void release() {
-        if (p) cudaFree(p);
+        if (p && own) cudaFree(p);
         p = nullptr;
         n = 0;
+        own = true;
+    }
+    void view(T *q, size_t count) {
+        release();
+        p = q;
+        n = count;
+        own = false;
     }
     ~DBuf() { release(); }
     DBuf() = default;
@@ -210,9 +223,40 @@ struct E3BParams {  // EvaluatorE3B (EvaluatorE3B.h:9-65), FixE3B.cu:515-593
     float rmax;       // RMAX_E3B (ThreeBodyE3B.h:16)
 };
 
+// Learned surrogate of the E3B three-body forces (no reference counterpart):
+// per-molecule local-frame features -> MLP (3 x 64 SiLU, BF16 operands, FP32
+// accumulation) -> the three-body forces on O, H1, H2 in the molecule's frame.
+struct E3BSurrogate {
+    static constexpr int kIn = 128, kHid = 64, kOut = 16, kOutUsed = 9;
+    // parameter blob (floats): W1 [kIn x kHid], b1, W2 [kHid x kHid], b2, W3, b3, W4 [kHid x kOut], b4
+    static constexpr int kOffW1 = 0, kOffB1 = kIn * kHid, kOffW2 = kOffB1 + kHid, kOffB2 = kOffW2 + kHid * kHid,
+                         kOffW3 = kOffB2 + kHid, kOffB3 = kOffW3 + kHid * kHid, kOffW4 = kOffB3 + kHid,
+                         kOffB4 = kOffW4 + kHid * kOut, kParams = kOffB4 + kOut;
+    DBuf<float> w, grad, adam_m, adam_v;  // FP32 master weights, gradient, Adam moments
+    DBuf<__nv_bfloat16> wb;               // BF16 copy used by every GEMM (same offsets)
+    DBuf<float> mean, inv_std;            // feature standardisation
+    float force_scale = 1.f;              // targets are local-frame forces / force_scale
+    bool stats = false, trained = false, enabled = false;
+    int64_t adam_t = 0;
+    // dataset (raw features, local-frame exact three-body forces)
+    DBuf<float> X, Y;
+    size_t n = 0, cap = 0;
+    // per-step scratch
+    DBuf<__nv_bfloat16> feat;
+    DBuf<float> raw;
+    DBuf<float4> frame;
+    DBuf<float4> fexact;
+    // training scratch
+    DBuf<__nv_bfloat16> xb, act[3], dz;
+    DBuf<float> z[4], yb, da;
+    DBuf<double> loss;
+    int batch = 0;
+};
+
 class FixE3B : public Fix {
    public:
     std::string style;
+    std::unique_ptr<E3BSurrogate> sur;
     std::vector<int4> mol_ids;
     E3BParams prm{};
     DBuf<int4> d_mol_ids, d_mol_idx;
@@ -322,6 +366,67 @@ class State {
     double maxRCut();
 };
 
+// ---------------------------------------------------------------- Batch
+// Independent replicas (each a full State with its own box, temperature and
+// size) advanced together: every phase of the step is ONE launch whose
+// gridDim.y is the replica count and whose blockIdx.y selects the replica's
+// argument record in a device table; gridDim.x is sized for the largest
+// replica and blocks past a smaller replica's work return at once.  The whole
+// step (rebuild group included) is captured into one CUDA graph per chunk.
+class Batch {
+   public:
+    std::vector<State *> reps;
+    cudaStream_t stream = nullptr;
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
+    bool prepared = false;
+    int periodicInterval = 10;
+    int64_t turn = 0;
+    // argument tables (device), one record per replica, built at prepare
+    DBuf<char> tab_pair, tab_grid, tab_build, tab_p3m, tab_e3b, tab_first, tab_second;
+    int pair_big = 0;
+    int max_n = 0, max_mol = 0, max_cell = 0;
+    size_t max_nk = 0;
+    // P3M: replicas grouped by mesh size; each class owns contiguous pools
+    // that the replicas' FixChargeEwald buffers view, so one batched cuFFT
+    // plan per class transforms every replica of that class
+    struct FFTClass {
+        int3 sz{0, 0, 0};
+        std::vector<int> reps;
+        DBuf<float> rho, e_r;
+        DBuf<float2> rho_k, e_k;
+        cufftHandle r2c = 0, c2r = 0;
+    };
+    std::vector<std::unique_ptr<FFTClass>> fft;
+    std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
+    std::map<std::pair<int, int>, uint64_t> graph_kernels;
+    Batch();
+    ~Batch();
+    int biggest_rep() const;
+    int prepare();
+    int step();
+    int enqueue(int nsteps, bool with_group);
+    int launchGraph(int nsteps, bool with_group);
+    int run(int nturns, double *ms);
+    int runTimed(int nturns, int chunk, size_t flush_bytes, double *ms_total);
+    int checkStatus();
+    void clearGraphs();
+};
+int batch_pair_tables(Batch &b);
+int batch_nlist_tables(Batch &b);
+int batch_mol_tables(Batch &b);
+int batch_e3b_tables(Batch &b);
+int batch_pair_launch(Batch &b, cudaStream_t stream);
+int batch_nlist_rebuild(Batch &b);
+int batch_p3m_prepare(Batch &b);
+int batch_p3m_spread_solve(Batch &b, cudaStream_t stream);
+int batch_p3m_gather(Batch &b, cudaStream_t stream);
+int batch_e3b_list(Batch &b);
+int batch_e3b_forces(Batch &b, cudaStream_t stream);
+int batch_first_half(Batch &b);
+int batch_second_half(Batch &b, bool with_e3b);
+int batch_rigid_maps(Batch &b);
+
 // ---------------------------------------------------------------- kernels
 // neighbour list (nlist.cu)
 int nlist_rebuild(State &s, bool force, bool conditional);
@@ -340,6 +445,11 @@ int e3b_build_list(State &s, FixE3B &f, bool conditional);
 int e3b_forces(State &s, FixE3B &f);
 int e3b_forces_to(State &s, FixE3B &f, float4 *out, bool side, cudaStream_t stream);
 int e3b_energy(State &s, FixE3B &f, double out[2]);
+int e3b_exact_to(State &s, FixE3B &f, float4 *out, int twobody, cudaStream_t stream);
+int e3b_twobody_to(State &s, FixE3B &f, float4 *out, cudaStream_t stream);
+// learned E3B three-body surrogate (surrogate.cu)
+int surrogate_forces_to(State &s, FixE3B &f, float4 *out, cudaStream_t stream);
+int surrogate_compute(State &s, FixE3B &f);
 // rigid + integration (integrate.cu)
 int rigid_update_maps(State &s, FixRigid &r, bool conditional);
 int step_first_half(State &s, bool fused);
@@ -363,4 +473,7 @@ struct mdx_state {
 struct mdx_fix {
     mdx::Fix *f;
     mdx_state *owner;
+};
+struct mdx_batch {
+    mdx::Batch *b;
 };

@@ -18,6 +18,7 @@
 // make_int3((x-lo+h/2)/h), a truncation toward zero, which mis-assigns the
 // stencil of an atom more than h/2 below lo (atoms drift out of the box
 // between list rebuilds); floorf is used here.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <vector>
@@ -58,16 +59,37 @@ __device__ __forceinline__ void stencil(const P3MGeom &g, float4 x, int3 &ng, fl
     d.z = pz / g.h.z - (float)ng.z;
 }
 
-__global__ void k_spread(int n, const float4 *__restrict__ xs, const float *__restrict__ qs, P3MGeom g,
-                         float *__restrict__ rho) {
+// Arguments of the P3M kernels for one system: a0 (single system) or
+// tab[blockIdx.y] (batched replicas; a0 then only sizes the grid).
+struct P3MArgs {
+    int n;
+    const float4 *xs;
+    const float *qs;
+    float4 *fs;
+    P3MGeom g;
+    float *rho;
+    const float2 *rho_k;
+    float2 *e_k;
+    const float *e_r;
+    const float *green;
+    float3 tpl;  // 2 pi / L
+    size_t nk, ngrid;
+    float niv;   // -1 / V
+};
+#define MDX_P3M_ARGS const P3MArgs A = tab ? tab[blockIdx.y] : a0
+
+__global__ void k_spread(const P3MArgs a0, const P3MArgs *__restrict__ tab) {
+    MDX_P3M_ARGS;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float q = qs[i];
+    if (i >= A.n) return;
+    const P3MGeom &g = A.g;
+    float *__restrict__ rho = A.rho;
+    const float q = A.qs[i];
     if (q == 0.f) return;
     const float qi = g.qunit * q;
     int3 ng;
     float3 d;
-    stencil(g, xs[i], ng, d);
+    stencil(g, A.xs[i], ng, d);
     float wx[5], wy[5], wz[5];
     w5(d.x, wx);
     w5(d.y, wy);
@@ -91,10 +113,16 @@ __global__ void k_spread(int n, const float4 *__restrict__ xs, const float *__re
 }
 
 // E_d(k) = i k_d G rho on the half spectrum (z halved), batched output
-__global__ void k_efield(int3 sz, float3 twopi_over_L, const float2 *__restrict__ rho_k,
-                         const float *__restrict__ green, float2 *__restrict__ ek, size_t nk) {
+__global__ void k_efield(const P3MArgs a0, const P3MArgs *__restrict__ tab) {
+    MDX_P3M_ARGS;
+    const size_t nk = A.nk;
     size_t id = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= nk) return;
+    const int3 sz = A.g.sz;
+    const float3 twopi_over_L = A.tpl;
+    const float2 *__restrict__ rho_k = A.rho_k;
+    const float *__restrict__ green = A.green;
+    float2 *__restrict__ ek = A.e_k;
     const int nzh = sz.z / 2 + 1;
     const int iz = (int)(id % nzh);
     const int iy = (int)((id / nzh) % sz.y);
@@ -114,10 +142,17 @@ __global__ void k_efield(int3 sz, float3 twopi_over_L, const float2 *__restrict_
 }
 
 template <bool ACC>
-__global__ void k_gather(int n, const float4 *__restrict__ xs, const float *__restrict__ qs, P3MGeom g,
-                         const float *__restrict__ er, size_t ngrid, float neg_inv_vol, float4 *__restrict__ fs) {
+__global__ void k_gather(const P3MArgs a0, const P3MArgs *__restrict__ tab) {
+    MDX_P3M_ARGS;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= A.n) return;
+    const float4 *__restrict__ xs = A.xs;
+    const float *__restrict__ qs = A.qs;
+    const P3MGeom &g = A.g;
+    const float *__restrict__ er = A.e_r;
+    const size_t ngrid = A.ngrid;
+    const float neg_inv_vol = A.niv;
+    float4 *__restrict__ fs = A.fs;
     const float q = qs[i];
     if (q == 0.f) {
         if (!ACC) {
@@ -208,6 +243,26 @@ P3MGeom geom(State &s, FixChargeEwald &f) {
     g.invh = make_float3(1.f / g.h.x, 1.f / g.h.y, 1.f / g.h.z);
     g.qunit = (float)std::sqrt(s.units.qqr_to_eng);
     return g;
+}
+
+P3MArgs p3m_args(State &s, FixChargeEwald &f) {
+    P3MArgs A{};
+    A.n = s.gpd.n;
+    A.xs = s.gpd.xs.p;
+    A.qs = s.gpd.qs.p;
+    A.fs = s.gpd.fs.p;
+    A.g = geom(s, f);
+    A.rho = f.rho.p;
+    A.rho_k = f.rho_k.p;
+    A.e_k = f.e_k.p;
+    A.e_r = f.e_r.p;
+    A.green = f.green.p;
+    A.tpl = make_float3((float)(6.28318530717958647693 / s.box.Ld.x), (float)(6.28318530717958647693 / s.box.Ld.y),
+                        (float)(6.28318530717958647693 / s.box.Ld.z));
+    A.nk = (size_t)f.sz.x * f.sz.y * (f.sz.z / 2 + 1);
+    A.ngrid = (size_t)f.sz.x * f.sz.y * f.sz.z;
+    A.niv = (float)(-1.0 / (s.box.Ld.x * s.box.Ld.y * s.box.Ld.z));
+    return A;
 }
 
 }  // namespace
@@ -343,8 +398,7 @@ int FixChargeEwald::spread(cudaStream_t st) {
     State &s = *state;
     const size_t ng = (size_t)sz.x * sz.y * sz.z;
     MDX_CUDA_TRY(cudaMemsetAsync(rho.p, 0, ng * sizeof(float), st));
-    P3MGeom g = geom(s, *this);
-    k_spread<<<(s.gpd.n + 127) / 128, 128, 0, st>>>(s.gpd.n, s.gpd.xs.p, s.gpd.qs.p, g, rho.p);
+    k_spread<<<(s.gpd.n + 127) / 128, 128, 0, st>>>(p3m_args(s, *this), nullptr);
     MDX_LAUNCHED();
     return 0;
 }
@@ -358,10 +412,7 @@ int FixChargeEwald::solve(cudaStream_t st) {
         set_error(MDX_ERR_CUDA, "cufftExecR2C failed");
         return MDX_ERR_CUDA;
     }
-    const float3 tpl = make_float3((float)(6.28318530717958647693 / s.box.Ld.x),
-                                   (float)(6.28318530717958647693 / s.box.Ld.y),
-                                   (float)(6.28318530717958647693 / s.box.Ld.z));
-    k_efield<<<(unsigned)((nk + 255) / 256), 256, 0, st>>>(sz, tpl, rho_k.p, green.p, e_k.p, nk);
+    k_efield<<<(unsigned)((nk + 255) / 256), 256, 0, st>>>(p3m_args(s, *this), nullptr);
     MDX_LAUNCHED();
     if (cufftExecC2R(plan_c2r, (cufftComplex *)e_k.p, e_r.p) != CUFFT_SUCCESS) {
         set_error(MDX_ERR_CUDA, "cufftExecC2R failed");
@@ -372,16 +423,11 @@ int FixChargeEwald::solve(cudaStream_t st) {
 
 int FixChargeEwald::gather(bool accumulate, cudaStream_t st) {
     State &s = *state;
-    P3MGeom g = geom(s, *this);
-    const size_t ng = (size_t)sz.x * sz.y * sz.z;
-    const float niv = (float)(-1.0 / (s.box.Ld.x * s.box.Ld.y * s.box.Ld.z));
-    if (accumulate) {
-        k_gather<true><<<(s.gpd.n + 127) / 128, 128, 0, st>>>(s.gpd.n, s.gpd.xs.p, s.gpd.qs.p, g, e_r.p, ng, niv,
-                                                              s.gpd.fs.p);
-    } else {
-        k_gather<false><<<(s.gpd.n + 127) / 128, 128, 0, st>>>(s.gpd.n, s.gpd.xs.p, s.gpd.qs.p, g, e_r.p, ng, niv,
-                                                               s.gpd.fs.p);
-    }
+    const P3MArgs A = p3m_args(s, *this);
+    if (accumulate)
+        k_gather<true><<<(s.gpd.n + 127) / 128, 128, 0, st>>>(A, nullptr);
+    else
+        k_gather<false><<<(s.gpd.n + 127) / 128, 128, 0, st>>>(A, nullptr);
     MDX_LAUNCHED();
     return 0;
 }
@@ -413,6 +459,93 @@ int ewald_recip_energy(State &s, FixChargeEwald &f, double *out) {
     Q2 *= s.units.qqr_to_eng;
     const double V = s.box.Ld.x * s.box.Ld.y * s.box.Ld.z;
     *out = 0.5 * sumG / V - f.alpha / std::sqrt(M_PI) * Q2;
+    return 0;
+}
+
+// ---- batched replicas -------------------------------------------------------
+// Replicas are grouped by mesh size; each class gets contiguous pools that its
+// replicas' buffers view, so a batched cuFFT plan per class covers them all.
+// Spread, E(k) and gather are one launch each for every replica.
+int batch_p3m_prepare(Batch &b) {
+    const int R = (int)b.reps.size();
+    for (int r = 0; r < R; r++) {
+        FixChargeEwald *f = b.reps[r]->ewaldFix();
+        Batch::FFTClass *c = nullptr;
+        for (auto &k : b.fft)
+            if (k->sz.x == f->sz.x && k->sz.y == f->sz.y && k->sz.z == f->sz.z) c = k.get();
+        if (!c) {
+            b.fft.emplace_back(new Batch::FFTClass());
+            c = b.fft.back().get();
+            c->sz = f->sz;
+        }
+        c->reps.push_back(r);
+    }
+    for (auto &cp : b.fft) {
+        Batch::FFTClass &c = *cp;
+        const int K = (int)c.reps.size();
+        const size_t ng = (size_t)c.sz.x * c.sz.y * c.sz.z;
+        const size_t nk = (size_t)c.sz.x * c.sz.y * (c.sz.z / 2 + 1);
+        if (int e = c.rho.alloc(K * ng)) return e;
+        if (int e = c.rho_k.alloc(K * nk)) return e;
+        if (int e = c.e_k.alloc(K * 3 * nk)) return e;
+        if (int e = c.e_r.alloc(K * 3 * ng)) return e;
+        for (int j = 0; j < K; j++) {
+            FixChargeEwald *f = b.reps[c.reps[j]]->ewaldFix();
+            f->rho.view(c.rho.p + j * ng, ng);
+            f->rho_k.view(c.rho_k.p + j * nk, nk);
+            f->e_k.view(c.e_k.p + j * 3 * nk, 3 * nk);
+            f->e_r.view(c.e_r.p + j * 3 * ng, 3 * ng);
+        }
+        int dims[3] = {c.sz.x, c.sz.y, c.sz.z};
+        if (cufftPlanMany(&c.r2c, 3, dims, nullptr, 1, (int)ng, nullptr, 1, (int)nk, CUFFT_R2C, K) != CUFFT_SUCCESS ||
+            cufftPlanMany(&c.c2r, 3, dims, nullptr, 1, (int)nk, nullptr, 1, (int)ng, CUFFT_C2R, 3 * K) !=
+                CUFFT_SUCCESS) {
+            set_error(MDX_ERR_CUDA, "batched cufftPlanMany failed");
+            return MDX_ERR_CUDA;
+        }
+        b.max_nk = std::max(b.max_nk, nk);
+    }
+    std::vector<P3MArgs> h(R);
+    for (int r = 0; r < R; r++) h[r] = p3m_args(*b.reps[r], *b.reps[r]->ewaldFix());
+    if (int e = b.tab_p3m.alloc(R * sizeof(P3MArgs))) return e;
+    MDX_CUDA_TRY(cudaMemcpy(b.tab_p3m.p, h.data(), R * sizeof(P3MArgs), cudaMemcpyHostToDevice));
+    return 0;
+}
+
+int batch_p3m_spread_solve(Batch &b, cudaStream_t st) {
+    const unsigned R = (unsigned)b.reps.size();
+    const P3MArgs *tab = reinterpret_cast<const P3MArgs *>(b.tab_p3m.p);
+    P3MArgs A = p3m_args(*b.reps[0], *b.reps[0]->ewaldFix());  // sizing only
+    A.n = b.max_n;
+    A.nk = b.max_nk;
+    for (auto &c : b.fft) MDX_CUDA_TRY(cudaMemsetAsync(c->rho.p, 0, c->rho.n * sizeof(float), st));
+    k_spread<<<dim3((A.n + 127) / 128, R), 128, 0, st>>>(A, tab);
+    MDX_LAUNCHED();
+    for (auto &c : b.fft) {
+        cufftSetStream(c->r2c, st);
+        if (cufftExecR2C(c->r2c, c->rho.p, (cufftComplex *)c->rho_k.p) != CUFFT_SUCCESS) {
+            set_error(MDX_ERR_CUDA, "batched cufftExecR2C failed");
+            return MDX_ERR_CUDA;
+        }
+    }
+    k_efield<<<dim3((unsigned)((A.nk + 255) / 256), R), 256, 0, st>>>(A, tab);
+    MDX_LAUNCHED();
+    for (auto &c : b.fft) {
+        cufftSetStream(c->c2r, st);
+        if (cufftExecC2R(c->c2r, (cufftComplex *)c->e_k.p, c->e_r.p) != CUFFT_SUCCESS) {
+            set_error(MDX_ERR_CUDA, "batched cufftExecC2R failed");
+            return MDX_ERR_CUDA;
+        }
+    }
+    return 0;
+}
+
+int batch_p3m_gather(Batch &b, cudaStream_t st) {
+    const P3MArgs *tab = reinterpret_cast<const P3MArgs *>(b.tab_p3m.p);
+    P3MArgs A = p3m_args(*b.reps[0], *b.reps[0]->ewaldFix());
+    A.n = b.max_n;
+    k_gather<true><<<dim3((A.n + 127) / 128, (unsigned)b.reps.size()), 128, 0, st>>>(A, tab);
+    MDX_LAUNCHED();
     return 0;
 }
 

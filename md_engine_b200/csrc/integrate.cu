@@ -175,14 +175,40 @@ __device__ __forceinline__ float4 msite(const RigidConsts &rc, const Box &box, c
     return make_float4(m.x, m.y, m.z, w);
 }
 
+int rigid_blocks(int nmol) { return (nmol + 127) / 128; }
+
+// Arguments of the per-molecule kernels for one system: a0 (single system)
+// or tab[blockIdx.y] (batched replicas; a0 then only sizes the grid).
+struct MolArgs {
+    int nmol;
+    const int4 *mol_ids;
+    int4 *mol_idx;
+    const int *idToIdx;
+    float4 *xs, *vs, *fs;
+    RigidConsts rc;
+    Box box;
+    float dt, dtf;
+    NHChain *chain;
+    DeviceStatus *st;
+    double *partials;
+    int part_off, nparts;
+    unsigned int *counter;
+    int nh;
+    double *ke_out;
+    const float4 *fextra;
+    int nblk;  // blocks of k_second_mol that carry this system's molecules
+};
+#define MDX_MOL_ARGS const MolArgs A = tab ? tab[blockIdx.y] : a0
+
 // rebuild-group kernel: molecule -> current atom indices (idToIdx after sort)
-__global__ void k_rigid_maps(int nmol, const int4 *__restrict__ ids, const int *__restrict__ idToIdx,
-                             int4 *__restrict__ idx, const DeviceStatus *st, int conditional) {
-    if (conditional && !st->rebuild) return;
+__global__ void k_rigid_maps(const MolArgs a0, const MolArgs *__restrict__ tab, int conditional) {
+    MDX_MOL_ARGS;
+    if (conditional && !A.st->rebuild) return;
     int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= nmol) return;
-    int4 a = ids[m];
-    idx[m] = make_int4(idToIdx[a.x], idToIdx[a.y], idToIdx[a.z], a.w >= 0 ? idToIdx[a.w] : -1);
+    if (m >= A.nmol) return;
+    const int *__restrict__ idToIdx = A.idToIdx;
+    int4 a = A.mol_ids[m];
+    A.mol_idx[m] = make_int4(idToIdx[a.x], idToIdx[a.y], idToIdx[a.z], a.w >= 0 ? idToIdx[a.w] : -1);
 }
 
 // ---- first half ---------------------------------------------------------
@@ -219,11 +245,19 @@ __global__ void k_first_atoms(int n, float4 *__restrict__ xs, float4 *__restrict
 
 // per-molecule fused: NH rescale + save_prev_val + nve_v + nve_x + SETTLE + M-site
 template <bool NH>
-__global__ void k_first_mol(int nmol, const int4 *__restrict__ mol_idx, float4 *__restrict__ xs,
-                            float4 *__restrict__ vs, float4 *__restrict__ fs, RigidConsts rc, Box box, float dt,
-                            float dtf, const NHChain *__restrict__ chain, DeviceStatus *st) {
+__global__ void k_first_mol(const MolArgs a0, const MolArgs *__restrict__ tab) {
+    MDX_MOL_ARGS;
     int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= nmol) return;
+    if (m >= A.nmol) return;
+    const int4 *__restrict__ mol_idx = A.mol_idx;
+    float4 *__restrict__ xs = A.xs;
+    float4 *__restrict__ vs = A.vs;
+    float4 *__restrict__ fs = A.fs;
+    const RigidConsts &rc = A.rc;
+    const Box &box = A.box;
+    const float dt = A.dt, dtf = A.dtf;
+    const NHChain *__restrict__ chain = A.chain;
+    DeviceStatus *st = A.st;
     const int4 ix = mol_idx[m];
     const int id3[3] = {ix.x, ix.y, ix.z};
     float4 x0[3], x[3], v[3];
@@ -275,12 +309,12 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
 // Nose-Hoover stepFinal + next stepInit on one thread, and the turn counter.
 // nparts partials are summed; the counter target is this kernel's grid size
 __device__ void finish_step(double *partials, int nparts, unsigned int *counter, NHChain *chain, int nh,
-                            DeviceStatus *st, double *ke_out) {
+                            DeviceStatus *st, double *ke_out, unsigned int nblk) {
     __shared__ bool last;
     __threadfence();
     if (threadIdx.x == 0) {
         unsigned int prev = atomicAdd(counter, 1u);
-        last = (prev == gridDim.x - 1u);
+        last = (prev == nblk - 1u);
     }
     __syncthreads();
     if (!last) return;
@@ -325,19 +359,27 @@ __global__ void k_second_atoms(int n, float4 *__restrict__ vs, const float4 *__r
     }
     const double b = block_sum(mv2, sh);
     if (threadIdx.x == 0) partials[part_off + blockIdx.x] = b;
-    if (do_finish) finish_step(partials, nparts, counter, chain, nh, st, ke_out);
+    if (do_finish) finish_step(partials, nparts, counter, chain, nh, st, ke_out, gridDim.x);
 }
 
 // per-molecule fused: postForce + distributeMSite + settleVelocities +
 // validateConstraints + m v^2 partials (+ last-block NH / turn)
 // fextra (may be null): per-molecule-atom forces computed beside the pair
 // kernel (E3B), indexed like fs, merged into O/H1/H2 here
-__global__ void k_second_mol(int nmol, const int4 *__restrict__ mol_idx, const float4 *__restrict__ xs,
-                             float4 *__restrict__ vs, float4 *__restrict__ fs, RigidConsts rc, Box box, float dtf,
-                             double *__restrict__ partials, int part_off, int nparts, unsigned int *counter,
-                             NHChain *chain, int nh, DeviceStatus *st, double *ke_out,
-                             const float4 *__restrict__ fextra) {
+__global__ void k_second_mol(const MolArgs a0, const MolArgs *__restrict__ tab) {
+    MDX_MOL_ARGS;
+    if ((int)blockIdx.x >= A.nblk) return;  // the whole block: not counted
     __shared__ double sh[32];
+    const int nmol = A.nmol;
+    const int4 *__restrict__ mol_idx = A.mol_idx;
+    const float4 *__restrict__ xs = A.xs;
+    float4 *__restrict__ vs = A.vs;
+    float4 *__restrict__ fs = A.fs;
+    const RigidConsts &rc = A.rc;
+    const Box &box = A.box;
+    const float dtf = A.dtf;
+    DeviceStatus *st = A.st;
+    const float4 *__restrict__ fextra = A.fextra;
     int m = blockIdx.x * blockDim.x + threadIdx.x;
     double mv2 = 0.0;
     if (m < nmol) {
@@ -390,8 +432,8 @@ __global__ void k_second_mol(int nmol, const int4 *__restrict__ mol_idx, const f
         }
     }
     const double b = block_sum(mv2, sh);
-    if (threadIdx.x == 0) partials[part_off + blockIdx.x] = b;
-    finish_step(partials, nparts, counter, chain, nh, st, ke_out);
+    if (threadIdx.x == 0) A.partials[A.part_off + blockIdx.x] = b;
+    finish_step(A.partials, A.nparts, A.counter, A.chain, A.nh, st, A.ke_out, (unsigned int)A.nblk);
 }
 
 // ---- stand-alone hooks (one kernel per reference hook) ------------------
@@ -597,15 +639,39 @@ __global__ void k_nh_end_of_run_fix(NHChain *chain) {
     chain[1].scale = 1.0;
 }
 
-int rigid_blocks(int nmol) { return (nmol + 127) / 128; }
-
 }  // namespace
+
+MolArgs mol_args(State &s, FixRigid &r) {
+    MolArgs A{};
+    FixNoseHoover *nh = s.nhFix();
+    A.nmol = (int)r.mol_ids.size();
+    A.mol_ids = r.d_mol_ids.p;
+    A.mol_idx = r.d_mol_idx.p;
+    A.idToIdx = s.gpd.idToIdx.p;
+    A.xs = s.gpd.xs.p;
+    A.vs = s.gpd.vs.p;
+    A.fs = s.gpd.fs.p;
+    A.rc = r.rc;
+    A.box = s.box;
+    A.dt = (float)s.dt;
+    A.dtf = (float)(0.5 * s.dt * s.units.ftm_to_v);
+    A.chain = nh ? nh->d_chain.p : nullptr;
+    A.st = s.d_status.p;
+    A.partials = s.red_partials.p;
+    A.part_off = 0;
+    A.nparts = rigid_blocks(A.nmol);
+    A.counter = s.red_counter.p;
+    A.nh = nh ? 1 : 0;
+    A.ke_out = s.red_out.p;
+    A.fextra = nullptr;
+    A.nblk = rigid_blocks(A.nmol);
+    return A;
+}
 
 int rigid_update_maps(State &s, FixRigid &r, bool conditional) {
     const int nmol = (int)r.mol_ids.size();
     if (nmol == 0 || !r.d_mol_ids.p) return 0;
-    k_rigid_maps<<<(nmol + 255) / 256, 256, 0, s.stream>>>(nmol, r.d_mol_ids.p, s.gpd.idToIdx.p, r.d_mol_idx.p,
-                                                          s.d_status.p, conditional ? 1 : 0);
+    k_rigid_maps<<<(nmol + 255) / 256, 256, 0, s.stream>>>(mol_args(s, r), nullptr, conditional ? 1 : 0);
     MDX_LAUNCHED();
     return 0;
 }
@@ -674,15 +740,11 @@ int step_first_half(State &s, bool fused) {
         MDX_LAUNCHED();
     }
     if (r) {
-        const int nmol = (int)r->mol_ids.size();
+        const MolArgs A = mol_args(s, *r);
         if (nh)
-            k_first_mol<true><<<rigid_blocks(nmol), 128, 0, s.stream>>>(nmol, r->d_mol_idx.p, s.gpd.xs.p, s.gpd.vs.p,
-                                                                       s.gpd.fs.p, r->rc, s.box, dt, dtf, chain,
-                                                                       s.d_status.p);
+            k_first_mol<true><<<rigid_blocks(A.nmol), 128, 0, s.stream>>>(A, nullptr);
         else
-            k_first_mol<false><<<rigid_blocks(nmol), 128, 0, s.stream>>>(nmol, r->d_mol_idx.p, s.gpd.xs.p,
-                                                                        s.gpd.vs.p, s.gpd.fs.p, r->rc, s.box, dt,
-                                                                        dtf, chain, s.d_status.p);
+            k_first_mol<false><<<rigid_blocks(A.nmol), 128, 0, s.stream>>>(A, nullptr);
         MDX_LAUNCHED();
     }
     return 0;
@@ -726,10 +788,11 @@ int step_second_half(State &s, bool fused, const float4 *fextra) {
         MDX_LAUNCHED();
     }
     if (r) {
-        const int nmol = (int)r->mol_ids.size();
-        k_second_mol<<<mb, 128, 0, s.stream>>>(nmol, r->d_mol_idx.p, s.gpd.xs.p, s.gpd.vs.p, s.gpd.fs.p, r->rc,
-                                               s.box, dtf, s.red_partials.p, free_atoms ? ab : 0, nparts,
-                                               s.red_counter.p, chain, nh ? 1 : 0, s.d_status.p, s.red_out.p, fextra);
+        MolArgs A = mol_args(s, *r);
+        A.part_off = free_atoms ? ab : 0;
+        A.nparts = nparts;
+        A.fextra = fextra;
+        k_second_mol<<<mb, 128, 0, s.stream>>>(A, nullptr);
         MDX_LAUNCHED();
     }
     return 0;
@@ -872,6 +935,65 @@ int nh_end_of_run(State &s) {
 int zero_forces(State &s) {
     const int n = s.gpd.n;
     k_zero_f<<<(n + 255) / 256, 256, 0, s.stream>>>(n, s.gpd.fs.p, s.gpd.virials.p);
+    MDX_LAUNCHED();
+    return 0;
+}
+
+// ---- batched replicas: one launch per phase, blockIdx.y = replica ----------
+int batch_mol_tables(Batch &b) {
+    const int R = (int)b.reps.size();
+    std::vector<MolArgs> h1(R), h2(R);
+    for (int r = 0; r < R; r++) {
+        State &s = *b.reps[r];
+        FixRigid *fr = s.rigidFix();
+        h1[r] = mol_args(s, *fr);
+        h2[r] = h1[r];
+        FixE3B *e3 = s.e3bFix();
+        h2[r].fextra = (e3 && e3->side_ok) ? e3->f_side.p : nullptr;
+    }
+    if (int e = b.tab_first.alloc(R * sizeof(MolArgs))) return e;
+    if (int e = b.tab_second.alloc(R * sizeof(MolArgs))) return e;
+    MDX_CUDA_TRY(cudaMemcpy(b.tab_first.p, h1.data(), R * sizeof(MolArgs), cudaMemcpyHostToDevice));
+    MDX_CUDA_TRY(cudaMemcpy(b.tab_second.p, h2.data(), R * sizeof(MolArgs), cudaMemcpyHostToDevice));
+    return 0;
+}
+
+static int batch_sizing(Batch &b, MolArgs *out) {
+    if (!b.tab_first.p) {
+        set_error(MDX_ERR_STATE, "batch tables not built (prepare the batch)");
+        return MDX_ERR_STATE;
+    }
+    State &s0 = *b.reps[0];
+    MolArgs A = mol_args(s0, *s0.rigidFix());
+    A.nmol = b.max_mol;
+    A.nblk = rigid_blocks(b.max_mol);
+    *out = A;
+    return 0;
+}
+
+int batch_rigid_maps(Batch &b) {
+    MolArgs A;
+    if (int e = batch_sizing(b, &A)) return e;
+    k_rigid_maps<<<dim3((A.nmol + 255) / 256, (unsigned)b.reps.size()), 256, 0, b.stream>>>(
+        A, reinterpret_cast<const MolArgs *>(b.tab_first.p), 1);
+    MDX_LAUNCHED();
+    return 0;
+}
+
+int batch_first_half(Batch &b) {
+    MolArgs A;
+    if (int e = batch_sizing(b, &A)) return e;
+    k_first_mol<true><<<dim3(A.nblk, (unsigned)b.reps.size()), 128, 0, b.stream>>>(
+        A, reinterpret_cast<const MolArgs *>(b.tab_first.p));
+    MDX_LAUNCHED();
+    return 0;
+}
+
+int batch_second_half(Batch &b, bool with_e3b) {
+    MolArgs A;
+    if (int e = batch_sizing(b, &A)) return e;
+    k_second_mol<<<dim3(A.nblk, (unsigned)b.reps.size()), 128, 0, b.stream>>>(
+        A, reinterpret_cast<const MolArgs *>(with_e3b ? b.tab_second.p : b.tab_first.p));
     MDX_LAUNCHED();
     return 0;
 }

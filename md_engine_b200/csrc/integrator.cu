@@ -80,7 +80,11 @@ class IntegratorVerlet {
         }
         if (e3side) {
             MDX_CUDA_TRY(cudaStreamWaitEvent(s->side[1], s->ev_fork, 0));
-            if (int e = e3b_forces_to(*s, *e3, e3->f_side.p, true, s->side[1])) return e;
+            if (e3->sur && e3->sur->enabled) {
+                if (int e = surrogate_forces_to(*s, *e3, e3->f_side.p, s->side[1])) return e;
+            } else {
+                if (int e = e3b_forces_to(*s, *e3, e3->f_side.p, true, s->side[1])) return e;
+            }
             MDX_CUDA_TRY(cudaEventRecord(s->ev_join[1], s->side[1]));
         }
         if (pf)

@@ -48,34 +48,59 @@ __device__ __forceinline__ int cell_of_pos(const CellGrid &g, float3 p) {
     return (cx * g.ns.y + cy) * g.ns.z + cz;
 }
 
+// Arguments of the rebuild-group kernels for one system.  Every kernel takes
+// a0 (single system) and tab (batched replicas: tab[blockIdx.y], a0 is then
+// only the largest replica used to size the grid).
+struct GridArgs {
+    float4 *xs, *vs, *fs;
+    float *qs;
+    uint32_t *ids;
+    float4 *xs2, *vs2, *fs2;
+    float *qs2;
+    uint32_t *ids2;
+    const float4 *xs_last;
+    int *idToIdx;
+    int *cell_of;
+    uint32_t *cell_count, *cell_start, *cell_fill;
+    int *perm_tmp, *perm;
+    DeviceStatus *st;
+    Box box;
+    CellGrid g;
+    int n, ncell, interval;
+    float skin2q;
+};
+#define MDX_GRID_ARGS const GridArgs A = tab ? tab[blockIdx.y] : a0
+
 // setBuildFlag (GridGPU.cu:755-774) + the periodicInterval gate of
 // IntegratorVerlet.cu:696: rebuild iff forced, or turn % interval == 0 and
 // any atom moved more than skin/2 since the last build.
-__global__ void k_check(const float4 *__restrict__ xs, const float4 *__restrict__ xs_last, int n, Box box,
-                        float skin2_quarter, int interval, int force, DeviceStatus *st) {
+__global__ void k_check(const GridArgs a0, const GridArgs *__restrict__ tab, int force) {
+    MDX_GRID_ARGS;
+    DeviceStatus *st = A.st;
     if (!force) {
         long long t = st->turn;
-        if (interval <= 0 || (t % interval) != 0) return;
+        if (A.interval <= 0 || (t % A.interval) != 0) return;
     } else {
         if (blockIdx.x == 0 && threadIdx.x == 0) st->rebuild = 1u;
         return;
     }
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int moved = 0;
-    if (i < n) {
-        float3 d = min_image(box, f3(xs[i]) - f3(xs_last[i]));
-        moved = dot3(d, d) > skin2_quarter;
+    if (i < A.n) {
+        float3 d = min_image(A.box, f3(A.xs[i]) - f3(A.xs_last[i]));
+        moved = dot3(d, d) > A.skin2q;
     }
     if (__syncthreads_or(moved) && threadIdx.x == 0) atomicOr(&st->rebuild, 1u);
 }
 
 // periodicWrap (GridGPU.cu:138-161) + countNumInGridCells (GridGPU.cu:190-203)
-__global__ void k_wrap_bin(float4 *__restrict__ xs, int n, Box box, CellGrid g, int *__restrict__ cell_of,
-                           uint32_t *__restrict__ cell_count, const DeviceStatus *st) {
-    if (!st->rebuild) return;
+__global__ void k_wrap_bin(const GridArgs a0, const GridArgs *__restrict__ tab) {
+    MDX_GRID_ARGS;
+    if (!A.st->rebuild) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    float4 p = xs[i];
+    if (i >= A.n) return;
+    const Box &box = A.box;
+    float4 p = A.xs[i];
     float ix = floorf((p.x - box.lo.x) / box.L.x);
     float iy = floorf((p.y - box.lo.y) / box.L.y);
     float iz = floorf((p.z - box.lo.z) / box.L.z);
@@ -83,18 +108,22 @@ __global__ void k_wrap_bin(float4 *__restrict__ xs, int n, Box box, CellGrid g, 
         p.x = p.x - box.L.x * ix;
         p.y = p.y - box.L.y * iy;
         p.z = p.z - box.L.z * iz;
-        xs[i] = p;
+        A.xs[i] = p;
     }
-    int c = cell_of_pos(g, f3(p));
-    cell_of[i] = c;
-    atomicAdd(cell_count + c, 1u);
+    int c = cell_of_pos(A.g, f3(p));
+    A.cell_of[i] = c;
+    atomicAdd(A.cell_count + c, 1u);
 }
 
-// exclusive scan of the cell histogram in one block (replaces the host
-// cumulativeSum, helpers.h:15-24); also clears the fill counters
-__global__ void k_scan_cells(const uint32_t *__restrict__ count, uint32_t *__restrict__ start,
-                             uint32_t *__restrict__ fill, int ncell, const DeviceStatus *st) {
-    if (!st->rebuild) return;
+// exclusive scan of the cell histogram in one block per system (replaces the
+// host cumulativeSum, helpers.h:15-24); also clears the fill counters
+__global__ void k_scan_cells(const GridArgs a0, const GridArgs *__restrict__ tab) {
+    MDX_GRID_ARGS;
+    if (!A.st->rebuild) return;
+    const uint32_t *__restrict__ count = A.cell_count;
+    uint32_t *__restrict__ start = A.cell_start;
+    uint32_t *__restrict__ fill = A.cell_fill;
+    const int ncell = A.ncell;
     __shared__ uint32_t warp_tot[32];
     __shared__ uint32_t carry;
     if (threadIdx.x == 0) carry = 0;
@@ -131,25 +160,27 @@ __global__ void k_scan_cells(const uint32_t *__restrict__ count, uint32_t *__res
     if (threadIdx.x == 0) start[ncell] = carry;
 }
 
-__global__ void k_scatter(const int *__restrict__ cell_of, const uint32_t *__restrict__ start,
-                          uint32_t *__restrict__ fill, int *__restrict__ perm_tmp, int n, const DeviceStatus *st) {
-    if (!st->rebuild) return;
+__global__ void k_scatter(const GridArgs a0, const GridArgs *__restrict__ tab) {
+    MDX_GRID_ARGS;
+    if (!A.st->rebuild) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    int c = cell_of[i];
-    uint32_t slot = atomicAdd(fill + c, 1u);
-    perm_tmp[start[c] + slot] = i;
+    if (i >= A.n) return;
+    int c = A.cell_of[i];
+    uint32_t slot = atomicAdd(A.cell_fill + c, 1u);
+    A.perm_tmp[A.cell_start[c] + slot] = i;
 }
 
 // deterministic order inside each cell: rank by (type, id); one warp per cell
-__global__ void k_rank(const uint32_t *__restrict__ start, const int *__restrict__ perm_tmp,
-                       const float4 *__restrict__ xs, const uint32_t *__restrict__ ids, int *__restrict__ perm,
-                       int ncell, const DeviceStatus *st) {
-    if (!st->rebuild) return;
+__global__ void k_rank(const GridArgs a0, const GridArgs *__restrict__ tab) {
+    MDX_GRID_ARGS;
+    if (!A.st->rebuild) return;
     int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
-    if (c >= ncell) return;
-    uint32_t s = start[c], e = start[c + 1];
+    if (c >= A.ncell) return;
+    const int *__restrict__ perm_tmp = A.perm_tmp;
+    const float4 *__restrict__ xs = A.xs;
+    const uint32_t *__restrict__ ids = A.ids;
+    uint32_t s = A.cell_start[c], e = A.cell_start[c + 1];
     for (uint32_t p = s + lane; p < e; p += 32) {
         int a = perm_tmp[p];
         unsigned long long ka = ((unsigned long long)(uint32_t)type_of(xs[a]) << 32) | ids[a];
@@ -159,28 +190,25 @@ __global__ void k_rank(const uint32_t *__restrict__ start, const int *__restrict
             unsigned long long kb = ((unsigned long long)(uint32_t)type_of(xs[b]) << 32) | ids[b];
             r += kb < ka;
         }
-        perm[s + r] = a;
+        A.perm[s + r] = a;
     }
 }
 
 // sortPerAtomArrays (GridGPU.cu:253-293): gather every stream into the
 // alternate buffers and rebuild idToIdx
-__global__ void k_gather(const int *__restrict__ perm, int n, const float4 *__restrict__ xs,
-                         const float4 *__restrict__ vs, const float4 *__restrict__ fs, const float *__restrict__ qs,
-                         const uint32_t *__restrict__ ids, float4 *__restrict__ xs2, float4 *__restrict__ vs2,
-                         float4 *__restrict__ fs2, float *__restrict__ qs2, uint32_t *__restrict__ ids2,
-                         int *__restrict__ idToIdx, const DeviceStatus *st) {
-    if (!st->rebuild) return;
+__global__ void k_gather(const GridArgs a0, const GridArgs *__restrict__ tab) {
+    MDX_GRID_ARGS;
+    if (!A.st->rebuild) return;
     int d = blockIdx.x * blockDim.x + threadIdx.x;
-    if (d >= n) return;
-    int s = perm[d];
-    xs2[d] = xs[s];
-    vs2[d] = vs[s];
-    fs2[d] = fs[s];
-    qs2[d] = qs[s];
-    uint32_t id = ids[s];
-    ids2[d] = id;
-    idToIdx[id] = d;
+    if (d >= A.n) return;
+    int s = A.perm[d];
+    A.xs2[d] = A.xs[s];
+    A.vs2[d] = A.vs[s];
+    A.fs2[d] = A.fs[s];
+    A.qs2[d] = A.qs[s];
+    uint32_t id = A.ids[s];
+    A.ids2[d] = id;
+    A.idToIdx[id] = d;
 }
 
 // assignNeighbors / assignFromCell (GridGPU.cu:482-734) with the exclusion
@@ -224,8 +252,11 @@ struct BuildArgs {
 };
 
 template <int TP, bool COUNT>
-__global__ void __launch_bounds__(kBuildWarps * 32, 3) k_build_cells(const BuildArgs A) {
+__global__ void __launch_bounds__(kBuildWarps * 32, 3) k_build_cells(const BuildArgs a0,
+                                                                       const BuildArgs *__restrict__ tab) {
+    const BuildArgs A = tab ? tab[blockIdx.y] : a0;
     if (!COUNT && !A.st->rebuild) return;
+    if ((int)blockIdx.x >= A.ncell) return;
     constexpr int GP = 32 / TP;
     __shared__ float4 sh_x[kBuildWarps][32];
     __shared__ uint2 sh_it[kBuildWarps][32];
@@ -415,9 +446,11 @@ __global__ void __launch_bounds__(kBuildWarps * 32, 3) k_build_cells(const Build
 }
 
 // single block: every thread must read the flag before it is cleared
-__global__ void k_finish(uint32_t *__restrict__ cell_count, int ncell, DeviceStatus *st) {
+__global__ void k_finish(const GridArgs a0, const GridArgs *__restrict__ tab) {
+    MDX_GRID_ARGS;
+    DeviceStatus *st = A.st;
     if (!st->rebuild) return;
-    for (int c = threadIdx.x; c < ncell; c += blockDim.x) cell_count[c] = 0u;
+    for (int c = threadIdx.x; c < A.ncell; c += blockDim.x) A.cell_count[c] = 0u;
     __syncthreads();
     if (threadIdx.x == 0) {
         st->n_builds += 1;
@@ -432,6 +465,38 @@ CellGrid make_grid(const State &s) {
     g.inv_ds = make_float3((float)(s.grid.ns.x / s.box.Ld.x), (float)(s.grid.ns.y / s.box.Ld.y),
                            (float)(s.grid.ns.z / s.box.Ld.z));
     return g;
+}
+
+GridArgs grid_args(State &s) {
+    GridGPU &gr = s.grid;
+    GPUData &d = s.gpd;
+    GridArgs A{};
+    A.xs = d.xs.p;
+    A.vs = d.vs.p;
+    A.fs = d.fs.p;
+    A.qs = d.qs.p;
+    A.ids = d.ids.p;
+    A.xs2 = d.xs_alt.p;
+    A.vs2 = d.vs_alt.p;
+    A.fs2 = d.fs_alt.p;
+    A.qs2 = d.qs_alt.p;
+    A.ids2 = d.ids_alt.p;
+    A.xs_last = d.xs_last_build.p;
+    A.idToIdx = d.idToIdx.p;
+    A.cell_of = gr.cell_of.p;
+    A.cell_count = gr.cell_count.p;
+    A.cell_start = gr.cell_start.p;
+    A.cell_fill = gr.cell_fill.p;
+    A.perm_tmp = gr.perm_tmp.p;
+    A.perm = gr.perm.p;
+    A.st = s.d_status.p;
+    A.box = s.box;
+    A.g = make_grid(s);
+    A.n = d.n;
+    A.ncell = gr.ns.x * gr.ns.y * gr.ns.z;
+    A.interval = s.periodicInterval;
+    A.skin2q = (float)(s.padding * s.padding) * 0.25f;
+    return A;
 }
 
 BuildArgs build_args(State &s, const CellGrid &g, float cutsq) {
@@ -473,7 +538,7 @@ BuildArgs build_args(State &s, const CellGrid &g, float cutsq) {
 template <int T>
 void launch_build(State &s, const CellGrid &g, float cutsq) {
     const BuildArgs A = build_args(s, g, cutsq);
-    k_build_cells<T, false><<<A.ncell, kBuildWarps * 32, 0, s.stream>>>(A);
+    k_build_cells<T, false><<<A.ncell, kBuildWarps * 32, 0, s.stream>>>(A, nullptr);
     MDX_LAUNCHED();
 }
 
@@ -484,7 +549,7 @@ void launch_count(State &s, const CellGrid &g, float cutsq) {
     A.ljmask = nullptr;
     A.part_q = 0;
     A.cap = 0;
-    k_build_cells<T, true><<<A.ncell, kBuildWarps * 32, 0, s.stream>>>(A);
+    k_build_cells<T, true><<<A.ncell, kBuildWarps * 32, 0, s.stream>>>(A, nullptr);
     MDX_LAUNCHED();
 }
 
@@ -585,6 +650,15 @@ int nlist_init(State &s) {
     GridGPU &gr = s.grid;
     gr.cut = (float)((double)(float)s.maxRCut() + s.padding);
     gr.skin = (float)s.padding;
+    // minimum image: one periodic image of a pair at most can lie within cut
+    if (2.0 * (double)gr.cut >= std::min(s.box.Ld.x, std::min(s.box.Ld.y, s.box.Ld.z))) {
+        set_error(MDX_ERR_UNSUPPORTED, "neighbour cutoff %g (rCut + padding) must be below half the box (%g %g %g)",
+                  (double)gr.cut, s.box.Ld.x, s.box.Ld.y, s.box.Ld.z);
+        return MDX_ERR_UNSUPPORTED;
+    }
+    // cells of at least cut/m; m = 2 needs 4 cells per side (a 5-cell stencil
+    // row on a 4-cell ring visits one cell under two images, of which at most
+    // one is within cut < L/2), m = 1 needs 3
     int m = 2;
     int3 ns;
     for (;; m--) {
@@ -595,7 +669,8 @@ int nlist_init(State &s) {
         }
         double w = (double)gr.cut / m * (1.0 + 1e-5);
         ns = make_int3((int)(s.box.Ld.x / w), (int)(s.box.Ld.y / w), (int)(s.box.Ld.z / w));
-        if (ns.x >= 2 * m + 1 && ns.y >= 2 * m + 1 && ns.z >= 2 * m + 1) break;
+        const int need = m == 2 ? 4 : 3;
+        if (ns.x >= need && ns.y >= need && ns.z >= need) break;
     }
     gr.m = m;
     gr.ns = ns;
@@ -635,24 +710,20 @@ int nlist_rebuild(State &s, bool force, bool conditional) {
     const int ncell = gr.ns.x * gr.ns.y * gr.ns.z;
     const CellGrid g = make_grid(s);
     const float cutsq = gr.cut * gr.cut;
-    const float skin2q = (float)(s.padding * s.padding) * 0.25f;
     (void)conditional;
-    k_check<<<(n + 255) / 256, 256, 0, s.stream>>>(d.xs.p, d.xs_last_build.p, n, s.box, skin2q, s.periodicInterval,
-                                                   force ? 1 : 0, s.d_status.p);
+    const GridArgs A = grid_args(s);
+    const int nb = (n + 255) / 256;
+    k_check<<<nb, 256, 0, s.stream>>>(A, nullptr, force ? 1 : 0);
     MDX_LAUNCHED();
-    k_wrap_bin<<<(n + 255) / 256, 256, 0, s.stream>>>(d.xs.p, n, s.box, g, gr.cell_of.p, gr.cell_count.p, s.d_status.p);
+    k_wrap_bin<<<nb, 256, 0, s.stream>>>(A, nullptr);
     MDX_LAUNCHED();
-    k_scan_cells<<<1, 1024, 0, s.stream>>>(gr.cell_count.p, gr.cell_start.p, gr.cell_fill.p, ncell, s.d_status.p);
+    k_scan_cells<<<1, 1024, 0, s.stream>>>(A, nullptr);
     MDX_LAUNCHED();
-    k_scatter<<<(n + 255) / 256, 256, 0, s.stream>>>(gr.cell_of.p, gr.cell_start.p, gr.cell_fill.p, gr.perm_tmp.p, n,
-                                                     s.d_status.p);
+    k_scatter<<<nb, 256, 0, s.stream>>>(A, nullptr);
     MDX_LAUNCHED();
-    k_rank<<<(ncell * 32 + 255) / 256, 256, 0, s.stream>>>(gr.cell_start.p, gr.perm_tmp.p, d.xs.p, d.ids.p, gr.perm.p,
-                                                           ncell, s.d_status.p);
+    k_rank<<<(ncell * 32 + 255) / 256, 256, 0, s.stream>>>(A, nullptr);
     MDX_LAUNCHED();
-    k_gather<<<(n + 255) / 256, 256, 0, s.stream>>>(gr.perm.p, n, d.xs.p, d.vs.p, d.fs.p, d.qs.p, d.ids.p, d.xs_alt.p,
-                                                    d.vs_alt.p, d.fs_alt.p, d.qs_alt.p, d.ids_alt.p, d.idToIdx.p,
-                                                    s.d_status.p);
+    k_gather<<<nb, 256, 0, s.stream>>>(A, nullptr);
     MDX_LAUNCHED();
     if (gr.cap == 0) {
         // first build: size the per-atom capacity from a counting sweep
@@ -690,9 +761,69 @@ int nlist_rebuild(State &s, bool force, bool conditional) {
     if (FixE3B *e3 = s.e3bFix()) {
         if (int e = e3b_build_list(s, *e3, true)) return e;
     }
-    k_finish<<<1, 1024, 0, s.stream>>>(gr.cell_count.p, ncell, s.d_status.p);
+    k_finish<<<1, 1024, 0, s.stream>>>(A, nullptr);
     MDX_LAUNCHED();
     gr.built = true;
+    return 0;
+}
+
+// batched replicas: the same group, one launch per kernel for all replicas
+// (blockIdx.y = replica); every kernel returns at once for a replica whose
+// skin check did not fire.  Tables are built at prepare, before any capture.
+int batch_nlist_tables(Batch &b) {
+    const int R = (int)b.reps.size();
+    std::vector<GridArgs> hg(R);
+    std::vector<BuildArgs> hb(R);
+    for (int r = 0; r < R; r++) {
+        State &s = *b.reps[r];
+        hg[r] = grid_args(s);
+        hb[r] = build_args(s, make_grid(s), s.grid.cut * s.grid.cut);
+    }
+    if (int e = b.tab_grid.alloc(R * sizeof(GridArgs))) return e;
+    if (int e = b.tab_build.alloc(R * sizeof(BuildArgs))) return e;
+    MDX_CUDA_TRY(cudaMemcpy(b.tab_grid.p, hg.data(), R * sizeof(GridArgs), cudaMemcpyHostToDevice));
+    MDX_CUDA_TRY(cudaMemcpy(b.tab_build.p, hb.data(), R * sizeof(BuildArgs), cudaMemcpyHostToDevice));
+    return 0;
+}
+
+int batch_nlist_rebuild(Batch &b) {
+    const int R = (int)b.reps.size();
+    if (!b.tab_grid.p) {
+        set_error(MDX_ERR_STATE, "batch tables not built (prepare the batch)");
+        return MDX_ERR_STATE;
+    }
+    const GridArgs *tg = reinterpret_cast<const GridArgs *>(b.tab_grid.p);
+    const BuildArgs *tb = reinterpret_cast<const BuildArgs *>(b.tab_build.p);
+    State &s0 = *b.reps[0];
+    GridArgs A = grid_args(s0);  // sizing only: the kernels read tab
+    A.n = b.max_n;
+    A.ncell = b.max_cell;
+    BuildArgs B = build_args(s0, make_grid(s0), s0.grid.cut * s0.grid.cut);
+    B.ncell = b.max_cell;
+    const dim3 nb((b.max_n + 255) / 256, R);
+    cudaStream_t st = b.stream;
+    k_check<<<nb, 256, 0, st>>>(A, tg, 0);
+    k_wrap_bin<<<nb, 256, 0, st>>>(A, tg);
+    k_scan_cells<<<dim3(1, R), 1024, 0, st>>>(A, tg);
+    k_scatter<<<nb, 256, 0, st>>>(A, tg);
+    k_rank<<<dim3((b.max_cell * 32 + 255) / 256, R), 256, 0, st>>>(A, tg);
+    k_gather<<<nb, 256, 0, st>>>(A, tg);
+    const dim3 cb(b.max_cell, R);
+    switch (s0.grid.team) {
+        case 1: k_build_cells<1, false><<<cb, kBuildWarps * 32, 0, st>>>(B, tb); break;
+        case 2: k_build_cells<2, false><<<cb, kBuildWarps * 32, 0, st>>>(B, tb); break;
+        case 4: k_build_cells<4, false><<<cb, kBuildWarps * 32, 0, st>>>(B, tb); break;
+        case 8: k_build_cells<8, false><<<cb, kBuildWarps * 32, 0, st>>>(B, tb); break;
+        case 16: k_build_cells<16, false><<<cb, kBuildWarps * 32, 0, st>>>(B, tb); break;
+        default: k_build_cells<32, false><<<cb, kBuildWarps * 32, 0, st>>>(B, tb); break;
+    }
+    g_launches += 7;
+    if (int e = batch_rigid_maps(b)) return e;
+    if (s0.e3bFix())
+        if (int e = batch_e3b_list(b)) return e;
+    k_finish<<<dim3(1, R), 1024, 0, st>>>(A, tg);
+    MDX_LAUNCHED();
+    MDX_CUDA_TRY(cudaGetLastError());
     return 0;
 }
 

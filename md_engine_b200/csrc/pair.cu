@@ -115,8 +115,11 @@ __device__ __forceinline__ bool pair_term(const PairArgs &A, const float *sp, in
     return any;
 }
 
+// tab: one argument record per replica (batched launch, blockIdx.y = replica)
+// or null (single system, a0)
 template <int T, int LJ, bool EW, bool VIR, bool ENERGY>
-__global__ void __launch_bounds__(256) k_pair(PairArgs A, int accumulate) {
+__global__ void __launch_bounds__(256) k_pair(const PairArgs a0, const PairArgs *__restrict__ tab, int accumulate) {
+    const PairArgs A = tab ? tab[blockIdx.y] : a0;
     extern __shared__ float sp[];
     const int nt2 = A.ntypes * A.ntypes;
     if (LJ) {
@@ -227,40 +230,44 @@ __global__ void __launch_bounds__(256) k_pair(PairArgs A, int accumulate) {
     }
 }
 
+// nrep > 1: tab holds nrep records, A is the largest replica (grid sizing)
 template <int T, int LJ, bool EW>
-void launch_t(const PairArgs &A, bool vir, bool energy, bool accumulate, cudaStream_t st) {
+void launch_t(const PairArgs &A, const PairArgs *tab, int nrep, bool vir, bool energy, bool accumulate,
+              cudaStream_t st) {
     const int G = 32 / T;
     const int warps = (A.n + G - 1) / G;
-    const int blocks = (warps * 32 + 255) / 256;
+    const dim3 blocks((warps * 32 + 255) / 256, nrep);
     const size_t smem = LJ ? 3 * A.ntypes * A.ntypes * sizeof(float) : 0;
     if (energy)
-        k_pair<T, LJ, EW, false, true><<<blocks, 256, smem, st>>>(A, 0);
+        k_pair<T, LJ, EW, false, true><<<blocks, 256, smem, st>>>(A, tab, 0);
     else if (vir)
-        k_pair<T, LJ, EW, true, false><<<blocks, 256, smem, st>>>(A, accumulate ? 1 : 0);
+        k_pair<T, LJ, EW, true, false><<<blocks, 256, smem, st>>>(A, tab, accumulate ? 1 : 0);
     else
-        k_pair<T, LJ, EW, false, false><<<blocks, 256, smem, st>>>(A, accumulate ? 1 : 0);
+        k_pair<T, LJ, EW, false, false><<<blocks, 256, smem, st>>>(A, tab, accumulate ? 1 : 0);
     MDX_LAUNCHED();
 }
 
 template <int T>
-int launch_kind(const PairArgs &A, int lj, bool ew, bool vir, bool energy, bool acc, cudaStream_t st) {
-    if (lj == 0 && ew) launch_t<T, 0, true>(A, vir, energy, acc, st);
-    else if (lj == 1 && ew) launch_t<T, 1, true>(A, vir, energy, acc, st);
-    else if (lj == 1) launch_t<T, 1, false>(A, vir, energy, acc, st);
-    else if (lj == 2 && ew) launch_t<T, 2, true>(A, vir, energy, acc, st);
-    else if (lj == 2) launch_t<T, 2, false>(A, vir, energy, acc, st);
+int launch_kind(const PairArgs &A, const PairArgs *tab, int nrep, int lj, bool ew, bool vir, bool energy, bool acc,
+                cudaStream_t st) {
+    if (lj == 0 && ew) launch_t<T, 0, true>(A, tab, nrep, vir, energy, acc, st);
+    else if (lj == 1 && ew) launch_t<T, 1, true>(A, tab, nrep, vir, energy, acc, st);
+    else if (lj == 1) launch_t<T, 1, false>(A, tab, nrep, vir, energy, acc, st);
+    else if (lj == 2 && ew) launch_t<T, 2, true>(A, tab, nrep, vir, energy, acc, st);
+    else if (lj == 2) launch_t<T, 2, false>(A, tab, nrep, vir, energy, acc, st);
     else return MDX_ERR_ARG;
     return 0;
 }
 
-int launch_any(const PairArgs &A, int team, int lj, bool ew, bool vir, bool energy, bool acc, cudaStream_t st) {
+int launch_any(const PairArgs &A, int team, int lj, bool ew, bool vir, bool energy, bool acc, cudaStream_t st,
+               const PairArgs *tab = nullptr, int nrep = 1) {
     switch (team) {
-        case 1: return launch_kind<1>(A, lj, ew, vir, energy, acc, st);
-        case 2: return launch_kind<2>(A, lj, ew, vir, energy, acc, st);
-        case 4: return launch_kind<4>(A, lj, ew, vir, energy, acc, st);
-        case 8: return launch_kind<8>(A, lj, ew, vir, energy, acc, st);
-        case 16: return launch_kind<16>(A, lj, ew, vir, energy, acc, st);
-        case 32: return launch_kind<32>(A, lj, ew, vir, energy, acc, st);
+        case 1: return launch_kind<1>(A, tab, nrep, lj, ew, vir, energy, acc, st);
+        case 2: return launch_kind<2>(A, tab, nrep, lj, ew, vir, energy, acc, st);
+        case 4: return launch_kind<4>(A, tab, nrep, lj, ew, vir, energy, acc, st);
+        case 8: return launch_kind<8>(A, tab, nrep, lj, ew, vir, energy, acc, st);
+        case 16: return launch_kind<16>(A, tab, nrep, lj, ew, vir, energy, acc, st);
+        case 32: return launch_kind<32>(A, tab, nrep, lj, ew, vir, energy, acc, st);
     }
     set_error(MDX_ERR_ARG, "team size %d not in {1,2,4,8,16,32}", team);
     return MDX_ERR_ARG;
@@ -318,6 +325,30 @@ int pair_energy(State &s, FixPair &f, double *out) {
     for (int i = 0; i < A.n; i++) sum += (double)h[i];
     *out = sum;
     return 0;
+}
+
+// batched replicas: one launch, blockIdx.y = replica; tables built at prepare
+int batch_pair_tables(Batch &b) {
+    const int R = (int)b.reps.size();
+    std::vector<PairArgs> h(R);
+    for (int r = 0; r < R; r++) h[r] = make_args(*b.reps[r], *b.reps[r]->pairFix());
+    if (int e = b.tab_pair.alloc(R * sizeof(PairArgs))) return e;
+    MDX_CUDA_TRY(cudaMemcpy(b.tab_pair.p, h.data(), R * sizeof(PairArgs), cudaMemcpyHostToDevice));
+    b.pair_big = b.biggest_rep();
+    return 0;
+}
+
+int batch_pair_launch(Batch &b, cudaStream_t stream) {
+    const int R = (int)b.reps.size();
+    if (!b.tab_pair.p) {
+        set_error(MDX_ERR_STATE, "batch tables not built (prepare the batch)");
+        return MDX_ERR_STATE;
+    }
+    State &big = *b.reps[b.pair_big];
+    FixPair &f = *big.pairFix();
+    const PairArgs A = make_args(big, f);
+    return launch_any(A, big.grid.team, f.lj_kind, f.chargeFix != nullptr, false, false, true, stream,
+                      reinterpret_cast<const PairArgs *>(b.tab_pair.p), R);
 }
 
 int pair_force_raw(int n, const float4 *xs, float4 *fs, const float *qs, const uint32_t *counts,

@@ -20,7 +20,7 @@ import ctypes
 
 import numpy as np
 
-from ._lib import P, c_dbl, c_i64, c_int, c_u32, c_u64, c_void_p, check, lib
+from ._lib import P, c_dbl, c_flt, c_i64, c_int, c_u32, c_u64, c_void_p, check, lib
 
 UNITS_REAL = 0
 UNITS_LJ = 1
@@ -340,6 +340,75 @@ class FixE3B(_Fix):
     def addMolecule(self, id_O, id_H1, id_H2, id_M):
         check(lib().mdx_fix_e3b_add_molecule(self._h, int(id_O), int(id_H1), int(id_H2), int(id_M)))
 
+    # ---- learned three-body surrogate (no DASH counterpart) ----------------
+    N_IN, N_OUT, N_PARAMS = 128, 16, 17552
+
+    def surrogateCollect(self):
+        """append the current frame: features + exact three-body forces"""
+        check(lib().mdx_e3b_surrogate_collect(self.state._h, self._h))
+
+    def surrogateDatasetSize(self):
+        n = ctypes.c_int64()
+        check(lib().mdx_e3b_surrogate_dataset_size(self._h, ctypes.byref(n)))
+        return n.value
+
+    def surrogateTrain(self, iters, batch=4096, lr=1e-3, seed=1):
+        """(loss of the first, loss of the last minibatch)"""
+        a, b = c_dbl(), c_dbl()
+        check(lib().mdx_e3b_surrogate_train(self.state._h, self._h, int(iters), int(batch), float(lr), int(seed),
+                                            ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def surrogateEnable(self, on=True):
+        check(lib().mdx_e3b_surrogate_enable(self._h, 1 if on else 0))
+
+    def surrogateEval(self):
+        """(rmse, rms) of the surrogate's three-body forces on the current frame"""
+        a, b = c_dbl(), c_dbl()
+        check(lib().mdx_e3b_surrogate_eval(self.state._h, self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def surrogateParams(self):
+        w = np.zeros(self.N_PARAMS, np.float32)
+        mu = np.zeros(self.N_IN, np.float32)
+        isd = np.zeros(self.N_IN, np.float32)
+        sc = c_flt()
+        check(lib().mdx_e3b_surrogate_get_params(self._h, w.ctypes.data_as(P(c_flt)), mu.ctypes.data_as(P(c_flt)),
+                                                 isd.ctypes.data_as(P(c_flt)), ctypes.byref(sc)))
+        return w, mu, isd, sc.value
+
+    def surrogateSetParams(self, w, mean, inv_std, scale):
+        w = np.ascontiguousarray(w, np.float32)
+        mean = np.ascontiguousarray(mean, np.float32)
+        inv_std = np.ascontiguousarray(inv_std, np.float32)
+        check(lib().mdx_e3b_surrogate_set_params(self.state._h, self._h, w.ctypes.data_as(P(c_flt)),
+                                                 mean.ctypes.data_as(P(c_flt)), inv_std.ctypes.data_as(P(c_flt)),
+                                                 float(scale)))
+
+    def surrogateFeatures(self, nmol):
+        raw = np.zeros((nmol, self.N_IN), np.float32)
+        fr = np.zeros((nmol, 9), np.float32)
+        check(lib().mdx_e3b_surrogate_features(self.state._h, self._h, raw.ctypes.data_as(P(c_flt)),
+                                               fr.ctypes.data_as(P(c_flt))))
+        return raw, fr.reshape(nmol, 3, 3)
+
+    def surrogateInfer(self, x):
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.zeros((len(x), self.N_OUT), np.float32)
+        check(lib().mdx_e3b_surrogate_infer(self.state._h, self._h, x.ctypes.data_as(P(c_flt)), len(x),
+                                            y.ctypes.data_as(P(c_flt))))
+        return y
+
+    def surrogateGrad(self, x, t):
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        g = np.zeros(self.N_PARAMS, np.float32)
+        loss = c_dbl()
+        check(lib().mdx_e3b_surrogate_grad(self.state._h, self._h, x.ctypes.data_as(P(c_flt)),
+                                           t.ctypes.data_as(P(c_flt)), len(x), g.ctypes.data_as(P(c_flt)),
+                                           ctypes.byref(loss)))
+        return loss.value, g
+
 
 class FixRigid(_Fix):
     """FixRigid(state, handle, style) (src/Fixes/FixRigid.cu:18-37)"""
@@ -436,6 +505,46 @@ class IntegratorVerlet:
 
     def secondHalf(self):
         check(lib().mdx_verlet_second_half(self.state._h))
+
+
+class BatchReplicas:
+    """Independent rigid-water States advanced together, one launch per phase
+    for all replicas (no DASH counterpart; each replica keeps
+    IntegratorVerlet's per-step semantics).  The states must stay alive while
+    the batch exists."""
+
+    def __init__(self, states):
+        h = c_void_p()
+        check(lib().mdx_batch_create(ctypes.byref(h)))
+        self._h = h
+        self.states = list(states)
+        for st in self.states:
+            check(lib().mdx_batch_add(self._h, st._h))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                lib().mdx_batch_destroy(h)
+            except Exception:
+                pass
+
+    def __len__(self):
+        return len(self.states)
+
+    def prepare(self):
+        check(lib().mdx_batch_prepare(self._h))
+
+    def run(self, numTurns):
+        """device milliseconds of the call"""
+        out = c_dbl()
+        check(lib().mdx_batch_run(self._h, int(numTurns), ctypes.byref(out)))
+        return out.value
+
+    def runTimed(self, numTurns, chunk, flushBytes):
+        out = c_dbl()
+        check(lib().mdx_batch_run_timed(self._h, int(numTurns), int(chunk), int(flushBytes), ctypes.byref(out)))
+        return out.value
 
 
 def kernel_launches():

@@ -95,14 +95,21 @@ def _random_rotations(rng, m):
     return R
 
 
-def water_tip4p2005(nside=16, density=0.997, T=298.0, seed=DEFAULT_SEED):
+def water_tip4p2005(nside=16, density=0.997, T=298.0, seed=DEFAULT_SEED, nmol=None):
     """nside^3 rigid TIP4P/2005 molecules on a cubic lattice at `density`
-    g/cm^3 with seeded random orientations; ids per molecule O, H1, H2, M."""
-    m = nside ** 3
+    g/cm^3 with seeded random orientations; ids per molecule O, H1, H2, M.
+    With nmol, a box for nmol molecules at that density whose lattice of
+    ceil(nmol^(1/3))^3 sites is filled at nmol seeded random sites."""
+    m = nside ** 3 if nmol is None else int(nmol)
+    if nmol is not None:
+        nside = int(math.ceil(m ** (1.0 / 3.0) - 1e-9))
     vol_per = WATER_MOLAR_MASS / (density * AVOGADRO) * 1e24  # A^3
     L = (m * vol_per) ** (1.0 / 3.0)
     sp = L / nside
     g = np.stack(np.meshgrid(np.arange(nside), np.arange(nside), np.arange(nside), indexing="ij"), -1).reshape(-1, 3)
+    if nmol is not None:
+        pick = np.sort(np.random.default_rng(seed + 1).choice(len(g), m, replace=False))
+        g = g[pick]
     centers = (g + 0.5) * sp
     half = math.asin(0.5 * R_HH / R_OH)
     local = np.array([
@@ -198,3 +205,21 @@ def build_water_state(sysd: System, rcut=9.0, skin=1.0, dt=2.0, interval=10, gri
         st.activateFix(nh)
         fixes["nh"] = nh
     return st, fixes
+
+
+def water_replica_sizes(nrep=64, lo=256, hi=2048, seed=DEFAULT_SEED):
+    """molecule counts drawn log-uniform in [lo, hi] and temperatures uniform
+    in [260, 360] K, seeded (the batched-replica workload)"""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(math.log(lo), math.log(hi), nrep)).round().astype(int)
+    temps = rng.uniform(260.0, 360.0, nrep)
+    return sizes, temps
+
+
+def p3m_mesh_for(L, h_max=1.0):
+    """smallest power-of-two mesh with spacing <= h_max (the 2^N rule of the
+    reference's examples)"""
+    n = 8
+    while L / n > h_max:
+        n *= 2
+    return n

@@ -1,0 +1,44 @@
+"""Generate tests/golden/ref_functors.json from the reference's own
+host-callable functors (EvaluatorLJ::force, PairEvaluatorLJ.h:17-60;
+EvaluatorE3B switching / pair energy / force, EvaluatorE3B.h:67-249),
+compiled from the reference source by oracle/ref.mk into oracle/_ref.
+
+Run in a checkout where the reference source is present:
+    make -f oracle/ref.mk && python tests/golden/make_ref_functors.py
+The committed JSON lets the CPU tests pin the oracle without the reference."""
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle import refkernels as R  # noqa: E402
+
+
+def main():
+    if not R.available():
+        raise SystemExit("oracle/_ref/librefkernels.so is not built")
+    rng = np.random.default_rng(20261203)
+    lj = []
+    for _ in range(40):
+        dr = rng.uniform(-3, 3, 3)
+        if np.linalg.norm(dr) < 2.0:
+            continue
+        lj.append({"sigma": 3.0, "eps": 6.0, "rcut": 10.0, "dr": [float(v) for v in dr.astype(np.float32)],
+                   "force": [float(v) for v in R.lj_force_host(3.0, 6.0, 10.0, dr)]})
+    e3b = []
+    for r in np.linspace(0.8, 5.5, 48):
+        e3b.append({"r": float(r), "out": [float(v) for v in R.e3b_single_host(float(r))]})
+    out = {"source": "reference functors compiled from source by oracle/ref.mk (EvaluatorLJ::force; "
+                     "EvaluatorE3B E3B3 single O-H term: switching, energy, force)",
+           "lj": lj, "e3b3_single": e3b}
+    with open(os.path.join(HERE, "ref_functors.json"), "w") as f:
+        json.dump(out, f, indent=1)
+    print(f"wrote {len(lj)} LJ and {len(e3b)} E3B vectors")
+
+
+if __name__ == "__main__":
+    main()

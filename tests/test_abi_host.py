@@ -100,3 +100,23 @@ def test_product_path_has_no_oracle_import():
             if f.endswith(".py"):
                 txt = open(os.path.join(root, f)).read()
                 assert "import oracle" not in txt and "from oracle" not in txt, f
+
+
+def test_batch_argument_errors_without_gpu():
+    """batch entry points reject bad input before touching the device"""
+    from md_engine_b200 import _lib
+    lib = _lib.lib()
+    b = ctypes.c_void_p()
+    assert lib.mdx_batch_create(ctypes.byref(b)) == 0
+    assert lib.mdx_batch_add(b, None) == 1
+    assert lib.mdx_batch_prepare(b) == 3  # no replicas
+    n = ctypes.c_int(-1)
+    assert lib.mdx_batch_size(b, ctypes.byref(n)) == 0 and n.value == 0
+    st = ctypes.c_void_p()
+    assert lib.mdx_state_create(ctypes.byref(st)) == 0
+    assert lib.mdx_batch_add(b, st) == 0
+    assert lib.mdx_batch_add(b, st) == 1  # the same state twice
+    assert lib.mdx_batch_size(b, ctypes.byref(n)) == 0 and n.value == 1
+    assert lib.mdx_batch_run_timed(b, 10, 0, 0, None) == 1
+    assert lib.mdx_batch_destroy(b) == 0
+    assert lib.mdx_state_destroy(st) == 0

@@ -254,3 +254,23 @@ def test_oracle_per_pair_maths_vs_reference_functors(oracle):
         b = np.zeros(4)
         oracle.lib().orc_e3b_single(prm.ctypes.data_as(ctypes.c_void_p), float(rr), b.ctypes.data_as(ctypes.c_void_p))
         assert np.max(np.abs(a - b)) <= 2e-5 * max(1.0, np.abs(b).max())
+
+
+def test_oracle_vs_committed_reference_functor_vectors(oracle):
+    """golden vectors produced by the reference's own functors (compiled from
+    its source; tests/golden/make_ref_functors.py) pin the oracle's per-pair
+    LJ and E3B maths without the reference present"""
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "ref_functors.json")) as f:
+        g = json.load(f)
+    assert len(g["lj"]) > 20 and len(g["e3b3_single"]) > 40
+    for v in g["lj"]:
+        o = _lj(oracle, v["sigma"], v["eps"], v["rcut"], np.array(v["dr"], np.float64))
+        ref = np.array(v["force"])
+        assert np.max(np.abs(ref - o)) <= 2e-6 * max(1.0, np.abs(o).max())
+    prm = oracle.e3b_params("E3B3")
+    for v in g["e3b3_single"]:
+        b = np.zeros(4)
+        oracle.lib().orc_e3b_single(prm.ctypes.data_as(ctypes.c_void_p), float(v["r"]), b.ctypes.data_as(ctypes.c_void_p))
+        assert np.max(np.abs(np.array(v["out"]) - b)) <= 2e-5 * max(1.0, np.abs(b).max())
