@@ -212,7 +212,7 @@ int mdx_pair_force_raw(int n, const float *xs4, float *fs4, const float *qs, con
  * evaluations (fused step and compute) between exact (0) and surrogate (1);
  * eval compares surrogate and exact three-body forces on the current frame.
  * The exact O-O two-body term is always evaluated exactly.  Parameters are
- * kParams = 17,552 floats: W1[128x64] b1 W2[64x64] b2 W3[64x64] b3 W4[64x16]
+ * kParams = 17,616 floats: W1[128x64] b1 W2[64x64] b2 W3[64x64] b3 W4[64x16]
  * b4[16] (outputs 9..15 unused). */
 int mdx_e3b_surrogate_collect(mdx_state *st, mdx_fix *e3b);
 int mdx_e3b_surrogate_dataset_size(mdx_fix *e3b, int64_t *n);
@@ -227,7 +227,7 @@ int mdx_e3b_surrogate_set_params(mdx_state *st, mdx_fix *e3b, const float *w, co
 int mdx_e3b_surrogate_features(mdx_state *st, mdx_fix *e3b, float *raw, float *frames);
 /* model outputs (n x 16) for n standardised feature rows (n x 128) */
 int mdx_e3b_surrogate_infer(mdx_state *st, mdx_fix *e3b, const float *x, int n, float *y);
-/* mean-squared-error loss and its gradient (17,552 floats) for n rows of
+/* mean-squared-error loss and its gradient (17,616 floats) for n rows of
  * standardised features x (n x 128) and scaled targets t (n x 16); n % 64 == 0 */
 int mdx_e3b_surrogate_grad(mdx_state *st, mdx_fix *e3b, const float *x, const float *t, int n, float *grad,
                            double *loss);

@@ -341,7 +341,8 @@ class FixE3B(_Fix):
         check(lib().mdx_fix_e3b_add_molecule(self._h, int(id_O), int(id_H1), int(id_H2), int(id_M)))
 
     # ---- learned three-body surrogate (no DASH counterpart) ----------------
-    N_IN, N_OUT, N_PARAMS = 128, 16, 17552
+    N_IN, N_OUT = 128, 16
+    N_PARAMS = (128 * 64 + 64) + 2 * (64 * 64 + 64) + (64 * 16 + 16)  # 17,616
 
     def surrogateCollect(self):
         """append the current frame: features + exact three-body forces"""

@@ -120,3 +120,12 @@ def test_batch_argument_errors_without_gpu():
     assert lib.mdx_batch_run_timed(b, 10, 0, 0, None) == 1
     assert lib.mdx_batch_destroy(b) == 0
     assert lib.mdx_state_destroy(st) == 0
+
+
+def test_surrogate_parameter_count_agrees():
+    """the Python binding, the header and the CPU restatement agree on the
+    surrogate's parameter blob size (the library writes that many floats)"""
+    from md_engine_b200.dash import FixE3B
+    from oracle import surrogate_ref
+    assert FixE3B.N_PARAMS == surrogate_ref.N_PARAMS == 17616
+    assert "17,616 floats" in open(os.path.join(ROOT, "include", "mdx.h")).read()
