@@ -6,7 +6,8 @@ Workload (default): 4,096 molecules (16,384 sites incl. M), cubic lattice at
 298 K, FP32 with FP64 reductions and FP64 SETTLE, neighbour check every 10
 steps.  A "step" is one MD timestep of that system.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload water|water_e3b|lj]
+  python bench.py [--gpus N] [--steps K] [--warmup W]
+                  [--workload water|water_e3b|lj|batched|surrogate]
   python bench.py --impl reference ...   # the reference's CPU arm (the oracle)
 
 Under torchrun every rank steps its own independent replica (the path does
@@ -37,7 +38,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="water", choices=["water", "water_e3b", "lj"])
+    ap.add_argument("--workload", default="water", choices=["water", "water_e3b", "lj", "batched", "surrogate"])
+    ap.add_argument("--replicas", type=int, default=64)
+    ap.add_argument("--frames", type=int, default=40, help="surrogate: frames per training temperature")
+    ap.add_argument("--train-iters", type=int, default=4000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -197,11 +201,161 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line))
 
 
+def batched_states(nrep, seed, e3b=True):
+    """the batched-replica workload: nrep TIP4P/2005(+E3B3) boxes, molecule
+    counts log-uniform in [256, 2048], T uniform in [260, 360] K, rc 9 A,
+    skin 0.8 A, P3M mesh 32^3 or 64^3 by box size"""
+    from md_engine_b200 import systems
+    sizes, temps = systems.water_replica_sizes(nrep, seed=seed)
+    out = []
+    for r, (m, T) in enumerate(zip(sizes, temps)):
+        sysd = systems.water_tip4p2005(nmol=int(m), T=float(T), seed=seed + 1000 + r)
+        st, _ = systems.build_water_state(sysd, rcut=9.0, skin=0.8, dt=2.0, interval=10,
+                                          grid=systems.p3m_mesh_for(sysd.L[0]), e3b=e3b, T=float(T), tau=100.0)
+        st.nThreadPerAtom = 8
+        out.append((st, int(m)))
+    return out
+
+
+def side_line(args, world, value, unit, K, ms_max, cfg, extra, clk, launches):
+    line = {"metric": METRIC, "value": value, "unit": unit, "n_gpus": world, "steps": K,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms_max / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 reductions, f64 SETTLE)",
+            "data": "synthetic (seeded lattice + random orientations + Maxwell-Boltzmann)", "config": cfg,
+            "gpu_launches": launches, "clocks": clk.summary()}
+    line.update(extra)
+    print(json.dumps(line))
+
+
+def run_batched(args, rank, world, local):
+    """replica timesteps/s of the batched form against the same replicas run
+    one after another through IntegratorVerlet (the plain per-replica path)"""
+    import torch
+    from md_engine_b200 import BatchReplicas, IntegratorVerlet, kernel_launches
+    dist = init_pg(world, "nccl")
+    dev = torch.device("cuda", local)
+    seed = 20261203 + 7919 * rank
+    reps = batched_states(args.replicas, seed)
+    states = [s for s, _ in reps]
+    mols = sum(m for _, m in reps)
+    b = BatchReplicas(states)
+    team, tune_ms = b.autotune(steps=20, teams=(4, 8, 16))
+    b.run(max(args.warmup, 3))
+    K = args.steps
+    barrier(dist, dev)
+    torch.cuda.synchronize()
+    k0 = kernel_launches()
+    with ClockSampler(local) as clk:
+        ms = b.runTimed(K, 10, L2_FLUSH_BYTES)
+    k1 = kernel_launches()
+    barrier(dist, dev)
+    ms_max = reduce_max(dist, ms, dev)
+    R = len(states)
+    value = world * R * K / (ms_max * 1e-3)
+    # the plain path: every replica alone (fresh copies), same step count
+    seq_ms = 0.0
+    Ks = min(K, 50)
+    for st, _ in batched_states(args.replicas, seed):
+        it = IntegratorVerlet(st)
+        it.run(3)
+        seq_ms += it.runTimed(Ks, 10, 0)
+    seq = R * Ks / (seq_ms * 1e-3)
+    if rank == 0:
+        cfg = {"workload": f"{R} TIP4P/2005+E3B3 replicas, {mols} molecules, sizes log-uniform 256-2048, "
+                           "T 260-360 K, rc 9 A, skin 0.8 A, P3M 32^3/64^3",
+               "replicas": R, "molecules": mols, "autotuned_team": team,
+               "l2": "flushed between timed 10-step chunks (256 MiB write)",
+               "parallelism": "replicas only" if world > 1 else "one batch"}
+        side_line(args, world, value, "replica timesteps/s", K, ms_max, cfg,
+                  {"sequential_plain": {"value": seq, "unit": "replica timesteps/s", "steps_per_replica": Ks},
+                   "batched_over_sequential": value / world / seq}, clk, int(k1 - k0))
+    if dist is not None:
+        barrier(dist, dev)
+        dist.destroy_process_group()
+
+
+def run_surrogate(args, rank, world, local):
+    """TIP4P/2005+E3B3, 4,096 molecules: the exact E3B step against the step
+    with the learned three-body surrogate, trained here on frames the exact
+    kernel labels (NVT runs at 260, 310 and 360 K), judged on a frame of an
+    unseen 330 K run"""
+    import torch
+    from md_engine_b200 import IntegratorVerlet, kernel_launches, systems
+    dist = init_pg(world, "nccl")
+    dev = torch.device("cuda", local)
+    seed = 20261203 + 7919 * rank
+
+    def state(T, sd):
+        sysd = systems.water_tip4p2005(nside=16, seed=sd, T=T)
+        return systems.build_water_state(sysd, rcut=9.0, skin=1.0, dt=2.0, interval=10, grid=64, e3b=True,
+                                         T=T, tau=100.0)
+
+    st, fx = state(298.0, seed)
+    it = IntegratorVerlet(st)
+    it.run(max(args.warmup, 3))
+    K = args.steps
+    ms_exact = it.runTimed(K, 10, L2_FLUSH_BYTES)
+    e3 = fx["e3b"]
+    t0 = time.perf_counter()
+    nframes = 0
+    for T, sd in ((260.0, seed + 1), (310.0, seed + 2), (360.0, seed + 3)):
+        st_t, _ = state(T, sd)
+        it_t = IntegratorVerlet(st_t)
+        it_t.run(200)
+        for _ in range(args.frames):
+            it_t.run(10)
+            x, v, _ = st_t.getAtoms()
+            st.putAtoms(x, v)
+            st.buildNeighborlists(force=True)
+            e3.surrogateCollect()
+            nframes += 1
+    t_collect = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    l0, l1 = e3.surrogateTrain(args.train_iters, batch=4096, lr=2e-3, seed=seed)
+    t_train = time.perf_counter() - t0
+    st_h, _ = state(330.0, seed + 4)
+    IntegratorVerlet(st_h).run(300)
+    x, v, _ = st_h.getAtoms()
+    st.putAtoms(x, v)
+    st.buildNeighborlists(force=True)
+    rmse, rms = e3.surrogateEval()
+    e3.surrogateEnable(True)
+    it.run(max(args.warmup, 3))
+    barrier(dist, dev)
+    k0 = kernel_launches()
+    with ClockSampler(local) as clk:
+        ms_sur = it.runTimed(K, 10, L2_FLUSH_BYTES)
+    k1 = kernel_launches()
+    ms_max = reduce_max(dist, ms_sur, dev)
+    value = world * K / (ms_max * 1e-3)
+    if rank == 0:
+        cfg = {"workload": "TIP4P/2005+E3B3 4,096 molecules, LJ+Coulomb 9 A, skin 1 A, P3M 64^3, SETTLE, "
+                           "dt 2 fs, Nose-Hoover 298 K; E3B three-body from the BF16 MLP surrogate",
+               "molecules": 4096, "training_frames": nframes, "train_iters": args.train_iters,
+               "l2": "flushed between timed 10-step chunks (256 MiB write)", "parallelism": "single system"}
+        side_line(args, world, value, "timesteps/s", K, ms_max, cfg,
+                  {"exact_e3b": {"value": K / (ms_exact * 1e-3), "unit": "timesteps/s"},
+                   "surrogate_over_exact": (K / (ms_max * 1e-3)) / (K / (ms_exact * 1e-3)),
+                   "threebody_force_rmse_over_rms": rmse / rms, "threebody_force_rms": rms,
+                   "train_loss_first_last": [l0, l1], "collect_s": t_collect, "train_s": t_train},
+                  clk, int(k1 - k0))
+    if dist is not None:
+        barrier(dist, dev)
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
+        return
+    if args.workload in ("batched", "surrogate"):
+        import torch
+        from md_engine_b200._lib import lib
+        torch.cuda.set_device(local)
+        lib().mdx_set_device(local)
+        (run_batched if args.workload == "batched" else run_surrogate)(args, rank, world, local)
         return
     import torch
     from md_engine_b200 import IntegratorVerlet, kernel_launches

@@ -251,6 +251,12 @@ int mdx_batch_size(mdx_batch *b, int *n);
 int mdx_batch_prepare(mdx_batch *b);
 int mdx_batch_run(mdx_batch *b, int num_turns, double *device_ms);
 int mdx_batch_run_timed(mdx_batch *b, int num_turns, int chunk, size_t flush_bytes, double *device_ms);
+/* autotuner (replaces Integrator::tune, src/Integrators/Integrator.cu:272-376):
+ * resets the replicas to their configured initial state, times `steps` batched
+ * steps for each neighbour team size in teams[0..nteams) and leaves the batch
+ * prepared with the fastest (best_team, device ms per step in best_ms).  Call
+ * it before the production run: the timing runs start from the initial state. */
+int mdx_batch_autotune(mdx_batch *b, int steps, const int *teams, int nteams, int *best_team, double *best_ms);
 int mdx_batch_destroy(mdx_batch *b);
 
 #ifdef __cplusplus

@@ -102,6 +102,7 @@ SIGNATURES = [
     ("mdx_batch_prepare", c_int, [c_void_p]),
     ("mdx_batch_run", c_int, [c_void_p, c_int, P(c_dbl)]),
     ("mdx_batch_run_timed", c_int, [c_void_p, c_int, c_int, ctypes.c_size_t, P(c_dbl)]),
+    ("mdx_batch_autotune", c_int, [c_void_p, c_int, P(c_int), c_int, P(c_int), P(c_dbl)]),
     ("mdx_batch_destroy", c_int, [c_void_p]),
 ]
 

@@ -47,10 +47,80 @@ int Batch::biggest_rep() const {
     return best;
 }
 
+void Batch::reset() {
+    clearGraphs();
+    for (State *s : reps) {
+        if (FixChargeEwald *ew = s->ewaldFix()) {
+            // views into the pools below: let the fix own its buffers again
+            ew->rho.release();
+            ew->rho_k.release();
+            ew->e_k.release();
+            ew->e_r.release();
+        }
+        s->prepared = false;
+        s->grid.cap = 0;
+        s->turn = turn0;
+    }
+    for (auto &c : fft) {
+        if (c->r2c) cufftDestroy(c->r2c);
+        if (c->c2r) cufftDestroy(c->c2r);
+    }
+    fft.clear();
+    for (DBuf<char> *t : {&tab_pair, &tab_grid, &tab_build, &tab_p3m, &tab_e3b, &tab_first, &tab_second}) t->release();
+    max_n = max_mol = max_cell = 0;
+    max_nk = 0;
+    prepared = false;
+}
+
+// The reference's Integrator::tune (Integrator.cu:272-376) times 30 force
+// evaluations for every (threads per block, threads per atom) pair; here the
+// whole batched step is timed for each neighbour team size (threads per
+// atom; the pair kernel's list layout and the build follow it) from the same
+// initial state, and the batch is left prepared with the fastest.
+int Batch::autotune(int steps, const int *cands, int ncand, int *best, double *best_ms) {
+    if (steps <= 0 || ncand <= 0 || !cands) {
+        set_error(MDX_ERR_ARG, "need steps > 0 and candidate team sizes");
+        return MDX_ERR_ARG;
+    }
+    if (!turn0_set) {
+        turn0 = reps.empty() ? 0 : reps[0]->turn;
+        turn0_set = true;
+    }
+    int arg = -1;
+    double tbest = 1e300;
+    for (int k = 0; k < ncand; k++) {
+        const int t = cands[k];
+        if (t != 1 && t != 2 && t != 4 && t != 8 && t != 16 && t != 32) {
+            set_error(MDX_ERR_ARG, "team size %d not in {1,2,4,8,16,32}", t);
+            return MDX_ERR_ARG;
+        }
+        reset();
+        for (State *s : reps) s->nThreadPerAtom = t;
+        if (int e = prepare()) return e;
+        if (int e = run(periodicInterval, nullptr)) return e;  // capture the graphs
+        double ms = 0.0;
+        if (int e = runTimed(steps, periodicInterval, 0, &ms)) return e;
+        if (ms < tbest) {
+            tbest = ms;
+            arg = t;
+        }
+    }
+    reset();
+    for (State *s : reps) s->nThreadPerAtom = arg;
+    if (int e = prepare()) return e;
+    if (best) *best = arg;
+    if (best_ms) *best_ms = tbest / steps;
+    return 0;
+}
+
 int Batch::prepare() {
     if (reps.empty()) {
         set_error(MDX_ERR_STATE, "batch has no replicas");
         return MDX_ERR_STATE;
+    }
+    if (!turn0_set) {
+        turn0 = reps[0]->turn;
+        turn0_set = true;
     }
     State &s0 = *reps[0];
     const bool e3b0 = s0.e3bFix() != nullptr;
@@ -347,6 +417,19 @@ int mdx_batch_run_timed(mdx_batch *b, int num_turns, int chunk, size_t flush_byt
         return b->b->runTimed(num_turns, chunk, flush_bytes, device_ms);
     } catch (...) {
         set_error(MDX_ERR_STATE, "exception in batch run");
+        return MDX_ERR_STATE;
+    }
+}
+
+int mdx_batch_autotune(mdx_batch *b, int steps, const int *teams, int nteams, int *best_team, double *best_ms) {
+    if (!b) {
+        set_error(MDX_ERR_ARG, "null batch");
+        return MDX_ERR_ARG;
+    }
+    try {
+        return b->b->autotune(steps, teams, nteams, best_team, best_ms);
+    } catch (...) {
+        set_error(MDX_ERR_STATE, "exception in batch autotune");
         return MDX_ERR_STATE;
     }
 }

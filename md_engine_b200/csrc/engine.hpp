@@ -411,6 +411,12 @@ class Batch {
     int runTimed(int nturns, int chunk, size_t flush_bytes, double *ms_total);
     int checkStatus();
     void clearGraphs();
+    // back to the configured, unprepared replicas (their initial host state)
+    void reset();
+    // time `steps` steps for each neighbour team size in cands, keep the fastest
+    int autotune(int steps, const int *cands, int ncand, int *best, double *best_ms);
+    int64_t turn0 = 0;
+    bool turn0_set = false;
 };
 int batch_pair_tables(Batch &b);
 int batch_nlist_tables(Batch &b);

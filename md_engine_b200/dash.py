@@ -547,6 +547,14 @@ class BatchReplicas:
         check(lib().mdx_batch_run_timed(self._h, int(numTurns), int(chunk), int(flushBytes), ctypes.byref(out)))
         return out.value
 
+    def autotune(self, steps=20, teams=(4, 8, 16)):
+        """(best team size, device ms per step); leaves the batch prepared with it"""
+        arr = (c_int * len(teams))(*teams)
+        best = c_int()
+        ms = c_dbl()
+        check(lib().mdx_batch_autotune(self._h, int(steps), arr, len(teams), ctypes.byref(best), ctypes.byref(ms)))
+        return best.value, ms.value
+
 
 def kernel_launches():
     return int(lib().mdx_kernel_launch_count())

@@ -88,3 +88,21 @@ def test_batch_thermostats_hold_each_temperature():
     assert np.all(np.isfinite(temps))
     assert 150 < temps[0] < 600 and 200 < temps[1] < 700, temps
     assert temps[1] > temps[0], temps
+
+
+def test_autotune_picks_a_team_and_keeps_the_trajectory():
+    """the autotuner times each team size from the initial state and leaves
+    the batch prepared from that state: the run that follows matches the
+    replicas run one at a time"""
+    spec = [(256, 270.0, 51), (333, 330.0, 52)]
+    states = [_replica(m, T, seed)[0] for m, T, seed in spec]
+    b = BatchReplicas(states)
+    best, ms = b.autotune(steps=10, teams=(4, 8, 16))
+    assert best in (4, 8, 16) and ms > 0
+    b.run(25)
+    for (m, T, seed), st in zip(spec, states):
+        ref, _ = _replica(m, T, seed)
+        IntegratorVerlet(ref).run(25)
+        d = np.abs(st.getAtoms()[0] - ref.getAtoms()[0]).max()
+        assert d < 1e-3, d
+        assert st.status()[0] == 0
