@@ -204,6 +204,10 @@ class FixChargeEwald : public Fix {
     DBuf<float> e_r;        // 3 real grids
     DBuf<float> green;      // half spectrum Green function
     DBuf<double> energy_acc;
+    // own FFT path (cubic 32^3 / 64^3 meshes): field interleaved as float4
+    bool own_fft = false;
+    DBuf<float4> e4;
+    DBuf<float2> tw;        // W_32^k then W_64^k
     FixChargeEwald(State *s, std::string h, std::string g);
     ~FixChargeEwald() override;
     int setParameters(int nx, int ny, int nz, double rcut, int ord);

@@ -78,14 +78,27 @@ struct P3MArgs {
 };
 #define MDX_P3M_ARGS const P3MArgs A = tab ? tab[blockIdx.y] : a0
 
-__global__ void k_spread(const P3MArgs a0, const P3MArgs *__restrict__ tab) {
+// map_charge_to_grid_order_5_cu (FixChargeEwald.cu:174-217) with five lanes
+// per atom: lane t adds the 25 points of stencil plane a = t.  The six atoms
+// of a warp are taken W = n/6 apart (atom g W + warp) so that the float
+// atomics of one warp instruction land in distant parts of the mesh instead
+// of piling onto the same points (neighbouring atoms are adjacent in the
+// cell-sorted order)
+__device__ __forceinline__ float pick5(const float w[5], int t) {
+    return t == 0 ? w[0] : t == 1 ? w[1] : t == 2 ? w[2] : t == 3 ? w[3] : w[4];
+}
+
+__global__ void k_spread5(const P3MArgs a0, const P3MArgs *__restrict__ tab) {
     MDX_P3M_ARGS;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.n) return;
-    const P3MGeom &g = A.g;
-    float *__restrict__ rho = A.rho;
+    const int lane = threadIdx.x & 31;
+    const int t = lane % 5;
+    const int W = (A.n + 5) / 6;
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int i = (lane / 5) * W + w;
+    if (lane >= 30 || w >= W || i >= A.n) return;
     const float q = A.qs[i];
     if (q == 0.f) return;
+    const P3MGeom &g = A.g;
     const float qi = g.qunit * q;
     int3 ng;
     float3 d;
@@ -97,18 +110,15 @@ __global__ void k_spread(const P3MArgs a0, const P3MArgs *__restrict__ tab) {
     int pz[5];
 #pragma unroll
     for (int c = 0; c < 5; c++) pz[c] = wrapi(ng.z + c - 2, g.sz.z);
+    const int px = wrapi(ng.x + t - 2, g.sz.x);
+    const float cyz = qi * pick5(wx, t);
 #pragma unroll
-    for (int a = 0; a < 5; a++) {
-        const int px = wrapi(ng.x + a - 2, g.sz.x);
-        const float cyz = qi * wx[a];
+    for (int b = 0; b < 5; b++) {
+        const int py = wrapi(ng.y + b - 2, g.sz.y);
+        const float cz = cyz * wy[b];
+        float *row = A.rho + ((size_t)px * g.sz.y + py) * g.sz.z;
 #pragma unroll
-        for (int b = 0; b < 5; b++) {
-            const int py = wrapi(ng.y + b - 2, g.sz.y);
-            const float cz = cyz * wy[b];
-            float *row = rho + ((size_t)px * g.sz.y + py) * g.sz.z;
-#pragma unroll
-            for (int c = 0; c < 5; c++) atomicAdd(row + pz[c], cz * wz[c]);
-        }
+        for (int c = 0; c < 5; c++) atomicAdd(row + pz[c], cz * wz[c]);
     }
 }
 
@@ -265,6 +275,279 @@ P3MArgs p3m_args(State &s, FixChargeEwald &f) {
     return A;
 }
 
+// ---- P3M reciprocal solve on our own FFT (cubic 32^3 / 64^3 meshes) --------
+// One warp transforms one line of N = 32 R points held as v[r] = x[32 r + lane]:
+// R-point DFTs inside each lane, twiddles W_N^(lane k1), then a radix-2
+// decimation-in-frequency FFT of 32 points across the lanes (shuffles); lane
+// l then holds X[k1 + R bitrev5(l)] in v[k1].  Unnormalised, as cuFFT.
+// Three kernels replace R2C + E(k) + batched C2R:
+//   k_fft_zy   per x plane: real FFT along z (half spectrum kept) then along y
+//   k_fft_xe   per (ky, kz) line: FFT along x, E_d(k) = i k_d G rho (Nyquist
+//              planes dropped per component, as k_efield), 3 inverse FFTs along x
+//   k_ifft_yz  per (x plane, component): inverse along y, then the real inverse along z of
+//              the Hermitian half spectrum, E written as float4 (Ex, Ey, Ez, 0)
+// so the gather reads one 16-byte field value per stencil point.
+struct FFTArgs {
+    int n;                   // points per side (32 or 64)
+    const float *rho;        // [n][n][n]
+    float2 *mid1;            // [n][n][n/2+1]: after the z and y passes
+    float2 *mid2;            // [3][n][n][n/2+1]: E_d after the inverse x pass
+    float4 *e4;              // [n][n][n]
+    const float *green;      // [n][n][n/2+1]
+    const float2 *tw;        // W_32^k (32) then W_64^k (64), forward sign
+    float3 tpl;              // 2 pi / L
+};
+
+__device__ __forceinline__ int brev5(int l) { return (int)(__brev((unsigned)l) >> 27); }
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// this lane's twiddles: W_2h^(lane mod h) for the five lane stages and
+// W_N^lane for the R = 2 step (forward sign; conjugated for the inverse)
+struct LaneTw {
+    float2 st[5];
+    float2 wn;
+};
+
+template <int R>
+__device__ __forceinline__ LaneTw lane_twiddles(int lane, const float2 *__restrict__ tw) {
+    LaneTw T;
+#pragma unroll
+    for (int s = 0; s < 5; s++) {
+        const int h = 16 >> s;
+        T.st[s] = __ldg(tw + (lane & (h - 1)) * (16 / h));
+    }
+    T.wn = R == 2 ? __ldg(tw + 32 + lane) : make_float2(1.f, 0.f);
+    return T;
+}
+
+// forward (INV = false: W = exp(-2 pi i k / N)) or inverse (W conjugated)
+template <int R, bool INV>
+__device__ __forceinline__ void warp_fft(float2 (&v)[R], int lane, const LaneTw &T) {
+    if (R == 2) {
+        const float2 a = v[0], b = v[1];
+        v[0] = make_float2(a.x + b.x, a.y + b.y);
+        float2 w = T.wn;
+        if (INV) w.y = -w.y;
+        v[1] = cmul(make_float2(a.x - b.x, a.y - b.y), w);
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < R; k1++) {
+#pragma unroll
+        for (int s = 0; s < 5; s++) {
+            const int h = 16 >> s;
+            const float px = __shfl_xor_sync(0xffffffffu, v[k1].x, h);
+            const float py = __shfl_xor_sync(0xffffffffu, v[k1].y, h);
+            if ((lane & h) == 0) {
+                v[k1] = make_float2(v[k1].x + px, v[k1].y + py);
+            } else {
+                float2 w = T.st[s];
+                if (INV) w.y = -w.y;
+                v[k1] = cmul(make_float2(px - v[k1].x, py - v[k1].y), w);
+            }
+        }
+    }
+}
+
+template <int R>
+__device__ __forceinline__ int fft_out_index(int k1, int lane) { return k1 + R * brev5(lane); }
+
+template <int R>
+__global__ void __launch_bounds__(512) k_fft_zy(const FFTArgs A) {
+    extern __shared__ float2 plane[];  // [n][n/2+1]
+    constexpr int N = 32 * R, NH = N / 2 + 1;
+    const int x = blockIdx.x;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const LaneTw T = lane_twiddles<R>(lane, A.tw);
+    for (int y = w; y < N; y += nw) {
+        float2 v[R];
+        const float *line = A.rho + ((size_t)x * N + y) * N;
+#pragma unroll
+        for (int r = 0; r < R; r++) v[r] = make_float2(line[32 * r + lane], 0.f);
+        warp_fft<R, false>(v, lane, T);
+#pragma unroll
+        for (int k1 = 0; k1 < R; k1++) {
+            const int k = fft_out_index<R>(k1, lane);
+            if (k < NH) plane[y * NH + k] = v[k1];
+        }
+    }
+    __syncthreads();
+    for (int kz = w; kz < NH; kz += nw) {
+        float2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) v[r] = plane[(32 * r + lane) * NH + kz];
+        warp_fft<R, false>(v, lane, T);
+#pragma unroll
+        for (int k1 = 0; k1 < R; k1++) {
+            const int ky = fft_out_index<R>(k1, lane);
+            A.mid1[((size_t)x * N + ky) * NH + kz] = v[k1];
+        }
+    }
+}
+
+template <int R>
+__global__ void __launch_bounds__(256) k_fft_xe(const FFTArgs A) {
+    constexpr int N = 32 * R, NH = N / 2 + 1;
+    __shared__ float2 sline[8][N];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int line_id = blockIdx.x * 8 + w;
+    if (line_id >= N * NH) return;  // warp-uniform; no block barrier below
+    const LaneTw T = lane_twiddles<R>(lane, A.tw);
+    const int ky = line_id / NH, kz = line_id % NH;
+    const size_t stride = (size_t)N * NH;
+    const size_t base = (size_t)ky * NH + kz;
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) v[r] = A.mid1[(32 * r + lane) * stride + base];
+    warp_fft<R, false>(v, lane, T);
+    const float kyv = A.tpl.y * (float)(ky > N / 2 ? ky - N : ky);
+    const float kzv = A.tpl.z * (float)kz;
+    float2 e[3][R];
+#pragma unroll
+    for (int k1 = 0; k1 < R; k1++) {
+        const int kx = fft_out_index<R>(k1, lane);
+        const float kxv = A.tpl.x * (float)(kx > N / 2 ? kx - N : kx);
+        const float G = __ldg(A.green + (size_t)kx * stride + base);
+        const float2 q = v[k1];
+        const float gx = (2 * kx == N) ? 0.f : kxv * G;
+        const float gy = (2 * ky == N) ? 0.f : kyv * G;
+        const float gz = (2 * kz == N) ? 0.f : kzv * G;
+        e[0][k1] = make_float2(-gx * q.y, gx * q.x);
+        e[1][k1] = make_float2(-gy * q.y, gy * q.x);
+        e[2][k1] = make_float2(-gz * q.y, gz * q.x);
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+#pragma unroll
+        for (int k1 = 0; k1 < R; k1++) sline[w][fft_out_index<R>(k1, lane)] = e[d][k1];
+        __syncwarp();
+        float2 u[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) u[r] = sline[w][32 * r + lane];
+        __syncwarp();
+        warp_fft<R, true>(u, lane, T);
+        float2 *out = A.mid2 + (size_t)d * N * stride;
+#pragma unroll
+        for (int k1 = 0; k1 < R; k1++) out[fft_out_index<R>(k1, lane) * stride + base] = u[k1];
+    }
+}
+
+// one block per (x plane, field component): inverse along y for every kz,
+// then the real inverse along z; component d of the float4 field is written
+template <int R>
+__global__ void __launch_bounds__(512) k_ifft_yz(const FFTArgs A) {
+    extern __shared__ float2 plane[];  // [n][n/2+1]
+    constexpr int N = 32 * R, NH = N / 2 + 1;
+    const int x = blockIdx.x, d = blockIdx.y;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const LaneTw T = lane_twiddles<R>(lane, A.tw);
+    const size_t stride = (size_t)N * NH;
+    const float2 *src0 = A.mid2 + (size_t)d * N * stride + (size_t)x * stride;
+    for (int kz = w; kz < NH; kz += nw) {
+        float2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) v[r] = src0[(size_t)(32 * r + lane) * NH + kz];
+        warp_fft<R, true>(v, lane, T);
+#pragma unroll
+        for (int k1 = 0; k1 < R; k1++) plane[fft_out_index<R>(k1, lane) * NH + kz] = v[k1];
+    }
+    __syncthreads();
+    float *e = reinterpret_cast<float *>(A.e4) + d;
+    for (int y = w; y < N; y += nw) {
+        const float2 *row = plane + y * NH;
+        float2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int n = 32 * r + lane;
+            float2 X;
+            if (n == 0 || n == N / 2) {
+                X = make_float2(row[n].x, 0.f);
+            } else if (n < N / 2) {
+                X = row[n];
+            } else {
+                const float2 c = row[N - n];
+                X = make_float2(c.x, -c.y);
+            }
+            v[r] = X;
+        }
+        warp_fft<R, true>(v, lane, T);
+        const size_t base = ((size_t)x * N + y) * N;
+#pragma unroll
+        for (int k1 = 0; k1 < R; k1++) e[4 * (base + fft_out_index<R>(k1, lane))] = v[k1].x;
+    }
+}
+
+// gather on the interleaved field, five lanes per atom (six atoms per warp):
+// lane t sums the 25 points of stencil plane a = t with one 16-byte load per
+// point; the five partial fields are added with shuffles
+template <bool ACC>
+__global__ void k_gather4(const P3MArgs A, const float4 *__restrict__ e4) {
+    const int lane = threadIdx.x & 31;
+    const int t = lane % 5, base = lane - t;
+    const int i = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 6 + lane / 5;
+    const bool valid = lane < 30 && i < A.n;
+    const float q = valid ? A.qs[i] : 0.f;
+    float ex = 0.f, ey = 0.f, ez = 0.f;
+    const P3MGeom &g = A.g;
+    if (q != 0.f) {
+        int3 ng;
+        float3 d;
+        stencil(g, A.xs[i], ng, d);
+        float wx[5], wy[5], wz[5];
+        w5(d.x, wx);
+        w5(d.y, wy);
+        w5(d.z, wz);
+        int pz[5];
+#pragma unroll
+        for (int c = 0; c < 5; c++) pz[c] = wrapi(ng.z + c - 2, g.sz.z);
+        const int px = wrapi(ng.x + t - 2, g.sz.x);
+        const float wa = pick5(wx, t);
+#pragma unroll
+        for (int b = 0; b < 5; b++) {
+            const int py = wrapi(ng.y + b - 2, g.sz.y);
+            const size_t row = ((size_t)px * g.sz.y + py) * g.sz.z;
+            const float wab = wa * wy[b];
+#pragma unroll
+            for (int c = 0; c < 5; c++) {
+                const float w = wab * wz[c];
+                const float4 e = __ldg(e4 + row + pz[c]);
+                ex += w * e.x;
+                ey += w * e.y;
+                ez += w * e.z;
+            }
+        }
+    }
+    // whole warp takes part; lane base of each group of five adds the group
+    float sx = ex, sy = ey, sz = ez;
+#pragma unroll
+    for (int k = 1; k < 5; k++) {
+        const int src = (base + k) & 31;
+        sx += __shfl_sync(0xffffffffu, ex, src);
+        sy += __shfl_sync(0xffffffffu, ey, src);
+        sz += __shfl_sync(0xffffffffu, ez, src);
+    }
+    if (!valid || t != 0) return;
+    float4 *__restrict__ fs = A.fs;
+    float4 f = fs[i];
+    if (q == 0.f) {
+        if (!ACC) fs[i] = make_float4(0.f, 0.f, 0.f, f.w);
+        return;
+    }
+    const float s = g.qunit * q * A.niv;
+    if (ACC) {
+        f.x += s * sx;
+        f.y += s * sy;
+        f.z += s * sz;
+    } else {
+        f.x = s * sx;
+        f.y = s * sy;
+        f.z = s * sz;
+    }
+    fs[i] = f;
+}
+
 }  // namespace
 
 FixChargeEwald::FixChargeEwald(State *s, std::string h, std::string g)
@@ -328,6 +611,11 @@ double FixChargeEwald::findAlpha() {
     return xb;
 }
 
+namespace {
+template <int R>
+int own_fft_setup();
+}  // namespace
+
 int FixChargeEwald::prepareForRun() {
     State &s = *state;
     if (r_cut < 0) r_cut = s.rCut;
@@ -390,21 +678,74 @@ int FixChargeEwald::prepareForRun() {
         }
     }
     MDX_CUDA_TRY(cudaMemcpy(green.p, G.data(), nk * sizeof(float), cudaMemcpyHostToDevice));
+    // own FFT for cubic 32^3 / 64^3 meshes (cuFFT for every other size)
+    own_fft = sz.x == sz.y && sz.y == sz.z && (sz.x == 32 || sz.x == 64);
+    if (own_fft) {
+        if (int e = e4.alloc(ng)) return e;
+        if (int e = tw.alloc(96)) return e;
+        std::vector<float2> h(96);
+        for (int k = 0; k < 32; k++)
+            h[k] = make_float2((float)std::cos(-2.0 * M_PI * k / 32.0), (float)std::sin(-2.0 * M_PI * k / 32.0));
+        for (int k = 0; k < 64; k++)
+            h[32 + k] = make_float2((float)std::cos(-2.0 * M_PI * k / 64.0), (float)std::sin(-2.0 * M_PI * k / 64.0));
+        MDX_CUDA_TRY(cudaMemcpy(tw.p, h.data(), 96 * sizeof(float2), cudaMemcpyHostToDevice));
+        if (int e = sz.x == 64 ? own_fft_setup<2>() : own_fft_setup<1>()) return e;
+    }
     prepared = true;
     return 0;
 }
+
+namespace {
+FFTArgs fft_args(State &s, FixChargeEwald &f) {
+    FFTArgs A{};
+    A.n = f.sz.x;
+    A.rho = f.rho.p;
+    A.mid1 = f.rho_k.p;
+    A.mid2 = f.e_k.p;
+    A.e4 = f.e4.p;
+    A.green = f.green.p;
+    A.tw = f.tw.p;
+    A.tpl = make_float3((float)(6.28318530717958647693 / s.box.Ld.x), (float)(6.28318530717958647693 / s.box.Ld.y),
+                        (float)(6.28318530717958647693 / s.box.Ld.z));
+    return A;
+}
+
+template <int R>
+int own_solve(State &s, FixChargeEwald &f, cudaStream_t st) {
+    constexpr int N = 32 * R, NH = N / 2 + 1;
+    const FFTArgs A = fft_args(s, f);
+    k_fft_zy<R><<<N, 512, (size_t)N * NH * sizeof(float2), st>>>(A);
+    MDX_LAUNCHED();
+    k_fft_xe<R><<<(N * NH + 7) / 8, 256, 0, st>>>(A);
+    MDX_LAUNCHED();
+    k_ifft_yz<R><<<dim3(N, 3), 512, (size_t)N * NH * sizeof(float2), st>>>(A);
+    MDX_LAUNCHED();
+    return 0;
+}
+
+template <int R>
+int own_fft_setup() {
+    constexpr int N = 32 * R, NH = N / 2 + 1;
+    MDX_CUDA_TRY(cudaFuncSetAttribute(k_ifft_yz<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      N * NH * (int)sizeof(float2)));
+    MDX_CUDA_TRY(cudaFuncSetAttribute(k_fft_zy<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      N * NH * (int)sizeof(float2)));
+    return 0;
+}
+}  // namespace
 
 int FixChargeEwald::spread(cudaStream_t st) {
     State &s = *state;
     const size_t ng = (size_t)sz.x * sz.y * sz.z;
     MDX_CUDA_TRY(cudaMemsetAsync(rho.p, 0, ng * sizeof(float), st));
-    k_spread<<<(s.gpd.n + 127) / 128, 128, 0, st>>>(p3m_args(s, *this), nullptr);
+    k_spread5<<<(s.gpd.n + 47) / 48, 256, 0, st>>>(p3m_args(s, *this), nullptr);
     MDX_LAUNCHED();
     return 0;
 }
 
 int FixChargeEwald::solve(cudaStream_t st) {
     State &s = *state;
+    if (own_fft) return sz.x == 64 ? own_solve<2>(s, *this, st) : own_solve<1>(s, *this, st);
     const size_t nk = (size_t)sz.x * sz.y * (sz.z / 2 + 1);
     cufftSetStream(plan_r2c, st);
     cufftSetStream(plan_c2r, st);
@@ -424,6 +765,14 @@ int FixChargeEwald::solve(cudaStream_t st) {
 int FixChargeEwald::gather(bool accumulate, cudaStream_t st) {
     State &s = *state;
     const P3MArgs A = p3m_args(s, *this);
+    if (own_fft) {
+        if (accumulate)
+            k_gather4<true><<<(s.gpd.n + 47) / 48, 256, 0, st>>>(A, e4.p);
+        else
+            k_gather4<false><<<(s.gpd.n + 47) / 48, 256, 0, st>>>(A, e4.p);
+        MDX_LAUNCHED();
+        return 0;
+    }
     if (accumulate)
         k_gather<true><<<(s.gpd.n + 127) / 128, 128, 0, st>>>(A, nullptr);
     else
@@ -519,7 +868,7 @@ int batch_p3m_spread_solve(Batch &b, cudaStream_t st) {
     A.n = b.max_n;
     A.nk = b.max_nk;
     for (auto &c : b.fft) MDX_CUDA_TRY(cudaMemsetAsync(c->rho.p, 0, c->rho.n * sizeof(float), st));
-    k_spread<<<dim3((A.n + 127) / 128, R), 128, 0, st>>>(A, tab);
+    k_spread5<<<dim3((A.n + 47) / 48, R), 256, 0, st>>>(A, tab);
     MDX_LAUNCHED();
     for (auto &c : b.fft) {
         cufftSetStream(c->r2c, st);
