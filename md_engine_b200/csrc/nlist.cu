@@ -228,6 +228,8 @@ __global__ void k_gather(const GridArgs a0, const GridArgs *__restrict__ tab) {
 // exclusions).  COUNT runs pass 1 alone to size the first build.  Also copies
 // the sorted streams back to the primary buffers.
 constexpr int kBuildWarps = 8;
+constexpr int kBuildMaxChunks = 32;  // chunks a warp replays from masks; more are recomputed
+constexpr size_t kBuildDynSmem = 2 * kBuildWarps * kBuildMaxChunks * 32 * sizeof(uint32_t);
 
 struct BuildArgs {
     const float4 *xs2, *vs2, *fs2;
@@ -261,6 +263,10 @@ __global__ void __launch_bounds__(kBuildWarps * 32, 3) k_build_cells(const Build
     __shared__ float4 sh_x[kBuildWarps][32];
     __shared__ uint2 sh_it[kBuildWarps][32];
     __shared__ uint32_t sh_ci[kBuildWarps][32], sh_cn[kBuildWarps][32];
+    // pass-1 hit / interacting bit masks per (warp, chunk of 32 candidates, lane)
+    extern __shared__ uint32_t dyn[];
+    uint32_t *const hmask = dyn;
+    uint32_t *const amask_s = dyn + kBuildWarps * kBuildMaxChunks * 32;
     const CellGrid &g = A.g;
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -317,9 +323,36 @@ __global__ void __launch_bounds__(kBuildWarps * 32, 3) k_build_cells(const Build
         }
         uint32_t *const row_i = A.nlist + (size_t)(i / GP) * A.cap * GP + (i % GP) * TP;
         int base_i = 0, base_n = 0;  // this warp's slice of the row (pass 2)
+        // write one listed pair at the next front (interacting) or back slot
+        // of this warp's slice of atom i's row
+        auto emit = [&](int p, bool act, uint32_t oid, int &ci_, int &cn_) {
+            const int pos = act ? base_i + ci_ : A.cap - 1 - (base_n + cn_);
+            if (base_i + ci_ + base_n + cn_ < A.cap) {
+                uint32_t entry = (uint32_t)p;
+                if (A.use_excl) {
+                    const uint32_t dd = oid - myid + 32u;
+                    uint32_t depth = 0u;
+                    if (dd < 64u) depth = (uint32_t)((w1 >> dd) & 1ull) | ((uint32_t)((w2 >> dd) & 1ull) << 1);
+                    if (far && depth == 0u) {
+                        for (int e = A.excl_start[myid]; e < A.excl_start[myid + 1]; e++) {
+                            const uint32_t x = A.excl_ids[e];
+                            if ((x & kExclMask) == oid) {
+                                depth = x >> 30;
+                                break;
+                            }
+                        }
+                    }
+                    entry |= depth << 30;
+                }
+                row_i[(size_t)(pos / TP) * 32 + (pos % TP)] = entry;
+            }
+            ci_ += act ? 1 : 0;
+            cn_ += act ? 0 : 1;
+        };
         for (int pass = 0; pass < (COUNT ? 1 : 2); pass++) {
             const bool write = pass == 1;
             int ci = 0, cn = 0;
+            int nchunk = 0;
             for (int r = wib; r < side * side; r += kBuildWarps) {
                 const int kx = cx - m + r / side, ky = cy - m + r % side;
                 const int kxw = kx < 0 ? kx + g.ns.x : (kx >= g.ns.x ? kx - g.ns.x : kx);
@@ -362,16 +395,35 @@ __global__ void __launch_bounds__(kBuildWarps * 32, 3) k_build_cells(const Build
                     kz = kend + 1;
                     for (int p0 = pbeg; p0 < pend; p0 += 32) {
                         const int nc = min(32, pend - p0);
+                        const int chk = nchunk++;  // warp-uniform
+                        const bool replay = !COUNT && write && chk < kBuildMaxChunks;
                         __syncwarp();
                         if (lane < nc) {
                             const int p = p0 + lane;
-                            const float4 pj = A.xs2[p];
-                            shx[lane] = make_float4(__fadd_rn(pj.x, sx), __fadd_rn(pj.y, sy), __fadd_rn(pj.z, sz),
-                                                    (A.part_q && A.ljmask) ? A.qs2[p] : 0.f);
-                            shi[lane] = make_uint2(A.use_excl ? A.ids2[p] : 0u, (uint32_t)type_of(pj));
+                            if (!replay) {
+                                const float4 pj = A.xs2[p];
+                                shx[lane] = make_float4(__fadd_rn(pj.x, sx), __fadd_rn(pj.y, sy), __fadd_rn(pj.z, sz),
+                                                        (A.part_q && A.ljmask) ? A.qs2[p] : 0.f);
+                                shi[lane] = make_uint2(A.use_excl ? A.ids2[p] : 0u, (uint32_t)type_of(pj));
+                            } else if (A.use_excl) {
+                                shi[lane] = make_uint2(A.ids2[p], 0u);
+                            }
                         }
                         __syncwarp();
                         if (!valid) continue;
+                        if (replay) {
+                            // pass 2 from the pass-1 bit masks: only the hits are visited
+                            uint32_t hm = hmask[(wib * kBuildMaxChunks + chk) * 32 + lane];
+                            const uint32_t am = amask_s[(wib * kBuildMaxChunks + chk) * 32 + lane];
+                            while (hm) {
+                                const int k = __ffs(hm) - 1;
+                                hm &= hm - 1u;
+                                const bool act = (am >> k) & 1u;
+                                emit(p0 + k, act, A.use_excl ? shi[k].x : 0u, ci, cn);
+                            }
+                            continue;
+                        }
+                        uint32_t hm = 0u, am = 0u;
 #pragma unroll 4
                         for (int k = 0; k < nc; k++) {
                             const float4 cj = shx[k];
@@ -388,28 +440,20 @@ __global__ void __launch_bounds__(kBuildWarps * 32, 3) k_build_cells(const Build
                                 act = ((amask >> it.y) & 1u) != 0u;
                                 if (!act && A.part_q) act = qi * cj.w != 0.f;
                             }
-                            if (write) {
-                                const int pos = act ? base_i + ci : A.cap - 1 - (base_n + cn);
-                                if (base_i + ci + base_n + cn < A.cap) {
-                                    uint32_t entry = (uint32_t)p;
-                                    if (A.use_excl) {
-                                        const uint32_t dd = it.x - myid + 32u;
-                                        uint32_t depth = 0u;
-                                        if (dd < 64u)
-                                            depth = (uint32_t)((w1 >> dd) & 1ull) | ((uint32_t)((w2 >> dd) & 1ull) << 1);
-                                        if (far && depth == 0u) {
-                                            for (int e = A.excl_start[myid]; e < A.excl_start[myid + 1]; e++) {
-                                                const uint32_t x = A.excl_ids[e];
-                                                if ((x & kExclMask) == it.x) { depth = x >> 30; break; }
-                                            }
-                                        }
-                                        entry |= depth << 30;
-                                    }
-                                    row_i[(size_t)(pos / TP) * 32 + (pos % TP)] = entry;
-                                }
+                            if (!COUNT && !write) {
+                                hm |= 1u << k;
+                                am |= (act ? 1u : 0u) << k;
                             }
-                            ci += act ? 1 : 0;
-                            cn += act ? 0 : 1;
+                            if (write) {
+                                emit(p, act, it.x, ci, cn);
+                            } else {
+                                ci += act ? 1 : 0;
+                                cn += act ? 0 : 1;
+                            }
+                        }
+                        if (!COUNT && !write && chk < kBuildMaxChunks) {
+                            hmask[(wib * kBuildMaxChunks + chk) * 32 + lane] = hm;
+                            amask_s[(wib * kBuildMaxChunks + chk) * 32 + lane] = am;
                         }
                     }
                 }
@@ -538,7 +582,7 @@ BuildArgs build_args(State &s, const CellGrid &g, float cutsq) {
 template <int T>
 void launch_build(State &s, const CellGrid &g, float cutsq) {
     const BuildArgs A = build_args(s, g, cutsq);
-    k_build_cells<T, false><<<A.ncell, kBuildWarps * 32, 0, s.stream>>>(A, nullptr);
+    k_build_cells<T, false><<<A.ncell, kBuildWarps * 32, kBuildDynSmem, s.stream>>>(A, nullptr);
     MDX_LAUNCHED();
 }
 
@@ -646,7 +690,23 @@ int nlist_set_interactions(State &s) {
 
 // Grid set-up (GridGPU::setBounds, GridGPU.cu:46-66): cells of width
 // >= cut/m, m = 2 when the box allows 2m+1 cells per side, else 1.
+static int build_smem_setup() {
+    static bool done[64] = {false};
+    int dev = 0;
+    MDX_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 64 && done[dev]) return 0;
+    MDX_CUDA_TRY(cudaFuncSetAttribute(k_build_cells<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBuildDynSmem));
+    MDX_CUDA_TRY(cudaFuncSetAttribute(k_build_cells<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBuildDynSmem));
+    MDX_CUDA_TRY(cudaFuncSetAttribute(k_build_cells<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBuildDynSmem));
+    MDX_CUDA_TRY(cudaFuncSetAttribute(k_build_cells<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBuildDynSmem));
+    MDX_CUDA_TRY(cudaFuncSetAttribute(k_build_cells<16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBuildDynSmem));
+    MDX_CUDA_TRY(cudaFuncSetAttribute(k_build_cells<32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBuildDynSmem));
+    if (dev < 64) done[dev] = true;
+    return 0;
+}
+
 int nlist_init(State &s) {
+    if (int e = build_smem_setup()) return e;
     GridGPU &gr = s.grid;
     gr.cut = (float)((double)(float)s.maxRCut() + s.padding);
     gr.skin = (float)s.padding;
@@ -810,12 +870,12 @@ int batch_nlist_rebuild(Batch &b) {
     k_gather<<<nb, 256, 0, st>>>(A, tg);
     const dim3 cb(b.max_cell, R);
     switch (s0.grid.team) {
-        case 1: k_build_cells<1, false><<<cb, kBuildWarps * 32, 0, st>>>(B, tb); break;
-        case 2: k_build_cells<2, false><<<cb, kBuildWarps * 32, 0, st>>>(B, tb); break;
-        case 4: k_build_cells<4, false><<<cb, kBuildWarps * 32, 0, st>>>(B, tb); break;
-        case 8: k_build_cells<8, false><<<cb, kBuildWarps * 32, 0, st>>>(B, tb); break;
-        case 16: k_build_cells<16, false><<<cb, kBuildWarps * 32, 0, st>>>(B, tb); break;
-        default: k_build_cells<32, false><<<cb, kBuildWarps * 32, 0, st>>>(B, tb); break;
+        case 1: k_build_cells<1, false><<<cb, kBuildWarps * 32, kBuildDynSmem, st>>>(B, tb); break;
+        case 2: k_build_cells<2, false><<<cb, kBuildWarps * 32, kBuildDynSmem, st>>>(B, tb); break;
+        case 4: k_build_cells<4, false><<<cb, kBuildWarps * 32, kBuildDynSmem, st>>>(B, tb); break;
+        case 8: k_build_cells<8, false><<<cb, kBuildWarps * 32, kBuildDynSmem, st>>>(B, tb); break;
+        case 16: k_build_cells<16, false><<<cb, kBuildWarps * 32, kBuildDynSmem, st>>>(B, tb); break;
+        default: k_build_cells<32, false><<<cb, kBuildWarps * 32, kBuildDynSmem, st>>>(B, tb); break;
     }
     g_launches += 7;
     if (int e = batch_rigid_maps(b)) return e;
