@@ -16,6 +16,10 @@
 namespace mdx {
 
 extern uint64_t g_launches;  // kernels launched by this library
+// threads per block of the fused per-molecule step kernels: one warp, so a
+// few thousand molecules spread over as many SMs as possible (each thread's
+// FP64 SETTLE is a long dependent chain)
+constexpr int kMolBlock = 32;
 #define MDX_LAUNCHED() (++::mdx::g_launches)
 
 template <class T>

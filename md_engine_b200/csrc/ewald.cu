@@ -355,7 +355,7 @@ template <int R>
 __device__ __forceinline__ int fft_out_index(int k1, int lane) { return k1 + R * brev5(lane); }
 
 template <int R>
-__global__ void __launch_bounds__(512) k_fft_zy(const FFTArgs A) {
+__global__ void __launch_bounds__(1024) k_fft_zy(const FFTArgs A) {
     extern __shared__ float2 plane[];  // [n][n/2+1]
     constexpr int N = 32 * R, NH = N / 2 + 1;
     const int x = blockIdx.x;
@@ -437,7 +437,7 @@ __global__ void __launch_bounds__(256) k_fft_xe(const FFTArgs A) {
 // one block per (x plane, field component): inverse along y for every kz,
 // then the real inverse along z; component d of the float4 field is written
 template <int R>
-__global__ void __launch_bounds__(512) k_ifft_yz(const FFTArgs A) {
+__global__ void __launch_bounds__(1024) k_ifft_yz(const FFTArgs A) {
     extern __shared__ float2 plane[];  // [n][n/2+1]
     constexpr int N = 32 * R, NH = N / 2 + 1;
     const int x = blockIdx.x, d = blockIdx.y;
@@ -714,11 +714,11 @@ template <int R>
 int own_solve(State &s, FixChargeEwald &f, cudaStream_t st) {
     constexpr int N = 32 * R, NH = N / 2 + 1;
     const FFTArgs A = fft_args(s, f);
-    k_fft_zy<R><<<N, 512, (size_t)N * NH * sizeof(float2), st>>>(A);
+    k_fft_zy<R><<<N, 1024, (size_t)N * NH * sizeof(float2), st>>>(A);
     MDX_LAUNCHED();
     k_fft_xe<R><<<(N * NH + 7) / 8, 256, 0, st>>>(A);
     MDX_LAUNCHED();
-    k_ifft_yz<R><<<dim3(N, 3), 512, (size_t)N * NH * sizeof(float2), st>>>(A);
+    k_ifft_yz<R><<<dim3(N, 3), 1024, (size_t)N * NH * sizeof(float2), st>>>(A);
     MDX_LAUNCHED();
     return 0;
 }

@@ -94,9 +94,11 @@ __device__ void settle_pos(const RigidConsts &rc, const Box &box, double dt, con
     double3 ax3 = crossd(b0v, c0v);
     double3 ax1 = crossd(a1, ax3);
     double3 ax2 = crossd(ax3, ax1);
-    ax1 /= lend(ax1);
-    ax2 /= lend(ax2);
-    ax3 /= lend(ax3);
+    // unit axes: one reciprocal square root each instead of a square root
+    // and three divisions
+    ax1 = ax1 * rsqrt(dotd(ax1, ax1));
+    ax2 = ax2 * rsqrt(dotd(ax2, ax2));
+    ax3 = ax3 * rsqrt(dotd(ax3, ax3));
     auto rot = [&](double3 u) { return make_double3(dotd(ax1, u), dotd(ax2, u), dotd(ax3, u)); };
     const double3 rb0 = rot(b0v), rc0 = rot(c0v), ra1 = rot(a1), rb1 = rot(b1), rc1 = rot(c1);
     const double sinPhi = ra1.z / ra;
@@ -175,7 +177,7 @@ __device__ __forceinline__ float4 msite(const RigidConsts &rc, const Box &box, c
     return make_float4(m.x, m.y, m.z, w);
 }
 
-int rigid_blocks(int nmol) { return (nmol + 127) / 128; }
+int rigid_blocks(int nmol) { return (nmol + kMolBlock - 1) / kMolBlock; }
 
 // Arguments of the per-molecule kernels for one system: a0 (single system)
 // or tab[blockIdx.y] (batched replicas; a0 then only sizes the grid).
@@ -319,9 +321,14 @@ __device__ void finish_step(double *partials, int nparts, unsigned int *counter,
     __syncthreads();
     if (!last) return;
     __threadfence();
+    // every thread of the last block sums a fixed strided share of the
+    // partials (L2 reads), then a fixed-order block reduction: deterministic
+    __shared__ double red[32];
+    double acc = 0.0;
+    for (int b = threadIdx.x; b < nparts; b += blockDim.x) acc += __ldcg(partials + b);
+    const double tot_all = block_sum(acc, red);
     if (threadIdx.x == 0) {
-        double tot = 0.0;
-        for (int b = 0; b < nparts; b++) tot += ((volatile double *)partials)[b];
+        const double tot = tot_all;
         *counter = 0u;
         if (ke_out) *ke_out = tot;
         if (nh) {
@@ -742,9 +749,9 @@ int step_first_half(State &s, bool fused) {
     if (r) {
         const MolArgs A = mol_args(s, *r);
         if (nh)
-            k_first_mol<true><<<rigid_blocks(A.nmol), 128, 0, s.stream>>>(A, nullptr);
+            k_first_mol<true><<<rigid_blocks(A.nmol), kMolBlock, 0, s.stream>>>(A, nullptr);
         else
-            k_first_mol<false><<<rigid_blocks(A.nmol), 128, 0, s.stream>>>(A, nullptr);
+            k_first_mol<false><<<rigid_blocks(A.nmol), kMolBlock, 0, s.stream>>>(A, nullptr);
         MDX_LAUNCHED();
     }
     return 0;
@@ -792,7 +799,7 @@ int step_second_half(State &s, bool fused, const float4 *fextra) {
         A.part_off = free_atoms ? ab : 0;
         A.nparts = nparts;
         A.fextra = fextra;
-        k_second_mol<<<mb, 128, 0, s.stream>>>(A, nullptr);
+        k_second_mol<<<mb, kMolBlock, 0, s.stream>>>(A, nullptr);
         MDX_LAUNCHED();
     }
     return 0;
@@ -983,7 +990,7 @@ int batch_rigid_maps(Batch &b) {
 int batch_first_half(Batch &b) {
     MolArgs A;
     if (int e = batch_sizing(b, &A)) return e;
-    k_first_mol<true><<<dim3(A.nblk, (unsigned)b.reps.size()), 128, 0, b.stream>>>(
+    k_first_mol<true><<<dim3(A.nblk, (unsigned)b.reps.size()), kMolBlock, 0, b.stream>>>(
         A, reinterpret_cast<const MolArgs *>(b.tab_first.p));
     MDX_LAUNCHED();
     return 0;
@@ -992,7 +999,7 @@ int batch_first_half(Batch &b) {
 int batch_second_half(Batch &b, bool with_e3b) {
     MolArgs A;
     if (int e = batch_sizing(b, &A)) return e;
-    k_second_mol<<<dim3(A.nblk, (unsigned)b.reps.size()), 128, 0, b.stream>>>(
+    k_second_mol<<<dim3(A.nblk, (unsigned)b.reps.size()), kMolBlock, 0, b.stream>>>(
         A, reinterpret_cast<const MolArgs *>(with_e3b ? b.tab_second.p : b.tab_first.p));
     MDX_LAUNCHED();
     return 0;

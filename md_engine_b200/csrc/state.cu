@@ -255,7 +255,7 @@ int State::prepare() {
         // reduction partials for the per-step kinetic sums (allocated here, never
         // while a graph is being captured)
         const int ab = (gpd.n + 255) / 256;
-        const int mb = rigidFix() ? ((int)rigidFix()->mol_ids.size() + 127) / 128 : 0;
+        const int mb = rigidFix() ? ((int)rigidFix()->mol_ids.size() + kMolBlock - 1) / kMolBlock : 0;
         if (int e = red_partials.alloc(ab + mb + 8)) return e;
         if (int e = rigid_flags_prepare(*this)) return e;
     }
