@@ -222,6 +222,8 @@ class FixChargeEwald : public Fix {
     int spread(cudaStream_t st);   // zero + spread
     int solve(cudaStream_t st);    // FFT, E-field, inverse FFTs
     int gather(bool accumulate, cudaStream_t st);
+    int gather_to(float4 *out, cudaStream_t st);  // reciprocal forces stored into out
+    DBuf<float4> f_recip;                         // per-step reciprocal forces (fused step)
 };
 
 struct E3BParams {  // EvaluatorE3B (EvaluatorE3B.h:9-65), FixE3B.cu:515-593
@@ -467,7 +469,8 @@ int surrogate_compute(State &s, FixE3B &f);
 // rigid + integration (integrate.cu)
 int rigid_update_maps(State &s, FixRigid &r, bool conditional);
 int step_first_half(State &s, bool fused);
-int step_second_half(State &s, bool fused, const float4 *fextra = nullptr);
+int step_second_half(State &s, bool fused, const float4 *fextra = nullptr, const float4 *frecip = nullptr);
+bool has_free_atoms(State &s);
 int rigid_prepare(State &s, FixRigid &r);
 int rigid_hook(State &s, FixRigid &r, int which);
 int kinetic_sum(State &s, double *out);

@@ -112,13 +112,27 @@ __global__ void k_spread5(const P3MArgs a0, const P3MArgs *__restrict__ tab) {
     for (int c = 0; c < 5; c++) pz[c] = wrapi(ng.z + c - 2, g.sz.z);
     const int px = wrapi(ng.x + t - 2, g.sz.x);
     const float cyz = qi * pick5(wx, t);
+    // the five z points of a row lie in two aligned groups of four (the mesh
+    // side is a multiple of 4): two 16-byte vector atomics instead of five
+    const int z0 = pz[0], g0 = z0 & ~3, sh = z0 - g0;
+    const int g1 = (g0 + 4) % g.sz.z;
 #pragma unroll
     for (int b = 0; b < 5; b++) {
         const int py = wrapi(ng.y + b - 2, g.sz.y);
         const float cz = cyz * wy[b];
-        float *row = A.rho + ((size_t)px * g.sz.y + py) * g.sz.z;
+        float w[5];
 #pragma unroll
-        for (int c = 0; c < 5; c++) atomicAdd(row + pz[c], cz * wz[c]);
+        for (int c = 0; c < 5; c++) w[c] = cz * wz[c];
+        float4 v1, v2;
+        switch (sh) {
+            case 0: v1 = make_float4(w[0], w[1], w[2], w[3]); v2 = make_float4(w[4], 0.f, 0.f, 0.f); break;
+            case 1: v1 = make_float4(0.f, w[0], w[1], w[2]); v2 = make_float4(w[3], w[4], 0.f, 0.f); break;
+            case 2: v1 = make_float4(0.f, 0.f, w[0], w[1]); v2 = make_float4(w[2], w[3], w[4], 0.f); break;
+            default: v1 = make_float4(0.f, 0.f, 0.f, w[0]); v2 = make_float4(w[1], w[2], w[3], w[4]); break;
+        }
+        float *row = A.rho + ((size_t)px * g.sz.y + py) * g.sz.z;
+        atomicAdd(reinterpret_cast<float4 *>(row + g0), v1);
+        atomicAdd(reinterpret_cast<float4 *>(row + g1), v2);
     }
 }
 
@@ -679,6 +693,7 @@ int FixChargeEwald::prepareForRun() {
     }
     MDX_CUDA_TRY(cudaMemcpy(green.p, G.data(), nk * sizeof(float), cudaMemcpyHostToDevice));
     // own FFT for cubic 32^3 / 64^3 meshes (cuFFT for every other size)
+    if (int e = f_recip.alloc(std::max(s.gpd.n, 1))) return e;
     own_fft = sz.x == sz.y && sz.y == sz.z && (sz.x == 32 || sz.x == 64);
     if (own_fft) {
         if (int e = e4.alloc(ng)) return e;
@@ -775,6 +790,18 @@ int FixChargeEwald::gather(bool accumulate, cudaStream_t st) {
     }
     if (accumulate)
         k_gather<true><<<(s.gpd.n + 127) / 128, 128, 0, st>>>(A, nullptr);
+    else
+        k_gather<false><<<(s.gpd.n + 127) / 128, 128, 0, st>>>(A, nullptr);
+    MDX_LAUNCHED();
+    return 0;
+}
+
+int FixChargeEwald::gather_to(float4 *out, cudaStream_t st) {
+    State &s = *state;
+    P3MArgs A = p3m_args(s, *this);
+    A.fs = out;
+    if (own_fft)
+        k_gather4<false><<<(s.gpd.n + 47) / 48, 256, 0, st>>>(A, e4.p);
     else
         k_gather<false><<<(s.gpd.n + 127) / 128, 128, 0, st>>>(A, nullptr);
     MDX_LAUNCHED();

@@ -198,6 +198,7 @@ struct MolArgs {
     int nh;
     double *ke_out;
     const float4 *fextra;
+    const float4 *frecip;  // P3M reciprocal forces of every site (may be null)
     int nblk;  // blocks of k_second_mol that carry this system's molecules
 };
 #define MDX_MOL_ARGS const MolArgs A = tab ? tab[blockIdx.y] : a0
@@ -387,6 +388,7 @@ __global__ void k_second_mol(const MolArgs a0, const MolArgs *__restrict__ tab) 
     const float dtf = A.dtf;
     DeviceStatus *st = A.st;
     const float4 *__restrict__ fextra = A.fextra;
+    const float4 *__restrict__ frecip = A.frecip;
     int m = blockIdx.x * blockDim.x + threadIdx.x;
     double mv2 = 0.0;
     if (m < nmol) {
@@ -403,10 +405,22 @@ __global__ void k_second_mol(const MolArgs a0, const MolArgs *__restrict__ tab) 
                 f[k].y += fe.y;
                 f[k].z += fe.z;
             }
+            if (frecip) {
+                const float4 fr = frecip[id3[k]];
+                f[k].x += fr.x;
+                f[k].y += fr.y;
+                f[k].z += fr.z;
+            }
             v[k] = kick(vs[id3[k]], f[k], dtf);
         }
         if (rc.foursite) {
-            const float4 fm = fs[ix.w];
+            float4 fm = fs[ix.w];
+            if (frecip) {
+                const float4 fr = frecip[ix.w];
+                fm.x += fr.x;
+                fm.y += fr.y;
+                fm.z += fr.z;
+            }
             const float4 vm = vs[ix.w];
             const float g = (float)rc.gamma;
             const float3 fOd = f3(fm) * g;
@@ -422,7 +436,7 @@ __global__ void k_second_mol(const MolArgs a0, const MolArgs *__restrict__ tab) 
             vs[ix.w] = make_float4(0.f, 0.f, 0.f, vm.w);
             fs[ix.w] = make_float4(0.f, 0.f, 0.f, fm.w);
         }
-        if (rc.foursite || fextra) {
+        if (rc.foursite || fextra || frecip) {
 #pragma unroll
             for (int k = 0; k < 3; k++) fs[id3[k]] = f[k];
         }
@@ -671,6 +685,7 @@ MolArgs mol_args(State &s, FixRigid &r) {
     A.nh = nh ? 1 : 0;
     A.ke_out = s.red_out.p;
     A.fextra = nullptr;
+    A.frecip = nullptr;
     A.nblk = rigid_blocks(A.nmol);
     return A;
 }
@@ -704,7 +719,7 @@ static uint8_t *rigid_flags(State &s) {
 
 int rigid_flags_prepare(State &s) { return (s.rigidFix() && !rigid_flags(s)) ? MDX_ERR_CUDA : 0; }
 
-static bool has_free_atoms(State &s) {
+bool has_free_atoms(State &s) {
     FixRigid *r = s.rigidFix();
     if (!r) return true;
     size_t members = 0;
@@ -757,7 +772,7 @@ int step_first_half(State &s, bool fused) {
     return 0;
 }
 
-int step_second_half(State &s, bool fused, const float4 *fextra) {
+int step_second_half(State &s, bool fused, const float4 *fextra, const float4 *frecip) {
     const int n = s.gpd.n;
     const float dtf = (float)(0.5 * s.dt * s.units.ftm_to_v);
     FixNoseHoover *nh = s.nhFix();
@@ -799,6 +814,7 @@ int step_second_half(State &s, bool fused, const float4 *fextra) {
         A.part_off = free_atoms ? ab : 0;
         A.nparts = nparts;
         A.fextra = fextra;
+        A.frecip = frecip;
         k_second_mol<<<mb, kMolBlock, 0, s.stream>>>(A, nullptr);
         MDX_LAUNCHED();
     }

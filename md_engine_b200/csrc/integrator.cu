@@ -72,10 +72,15 @@ class IntegratorVerlet {
         const bool e3side = e3 && e3->side_ok && s->rigidFix();
         if (int e = step_first_half(*s, true)) return e;
         if (ew || e3side) MDX_CUDA_TRY(cudaEventRecord(s->ev_fork, s->stream));
+        // all-rigid systems: the gather also runs on the side stream, into a
+        // per-step buffer the second half adds (so it overlaps the pair kernel)
+        const bool recip_side = ew && s->rigidFix() && !has_free_atoms(*s);
         if (ew) {
             MDX_CUDA_TRY(cudaStreamWaitEvent(s->side[0], s->ev_fork, 0));
             if (int e = ew->spread(s->side[0])) return e;
             if (int e = ew->solve(s->side[0])) return e;
+            if (recip_side)
+                if (int e = ew->gather_to(ew->f_recip.p, s->side[0])) return e;
             MDX_CUDA_TRY(cudaEventRecord(s->ev_join[0], s->side[0]));
         }
         if (e3side) {
@@ -93,10 +98,11 @@ class IntegratorVerlet {
             if (int e = e3b_forces(*s, *e3)) return e;
         if (ew) {
             MDX_CUDA_TRY(cudaStreamWaitEvent(s->stream, s->ev_join[0], 0));
-            if (int e = ew->gather(true, s->stream)) return e;
+            if (!recip_side)
+                if (int e = ew->gather(true, s->stream)) return e;
         }
         if (e3side) MDX_CUDA_TRY(cudaStreamWaitEvent(s->stream, s->ev_join[1], 0));
-        return step_second_half(*s, true, e3side ? e3->f_side.p : nullptr);
+        return step_second_half(*s, true, e3side ? e3->f_side.p : nullptr, recip_side ? ew->f_recip.p : nullptr);
     }
     int stepBody() {
         if (mode == 0) return stepFused();
