@@ -75,7 +75,33 @@ RefLayout make_layout(int n, const int *counts, const uint32_t *nbr, int maxn, i
 
 }  // namespace
 
+// optional timing: after the checked run, the same launch(es) g_iters more
+// times between CUDA events; the mean device ms per launch lands in g_ms
+int g_iters = 0;
+float g_ms = 0.f;
+
+template <class F>
+void time_launches(F &&launch) {
+    g_ms = 0.f;
+    if (g_iters <= 0) return;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    launch();  // warm
+    cudaEventRecord(a);
+    for (int k = 0; k < g_iters; k++) launch();
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(&g_ms, a, b);
+    g_ms /= (float)g_iters;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+}
+
 extern "C" {
+
+void ref_set_timing(int iters) { g_iters = iters; }
+float ref_last_ms() { return g_ms; }
 
 // compute_force_iso<EvaluatorLJ|EvaluatorWCA, ..., ChargeEvaluatorEwald|None>
 // on atoms in the given order.  lj_kind 1 LJ, 2 WCA; qcut <= 0: no charges.
@@ -97,21 +123,25 @@ int ref_pair_forces(int n, const float *xs4, const float *qs, const int *counts,
     ChargeEvaluatorEwald ew(alpha, qqr);
     ChargeEvaluatorNone none;
     if (ntpa < 2) return -2;
-    if (lj_kind == 1 && qcut > 0)
-        compute_force_iso<EvaluatorLJ, true, 3, false, ChargeEvaluatorEwald, true, 1><<<blocks, ntpb, smem>>>(
-            n, 1, dx, df, dc, dl, dcum, 32, dp, ntypes, b, c12, c13, c14, nullptr, dq, qcut * qcut, ntpa,
-            EvaluatorLJ(), ew);
-    else if (lj_kind == 1)
-        compute_force_iso<EvaluatorLJ, true, 3, false, ChargeEvaluatorNone, false, 1><<<blocks, ntpb, smem>>>(
-            n, 1, dx, df, dc, dl, dcum, 32, dp, ntypes, b, c12, c13, c14, nullptr, dq, 0.f, ntpa, EvaluatorLJ(), none);
-    else if (lj_kind == 2)
-        compute_force_iso<EvaluatorWCA, true, 3, false, ChargeEvaluatorNone, false, 1><<<blocks, ntpb, smem>>>(
-            n, 1, dx, df, dc, dl, dcum, 32, dp, ntypes, b, c12, c13, c14, nullptr, dq, 0.f, ntpa, EvaluatorWCA(),
-            none);
-    else
-        return -1;
+    if (lj_kind < 1 || lj_kind > 2) return -1;
+    auto launch = [&]() {
+        if (lj_kind == 1 && qcut > 0)
+            compute_force_iso<EvaluatorLJ, true, 3, false, ChargeEvaluatorEwald, true, 1><<<blocks, ntpb, smem>>>(
+                n, 1, dx, df, dc, dl, dcum, 32, dp, ntypes, b, c12, c13, c14, nullptr, dq, qcut * qcut, ntpa,
+                EvaluatorLJ(), ew);
+        else if (lj_kind == 1)
+            compute_force_iso<EvaluatorLJ, true, 3, false, ChargeEvaluatorNone, false, 1><<<blocks, ntpb, smem>>>(
+                n, 1, dx, df, dc, dl, dcum, 32, dp, ntypes, b, c12, c13, c14, nullptr, dq, 0.f, ntpa, EvaluatorLJ(),
+                none);
+        else
+            compute_force_iso<EvaluatorWCA, true, 3, false, ChargeEvaluatorNone, false, 1><<<blocks, ntpb, smem>>>(
+                n, 1, dx, df, dc, dl, dcum, 32, dp, ntypes, b, c12, c13, c14, nullptr, dq, 0.f, ntpa, EvaluatorWCA(),
+                none);
+    };
+    launch();
     cudaError_t e = cudaDeviceSynchronize();
     if (e == cudaSuccess) e = cudaMemcpy(hf.data(), df, n * sizeof(float4), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) time_launches(launch);
     std::memcpy(fs4_out, hf.data(), n * sizeof(float4));
     cudaFree(dx); cudaFree(df); cudaFree(dq); cudaFree(dp); cudaFree(dc); cudaFree(dl); cudaFree(dcum);
     return e == cudaSuccess ? 0 : (int)e;
@@ -146,12 +176,16 @@ int ref_e3b_forces(int natoms, const float *xs4, int nmol, const int *mol4, cons
     const int blocks = NBLOCKTEAM(nmol, ntpb, ntpa);
     const size_t smem = ntpb * 3 * (sizeof(float3) + sizeof(Virial));
     if (ntpa < 2) return -2;
-    compute_E3B_force_twobody<false, true><<<blocks, ntpb, smem>>>(nmol, 1, dm, dx, df, dc, dl, dcum, 32, tot, es, f1,
-                                                                  f2, f3, f4, ct, ntpa, b, nullptr, ev);
-    compute_E3B_force_threebody<false, true><<<blocks, ntpb, smem>>>(nmol, 1, dm, dx, df, dc, dl, dcum, 32, b, tot,
-                                                                    es, f1, f2, f3, f4, ct, nullptr, ntpa, ev);
+    auto launch = [&]() {
+        compute_E3B_force_twobody<false, true><<<blocks, ntpb, smem>>>(nmol, 1, dm, dx, df, dc, dl, dcum, 32, tot, es,
+                                                                      f1, f2, f3, f4, ct, ntpa, b, nullptr, ev);
+        compute_E3B_force_threebody<false, true><<<blocks, ntpb, smem>>>(nmol, 1, dm, dx, df, dc, dl, dcum, 32, b, tot,
+                                                                        es, f1, f2, f3, f4, ct, nullptr, ntpa, ev);
+    };
+    launch();
     cudaError_t e = cudaDeviceSynchronize();
     if (e == cudaSuccess) e = cudaMemcpy(hf.data(), df, natoms * sizeof(float4), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) time_launches(launch);
     std::memcpy(fs4_out, hf.data(), natoms * sizeof(float4));
     cudaFree(dx); cudaFree(df); cudaFree(dm); cudaFree(dc); cudaFree(dl); cudaFree(dcum);
     cudaFree(tot); cudaFree(es); cudaFree(f1); cudaFree(f2); cudaFree(f3); cudaFree(f4); cudaFree(ct);

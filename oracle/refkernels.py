@@ -30,6 +30,8 @@ def lib():
         _L.ref_pair_forces.restype = I
         _L.ref_e3b_forces.argtypes = [I, V, I, V, V, V, I, V, V, I, I, I, V]
         _L.ref_e3b_forces.restype = I
+        _L.ref_set_timing.argtypes = [I]
+        _L.ref_last_ms.restype = F
         _L.ref_lj_force_host.argtypes = [F, F, F, V, V]
         _L.ref_e3b_single_host.argtypes = [F, V]
     return _L
@@ -83,3 +85,14 @@ def e3b_single_host(r):
     o = np.zeros(4, np.float32)
     lib().ref_e3b_single_host(float(r), _p(o))
     return o
+
+
+def timed(fn, iters, *a, **kw):
+    """run fn (pair_forces / e3b_forces) once for its result, then its
+    launch(es) `iters` more times between CUDA events: (result, mean ms)"""
+    lib().ref_set_timing(int(iters))
+    try:
+        out = fn(*a, **kw)
+        return out, float(lib().ref_last_ms())
+    finally:
+        lib().ref_set_timing(0)

@@ -89,3 +89,46 @@ def test_e3b_kernels_match_reference_kernels(oracle):
     fr = R.e3b_forces(_xs4(x, sysd.types), mol, mc, mn, sysd.lo, sysd.L)
     rms = np.sqrt(np.mean(np.sum(fr ** 2, 1)))
     assert np.max(np.linalg.norm(f_e3b - fr, axis=1)) < 2e-3 * rms
+
+
+def test_kernel_times_vs_reference_water4096(oracle):
+    """Times the reference's own pair and E3B kernels (compiled from its
+    source, the NTPB x NTPA sweep of Integrator::tune, Integrator.cu:275-276)
+    against this library's on the same 4,096-molecule water inputs and prints
+    both; the numbers are recorded in profiles/ (this is a measurement, the
+    parity is checked by the tests above)."""
+    sysd = systems.water_tip4p2005(nside=16)
+    st, fx = systems.build_water_state(sysd, rcut=9.0, skin=1.0, grid=64, e3b=True, thermostat=False)
+    st.prepare()
+    st.computeForces()
+    x, _, _ = st.getAtoms()
+    counts, nbr, tags = st.getNeighborList()
+    ent = (nbr.astype(np.uint32) | (tags.astype(np.uint32) << 30))
+    sig = {(0, 0): systems.SIG_OO, (1, 1): 0.0, (0, 1): 0.0, (2, 2): 0.0}
+    eps = {(0, 0): systems.EPS_OO, (1, 1): 0.0, (0, 1): 0.0, (2, 2): 0.0}
+    p = oracle.lj_params(3, sig, eps, 9.0)
+    alpha = fx["ewald"].alpha
+    xs4 = _xs4(x, sysd.types)
+    best = None
+    for ntpb in (64, 128, 256):
+        for ntpa in (4, 8, 16, 32):
+            _, ms = R.timed(R.pair_forces, 50, xs4, sysd.q, counts, ent, _params_flat(p), 3, sysd.lo, sysd.L,
+                            (0.0, 0.0, 0.5), 1, 9.0, alpha, oracle.REAL_UNITS["qqr_to_eng"], ntpb=ntpb, ntpa=ntpa)
+            if ms > 0 and (best is None or ms < best[0]):
+                best = (ms, ntpb, ntpa)
+    ours = st.timeStage("pair", iters=50, flushBytes=0)
+    mol = sysd.molecules
+    o = np.zeros((len(mol), 4), np.float32)
+    o[:, :3] = x[mol[:, 0]]
+    oracle.wrap_f32(o, sysd.lo, sysd.L)
+    mc, mn = oracle.nlist_cells(o, sysd.lo, sysd.L, np.float32(6.2))
+    best3 = None
+    for ntpb in (64, 128, 256):
+        for ntpa in (4, 8, 16, 32):
+            _, ms = R.timed(R.e3b_forces, 50, xs4, mol, mc, mn, sysd.lo, sysd.L, ntpb=ntpb, ntpa=ntpa)
+            if ms > 0 and (best3 is None or ms < best3[0]):
+                best3 = (ms, ntpb, ntpa)
+    ours3 = st.timeStage("e3b", iters=50, flushBytes=0)
+    print(f"\npair: reference {best[0] * 1e3:.1f} us (NTPB {best[1]}, NTPA {best[2]}), this library {ours * 1e3:.1f} us")
+    print(f"E3B: reference {best3[0] * 1e3:.1f} us (NTPB {best3[1]}, NTPA {best3[2]}), this library {ours3 * 1e3:.1f} us")
+    assert best is not None and best3 is not None and ours > 0 and ours3 > 0
