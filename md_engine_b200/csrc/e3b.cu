@@ -120,6 +120,50 @@ __device__ __forceinline__ void pair_force(const E3BParams &p, const PairGeom &g
     else { fa = a2; fb = b2; fc = c2; }
 }
 
+// both molecules' forces of one unordered pair (molecule 1 = lower index)
+__device__ __forceinline__ void pair_force_both(const E3BParams &p, const PairGeom &g, float4 T1, float4 T2,
+                                                float3 &a1, float3 &b1, float3 &c1, float3 &a2, float3 &b2,
+                                                float3 &c2) {
+    const float *e = g.es;
+    a1 = make_float3(0.f, 0.f, 0.f);
+    b1 = a1; c1 = a1; a2 = a1; b2 = a1; c2 = a1;
+    float3 fj;
+    float sc;
+    sc = p.Ea * (T2.y - e[0]);
+    fj = sc * g.fv[1]; a1 -= fj; c2 += fj;
+    sc = p.Ea * (T1.y - e[2]);
+    fj = sc * g.fv[3]; a2 -= fj; c1 += fj;
+    sc = p.Ea * (T2.z - e[1]);
+    fj = sc * g.fv[0]; a1 -= fj; b2 += fj;
+    sc = p.Ea * (T1.z - e[3]);
+    fj = sc * g.fv[2]; a2 -= fj; b1 += fj;
+    sc = p.Eb * (T2.x + T1.y + T1.z - 2.0f * (e[2] + e[3]));
+    fj = sc * g.fv[0]; a1 -= fj; b2 += fj;
+    fj = sc * g.fv[1]; a1 -= fj; c2 += fj;
+    sc = p.Eb * (T1.x + T2.y + T2.z - 2.0f * (e[0] + e[1]));
+    fj = sc * g.fv[2]; a2 -= fj; b1 += fj;
+    fj = sc * g.fv[3]; a2 -= fj; c1 += fj;
+    sc = p.Ec * (T1.x - e[1] - e[0]);
+    fj = sc * g.fv[0]; a1 -= fj; b2 += fj;
+    fj = sc * g.fv[1]; a1 -= fj; c2 += fj;
+    sc = p.Ec * (T2.x - e[2] - e[3]);
+    fj = sc * g.fv[2]; a2 -= fj; b1 += fj;
+    fj = sc * g.fv[3]; a2 -= fj; c1 += fj;
+}
+
+// VEC: one 16-byte atomic (side buffers, whose .w is unused); otherwise three
+// scalar atomics so that .w (the force stream's group-tag bits) is untouched
+template <bool VEC>
+__device__ __forceinline__ void add_force(float4 *f, float3 v) {
+    if (VEC) {
+        atomicAdd(f, make_float4(v.x, v.y, v.z, 0.f));
+    } else {
+        atomicAdd(&f->x, v.x);
+        atomicAdd(&f->y, v.y);
+        atomicAdd(&f->z, v.z);
+    }
+}
+
 // total three-body energy of one unordered pair (EvaluatorE3B.h:251-345)
 __device__ __forceinline__ float pair_energy(const E3BParams &p, const float *e, float4 T1, float4 T2) {
     float s = 0.f, sc;
@@ -309,7 +353,10 @@ __global__ void k_e3b_totals(const E3BArgs a0, const E3BArgs *__restrict__ tab) 
     if (valid && t == 0) {
         totals[m] = make_float4(tx, ty, tz, 0.f);
         if (STORE) {
+            // the forces pass adds into these with atomics
             fs[ix.x] = make_float4(fx, fy, fz, 0.f);
+            fs[ix.y] = make_float4(0.f, 0.f, 0.f, 0.f);
+            fs[ix.z] = make_float4(0.f, 0.f, 0.f, 0.f);
         } else {
             float4 f = fs[ix.x];
             f.x += fx;
@@ -365,18 +412,25 @@ __global__ void k_e3b_forces(const E3BArgs a0, const E3BArgs *__restrict__ tab) 
             const float4 Tj = __ldg(totals + mj);
             const bool first = m < mj;
             PairGeom g;
-            if (first) pair_geom(p, box, mi, mjp, g);
-            else pair_geom(p, box, mjp, mi, g);
             if (ENERGY) {
+                if (first) pair_geom(p, box, mi, mjp, g);
+                else pair_geom(p, box, mjp, mi, g);
                 e3 += 0.5f * (first ? pair_energy(p, g.es, Ti, Tj) : pair_energy(p, g.es, Tj, Ti));
                 continue;
             }
-            float3 da, db, dc;
-            if (first) pair_force(p, g, Ti, Tj, true, da, db, dc);
-            else pair_force(p, g, Tj, Ti, false, da, db, dc);
-            fa += da;
-            fb += db;
-            fc += dc;
+            // forces: each unordered pair once, from its lower-index molecule
+            // (molecule 1, as the reference's i < j); the partner's share is
+            // scattered with vector atomics
+            if (!first) continue;
+            pair_geom(p, box, mi, mjp, g);
+            float3 a1, b1, c1, a2, b2, c2;
+            pair_force_both(p, g, Ti, Tj, a1, b1, c1, a2, b2, c2);
+            fa += a1;
+            fb += b1;
+            fc += c1;
+            add_force<STORE>(fs + jx.x, a2);
+            add_force<STORE>(fs + jx.y, b2);
+            add_force<STORE>(fs + jx.z, c2);
         }
     }
     if (ENERGY) {
@@ -388,24 +442,13 @@ __global__ void k_e3b_forces(const E3BArgs a0, const E3BArgs *__restrict__ tab) 
     fb.x = tsum<T>(fb.x); fb.y = tsum<T>(fb.y); fb.z = tsum<T>(fb.z);
     fc.x = tsum<T>(fc.x); fc.y = tsum<T>(fc.y); fc.z = tsum<T>(fc.z);
     if (valid && t == 0) {
-        float4 f = fs[ix.x];
-        f.x += fa.x; f.y += fa.y; f.z += fa.z;
-        fs[ix.x] = f;
-        if (STORE) {
-            fs[ix.y] = make_float4(fb.x, fb.y, fb.z, 0.f);
-            fs[ix.z] = make_float4(fc.x, fc.y, fc.z, 0.f);
-        } else {
-            f = fs[ix.y];
-            f.x += fb.x; f.y += fb.y; f.z += fb.z;
-            fs[ix.y] = f;
-            f = fs[ix.z];
-            f.x += fc.x; f.y += fc.y; f.z += fc.z;
-            fs[ix.z] = f;
-        }
+        add_force<STORE>(fs + ix.x, fa);
+        add_force<STORE>(fs + ix.y, fb);
+        add_force<STORE>(fs + ix.z, fc);
     }
 }
 
-constexpr int kMolTeam = 8;
+constexpr int kMolTeam = kE3BTeam;
 
 }  // namespace
 

@@ -20,6 +20,9 @@ extern uint64_t g_launches;  // kernels launched by this library
 // few thousand molecules spread over as many SMs as possible (each thread's
 // FP64 SETTLE is a long dependent chain)
 constexpr int kMolBlock = 32;
+// lanes per molecule in the E3B list and kernels (the molecule list is laid
+// out for teams of this size)
+constexpr int kE3BTeam = 16;
 #define MDX_LAUNCHED() (++::mdx::g_launches)
 
 template <class T>

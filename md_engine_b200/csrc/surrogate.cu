@@ -32,6 +32,7 @@ namespace {
 
 using S = E3BSurrogate;
 constexpr int kTeam = 8;      // lanes per molecule in the feature kernel
+constexpr int kListTeam = kE3BTeam;  // team layout of the E3B molecule list
 constexpr float kCut = 5.6f;  // feature cutoff (A)
 constexpr float kPi = 3.14159265358979f;
 
@@ -92,9 +93,10 @@ __global__ void k_features(const FeatArgs A) {
     for (int b = 0; b < 4; b++) mu[b] = shell_mu(ch, b0 + b);
     int cnt = (int)A.mcounts[m];
     cnt = cnt < A.mcap ? cnt : A.mcap;
-    const uint32_t *row = A.mlist + (size_t)(m / G) * A.mcap * G + a * kTeam;
+    constexpr int GL = 32 / kListTeam;
+    const uint32_t *row = A.mlist + (size_t)(m / GL) * A.mcap * GL + (m % GL) * kListTeam;
     for (int k = 0; k < cnt; k++) {
-        const int mj = (int)row[(size_t)(k / kTeam) * 32 + (k % kTeam)];
+        const int mj = (int)row[(size_t)(k / kListTeam) * 32 + (k % kListTeam)];
         const int4 jx = A.mol_idx[mj];
         const int nv = ch == 1 ? 2 : 1;
         for (int v = 0; v < nv; v++) {
