@@ -85,42 +85,8 @@ __device__ __forceinline__ void pair_geom(const E3BParams &p, const Box &box, co
     e3b_ef(p, min_image(box, m1.c - m2.a), g.es[3], g.fv[3]);
 }
 
-// EvaluatorE3B::threeBodyPairForce (EvaluatorE3B.h:145-249); returns the
-// forces on molecule 1's atoms (first) or molecule 2's atoms (!first)
-__device__ __forceinline__ void pair_force(const E3BParams &p, const PairGeom &g, float4 T1, float4 T2, bool first,
-                                           float3 &fa, float3 &fb, float3 &fc) {
-    const float *e = g.es;
-    float3 a1 = make_float3(0.f, 0.f, 0.f), b1 = a1, c1 = a1, a2 = a1, b2 = a1, c2 = a1;
-    float3 fj;
-    float sc;
-    // type A
-    sc = p.Ea * (T2.y - e[0]);
-    fj = sc * g.fv[1]; a1 -= fj; c2 += fj;
-    sc = p.Ea * (T1.y - e[2]);
-    fj = sc * g.fv[3]; a2 -= fj; c1 += fj;
-    sc = p.Ea * (T2.z - e[1]);
-    fj = sc * g.fv[0]; a1 -= fj; b2 += fj;
-    sc = p.Ea * (T1.z - e[3]);
-    fj = sc * g.fv[2]; a2 -= fj; b1 += fj;
-    // type B
-    sc = p.Eb * (T2.x + T1.y + T1.z - 2.0f * (e[2] + e[3]));
-    fj = sc * g.fv[0]; a1 -= fj; b2 += fj;
-    fj = sc * g.fv[1]; a1 -= fj; c2 += fj;
-    sc = p.Eb * (T1.x + T2.y + T2.z - 2.0f * (e[0] + e[1]));
-    fj = sc * g.fv[2]; a2 -= fj; b1 += fj;
-    fj = sc * g.fv[3]; a2 -= fj; c1 += fj;
-    // type C
-    sc = p.Ec * (T1.x - e[1] - e[0]);
-    fj = sc * g.fv[0]; a1 -= fj; b2 += fj;
-    fj = sc * g.fv[1]; a1 -= fj; c2 += fj;
-    sc = p.Ec * (T2.x - e[2] - e[3]);
-    fj = sc * g.fv[2]; a2 -= fj; b1 += fj;
-    fj = sc * g.fv[3]; a2 -= fj; c1 += fj;
-    if (first) { fa = a1; fb = b1; fc = c1; }
-    else { fa = a2; fb = b2; fc = c2; }
-}
-
-// both molecules' forces of one unordered pair (molecule 1 = lower index)
+// EvaluatorE3B::threeBodyPairForce (EvaluatorE3B.h:145-249): the forces on
+// both molecules' atoms of one unordered pair (molecule 1 = lower index)
 __device__ __forceinline__ void pair_force_both(const E3BParams &p, const PairGeom &g, float4 T1, float4 T2,
                                                 float3 &a1, float3 &b1, float3 &c1, float3 &a2, float3 &b2,
                                                 float3 &c2) {
