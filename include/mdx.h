@@ -54,7 +54,10 @@ int mdx_state_set_units(mdx_state *st, int unit_type);
 int mdx_state_set_bounds(mdx_state *st, const double lo[3], const double hi[3]);
 /* State attributes exported at src/State.cpp:1220-1247: keys "rCut",
  * "padding", "dt" (double); "periodicInterval", "nThreadPerAtom",
- * "nThreadPerBlock", "turn" (int) */
+ * "nThreadPerBlock", "turn" (int).  Tunables of this library's list build
+ * (0 = automatic, the default): "gridStencil" (cells of at least
+ * (rCut + padding) / gridStencil, 1..4), "gridHomeGroup" (2 or 4 home atoms
+ * tested at once per warp).  Read-only: "nlistCapacity", "cellsPerSide". */
 int mdx_state_set_double(mdx_state *st, const char *key, double value);
 int mdx_state_get_double(mdx_state *st, const char *key, double *value);
 int mdx_state_set_int(mdx_state *st, const char *key, int64_t value);

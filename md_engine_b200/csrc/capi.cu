@@ -117,6 +117,8 @@ int mdx_state_set_int(mdx_state *st, const char *key, int64_t v) {
     if (k == "periodicInterval") s.periodicInterval = (int)v;
     else if (k == "nThreadPerAtom") s.nThreadPerAtom = (int)v;
     else if (k == "nThreadPerBlock") s.nThreadPerBlock = (int)v;
+    else if (k == "gridStencil") s.gridStencil = (int)v;
+    else if (k == "gridHomeGroup") s.gridHomeGroup = (int)v;
     else if (k == "turn") s.turn = v;
     else {
         set_error(MDX_ERR_ARG, "unknown int key '%s'", key);
@@ -136,6 +138,8 @@ int mdx_state_get_int(mdx_state *st, const char *key, int64_t *v) {
     else if (k == "turn") *v = s.turn;
     else if (k == "nlistCapacity") *v = s.grid.cap;
     else if (k == "cellsPerSide") *v = s.grid.ns.x;
+    else if (k == "gridStencil") *v = s.grid.m;
+    else if (k == "gridHomeGroup") *v = s.grid.home_group;
     else {
         set_error(MDX_ERR_ARG, "unknown int key '%s'", key);
         return MDX_ERR_ARG;

@@ -124,6 +124,7 @@ struct GridGPU {
     int cap = 0;         // per-atom capacity (multiple of team)
     int3 ns{0, 0, 0};    // cells per dimension
     int m = 2;           // stencil half width in cells (cells >= cut/m)
+    int home_group = 2;  // home atoms a warp of the list build tests at once
     float cut = 0.f;     // neighCut = rCut + padding (float, as GridGPU)
     float skin = 0.f;    // padding
     DBuf<uint32_t> cell_start, cell_count, cell_fill, block_sums;
@@ -340,6 +341,9 @@ class State {
     int64_t turn = 0;
     int periodicInterval = 50;
     int nThreadPerAtom = 0, nThreadPerBlock = 256;  // 0 = automatic team size
+    // list build tunables, 0 = automatic: cells of >= cut/gridStencil (1..4),
+    // home atoms tested at once per warp (2 or 4)
+    int gridStencil = 0, gridHomeGroup = 0;
     float specialNeighborCoefs[3] = {0.f, 0.f, 0.5f};
     double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
     bool bounds_set = false;

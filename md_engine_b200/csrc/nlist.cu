@@ -8,8 +8,8 @@
 //    kernel of the rebuild group reads DeviceStatus::rebuild and returns
 //    immediately when no rebuild is due, so the group can sit inside a
 //    captured CUDA graph.
-//  * search cells are >= cut/m wide (m = 2: a 5x5x5 stencil walked as 25
-//    contiguous z-rows) instead of >= cut with 27 cells; the atoms tested are
+//  * search cells are >= cut/m wide (m <= 4: a (2m+1)^3 stencil walked as
+//    (2m+1)^2 contiguous z-rows) instead of >= cut with 27 cells; the atoms tested are
 //    a superset of every pair within cut, and each pair is tested once with
 //    the minimum-image shift, so the pair set is unchanged.
 //  * atoms are ordered by (cell, type, id) -- deterministic -- instead of the
@@ -21,6 +21,7 @@
 // 518-522): d = (x_j + shift) - x_i, r2 = dot(d, d) as nvcc contracts it,
 // fma(dz, dz, fma(dy, dy, dx*dx)), pair kept iff r2 < cut*cut (float).
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <vector>
 
@@ -212,24 +213,30 @@ __global__ void k_gather(const GridArgs a0, const GridArgs *__restrict__ tab) {
 }
 
 // assignNeighbors / assignFromCell (GridGPU.cu:482-734) with the exclusion
-// lookup of addExclusion (GridGPU.cu:466-478), one block of kBuildWarps warps
-// per home cell.  Lane l of every warp owns home atom l of the cell (chunks of
-// 32 for fuller cells); the 25 stencil rows are dealt round-robin to the
-// warps.  For each of its rows a warp stages 32 candidates at a time in shared
-// memory, already shifted by the periodic image (x_j + shift, the reference's
-// first rounding), and each lane tests all of them against its atom with the
-// reference's predicate.  Rows and z ranges are trimmed to the cells that can
-// hold a point within cut of the chunk's bounding box (conservative margin of
-// 1e-3 cell), so the pair set equals the full stencil's.  Two passes keep the
-// row deterministic: pass 1 counts per (warp, atom), a prefix over the warps
-// gives each warp its slice, pass 2 writes.  Pairs that can interact fill the
-// row from the front, provably zero ones from the back.  Exclusion depths come
-// from the id-window bit planes (the id list only for atoms with far
-// exclusions).  COUNT runs pass 1 alone to size the first build.  Also copies
-// the sorted streams back to the primary buffers.
-constexpr int kBuildWarps = 8;
-constexpr int kBuildMaxChunks = 32;  // chunks a warp replays from masks; more are recomputed
-constexpr size_t kBuildDynSmem = 2 * kBuildWarps * kBuildMaxChunks * 32 * sizeof(uint32_t);
+// lookup of addExclusion (GridGPU.cu:466-478), one warp per home cell.
+// The candidates of the cell -- its (2m+1)^2 stencil rows, each row's z range
+// and each row trimmed to the cells that can hold a point within cut of the
+// home atoms' bounding box (conservative margin of 1e-3 cell) -- are laid out
+// as one sequence of contiguous segments of the sorted streams.  The warp
+// walks that sequence 32 candidates at a time, one candidate per lane,
+// already shifted by its periodic image (x_j + shift, the reference's first
+// rounding), for HG home atoms at once held in registers.  The sequence is
+// first expanded into shared memory (sorted index and image code per
+// candidate, windows of kCandWin) so a chunk costs one shared load; every lane tests
+// its candidate against each of them with the reference's predicate and two
+// ballots give the hit and the "can interact" masks.  The warp owns whole
+// rows, so a single pass writes them: interacting pairs at the front,
+// provably zero ones at the back, each slot from the running counts (the same
+// in every lane) plus a popcount of the lower lanes' hits -- deterministic,
+// and the entries written for one home atom at a time are consecutive slots
+// of its row.  Exclusion depths come from the id-window bit planes (the id
+// list only for atoms with far exclusions).  COUNT counts alone to size the
+// first build.  Also copies the sorted streams back to the primary buffers.
+constexpr int kBuildCellsPerBlock = 4;            // one warp per cell
+constexpr int kStencilMax = 4;                    // largest m (cells >= cut/m)
+constexpr int kBuildSegMax = 2 * (2 * kStencilMax + 1) * (2 * kStencilMax + 1);  // two z segments per row
+constexpr int kCandWin = 2048;                    // expanded candidates per warp and window
+constexpr int kCandIdxBits = 27;                  // sorted index bits of an expanded candidate
 
 struct BuildArgs {
     const float4 *xs2, *vs2, *fs2;
@@ -253,239 +260,296 @@ struct BuildArgs {
     float cutsq;
 };
 
-template <int TP, bool COUNT>
-__global__ void __launch_bounds__(kBuildWarps * 32, 3) k_build_cells(const BuildArgs a0,
-                                                                       const BuildArgs *__restrict__ tab) {
+// exclusion depth of the pair (home id myid, candidate id oid): bit planes of
+// the id window (w, in registers), else the id list of an atom with far
+// exclusions
+__device__ __forceinline__ uint32_t excl_depth(const BuildArgs &A, uint32_t myid, bool far, ulonglong2 w,
+                                               uint32_t oid) {
+    const uint32_t dd = oid - myid + 32u;
+    uint32_t depth = 0u;
+    if (dd < 64u) depth = (uint32_t)((w.x >> dd) & 1ull) | ((uint32_t)((w.y >> dd) & 1ull) << 1);
+    if (far && depth == 0u) {
+        for (int e = A.excl_start[myid]; e < A.excl_start[myid + 1]; e++) {
+            const uint32_t x = A.excl_ids[e];
+            if ((x & kExclMask) == oid) {
+                depth = x >> 30;
+                break;
+            }
+        }
+    }
+    return depth;
+}
+
+template <int TP, int HG, bool COUNT>
+__global__ void __launch_bounds__(kBuildCellsPerBlock * 32) k_build_cells(const BuildArgs a0,
+                                                                            const BuildArgs *__restrict__ tab) {
     const BuildArgs A = tab ? tab[blockIdx.y] : a0;
     if (!COUNT && !A.st->rebuild) return;
-    if ((int)blockIdx.x >= A.ncell) return;
     constexpr int GP = 32 / TP;
-    __shared__ float4 sh_x[kBuildWarps][32];
-    __shared__ uint2 sh_it[kBuildWarps][32];
-    __shared__ uint32_t sh_ci[kBuildWarps][32], sh_cn[kBuildWarps][32];
-    // pass-1 hit / interacting bit masks per (warp, chunk of 32 candidates, lane)
-    extern __shared__ uint32_t dyn[];
-    uint32_t *const hmask = dyn;
-    uint32_t *const amask_s = dyn + kBuildWarps * kBuildMaxChunks * 32;
-    const CellGrid &g = A.g;
+    __shared__ int sh_seg_off_all[kBuildCellsPerBlock][kBuildSegMax + 1];
+    __shared__ int sh_seg_beg_all[kBuildCellsPerBlock][kBuildSegMax];
+    __shared__ uint32_t sh_seg_code_all[kBuildCellsPerBlock][kBuildSegMax];
+    __shared__ uint32_t sh_cand_all[kBuildCellsPerBlock][kCandWin];
+    __shared__ float4 sh_shift[27];  // image shift by code (ix+1) + 3 (iy+1) + 9 (iz+1)
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    const int c = blockIdx.x;
+    if (threadIdx.x < 27) {
+        const int t = threadIdx.x;
+        sh_shift[t] = make_float4((float)(t % 3 - 1) * A.box.L.x, (float)(t / 3 % 3 - 1) * A.box.L.y,
+                                  (float)(t / 9 - 1) * A.box.L.z, 0.f);
+    }
+    __syncthreads();  // the only block-wide barrier: warps own cells from here on
+    const int c = blockIdx.x * kBuildCellsPerBlock + wib;
+    if (c >= A.ncell) return;
+    int *const sh_seg_off = sh_seg_off_all[wib];
+    int *const sh_seg_beg = sh_seg_beg_all[wib];
+    uint32_t *const sh_seg_code = sh_seg_code_all[wib];
+    uint32_t *const sh_cand = sh_cand_all[wib];
+    const CellGrid &g = A.g;
     const int cs = (int)A.cell_start[c], ce = (int)A.cell_start[c + 1];
+    if (ce <= cs) return;
     const int cz = c % g.ns.z, cy = (c / g.ns.z) % g.ns.y, cx = c / (g.ns.z * g.ns.y);
     const int m = A.m, side = 2 * m + 1;
     const float cutsq = A.cutsq;
+    const int cap = A.cap;
+    const bool use_excl = A.use_excl != 0;
+    const bool split = A.ljmask != nullptr;
+    const bool split_q = split && A.part_q;
+    uint32_t *const nlist = A.nlist;
     const float dsx = 1.0f / g.inv_ds.x, dsy = 1.0f / g.inv_ds.y, dsz = 1.0f / g.inv_ds.z;
-    float4 *const shx = sh_x[wib];
-    uint2 *const shi = sh_it[wib];
-    for (int h0 = cs; h0 < ce; h0 += 32) {
-        const int i = h0 + lane;
-        const bool valid = i < ce;
-        float xi = 0.f, yi = 0.f, zi = 0.f, qi = 0.f;
-        uint32_t amask = 0xffffffffu, myid = 0u;
-        unsigned long long w1 = 0ull, w2 = 0ull;
-        bool far = false;
-        if (valid) {
-            const float4 p4 = A.xs2[i];
-            xi = p4.x;
-            yi = p4.y;
-            zi = p4.z;
-            if (A.ljmask) amask = A.ljmask[type_of(p4)];
-            if (A.part_q) qi = A.qs2[i];
-            if (A.use_excl) {
-                myid = A.ids2[i];
-                const ulonglong2 w = A.excl_win[myid];
-                w1 = w.x;
-                w2 = w.y;
-                far = A.excl_far[myid] != 0;
-            }
-            if (!COUNT && wib == 0) {
-                A.xs[i] = p4;
-                A.xs_last[i] = p4;
-                A.vs[i] = A.vs2[i];
-                A.fs[i] = A.fs2[i];
-                A.qs[i] = A.qs2[i];
-                A.ids[i] = A.ids2[i];
-            }
+    const uint32_t lt = (1u << lane) - 1u;
+    // copy the home atoms' sorted streams back; bounding box of their positions
+    float bxl = 3.0e38f, bxh = -3.0e38f, byl = 3.0e38f, byh = -3.0e38f, bzl = 3.0e38f, bzh = -3.0e38f;
+    for (int i = cs + lane; i < ce; i += 32) {
+        const float4 p4 = A.xs2[i];
+        if (!COUNT) {
+            A.xs[i] = p4;
+            A.xs_last[i] = p4;
+            A.vs[i] = A.vs2[i];
+            A.fs[i] = A.fs2[i];
+            A.qs[i] = A.qs2[i];
+            A.ids[i] = A.ids2[i];
         }
-        // chunk bounding box (warp-uniform, identical in every warp)
-        float bxl = valid ? xi : 3.0e38f, bxh = valid ? xi : -3.0e38f;
-        float byl = valid ? yi : 3.0e38f, byh = valid ? yi : -3.0e38f;
-        float bzl = valid ? zi : 3.0e38f, bzh = valid ? zi : -3.0e38f;
+        bxl = fminf(bxl, p4.x);
+        bxh = fmaxf(bxh, p4.x);
+        byl = fminf(byl, p4.y);
+        byh = fmaxf(byh, p4.y);
+        bzl = fminf(bzl, p4.z);
+        bzh = fmaxf(bzh, p4.z);
+    }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            bxl = fminf(bxl, __shfl_xor_sync(0xffffffffu, bxl, o));
-            bxh = fmaxf(bxh, __shfl_xor_sync(0xffffffffu, bxh, o));
-            byl = fminf(byl, __shfl_xor_sync(0xffffffffu, byl, o));
-            byh = fmaxf(byh, __shfl_xor_sync(0xffffffffu, byh, o));
-            bzl = fminf(bzl, __shfl_xor_sync(0xffffffffu, bzl, o));
-            bzh = fmaxf(bzh, __shfl_xor_sync(0xffffffffu, bzh, o));
-        }
-        uint32_t *const row_i = A.nlist + (size_t)(i / GP) * A.cap * GP + (i % GP) * TP;
-        int base_i = 0, base_n = 0;  // this warp's slice of the row (pass 2)
-        // write one listed pair at the next front (interacting) or back slot
-        // of this warp's slice of atom i's row
-        auto emit = [&](int p, bool act, uint32_t oid, int &ci_, int &cn_) {
-            const int pos = act ? base_i + ci_ : A.cap - 1 - (base_n + cn_);
-            if (base_i + ci_ + base_n + cn_ < A.cap) {
-                uint32_t entry = (uint32_t)p;
-                if (A.use_excl) {
-                    const uint32_t dd = oid - myid + 32u;
-                    uint32_t depth = 0u;
-                    if (dd < 64u) depth = (uint32_t)((w1 >> dd) & 1ull) | ((uint32_t)((w2 >> dd) & 1ull) << 1);
-                    if (far && depth == 0u) {
-                        for (int e = A.excl_start[myid]; e < A.excl_start[myid + 1]; e++) {
-                            const uint32_t x = A.excl_ids[e];
-                            if ((x & kExclMask) == oid) {
-                                depth = x >> 30;
-                                break;
-                            }
-                        }
-                    }
-                    entry |= depth << 30;
-                }
-                row_i[(size_t)(pos / TP) * 32 + (pos % TP)] = entry;
-            }
-            ci_ += act ? 1 : 0;
-            cn_ += act ? 0 : 1;
-        };
-        for (int pass = 0; pass < (COUNT ? 1 : 2); pass++) {
-            const bool write = pass == 1;
-            int ci = 0, cn = 0;
-            int nchunk = 0;
-            for (int r = wib; r < side * side; r += kBuildWarps) {
-                const int kx = cx - m + r / side, ky = cy - m + r % side;
-                const int kxw = kx < 0 ? kx + g.ns.x : (kx >= g.ns.x ? kx - g.ns.x : kx);
-                const float sx = kx < 0 ? -A.box.L.x : (kx >= g.ns.x ? A.box.L.x : 0.f);
-                const int kyw = ky < 0 ? ky + g.ns.y : (ky >= g.ns.y ? ky - g.ns.y : ky);
-                const float sy = ky < 0 ? -A.box.L.y : (ky >= g.ns.y ? A.box.L.y : 0.f);
-                // distance from the chunk's box to this row of cells (image
-                // frame), shrunk by the margin
-                const float clx = g.lo.x + (float)kx * dsx;
-                const float cly = g.lo.y + (float)ky * dsy;
-                float dxm = fmaxf(fmaxf(clx - bxh, bxl - (clx + dsx)), 0.f);
-                float dym = fmaxf(fmaxf(cly - byh, byl - (cly + dsy)), 0.f);
-                dxm = fmaxf(dxm - 1e-3f * dsx, 0.f);
-                dym = fmaxf(dym - 1e-3f * dsy, 0.f);
-                const float rz2 = cutsq - dxm * dxm - dym * dym;
-                if (rz2 <= 0.f) continue;
+    for (int o = 16; o > 0; o >>= 1) {
+        bxl = fminf(bxl, __shfl_xor_sync(0xffffffffu, bxl, o));
+        bxh = fmaxf(bxh, __shfl_xor_sync(0xffffffffu, bxh, o));
+        byl = fminf(byl, __shfl_xor_sync(0xffffffffu, byl, o));
+        byh = fmaxf(byh, __shfl_xor_sync(0xffffffffu, byh, o));
+        bzl = fminf(bzl, __shfl_xor_sync(0xffffffffu, bzl, o));
+        bzh = fmaxf(bzh, __shfl_xor_sync(0xffffffffu, bzh, o));
+    }
+    // segment table: lane r builds stencil row r's z segments, rows in
+    // chunks of 32 with the running totals carried
+    int seg_base = 0, cand_base = 0;
+    for (int r0 = 0; r0 < side * side; r0 += 32) {
+        // up to two segments per row (the stencil wraps at most once):
+        // the parts of the z range below, inside and above the box
+        int nseg = 0, b0 = 0, l0 = 0, b1 = 0, l1 = 0;
+        uint32_t cxy = 0u, cz0 = 0u, cz1 = 0u;  // image codes
+        const int r = r0 + lane;
+        if (r < side * side) {
+            const int kx = cx - m + r / side, ky = cy - m + r % side;
+            const int kxw = kx < 0 ? kx + g.ns.x : (kx >= g.ns.x ? kx - g.ns.x : kx);
+            const uint32_t ix = kx < 0 ? 0u : (kx >= g.ns.x ? 2u : 1u);
+            const int kyw = ky < 0 ? ky + g.ns.y : (ky >= g.ns.y ? ky - g.ns.y : ky);
+            const uint32_t iy = ky < 0 ? 0u : (ky >= g.ns.y ? 2u : 1u);
+            cxy = ix + 3u * iy;
+            // distance from the home box to this row of cells (image
+            // frame), shrunk by the margin
+            const float clx = g.lo.x + (float)kx * dsx;
+            const float cly = g.lo.y + (float)ky * dsy;
+            float dxm = fmaxf(fmaxf(clx - bxh, bxl - (clx + dsx)), 0.f);
+            float dym = fmaxf(fmaxf(cly - byh, byl - (cly + dsy)), 0.f);
+            dxm = fmaxf(dxm - 1e-3f * dsx, 0.f);
+            dym = fmaxf(dym - 1e-3f * dsy, 0.f);
+            const float rz2 = cutsq - dxm * dxm - dym * dym;
+            if (rz2 > 0.f) {
                 const float rz = sqrtf(rz2) + 1e-3f * dsz;
                 const int zlo = max(cz - m, (int)floorf((bzl - rz - g.lo.z) * g.inv_ds.z));
                 const int zhi = min(cz + m, (int)floorf((bzh + rz - g.lo.z) * g.inv_ds.z));
                 const int rowbase = (kxw * g.ns.y + kyw) * g.ns.z;
-                // up to two contiguous z segments (the stencil wraps at most once)
-                for (int kz = zlo; kz <= zhi;) {
-                    int kzw, kend;
-                    float sz;
-                    if (kz < 0) {
-                        kzw = kz + g.ns.z;
-                        kend = min(zhi, -1);
-                        sz = -A.box.L.z;
-                    } else if (kz >= g.ns.z) {
-                        kzw = kz - g.ns.z;
-                        kend = zhi;
-                        sz = A.box.L.z;
-                    } else {
-                        kzw = kz;
-                        kend = min(zhi, g.ns.z - 1);
-                        sz = 0.f;
-                    }
-                    const int pbeg = (int)A.cell_start[rowbase + kzw];
-                    const int pend = (int)A.cell_start[rowbase + kzw + (kend - kz) + 1];
-                    kz = kend + 1;
-                    for (int p0 = pbeg; p0 < pend; p0 += 32) {
-                        const int nc = min(32, pend - p0);
-                        const int chk = nchunk++;  // warp-uniform
-                        const bool replay = !COUNT && write && chk < kBuildMaxChunks;
-                        __syncwarp();
-                        if (lane < nc) {
-                            const int p = p0 + lane;
-                            if (!replay) {
-                                const float4 pj = A.xs2[p];
-                                shx[lane] = make_float4(__fadd_rn(pj.x, sx), __fadd_rn(pj.y, sy), __fadd_rn(pj.z, sz),
-                                                        (A.part_q && A.ljmask) ? A.qs2[p] : 0.f);
-                                shi[lane] = make_uint2(A.use_excl ? A.ids2[p] : 0u, (uint32_t)type_of(pj));
-                            } else if (A.use_excl) {
-                                shi[lane] = make_uint2(A.ids2[p], 0u);
-                            }
-                        }
-                        __syncwarp();
-                        if (!valid) continue;
-                        if (replay) {
-                            // pass 2 from the pass-1 bit masks: only the hits are visited
-                            uint32_t hm = hmask[(wib * kBuildMaxChunks + chk) * 32 + lane];
-                            const uint32_t am = amask_s[(wib * kBuildMaxChunks + chk) * 32 + lane];
-                            while (hm) {
-                                const int k = __ffs(hm) - 1;
-                                hm &= hm - 1u;
-                                const bool act = (am >> k) & 1u;
-                                emit(p0 + k, act, A.use_excl ? shi[k].x : 0u, ci, cn);
-                            }
-                            continue;
-                        }
-                        uint32_t hm = 0u, am = 0u;
-#pragma unroll 4
-                        for (int k = 0; k < nc; k++) {
-                            const float4 cj = shx[k];
-                            const float ddx = __fsub_rn(cj.x, xi);
-                            const float ddy = __fsub_rn(cj.y, yi);
-                            const float ddz = __fsub_rn(cj.z, zi);
-                            const float r2 = __fmaf_rn(ddz, ddz, __fmaf_rn(ddy, ddy, __fmul_rn(ddx, ddx)));
-                            const int p = p0 + k;
-                            if (!(r2 < cutsq) || p == i) continue;
-                            bool act = true;
-                            uint2 it;
-                            if (A.ljmask || write) it = shi[k];
-                            if (A.ljmask) {
-                                act = ((amask >> it.y) & 1u) != 0u;
-                                if (!act && A.part_q) act = qi * cj.w != 0.f;
-                            }
-                            if (!COUNT && !write) {
-                                hm |= 1u << k;
-                                am |= (act ? 1u : 0u) << k;
-                            }
-                            if (write) {
-                                emit(p, act, it.x, ci, cn);
+#pragma unroll
+                for (int part = 0; part < 3; part++) {
+                    const int za = part == 0 ? zlo : (part == 1 ? max(zlo, 0) : max(zlo, g.ns.z));
+                    const int ze = part == 0 ? min(zhi, -1) : (part == 1 ? min(zhi, g.ns.z - 1) : zhi);
+                    const int wrap = part == 0 ? g.ns.z : (part == 1 ? 0 : -g.ns.z);
+                    const uint32_t czp = 9u * (uint32_t)part;
+                    if (za <= ze) {
+                        const int pbeg = (int)A.cell_start[rowbase + za + wrap];
+                        const int pend = (int)A.cell_start[rowbase + ze + wrap + 1];
+                        if (pend > pbeg) {
+                            if (nseg == 0) {
+                                b0 = pbeg;
+                                l0 = pend - pbeg;
+                                cz0 = czp;
                             } else {
-                                ci += act ? 1 : 0;
-                                cn += act ? 0 : 1;
+                                b1 = pbeg;
+                                l1 = pend - pbeg;
+                                cz1 = czp;
                             }
+                            nseg++;
                         }
-                        if (!COUNT && !write && chk < kBuildMaxChunks) {
-                            hmask[(wib * kBuildMaxChunks + chk) * 32 + lane] = hm;
-                            amask_s[(wib * kBuildMaxChunks + chk) * 32 + lane] = am;
-                        }
-                    }
-                }
-            }
-            if (pass == 0) {
-                sh_ci[wib][lane] = (uint32_t)ci;
-                sh_cn[wib][lane] = (uint32_t)cn;
-                __syncthreads();
-                uint32_t ti = 0u, tn = 0u;
-                for (int w = 0; w < kBuildWarps; w++) {
-                    const uint32_t a = sh_ci[w][lane], b = sh_cn[w][lane];
-                    if (w < wib) {
-                        base_i += (int)a;
-                        base_n += (int)b;
-                    }
-                    ti += a;
-                    tn += b;
-                }
-                if (valid && wib == 0) {
-                    const uint32_t cnt = ti + tn;
-                    if (COUNT) {
-                        atomicMax(&A.st->max_neighbors, cnt);
-                    } else {
-                        A.counts[i] = cnt;
-                        A.counts_int[i] = ti;
-                        if (cnt > (uint32_t)A.cap) atomicOr(&A.st->bits, kStatusNlistOverflow);
-                        atomicMax(&A.st->max_neighbors, cnt);
                     }
                 }
             }
         }
-        __syncthreads();  // sh_ci / sh_cn are reused by the next chunk
+        // inclusive scans of the segment counts and lengths
+        int so = nseg, lo = l0 + l1;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int a = __shfl_up_sync(0xffffffffu, so, o);
+            const int b = __shfl_up_sync(0xffffffffu, lo, o);
+            if (lane >= o) {
+                so += a;
+                lo += b;
+            }
+        }
+        const int slot = seg_base + so - nseg, off = cand_base + lo - (l0 + l1);
+        if (nseg > 0) {
+            sh_seg_beg[slot] = b0;
+            sh_seg_off[slot] = off;
+            sh_seg_code[slot] = cxy + cz0;
+        }
+        if (nseg > 1) {
+            sh_seg_beg[slot + 1] = b1;
+            sh_seg_off[slot + 1] = off + l0;
+            sh_seg_code[slot + 1] = cxy + cz1;
+        }
+        seg_base += __shfl_sync(0xffffffffu, so, 31);
+        cand_base += __shfl_sync(0xffffffffu, lo, 31);
+    }
+    if (lane == 0) sh_seg_off[seg_base] = cand_base;  // total candidates
+
+    __syncwarp();
+    const int nseg = seg_base;
+    const int total = cand_base;
+
+    // expand candidates [w0, w0 + wn) of the segment sequence into sh_cand
+    auto expand = [&](int w0, int wn) {
+        __syncwarp();
+        for (int sg = 0; sg < nseg; sg++) {
+            const int off = sh_seg_off[sg];
+            const int lo = max(off, w0), hi = min(sh_seg_off[sg + 1], w0 + wn);
+            const uint32_t beg = (uint32_t)(sh_seg_beg[sg] - off), code = sh_seg_code[sg] << kCandIdxBits;
+            for (int t = lo + lane; t < hi; t += 32) sh_cand[t - w0] = (beg + (uint32_t)t) | code;
+        }
+        __syncwarp();
+    };
+    const bool single = total <= kCandWin;
+    if (single) expand(0, total);
+    // home atoms HG at a time, in registers (warp-uniform values)
+    for (int g0 = cs; g0 < ce; g0 += HG) {
+        float hx[HG], hy[HG], hz[HG], hq[HG];
+        uint32_t hmask[HG], hid[HG];
+        ulonglong2 hwin[HG];
+        bool hfar[HG], hval[HG];
+        int ci[HG], cn[HG];
+#pragma unroll
+        for (int k = 0; k < HG; k++) {
+            const int i = g0 + k;
+            hval[k] = i < ce;
+            const int ii = hval[k] ? i : cs;
+            const float4 p4 = A.xs2[ii];
+            hx[k] = p4.x;
+            hy[k] = p4.y;
+            hz[k] = p4.z;
+            hq[k] = split_q ? A.qs2[ii] : 0.f;
+            hmask[k] = split ? A.ljmask[type_of(p4)] : 0xffffffffu;
+            hid[k] = use_excl ? A.ids2[ii] : 0u;
+            hfar[k] = use_excl ? A.excl_far[hid[k]] != 0 : false;
+            hwin[k] = use_excl ? A.excl_win[hid[k]] : make_ulonglong2(0ull, 0ull);
+            ci[k] = 0;
+            cn[k] = 0;
+        }
+        for (int w0 = 0; w0 < total; w0 += kCandWin) {
+            const int wn = min(kCandWin, total - w0);
+            if (!single) expand(w0, wn);
+            // candidate: sorted index, raw position, image shift, charge, id;
+            // the next chunk's loads are issued before the current one is tested
+            int pn = -1;
+            float4 pjn = make_float4(0.f, 0.f, 0.f, 0.f), shn = pjn;
+            float qn = 0.f;
+            uint32_t idn = 0u;
+            auto fetch = [&](int k) {
+                pn = -1;
+                if (k < wn) {
+                    const uint32_t e = sh_cand[k];
+                    pn = (int)(e & ((1u << kCandIdxBits) - 1u));
+                    shn = sh_shift[e >> kCandIdxBits];
+                    pjn = A.xs2[pn];
+                    if (split_q) qn = A.qs2[pn];
+                    if (use_excl) idn = A.ids2[pn];
+                }
+            };
+            fetch(lane);
+            for (int c0 = 0; c0 < wn; c0 += 32) {
+                const int p = pn;
+                const bool cval = p >= 0;
+                const float cxj = __fadd_rn(pjn.x, shn.x);
+                const float cyj = __fadd_rn(pjn.y, shn.y);
+                const float czj = __fadd_rn(pjn.z, shn.z);
+                const uint32_t tj = (uint32_t)type_of(pjn);
+                const float qj = qn;
+                const uint32_t oid = idn;
+                fetch(c0 + 32 + lane);
+                bool hit[HG], act[HG];
+                uint32_t hm[HG], am[HG];
+#pragma unroll
+                for (int k = 0; k < HG; k++) {
+                    const float ddx = __fsub_rn(cxj, hx[k]);
+                    const float ddy = __fsub_rn(cyj, hy[k]);
+                    const float ddz = __fsub_rn(czj, hz[k]);
+                    const float r2 = __fmaf_rn(ddz, ddz, __fmaf_rn(ddy, ddy, __fmul_rn(ddx, ddx)));
+                    hit[k] = hval[k] && cval && r2 < cutsq && p != g0 + k;
+                    act[k] = true;
+                    if (split) {
+                        act[k] = ((hmask[k] >> tj) & 1u) != 0u;
+                        if (split_q) act[k] = act[k] || hq[k] * qj != 0.f;
+                    }
+                    hm[k] = __ballot_sync(0xffffffffu, hit[k]);
+                    am[k] = split ? __ballot_sync(0xffffffffu, hit[k] && act[k]) : hm[k];
+                }
+#pragma unroll
+                for (int k = 0; k < HG; k++) {
+                    if (!COUNT && hm[k] != 0u) {
+                        const int before = __popc(hm[k] & lt);
+                        const int bi = __popc(am[k] & lt);
+                        const int pos = act[k] ? ci[k] + bi : cap - 1 - cn[k] - (before - bi);
+                        uint32_t entry = (uint32_t)p;
+                        if (use_excl) entry |= excl_depth(A, hid[k], hfar[k], hwin[k], oid) << 30;
+                        const int i = g0 + k;
+                        if (hit[k] && ci[k] + cn[k] + before < cap)
+                            nlist[(size_t)(i / GP) * cap * GP + (i % GP) * TP + (pos / TP) * 32 + pos % TP] = entry;
+                    }
+                    const int na = __popc(am[k]);
+                    ci[k] += na;
+                    cn[k] += __popc(hm[k]) - na;
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < HG; k++) {
+            if (lane == k && hval[k]) {
+                const int i = g0 + k;
+                const uint32_t cnt = (uint32_t)(ci[k] + cn[k]);
+                if (COUNT) {
+                    atomicMax(&A.st->max_neighbors, cnt);
+                } else {
+                    A.counts[i] = cnt;
+                    A.counts_int[i] = (uint32_t)ci[k];
+                    if (cnt > (uint32_t)cap) atomicOr(&A.st->bits, kStatusNlistOverflow);
+                    atomicMax(&A.st->max_neighbors, cnt);
+                }
+            }
+        }
     }
 }
 
@@ -579,21 +643,44 @@ BuildArgs build_args(State &s, const CellGrid &g, float cutsq) {
     return A;
 }
 
-template <int T>
+template <int T, bool COUNT>
+void launch_build_hg(int hg, dim3 grid, cudaStream_t st, const BuildArgs &A, const BuildArgs *tab) {
+    if (hg == 4)
+        k_build_cells<T, 4, COUNT><<<grid, kBuildCellsPerBlock * 32, 0, st>>>(A, tab);
+    else
+        k_build_cells<T, 2, COUNT><<<grid, kBuildCellsPerBlock * 32, 0, st>>>(A, tab);
+}
+
+// grid.x covers ncell (or the largest replica's) cells, one warp each
+template <bool COUNT>
+void launch_build_any(int team, int hg, dim3 grid, cudaStream_t st, const BuildArgs &A, const BuildArgs *tab) {
+    switch (team) {
+        case 1: launch_build_hg<1, COUNT>(hg, grid, st, A, tab); break;
+        case 2: launch_build_hg<2, COUNT>(hg, grid, st, A, tab); break;
+        case 4: launch_build_hg<4, COUNT>(hg, grid, st, A, tab); break;
+        case 8: launch_build_hg<8, COUNT>(hg, grid, st, A, tab); break;
+        case 16: launch_build_hg<16, COUNT>(hg, grid, st, A, tab); break;
+        default: launch_build_hg<32, COUNT>(hg, grid, st, A, tab); break;
+    }
+}
+
+inline dim3 build_grid(int ncell, int nrep) {
+    return dim3((ncell + kBuildCellsPerBlock - 1) / kBuildCellsPerBlock, nrep);
+}
+
 void launch_build(State &s, const CellGrid &g, float cutsq) {
     const BuildArgs A = build_args(s, g, cutsq);
-    k_build_cells<T, false><<<A.ncell, kBuildWarps * 32, kBuildDynSmem, s.stream>>>(A, nullptr);
+    launch_build_any<false>(s.grid.team, s.grid.home_group, build_grid(A.ncell, 1), s.stream, A, nullptr);
     MDX_LAUNCHED();
 }
 
-template <int T>
 void launch_count(State &s, const CellGrid &g, float cutsq) {
     BuildArgs A = build_args(s, g, cutsq);
     A.use_excl = 0;
     A.ljmask = nullptr;
     A.part_q = 0;
     A.cap = 0;
-    k_build_cells<T, true><<<A.ncell, kBuildWarps * 32, 0, s.stream>>>(A, nullptr);
+    launch_build_any<true>(s.grid.team, s.grid.home_group, build_grid(A.ncell, 1), s.stream, A, nullptr);
     MDX_LAUNCHED();
 }
 
@@ -689,24 +776,8 @@ int nlist_set_interactions(State &s) {
 }
 
 // Grid set-up (GridGPU::setBounds, GridGPU.cu:46-66): cells of width
-// >= cut/m, m = 2 when the box allows 2m+1 cells per side, else 1.
-static int build_smem_setup() {
-    static bool done[64] = {false};
-    int dev = 0;
-    MDX_CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 64 && done[dev]) return 0;
-    MDX_CUDA_TRY(cudaFuncSetAttribute(k_build_cells<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBuildDynSmem));
-    MDX_CUDA_TRY(cudaFuncSetAttribute(k_build_cells<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBuildDynSmem));
-    MDX_CUDA_TRY(cudaFuncSetAttribute(k_build_cells<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBuildDynSmem));
-    MDX_CUDA_TRY(cudaFuncSetAttribute(k_build_cells<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBuildDynSmem));
-    MDX_CUDA_TRY(cudaFuncSetAttribute(k_build_cells<16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBuildDynSmem));
-    MDX_CUDA_TRY(cudaFuncSetAttribute(k_build_cells<32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBuildDynSmem));
-    if (dev < 64) done[dev] = true;
-    return 0;
-}
-
+// >= cut/m instead of >= cut, m chosen below.
 int nlist_init(State &s) {
-    if (int e = build_smem_setup()) return e;
     GridGPU &gr = s.grid;
     gr.cut = (float)((double)(float)s.maxRCut() + s.padding);
     gr.skin = (float)s.padding;
@@ -716,10 +787,16 @@ int nlist_init(State &s) {
                   (double)gr.cut, s.box.Ld.x, s.box.Ld.y, s.box.Ld.z);
         return MDX_ERR_UNSUPPORTED;
     }
-    // cells of at least cut/m; m = 2 needs 4 cells per side (a 5-cell stencil
-    // row on a 4-cell ring visits one cell under two images, of which at most
-    // one is within cut < L/2), m = 1 needs 3
-    int m = 2;
+    // cells of at least cut/m, m as large as keeps a mean of 2 atoms per
+    // cell (finer cells trim the candidate volume toward the cutoff sphere).
+    // A (2m+1)-cell stencil row wraps the box at most once when there are
+    // >= 2m cells per side; a cell it visits under two images holds at most
+    // one image within cut < L/2.  m = 1 needs 3 cells per side.
+    if (s.gridStencil < 0 || s.gridStencil > kStencilMax) {
+        set_error(MDX_ERR_ARG, "gridStencil must be 0 (automatic) or 1..%d (got %d)", kStencilMax, s.gridStencil);
+        return MDX_ERR_ARG;
+    }
+    int m = s.gridStencil > 0 ? s.gridStencil : kStencilMax;
     int3 ns;
     for (;; m--) {
         if (m == 0) {
@@ -729,12 +806,23 @@ int nlist_init(State &s) {
         }
         double w = (double)gr.cut / m * (1.0 + 1e-5);
         ns = make_int3((int)(s.box.Ld.x / w), (int)(s.box.Ld.y / w), (int)(s.box.Ld.z / w));
-        const int need = m == 2 ? 4 : 3;
-        if (ns.x >= need && ns.y >= need && ns.z >= need) break;
+        const int need = std::max(3, 2 * m);
+        if (ns.x < need || ns.y < need || ns.z < need) continue;
+        if (m == 1 || s.gridStencil > 0 || (double)s.gpd.n >= 2.0 * ns.x * ns.y * ns.z) break;
+    }
+    if (s.gpd.n >= (1 << kCandIdxBits)) {
+        set_error(MDX_ERR_UNSUPPORTED, "neighbour list build limited to %d atoms (got %d)", 1 << kCandIdxBits, s.gpd.n);
+        return MDX_ERR_UNSUPPORTED;
     }
     gr.m = m;
     gr.ns = ns;
     int ncell = ns.x * ns.y * ns.z;
+    // list build: home atoms tested four at a time when cells hold that many
+    if (s.gridHomeGroup != 0 && s.gridHomeGroup != 2 && s.gridHomeGroup != 4) {
+        set_error(MDX_ERR_ARG, "gridHomeGroup must be 0 (automatic), 2 or 4 (got %d)", s.gridHomeGroup);
+        return MDX_ERR_ARG;
+    }
+    gr.home_group = s.gridHomeGroup ? s.gridHomeGroup : ((double)s.gpd.n >= 4.0 * ncell ? 4 : 2);
     if (int e = gr.cell_start.alloc(ncell + 1)) return e;
     if (int e = gr.cell_count.alloc(ncell)) return e;
     if (int e = gr.cell_fill.alloc(ncell)) return e;
@@ -788,14 +876,7 @@ int nlist_rebuild(State &s, bool force, bool conditional) {
     if (gr.cap == 0) {
         // first build: size the per-atom capacity from a counting sweep
         MDX_CUDA_TRY(cudaMemsetAsync(&s.d_status.p->max_neighbors, 0, sizeof(uint32_t), s.stream));
-        switch (gr.team) {
-            case 1: launch_count<1>(s, g, cutsq); break;
-            case 2: launch_count<2>(s, g, cutsq); break;
-            case 4: launch_count<4>(s, g, cutsq); break;
-            case 8: launch_count<8>(s, g, cutsq); break;
-            case 16: launch_count<16>(s, g, cutsq); break;
-            default: launch_count<32>(s, g, cutsq); break;
-        }
+        launch_count(s, g, cutsq);
         uint32_t mx = 0;
         MDX_CUDA_TRY(cudaMemcpyAsync(&mx, &s.d_status.p->max_neighbors, sizeof(uint32_t), cudaMemcpyDeviceToHost,
                                      s.stream));
@@ -806,14 +887,7 @@ int nlist_rebuild(State &s, bool force, bool conditional) {
         size_t groups = (size_t)(n + (32 / gr.team) - 1) / (32 / gr.team);
         if (int e = gr.nlist.alloc(groups * (size_t)c * (32 / gr.team))) return e;
     }
-    switch (gr.team) {
-        case 1: launch_build<1>(s, g, cutsq); break;
-        case 2: launch_build<2>(s, g, cutsq); break;
-        case 4: launch_build<4>(s, g, cutsq); break;
-        case 8: launch_build<8>(s, g, cutsq); break;
-        case 16: launch_build<16>(s, g, cutsq); break;
-        default: launch_build<32>(s, g, cutsq); break;
-    }
+    launch_build(s, g, cutsq);
     // molecule maps / molecule list of the fixes that keep atom indices
     if (FixRigid *r = s.rigidFix()) {
         if (int e = rigid_update_maps(s, *r, true)) return e;
@@ -868,15 +942,9 @@ int batch_nlist_rebuild(Batch &b) {
     k_scatter<<<nb, 256, 0, st>>>(A, tg);
     k_rank<<<dim3((b.max_cell * 32 + 255) / 256, R), 256, 0, st>>>(A, tg);
     k_gather<<<nb, 256, 0, st>>>(A, tg);
-    const dim3 cb(b.max_cell, R);
-    switch (s0.grid.team) {
-        case 1: k_build_cells<1, false><<<cb, kBuildWarps * 32, kBuildDynSmem, st>>>(B, tb); break;
-        case 2: k_build_cells<2, false><<<cb, kBuildWarps * 32, kBuildDynSmem, st>>>(B, tb); break;
-        case 4: k_build_cells<4, false><<<cb, kBuildWarps * 32, kBuildDynSmem, st>>>(B, tb); break;
-        case 8: k_build_cells<8, false><<<cb, kBuildWarps * 32, kBuildDynSmem, st>>>(B, tb); break;
-        case 16: k_build_cells<16, false><<<cb, kBuildWarps * 32, kBuildDynSmem, st>>>(B, tb); break;
-        default: k_build_cells<32, false><<<cb, kBuildWarps * 32, kBuildDynSmem, st>>>(B, tb); break;
-    }
+    int hg = 2;
+    for (State *r : b.reps) hg = std::max(hg, r->grid.home_group);
+    launch_build_any<false>(s0.grid.team, hg, build_grid(b.max_cell, R), st, B, tb);
     g_launches += 7;
     if (int e = batch_rigid_maps(b)) return e;
     if (s0.e3bFix())

@@ -100,7 +100,7 @@ class State:
     """src/State.h:63-146 -- owns the atoms and the device copy."""
 
     _DOUBLE_KEYS = ("rCut", "padding", "dt")
-    _INT_KEYS = ("periodicInterval", "nThreadPerAtom", "nThreadPerBlock", "turn")
+    _INT_KEYS = ("periodicInterval", "nThreadPerAtom", "nThreadPerBlock", "gridStencil", "gridHomeGroup", "turn")
 
     def __init__(self):
         h = c_void_p()

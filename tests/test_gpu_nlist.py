@@ -125,3 +125,16 @@ def test_water_far_exclusions_bit_exact(oracle):
     excl = oracle.exclusions_from_bonds(len(sysd.pos), water_bonds(sysd.molecules))
     counts = _compare(oracle, st, sysd, 6.5, 1.0, excl=excl)
     assert counts.mean() > 150
+
+
+@pytest.mark.parametrize("stencil,group", [(1, 2), (2, 4), (3, 2), (4, 4)])
+def test_water_pair_set_every_stencil_and_home_group(oracle, stencil, group):
+    """the list-build tunables (cells of >= cut/stencil, home atoms tested
+    per warp) change the candidate walk, never the pair set or its tags"""
+    sysd = systems.water_tip4p2005(nside=10)
+    st, _ = systems.build_water_state(sysd, rcut=9.0, skin=1.0, grid=32)
+    st.gridStencil = stencil
+    st.gridHomeGroup = group
+    excl = oracle.exclusions_from_bonds(len(sysd.pos), water_bonds(sysd.molecules))
+    _compare(oracle, st, sysd, 9.0, 1.0, excl=excl)
+    assert st.gridStencil == stencil and st.gridHomeGroup == group
