@@ -68,6 +68,16 @@ __host__ __device__ inline double3 crossd(double3 a, double3 b) {
     return make_double3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }
 
+// programmatic dependent launch (sm_90+): pdl_trigger lets the next kernel of
+// the stream be scheduled now (without it, once this block exits); pdl_wait
+// blocks until the previous kernel of the stream has completed and its writes
+// are visible.  Both are no-ops for a kernel launched without the
+// programmatic-serialization attribute.  Triggers sit late in a kernel: a
+// dependent scheduled early holds SM slots idle that kernels of other streams
+// (the pair kernel beside the P3M chain) would use.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // minimum image (BoundsGPU::minImage, BoundsGPU.h:91-108)
 __device__ inline float3 min_image(const Box &b, float3 v) {
     v.x -= b.L.x * rintf(v.x * b.invL.x);

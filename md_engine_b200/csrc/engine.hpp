@@ -25,6 +25,30 @@ constexpr int kMolBlock = 32;
 constexpr int kE3BTeam = 16;
 #define MDX_LAUNCHED() (++::mdx::g_launches)
 
+// Programmatic dependent launch for the kernels of the fused step: the kernel
+// may be scheduled while its predecessor in the stream is still running (once
+// every block of that one has called pdl_trigger()); it calls pdl_wait()
+// before touching anything the predecessor writes, which returns when that
+// grid has completed and its memory is visible.  A CUDA graph captured from
+// such launches keeps them as programmatic edges, so consecutive kernels of a
+// step no longer pay a full drain-and-launch gap.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args... args) {
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    MDX_LAUNCHED();
+    return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 template <class T>
 struct DBuf {
     T *p = nullptr;
@@ -214,6 +238,10 @@ class FixChargeEwald : public Fix {
     DBuf<double> energy_acc;
     // own FFT path (cubic 32^3 / 64^3 meshes): field interleaved as float4
     bool own_fft = false;
+    // the charge grid is known to be zero (the library's own FFT clears it as
+    // it reads it; every other user of rho clears it after use): spread()
+    // then needs no memset
+    bool rho_zero = false;
     DBuf<float4> e4;
     DBuf<float2> tw;        // W_32^k then W_64^k
     FixChargeEwald(State *s, std::string h, std::string g);
@@ -310,8 +338,10 @@ class FixRigid : public Fix {
     int setConsts();
 };
 
+constexpr int kNHChain = 10;  // chain links (FixNoseHoover's default chainLength)
 struct NHChain {  // FixNoseHoover chain state (FixNoseHoover.h), FP64
     double vel[10], force[10], mass[10];
+    double inv_mass[10];  // 1 / mass, set with mass
     double ke;       // sum m v^2 * mvv_to_eng
     double T, freq, ndf, kB, dt;
     double mvv_to_eng;

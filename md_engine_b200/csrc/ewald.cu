@@ -89,6 +89,7 @@ __device__ __forceinline__ float pick5(const float w[5], int t) {
 }
 
 __global__ void k_spread5(const P3MArgs a0, const P3MArgs *__restrict__ tab) {
+    pdl_wait();
     MDX_P3M_ARGS;
     const int lane = threadIdx.x & 31;
     const int t = lane % 5;
@@ -303,7 +304,7 @@ P3MArgs p3m_args(State &s, FixChargeEwald &f) {
 // so the gather reads one 16-byte field value per stencil point.
 struct FFTArgs {
     int n;                   // points per side (32 or 64)
-    const float *rho;        // [n][n][n]
+    float *rho;              // [n][n][n]: read, then left zeroed for the next spread
     float2 *mid1;            // [n][n][n/2+1]: after the z and y passes
     float2 *mid2;            // [3][n][n][n/2+1]: E_d after the inverse x pass
     float4 *e4;              // [n][n][n]
@@ -372,14 +373,18 @@ template <int R>
 __global__ void __launch_bounds__(1024) k_fft_zy(const FFTArgs A) {
     extern __shared__ float2 plane[];  // [n][n/2+1]
     constexpr int N = 32 * R, NH = N / 2 + 1;
+    pdl_wait();
     const int x = blockIdx.x;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const LaneTw T = lane_twiddles<R>(lane, A.tw);
     for (int y = w; y < N; y += nw) {
         float2 v[R];
-        const float *line = A.rho + ((size_t)x * N + y) * N;
+        float *line = A.rho + ((size_t)x * N + y) * N;
 #pragma unroll
         for (int r = 0; r < R; r++) v[r] = make_float2(line[32 * r + lane], 0.f);
+        // the charge grid starts the next spread at zero (no memset node)
+#pragma unroll
+        for (int r = 0; r < R; r++) line[32 * r + lane] = 0.f;
         warp_fft<R, false>(v, lane, T);
 #pragma unroll
         for (int k1 = 0; k1 < R; k1++) {
@@ -404,6 +409,7 @@ __global__ void __launch_bounds__(1024) k_fft_zy(const FFTArgs A) {
 template <int R>
 __global__ void __launch_bounds__(256) k_fft_xe(const FFTArgs A) {
     constexpr int N = 32 * R, NH = N / 2 + 1;
+    pdl_wait();
     __shared__ float2 sline[8][N];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int line_id = blockIdx.x * 8 + w;
@@ -454,6 +460,7 @@ template <int R>
 __global__ void __launch_bounds__(1024) k_ifft_yz(const FFTArgs A) {
     extern __shared__ float2 plane[];  // [n][n/2+1]
     constexpr int N = 32 * R, NH = N / 2 + 1;
+    pdl_wait();
     const int x = blockIdx.x, d = blockIdx.y;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const LaneTw T = lane_twiddles<R>(lane, A.tw);
@@ -498,6 +505,7 @@ __global__ void __launch_bounds__(1024) k_ifft_yz(const FFTArgs A) {
 // point; the five partial fields are added with shuffles
 template <bool ACC>
 __global__ void k_gather4(const P3MArgs A, const float4 *__restrict__ e4) {
+    pdl_wait();
     const int lane = threadIdx.x & 31;
     const int t = lane % 5, base = lane - t;
     const int i = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 6 + lane / 5;
@@ -637,6 +645,7 @@ int FixChargeEwald::prepareForRun() {
     const size_t ng = (size_t)sz.x * sz.y * sz.z;
     const size_t nk = (size_t)sz.x * sz.y * (sz.z / 2 + 1);
     if (int e = rho.alloc(ng)) return e;
+    rho_zero = false;  // the first spread clears the grid
     if (int e = rho_k.alloc(nk)) return e;
     if (int e = e_k.alloc(3 * nk)) return e;
     if (int e = e_r.alloc(3 * ng)) return e;
@@ -729,12 +738,10 @@ template <int R>
 int own_solve(State &s, FixChargeEwald &f, cudaStream_t st) {
     constexpr int N = 32 * R, NH = N / 2 + 1;
     const FFTArgs A = fft_args(s, f);
-    k_fft_zy<R><<<N, 1024, (size_t)N * NH * sizeof(float2), st>>>(A);
-    MDX_LAUNCHED();
-    k_fft_xe<R><<<(N * NH + 7) / 8, 256, 0, st>>>(A);
-    MDX_LAUNCHED();
-    k_ifft_yz<R><<<dim3(N, 3), 1024, (size_t)N * NH * sizeof(float2), st>>>(A);
-    MDX_LAUNCHED();
+    MDX_CUDA_TRY(launch_pdl(k_fft_zy<R>, dim3(N), dim3(1024), (size_t)N * NH * sizeof(float2), st, A));
+    f.rho_zero = true;  // k_fft_zy leaves the charge grid zeroed
+    MDX_CUDA_TRY(launch_pdl(k_fft_xe<R>, dim3((N * NH + 7) / 8), dim3(256), 0, st, A));
+    MDX_CUDA_TRY(launch_pdl(k_ifft_yz<R>, dim3(N, 3), dim3(1024), (size_t)N * NH * sizeof(float2), st, A));
     return 0;
 }
 
@@ -752,9 +759,10 @@ int own_fft_setup() {
 int FixChargeEwald::spread(cudaStream_t st) {
     State &s = *state;
     const size_t ng = (size_t)sz.x * sz.y * sz.z;
-    MDX_CUDA_TRY(cudaMemsetAsync(rho.p, 0, ng * sizeof(float), st));
-    k_spread5<<<(s.gpd.n + 47) / 48, 256, 0, st>>>(p3m_args(s, *this), nullptr);
-    MDX_LAUNCHED();
+    if (!rho_zero) MDX_CUDA_TRY(cudaMemsetAsync(rho.p, 0, ng * sizeof(float), st));
+    MDX_CUDA_TRY(launch_pdl(k_spread5, dim3((s.gpd.n + 47) / 48), dim3(256), 0, st, p3m_args(s, *this),
+                            (const P3MArgs *)nullptr));
+    rho_zero = false;
     return 0;
 }
 
@@ -782,10 +790,11 @@ int FixChargeEwald::gather(bool accumulate, cudaStream_t st) {
     const P3MArgs A = p3m_args(s, *this);
     if (own_fft) {
         if (accumulate)
-            k_gather4<true><<<(s.gpd.n + 47) / 48, 256, 0, st>>>(A, e4.p);
+            MDX_CUDA_TRY(launch_pdl(k_gather4<true>, dim3((s.gpd.n + 47) / 48), dim3(256), 0, st, A,
+                                    (const float4 *)e4.p));
         else
-            k_gather4<false><<<(s.gpd.n + 47) / 48, 256, 0, st>>>(A, e4.p);
-        MDX_LAUNCHED();
+            MDX_CUDA_TRY(launch_pdl(k_gather4<false>, dim3((s.gpd.n + 47) / 48), dim3(256), 0, st, A,
+                                    (const float4 *)e4.p));
         return 0;
     }
     if (accumulate)
@@ -800,11 +809,13 @@ int FixChargeEwald::gather_to(float4 *out, cudaStream_t st) {
     State &s = *state;
     P3MArgs A = p3m_args(s, *this);
     A.fs = out;
-    if (own_fft)
-        k_gather4<false><<<(s.gpd.n + 47) / 48, 256, 0, st>>>(A, e4.p);
-    else
+    if (own_fft) {
+        MDX_CUDA_TRY(launch_pdl(k_gather4<false>, dim3((s.gpd.n + 47) / 48), dim3(256), 0, st, A,
+                                (const float4 *)e4.p));
+    } else {
         k_gather<false><<<(s.gpd.n + 127) / 128, 128, 0, st>>>(A, nullptr);
-    MDX_LAUNCHED();
+        MDX_LAUNCHED();
+    }
     return 0;
 }
 
@@ -823,6 +834,10 @@ int ewald_recip_energy(State &s, FixChargeEwald &f, double *out) {
         set_error(MDX_ERR_CUDA, "cufftExecR2C failed");
         return MDX_ERR_CUDA;
     }
+    // leave the charge grid zeroed, as the step's own FFT does (captured
+    // steps spread onto it without clearing it)
+    MDX_CUDA_TRY(cudaMemsetAsync(f.rho.p, 0, (size_t)f.sz.x * f.sz.y * f.sz.z * sizeof(float), s.stream));
+    f.rho_zero = true;
     const size_t nk = (size_t)f.sz.x * f.sz.y * (f.sz.z / 2 + 1);
     MDX_CUDA_TRY(cudaMemsetAsync(f.energy_acc.p, 0, sizeof(double), s.stream));
     k_recip_energy<<<148, 256, 0, s.stream>>>(f.sz, f.rho_k.p, f.green.p, nk, f.energy_acc.p);
@@ -868,6 +883,7 @@ int batch_p3m_prepare(Batch &b) {
         for (int j = 0; j < K; j++) {
             FixChargeEwald *f = b.reps[c.reps[j]]->ewaldFix();
             f->rho.view(c.rho.p + j * ng, ng);
+            f->rho_zero = false;
             f->rho_k.view(c.rho_k.p + j * nk, nk);
             f->e_k.view(c.e_k.p + j * 3 * nk, 3 * nk);
             f->e_r.view(c.e_r.p + j * 3 * ng, 3 * ng);

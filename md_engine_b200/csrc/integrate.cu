@@ -17,40 +17,68 @@
 namespace mdx {
 
 // ---------------------------------------------------------------- NH chain
-// thermostatIntegrate (FixNoseHoover.cu:795-866), nTimesteps = n_ys = 1
-__host__ __device__ double nh_integrate(NHChain &c, bool stepInit) {
+// exp(x) for the chain's arguments, -dt/8 .. -dt/2 times a thermostat
+// velocity (|x| well below 1/64 for any stable run): the Taylor polynomial of
+// degree 8 by Horner's rule (truncation below 1e-22 relative, under FP64
+// rounding), a short dependent chain on the device's serial tail; larger
+// arguments use exp().  Host and device run the same code.
+__host__ __device__ inline double nh_exp(double x) {
+    if (fabs(x) >= 0.015625) return exp(x);
+    double p = 1.0 / 40320.0;
+    p = fma(p, x, 1.0 / 5040.0);
+    p = fma(p, x, 1.0 / 720.0);
+    p = fma(p, x, 1.0 / 120.0);
+    p = fma(p, x, 1.0 / 24.0);
+    p = fma(p, x, 1.0 / 6.0);
+    p = fma(p, x, 0.5);
+    p = fma(p, x, 1.0);
+    return fma(p, x, 1.0);
+}
+
+// thermostatIntegrate (FixNoseHoover.cu:795-866), nTimesteps = n_ys = 1, for
+// a chain of compile-time length N (loops unrolled, so a chain held in
+// registers stays there); C has the fields of NHChain used here.  Divisions
+// by the chain masses are products with their reciprocals.
+template <int N, class C>
+__host__ __device__ __forceinline__ double nh_integrate_n(C &c, bool stepInit) {
     const double nkt = c.ndf * c.kB * c.T;
-    if (!stepInit) c.force[0] = (c.ke - nkt) / c.mass[0];
+    if (!stepInit) c.force[0] = (c.ke - nkt) * c.inv_mass[0];
     const double ts = c.dt;
     const double t2 = 0.5 * ts, t4 = 0.25 * ts, t8 = 0.125 * ts;
-    const int n = c.n;
-    c.vel[n - 1] += t4 * c.force[n - 1];
-    for (int k = n - 2; k > 0; --k) {
-        double pf = exp(-t8 * c.vel[k + 1]);
+    c.vel[N - 1] += t4 * c.force[N - 1];
+#pragma unroll
+    for (int k = N - 2; k > 0; --k) {
+        double pf = nh_exp(-t8 * c.vel[k + 1]);
         c.vel[k] *= pf;
         c.vel[k] += t4 * c.force[k];
         c.vel[k] *= pf;
     }
-    double pf = exp(-t8 * c.vel[1]);
+    double pf = nh_exp(-t8 * c.vel[1]);
     c.vel[0] *= pf;
     c.vel[0] += t4 * c.force[0];
     c.vel[0] *= pf;
-    const double sf = exp(-t2 * c.vel[0]);
+    const double sf = nh_exp(-t2 * c.vel[0]);
     c.ke *= sf * sf;
     c.vel[0] *= pf;
-    c.force[0] = (c.ke - nkt) / c.mass[0];
+    c.force[0] = (c.ke - nkt) * c.inv_mass[0];
     c.vel[0] += t4 * c.force[0];
     c.vel[0] *= pf;
-    for (int k = 1; k < n - 1; ++k) {
-        pf = exp(-t8 * c.vel[k + 1]);
+#pragma unroll
+    for (int k = 1; k < N - 1; ++k) {
+        pf = nh_exp(-t8 * c.vel[k + 1]);
         c.vel[k] *= pf;
-        c.force[k] = (c.mass[k - 1] * c.vel[k - 1] * c.vel[k - 1] - c.kB * c.T) / c.mass[k];
+        c.force[k] = (c.mass[k - 1] * c.vel[k - 1] * c.vel[k - 1] - c.kB * c.T) * c.inv_mass[k];
         c.vel[k] += t4 * c.force[k];
         c.vel[k] *= pf;
     }
-    c.force[n - 1] = (c.mass[n - 2] * c.vel[n - 2] * c.vel[n - 2] - c.kB * c.T) / c.mass[n - 1];
-    c.vel[n - 1] += t4 * c.force[n - 1];
+    c.force[N - 1] = (c.mass[N - 2] * c.vel[N - 2] * c.vel[N - 2] - c.kB * c.T) * c.inv_mass[N - 1];
+    c.vel[N - 1] += t4 * c.force[N - 1];
     return sf;
+}
+
+// the chain has kNHChain links (FixNoseHoover's default chain length)
+__host__ __device__ double nh_integrate(NHChain &c, bool stepInit) {
+    return nh_integrate_n<kNHChain>(c, stepInit);
 }
 
 // device copy: [0] = state after stepInit of the coming step ("next"),
@@ -249,6 +277,7 @@ __global__ void k_first_atoms(int n, float4 *__restrict__ xs, float4 *__restrict
 // per-molecule fused: NH rescale + save_prev_val + nve_v + nve_x + SETTLE + M-site
 template <bool NH>
 __global__ void k_first_mol(const MolArgs a0, const MolArgs *__restrict__ tab) {
+    pdl_wait();
     MDX_MOL_ARGS;
     int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= A.nmol) return;
@@ -308,6 +337,23 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
     return r;  // valid in thread 0
 }
 
+// the time-dependent part of a chain, held in registers by the last block
+struct NHRegs {
+    double vel[kNHChain], force[kNHChain], mass[kNHChain], inv_mass[kNHChain];
+    double ke, ndf, kB, T, dt;
+};
+
+__device__ __forceinline__ void store_chain(NHChain &d, const NHRegs &c, double last_ke, double scale) {
+#pragma unroll
+    for (int k = 0; k < kNHChain; k++) {
+        d.vel[k] = c.vel[k];
+        d.force[k] = c.force[k];
+    }
+    d.ke = c.ke;
+    d.last_ke = last_ke;
+    d.scale = scale;
+}
+
 // Last-block epilogue: fixed-order FP64 sum of the block partials, then the
 // Nose-Hoover stepFinal + next stepInit on one thread, and the turn counter.
 // nparts partials are summed; the counter target is this kernel's grid size
@@ -333,15 +379,27 @@ __device__ void finish_step(double *partials, int nparts, unsigned int *counter,
         *counter = 0u;
         if (ke_out) *ke_out = tot;
         if (nh) {
-            NHChain c = chain[0];
-            c.ke = tot * c.mvv_to_eng;
-            c.last_ke = c.ke;
-            const double sf1 = nh_integrate(c, false);  // stepFinal
-            c.scale = sf1;
-            chain[1] = c;
-            const double sf2 = nh_integrate(c, true);   // stepInit of the next step
-            c.scale = sf1 * sf2;
-            chain[0] = c;
+            // the chain in registers (a copy of the struct would sit in local
+            // memory on this serial path); constants stay in chain[0/1]
+            NHRegs c;
+            const NHChain &g = chain[0];
+#pragma unroll
+            for (int k = 0; k < kNHChain; k++) {
+                c.vel[k] = g.vel[k];
+                c.force[k] = g.force[k];
+                c.mass[k] = g.mass[k];
+                c.inv_mass[k] = g.inv_mass[k];
+            }
+            c.ndf = g.ndf;
+            c.kB = g.kB;
+            c.T = g.T;
+            c.dt = g.dt;
+            c.ke = tot * g.mvv_to_eng;
+            const double last_ke = c.ke;
+            const double sf1 = nh_integrate_n<kNHChain>(c, false);  // stepFinal
+            store_chain(chain[1], c, last_ke, sf1);
+            const double sf2 = nh_integrate_n<kNHChain>(c, true);   // stepInit of the next step
+            store_chain(chain[0], c, last_ke, sf1 * sf2);
         }
         st->turn += 1;
     }
@@ -375,6 +433,7 @@ __global__ void k_second_atoms(int n, float4 *__restrict__ vs, const float4 *__r
 // fextra (may be null): per-molecule-atom forces computed beside the pair
 // kernel (E3B), indexed like fs, merged into O/H1/H2 here
 __global__ void k_second_mol(const MolArgs a0, const MolArgs *__restrict__ tab) {
+    pdl_wait();
     MDX_MOL_ARGS;
     if ((int)blockIdx.x >= A.nblk) return;  // the whole block: not counted
     __shared__ double sh[32];
@@ -454,6 +513,9 @@ __global__ void k_second_mol(const MolArgs a0, const MolArgs *__restrict__ tab) 
     }
     const double b = block_sum(mv2, sh);
     if (threadIdx.x == 0) A.partials[A.part_off + blockIdx.x] = b;
+    // the next step's first half may be scheduled now: it waits for this
+    // grid (the last block's chain update included) before reading anything
+    pdl_trigger();
     finish_step(A.partials, A.nparts, A.counter, A.chain, A.nh, st, A.ke_out, (unsigned int)A.nblk);
 }
 
@@ -764,10 +826,11 @@ int step_first_half(State &s, bool fused) {
     if (r) {
         const MolArgs A = mol_args(s, *r);
         if (nh)
-            k_first_mol<true><<<rigid_blocks(A.nmol), kMolBlock, 0, s.stream>>>(A, nullptr);
+            MDX_CUDA_TRY(launch_pdl(k_first_mol<true>, dim3(rigid_blocks(A.nmol)), dim3(kMolBlock), 0, s.stream, A,
+                                    (const MolArgs *)nullptr));
         else
-            k_first_mol<false><<<rigid_blocks(A.nmol), kMolBlock, 0, s.stream>>>(A, nullptr);
-        MDX_LAUNCHED();
+            MDX_CUDA_TRY(launch_pdl(k_first_mol<false>, dim3(rigid_blocks(A.nmol)), dim3(kMolBlock), 0, s.stream, A,
+                                    (const MolArgs *)nullptr));
     }
     return 0;
 }
@@ -815,8 +878,7 @@ int step_second_half(State &s, bool fused, const float4 *fextra, const float4 *f
         A.nparts = nparts;
         A.fextra = fextra;
         A.frecip = frecip;
-        k_second_mol<<<mb, kMolBlock, 0, s.stream>>>(A, nullptr);
-        MDX_LAUNCHED();
+        MDX_CUDA_TRY(launch_pdl(k_second_mol, dim3(mb), dim3(kMolBlock), 0, s.stream, A, (const MolArgs *)nullptr));
     }
     return 0;
 }
@@ -916,7 +978,7 @@ int nh_prepare(State &s, FixNoseHoover &nh) {
     NHChain &c = nh.h;
     int ndf = 0;
     for (auto &a : s.atoms) ndf += a.ndf;
-    c.n = 10;
+    c.n = kNHChain;
     c.T = nh.T;
     c.freq = 1.0 / nh.tau;
     c.ndf = ndf;
@@ -929,6 +991,7 @@ int nh_prepare(State &s, FixNoseHoover &nh) {
     c.ke = mv2 * s.units.mvv_to_eng;
     c.mass[0] = c.ndf * c.kB * c.T / (c.freq * c.freq);
     for (int k = 1; k < c.n; k++) c.mass[k] = c.kB * c.T / (c.freq * c.freq);
+    for (int k = 0; k < c.n; k++) c.inv_mass[k] = 1.0 / c.mass[k];
     c.force[0] = (c.ke - c.ndf * c.kB * c.T) / c.mass[0];
     for (int k = 1; k < c.n; k++) c.force[k] = (c.mass[k - 1] * c.vel[k - 1] * c.vel[k - 1] - c.kB * c.T) / c.mass[k];
     NHChain pair[2];

@@ -121,6 +121,7 @@ __device__ __forceinline__ bool pair_term(const PairArgs &A, const float *sp, in
 // or null (single system, a0)
 template <int T, int LJ, bool EW, bool VIR, bool ENERGY>
 __global__ void __launch_bounds__(256) k_pair(const PairArgs a0, const PairArgs *__restrict__ tab, int accumulate) {
+    pdl_wait();
     const PairArgs A = tab ? tab[blockIdx.y] : a0;
     extern __shared__ float sp[];
     const int nt2 = A.ntypes * A.ntypes;
@@ -240,13 +241,15 @@ void launch_t(const PairArgs &A, const PairArgs *tab, int nrep, bool vir, bool e
     const int warps = (A.n + G - 1) / G;
     const dim3 blocks((warps * 32 + 255) / 256, nrep);
     const size_t smem = LJ ? 3 * A.ntypes * A.ntypes * sizeof(float) : 0;
-    if (energy)
+    if (energy) {
         k_pair<T, LJ, EW, false, true><<<blocks, 256, smem, st>>>(A, tab, 0);
-    else if (vir)
+        MDX_LAUNCHED();
+    } else if (vir) {
         k_pair<T, LJ, EW, true, false><<<blocks, 256, smem, st>>>(A, tab, accumulate ? 1 : 0);
-    else
-        k_pair<T, LJ, EW, false, false><<<blocks, 256, smem, st>>>(A, tab, accumulate ? 1 : 0);
-    MDX_LAUNCHED();
+        MDX_LAUNCHED();
+    } else {
+        launch_pdl(k_pair<T, LJ, EW, false, false>, blocks, dim3(256), smem, st, A, tab, accumulate ? 1 : 0);
+    }
 }
 
 template <int T>
