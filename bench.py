@@ -43,6 +43,7 @@ def parse():
     ap.add_argument("--frames", type=int, default=40, help="surrogate: frames per training temperature")
     ap.add_argument("--train-iters", type=int, default=4000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-nve", action="store_true", help="skip the NVE energy-drift measurement")
     return ap.parse_args()
 
 
@@ -98,6 +99,42 @@ def workload(name, seed=20261203):
                         "SETTLE, dt 2 fs, Nose-Hoover 298 K"),
            "molecules": int(len(sysd.molecules)), "sites": int(len(sysd.pos))}
     return sysd, st, cfg, 2.0
+
+
+def nve_drift(name, x, v, seed):
+    """Total-energy drift of an NVE continuation of the timed run: the same
+    system, cutoffs, mesh and step with the thermostat off, started from the
+    timed run's final positions and velocities.  After 200 steps, the total
+    energy (FP64 kinetic sum + the potential energy of every fix) is sampled
+    every 500 steps over 5,000 steps; the drift is the least-squares slope,
+    per molecule in kcal/mol per ns (water) or per atom in epsilon per tau
+    (LJ).  Not timed."""
+    import dataclasses
+    from md_engine_b200 import IntegratorVerlet, systems
+    if name == "lj":
+        sysd = systems.lj_fcc(ncell=20, seed=seed)
+        sysd = dataclasses.replace(sysd, pos=np.asarray(x), vel=np.asarray(v))
+        st, _ = systems.build_lj_state(sysd, rcut=2.5, skin=0.3, dt=0.005, interval=10)
+        nunit, mvv, t_step, unit = len(sysd.pos), 1.0, 0.005, "epsilon per atom per tau"
+    else:
+        sysd = systems.water_tip4p2005(nside=16, seed=seed)
+        sysd = dataclasses.replace(sysd, pos=np.asarray(x), vel=np.asarray(v))
+        st, _ = systems.build_water_state(sysd, rcut=9.0, skin=1.0, dt=2.0, interval=10, grid=64,
+                                          e3b=name == "water_e3b", thermostat=False)
+        nunit, mvv, t_step, unit = len(sysd.molecules), systems.MVV_TO_ENG_REAL, 2.0e-6, "kcal/mol per molecule per ns"
+    it = IntegratorVerlet(st)
+    it.run(200)
+    ts, es = [], []
+    for k in range(11):
+        if k:
+            it.run(500)
+        mv2, _ = st.kinetic()
+        es.append((0.5 * mv2 * mvv + float(np.sum(st.potentialEnergy()))) / nunit)
+        ts.append(k * 500 * t_step)
+    slope = float(np.polyfit(ts, es, 1)[0])
+    return {"value": slope, "unit": unit, "steps": 5000, "samples": len(es),
+            "energy_per_unit_first_last": [es[0], es[-1]],
+            "integrator": "velocity Verlet, FP32 forces, FP64 SETTLE, same dt, thermostat off"}
 
 
 class ClockSampler:
@@ -429,6 +466,12 @@ def main():
             "stage_us": stages,
             "clocks": clk.summary(),
         }
+        if not args.no_nve:
+            try:
+                xf, vf, _ = st.getAtoms()
+                line["nve_drift"] = nve_drift(args.workload, xf, vf, 20261203 + rank)
+            except Exception as ex:  # reported, never required
+                line["nve_drift"] = {"value": None, "error": str(ex)}
         if world == 1 and not args.no_cpu_baseline:
             try:
                 from oracle import cpu_step

@@ -414,6 +414,80 @@ __global__ void k_e3b_forces(const E3BArgs a0, const E3BArgs *__restrict__ tab) 
     }
 }
 
+// E3B virial (virialMode): per molecule i, the two-body term as the
+// reference, 0.5 F (x) dr per listed O-O pair (computeVirial,
+// ThreeBodyE3B.h:129, 222-245), plus -- which the reference leaves out
+// (ThreeBodyE3B.h:449-451) -- the three-body forces of each unordered pair,
+// counted once on its lower-index molecule: every term of pair_force_both is
+// a central O-H force sc fv[k] along d[k] (H minus O), so the pair adds
+// sum_k S_k fv[k] (x) d[k], S_k the sum of the coefficients of fv[k].  Added
+// to the O atom's per-atom virial (xx yy zz xy xz yz).
+template <int T>
+__global__ void k_e3b_virial(const E3BArgs A, float *__restrict__ vir) {
+    const int4 *__restrict__ mol_idx = A.mol_idx;
+    const float4 *__restrict__ xs = A.xs;
+    const Box &box = A.box;
+    const E3BParams &p = A.p;
+    constexpr int G = 32 / T;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int a = lane / T, t = lane % T;
+    const int m = warp * G + a;
+    const bool valid = m < A.nmol;
+    float w[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    auto add = [&](float s, float3 f, float3 d) {
+        w[0] += s * f.x * d.x;
+        w[1] += s * f.y * d.y;
+        w[2] += s * f.z * d.z;
+        w[3] += s * f.x * d.y;
+        w[4] += s * f.x * d.z;
+        w[5] += s * f.y * d.z;
+    };
+    int4 ix = make_int4(0, 0, 0, 0);
+    if (valid) {
+        ix = mol_idx[m];
+        const MolPos mi = load_mol(xs, ix);
+        const float4 Ti = A.totals[m];
+        int cnt = (int)A.mcounts[m];
+        cnt = cnt < A.mcap ? cnt : A.mcap;
+        const uint32_t *row = A.mlist + (size_t)(m / G) * A.mcap * G + a * T + t;
+        for (int k = t; k < cnt; k += T) {
+            const int mj = (int)row[(size_t)(k / T) * 32];
+            const int4 jx = __ldg(mol_idx + mj);
+            MolPos mjp;
+            mjp.a = f3(__ldg(xs + jx.x));
+            const float3 dr = min_image(box, mi.a - mjp.a);
+            const float r2 = dot3(dr, dr);
+            if (r2 >= p.list_cut2) continue;
+            const float r = sqrtf(r2);
+            add(0.5f * p.k2 * p.E2 * expf(-p.k2 * r) / r, dr, dr);
+            if (r > p.rmax || m >= mj) continue;
+            mjp.b = f3(__ldg(xs + jx.y));
+            mjp.c = f3(__ldg(xs + jx.z));
+            const float4 Tj = __ldg(A.totals + mj);
+            PairGeom g;
+            pair_geom(p, box, mi, mjp, g);
+            const float3 d[4] = {min_image(box, mjp.b - mi.a), min_image(box, mjp.c - mi.a),
+                                 min_image(box, mi.b - mjp.a), min_image(box, mi.c - mjp.a)};
+            const float *e = g.es;
+            const float B1 = p.Eb * (Tj.x + Ti.y + Ti.z - 2.0f * (e[2] + e[3]));
+            const float B2 = p.Eb * (Ti.x + Tj.y + Tj.z - 2.0f * (e[0] + e[1]));
+            const float C1 = p.Ec * (Ti.x - e[1] - e[0]);
+            const float C2 = p.Ec * (Tj.x - e[2] - e[3]);
+            add(p.Ea * (Tj.z - e[1]) + B1 + C1, g.fv[0], d[0]);
+            add(p.Ea * (Tj.y - e[0]) + B1 + C1, g.fv[1], d[1]);
+            add(p.Ea * (Ti.z - e[3]) + B2 + C2, g.fv[2], d[2]);
+            add(p.Ea * (Ti.y - e[2]) + B2 + C2, g.fv[3], d[3]);
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 6; c++) w[c] = tsum<T>(w[c]);
+    if (valid && t == 0) {
+#pragma unroll
+        for (int c = 0; c < 6; c++) vir[6 * (size_t)ix.x + c] += w[c];
+    }
+}
+
 constexpr int kMolTeam = kE3BTeam;
 
 }  // namespace
@@ -661,9 +735,19 @@ int batch_e3b_forces(Batch &b, cudaStream_t stream) {
 }
 
 int FixE3B::compute(int virialMode) {
-    (void)virialMode;
     if (sur && sur->enabled) return surrogate_compute(*state, *this);
-    return e3b_forces(*state, *this);
+    if (int e = e3b_forces(*state, *this)) return e;
+    return virialMode ? e3b_virial(*state, *this) : 0;
+}
+
+// after e3b_forces (the totals are current)
+int e3b_virial(State &s, FixE3B &f) {
+    const int nmol = (int)f.mol_ids.size();
+    if (nmol == 0) return 0;
+    const E3BArgs A = e3b_args(s, f, s.gpd.fs.p);
+    k_e3b_virial<kMolTeam><<<e3b_blocks(nmol), 256, 0, s.stream>>>(A, s.gpd.virials.p);
+    MDX_LAUNCHED();
+    return 0;
 }
 
 int FixE3B::handleLocalData() { return 0; }

@@ -242,6 +242,7 @@ class FixChargeEwald : public Fix {
     // it reads it; every other user of rho clears it after use): spread()
     // then needs no memset
     bool rho_zero = false;
+    DBuf<double> vir_acc;  // reciprocal-space virial sum (6)
     DBuf<float4> e4;
     DBuf<float2> tw;        // W_32^k then W_64^k
     FixChargeEwald(State *s, std::string h, std::string g);
@@ -499,6 +500,8 @@ int e3b_forces(State &s, FixE3B &f);
 int e3b_forces_to(State &s, FixE3B &f, float4 *out, bool side, cudaStream_t stream);
 int e3b_energy(State &s, FixE3B &f, double out[2]);
 int e3b_exact_to(State &s, FixE3B &f, float4 *out, int twobody, cudaStream_t stream);
+int e3b_virial(State &s, FixE3B &f);
+int ewald_recip_virial(State &s, FixChargeEwald &f);
 int e3b_twobody_to(State &s, FixE3B &f, float4 *out, cudaStream_t stream);
 // learned E3B three-body surrogate (surrogate.cu)
 int surrogate_forces_to(State &s, FixE3B &f, float4 *out, cudaStream_t stream);

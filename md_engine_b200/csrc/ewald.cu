@@ -244,6 +244,49 @@ __global__ void k_recip_energy(int3 sz, const float2 *__restrict__ rho_k, const 
     if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
 }
 
+// virials_cu (FixChargeEwald.cu:731-812) on the half spectrum: the 6-vector
+// sum_k w G |rho_k|^2 (delta_ab - 2 (1/k^2 + 1/(4 alpha^2)) k_a k_b), k != 0,
+// w = 2 for the kz planes that stand for their conjugates; FP64 sums
+__global__ void k_recip_virial(int3 sz, const float2 *__restrict__ rho_k, const float *__restrict__ green, size_t nk,
+                               double3 tpl, double alpha, double *out) {
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    const int nzh = sz.z / 2 + 1;
+    const double f4a = 0.25 / (alpha * alpha);
+    for (size_t id = (size_t)blockIdx.x * blockDim.x + threadIdx.x; id < nk; id += (size_t)gridDim.x * blockDim.x) {
+        const int iz = (int)(id % nzh);
+        const int iy = (int)((id / nzh) % sz.y);
+        const int ix = (int)(id / ((size_t)nzh * sz.y));
+        const double kx = tpl.x * (ix > sz.x / 2 ? ix - sz.x : ix);
+        const double ky = tpl.y * (iy > sz.y / 2 ? iy - sz.y : iy);
+        const double kz = tpl.z * iz;
+        const double k2 = kx * kx + ky * ky + kz * kz;
+        if (k2 == 0.0) continue;
+        const double w = (iz == 0 || 2 * iz == sz.z) ? 1.0 : 2.0;
+        const float2 q = rho_k[id];
+        const double E = w * (double)green[id] * ((double)q.x * q.x + (double)q.y * q.y);
+        const double d = -2.0 * (1.0 / k2 + f4a);
+        acc[0] += (1.0 + d * kx * kx) * E;
+        acc[1] += (1.0 + d * ky * ky) * E;
+        acc[2] += (1.0 + d * kz * kz) * E;
+        acc[3] += d * kx * ky * E;
+        acc[4] += d * kx * kz * E;
+        acc[5] += d * ky * kz * E;
+    }
+#pragma unroll
+    for (int c = 0; c < 6; c++) {
+        double v = acc[c];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(out + c, v);
+    }
+}
+
+// mapVirialToSingleAtom (FixChargeEwald.cu:815-818): the field virial, 0.5/V
+// of the sum, goes onto the first atom's per-atom virial
+__global__ void k_add_field_virial(float *__restrict__ vir, const double *__restrict__ sum6, double scale) {
+    const int c = threadIdx.x;
+    if (c < 6) vir[c] += (float)(scale * sum6[c]);
+}
+
 double sinc(double x) {
     if (x < 0.1 && x > -0.1) {
         double x2 = x * x;
@@ -820,11 +863,34 @@ int FixChargeEwald::gather_to(float4 *out, cudaStream_t st) {
 }
 
 int FixChargeEwald::compute(int virialMode) {
-    (void)virialMode;
     State &s = *state;
     if (int e = spread(s.stream)) return e;
     if (int e = solve(s.stream)) return e;
-    return gather(true, s.stream);
+    if (int e = gather(true, s.stream)) return e;
+    return virialMode ? ewald_recip_virial(s, *this) : 0;
+}
+
+// the reciprocal-space virial (FixChargeEwald::compute with virialMode,
+// FixChargeEwald.cu:1455-1466): spread, R2C, k-space sum, onto atom 0
+int ewald_recip_virial(State &s, FixChargeEwald &f) {
+    if (int e = f.spread(s.stream)) return e;
+    cufftSetStream(f.plan_r2c, s.stream);
+    if (cufftExecR2C(f.plan_r2c, f.rho.p, (cufftComplex *)f.rho_k.p) != CUFFT_SUCCESS) {
+        set_error(MDX_ERR_CUDA, "cufftExecR2C failed");
+        return MDX_ERR_CUDA;
+    }
+    MDX_CUDA_TRY(cudaMemsetAsync(f.rho.p, 0, (size_t)f.sz.x * f.sz.y * f.sz.z * sizeof(float), s.stream));
+    f.rho_zero = true;
+    if (int e = f.vir_acc.alloc(6)) return e;
+    MDX_CUDA_TRY(cudaMemsetAsync(f.vir_acc.p, 0, 6 * sizeof(double), s.stream));
+    const size_t nk = (size_t)f.sz.x * f.sz.y * (f.sz.z / 2 + 1);
+    const double3 tpl = make_double3(2.0 * M_PI / s.box.Ld.x, 2.0 * M_PI / s.box.Ld.y, 2.0 * M_PI / s.box.Ld.z);
+    k_recip_virial<<<148, 256, 0, s.stream>>>(f.sz, f.rho_k.p, f.green.p, nk, tpl, f.alpha, f.vir_acc.p);
+    MDX_LAUNCHED();
+    const double V = s.box.Ld.x * s.box.Ld.y * s.box.Ld.z;
+    k_add_field_virial<<<1, 32, 0, s.stream>>>(s.gpd.virials.p, f.vir_acc.p, 0.5 / V);
+    MDX_LAUNCHED();
+    return 0;
 }
 
 int ewald_recip_energy(State &s, FixChargeEwald &f, double *out) {

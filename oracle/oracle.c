@@ -415,15 +415,43 @@ static double e3b_pair_energy(const e3b_par *p, const double *e, const double T1
 }
 
 /* returns number of three-body pairs evaluated */
+/* e3b_pair_force's forces are central O-H pair forces sc * fv[k] along
+ * d[k] (H minus O, minimum image); their virial is sum_k S_k fv[k] (x) d[k]
+ * with S_k the sum of the coefficients that multiply fv[k] there.  Adds to
+ * vir[6] (xx yy zz xy xz yz, computeVirial's order, helpers.h:34-41). */
+static void e3b_pair_virial(const e3b_par *p, const e3b_pair *g, const double d[4][3], const double T1[3],
+                            const double T2[3], double vir[6]) {
+    const double *e = g->es;
+    const double B1 = p->Eb * (T2[0] + T1[1] + T1[2] - 2.0 * (e[2] + e[3]));
+    const double B2 = p->Eb * (T1[0] + T2[1] + T2[2] - 2.0 * (e[0] + e[1]));
+    const double C1 = p->Ec * (T1[0] - e[1] - e[0]);
+    const double C2 = p->Ec * (T2[0] - e[2] - e[3]);
+    const double S[4] = {p->Ea * (T2[2] - e[1]) + B1 + C1, p->Ea * (T2[1] - e[0]) + B1 + C1,
+                         p->Ea * (T1[2] - e[3]) + B2 + C2, p->Ea * (T1[1] - e[2]) + B2 + C2};
+    for (int k = 0; k < 4; k++) {
+        const double *fv = g->fv[k], *dk = d[k];
+        vir[0] += S[k] * fv[0] * dk[0];
+        vir[1] += S[k] * fv[1] * dk[1];
+        vir[2] += S[k] * fv[2] * dk[2];
+        vir[3] += S[k] * fv[0] * dk[1];
+        vir[4] += S[k] * fv[0] * dk[2];
+        vir[5] += S[k] * fv[1] * dk[2];
+    }
+}
+
+/* vir (may be NULL): total virial, two-body as the reference (0.5 F (x) dr
+ * per ordered pair, ThreeBodyE3B.h:129, 222-245) plus the three-body pair
+ * forces (which the reference leaves out, ThreeBodyE3B.h:449-451) */
 int orc_e3b(int nmol, const int *mol, const double *x, const double L[3], const double *prm,
-            double *f, double *energy_total) {
+            double *f, double *energy_total, double *vir) {
     e3b_par p = {prm[0], prm[1], prm[2], prm[3], prm[4], prm[5], prm[6], prm[7]};
     const double r2b = prm[8], rmax3 = prm[9];
     double *T = (double *)calloc((size_t)3 * nmol, sizeof(double));
     double e2 = 0.0, e3 = 0.0;
+    double v2[6] = {0, 0, 0, 0, 0, 0};
     int npairs = 0;
     /* pass 1: totals (ThreeBodyE3B.h:170-211) and the two-body force */
-#pragma omp parallel for schedule(dynamic, 16) reduction(+ : e2)
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : e2, v2[:6])
     for (int a = 0; a < nmol; a++) {
         const int *ma = mol + 4 * a;
         double fo[3] = {0, 0, 0};
@@ -438,6 +466,12 @@ int orc_e3b(int nmol, const int *mol, const double *x, const double L[3], const 
             fo[0] += d[0] * s;
             fo[1] += d[1] * s;
             fo[2] += d[2] * s;
+            v2[0] += 0.5 * s * d[0] * d[0];
+            v2[1] += 0.5 * s * d[1] * d[1];
+            v2[2] += 0.5 * s * d[2] * d[2];
+            v2[3] += 0.5 * s * d[0] * d[1];
+            v2[4] += 0.5 * s * d[0] * d[2];
+            v2[5] += 0.5 * s * d[1] * d[2];
             e2 += 0.5 * p.E2 * exp(-p.k2 * r);
             if (r <= rmax3) {
                 e3b_pair g;
@@ -467,6 +501,14 @@ int orc_e3b(int nmol, const int *mol, const double *x, const double L[3], const 
             e3b_pair_geom(&p, x, ma, mb, L, &g);
             double f1[3][3] = {{0}}, f2[3][3] = {{0}};
             e3b_pair_force(&p, &g, T + 3 * a, T + 3 * b, f1, f2);
+            if (vir) {
+                double dd[4][3];
+                mimg(x + 3 * mb[1], x + 3 * ma[0], L, dd[0]);
+                mimg(x + 3 * mb[2], x + 3 * ma[0], L, dd[1]);
+                mimg(x + 3 * ma[1], x + 3 * mb[0], L, dd[2]);
+                mimg(x + 3 * ma[2], x + 3 * mb[0], L, dd[3]);
+                e3b_pair_virial(&p, &g, (const double(*)[3])dd, T + 3 * a, T + 3 * b, vir);
+            }
             if (f) {
                 for (int s = 0; s < 3; s++)
                     for (int c = 0; c < 3; c++) {
@@ -482,6 +524,8 @@ int orc_e3b(int nmol, const int *mol, const double *x, const double L[3], const 
         energy_total[0] = e2;
         energy_total[1] = e3;
     }
+    if (vir)
+        for (int c = 0; c < 6; c++) vir[c] += v2[c];
     free(T);
     return npairs;
 }

@@ -58,7 +58,7 @@ def lib():
         L.orc_nlist_brute.argtypes = [I, P, P, F, P, P, I]
         L.orc_nlist_brute.restype = I
         L.orc_pair_forces.argtypes = [I, P, P, P, I, P, P, P, I, D, D, D, P, P, P, I, P, P, P, P]
-        L.orc_e3b.argtypes = [I, P, P, P, P, P, P]
+        L.orc_e3b.argtypes = [I, P, P, P, P, P, P, P]
         L.orc_e3b.restype = I
         L.orc_lj_force_single.argtypes = [D, D, D, P, P]
         L.orc_e3b_single.argtypes = [P, D, P]
@@ -265,8 +265,10 @@ def e3b_params(style="E3B3"):
     return np.array([5.0, 5.2, E2 * k, Ea * k, Eb * k, Ec * k, 4.872, 1.907, 6.2, 6.1572], np.float64)
 
 
-def e3b_forces(mol, x, L, prm, natoms=None):
-    """Returns (f (natoms,3), (E2body, E3body), n_threebody_pairs)."""
+def e3b_forces(mol, x, L, prm, natoms=None, virial=None):
+    """Returns (f (natoms,3), (E2body, E3body), n_threebody_pairs).  virial: a
+    6-vector (xx yy zz xy xz yz) the total E3B virial is added to -- two-body
+    as the reference, plus the three-body pair forces."""
     x = np.ascontiguousarray(x, np.float64)
     natoms = len(x) if natoms is None else natoms
     m = np.ascontiguousarray(mol, np.int32)
@@ -274,7 +276,10 @@ def e3b_forces(mol, x, L, prm, natoms=None):
     e = np.zeros(2)
     Ld = np.asarray(L, np.float64)
     pr = np.ascontiguousarray(prm, np.float64)
-    npairs = lib().orc_e3b(len(m), _p(m), _p(x), _p(Ld), _p(pr), _p(f), _p(e))
+    vir = np.zeros(6)
+    npairs = lib().orc_e3b(len(m), _p(m), _p(x), _p(Ld), _p(pr), _p(f), _p(e), _p(vir))
+    if virial is not None:
+        virial += vir
     return f, (e[0], e[1]), npairs
 
 
@@ -389,7 +394,7 @@ def _p3m_stencil(x, lo, L, sz):
 
 
 def p3m_forces(x, q, lo, L, sz, alpha, order=5, qqr_to_eng=REAL_UNITS["qqr_to_eng"],
-               G=None, want_energy=False):
+               G=None, want_energy=False, virial=None):
     """Reciprocal-space P3M force (FixChargeEwald::compute, order 5), FP64.
 
     Spread (map_charge_to_grid_order_5_cu) -> FFT -> ik G rho (E_field_cu) ->
@@ -431,6 +436,17 @@ def p3m_forces(x, q, lo, L, sz, alpha, order=5, qqr_to_eng=REAL_UNITS["qqr_to_en
                 for dim in range(3):
                     f[:, dim] += w * E[dim][px, py, pz]
     f *= (Qu * q)[:, None]
+    if virial is not None:
+        # virials_cu + mapVirialToSingleAtom (FixChargeEwald.cu:731-818):
+        # 0.5/V sum_k G |rho_k|^2 (delta_ab - 2 (1/k^2 + 1/(4 alpha^2)) k_a k_b), k != 0
+        k2 = kx * kx + ky * ky + kz * kz
+        Ek = G * np.abs(rho) ** 2
+        with np.errstate(divide="ignore", invalid="ignore"):
+            dif = np.where(k2 > 0, -2.0 * (1.0 / np.where(k2 > 0, k2, 1.0) + 0.25 / (alpha * alpha)), 0.0)
+        Ek = np.where(k2 > 0, Ek, 0.0)
+        comps = ((kx, kx, 1.0), (ky, ky, 1.0), (kz, kz, 1.0), (kx, ky, 0.0), (kx, kz, 0.0), (ky, kz, 0.0))
+        for c, (ka, kb, dl) in enumerate(comps):
+            virial[c] += 0.5 / V * float(np.sum((dl + dif * ka * kb) * Ek))
     if want_energy:
         # 0.5/V sum_k G |rho_k|^2 (FixChargeEwald::singlePointEng, Energy_cu)
         eng = 0.5 / V * float(np.sum(G * np.abs(rho) ** 2))

@@ -94,3 +94,34 @@ def test_e3b_forces_vs_oracle(oracle):
     e = st.potentialEnergy()
     assert abs(e[2] - e2) < 1e-4 * abs(e2) + 1e-6
     assert abs(e[3] - e3) < 1e-3 * abs(e3) + 1e-6
+
+
+def test_water_e3b_total_virial_vs_oracle(oracle):
+    """virialMode: the total virial of LJ + Ewald real space (pair kernel),
+    the P3M reciprocal term (virials_cu, FixChargeEwald.cu:731-818) and E3B
+    (two-body as the reference, plus the three-body term the reference leaves
+    out) vs the FP64 oracle; the E3B part alone to 1e-3 of its size"""
+    sysd = water_small(seed=9)
+    rcut, pad, alpha, grid = 6.5, 1.0, 0.35, 32
+    st, fx = systems.build_water_state(sysd, rcut=rcut, skin=pad, grid=grid, e3b=True, alpha=alpha,
+                                       thermostat=False)
+    st.prepare()
+    st.computeForces(virialMode=1)
+    _, v_all = st.virials()
+    x, _, _ = st.getAtoms()
+    excl = oracle.exclusions_from_bonds(len(sysd.pos), water_bonds(sysd.molecules))
+    ref, _ = _oracle_pair(oracle, st, sysd, oracle_water_params(oracle, rcut), rcut, pad, qrc=rcut, alpha=alpha,
+                          qqr=oracle.REAL_UNITS["qqr_to_eng"], excl=excl)
+    v_pair = ref["virial"].sum(0)
+    v_rec = np.zeros(6)
+    oracle.p3m_forces(x, sysd.q, sysd.lo, sysd.L, (grid,) * 3, alpha, virial=v_rec)
+    v_e3b = np.zeros(6)
+    oracle.e3b_forces(sysd.molecules, x, sysd.L, oracle.e3b_params("E3B3"), virial=v_e3b)
+    scale = max(np.abs(v_pair).max(), np.abs(v_rec).max(), np.abs(v_e3b).max())
+    assert np.abs(v_all - (v_pair + v_rec + v_e3b)).max() < 2e-4 * scale, (v_all, v_pair, v_rec, v_e3b)
+    st.deactivateFix(fx["e3b"])
+    st.prepare()
+    st.computeForces(virialMode=1)
+    _, v_no = st.virials()
+    assert np.abs(v_no - (v_pair + v_rec)).max() < 2e-4 * scale
+    assert np.abs((v_all - v_no) - v_e3b).max() < 1e-3 * np.abs(v_e3b).max(), (v_all - v_no, v_e3b)
