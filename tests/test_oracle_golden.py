@@ -274,3 +274,37 @@ def test_oracle_vs_committed_reference_functor_vectors(oracle):
         b = np.zeros(4)
         oracle.lib().orc_e3b_single(prm.ctypes.data_as(ctypes.c_void_p), float(v["r"]), b.ctypes.data_as(ctypes.c_void_p))
         assert np.max(np.abs(np.array(v["out"]) - b)) <= 2e-5 * max(1.0, np.abs(b).max())
+
+
+def test_e3b_and_p3m_virials_are_volume_derivatives(oracle):
+    """every E3B force is a central pair force and the P3M reciprocal energy
+    depends on positions and box through k and G(k): both virial traces equal
+    -dE/d(eps) under the uniform scaling x -> (1 + eps) x, L -> (1 + eps) L"""
+    sysd = systems.water_tip4p2005(nside=6, seed=3)
+    x = sysd.pos.astype(np.float64)
+    L = sysd.L.astype(np.float64)
+    lo = sysd.lo.astype(np.float64)
+    mol = np.asarray(sysd.molecules, np.int32)
+    prm = oracle.e3b_params("E3B3")
+    h = 1e-5
+
+    vir = np.zeros(6)
+    oracle.e3b_forces(mol, x, L, prm, virial=vir)
+
+    def e3b(eps):
+        _, (a, b), _ = oracle.e3b_forces(mol, x * (1 + eps), L * (1 + eps), prm)
+        return a + b
+
+    d = (e3b(h) - e3b(-h)) / (2 * h)
+    assert abs(vir[:3].sum() + d) < 1e-6 * abs(d)
+
+    sz, alpha = (32, 32, 32), 0.3
+    vir = np.zeros(6)
+    oracle.p3m_forces(x, sysd.q, lo, L, sz, alpha, virial=vir)
+
+    def rec(eps):
+        _, e = oracle.p3m_forces(lo + (x - lo) * (1 + eps), sysd.q, lo, L * (1 + eps), sz, alpha, want_energy=True)
+        return e
+
+    d = (rec(h) - rec(-h)) / (2 * h)
+    assert abs(vir[:3].sum() + d) < 1e-6 * abs(d)
