@@ -166,7 +166,9 @@ struct E3BArgs {
     double *e_out;    // energy passes
     int twobody;      // 0: the totals pass leaves out the O-O two-body force
 };
-#define MDX_E3B_ARGS const E3BArgs A = tab ? tab[blockIdx.y] : a0
+#define MDX_E3B_ARGS \
+    pdl_wait();      \
+    const E3BArgs A = tab ? tab[blockIdx.y] : a0
 
 // updateMoleculeIdxsMap (FixE3B.cu:41-65) + molecule list cut from the atom
 // list: O-O pairs with r^2 < (rf + 1 + skin)^2.  Team of T lanes per molecule.
@@ -601,9 +603,8 @@ static dim3 e3b_blocks(int nmol, unsigned nrep = 1) {
 int e3b_build_list(State &s, FixE3B &f, bool conditional) {
     const int nmol = (int)f.mol_ids.size();
     if (nmol == 0 || !f.prepared) return 0;
-    k_e3b_list<kMolTeam><<<e3b_blocks(nmol), 256, 0, s.stream>>>(e3b_args(s, f, nullptr), nullptr,
-                                                                 conditional ? 1 : 0);
-    MDX_LAUNCHED();
+    MDX_CUDA_TRY(launch_pdl(k_e3b_list<kMolTeam>, e3b_blocks(nmol), dim3(256), 0, s.stream, e3b_args(s, f, nullptr),
+                            (const E3BArgs *)nullptr, conditional ? 1 : 0));
     return 0;
 }
 
@@ -616,11 +617,10 @@ int e3b_forces_to(State &s, FixE3B &f, float4 *out, bool side, cudaStream_t stre
     if (nmol == 0) return 0;
     const E3BArgs A = e3b_args(s, f, out);
     const dim3 blocks = e3b_blocks(nmol);
+    const E3BArgs *nt = nullptr;
     if (side) {
-        k_e3b_totals<kMolTeam, false, true><<<blocks, 256, 0, stream>>>(A, nullptr);
-        MDX_LAUNCHED();
-        k_e3b_forces<kMolTeam, false, true><<<blocks, 256, 0, stream>>>(A, nullptr);
-        MDX_LAUNCHED();
+        MDX_CUDA_TRY(launch_pdl(k_e3b_totals<kMolTeam, false, true>, blocks, dim3(256), 0, stream, A, nt));
+        MDX_CUDA_TRY(launch_pdl(k_e3b_forces<kMolTeam, false, true>, blocks, dim3(256), 0, stream, A, nt));
         return 0;
     }
     k_e3b_totals<kMolTeam, false><<<blocks, 256, 0, stream>>>(A, nullptr);

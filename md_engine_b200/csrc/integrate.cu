@@ -229,7 +229,9 @@ struct MolArgs {
     const float4 *frecip;  // P3M reciprocal forces of every site (may be null)
     int nblk;  // blocks of k_second_mol that carry this system's molecules
 };
-#define MDX_MOL_ARGS const MolArgs A = tab ? tab[blockIdx.y] : a0
+#define MDX_MOL_ARGS \
+    pdl_wait();      \
+    const MolArgs A = tab ? tab[blockIdx.y] : a0
 
 // rebuild-group kernel: molecule -> current atom indices (idToIdx after sort)
 __global__ void k_rigid_maps(const MolArgs a0, const MolArgs *__restrict__ tab, int conditional) {
@@ -277,7 +279,6 @@ __global__ void k_first_atoms(int n, float4 *__restrict__ xs, float4 *__restrict
 // per-molecule fused: NH rescale + save_prev_val + nve_v + nve_x + SETTLE + M-site
 template <bool NH>
 __global__ void k_first_mol(const MolArgs a0, const MolArgs *__restrict__ tab) {
-    pdl_wait();
     MDX_MOL_ARGS;
     int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= A.nmol) return;
@@ -433,7 +434,6 @@ __global__ void k_second_atoms(int n, float4 *__restrict__ vs, const float4 *__r
 // fextra (may be null): per-molecule-atom forces computed beside the pair
 // kernel (E3B), indexed like fs, merged into O/H1/H2 here
 __global__ void k_second_mol(const MolArgs a0, const MolArgs *__restrict__ tab) {
-    pdl_wait();
     MDX_MOL_ARGS;
     if ((int)blockIdx.x >= A.nblk) return;  // the whole block: not counted
     __shared__ double sh[32];
@@ -755,8 +755,8 @@ MolArgs mol_args(State &s, FixRigid &r) {
 int rigid_update_maps(State &s, FixRigid &r, bool conditional) {
     const int nmol = (int)r.mol_ids.size();
     if (nmol == 0 || !r.d_mol_ids.p) return 0;
-    k_rigid_maps<<<(nmol + 255) / 256, 256, 0, s.stream>>>(mol_args(s, r), nullptr, conditional ? 1 : 0);
-    MDX_LAUNCHED();
+    MDX_CUDA_TRY(launch_pdl(k_rigid_maps, dim3((nmol + 255) / 256), dim3(256), 0, s.stream, mol_args(s, r),
+                            (const MolArgs *)nullptr, conditional ? 1 : 0));
     return 0;
 }
 

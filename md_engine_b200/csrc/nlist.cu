@@ -70,7 +70,9 @@ struct GridArgs {
     int n, ncell, interval;
     float skin2q;
 };
-#define MDX_GRID_ARGS const GridArgs A = tab ? tab[blockIdx.y] : a0
+#define MDX_GRID_ARGS \
+    pdl_wait();       \
+    const GridArgs A = tab ? tab[blockIdx.y] : a0
 
 // setBuildFlag (GridGPU.cu:755-774) + the periodicInterval gate of
 // IntegratorVerlet.cu:696: rebuild iff forced, or turn % interval == 0 and
@@ -283,6 +285,7 @@ __device__ __forceinline__ uint32_t excl_depth(const BuildArgs &A, uint32_t myid
 template <int TP, int HG, bool COUNT>
 __global__ void __launch_bounds__(kBuildCellsPerBlock * 32) k_build_cells(const BuildArgs a0,
                                                                             const BuildArgs *__restrict__ tab) {
+    pdl_wait();
     const BuildArgs A = tab ? tab[blockIdx.y] : a0;
     if (!COUNT && !A.st->rebuild) return;
     constexpr int GP = 32 / TP;
@@ -645,10 +648,13 @@ BuildArgs build_args(State &s, const CellGrid &g, float cutsq) {
 
 template <int T, bool COUNT>
 void launch_build_hg(int hg, dim3 grid, cudaStream_t st, const BuildArgs &A, const BuildArgs *tab) {
-    if (hg == 4)
-        k_build_cells<T, 4, COUNT><<<grid, kBuildCellsPerBlock * 32, 0, st>>>(A, tab);
-    else
-        k_build_cells<T, 2, COUNT><<<grid, kBuildCellsPerBlock * 32, 0, st>>>(A, tab);
+    auto k = hg == 4 ? k_build_cells<T, 4, COUNT> : k_build_cells<T, 2, COUNT>;
+    if (tab) {
+        k<<<grid, kBuildCellsPerBlock * 32, 0, st>>>(A, tab);
+        MDX_LAUNCHED();
+    } else {
+        launch_pdl(k, grid, dim3(kBuildCellsPerBlock * 32), 0, st, A, tab);
+    }
 }
 
 // grid.x covers ncell (or the largest replica's) cells, one warp each
@@ -671,7 +677,6 @@ inline dim3 build_grid(int ncell, int nrep) {
 void launch_build(State &s, const CellGrid &g, float cutsq) {
     const BuildArgs A = build_args(s, g, cutsq);
     launch_build_any<false>(s.grid.team, s.grid.home_group, build_grid(A.ncell, 1), s.stream, A, nullptr);
-    MDX_LAUNCHED();
 }
 
 void launch_count(State &s, const CellGrid &g, float cutsq) {
@@ -681,7 +686,6 @@ void launch_count(State &s, const CellGrid &g, float cutsq) {
     A.part_q = 0;
     A.cap = 0;
     launch_build_any<true>(s.grid.team, s.grid.home_group, build_grid(A.ncell, 1), s.stream, A, nullptr);
-    MDX_LAUNCHED();
 }
 
 }  // namespace
@@ -861,18 +865,13 @@ int nlist_rebuild(State &s, bool force, bool conditional) {
     (void)conditional;
     const GridArgs A = grid_args(s);
     const int nb = (n + 255) / 256;
-    k_check<<<nb, 256, 0, s.stream>>>(A, nullptr, force ? 1 : 0);
-    MDX_LAUNCHED();
-    k_wrap_bin<<<nb, 256, 0, s.stream>>>(A, nullptr);
-    MDX_LAUNCHED();
-    k_scan_cells<<<1, 1024, 0, s.stream>>>(A, nullptr);
-    MDX_LAUNCHED();
-    k_scatter<<<nb, 256, 0, s.stream>>>(A, nullptr);
-    MDX_LAUNCHED();
-    k_rank<<<(ncell * 32 + 255) / 256, 256, 0, s.stream>>>(A, nullptr);
-    MDX_LAUNCHED();
-    k_gather<<<nb, 256, 0, s.stream>>>(A, nullptr);
-    MDX_LAUNCHED();
+    const GridArgs *nt = nullptr;
+    MDX_CUDA_TRY(launch_pdl(k_check, dim3(nb), dim3(256), 0, s.stream, A, nt, force ? 1 : 0));
+    MDX_CUDA_TRY(launch_pdl(k_wrap_bin, dim3(nb), dim3(256), 0, s.stream, A, nt));
+    MDX_CUDA_TRY(launch_pdl(k_scan_cells, dim3(1), dim3(1024), 0, s.stream, A, nt));
+    MDX_CUDA_TRY(launch_pdl(k_scatter, dim3(nb), dim3(256), 0, s.stream, A, nt));
+    MDX_CUDA_TRY(launch_pdl(k_rank, dim3((ncell * 32 + 255) / 256), dim3(256), 0, s.stream, A, nt));
+    MDX_CUDA_TRY(launch_pdl(k_gather, dim3(nb), dim3(256), 0, s.stream, A, nt));
     if (gr.cap == 0) {
         // first build: size the per-atom capacity from a counting sweep
         MDX_CUDA_TRY(cudaMemsetAsync(&s.d_status.p->max_neighbors, 0, sizeof(uint32_t), s.stream));
@@ -895,8 +894,7 @@ int nlist_rebuild(State &s, bool force, bool conditional) {
     if (FixE3B *e3 = s.e3bFix()) {
         if (int e = e3b_build_list(s, *e3, true)) return e;
     }
-    k_finish<<<1, 1024, 0, s.stream>>>(A, nullptr);
-    MDX_LAUNCHED();
+    MDX_CUDA_TRY(launch_pdl(k_finish, dim3(1), dim3(1024), 0, s.stream, A, (const GridArgs *)nullptr));
     gr.built = true;
     return 0;
 }
@@ -945,7 +943,7 @@ int batch_nlist_rebuild(Batch &b) {
     int hg = 2;
     for (State *r : b.reps) hg = std::max(hg, r->grid.home_group);
     launch_build_any<false>(s0.grid.team, hg, build_grid(b.max_cell, R), st, B, tb);
-    g_launches += 7;
+    g_launches += 6;
     if (int e = batch_rigid_maps(b)) return e;
     if (s0.e3bFix())
         if (int e = batch_e3b_list(b)) return e;
