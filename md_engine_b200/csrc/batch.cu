@@ -245,7 +245,7 @@ int Batch::launchGraph(int nsteps, bool with_group) {
             return MDX_ERR_CUDA;
         }
         cudaGraphExec_t ex;
-        MDX_CUDA_TRY(cudaGraphInstantiate(&ex, g, 0));
+        MDX_CUDA_TRY(cudaGraphInstantiate(&ex, g, cudaGraphInstantiateFlagUseNodePriority));
         cudaGraphDestroy(g);
         it = graphs.emplace(key, ex).first;
         graph_kernels[key] = captured;

@@ -32,21 +32,33 @@ constexpr int kE3BTeam = 16;
 // grid has completed and its memory is visible.  A CUDA graph captured from
 // such launches keeps them as programmatic edges, so consecutive kernels of a
 // step no longer pay a full drain-and-launch gap.
+// high: the launch also carries the device's greatest stream priority (the
+// P3M chain, the critical path of a water step, beside the pair kernel),
+// kept as a node priority by graphs instantiated with
+// cudaGraphInstantiateFlagUseNodePriority
+int high_priority();
 template <typename... KArgs, typename... Args>
-inline cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
-                              Args... args) {
-    cudaLaunchAttribute attr[1];
+inline cudaError_t launch_pdl_prio(bool high, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                                   cudaStream_t st, Args... args) {
+    cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
+    attr[1].id = cudaLaunchAttributePriority;
+    attr[1].val.priority = high ? high_priority() : 0;
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = grid;
     cfg.blockDim = block;
     cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = high ? 2 : 1;
     MDX_LAUNCHED();
     return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args... args) {
+    return launch_pdl_prio(false, kern, grid, block, smem, st, args...);
 }
 
 template <class T>
@@ -238,10 +250,6 @@ class FixChargeEwald : public Fix {
     DBuf<double> energy_acc;
     // own FFT path (cubic 32^3 / 64^3 meshes): field interleaved as float4
     bool own_fft = false;
-    // the charge grid is known to be zero (the library's own FFT clears it as
-    // it reads it; every other user of rho clears it after use): spread()
-    // then needs no memset
-    bool rho_zero = false;
     DBuf<double> vir_acc;  // reciprocal-space virial sum (6)
     DBuf<float4> e4;
     DBuf<float2> tw;        // W_32^k then W_64^k

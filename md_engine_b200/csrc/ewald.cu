@@ -347,7 +347,7 @@ P3MArgs p3m_args(State &s, FixChargeEwald &f) {
 // so the gather reads one 16-byte field value per stencil point.
 struct FFTArgs {
     int n;                   // points per side (32 or 64)
-    float *rho;              // [n][n][n]: read, then left zeroed for the next spread
+    const float *rho;        // [n][n][n]
     float2 *mid1;            // [n][n][n/2+1]: after the z and y passes
     float2 *mid2;            // [3][n][n][n/2+1]: E_d after the inverse x pass
     float4 *e4;              // [n][n][n]
@@ -422,12 +422,9 @@ __global__ void __launch_bounds__(1024) k_fft_zy(const FFTArgs A) {
     const LaneTw T = lane_twiddles<R>(lane, A.tw);
     for (int y = w; y < N; y += nw) {
         float2 v[R];
-        float *line = A.rho + ((size_t)x * N + y) * N;
+        const float *line = A.rho + ((size_t)x * N + y) * N;
 #pragma unroll
         for (int r = 0; r < R; r++) v[r] = make_float2(line[32 * r + lane], 0.f);
-        // the charge grid starts the next spread at zero (no memset node)
-#pragma unroll
-        for (int r = 0; r < R; r++) line[32 * r + lane] = 0.f;
         warp_fft<R, false>(v, lane, T);
 #pragma unroll
         for (int k1 = 0; k1 < R; k1++) {
@@ -688,7 +685,6 @@ int FixChargeEwald::prepareForRun() {
     const size_t ng = (size_t)sz.x * sz.y * sz.z;
     const size_t nk = (size_t)sz.x * sz.y * (sz.z / 2 + 1);
     if (int e = rho.alloc(ng)) return e;
-    rho_zero = false;  // the first spread clears the grid
     if (int e = rho_k.alloc(nk)) return e;
     if (int e = e_k.alloc(3 * nk)) return e;
     if (int e = e_r.alloc(3 * ng)) return e;
@@ -781,10 +777,9 @@ template <int R>
 int own_solve(State &s, FixChargeEwald &f, cudaStream_t st) {
     constexpr int N = 32 * R, NH = N / 2 + 1;
     const FFTArgs A = fft_args(s, f);
-    MDX_CUDA_TRY(launch_pdl(k_fft_zy<R>, dim3(N), dim3(1024), (size_t)N * NH * sizeof(float2), st, A));
-    f.rho_zero = true;  // k_fft_zy leaves the charge grid zeroed
-    MDX_CUDA_TRY(launch_pdl(k_fft_xe<R>, dim3((N * NH + 7) / 8), dim3(256), 0, st, A));
-    MDX_CUDA_TRY(launch_pdl(k_ifft_yz<R>, dim3(N, 3), dim3(1024), (size_t)N * NH * sizeof(float2), st, A));
+    MDX_CUDA_TRY(launch_pdl_prio(true, k_fft_zy<R>, dim3(N), dim3(1024), (size_t)N * NH * sizeof(float2), st, A));
+    MDX_CUDA_TRY(launch_pdl_prio(true, k_fft_xe<R>, dim3((N * NH + 7) / 8), dim3(256), 0, st, A));
+    MDX_CUDA_TRY(launch_pdl_prio(true, k_ifft_yz<R>, dim3(N, 3), dim3(1024), (size_t)N * NH * sizeof(float2), st, A));
     return 0;
 }
 
@@ -802,10 +797,9 @@ int own_fft_setup() {
 int FixChargeEwald::spread(cudaStream_t st) {
     State &s = *state;
     const size_t ng = (size_t)sz.x * sz.y * sz.z;
-    if (!rho_zero) MDX_CUDA_TRY(cudaMemsetAsync(rho.p, 0, ng * sizeof(float), st));
-    MDX_CUDA_TRY(launch_pdl(k_spread5, dim3((s.gpd.n + 47) / 48), dim3(256), 0, st, p3m_args(s, *this),
+    MDX_CUDA_TRY(cudaMemsetAsync(rho.p, 0, ng * sizeof(float), st));
+    MDX_CUDA_TRY(launch_pdl_prio(true, k_spread5, dim3((s.gpd.n + 47) / 48), dim3(256), 0, st, p3m_args(s, *this),
                             (const P3MArgs *)nullptr));
-    rho_zero = false;
     return 0;
 }
 
@@ -833,10 +827,10 @@ int FixChargeEwald::gather(bool accumulate, cudaStream_t st) {
     const P3MArgs A = p3m_args(s, *this);
     if (own_fft) {
         if (accumulate)
-            MDX_CUDA_TRY(launch_pdl(k_gather4<true>, dim3((s.gpd.n + 47) / 48), dim3(256), 0, st, A,
+            MDX_CUDA_TRY(launch_pdl_prio(true, k_gather4<true>, dim3((s.gpd.n + 47) / 48), dim3(256), 0, st, A,
                                     (const float4 *)e4.p));
         else
-            MDX_CUDA_TRY(launch_pdl(k_gather4<false>, dim3((s.gpd.n + 47) / 48), dim3(256), 0, st, A,
+            MDX_CUDA_TRY(launch_pdl_prio(true, k_gather4<false>, dim3((s.gpd.n + 47) / 48), dim3(256), 0, st, A,
                                     (const float4 *)e4.p));
         return 0;
     }
@@ -853,7 +847,7 @@ int FixChargeEwald::gather_to(float4 *out, cudaStream_t st) {
     P3MArgs A = p3m_args(s, *this);
     A.fs = out;
     if (own_fft) {
-        MDX_CUDA_TRY(launch_pdl(k_gather4<false>, dim3((s.gpd.n + 47) / 48), dim3(256), 0, st, A,
+        MDX_CUDA_TRY(launch_pdl_prio(true, k_gather4<false>, dim3((s.gpd.n + 47) / 48), dim3(256), 0, st, A,
                                 (const float4 *)e4.p));
     } else {
         k_gather<false><<<(s.gpd.n + 127) / 128, 128, 0, st>>>(A, nullptr);
@@ -879,8 +873,6 @@ int ewald_recip_virial(State &s, FixChargeEwald &f) {
         set_error(MDX_ERR_CUDA, "cufftExecR2C failed");
         return MDX_ERR_CUDA;
     }
-    MDX_CUDA_TRY(cudaMemsetAsync(f.rho.p, 0, (size_t)f.sz.x * f.sz.y * f.sz.z * sizeof(float), s.stream));
-    f.rho_zero = true;
     if (int e = f.vir_acc.alloc(6)) return e;
     MDX_CUDA_TRY(cudaMemsetAsync(f.vir_acc.p, 0, 6 * sizeof(double), s.stream));
     const size_t nk = (size_t)f.sz.x * f.sz.y * (f.sz.z / 2 + 1);
@@ -900,10 +892,6 @@ int ewald_recip_energy(State &s, FixChargeEwald &f, double *out) {
         set_error(MDX_ERR_CUDA, "cufftExecR2C failed");
         return MDX_ERR_CUDA;
     }
-    // leave the charge grid zeroed, as the step's own FFT does (captured
-    // steps spread onto it without clearing it)
-    MDX_CUDA_TRY(cudaMemsetAsync(f.rho.p, 0, (size_t)f.sz.x * f.sz.y * f.sz.z * sizeof(float), s.stream));
-    f.rho_zero = true;
     const size_t nk = (size_t)f.sz.x * f.sz.y * (f.sz.z / 2 + 1);
     MDX_CUDA_TRY(cudaMemsetAsync(f.energy_acc.p, 0, sizeof(double), s.stream));
     k_recip_energy<<<148, 256, 0, s.stream>>>(f.sz, f.rho_k.p, f.green.p, nk, f.energy_acc.p);
@@ -949,7 +937,6 @@ int batch_p3m_prepare(Batch &b) {
         for (int j = 0; j < K; j++) {
             FixChargeEwald *f = b.reps[c.reps[j]]->ewaldFix();
             f->rho.view(c.rho.p + j * ng, ng);
-            f->rho_zero = false;
             f->rho_k.view(c.rho_k.p + j * nk, nk);
             f->e_k.view(c.e_k.p + j * 3 * nk, 3 * nk);
             f->e_r.view(c.e_r.p + j * 3 * ng, 3 * ng);

@@ -138,7 +138,7 @@ class IntegratorVerlet {
             return MDX_ERR_CUDA;
         }
         cudaGraphExec_t ex;
-        MDX_CUDA_TRY(cudaGraphInstantiate(&ex, g, 0));
+        MDX_CUDA_TRY(cudaGraphInstantiate(&ex, g, cudaGraphInstantiateFlagUseNodePriority));
         cudaGraphDestroy(g);
         graphs[key] = ex;
         graph_kernels[key] = captured;

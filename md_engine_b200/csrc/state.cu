@@ -14,6 +14,16 @@ namespace mdx {
 
 uint64_t g_launches = 0;
 
+int high_priority() {
+    static int prio = 1;  // not yet read
+    if (prio == 1) {
+        int least = 0, greatest = 0;
+        if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess) greatest = 0;
+        prio = greatest;
+    }
+    return prio;
+}
+
 static thread_local char g_err[1024] = "";
 void set_error(int code, const char *fmt, ...) {
     (void)code;
