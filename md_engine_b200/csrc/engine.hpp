@@ -212,6 +212,7 @@ class Fix {
 };
 
 class FixChargeEwald;
+class FixRigid;
 
 // FixPair / FixLJCut / FixWCA (src/Fixes/FixPair.cpp, FixLJCut.cu, FixWCA.cu)
 class FixPair : public Fix {
@@ -264,6 +265,10 @@ class FixChargeEwald : public Fix {
     int solve(cudaStream_t st);    // FFT, E-field, inverse FFTs
     int gather(bool accumulate, cudaStream_t st);
     int gather_to(float4 *out, cudaStream_t st);  // reciprocal forces stored into out
+    // molecule form of spread / gather_to (rigid water, own FFT)
+    bool mol_form_ok(const FixRigid &r) const;
+    int spread_mol(cudaStream_t st, const FixRigid &r);
+    int gather_mol_to(float4 *out, cudaStream_t st, const FixRigid &r);
     DBuf<float4> f_recip;                         // per-step reciprocal forces (fused step)
 };
 

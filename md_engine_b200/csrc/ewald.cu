@@ -75,6 +75,10 @@ struct P3MArgs {
     float3 tpl;  // 2 pi / L
     size_t nk, ngrid;
     float niv;   // -1 / V
+    // molecule form (all-rigid water): the charged sites of molecule m are
+    // H1, H2, M of mol_idx[m] (four-site, uncharged O) or O, H1, H2
+    const int4 *mol_idx;
+    int nmol, four_site;
 };
 #define MDX_P3M_ARGS const P3MArgs A = tab ? tab[blockIdx.y] : a0
 
@@ -88,15 +92,10 @@ __device__ __forceinline__ float pick5(const float w[5], int t) {
     return t == 0 ? w[0] : t == 1 ? w[1] : t == 2 ? w[2] : t == 3 ? w[3] : w[4];
 }
 
-__global__ void k_spread5(const P3MArgs a0, const P3MArgs *__restrict__ tab) {
-    pdl_wait();
-    MDX_P3M_ARGS;
-    const int lane = threadIdx.x & 31;
-    const int t = lane % 5;
-    const int W = (A.n + 5) / 6;
-    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int i = (lane / 5) * W + w;
-    if (lane >= 30 || w >= W || i >= A.n) return;
+// stencil plane a = t of atom i's charge (25 points, as two 16-byte vector
+// atomics per z row: the five z points lie in two aligned groups of four,
+// the mesh side being a multiple of 4)
+__device__ __forceinline__ void spread_plane(const P3MArgs &A, int i, int t) {
     const float q = A.qs[i];
     if (q == 0.f) return;
     const P3MGeom &g = A.g;
@@ -113,8 +112,6 @@ __global__ void k_spread5(const P3MArgs a0, const P3MArgs *__restrict__ tab) {
     for (int c = 0; c < 5; c++) pz[c] = wrapi(ng.z + c - 2, g.sz.z);
     const int px = wrapi(ng.x + t - 2, g.sz.x);
     const float cyz = qi * pick5(wx, t);
-    // the five z points of a row lie in two aligned groups of four (the mesh
-    // side is a multiple of 4): two 16-byte vector atomics instead of five
     const int z0 = pz[0], g0 = z0 & ~3, sh = z0 - g0;
     const int g1 = (g0 + 4) % g.sz.z;
 #pragma unroll
@@ -135,6 +132,35 @@ __global__ void k_spread5(const P3MArgs a0, const P3MArgs *__restrict__ tab) {
         atomicAdd(reinterpret_cast<float4 *>(row + g0), v1);
         atomicAdd(reinterpret_cast<float4 *>(row + g1), v2);
     }
+}
+
+__global__ void k_spread5(const P3MArgs a0, const P3MArgs *__restrict__ tab) {
+    pdl_wait();
+    MDX_P3M_ARGS;
+    const int lane = threadIdx.x & 31;
+    const int t = lane % 5;
+    const int W = (A.n + 5) / 6;
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int i = (lane / 5) * W + w;
+    if (lane >= 30 || w >= W || i >= A.n) return;
+    spread_plane(A, i, t);
+}
+
+__device__ __forceinline__ int mol_site(int4 ix, int k, int four_site) {
+    return four_site ? (k == 0 ? ix.y : (k == 1 ? ix.z : ix.w)) : (k == 0 ? ix.x : (k == 1 ? ix.y : ix.z));
+}
+
+// the molecule form: lanes 15 j .. 15 j + 14 of a warp take the three
+// charged sites (five planes each) of one molecule, two molecules per warp,
+// the two W = nmol/2 apart; no lane is spent on an uncharged oxygen
+__global__ void k_spread_mol(const P3MArgs A) {
+    pdl_wait();
+    const int lane = threadIdx.x & 31;
+    const int W = (A.nmol + 1) / 2;
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int m = (lane / 15) * W + w;
+    if (lane >= 30 || w >= W || m >= A.nmol) return;
+    spread_plane(A, mol_site(A.mol_idx[m], (lane % 15) / 5, A.four_site), lane % 5);
 }
 
 // E_d(k) = i k_d G rho on the half spectrum (z halved), batched output
@@ -543,6 +569,53 @@ __global__ void __launch_bounds__(1024) k_ifft_yz(const FFTArgs A) {
 // gather on the interleaved field, five lanes per atom (six atoms per warp):
 // lane t sums the 25 points of stencil plane a = t with one 16-byte load per
 // point; the five partial fields are added with shuffles
+// the field at atom i's stencil plane a = t, weighted (one lane's share)
+__device__ __forceinline__ float3 gather_plane(const P3MArgs &A, const float4 *__restrict__ e4, int i, int t) {
+    const P3MGeom &g = A.g;
+    int3 ng;
+    float3 d;
+    stencil(g, A.xs[i], ng, d);
+    float wx[5], wy[5], wz[5];
+    w5(d.x, wx);
+    w5(d.y, wy);
+    w5(d.z, wz);
+    int pz[5];
+#pragma unroll
+    for (int c = 0; c < 5; c++) pz[c] = wrapi(ng.z + c - 2, g.sz.z);
+    const int px = wrapi(ng.x + t - 2, g.sz.x);
+    const float wa = pick5(wx, t);
+    float ex = 0.f, ey = 0.f, ez = 0.f;
+#pragma unroll
+    for (int b = 0; b < 5; b++) {
+        const int py = wrapi(ng.y + b - 2, g.sz.y);
+        const size_t row = ((size_t)px * g.sz.y + py) * g.sz.z;
+        const float wab = wa * wy[b];
+#pragma unroll
+        for (int c = 0; c < 5; c++) {
+            const float w = wab * wz[c];
+            const float4 e = __ldg(e4 + row + pz[c]);
+            ex += w * e.x;
+            ey += w * e.y;
+            ez += w * e.z;
+        }
+    }
+    return make_float3(ex, ey, ez);
+}
+
+// sum over the five lanes base .. base + 4 (valid in lane base); the whole
+// warp takes part
+__device__ __forceinline__ float3 group5_sum(float3 e, int base) {
+    float3 s = e;
+#pragma unroll
+    for (int k = 1; k < 5; k++) {
+        const int src = (base + k) & 31;
+        s.x += __shfl_sync(0xffffffffu, e.x, src);
+        s.y += __shfl_sync(0xffffffffu, e.y, src);
+        s.z += __shfl_sync(0xffffffffu, e.z, src);
+    }
+    return s;
+}
+
 template <bool ACC>
 __global__ void k_gather4(const P3MArgs A, const float4 *__restrict__ e4) {
     pdl_wait();
@@ -551,45 +624,8 @@ __global__ void k_gather4(const P3MArgs A, const float4 *__restrict__ e4) {
     const int i = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 6 + lane / 5;
     const bool valid = lane < 30 && i < A.n;
     const float q = valid ? A.qs[i] : 0.f;
-    float ex = 0.f, ey = 0.f, ez = 0.f;
-    const P3MGeom &g = A.g;
-    if (q != 0.f) {
-        int3 ng;
-        float3 d;
-        stencil(g, A.xs[i], ng, d);
-        float wx[5], wy[5], wz[5];
-        w5(d.x, wx);
-        w5(d.y, wy);
-        w5(d.z, wz);
-        int pz[5];
-#pragma unroll
-        for (int c = 0; c < 5; c++) pz[c] = wrapi(ng.z + c - 2, g.sz.z);
-        const int px = wrapi(ng.x + t - 2, g.sz.x);
-        const float wa = pick5(wx, t);
-#pragma unroll
-        for (int b = 0; b < 5; b++) {
-            const int py = wrapi(ng.y + b - 2, g.sz.y);
-            const size_t row = ((size_t)px * g.sz.y + py) * g.sz.z;
-            const float wab = wa * wy[b];
-#pragma unroll
-            for (int c = 0; c < 5; c++) {
-                const float w = wab * wz[c];
-                const float4 e = __ldg(e4 + row + pz[c]);
-                ex += w * e.x;
-                ey += w * e.y;
-                ez += w * e.z;
-            }
-        }
-    }
-    // whole warp takes part; lane base of each group of five adds the group
-    float sx = ex, sy = ey, sz = ez;
-#pragma unroll
-    for (int k = 1; k < 5; k++) {
-        const int src = (base + k) & 31;
-        sx += __shfl_sync(0xffffffffu, ex, src);
-        sy += __shfl_sync(0xffffffffu, ey, src);
-        sz += __shfl_sync(0xffffffffu, ez, src);
-    }
+    const float3 e = q != 0.f ? gather_plane(A, e4, i, t) : make_float3(0.f, 0.f, 0.f);
+    const float3 sm = group5_sum(e, base);
     if (!valid || t != 0) return;
     float4 *__restrict__ fs = A.fs;
     float4 f = fs[i];
@@ -597,17 +633,45 @@ __global__ void k_gather4(const P3MArgs A, const float4 *__restrict__ e4) {
         if (!ACC) fs[i] = make_float4(0.f, 0.f, 0.f, f.w);
         return;
     }
-    const float s = g.qunit * q * A.niv;
+    const float s = A.g.qunit * q * A.niv;
     if (ACC) {
-        f.x += s * sx;
-        f.y += s * sy;
-        f.z += s * sz;
+        f.x += s * sm.x;
+        f.y += s * sm.y;
+        f.z += s * sm.z;
     } else {
-        f.x = s * sx;
-        f.y = s * sy;
-        f.z = s * sz;
+        f.x = s * sm.x;
+        f.y = s * sm.y;
+        f.z = s * sm.z;
     }
     fs[i] = f;
+}
+
+// the molecule form of the gather into a per-step buffer (STORE): the
+// mapping of k_spread_mol, each charged site's force stored, the uncharged
+// oxygen of a four-site molecule stored as zero
+__global__ void k_gather_mol(const P3MArgs A, const float4 *__restrict__ e4) {
+    pdl_wait();
+    const int lane = threadIdx.x & 31;
+    const int t = lane % 5, base = lane - t;
+    const int W = (A.nmol + 1) / 2;
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int m = (lane / 15) * W + w;
+    const bool valid = lane < 30 && w < W && m < A.nmol;
+    const int k = (lane % 15) / 5;
+    int4 ix = make_int4(0, 0, 0, 0);
+    int i = 0;
+    float q = 0.f;
+    if (valid) {
+        ix = A.mol_idx[m];
+        i = mol_site(ix, k, A.four_site);
+        q = A.qs[i];
+    }
+    const float3 e = q != 0.f ? gather_plane(A, e4, i, t) : make_float3(0.f, 0.f, 0.f);
+    const float3 sm = group5_sum(e, base);
+    if (!valid || t != 0) return;
+    const float s = A.g.qunit * q * A.niv;
+    A.fs[i] = make_float4(s * sm.x, s * sm.y, s * sm.z, 0.f);
+    if (A.four_site && k == 0) A.fs[ix.x] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
 }  // namespace
@@ -853,6 +917,49 @@ int FixChargeEwald::gather_to(float4 *out, cudaStream_t st) {
         k_gather<false><<<(s.gpd.n + 127) / 128, 128, 0, st>>>(A, nullptr);
         MDX_LAUNCHED();
     }
+    return 0;
+}
+
+// the molecule form of spread and gather (every atom in a rigid molecule,
+// all molecules four-site with uncharged oxygens or all three-site, own FFT)
+bool FixChargeEwald::mol_form_ok(const FixRigid &r) const {
+    const State &s = *state;
+    if (!own_fft || r.mol_ids.empty() || !r.d_mol_idx.p) return false;
+    const bool four = r.mol_ids[0].w >= 0;
+    size_t members = 0;
+    for (const int4 &m : r.mol_ids) {
+        if ((m.w >= 0) != four) return false;
+        if (four && s.atoms[m.x].q != 0.0) return false;
+        members += four ? 4 : 3;
+    }
+    return members == s.atoms.size();
+}
+
+P3MArgs mol_args(State &s, FixChargeEwald &f, const FixRigid &r) {
+    P3MArgs A = p3m_args(s, f);
+    A.mol_idx = r.d_mol_idx.p;
+    A.nmol = (int)r.mol_ids.size();
+    A.four_site = r.mol_ids[0].w >= 0 ? 1 : 0;
+    return A;
+}
+
+int FixChargeEwald::spread_mol(cudaStream_t st, const FixRigid &r) {
+    State &s = *state;
+    const size_t ng = (size_t)sz.x * sz.y * sz.z;
+    MDX_CUDA_TRY(cudaMemsetAsync(rho.p, 0, ng * sizeof(float), st));
+    const P3MArgs A = mol_args(s, *this, r);
+    const int warps = (A.nmol + 1) / 2;
+    MDX_CUDA_TRY(launch_pdl_prio(true, k_spread_mol, dim3((warps + 7) / 8), dim3(256), 0, st, A));
+    return 0;
+}
+
+int FixChargeEwald::gather_mol_to(float4 *out, cudaStream_t st, const FixRigid &r) {
+    State &s = *state;
+    P3MArgs A = mol_args(s, *this, r);
+    A.fs = out;
+    const int warps = (A.nmol + 1) / 2;
+    MDX_CUDA_TRY(launch_pdl_prio(true, k_gather_mol, dim3((warps + 7) / 8), dim3(256), 0, st, A,
+                                 (const float4 *)e4.p));
     return 0;
 }
 

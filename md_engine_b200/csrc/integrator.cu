@@ -77,10 +77,14 @@ class IntegratorVerlet {
         const bool recip_side = ew && s->rigidFix() && !has_free_atoms(*s);
         if (ew) {
             MDX_CUDA_TRY(cudaStreamWaitEvent(s->side[0], s->ev_fork, 0));
-            if (int e = ew->spread(s->side[0])) return e;
+            // all-rigid water: spread and gather by molecule (charged sites only)
+            const bool by_mol = recip_side && ew->mol_form_ok(*s->rigidFix());
+            if (int e = by_mol ? ew->spread_mol(s->side[0], *s->rigidFix()) : ew->spread(s->side[0])) return e;
             if (int e = ew->solve(s->side[0])) return e;
             if (recip_side)
-                if (int e = ew->gather_to(ew->f_recip.p, s->side[0])) return e;
+                if (int e = by_mol ? ew->gather_mol_to(ew->f_recip.p, s->side[0], *s->rigidFix())
+                                   : ew->gather_to(ew->f_recip.p, s->side[0]))
+                    return e;
             MDX_CUDA_TRY(cudaEventRecord(s->ev_join[0], s->side[0]));
         }
         if (e3side) {
