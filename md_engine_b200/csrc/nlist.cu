@@ -237,7 +237,7 @@ __global__ void k_gather(const GridArgs a0, const GridArgs *__restrict__ tab) {
 constexpr int kBuildCellsPerBlock = 4;            // one warp per cell
 constexpr int kStencilMax = 4;                    // largest m (cells >= cut/m)
 constexpr int kBuildSegMax = 2 * (2 * kStencilMax + 1) * (2 * kStencilMax + 1);  // two z segments per row
-constexpr int kCandWin = 2048;                    // expanded candidates per warp and window
+constexpr int kCandWin = 1536;                    // expanded candidates per warp and window
 constexpr int kCandIdxBits = 27;                  // sorted index bits of an expanded candidate
 
 struct BuildArgs {
@@ -283,7 +283,7 @@ __device__ __forceinline__ uint32_t excl_depth(const BuildArgs &A, uint32_t myid
 }
 
 template <int TP, int HG, bool COUNT>
-__global__ void __launch_bounds__(kBuildCellsPerBlock * 32) k_build_cells(const BuildArgs a0,
+__global__ void __launch_bounds__(kBuildCellsPerBlock * 32, 6) k_build_cells(const BuildArgs a0,
                                                                             const BuildArgs *__restrict__ tab) {
     pdl_wait();
     const BuildArgs A = tab ? tab[blockIdx.y] : a0;
