@@ -40,6 +40,7 @@ struct PairArgs {
     float qrc2, alpha, qqr;
     float *__restrict__ virials;
     float *__restrict__ energy;  // per-atom (energy kernel)
+    uint32_t lj_types;           // bit ti: type ti has a pair with eps != 0
 };
 
 // erfc(x) for x >= 0 by Abramowitz & Stegun, Handbook of Mathematical
@@ -117,8 +118,63 @@ __device__ __forceinline__ bool pair_term(const PairArgs &A, const float *sp, in
     return any;
 }
 
+// one lane's share of atom i's row: U entries per trip -- all list loads,
+// then all position and charge gathers, then the arithmetic, so U memory
+// chains are in flight per lane instead of one dependent list->position chain
+template <int T, int LJ, bool EW, bool VIR, bool ENERGY>
+__device__ __forceinline__ void pair_row(const PairArgs &A, const float *sp, int nt2, int i, int ti, float qi,
+                                         float4 xi, const uint32_t *row, int cnt, int t, float &fx, float &fy,
+                                         float &fz, float &en, float (&v)[6]) {
+    constexpr int U = 4;
+    constexpr uint32_t kNone = 0xffffffffu;
+    for (int k0 = t; k0 < cnt; k0 += U * T) {
+        uint32_t ent[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int k = k0 + u * T;
+            ent[u] = k < cnt ? __ldg(row + (size_t)(k / T) * 32) : kNone;
+        }
+        float4 xj[U];
+        float qj[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int j = ent[u] == kNone ? i : (int)(ent[u] & kExclMask);
+            xj[u] = __ldg(A.xs + j);
+            qj[u] = EW ? __ldg(A.qs + j) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (ent[u] == kNone) continue;
+            const uint32_t tag = ent[u] >> 30;
+            float mult = 1.0f;
+            if (tag) mult = tag == 1u ? A.coef1 : (tag == 2u ? A.coef2 : A.coef3);
+            const float3 dr = min_image(A.box, make_float3(xi.x - xj[u].x, xi.y - xj[u].y, xi.z - xj[u].z));
+            const float r2 = dot3(dr, dr);
+            float s, eng;
+            if (pair_term<LJ, EW, ENERGY>(A, sp, nt2, ti, qi, xj[u], qj[u], dr, r2, mult, s, eng)) {
+                const float Fx = dr.x * s, Fy = dr.y * s, Fz = dr.z * s;
+                fx += Fx;
+                fy += Fy;
+                fz += Fz;
+                if (ENERGY) en += eng;
+                if (VIR) {
+                    v[0] += Fx * dr.x;
+                    v[1] += Fy * dr.y;
+                    v[2] += Fz * dr.z;
+                    v[3] += Fx * dr.y;
+                    v[4] += Fx * dr.z;
+                    v[5] += Fy * dr.z;
+                }
+            }
+        }
+    }
+}
+
 // tab: one argument record per replica (batched launch, blockIdx.y = replica)
-// or null (single system, a0)
+// or null (single system, a0).  With both LJ and Ewald terms, a warp whose
+// atoms have no LJ partner type (water H, M) runs the row without the LJ
+// term, and one whose atoms are all uncharged (water O) without the Ewald
+// term: both contribute exactly zero there, and the choice is warp-uniform.
 template <int T, int LJ, bool EW, bool VIR, bool ENERGY>
 __global__ void __launch_bounds__(256) k_pair(const PairArgs a0, const PairArgs *__restrict__ tab, int accumulate) {
     pdl_wait();
@@ -136,61 +192,31 @@ __global__ void __launch_bounds__(256) k_pair(const PairArgs a0, const PairArgs 
     const int i = warp * G + a;
     const bool valid = i < A.n;
     float fx = 0.f, fy = 0.f, fz = 0.f, en = 0.f;
-    float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f, v4 = 0.f, v5 = 0.f;
+    float v[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
+    int ti = 0, cnt = 0;
+    float qi = 0.f;
+    const uint32_t *row = nullptr;
     if (valid) {
         xi = A.xs[i];
-        const int ti = type_of(xi);
-        const float qi = EW ? A.qs[i] : 0.f;
-        int cnt = (int)A.counts[i];
+        ti = type_of(xi);
+        qi = EW ? A.qs[i] : 0.f;
+        cnt = (int)A.counts[i];
         cnt = cnt < A.cap ? cnt : A.cap;
-        const uint32_t *row = A.nlist + (size_t)(i / G) * A.cap * G + a * T + t;
-        // U entries per lane per trip: all list loads, then all position and
-        // charge gathers, then the arithmetic -- U independent memory chains
-        // in flight per lane instead of one dependent list->position chain
-        constexpr int U = 4;
-        constexpr uint32_t kNone = 0xffffffffu;
-        for (int k0 = t; k0 < cnt; k0 += U * T) {
-            uint32_t ent[U];
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                const int k = k0 + u * T;
-                ent[u] = k < cnt ? __ldg(row + (size_t)(k / T) * 32) : kNone;
-            }
-            float4 xj[U];
-            float qj[U];
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                const int j = ent[u] == kNone ? i : (int)(ent[u] & kExclMask);
-                xj[u] = __ldg(A.xs + j);
-                qj[u] = EW ? __ldg(A.qs + j) : 0.f;
-            }
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                if (ent[u] == kNone) continue;
-                const uint32_t tag = ent[u] >> 30;
-                float mult = 1.0f;
-                if (tag) mult = tag == 1u ? A.coef1 : (tag == 2u ? A.coef2 : A.coef3);
-                const float3 dr = min_image(A.box, make_float3(xi.x - xj[u].x, xi.y - xj[u].y, xi.z - xj[u].z));
-                const float r2 = dot3(dr, dr);
-                float s, eng;
-                if (pair_term<LJ, EW, ENERGY>(A, sp, nt2, ti, qi, xj[u], qj[u], dr, r2, mult, s, eng)) {
-                    const float Fx = dr.x * s, Fy = dr.y * s, Fz = dr.z * s;
-                    fx += Fx;
-                    fy += Fy;
-                    fz += Fz;
-                    if (ENERGY) en += eng;
-                    if (VIR) {
-                        v0 += Fx * dr.x;
-                        v1 += Fy * dr.y;
-                        v2 += Fz * dr.z;
-                        v3 += Fx * dr.y;
-                        v4 += Fx * dr.z;
-                        v5 += Fy * dr.z;
-                    }
-                }
-            }
+        row = A.nlist + (size_t)(i / G) * A.cap * G + a * T + t;
+    }
+    if (LJ && EW) {
+        const bool lj_row = valid && ti < 32 && ((A.lj_types >> ti) & 1u);
+        const bool q_row = valid && qi != 0.f;
+        if (!__any_sync(0xffffffffu, lj_row)) {
+            if (valid) pair_row<T, 0, true, VIR, ENERGY>(A, sp, nt2, i, ti, qi, xi, row, cnt, t, fx, fy, fz, en, v);
+        } else if (!__any_sync(0xffffffffu, q_row)) {
+            if (valid) pair_row<T, LJ, false, VIR, ENERGY>(A, sp, nt2, i, ti, qi, xi, row, cnt, t, fx, fy, fz, en, v);
+        } else if (valid) {
+            pair_row<T, LJ, EW, VIR, ENERGY>(A, sp, nt2, i, ti, qi, xi, row, cnt, t, fx, fy, fz, en, v);
         }
+    } else if (valid) {
+        pair_row<T, LJ, EW, VIR, ENERGY>(A, sp, nt2, i, ti, qi, xi, row, cnt, t, fx, fy, fz, en, v);
     }
     // invalid lanes carry zeros; whole warp takes part in the shuffles
     if (ENERGY) {
@@ -202,12 +228,8 @@ __global__ void __launch_bounds__(256) k_pair(const PairArgs a0, const PairArgs 
     fy = team_sum<T>(fy);
     fz = team_sum<T>(fz);
     if (VIR) {
-        v0 = team_sum<T>(v0);
-        v1 = team_sum<T>(v1);
-        v2 = team_sum<T>(v2);
-        v3 = team_sum<T>(v3);
-        v4 = team_sum<T>(v4);
-        v5 = team_sum<T>(v5);
+#pragma unroll
+        for (int c = 0; c < 6; c++) v[c] = team_sum<T>(v[c]);
     }
     if (valid && t == 0) {
         float4 f = A.fs[i];
@@ -222,13 +244,9 @@ __global__ void __launch_bounds__(256) k_pair(const PairArgs a0, const PairArgs 
         }
         A.fs[i] = f;
         if (VIR) {
-            float *v = A.virials + 6 * (size_t)i;
-            v[0] += 0.5f * v0;
-            v[1] += 0.5f * v1;
-            v[2] += 0.5f * v2;
-            v[3] += 0.5f * v3;
-            v[4] += 0.5f * v4;
-            v[5] += 0.5f * v5;
+            float *vv = A.virials + 6 * (size_t)i;
+#pragma unroll
+            for (int c = 0; c < 6; c++) vv[c] += 0.5f * v[c];
         }
     }
 }
@@ -303,6 +321,15 @@ PairArgs make_args(State &s, FixPair &f) {
     }
     A.virials = s.gpd.virials.p;
     A.energy = nullptr;
+    // types with an LJ partner (eps != 0); every type when unknown
+    A.lj_types = 0xffffffffu;
+    const int nt = A.ntypes;
+    if (nt <= 32 && f.h_params.size() == (size_t)3 * nt * nt) {
+        A.lj_types = 0u;
+        for (int x = 0; x < nt; x++)
+            for (int y = 0; y < nt; y++)
+                if (f.h_params[(size_t)nt * nt + x * nt + y] != 0.f) A.lj_types |= 1u << x;
+    }
     return A;
 }
 
@@ -379,6 +406,7 @@ int pair_force_raw(int n, const float4 *xs, float4 *fs, const float *qs, const u
     A.qqr = qqr;
     A.virials = virials;
     A.energy = nullptr;
+    A.lj_types = 0xffffffffu;  // parameters live on the device here: no skipping
     bool ew = qrc > 0.f;
     if (lj_kind == 0 && !ew) return 0;
     int r = launch_any(A, team, lj_kind, ew, virials != nullptr, false, accumulate, stream);
