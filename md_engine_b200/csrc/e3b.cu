@@ -600,10 +600,15 @@ static dim3 e3b_blocks(int nmol, unsigned nrep = 1) {
     return dim3((warps * 32 + 255) / 256, nrep);
 }
 
-int e3b_build_list(State &s, FixE3B &f, bool conditional) {
+// part of a list rebuild, after the sort: the O-O distances are taken on the
+// sorted copy of this build's positions (xs_alt), which the step's first half
+// running beside it on another stream does not move
+int e3b_build_list(State &s, FixE3B &f, bool conditional, cudaStream_t st) {
     const int nmol = (int)f.mol_ids.size();
     if (nmol == 0 || !f.prepared) return 0;
-    MDX_CUDA_TRY(launch_pdl(k_e3b_list<kMolTeam>, e3b_blocks(nmol), dim3(256), 0, s.stream, e3b_args(s, f, nullptr),
+    E3BArgs A = e3b_args(s, f, nullptr);
+    A.xs = s.gpd.xs_alt.p;
+    MDX_CUDA_TRY(launch_pdl(k_e3b_list<kMolTeam>, e3b_blocks(nmol), dim3(256), 0, st ? st : s.stream, A,
                             (const E3BArgs *)nullptr, conditional ? 1 : 0));
     return 0;
 }

@@ -404,8 +404,10 @@ class State {
     DBuf<unsigned int> red_counter;
     cudaStream_t stream = nullptr;
     bool own_stream = true;
-    cudaStream_t side[2] = {nullptr, nullptr};  // concurrent branches of the fused step
-    cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
+    // concurrent branches of the fused step: P3M, E3B, and the list build of
+    // a rebuild step
+    cudaStream_t side[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_join[3] = {nullptr, nullptr, nullptr}, ev_sorted = nullptr;
     bool uploaded = false;   // device copy is authoritative
     bool prepared = false;
     bool requiresCharges = false;
@@ -496,7 +498,7 @@ int batch_rigid_maps(Batch &b);
 
 // ---------------------------------------------------------------- kernels
 // neighbour list (nlist.cu)
-int nlist_rebuild(State &s, bool force, bool conditional);
+int nlist_rebuild(State &s, bool force, bool conditional, cudaStream_t bstream = nullptr);
 int nlist_init(State &s);
 int nlist_exclusions(State &s);
 int nlist_set_interactions(State &s);
@@ -508,7 +510,7 @@ int pair_force_raw(int n, const float4 *xs, float4 *fs, const float *qs, const u
                    const float coef[3], int lj_kind, float qrc, float alpha, float qqr, float *virials,
                    bool accumulate, cudaStream_t stream);
 // e3b (e3b.cu)
-int e3b_build_list(State &s, FixE3B &f, bool conditional);
+int e3b_build_list(State &s, FixE3B &f, bool conditional, cudaStream_t st = nullptr);
 int e3b_forces(State &s, FixE3B &f);
 int e3b_forces_to(State &s, FixE3B &f, float4 *out, bool side, cudaStream_t stream);
 int e3b_energy(State &s, FixE3B &f, double out[2]);

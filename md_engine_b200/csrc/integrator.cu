@@ -89,12 +89,18 @@ class IntegratorVerlet {
         }
         if (e3side) {
             MDX_CUDA_TRY(cudaStreamWaitEvent(s->side[1], s->ev_fork, 0));
+            if (build_pending) MDX_CUDA_TRY(cudaStreamWaitEvent(s->side[1], s->ev_join[2], 0));
             if (e3->sur && e3->sur->enabled) {
                 if (int e = surrogate_forces_to(*s, *e3, e3->f_side.p, s->side[1])) return e;
             } else {
                 if (int e = e3b_forces_to(*s, *e3, e3->f_side.p, true, s->side[1])) return e;
             }
             MDX_CUDA_TRY(cudaEventRecord(s->ev_join[1], s->side[1]));
+        }
+        if (build_pending) {
+            // the lists are read from here on
+            MDX_CUDA_TRY(cudaStreamWaitEvent(s->stream, s->ev_join[2], 0));
+            build_pending = false;
         }
         if (pf)
             if (int e = pair_launch(*s, *pf, 0, false)) return e;
@@ -115,11 +121,20 @@ class IntegratorVerlet {
         if (int e = step_second_half(*s, false)) return e;
         return 0;
     }
+    // fused graphs: the list build of a rebuild step runs on side stream 2
+    // beside the step's first half and P3M chain; the pair kernel and E3B of
+    // that step wait for it (build_pending)
+    bool build_pending = false;
     int enqueue(int nsteps, bool with_group) {
-        if (with_group)
-            if (int e = nlist_rebuild(*s, false, true)) return e;
+        if (with_group) {
+            const bool overlap = mode == 0 && s->grid.cap != 0;
+            if (int e = nlist_rebuild(*s, false, true, overlap ? s->side[2] : nullptr)) return e;
+            build_pending = overlap;
+        }
         for (int k = 0; k < nsteps; k++)
             if (int e = stepBody()) return e;
+        if (build_pending) MDX_CUDA_TRY(cudaStreamWaitEvent(s->stream, s->ev_join[2], 0));
+        build_pending = false;
         return 0;
     }
     int getGraph(int nsteps, bool with_group, cudaGraphExec_t *out) {

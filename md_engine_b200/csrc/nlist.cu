@@ -59,7 +59,7 @@ struct GridArgs {
     float4 *xs2, *vs2, *fs2;
     float *qs2;
     uint32_t *ids2;
-    const float4 *xs_last;
+    float4 *xs_last;
     int *idToIdx;
     int *cell_of;
     uint32_t *cell_count, *cell_start, *cell_fill;
@@ -120,6 +120,9 @@ __global__ void k_wrap_bin(const GridArgs a0, const GridArgs *__restrict__ tab) 
 
 // exclusive scan of the cell histogram in one block per system (replaces the
 // host cumulativeSum, helpers.h:15-24); also clears the fill counters
+// exclusive scan of the cell counts (one block): thread t owns a contiguous
+// run of cells, so its counts are loaded together (one memory round trip),
+// summed serially, and the run totals are scanned once across the block
 __global__ void k_scan_cells(const GridArgs a0, const GridArgs *__restrict__ tab) {
     MDX_GRID_ARGS;
     if (!A.st->rebuild) return;
@@ -128,39 +131,37 @@ __global__ void k_scan_cells(const GridArgs a0, const GridArgs *__restrict__ tab
     uint32_t *__restrict__ fill = A.cell_fill;
     const int ncell = A.ncell;
     __shared__ uint32_t warp_tot[32];
-    __shared__ uint32_t carry;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int base = 0; base < ncell; base += blockDim.x) {
-        int c = base + threadIdx.x;
-        uint32_t v = c < ncell ? count[c] : 0u;
-        if (c < ncell) fill[c] = 0u;
-        uint32_t x = v;
+    const int per = (ncell + blockDim.x - 1) / blockDim.x;
+    const int c0 = min(ncell, (int)threadIdx.x * per), c1 = min(ncell, c0 + per);
+    uint32_t run = 0u;
+    for (int c = c0; c < c1; c++) run += count[c];
+    uint32_t x = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_tot[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        uint32_t t = lane < nw ? warp_tot[lane] : 0u;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
+            const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
         }
-        if (lane == 31) warp_tot[w] = x;
-        __syncthreads();
-        if (w == 0) {
-            uint32_t t = lane < nw ? warp_tot[lane] : 0u;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
-                if (lane >= o) t += y;
-            }
-            if (lane < nw) warp_tot[lane] = t;
-        }
-        __syncthreads();
-        uint32_t excl = carry + (w > 0 ? warp_tot[w - 1] : 0u) + x - v;
-        if (c < ncell) start[c] = excl;
-        __syncthreads();
-        if (threadIdx.x == blockDim.x - 1) carry = excl + v;
-        __syncthreads();
+        if (lane < nw) warp_tot[lane] = t;
     }
-    if (threadIdx.x == 0) start[ncell] = carry;
+    __syncthreads();
+    uint32_t excl = (w > 0 ? warp_tot[w - 1] : 0u) + x - run;
+    for (int c = c0; c < c1; c++) {
+        const uint32_t v = count[c];
+        start[c] = excl;
+        fill[c] = 0u;
+        excl += v;
+    }
+    if (threadIdx.x == blockDim.x - 1) start[ncell] = excl;
 }
 
 __global__ void k_scatter(const GridArgs a0, const GridArgs *__restrict__ tab) {
@@ -214,6 +215,22 @@ __global__ void k_gather(const GridArgs a0, const GridArgs *__restrict__ tab) {
     A.idToIdx[id] = d;
 }
 
+// the sorted streams back into the primary buffers (the captured graph keeps
+// the same pointers), and the positions of this build for the skin check
+__global__ void k_copyback(const GridArgs a0, const GridArgs *__restrict__ tab) {
+    MDX_GRID_ARGS;
+    if (!A.st->rebuild) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    const float4 p = A.xs2[i];
+    A.xs[i] = p;
+    A.xs_last[i] = p;
+    A.vs[i] = A.vs2[i];
+    A.fs[i] = A.fs2[i];
+    A.qs[i] = A.qs2[i];
+    A.ids[i] = A.ids2[i];
+}
+
 // assignNeighbors / assignFromCell (GridGPU.cu:482-734) with the exclusion
 // lookup of addExclusion (GridGPU.cu:466-478), one warp per home cell.
 // The candidates of the cell -- its (2m+1)^2 stencil rows, each row's z range
@@ -233,7 +250,7 @@ __global__ void k_gather(const GridArgs a0, const GridArgs *__restrict__ tab) {
 // and the entries written for one home atom at a time are consecutive slots
 // of its row.  Exclusion depths come from the id-window bit planes (the id
 // list only for atoms with far exclusions).  COUNT counts alone to size the
-// first build.  Also copies the sorted streams back to the primary buffers.
+// first build.
 constexpr int kBuildCellsPerBlock = 4;            // one warp per cell
 constexpr int kStencilMax = 4;                    // largest m (cells >= cut/m)
 constexpr int kBuildSegMax = 2 * (2 * kStencilMax + 1) * (2 * kStencilMax + 1);  // two z segments per row
@@ -321,18 +338,10 @@ __global__ void __launch_bounds__(kBuildCellsPerBlock * 32, 6) k_build_cells(con
     uint32_t *const nlist = A.nlist;
     const float dsx = 1.0f / g.inv_ds.x, dsy = 1.0f / g.inv_ds.y, dsz = 1.0f / g.inv_ds.z;
     const uint32_t lt = (1u << lane) - 1u;
-    // copy the home atoms' sorted streams back; bounding box of their positions
+    // bounding box of the home atoms' positions
     float bxl = 3.0e38f, bxh = -3.0e38f, byl = 3.0e38f, byh = -3.0e38f, bzl = 3.0e38f, bzh = -3.0e38f;
     for (int i = cs + lane; i < ce; i += 32) {
         const float4 p4 = A.xs2[i];
-        if (!COUNT) {
-            A.xs[i] = p4;
-            A.xs_last[i] = p4;
-            A.vs[i] = A.vs2[i];
-            A.fs[i] = A.fs2[i];
-            A.qs[i] = A.qs2[i];
-            A.ids[i] = A.ids2[i];
-        }
         bxl = fminf(bxl, p4.x);
         bxh = fmaxf(bxh, p4.x);
         byl = fminf(byl, p4.y);
@@ -674,9 +683,9 @@ inline dim3 build_grid(int ncell, int nrep) {
     return dim3((ncell + kBuildCellsPerBlock - 1) / kBuildCellsPerBlock, nrep);
 }
 
-void launch_build(State &s, const CellGrid &g, float cutsq) {
+void launch_build(State &s, const CellGrid &g, float cutsq, cudaStream_t st) {
     const BuildArgs A = build_args(s, g, cutsq);
-    launch_build_any<false>(s.grid.team, s.grid.home_group, build_grid(A.ncell, 1), s.stream, A, nullptr);
+    launch_build_any<false>(s.grid.team, s.grid.home_group, build_grid(A.ncell, 1), st, A, nullptr);
 }
 
 void launch_count(State &s, const CellGrid &g, float cutsq) {
@@ -855,7 +864,11 @@ int nlist_init(State &s) {
 // GridGPU::periodicBoundaryConditions (GridGPU.cu:824-1103).  conditional:
 // run the check kernel that decides on the device (graph mode); otherwise
 // the rebuild is forced (force=true) or decided by the same check.
-int nlist_rebuild(State &s, bool force, bool conditional) {
+// bstream (optional): the list build, the E3B molecule list and k_finish go
+// to that stream after the sort, so the caller can run the step's first half
+// and the P3M chain beside them; it waits on s.ev_join[2] (recorded at the
+// end of bstream) before anything that reads the lists.
+int nlist_rebuild(State &s, bool force, bool conditional, cudaStream_t bstream) {
     GridGPU &gr = s.grid;
     GPUData &d = s.gpd;
     const int n = d.n;
@@ -872,6 +885,11 @@ int nlist_rebuild(State &s, bool force, bool conditional) {
     MDX_CUDA_TRY(launch_pdl(k_scatter, dim3(nb), dim3(256), 0, s.stream, A, nt));
     MDX_CUDA_TRY(launch_pdl(k_rank, dim3((ncell * 32 + 255) / 256), dim3(256), 0, s.stream, A, nt));
     MDX_CUDA_TRY(launch_pdl(k_gather, dim3(nb), dim3(256), 0, s.stream, A, nt));
+    MDX_CUDA_TRY(launch_pdl(k_copyback, dim3(nb), dim3(256), 0, s.stream, A, nt));
+    // molecule maps of the fixes that keep atom indices
+    if (FixRigid *r = s.rigidFix()) {
+        if (int e = rigid_update_maps(s, *r, true)) return e;
+    }
     if (gr.cap == 0) {
         // first build: size the per-atom capacity from a counting sweep
         MDX_CUDA_TRY(cudaMemsetAsync(&s.d_status.p->max_neighbors, 0, sizeof(uint32_t), s.stream));
@@ -886,15 +904,18 @@ int nlist_rebuild(State &s, bool force, bool conditional) {
         size_t groups = (size_t)(n + (32 / gr.team) - 1) / (32 / gr.team);
         if (int e = gr.nlist.alloc(groups * (size_t)c * (32 / gr.team))) return e;
     }
-    launch_build(s, g, cutsq);
-    // molecule maps / molecule list of the fixes that keep atom indices
-    if (FixRigid *r = s.rigidFix()) {
-        if (int e = rigid_update_maps(s, *r, true)) return e;
+    cudaStream_t bs = s.stream;
+    if (bstream) {
+        MDX_CUDA_TRY(cudaEventRecord(s.ev_sorted, s.stream));
+        MDX_CUDA_TRY(cudaStreamWaitEvent(bstream, s.ev_sorted, 0));
+        bs = bstream;
     }
+    launch_build(s, g, cutsq, bs);
     if (FixE3B *e3 = s.e3bFix()) {
-        if (int e = e3b_build_list(s, *e3, true)) return e;
+        if (int e = e3b_build_list(s, *e3, true, bs)) return e;
     }
-    MDX_CUDA_TRY(launch_pdl(k_finish, dim3(1), dim3(1024), 0, s.stream, A, (const GridArgs *)nullptr));
+    MDX_CUDA_TRY(launch_pdl(k_finish, dim3(1), dim3(1024), 0, bs, A, (const GridArgs *)nullptr));
+    if (bs != s.stream) MDX_CUDA_TRY(cudaEventRecord(s.ev_join[2], bs));
     gr.built = true;
     return 0;
 }
@@ -940,10 +961,11 @@ int batch_nlist_rebuild(Batch &b) {
     k_scatter<<<nb, 256, 0, st>>>(A, tg);
     k_rank<<<dim3((b.max_cell * 32 + 255) / 256, R), 256, 0, st>>>(A, tg);
     k_gather<<<nb, 256, 0, st>>>(A, tg);
+    k_copyback<<<nb, 256, 0, st>>>(A, tg);
     int hg = 2;
     for (State *r : b.reps) hg = std::max(hg, r->grid.home_group);
     launch_build_any<false>(s0.grid.team, hg, build_grid(b.max_cell, R), st, B, tb);
-    g_launches += 6;
+    g_launches += 7;
     if (int e = batch_rigid_maps(b)) return e;
     if (s0.e3bFix())
         if (int e = batch_e3b_list(b)) return e;

@@ -41,11 +41,12 @@ State::State() {
 
 State::~State() {
     if (h_status) cudaFreeHost(h_status);
-    for (int k = 0; k < 2; k++) {
+    for (int k = 0; k < 3; k++) {
         if (side[k]) cudaStreamDestroy(side[k]);
         if (ev_join[k]) cudaEventDestroy(ev_join[k]);
     }
     if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_sorted) cudaEventDestroy(ev_sorted);
     if (stream && own_stream) cudaStreamDestroy(stream);
 }
 
@@ -106,11 +107,12 @@ int State::upload() {
         MDX_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         own_stream = true;
     }
-    for (int k = 0; k < 2; k++) {
+    for (int k = 0; k < 3; k++) {
         if (!side[k]) MDX_CUDA_TRY(cudaStreamCreateWithFlags(&side[k], cudaStreamNonBlocking));
         if (!ev_join[k]) MDX_CUDA_TRY(cudaEventCreateWithFlags(&ev_join[k], cudaEventDisableTiming));
     }
     if (!ev_fork) MDX_CUDA_TRY(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    if (!ev_sorted) MDX_CUDA_TRY(cudaEventCreateWithFlags(&ev_sorted, cudaEventDisableTiming));
     if (!h_status) MDX_CUDA_TRY(cudaMallocHost(&h_status, sizeof(DeviceStatus)));
     if (int e = d_status.alloc(1)) return e;
     MDX_CUDA_TRY(cudaMemset(d_status.p, 0, sizeof(DeviceStatus)));
