@@ -238,14 +238,17 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line))
 
 
-def batched_states(nrep, seed, e3b=True):
+def batched_states(nrep, seed, e3b=True, subset=None):
     """the batched-replica workload: nrep TIP4P/2005(+E3B3) boxes, molecule
     counts log-uniform in [256, 2048], T uniform in [260, 360] K, rc 9 A,
-    skin 0.8 A, P3M mesh 32^3 or 64^3 by box size"""
+    skin 0.8 A, P3M mesh 32^3 or 64^3 by box size; subset: build only these
+    replica indices (each replica is seeded by its index, whoever builds it)"""
     from md_engine_b200 import systems
     sizes, temps = systems.water_replica_sizes(nrep, seed=seed)
     out = []
     for r, (m, T) in enumerate(zip(sizes, temps)):
+        if subset is not None and r not in subset:
+            continue
         sysd = systems.water_tip4p2005(nmol=int(m), T=float(T), seed=seed + 1000 + r)
         st, _ = systems.build_water_state(sysd, rcut=9.0, skin=0.8, dt=2.0, interval=10,
                                           grid=systems.p3m_mesh_for(sysd.L[0]), e3b=e3b, T=float(T), tau=100.0)
@@ -269,10 +272,18 @@ def run_batched(args, rank, world, local):
     one after another through IntegratorVerlet (the plain per-replica path)"""
     import torch
     from md_engine_b200 import BatchReplicas, IntegratorVerlet, kernel_launches
+    from md_engine_b200 import systems
+    from md_engine_b200.replicas import gather_replica_scalars, shard_by_sites
     dist = init_pg(world, "nccl")
     dev = torch.device("cuda", local)
-    seed = 20261203 + 7919 * rank
-    reps = batched_states(args.replicas, seed)
+    # one ensemble of replicas x world boxes (per-GPU work fixed: weak
+    # scaling), dealt to the ranks by balanced site count; no exchange while
+    # stepping, one gather of per-replica scalars at the end
+    seed = 20261203
+    total = args.replicas * world
+    sizes, _ = systems.water_replica_sizes(total, seed=seed)
+    mine = shard_by_sites([4 * int(m) for m in sizes], world)[rank]
+    reps = batched_states(total, seed, subset=set(mine))
     states = [s for s, _ in reps]
     mols = sum(m for _, m in reps)
     b = BatchReplicas(states)
@@ -288,24 +299,32 @@ def run_batched(args, rank, world, local):
     barrier(dist, dev)
     ms_max = reduce_max(dist, ms, dev)
     R = len(states)
-    value = world * R * K / (ms_max * 1e-3)
+    value = total * K / (ms_max * 1e-3)
+    # the end-of-run collective: every replica's temperature, in replica order
+    temps = []
+    for st in states:
+        mv2, ndf = st.kinetic()
+        temps.append(mv2 * systems.MVV_TO_ENG_REAL / (max(ndf, 1.0) * systems.BOLTZ_REAL))
+    all_t = gather_replica_scalars(dist, mine, temps, total, device=dev)
     # the plain path: every replica alone (fresh copies), same step count
     seq_ms = 0.0
     Ks = min(K, 50)
-    for st, _ in batched_states(args.replicas, seed):
+    for st, _ in batched_states(total, seed, subset=set(mine)):
         it = IntegratorVerlet(st)
         it.run(3)
         seq_ms += it.runTimed(Ks, 10, 0)
     seq = R * Ks / (seq_ms * 1e-3)
     if rank == 0:
-        cfg = {"workload": f"{R} TIP4P/2005+E3B3 replicas, {mols} molecules, sizes log-uniform 256-2048, "
-                           "T 260-360 K, rc 9 A, skin 0.8 A, P3M 32^3/64^3",
-               "replicas": R, "molecules": mols, "autotuned_team": team,
+        cfg = {"workload": f"{total} TIP4P/2005+E3B3 replicas ({args.replicas} per GPU), sizes log-uniform "
+                           "256-2048 molecules, T 260-360 K, rc 9 A, skin 0.8 A, P3M 32^3/64^3",
+               "replicas": total, "replicas_rank0": R, "molecules_rank0": mols, "autotuned_team": team,
                "l2": "flushed between timed 10-step chunks (256 MiB write)",
-               "parallelism": "replicas only" if world > 1 else "one batch"}
+               "parallelism": f"replicas dealt to {world} GPUs by site count" if world > 1 else "one batch"}
         side_line(args, world, value, "replica timesteps/s", K, ms_max, cfg,
                   {"sequential_plain": {"value": seq, "unit": "replica timesteps/s", "steps_per_replica": Ks},
-                   "batched_over_sequential": value / world / seq}, clk, int(k1 - k0))
+                   "batched_over_sequential": (R * K / (ms * 1e-3)) / seq,
+                   "replica_temperature_K": {"mean": float(np.mean(all_t)), "min": float(np.min(all_t)),
+                                             "max": float(np.max(all_t))}}, clk, int(k1 - k0))
     if dist is not None:
         barrier(dist, dev)
         dist.destroy_process_group()
