@@ -178,6 +178,12 @@ int mdx_kinetic(mdx_state *st, double *sum_mv2, double *ndf);
  * per device) and should come before any stream capture; all calls share the
  * array, so calls whose kernels overlap on the GPU race. */
 int mdx_kinetic_noalloc(mdx_state *st, double *sum_mv2);
+/* DataComputerPressure::computeScalar_CPU (src/DataStorageUser/
+ * DataComputerPressure.cu:76-92): scalar pressure (sum m v^2 + virial trace)
+ * / (3 V) * nktv_to_press from a virial-mode force evaluation at the current
+ * positions (pair, P3M reciprocal, E3B); virial6 (may be NULL) gets the total
+ * virial.  The forces the integrator holds are restored afterwards. */
+int mdx_pressure(mdx_state *st, double *pressure, double virial6[6]);
 /* per-atom virials (6 per atom, xx yy zz xy xz yz) by id, FP64 total in sum6 */
 int mdx_get_virials(mdx_state *st, double *per_atom, double sum6[6]);
 /* single hooks, for stage-level parity (src/Fixes/FixRigid.cu:1234-1279, 1916-1984) */

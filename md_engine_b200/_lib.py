@@ -77,6 +77,7 @@ SIGNATURES = [
     ("mdx_kinetic", c_int, [c_void_p, P(c_dbl), P(c_dbl)]),
     ("mdx_kinetic_noalloc", c_int, [c_void_p, P(c_dbl)]),
     ("mdx_get_virials", c_int, [c_void_p, P(c_dbl), P(c_dbl)]),
+    ("mdx_pressure", c_int, [c_void_p, P(c_dbl), P(c_dbl)]),
     ("mdx_rigid_settle_positions", c_int, [c_void_p, c_void_p]),
     ("mdx_rigid_save_prev", c_int, [c_void_p, c_void_p]),
     ("mdx_rigid_settle_velocities", c_int, [c_void_p, c_void_p]),

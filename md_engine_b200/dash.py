@@ -240,6 +240,14 @@ class State:
         check(lib().mdx_kinetic(self._h, ctypes.byref(s), ctypes.byref(n)))
         return s.value, n.value
 
+    def pressure(self):
+        """DataComputerPressure's scalar pressure and the total virial (6) from
+        a virial-mode force evaluation at the current positions (forces kept)"""
+        p = c_dbl()
+        v = (ctypes.c_double * 6)()
+        check(lib().mdx_pressure(self._h, ctypes.byref(p), v))
+        return p.value, np.array(list(v))
+
     def virials(self):
         n = self.nAtoms
         per = np.zeros((n, 6))

@@ -125,3 +125,29 @@ def test_water_e3b_total_virial_vs_oracle(oracle):
     _, v_no = st.virials()
     assert np.abs(v_no - (v_pair + v_rec)).max() < 2e-4 * scale
     assert np.abs((v_all - v_no) - v_e3b).max() < 1e-3 * np.abs(v_e3b).max(), (v_all - v_no, v_e3b)
+
+
+def test_pressure_vs_oracle_and_forces_kept(oracle):
+    """mdx_pressure (DataComputerPressure.cu:76-92): (sum m v^2 + virial
+    trace) / (3V) * nktv_to_press against the oracle's virials (pair, P3M,
+    E3B), and the integrator's forces are the same before and after"""
+    sysd = water_small(seed=12)
+    rcut, pad, alpha, grid = 6.5, 1.0, 0.35, 32
+    st, _ = systems.build_water_state(sysd, rcut=rcut, skin=pad, grid=grid, e3b=True, alpha=alpha,
+                                      thermostat=False)
+    st.prepare()
+    _, _, f0 = st.getAtoms()
+    p, v6 = st.pressure()
+    x, v, f1 = st.getAtoms()
+    assert np.array_equal(f0, f1)
+    excl = oracle.exclusions_from_bonds(len(sysd.pos), water_bonds(sysd.molecules))
+    ref, _ = _oracle_pair(oracle, st, sysd, oracle_water_params(oracle, rcut), rcut, pad, qrc=rcut, alpha=alpha,
+                          qqr=oracle.REAL_UNITS["qqr_to_eng"], excl=excl)
+    vir = ref["virial"].sum(0)
+    oracle.p3m_forces(x, sysd.q, sysd.lo, sysd.L, (grid,) * 3, alpha, virial=vir)
+    oracle.e3b_forces(sysd.molecules, x, sysd.L, oracle.e3b_params("E3B3"), virial=vir)
+    mv2 = float(np.sum(sysd.mass[:, None] * np.asarray(v) ** 2))
+    V = float(np.prod(sysd.L))
+    p_ref = (mv2 * systems.MVV_TO_ENG_REAL + vir[:3].sum()) / (3.0 * V) * 68568.415
+    scale = (mv2 * systems.MVV_TO_ENG_REAL + np.abs(vir[:3]).sum()) / (3.0 * V) * 68568.415
+    assert abs(p - p_ref) < 5e-4 * scale, (p, p_ref)
