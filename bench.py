@@ -47,6 +47,10 @@ def parse():
     return ap.parse_args()
 
 
+# nominal FP32 rate of a B200 at its maximum SM clock (no measured figure)
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -451,8 +455,19 @@ def main():
     e2e = world * e2e_calls * P / t_e2e
     # roofline of the dominant kernel (pair forces): algorithmic bytes per
     # launch = 16N (x) + 4N (q) + 16N (f) + 4 N nbar (directed list entries)
-    counts, _, _ = st.getNeighborList()
+    counts, nbr, _ = st.getNeighborList()
     nbar = float(np.mean(counts))
+    # FP32 view of the same kernel: 75 flops per directed pair within the
+    # pair cutoff (every listed pair with r < rc, zero pairs included, the
+    # counting convention of the water pair figure of 0.50 GFLOP per launch)
+    xa, _, _ = st.getAtoms()
+    rc = 2.5 if args.workload == "lj" else 9.0
+    Lb = np.asarray(sysd.L, np.float64)
+    ii = np.repeat(np.arange(len(counts)), counts)
+    jj = nbr[np.arange(nbr.shape[1])[None, :] < counts[:, None]]
+    dd = xa[jj] - xa[ii]
+    dd -= Lb * np.rint(dd / Lb)
+    pairs_rc = int(np.count_nonzero(np.einsum("ij,ij->i", dd, dd) < rc * rc))
     charged = args.workload != "lj"
     alg_bytes = n * (16 + (4 if charged else 0) + 16) + 4.0 * n * nbar
     pair_ms = st.timeStage("pair", iters=20, flushBytes=L2_FLUSH_BYTES)
@@ -481,7 +496,12 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": profile_traffic(args.workload + "_pair"),
                          "kernel": "k_pair (LJ + Ewald real space)", "kernel_ms": pair_ms,
-                         "alg_bytes_per_launch": alg_bytes, "nbar": nbar, "peak_source": peak_kind},
+                         "alg_bytes_per_launch": alg_bytes, "nbar": nbar, "peak_source": peak_kind,
+                         "fp32": None if not charged else {"achieved": 75.0 * pairs_rc / (pair_ms * 1e-3) / 1e12,
+                                  "peak": FP32_PEAK_TFLOPS, "unit": "TFLOP/s",
+                                  "frac": 75.0 * pairs_rc / (pair_ms * 1e-3) / 1e12 / FP32_PEAK_TFLOPS,
+                                  "pairs_within_rc": pairs_rc, "flops_per_pair": 75,
+                                  "peak_source": "nominal: 148 SMs x 128 FP32 lanes x 2 x 1.965 GHz"}},
             "stage_us": stages,
             "clocks": clk.summary(),
         }
