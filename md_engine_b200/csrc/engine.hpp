@@ -16,10 +16,11 @@
 namespace mdx {
 
 extern uint64_t g_launches;  // kernels launched by this library
-// threads per block of the fused per-molecule step kernels: one warp, so a
-// few thousand molecules spread over as many SMs as possible (each thread's
-// FP64 SETTLE is a long dependent chain)
-constexpr int kMolBlock = 32;
+// threads per block of the fused per-molecule step kernels: two warps, so a
+// few thousand molecules spread over many SMs (each thread's FP64 SETTLE is a
+// long dependent chain) with half as many block partials for the kinetic
+// sum's last-block tail as one-warp blocks (measured +0.6 % per water step)
+constexpr int kMolBlock = 64;
 // lanes per molecule in the E3B list and kernels (the molecule list is laid
 // out for teams of this size)
 constexpr int kE3BTeam = 16;
