@@ -601,7 +601,7 @@ static dim3 e3b_blocks(int nmol, unsigned nrep = 1) {
 }
 
 // part of a list rebuild, after the sort: the O-O distances are taken on the
-// sorted copy of this build's positions (xs_alt), which the step's first half
+// sorted copy of the positions of this list build (xs_alt), which the step's first half
 // running beside it on another stream does not move
 int e3b_build_list(State &s, FixE3B &f, bool conditional, cudaStream_t st) {
     const int nmol = (int)f.mol_ids.size();
@@ -637,7 +637,7 @@ int e3b_forces_to(State &s, FixE3B &f, float4 *out, bool side, cudaStream_t stre
 
 // exact E3B forces stored into out[O], out[H1], out[H2]; twobody = 0 leaves
 // out the O-O two-body term (the three-body forces alone: the surrogate's
-// training target and judge)
+// training target and the measure of its error)
 int e3b_exact_to(State &s, FixE3B &f, float4 *out, int twobody, cudaStream_t stream) {
     const int nmol = (int)f.mol_ids.size();
     if (nmol == 0) return 0;

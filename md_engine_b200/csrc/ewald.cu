@@ -696,7 +696,7 @@ int FixChargeEwald::setParameters(int nx, int ny, int nz, double rcut, int ord) 
         return MDX_ERR_ARG;
     }
     if (ord != 5) {
-        set_error(MDX_ERR_UNSUPPORTED, "P3M interpolation order %d: this build implements order 5", ord);
+        set_error(MDX_ERR_UNSUPPORTED, "P3M interpolation order %d: this library implements order 5", ord);
         return MDX_ERR_UNSUPPORTED;
     }
     sz = make_int3(nx, ny, nz);

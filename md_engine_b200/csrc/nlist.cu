@@ -216,7 +216,7 @@ __global__ void k_gather(const GridArgs a0, const GridArgs *__restrict__ tab) {
 }
 
 // the sorted streams back into the primary buffers (the captured graph keeps
-// the same pointers), and the positions of this build for the skin check
+// the same pointers), and the positions of this list build for the skin check
 __global__ void k_copyback(const GridArgs a0, const GridArgs *__restrict__ tab) {
     MDX_GRID_ARGS;
     if (!A.st->rebuild) return;

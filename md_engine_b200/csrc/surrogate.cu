@@ -1,6 +1,6 @@
 // Learned surrogate of the E3B three-body forces (no reference counterpart;
 // the exact term is ThreeBodyE3B.h:255-549 / EvaluatorE3B.h:145-345, which
-// stays the fallback and the judge of the surrogate's force error).
+// stays the fallback and the measure of the surrogate's force error).
 //
 // Model.  For molecule m a right-handed frame (e1 along the H-O-H bisector,
 // e2 toward H1, e3 = e1 x e2) and 128 rotation-invariant features: four

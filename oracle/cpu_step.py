@@ -1,4 +1,4 @@
-"""Whole-timestep CPU oracle -- TEST / BASELINE INFRASTRUCTURE ONLY.
+"""Whole-timestep CPU oracle -- TEST AND CPU-BASELINE INFRASTRUCTURE ONLY.
 
 Composes the oracle's FP64 restatements in the reference's hook order
 (IntegratorVerlet.cu:694-754): Nose-Hoover stepInit -> save_prev -> nve_v/x
