@@ -86,23 +86,29 @@ def barrier(dist, device=None):
     dist.all_reduce(t)
 
 
+def workload_cfg(name, sysd):
+    """the config object of a single-system workload (both arms print it)"""
+    if name == "lj":
+        return {"workload": "LJ fluid 32,000 atoms FCC rho*=0.8442 T*=1.2, rc 2.5 skin 0.3, dt 0.005, NH",
+                "atoms": len(sysd.pos)}
+    e3b = name == "water_e3b"
+    return {"workload": ("TIP4P/2005" + ("+E3B3" if e3b else "") +
+                         " 4,096 molecules (16,384 sites), LJ+Coulomb 9 A, skin 1 A, P3M 64^3 order 5, "
+                         "SETTLE, dt 2 fs, Nose-Hoover 298 K"),
+            "molecules": int(len(sysd.molecules)), "sites": int(len(sysd.pos))}
+
+
 def workload(name, seed=20261203):
     from md_engine_b200 import systems
     if name == "lj":
         sysd = systems.lj_fcc(ncell=20, seed=seed)
         st, _ = systems.build_lj_state(sysd, rcut=2.5, skin=0.3, dt=0.005, interval=10, T=1.2, tau=0.5)
-        cfg = {"workload": "LJ fluid 32,000 atoms FCC rho*=0.8442 T*=1.2, rc 2.5 skin 0.3, dt 0.005, NH",
-               "atoms": len(sysd.pos)}
-        return sysd, st, cfg, 0.005
+        return sysd, st, workload_cfg(name, sysd), 0.005
     e3b = name == "water_e3b"
     sysd = systems.water_tip4p2005(nside=16, seed=seed)
     st, _ = systems.build_water_state(sysd, rcut=9.0, skin=1.0, dt=2.0, interval=10, grid=64, e3b=e3b,
                                       T=298.0, tau=100.0)
-    cfg = {"workload": ("TIP4P/2005" + ("+E3B3" if e3b else "") +
-                        " 4,096 molecules (16,384 sites), LJ+Coulomb 9 A, skin 1 A, P3M 64^3 order 5, "
-                        "SETTLE, dt 2 fs, Nose-Hoover 298 K"),
-           "molecules": int(len(sysd.molecules)), "sites": int(len(sysd.pos))}
-    return sysd, st, cfg, 2.0
+    return sysd, st, workload_cfg(name, sysd), 2.0
 
 
 def nve_drift(name, x, v, seed):
@@ -234,7 +240,7 @@ def run_reference_arm(args, rank, world):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "timesteps/s", "n_gpus": world,
             "steps": steps, "warmup": warm, "ms_per_step": 1000.0 / v, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-            "config": {"workload": res["workload"]},
+            "config": dict(workload_cfg(args.workload, sysd), reference_sample=res["workload"]),
             "ns_per_day": v * dt * 86400 / 1e6 if args.workload != "lj" else None,
             "cpu_baseline": {"value": v, "unit": "timesteps/s", "cores": res["cores"], "kind": "port",
                              "sample": res["sample"]},
