@@ -297,7 +297,7 @@ def run_batched(args, rank, world, local):
     states = [s for s, _ in reps]
     mols = sum(m for _, m in reps)
     b = BatchReplicas(states)
-    team, tune_ms = b.autotune(steps=20, teams=(4, 8, 16))
+    team, tune_ms = b.autotune(steps=20, teams=(4, 8, 16, 32))
     b.run(max(args.warmup, 3))
     K = args.steps
     barrier(dist, dev)

@@ -555,7 +555,7 @@ class BatchReplicas:
         check(lib().mdx_batch_run_timed(self._h, int(numTurns), int(chunk), int(flushBytes), ctypes.byref(out)))
         return out.value
 
-    def autotune(self, steps=20, teams=(4, 8, 16)):
+    def autotune(self, steps=20, teams=(4, 8, 16, 32)):
         """(best team size, device ms per step); leaves the batch prepared with it"""
         arr = (c_int * len(teams))(*teams)
         best = c_int()
