@@ -18,6 +18,11 @@ namespace mdx {
 
 namespace {
 
+// threads per block of the pair kernel: small blocks retire and refill SM
+// slots finely, beside the P3M chain on another stream (measured against 256:
+// water step +1.8 %, LJ +2.4 %)
+constexpr int kPairBlock = 64;
+
 template <int T>
 __device__ __forceinline__ float team_sum(float v) {
 #pragma unroll
@@ -179,7 +184,7 @@ __device__ __forceinline__ void pair_row(const PairArgs &A, const float *sp, int
 // term, and one whose atoms are all uncharged (water O) without the Ewald
 // term: both contribute exactly zero there, and the choice is warp-uniform.
 template <int T, int LJ, bool EW, bool VIR, bool ENERGY>
-__global__ void __launch_bounds__(256) k_pair(const PairArgs a0, const PairArgs *__restrict__ tab, int accumulate) {
+__global__ void __launch_bounds__(kPairBlock) k_pair(const PairArgs a0, const PairArgs *__restrict__ tab, int accumulate) {
     pdl_wait();
     const PairArgs A = tab ? tab[blockIdx.y] : a0;
     extern __shared__ float sp[];
@@ -260,16 +265,16 @@ void launch_t(const PairArgs &A, const PairArgs *tab, int nrep, bool vir, bool e
               cudaStream_t st) {
     const int G = 32 / T;
     const int warps = (A.n + G - 1) / G;
-    const dim3 blocks((warps * 32 + 255) / 256, nrep);
+    const dim3 blocks((warps * 32 + kPairBlock - 1) / kPairBlock, nrep);
     const size_t smem = LJ ? 3 * A.ntypes * A.ntypes * sizeof(float) : 0;
     if (energy) {
-        k_pair<T, LJ, EW, false, true><<<blocks, 256, smem, st>>>(A, tab, 0);
+        k_pair<T, LJ, EW, false, true><<<blocks, kPairBlock, smem, st>>>(A, tab, 0);
         MDX_LAUNCHED();
     } else if (vir) {
-        k_pair<T, LJ, EW, true, false><<<blocks, 256, smem, st>>>(A, tab, accumulate ? 1 : 0);
+        k_pair<T, LJ, EW, true, false><<<blocks, kPairBlock, smem, st>>>(A, tab, accumulate ? 1 : 0);
         MDX_LAUNCHED();
     } else {
-        launch_pdl(k_pair<T, LJ, EW, false, false>, blocks, dim3(256), smem, st, A, tab, accumulate ? 1 : 0);
+        launch_pdl(k_pair<T, LJ, EW, false, false>, blocks, dim3(kPairBlock), smem, st, A, tab, accumulate ? 1 : 0);
     }
 }
 
