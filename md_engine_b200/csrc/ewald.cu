@@ -841,9 +841,11 @@ template <int R>
 int own_solve(State &s, FixChargeEwald &f, cudaStream_t st) {
     constexpr int N = 32 * R, NH = N / 2 + 1;
     const FFTArgs A = fft_args(s, f);
-    MDX_CUDA_TRY(launch_pdl_prio(true, k_fft_zy<R>, dim3(N), dim3(1024), (size_t)N * NH * sizeof(float2), st, A));
+    // 512-thread plane blocks (measured +0.8 % per water step against 1024
+    // beside the pair kernel; 256 was slower)
+    MDX_CUDA_TRY(launch_pdl_prio(true, k_fft_zy<R>, dim3(N), dim3(512), (size_t)N * NH * sizeof(float2), st, A));
     MDX_CUDA_TRY(launch_pdl_prio(true, k_fft_xe<R>, dim3((N * NH + 7) / 8), dim3(256), 0, st, A));
-    MDX_CUDA_TRY(launch_pdl_prio(true, k_ifft_yz<R>, dim3(N, 3), dim3(1024), (size_t)N * NH * sizeof(float2), st, A));
+    MDX_CUDA_TRY(launch_pdl_prio(true, k_ifft_yz<R>, dim3(N, 3), dim3(512), (size_t)N * NH * sizeof(float2), st, A));
     return 0;
 }
 
@@ -949,7 +951,9 @@ int FixChargeEwald::spread_mol(cudaStream_t st, const FixRigid &r) {
     MDX_CUDA_TRY(cudaMemsetAsync(rho.p, 0, ng * sizeof(float), st));
     const P3MArgs A = mol_args(s, *this, r);
     const int warps = (A.nmol + 1) / 2;
-    MDX_CUDA_TRY(launch_pdl_prio(true, k_spread_mol, dim3((warps + 7) / 8), dim3(256), 0, st, A));
+    // two-warp blocks: they slot in beside the pair kernel's (measured +1 % per
+    // water step against 256-thread blocks)
+    MDX_CUDA_TRY(launch_pdl_prio(true, k_spread_mol, dim3((warps + 1) / 2), dim3(64), 0, st, A));
     return 0;
 }
 
@@ -958,7 +962,7 @@ int FixChargeEwald::gather_mol_to(float4 *out, cudaStream_t st, const FixRigid &
     P3MArgs A = mol_args(s, *this, r);
     A.fs = out;
     const int warps = (A.nmol + 1) / 2;
-    MDX_CUDA_TRY(launch_pdl_prio(true, k_gather_mol, dim3((warps + 7) / 8), dim3(256), 0, st, A,
+    MDX_CUDA_TRY(launch_pdl_prio(true, k_gather_mol, dim3((warps + 1) / 2), dim3(64), 0, st, A,
                                  (const float4 *)e4.p));
     return 0;
 }
