@@ -478,7 +478,7 @@ __global__ void __launch_bounds__(256) k_fft_xe(const FFTArgs A) {
     pdl_wait();
     __shared__ float2 sline[8][N];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int line_id = blockIdx.x * 8 + w;
+    const int line_id = blockIdx.x * (blockDim.x >> 5) + w;  // at most 8 warps per block (sline)
     if (line_id >= N * NH) return;  // warp-uniform; no block barrier below
     const LaneTw T = lane_twiddles<R>(lane, A.tw);
     const int ky = line_id / NH, kz = line_id % NH;
