@@ -322,6 +322,9 @@ __global__ void k_first_mol(const MolArgs a0, const MolArgs *__restrict__ tab) {
         fs[ix.w] = make_float4(0.f, 0.f, 0.f, fm.w);
         xs[ix.w] = msite(rc, box, x, xs[ix.w].w);
     }
+    // late trigger: the dependent's blocks become resident during this
+    // grid's tail; their griddepcontrol.wait still waits for all of it
+    pdl_trigger();
 }
 
 // ---- second half --------------------------------------------------------

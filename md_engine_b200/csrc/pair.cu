@@ -226,6 +226,9 @@ __global__ void __launch_bounds__(kPairBlock) k_pair(const PairArgs a0, const Pa
     } else if (valid) {
         pair_row<T, LJ, EW, VIR, ENERGY>(A, sp, nt2, i, ti, qi, xi, row, cnt, t, fx, fy, fz, en, v);
     }
+    // late trigger (row loop done): the next kernel's blocks take SM slots
+    // as this grid drains; its griddepcontrol.wait still waits for the stores
+    pdl_trigger();
     // invalid lanes carry zeros; whole warp takes part in the shuffles
     if (ENERGY) {
         en = team_sum<T>(en);
