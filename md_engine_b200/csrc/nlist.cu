@@ -536,7 +536,11 @@ __global__ void __launch_bounds__(kBuildCellsPerBlock * 32, 6) k_build_cells(con
                         const int bi = __popc(am[k] & lt);
                         const int pos = act[k] ? ci[k] + bi : cap - 1 - cn[k] - (before - bi);
                         uint32_t entry = (uint32_t)p;
-                        if (use_excl) entry |= excl_depth(A, hid[k], hfar[k], hwin[k], oid) << 30;
+                        // a depth needs an id within 32 of the home's (the
+                        // bit window) or a home with far exclusions; most
+                        // chunks have neither
+                        if (use_excl && (hfar[k] || __any_sync(0xffffffffu, hit[k] && oid - hid[k] + 32u < 64u)))
+                            entry |= excl_depth(A, hid[k], hfar[k], hwin[k], oid) << 30;
                         const int i = g0 + k;
                         if (hit[k] && ci[k] + cn[k] + before < cap)
                             nlist[(size_t)(i / GP) * cap * GP + (i % GP) * TP + (pos / TP) * 32 + pos % TP] = entry;
