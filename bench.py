@@ -4,7 +4,9 @@ Workload (default): 4,096 molecules (16,384 sites incl. M), cubic lattice at
 0.997 g/cm^3 with seeded random orientations, LJ + Coulomb 9 A cutoff, skin
 1 A, Ewald real space + P3M 64^3 order 5, SETTLE, dt 2 fs, Nose-Hoover NVT at
 298 K, FP32 with FP64 reductions and FP64 SETTLE, neighbour check every 10
-steps.  A "step" is one MD timestep of that system.
+steps.  The seeded start is relaxed into the liquid (4,000 untimed steps
+with a tight thermostat) before the warm-up.  A "step" is one MD timestep of
+that system.
 
   python bench.py [--gpus N] [--steps K] [--warmup W]
                   [--workload water|water_e3b|lj|batched|surrogate]
@@ -98,17 +100,56 @@ def workload_cfg(name, sysd):
             "molecules": int(len(sysd.molecules)), "sites": int(len(sysd.pos))}
 
 
+EQ_STEPS = 4000
+
+
+def _water_state(sysd, e3b, tau):
+    from md_engine_b200 import systems
+    st, _ = systems.build_water_state(sysd, rcut=9.0, skin=1.0, dt=2.0, interval=10, grid=64, e3b=e3b,
+                                      T=298.0, tau=tau)
+    return st
+
+
+def _lj_state(sysd, tau):
+    from md_engine_b200 import systems
+    st, _ = systems.build_lj_state(sysd, rcut=2.5, skin=0.3, dt=0.005, interval=10, T=1.2, tau=tau)
+    return st
+
+
+def equilibrate(name, sysd, steps=EQ_STEPS):
+    """The seeded lattice start relaxed into the workload's liquid before
+    anything is timed: `steps` MD steps of the same system and step with a
+    tight Nose-Hoover coupling (tau 25 fs for water, 0.1 for the LJ fluid) at
+    the workload's temperature; returns the system with the final positions
+    and velocities.  The reference benchmarks equilibrated liquid water at
+    298 K; the lattice start alone turns its potential energy into heat and
+    the timed steps would run a hot, near-lattice system instead."""
+    import dataclasses
+    from md_engine_b200 import IntegratorVerlet
+    st = _lj_state(sysd, 0.1) if name == "lj" else _water_state(sysd, name == "water_e3b", 25.0)
+    IntegratorVerlet(st).run(steps)
+    x, v, _ = st.getAtoms()
+    return dataclasses.replace(sysd, pos=np.asarray(x, np.float64), vel=np.asarray(v, np.float64))
+
+
 def workload(name, seed=20261203):
     from md_engine_b200 import systems
     if name == "lj":
-        sysd = systems.lj_fcc(ncell=20, seed=seed)
-        st, _ = systems.build_lj_state(sysd, rcut=2.5, skin=0.3, dt=0.005, interval=10, T=1.2, tau=0.5)
-        return sysd, st, workload_cfg(name, sysd), 0.005
-    e3b = name == "water_e3b"
-    sysd = systems.water_tip4p2005(nside=16, seed=seed)
-    st, _ = systems.build_water_state(sysd, rcut=9.0, skin=1.0, dt=2.0, interval=10, grid=64, e3b=e3b,
-                                      T=298.0, tau=100.0)
-    return sysd, st, workload_cfg(name, sysd), 2.0
+        sysd = equilibrate(name, systems.lj_fcc(ncell=20, seed=seed))
+        return sysd, _lj_state(sysd, 0.5), workload_cfg(name, sysd), 0.005
+    sysd = equilibrate(name, systems.water_tip4p2005(nside=16, seed=seed))
+    return sysd, _water_state(sysd, name == "water_e3b", 100.0), workload_cfg(name, sysd), 2.0
+
+
+def timed_temperature(name, sysd, st):
+    """instantaneous temperature from the FP64 kinetic sum (rigid water:
+    6 degrees of freedom per molecule, 3 of them removed for the momentum)"""
+    from md_engine_b200 import systems
+    mv2, _ = st.kinetic()
+    if name == "lj":
+        return {"value": mv2 / (3 * len(sysd.pos) - 3), "unit": "epsilon/k_B"}
+    ndf = 6 * len(sysd.molecules) - 3
+    return {"value": mv2 * systems.MVV_TO_ENG_REAL / (ndf * systems.BOLTZ_REAL), "unit": "K"}
 
 
 def nve_drift(name, x, v, seed):
@@ -446,6 +487,7 @@ def main():
     barrier(dist, dev)
     ms_max = reduce_max(dist, ms, dev)
     value = world * K / (ms_max * 1e-3)
+    t_end = timed_temperature(args.workload, sysd, st)
     # end to end through the C ABI with host buffers: H2D positions+velocities,
     # P steps, D2H positions+velocities+forces, per call
     x, v, _ = st.getAtoms()
@@ -492,10 +534,13 @@ def main():
             "metric": METRIC, "value": value, "unit": "timesteps/s", "n_gpus": world, "steps": K,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_max / K, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 reductions, f64 SETTLE)",
-            "data": "synthetic (seeded lattice + random orientations + Maxwell-Boltzmann)",
+            "data": "synthetic (seeded lattice + random orientations + Maxwell-Boltzmann, "
+                    f"relaxed {EQ_STEPS} untimed steps at the target temperature)",
             "config": dict(cfg, l2="flushed between timed 10-step chunks (256 MiB write)",
+                           start=f"equilibrated: {EQ_STEPS} steps, tight Nose-Hoover, before warm-up",
                            parallelism="replicas only" if world > 1 else "single system"),
             "ns_per_day": ns_day,
+            "temperature_end_of_timed_region": t_end,
             "e2e": {"value": e2e, "unit": "timesteps/s",
                     "h2d_bytes_per_step": int(2 * 16 * n / P), "d2h_bytes_per_step": int(3 * 16 * n / P)},
             "gpu_launches": int(k1 - k0),
