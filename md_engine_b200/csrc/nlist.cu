@@ -256,6 +256,8 @@ constexpr int kStencilMax = 4;                    // largest m (cells >= cut/m)
 constexpr int kBuildSegMax = 2 * (2 * kStencilMax + 1) * (2 * kStencilMax + 1);  // two z segments per row
 constexpr int kCandWin = 1536;                    // expanded candidates per warp and window
 constexpr int kCandIdxBits = 27;                  // sorted index bits of an expanded candidate
+constexpr int kCandPad = 64;                      // harmless entries after a window (branch-free prefetch)
+constexpr uint32_t kNoShift = 13u;                // image code (1,1,1): no shift
 
 struct BuildArgs {
     const float4 *xs2, *vs2, *fs2;
@@ -299,7 +301,10 @@ __device__ __forceinline__ uint32_t excl_depth(const BuildArgs &A, uint32_t myid
     return depth;
 }
 
-template <int TP, int HG, bool COUNT>
+// SPLIT: interacting pairs to the front of a row, provably zero ones to the
+// back (ljmask, part_q); EXCL: exclusion depths from the id window.  Both are
+// compile-time so that the candidate loop carries no tests for them.
+template <int TP, int HG, bool COUNT, bool SPLIT, bool EXCL>
 __global__ void __launch_bounds__(kBuildCellsPerBlock * 32, 6) k_build_cells(const BuildArgs a0,
                                                                             const BuildArgs *__restrict__ tab) {
     pdl_wait();
@@ -309,7 +314,7 @@ __global__ void __launch_bounds__(kBuildCellsPerBlock * 32, 6) k_build_cells(con
     __shared__ int sh_seg_off_all[kBuildCellsPerBlock][kBuildSegMax + 1];
     __shared__ int sh_seg_beg_all[kBuildCellsPerBlock][kBuildSegMax];
     __shared__ uint32_t sh_seg_code_all[kBuildCellsPerBlock][kBuildSegMax];
-    __shared__ uint32_t sh_cand_all[kBuildCellsPerBlock][kCandWin];
+    __shared__ uint32_t sh_cand_all[kBuildCellsPerBlock][kCandWin + kCandPad];
     __shared__ float4 sh_shift[27];  // image shift by code (ix+1) + 3 (iy+1) + 9 (iz+1)
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -331,10 +336,7 @@ __global__ void __launch_bounds__(kBuildCellsPerBlock * 32, 6) k_build_cells(con
     const int cz = c % g.ns.z, cy = (c / g.ns.z) % g.ns.y, cx = c / (g.ns.z * g.ns.y);
     const int m = A.m, side = 2 * m + 1;
     const float cutsq = A.cutsq;
-    const int cap = A.cap;
-    const bool use_excl = A.use_excl != 0;
-    const bool split = A.ljmask != nullptr;
-    const bool split_q = split && A.part_q;
+    const uint32_t cap = (uint32_t)A.cap;
     uint32_t *const nlist = A.nlist;
     const float dsx = 1.0f / g.inv_ds.x, dsy = 1.0f / g.inv_ds.y, dsz = 1.0f / g.inv_ds.z;
     const uint32_t lt = (1u << lane) - 1u;
@@ -453,6 +455,9 @@ __global__ void __launch_bounds__(kBuildCellsPerBlock * 32, 6) k_build_cells(con
             const uint32_t beg = (uint32_t)(sh_seg_beg[sg] - off), code = sh_seg_code[sg] << kCandIdxBits;
             for (int t = lo + lane; t < hi; t += 32) sh_cand[t - w0] = (beg + (uint32_t)t) | code;
         }
+        // the prefetch reads up to kCandPad entries past the window: the
+        // cell's first site, unshifted (in bounds, never counted)
+        for (int t = wn + lane; t < wn + kCandPad; t += 32) sh_cand[t] = (uint32_t)cs | (kNoShift << kCandIdxBits);
         __syncwarp();
     };
     const bool single = total <= kCandWin;
@@ -460,51 +465,51 @@ __global__ void __launch_bounds__(kBuildCellsPerBlock * 32, 6) k_build_cells(con
     // home atoms HG at a time, in registers (warp-uniform values)
     for (int g0 = cs; g0 < ce; g0 += HG) {
         float hx[HG], hy[HG], hz[HG], hq[HG];
-        uint32_t hmask[HG], hid[HG];
+        uint32_t hmask[HG], hid[HG], ci[HG], cn[HG];
         ulonglong2 hwin[HG];
-        bool hfar[HG], hval[HG];
-        int ci[HG], cn[HG];
+        bool hfar[HG];
+        uint32_t *hrow[HG];
 #pragma unroll
         for (int k = 0; k < HG; k++) {
             const int i = g0 + k;
-            hval[k] = i < ce;
-            const int ii = hval[k] ? i : cs;
+            const bool v = i < ce;
+            const int ii = v ? i : cs;
             const float4 p4 = A.xs2[ii];
-            hx[k] = p4.x;
-            hy[k] = p4.y;
-            hz[k] = p4.z;
-            hq[k] = split_q ? A.qs2[ii] : 0.f;
-            hmask[k] = split ? A.ljmask[type_of(p4)] : 0xffffffffu;
-            hid[k] = use_excl ? A.ids2[ii] : 0u;
-            hfar[k] = use_excl ? A.excl_far[hid[k]] != 0 : false;
-            hwin[k] = use_excl ? A.excl_win[hid[k]] : make_ulonglong2(0ull, 0ull);
-            ci[k] = 0;
-            cn[k] = 0;
+            // an absent home slot sits far outside the box: r^2 overflows to
+            // infinity and it never hits
+            hx[k] = v ? p4.x : 3.0e37f;
+            hy[k] = v ? p4.y : 3.0e37f;
+            hz[k] = v ? p4.z : 3.0e37f;
+            hq[k] = SPLIT && A.part_q ? A.qs2[ii] : 0.f;
+            hmask[k] = SPLIT ? A.ljmask[type_of(p4)] : 0xffffffffu;
+            hid[k] = EXCL ? A.ids2[ii] : 0u;
+            hfar[k] = EXCL ? A.excl_far[hid[k]] != 0 : false;
+            hwin[k] = EXCL ? A.excl_win[hid[k]] : make_ulonglong2(0ull, 0ull);
+            hrow[k] = nlist + (size_t)(ii / GP) * cap * GP + (ii % GP) * TP;
+            ci[k] = 0u;
+            cn[k] = 0u;
         }
         for (int w0 = 0; w0 < total; w0 += kCandWin) {
             const int wn = min(kCandWin, total - w0);
             if (!single) expand(w0, wn);
             // candidate: sorted index, raw position, image shift, charge, id;
-            // the next chunk's loads are issued before the current one is tested
-            int pn = -1;
-            float4 pjn = make_float4(0.f, 0.f, 0.f, 0.f), shn = pjn;
+            // the next chunk's loads are issued before the current one is
+            // tested (indices up to wn + 63 < wn + kCandPad: no bounds test)
+            uint32_t pn = 0u, idn = 0u;
+            float4 pjn, shn;
             float qn = 0.f;
-            uint32_t idn = 0u;
             auto fetch = [&](int k) {
-                pn = -1;
-                if (k < wn) {
-                    const uint32_t e = sh_cand[k];
-                    pn = (int)(e & ((1u << kCandIdxBits) - 1u));
-                    shn = sh_shift[e >> kCandIdxBits];
-                    pjn = A.xs2[pn];
-                    if (split_q) qn = A.qs2[pn];
-                    if (use_excl) idn = A.ids2[pn];
-                }
+                const uint32_t e = sh_cand[k];
+                pn = e & ((1u << kCandIdxBits) - 1u);
+                shn = sh_shift[e >> kCandIdxBits];
+                pjn = A.xs2[pn];
+                if (SPLIT) qn = A.qs2[pn];
+                if (EXCL) idn = A.ids2[pn];
             };
             fetch(lane);
             for (int c0 = 0; c0 < wn; c0 += 32) {
-                const int p = pn;
-                const bool cval = p >= 0;
+                const uint32_t p = pn;
+                const bool cval = c0 + lane < wn;
                 const float cxj = __fadd_rn(pjn.x, shn.x);
                 const float cyj = __fadd_rn(pjn.y, shn.y);
                 const float czj = __fadd_rn(pjn.z, shn.z);
@@ -520,32 +525,32 @@ __global__ void __launch_bounds__(kBuildCellsPerBlock * 32, 6) k_build_cells(con
                     const float ddy = __fsub_rn(cyj, hy[k]);
                     const float ddz = __fsub_rn(czj, hz[k]);
                     const float r2 = __fmaf_rn(ddz, ddz, __fmaf_rn(ddy, ddy, __fmul_rn(ddx, ddx)));
-                    hit[k] = hval[k] && cval && r2 < cutsq && p != g0 + k;
-                    act[k] = true;
-                    if (split) {
-                        act[k] = ((hmask[k] >> tj) & 1u) != 0u;
-                        if (split_q) act[k] = act[k] || hq[k] * qj != 0.f;
-                    }
+                    hit[k] = cval && r2 < cutsq && p != (uint32_t)(g0 + k);
                     hm[k] = __ballot_sync(0xffffffffu, hit[k]);
-                    am[k] = split ? __ballot_sync(0xffffffffu, hit[k] && act[k]) : hm[k];
+                    act[k] = true;
+                    am[k] = hm[k];
+                    if (SPLIT && !COUNT) {
+                        act[k] = ((hmask[k] >> tj) & 1u) != 0u || hq[k] * qj != 0.f;
+                        am[k] = __ballot_sync(0xffffffffu, hit[k] && act[k]);
+                    }
                 }
 #pragma unroll
                 for (int k = 0; k < HG; k++) {
-                    if (!COUNT && hm[k] != 0u) {
-                        const int before = __popc(hm[k] & lt);
-                        const int bi = __popc(am[k] & lt);
-                        const int pos = act[k] ? ci[k] + bi : cap - 1 - cn[k] - (before - bi);
-                        uint32_t entry = (uint32_t)p;
-                        // a depth needs an id within 32 of the home's (the
-                        // bit window) or a home with far exclusions; most
-                        // chunks have neither
-                        if (use_excl && (hfar[k] || __any_sync(0xffffffffu, hit[k] && oid - hid[k] + 32u < 64u)))
-                            entry |= excl_depth(A, hid[k], hfar[k], hwin[k], oid) << 30;
-                        const int i = g0 + k;
-                        if (hit[k] && ci[k] + cn[k] + before < cap)
-                            nlist[(size_t)(i / GP) * cap * GP + (i % GP) * TP + (pos / TP) * 32 + pos % TP] = entry;
+                    if (COUNT) {
+                        ci[k] += __popc(hm[k]);
+                        continue;
                     }
-                    const int na = __popc(am[k]);
+                    const uint32_t before = __popc(hm[k] & lt);
+                    const uint32_t bi = __popc(am[k] & lt);
+                    const uint32_t pos = act[k] ? ci[k] + bi : cap - 1u - cn[k] - (before - bi);
+                    uint32_t entry = p;
+                    // a depth needs an id within 32 of the home's (the bit
+                    // window) or a home with far exclusions; most chunks have
+                    // neither
+                    if (EXCL && (hfar[k] || __any_sync(0xffffffffu, hit[k] && oid - hid[k] + 32u < 64u)))
+                        entry |= excl_depth(A, hid[k], hfar[k], hwin[k], oid) << 30;
+                    if (hit[k] && ci[k] + cn[k] + before < cap) hrow[k][(pos / TP) * 32u + pos % TP] = entry;
+                    const uint32_t na = __popc(am[k]);
                     ci[k] += na;
                     cn[k] += __popc(hm[k]) - na;
                 }
@@ -553,15 +558,15 @@ __global__ void __launch_bounds__(kBuildCellsPerBlock * 32, 6) k_build_cells(con
         }
 #pragma unroll
         for (int k = 0; k < HG; k++) {
-            if (lane == k && hval[k]) {
+            if (lane == k && g0 + k < ce) {
                 const int i = g0 + k;
-                const uint32_t cnt = (uint32_t)(ci[k] + cn[k]);
+                const uint32_t cnt = ci[k] + cn[k];
                 if (COUNT) {
                     atomicMax(&A.st->max_neighbors, cnt);
                 } else {
                     A.counts[i] = cnt;
-                    A.counts_int[i] = (uint32_t)ci[k];
-                    if (cnt > (uint32_t)cap) atomicOr(&A.st->bits, kStatusNlistOverflow);
+                    A.counts_int[i] = ci[k];
+                    if (cnt > cap) atomicOr(&A.st->bits, kStatusNlistOverflow);
                     atomicMax(&A.st->max_neighbors, cnt);
                 }
             }
@@ -659,9 +664,20 @@ BuildArgs build_args(State &s, const CellGrid &g, float cutsq) {
     return A;
 }
 
+template <int T, int HG, bool COUNT>
+auto build_kernel(bool split, bool excl) {
+    if constexpr (COUNT) {
+        return k_build_cells<T, HG, true, false, false>;
+    } else {
+        return split ? (excl ? k_build_cells<T, HG, false, true, true> : k_build_cells<T, HG, false, true, false>)
+                     : (excl ? k_build_cells<T, HG, false, false, true> : k_build_cells<T, HG, false, false, false>);
+    }
+}
+
 template <int T, bool COUNT>
 void launch_build_hg(int hg, dim3 grid, cudaStream_t st, const BuildArgs &A, const BuildArgs *tab) {
-    auto k = hg == 4 ? k_build_cells<T, 4, COUNT> : k_build_cells<T, 2, COUNT>;
+    const bool split = A.ljmask != nullptr, excl = A.use_excl != 0;
+    auto k = hg == 4 ? build_kernel<T, 4, COUNT>(split, excl) : build_kernel<T, 2, COUNT>(split, excl);
     if (tab) {
         k<<<grid, kBuildCellsPerBlock * 32, 0, st>>>(A, tab);
         MDX_LAUNCHED();
@@ -937,6 +953,14 @@ int batch_nlist_tables(Batch &b) {
         State &s = *b.reps[r];
         hg[r] = grid_args(s);
         hb[r] = build_args(s, make_grid(s), s.grid.cut * s.grid.cut);
+        // one list-build kernel serves the batch: its exclusion and
+        // front/back split forms are compile-time, so they must agree
+        if ((hb[r].use_excl != 0) != (hb[0].use_excl != 0) ||
+            (hb[r].ljmask != nullptr) != (hb[0].ljmask != nullptr)) {
+            set_error(MDX_ERR_UNSUPPORTED,
+                      "batched replicas must agree on exclusions and on the interacting-pair split (replica %d)", r);
+            return MDX_ERR_UNSUPPORTED;
+        }
     }
     if (int e = b.tab_grid.alloc(R * sizeof(GridArgs))) return e;
     if (int e = b.tab_build.alloc(R * sizeof(BuildArgs))) return e;
