@@ -540,6 +540,7 @@ __global__ void __launch_bounds__(kBuildCellsPerBlock * 32, 6) k_build_cells(con
                         ci[k] += __popc(hm[k]);
                         continue;
                     }
+                    if (hm[k] == 0u) continue;  // warp-uniform: no hit for this home in the chunk
                     const uint32_t before = __popc(hm[k] & lt);
                     const uint32_t bi = __popc(am[k] & lt);
                     const uint32_t pos = act[k] ? ci[k] + bi : cap - 1u - cn[k] - (before - bi);
