@@ -437,6 +437,14 @@ __global__ void __launch_bounds__(kBuildCellsPerBlock * 32, 6) k_build_cells(con
             sh_seg_off[slot + 1] = off + l0;
             sh_seg_code[slot + 1] = cxy + cz1;
         }
+        // the first window straight from the rows, every lane its own
+        // segments (later windows of a long sequence expand from the table)
+        {
+            const uint32_t w0c = (cxy + cz0) << kCandIdxBits, w1c = (cxy + cz1) << kCandIdxBits;
+            const int e0 = min(off + l0, kCandWin), e1 = min(off + l0 + l1, kCandWin);
+            for (int t = off; t < e0; t++) sh_cand[t] = (uint32_t)(b0 - off + t) | w0c;
+            for (int t = off + l0; t < e1; t++) sh_cand[t] = (uint32_t)(b1 - off - l0 + t) | w1c;
+        }
         seg_base += __shfl_sync(0xffffffffu, so, 31);
         cand_base += __shfl_sync(0xffffffffu, lo, 31);
     }
@@ -446,6 +454,11 @@ __global__ void __launch_bounds__(kBuildCellsPerBlock * 32, 6) k_build_cells(con
     const int nseg = seg_base;
     const int total = cand_base;
 
+    // the prefetch reads up to kCandPad entries past a window: the cell's
+    // first site, unshifted (in bounds, never counted)
+    auto pad = [&](int wn) {
+        for (int t = wn + lane; t < wn + kCandPad; t += 32) sh_cand[t] = (uint32_t)cs | (kNoShift << kCandIdxBits);
+    };
     // expand candidates [w0, w0 + wn) of the segment sequence into sh_cand
     auto expand = [&](int w0, int wn) {
         __syncwarp();
@@ -455,13 +468,14 @@ __global__ void __launch_bounds__(kBuildCellsPerBlock * 32, 6) k_build_cells(con
             const uint32_t beg = (uint32_t)(sh_seg_beg[sg] - off), code = sh_seg_code[sg] << kCandIdxBits;
             for (int t = lo + lane; t < hi; t += 32) sh_cand[t - w0] = (beg + (uint32_t)t) | code;
         }
-        // the prefetch reads up to kCandPad entries past the window: the
-        // cell's first site, unshifted (in bounds, never counted)
-        for (int t = wn + lane; t < wn + kCandPad; t += 32) sh_cand[t] = (uint32_t)cs | (kNoShift << kCandIdxBits);
+        pad(wn);
         __syncwarp();
     };
     const bool single = total <= kCandWin;
-    if (single) expand(0, total);
+    if (single) {
+        pad(total);
+        __syncwarp();
+    }
     // home atoms HG at a time, in registers (warp-uniform values)
     for (int g0 = cs; g0 < ce; g0 += HG) {
         float hx[HG], hy[HG], hz[HG], hq[HG];
@@ -507,6 +521,7 @@ __global__ void __launch_bounds__(kBuildCellsPerBlock * 32, 6) k_build_cells(con
                 if (EXCL) idn = A.ids2[pn];
             };
             fetch(lane);
+#pragma unroll 2
             for (int c0 = 0; c0 < wn; c0 += 32) {
                 const uint32_t p = pn;
                 const bool cval = c0 + lane < wn;
