@@ -305,15 +305,17 @@ __device__ __forceinline__ uint32_t excl_depth(const BuildArgs &A, uint32_t myid
 // back (ljmask, part_q); EXCL: exclusion depths from the id window.  Both are
 // compile-time so that the candidate loop carries no tests for them.
 template <int TP, int HG, bool COUNT, bool SPLIT, bool EXCL>
-__global__ void __launch_bounds__(kBuildCellsPerBlock * 32, 6) k_build_cells(const BuildArgs a0,
+__global__ void __launch_bounds__(kBuildCellsPerBlock * 32, 7) k_build_cells(const BuildArgs a0,
                                                                             const BuildArgs *__restrict__ tab) {
     pdl_wait();
     const BuildArgs A = tab ? tab[blockIdx.y] : a0;
     if (!COUNT && !A.st->rebuild) return;
     constexpr int GP = 32 / TP;
-    __shared__ int sh_seg_off_all[kBuildCellsPerBlock][kBuildSegMax + 1];
+    // segment table: offset in the sequence | image code << kCandIdxBits,
+    // and the first sorted index (two words per segment: seven blocks fit
+    // an SM beside the candidate windows)
+    __shared__ uint32_t sh_seg_offc_all[kBuildCellsPerBlock][kBuildSegMax + 1];
     __shared__ int sh_seg_beg_all[kBuildCellsPerBlock][kBuildSegMax];
-    __shared__ uint32_t sh_seg_code_all[kBuildCellsPerBlock][kBuildSegMax];
     __shared__ uint32_t sh_cand_all[kBuildCellsPerBlock][kCandWin + kCandPad];
     __shared__ float4 sh_shift[27];  // image shift by code (ix+1) + 3 (iy+1) + 9 (iz+1)
     const int lane = threadIdx.x & 31;
@@ -326,9 +328,8 @@ __global__ void __launch_bounds__(kBuildCellsPerBlock * 32, 6) k_build_cells(con
     __syncthreads();  // the only block-wide barrier: warps own cells from here on
     const int c = blockIdx.x * kBuildCellsPerBlock + wib;
     if (c >= A.ncell) return;
-    int *const sh_seg_off = sh_seg_off_all[wib];
+    uint32_t *const sh_seg_offc = sh_seg_offc_all[wib];
     int *const sh_seg_beg = sh_seg_beg_all[wib];
-    uint32_t *const sh_seg_code = sh_seg_code_all[wib];
     uint32_t *const sh_cand = sh_cand_all[wib];
     const CellGrid &g = A.g;
     const int cs = (int)A.cell_start[c], ce = (int)A.cell_start[c + 1];
@@ -429,13 +430,11 @@ __global__ void __launch_bounds__(kBuildCellsPerBlock * 32, 6) k_build_cells(con
         const int slot = seg_base + so - nseg, off = cand_base + lo - (l0 + l1);
         if (nseg > 0) {
             sh_seg_beg[slot] = b0;
-            sh_seg_off[slot] = off;
-            sh_seg_code[slot] = cxy + cz0;
+            sh_seg_offc[slot] = (uint32_t)off | ((cxy + cz0) << kCandIdxBits);
         }
         if (nseg > 1) {
             sh_seg_beg[slot + 1] = b1;
-            sh_seg_off[slot + 1] = off + l0;
-            sh_seg_code[slot + 1] = cxy + cz1;
+            sh_seg_offc[slot + 1] = (uint32_t)(off + l0) | ((cxy + cz1) << kCandIdxBits);
         }
         // the first window straight from the rows, every lane its own
         // segments (later windows of a long sequence expand from the table)
@@ -448,11 +447,15 @@ __global__ void __launch_bounds__(kBuildCellsPerBlock * 32, 6) k_build_cells(con
         seg_base += __shfl_sync(0xffffffffu, so, 31);
         cand_base += __shfl_sync(0xffffffffu, lo, 31);
     }
-    if (lane == 0) sh_seg_off[seg_base] = cand_base;  // total candidates
+    if (lane == 0) sh_seg_offc[seg_base] = (uint32_t)cand_base;  // total candidates
 
     __syncwarp();
     const int nseg = seg_base;
     const int total = cand_base;
+    if (total >= (1 << kCandIdxBits)) {  // the packed table offset cannot hold it
+        if (lane == 0) atomicOr(&A.st->bits, kStatusNlistOverflow);
+        return;
+    }
 
     // the prefetch reads up to kCandPad entries past a window: the cell's
     // first site, unshifted (in bounds, never counted)
@@ -463,9 +466,11 @@ __global__ void __launch_bounds__(kBuildCellsPerBlock * 32, 6) k_build_cells(con
     auto expand = [&](int w0, int wn) {
         __syncwarp();
         for (int sg = 0; sg < nseg; sg++) {
-            const int off = sh_seg_off[sg];
-            const int lo = max(off, w0), hi = min(sh_seg_off[sg + 1], w0 + wn);
-            const uint32_t beg = (uint32_t)(sh_seg_beg[sg] - off), code = sh_seg_code[sg] << kCandIdxBits;
+            constexpr uint32_t kOffMask = (1u << kCandIdxBits) - 1u;
+            const uint32_t oc = sh_seg_offc[sg];
+            const int off = (int)(oc & kOffMask);
+            const int lo = max(off, w0), hi = min((int)(sh_seg_offc[sg + 1] & kOffMask), w0 + wn);
+            const uint32_t beg = (uint32_t)(sh_seg_beg[sg] - off), code = oc & ~kOffMask;
             for (int t = lo + lane; t < hi; t += 32) sh_cand[t - w0] = (beg + (uint32_t)t) | code;
         }
         pad(wn);
