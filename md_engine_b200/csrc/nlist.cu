@@ -119,49 +119,79 @@ __global__ void k_wrap_bin(const GridArgs a0, const GridArgs *__restrict__ tab) 
 }
 
 // exclusive scan of the cell histogram in one block per system (replaces the
-// host cumulativeSum, helpers.h:15-24); also clears the fill counters
-// exclusive scan of the cell counts (one block): thread t owns a contiguous
-// run of cells, so its counts are loaded together (one memory round trip),
-// summed serially, and the run totals are scanned once across the block
-__global__ void k_scan_cells(const GridArgs a0, const GridArgs *__restrict__ tab) {
+// host cumulativeSum, helpers.h:15-24); also clears the fill counters.  The
+// counts pass through shared memory in tiles of kScanTile cells: coalesced
+// loads and stores, thread t scans its eight consecutive cells in registers,
+// warp and block totals by shuffles, a running carry across tiles.
+constexpr int kScanThreads = 1024;
+constexpr int kScanPer = 8;
+constexpr int kScanTile = kScanThreads * kScanPer;
+__global__ void __launch_bounds__(kScanThreads) k_scan_cells(const GridArgs a0, const GridArgs *__restrict__ tab) {
     MDX_GRID_ARGS;
     if (!A.st->rebuild) return;
     const uint32_t *__restrict__ count = A.cell_count;
     uint32_t *__restrict__ start = A.cell_start;
     uint32_t *__restrict__ fill = A.cell_fill;
     const int ncell = A.ncell;
+    __shared__ uint4 tile4[kScanTile / 4];
     __shared__ uint32_t warp_tot[32];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int per = (ncell + blockDim.x - 1) / blockDim.x;
-    const int c0 = min(ncell, (int)threadIdx.x * per), c1 = min(ncell, c0 + per);
-    uint32_t run = 0u;
-    for (int c = c0; c < c1; c++) run += count[c];
-    uint32_t x = run;
+    uint32_t *const tile = reinterpret_cast<uint32_t *>(tile4);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    constexpr int nw = kScanThreads / 32;
+    uint32_t carry = 0u;
+    for (int base = 0; base < ncell; base += kScanTile) {
+        const int nt = min(kScanTile, ncell - base);
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) warp_tot[w] = x;
-    __syncthreads();
-    if (w == 0) {
-        uint32_t t = lane < nw ? warp_tot[lane] : 0u;
+        for (int k = 0; k < kScanPer; k++) {
+            const int c = k * kScanThreads + (int)threadIdx.x;
+            tile[c] = c < nt ? count[base + c] : 0u;
+        }
+        __syncthreads();
+        const uint4 a = tile4[2 * threadIdx.x], b = tile4[2 * threadIdx.x + 1];
+        const uint32_t v[kScanPer] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+        uint32_t run = 0u;
+#pragma unroll
+        for (int k = 0; k < kScanPer; k++) run += v[k];
+        uint32_t x = run;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
-            if (lane >= o) t += y;
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
         }
-        if (lane < nw) warp_tot[lane] = t;
+        if (lane == 31) warp_tot[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            uint32_t t = warp_tot[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+                if (lane >= o) t += y;
+            }
+            warp_tot[lane] = t;
+        }
+        __syncthreads();
+        uint32_t excl = carry + (w > 0 ? warp_tot[w - 1] : 0u) + x - run;
+        uint32_t e[kScanPer];
+#pragma unroll
+        for (int k = 0; k < kScanPer; k++) {
+            e[k] = excl;
+            excl += v[k];
+        }
+        tile4[2 * threadIdx.x] = make_uint4(e[0], e[1], e[2], e[3]);
+        tile4[2 * threadIdx.x + 1] = make_uint4(e[4], e[5], e[6], e[7]);
+        carry += warp_tot[nw - 1];
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < kScanPer; k++) {
+            const int c = k * kScanThreads + (int)threadIdx.x;
+            if (c < nt) {
+                start[base + c] = tile[c];
+                fill[base + c] = 0u;
+            }
+        }
+        __syncthreads();  // tile and warp_tot are reused by the next tile
     }
-    __syncthreads();
-    uint32_t excl = (w > 0 ? warp_tot[w - 1] : 0u) + x - run;
-    for (int c = c0; c < c1; c++) {
-        const uint32_t v = count[c];
-        start[c] = excl;
-        fill[c] = 0u;
-        excl += v;
-    }
-    if (threadIdx.x == blockDim.x - 1) start[ncell] = excl;
+    if (threadIdx.x == 0) start[ncell] = carry;
 }
 
 __global__ void k_scatter(const GridArgs a0, const GridArgs *__restrict__ tab) {
@@ -924,7 +954,7 @@ int nlist_rebuild(State &s, bool force, bool conditional, cudaStream_t bstream) 
     const GridArgs *nt = nullptr;
     MDX_CUDA_TRY(launch_pdl(k_check, dim3(nb), dim3(256), 0, s.stream, A, nt, force ? 1 : 0));
     MDX_CUDA_TRY(launch_pdl(k_wrap_bin, dim3(nb), dim3(256), 0, s.stream, A, nt));
-    MDX_CUDA_TRY(launch_pdl(k_scan_cells, dim3(1), dim3(1024), 0, s.stream, A, nt));
+    MDX_CUDA_TRY(launch_pdl(k_scan_cells, dim3(1), dim3(kScanThreads), 0, s.stream, A, nt));
     MDX_CUDA_TRY(launch_pdl(k_scatter, dim3(nb), dim3(256), 0, s.stream, A, nt));
     MDX_CUDA_TRY(launch_pdl(k_rank, dim3((ncell * 32 + 255) / 256), dim3(256), 0, s.stream, A, nt));
     MDX_CUDA_TRY(launch_pdl(k_gather, dim3(nb), dim3(256), 0, s.stream, A, nt));
@@ -1008,7 +1038,7 @@ int batch_nlist_rebuild(Batch &b) {
     cudaStream_t st = b.stream;
     k_check<<<nb, 256, 0, st>>>(A, tg, 0);
     k_wrap_bin<<<nb, 256, 0, st>>>(A, tg);
-    k_scan_cells<<<dim3(1, R), 1024, 0, st>>>(A, tg);
+    k_scan_cells<<<dim3(1, R), kScanThreads, 0, st>>>(A, tg);
     k_scatter<<<nb, 256, 0, st>>>(A, tg);
     k_rank<<<dim3((b.max_cell * 32 + 255) / 256, R), 256, 0, st>>>(A, tg);
     k_gather<<<nb, 256, 0, st>>>(A, tg);
