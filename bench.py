@@ -32,6 +32,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "water timesteps/s & ns/day on 1 B200, plain vs surrogate/batched at force RMSE"
 L2_FLUSH_BYTES = 256 << 20
+EQ_STEPS = 4000  # untimed relaxation of the seeded start
 
 
 def parse():
@@ -46,6 +47,8 @@ def parse():
     ap.add_argument("--train-iters", type=int, default=4000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-nve", action="store_true", help="skip the NVE energy-drift measurement")
+    ap.add_argument("--eq-steps", type=int, default=EQ_STEPS,
+                    help="untimed relaxation steps of the seeded start before the warm-up")
     return ap.parse_args()
 
 
@@ -100,9 +103,6 @@ def workload_cfg(name, sysd):
             "molecules": int(len(sysd.molecules)), "sites": int(len(sysd.pos))}
 
 
-EQ_STEPS = 4000
-
-
 def _water_state(sysd, e3b, tau):
     from md_engine_b200 import systems
     st, _ = systems.build_water_state(sysd, rcut=9.0, skin=1.0, dt=2.0, interval=10, grid=64, e3b=e3b,
@@ -132,12 +132,12 @@ def equilibrate(name, sysd, steps=EQ_STEPS):
     return dataclasses.replace(sysd, pos=np.asarray(x, np.float64), vel=np.asarray(v, np.float64))
 
 
-def workload(name, seed=20261203):
+def workload(name, seed=20261203, eq_steps=EQ_STEPS):
     from md_engine_b200 import systems
     if name == "lj":
-        sysd = equilibrate(name, systems.lj_fcc(ncell=20, seed=seed))
+        sysd = equilibrate(name, systems.lj_fcc(ncell=20, seed=seed), eq_steps)
         return sysd, _lj_state(sysd, 0.5), workload_cfg(name, sysd), 0.005
-    sysd = equilibrate(name, systems.water_tip4p2005(nside=16, seed=seed))
+    sysd = equilibrate(name, systems.water_tip4p2005(nside=16, seed=seed), eq_steps)
     return sysd, _water_state(sysd, name == "water_e3b", 100.0), workload_cfg(name, sysd), 2.0
 
 
@@ -471,7 +471,7 @@ def main():
     lib().mdx_set_device(local)
     dist = init_pg(world, "nccl")
     dev = torch.device("cuda", local)
-    sysd, st, cfg, dt = workload(args.workload, seed=20261203 + rank)
+    sysd, st, cfg, dt = workload(args.workload, seed=20261203 + rank, eq_steps=args.eq_steps)
     it = IntegratorVerlet(st)
     # warm-up: prepare, capture graphs, settle clocks (untimed)
     it.run(max(args.warmup, 3))
@@ -535,9 +535,9 @@ def main():
             "warmup": max(args.warmup, 3), "ms_per_step": ms_max / K, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 reductions, f64 SETTLE)",
             "data": "synthetic (seeded lattice + random orientations + Maxwell-Boltzmann, "
-                    f"relaxed {EQ_STEPS} untimed steps at the target temperature)",
+                    f"relaxed {args.eq_steps} untimed steps at the target temperature)",
             "config": dict(cfg, l2="flushed between timed 10-step chunks (256 MiB write)",
-                           start=f"equilibrated: {EQ_STEPS} steps, tight Nose-Hoover, before warm-up",
+                           start=f"equilibrated: {args.eq_steps} steps, tight Nose-Hoover, before warm-up",
                            parallelism="replicas only" if world > 1 else "single system"),
             "ns_per_day": ns_day,
             "temperature_end_of_timed_region": t_end,
