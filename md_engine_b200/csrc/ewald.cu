@@ -438,14 +438,21 @@ __device__ __forceinline__ void warp_fft(float2 (&v)[R], int lane, const LaneTw 
 template <int R>
 __device__ __forceinline__ int fft_out_index(int k1, int lane) { return k1 + R * brev5(lane); }
 
+// plane kernels: kFftPlaneWarps warps per block, fixed at compile time so a
+// warp's line loop has a constant trip count and, for the small meshes,
+// unrolls (the lines' loads are in flight together)
+constexpr int kFftPlaneWarps = 16;
+
 template <int R>
-__global__ void __launch_bounds__(1024) k_fft_zy(const FFTArgs A) {
+__global__ void __launch_bounds__(kFftPlaneWarps * 32) k_fft_zy(const FFTArgs A) {
     extern __shared__ float2 plane[];  // [n][n/2+1]
     constexpr int N = 32 * R, NH = N / 2 + 1;
+    constexpr int nw = kFftPlaneWarps, UNR = R <= 2 ? 4 : 1;
     pdl_wait();
     const int x = blockIdx.x;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const LaneTw T = lane_twiddles<R>(lane, A.tw);
+#pragma unroll UNR
     for (int y = w; y < N; y += nw) {
         float2 v[R];
         const float *line = A.rho + ((size_t)x * N + y) * N;
@@ -459,6 +466,7 @@ __global__ void __launch_bounds__(1024) k_fft_zy(const FFTArgs A) {
         }
     }
     __syncthreads();
+#pragma unroll UNR
     for (int kz = w; kz < NH; kz += nw) {
         float2 v[R];
 #pragma unroll
@@ -523,15 +531,17 @@ __global__ void __launch_bounds__(256) k_fft_xe(const FFTArgs A) {
 // one block per (x plane, field component): inverse along y for every kz,
 // then the real inverse along z; component d of the float4 field is written
 template <int R>
-__global__ void __launch_bounds__(1024) k_ifft_yz(const FFTArgs A) {
+__global__ void __launch_bounds__(kFftPlaneWarps * 32) k_ifft_yz(const FFTArgs A) {
     extern __shared__ float2 plane[];  // [n][n/2+1]
     constexpr int N = 32 * R, NH = N / 2 + 1;
+    constexpr int nw = kFftPlaneWarps, UNR = R <= 2 ? 4 : 1;
     pdl_wait();
     const int x = blockIdx.x, d = blockIdx.y;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const LaneTw T = lane_twiddles<R>(lane, A.tw);
     const size_t stride = (size_t)N * NH;
     const float2 *src0 = A.mid2 + (size_t)d * N * stride + (size_t)x * stride;
+#pragma unroll UNR
     for (int kz = w; kz < NH; kz += nw) {
         float2 v[R];
 #pragma unroll
@@ -542,6 +552,7 @@ __global__ void __launch_bounds__(1024) k_ifft_yz(const FFTArgs A) {
     }
     __syncthreads();
     float *e = reinterpret_cast<float *>(A.e4) + d;
+#pragma unroll UNR
     for (int y = w; y < N; y += nw) {
         const float2 *row = plane + y * NH;
         float2 v[R];
@@ -843,9 +854,9 @@ int own_solve(State &s, FixChargeEwald &f, cudaStream_t st) {
     const FFTArgs A = fft_args(s, f);
     // 512-thread plane blocks (measured +0.8 % per water step against 1024
     // beside the pair kernel; 256 was slower)
-    MDX_CUDA_TRY(launch_pdl_prio(true, k_fft_zy<R>, dim3(N), dim3(512), (size_t)N * NH * sizeof(float2), st, A));
+    MDX_CUDA_TRY(launch_pdl_prio(true, k_fft_zy<R>, dim3(N), dim3(kFftPlaneWarps * 32), (size_t)N * NH * sizeof(float2), st, A));
     MDX_CUDA_TRY(launch_pdl_prio(true, k_fft_xe<R>, dim3((N * NH + 7) / 8), dim3(256), 0, st, A));
-    MDX_CUDA_TRY(launch_pdl_prio(true, k_ifft_yz<R>, dim3(N, 3), dim3(512), (size_t)N * NH * sizeof(float2), st, A));
+    MDX_CUDA_TRY(launch_pdl_prio(true, k_ifft_yz<R>, dim3(N, 3), dim3(kFftPlaneWarps * 32), (size_t)N * NH * sizeof(float2), st, A));
     return 0;
 }
 
