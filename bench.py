@@ -542,7 +542,7 @@ def main():
             "ns_per_day": ns_day,
             "temperature_end_of_timed_region": t_end,
             "e2e": {"value": e2e, "unit": "timesteps/s",
-                    "h2d_bytes_per_step": int(2 * 16 * n / P), "d2h_bytes_per_step": int(3 * 16 * n / P)},
+                    "h2d_bytes_per_step": int(2 * 24 * n / P), "d2h_bytes_per_step": int(3 * 24 * n / P)},
             "gpu_launches": int(k1 - k0),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": profile_traffic(args.workload + "_pair"),

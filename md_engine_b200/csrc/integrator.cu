@@ -8,6 +8,7 @@
 // followed by the steps.  Nothing in a step waits on the host.
 #include <chrono>
 #include <cstdio>
+#include <cstring>
 #include <algorithm>
 #include <map>
 #include <vector>
@@ -19,20 +20,26 @@ namespace mdx {
 namespace {
 // host-buffer run support: scatter by id into the sorted device streams and
 // gather them back in id order
-__global__ void k_put_by_id(int n, const float4 *__restrict__ in, const int *__restrict__ idToIdx,
+// host-buffer runs: (n,3) FP64 arrays by atom id in, rounded to FP32 here
+// (the host cast's round-to-nearest), and widened back out; .w is kept
+__global__ void k_put_by_id(int n, const double *__restrict__ in, const int *__restrict__ idToIdx,
                             float4 *__restrict__ dst) {
     int id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= n) return;
     const int i = idToIdx[id];
-    float4 d = dst[i];
-    const float4 v = in[id];
-    dst[i] = make_float4(v.x, v.y, v.z, d.w);
+    const float w = dst[i].w;
+    const double *v = in + 3 * (size_t)id;
+    dst[i] = make_float4((float)v[0], (float)v[1], (float)v[2], w);
 }
 __global__ void k_get_by_id(int n, const float4 *__restrict__ src, const uint32_t *__restrict__ ids,
-                            float4 *__restrict__ out) {
+                            double *__restrict__ out) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    out[ids[i]] = src[i];
+    const float4 v = src[i];
+    double *o = out + 3 * (size_t)ids[i];
+    o[0] = v.x;
+    o[1] = v.y;
+    o[2] = v.z;
 }
 }  // namespace
 
@@ -222,32 +229,33 @@ class IntegratorVerlet {
     // run with host buffers in/out (the call a host program makes): inputs are
     // copied from pinned staging and scattered by id, outputs gathered by id
     // and copied back, all inside the call
-    float4 *h_stage = nullptr;
+    double *h_stage = nullptr;  // pinned: 3 arrays of (n,3) FP64
     size_t h_stage_n = 0;
-    DBuf<float4> d_stage;
+    DBuf<double> d_stage;
     int runHost(int nturns, const double *pin, const double *vin, double *pout, double *vout, double *fout) {
         if (!s->prepared) {
             clearGraphs();
             if (int e = s->prepare()) return e;
         }
         const int n = s->gpd.n;
-        if (h_stage_n < (size_t)3 * n) {
+        const size_t a3 = 3 * (size_t)n;  // doubles per array
+        if (h_stage_n < 3 * a3) {
             if (h_stage) cudaFreeHost(h_stage);
-            MDX_CUDA_TRY(cudaMallocHost(&h_stage, 3 * (size_t)n * sizeof(float4)));
-            h_stage_n = 3 * (size_t)n;
+            MDX_CUDA_TRY(cudaMallocHost(&h_stage, 3 * a3 * sizeof(double)));
+            h_stage_n = 3 * a3;
         }
-        if (int e = d_stage.alloc(3 * (size_t)n)) return e;
+        if (int e = d_stage.alloc(3 * a3)) return e;
+        // inputs: a plain copy into pinned memory, one async copy each, the
+        // FP32 rounding and the scatter by id on the device
         const double *ins[2] = {pin, vin};
         float4 *dsts[2] = {s->gpd.xs.p, s->gpd.vs.p};
         for (int k = 0; k < 2; k++) {
             if (!ins[k]) continue;
-            float4 *h = h_stage + (size_t)k * n;
-            for (int i = 0; i < n; i++)
-                h[i] = make_float4((float)ins[k][3 * i], (float)ins[k][3 * i + 1], (float)ins[k][3 * i + 2], 0.f);
-            MDX_CUDA_TRY(cudaMemcpyAsync(d_stage.p + (size_t)k * n, h, n * sizeof(float4), cudaMemcpyHostToDevice,
+            double *h = h_stage + k * a3;
+            std::memcpy(h, ins[k], a3 * sizeof(double));
+            MDX_CUDA_TRY(cudaMemcpyAsync(d_stage.p + k * a3, h, a3 * sizeof(double), cudaMemcpyHostToDevice,
                                          s->stream));
-            k_put_by_id<<<(n + 255) / 256, 256, 0, s->stream>>>(n, d_stage.p + (size_t)k * n, s->gpd.idToIdx.p,
-                                                              dsts[k]);
+            k_put_by_id<<<(n + 255) / 256, 256, 0, s->stream>>>(n, d_stage.p + k * a3, s->gpd.idToIdx.p, dsts[k]);
             MDX_LAUNCHED();
         }
         const int P = s->periodicInterval > 0 ? s->periodicInterval : 1;
@@ -267,23 +275,16 @@ class IntegratorVerlet {
         const float4 *srcs[3] = {s->gpd.xs.p, s->gpd.vs.p, s->gpd.fs.p};
         for (int k = 0; k < 3; k++) {
             if (!outs[k]) continue;
-            k_get_by_id<<<(n + 255) / 256, 256, 0, s->stream>>>(n, srcs[k], s->gpd.ids.p, d_stage.p + (size_t)k * n);
+            k_get_by_id<<<(n + 255) / 256, 256, 0, s->stream>>>(n, srcs[k], s->gpd.ids.p, d_stage.p + k * a3);
             MDX_LAUNCHED();
-            MDX_CUDA_TRY(cudaMemcpyAsync(h_stage + (size_t)k * n, d_stage.p + (size_t)k * n, n * sizeof(float4),
+            MDX_CUDA_TRY(cudaMemcpyAsync(h_stage + k * a3, d_stage.p + k * a3, a3 * sizeof(double),
                                          cudaMemcpyDeviceToHost, s->stream));
         }
         MDX_CUDA_TRY(cudaMemcpyAsync(s->h_status, s->d_status.p, sizeof(DeviceStatus), cudaMemcpyDeviceToHost,
                                      s->stream));
         MDX_CUDA_TRY(cudaStreamSynchronize(s->stream));
-        for (int k = 0; k < 3; k++) {
-            if (!outs[k]) continue;
-            const float4 *h = h_stage + (size_t)k * n;
-            for (int i = 0; i < n; i++) {
-                outs[k][3 * i] = h[i].x;
-                outs[k][3 * i + 1] = h[i].y;
-                outs[k][3 * i + 2] = h[i].z;
-            }
-        }
+        for (int k = 0; k < 3; k++)
+            if (outs[k]) std::memcpy(outs[k], h_stage + k * a3, a3 * sizeof(double));
         if (s->h_status->bits) return s->checkStatus();
         return 0;
     }

@@ -497,7 +497,7 @@ class IntegratorVerlet:
 
         pa, pp = inp(positions)
         va, vp = inp(velocities)
-        outs = {k: np.zeros((n, 3)) for k in want}
+        outs = {k: np.empty((n, 3)) for k in want}  # every element is written
         op = [outs[k].ctypes.data_as(P(c_dbl)) if k in outs else None for k in ("pos", "vel", "force")]
         check(lib().mdx_integrator_run_host(self._h, int(numTurns), pp, vp, op[0], op[1], op[2]))
         return outs
