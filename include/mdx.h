@@ -134,7 +134,9 @@ int mdx_integrator_destroy(mdx_integrator *it);
  * buffers in the reference, State.cpp:529-610): positions/velocities (3
  * doubles per atom, by id; NULL keeps the resident copy) are copied in,
  * num_turns steps run on the fused graph path, and positions / velocities /
- * forces (NULL to skip) are copied back, all within this call. */
+ * forces (NULL to skip) are copied back, all within this call.  The arrays
+ * cross as FP64 through pinned staging; the FP32 rounding (to nearest) and
+ * the placement by id happen on the device. */
 int mdx_integrator_run_host(mdx_integrator *it, int num_turns, const double *pos_in, const double *vel_in,
                             double *pos_out, double *vel_out, double *force_out);
 /* Benchmark support (no reference counterpart): run num_turns in chunks of
