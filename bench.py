@@ -384,7 +384,7 @@ def run_batched(args, rank, world, local):
 def run_surrogate(args, rank, world, local):
     """TIP4P/2005+E3B3, 4,096 molecules: the exact E3B step against the step
     with the learned three-body surrogate, trained here on frames the exact
-    kernel labels (NVT runs at 260, 310 and 360 K), judged on a frame of an
+    kernel labels (NVT runs at 260, 310 and 360 K), scored on a frame of an
     unseen 330 K run"""
     import torch
     from md_engine_b200 import IntegratorVerlet, kernel_launches, systems

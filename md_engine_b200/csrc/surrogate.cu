@@ -11,7 +11,7 @@
 // 128 -> 64 -> 64 -> 64 -> 9 (SiLU) whose outputs are the three-body forces on
 // O, H1 and H2 of m in m's frame (scaled by the training set's force RMS);
 // they are rotated back to the lab frame.  Forces are not conservative (a
-// regression surrogate, judged by force RMSE); the exact O-O two-body term is
+// regression surrogate, scored by force RMSE); the exact O-O two-body term is
 // kept.
 //
 // Arithmetic.  Every GEMM uses BF16 operands with FP32 accumulation on the

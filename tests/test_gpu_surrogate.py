@@ -1,7 +1,7 @@
 """Learned E3B three-body surrogate: features, MLP inference and the
 hand-written backward pass against the CPU restatement in
 oracle/surrogate_ref.py; then training on frames the exact E3B kernel
-labels, judged by the exact kernel's three-body forces on frames it was not
+labels, scored against the exact kernel's three-body forces on frames it was not
 trained on, against the method without it (no three-body force)."""
 import numpy as np
 import pytest
@@ -62,7 +62,7 @@ def test_mlp_inference_and_gradient_match_oracle():
 
 def test_surrogate_learns_three_body_forces():
     """frames from NVT runs at 260 and 360 K train the network; a frame of a
-    third run at 300 K that it never saw judges it against the exact kernel"""
+    third run at 300 K that it never saw scores it against the exact kernel"""
     sysd, st0, fx0 = _water(nside=8, seed=31, T=260.0)
     e30 = fx0["e3b"]
     it0 = IntegratorVerlet(st0)
