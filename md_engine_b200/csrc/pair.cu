@@ -130,10 +130,11 @@ template <int T, int LJ, bool EW, bool VIR, bool ENERGY>
 __device__ __forceinline__ void pair_row(const PairArgs &A, const float *sp, int nt2, int i, int ti, float qi,
                                          float4 xi, const uint32_t *row, int cnt, int t, float &fx, float &fy,
                                          float &fz, float &en, float (&v)[6]) {
-    // entries per lane per trip: a full-warp team (long water rows) keeps two
-    // in flight -- fewer registers, more resident warps beside the P3M chain
-    // (measured: 32 lanes, U = 2 vs 4: pair 39.2 -> 38.0 us, step +2.5 %)
-    constexpr int U = T >= 32 ? 2 : 4;
+    // entries per lane per trip: a full-warp team (long water rows) keeps
+    // three in flight within its 40-register cap (measured at 24 blocks per
+    // SM: U = 3 vs 2, pair 35.1 -> 33.4 us; U = 4 at the old 256-thread
+    // shape cost registers and resident warps beside the P3M chain)
+    constexpr int U = T >= 32 ? 3 : 4;
     constexpr uint32_t kNone = 0xffffffffu;
     for (int k0 = t; k0 < cnt; k0 += U * T) {
         uint32_t ent[U];
