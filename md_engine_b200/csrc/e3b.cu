@@ -274,10 +274,26 @@ __global__ void k_e3b_totals(const E3BArgs a0, const E3BArgs *__restrict__ tab) 
         int cnt = (int)mcounts[m];
         cnt = cnt < mcap ? cnt : mcap;
         const uint32_t *row = mlist + (size_t)(m / G) * mcap * G + a * T + t;
-        for (int k = t; k < cnt; k += T) {
-            const int mj = (int)row[(size_t)(k / T) * 32];
-            const int4 jx = __ldg(mol_idx + mj);
-            const float3 oj = f3(__ldg(xs + jx.x));
+        // two entries per lane per trip: both list -> molecule -> O chains are
+        // in flight before either pair is evaluated
+        for (int k0 = t; k0 < cnt; k0 += 2 * T) {
+            int4 jxs[2];
+            float3 ojs[2];
+            bool has[2];
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                const int k = k0 + u * T;
+                has[u] = k < cnt;
+                const int mj = has[u] ? (int)row[(size_t)(k / T) * 32] : m;
+                jxs[u] = __ldg(mol_idx + mj);
+            }
+#pragma unroll
+            for (int u = 0; u < 2; u++) ojs[u] = f3(__ldg(xs + jxs[u].x));
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+            if (!has[u]) continue;
+            const int4 jx = jxs[u];
+            const float3 oj = ojs[u];
             const float3 dr = min_image(box, mi.a - oj);
             const float r2 = dot3(dr, dr);
             if (r2 >= p.list_cut2) continue;
@@ -303,6 +319,7 @@ __global__ void k_e3b_totals(const E3BArgs a0, const E3BArgs *__restrict__ tab) 
                 ty += e;
                 e3b_ef(p, min_image(box, mi.c - mj_.a), e, f);
                 tz += e;
+            }
             }
         }
     }
