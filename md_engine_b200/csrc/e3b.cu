@@ -383,11 +383,26 @@ __global__ void k_e3b_forces(const E3BArgs a0, const E3BArgs *__restrict__ tab) 
         int cnt = (int)mcounts[m];
         cnt = cnt < mcap ? cnt : mcap;
         const uint32_t *row = mlist + (size_t)(m / G) * mcap * G + a * T + t;
-        for (int k = t; k < cnt; k += T) {
-            const int mj = (int)row[(size_t)(k / T) * 32];
-            const int4 jx = __ldg(mol_idx + mj);
+        // two entries per lane per trip, as the totals pass
+        for (int k0 = t; k0 < cnt; k0 += 2 * T) {
+            int mjs[2];
+            int4 jxs[2];
+            float3 ojs[2];
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                const int k = k0 + u * T;
+                mjs[u] = k < cnt ? (int)row[(size_t)(k / T) * 32] : -1;
+                jxs[u] = __ldg(mol_idx + (mjs[u] < 0 ? m : mjs[u]));
+            }
+#pragma unroll
+            for (int u = 0; u < 2; u++) ojs[u] = f3(__ldg(xs + jxs[u].x));
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+            if (mjs[u] < 0) continue;
+            const int mj = mjs[u];
+            const int4 jx = jxs[u];
             MolPos mjp;
-            mjp.a = f3(__ldg(xs + jx.x));
+            mjp.a = ojs[u];
             const float3 dr = min_image(box, mi.a - mjp.a);
             const float r2 = dot3(dr, dr);
             if (r2 >= p.list_cut2) continue;
@@ -416,6 +431,7 @@ __global__ void k_e3b_forces(const E3BArgs a0, const E3BArgs *__restrict__ tab) 
             add_force<STORE>(fs + jx.x, a2);
             add_force<STORE>(fs + jx.y, b2);
             add_force<STORE>(fs + jx.z, c2);
+            }
         }
     }
     if (ENERGY) {
