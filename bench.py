@@ -105,15 +105,13 @@ def workload_cfg(name, sysd):
 
 def _water_state(sysd, e3b, tau):
     from md_engine_b200 import systems
-    st, _ = systems.build_water_state(sysd, rcut=9.0, skin=1.0, dt=2.0, interval=10, grid=64, e3b=e3b,
-                                      T=298.0, tau=tau)
-    return st
+    return systems.build_water_state(sysd, rcut=9.0, skin=1.0, dt=2.0, interval=10, grid=64, e3b=e3b,
+                                     T=298.0, tau=tau)
 
 
 def _lj_state(sysd, tau):
     from md_engine_b200 import systems
-    st, _ = systems.build_lj_state(sysd, rcut=2.5, skin=0.3, dt=0.005, interval=10, T=1.2, tau=tau)
-    return st
+    return systems.build_lj_state(sysd, rcut=2.5, skin=0.3, dt=0.005, interval=10, T=1.2, tau=tau)
 
 
 def equilibrate(name, sysd, steps=EQ_STEPS):
@@ -126,7 +124,7 @@ def equilibrate(name, sysd, steps=EQ_STEPS):
     the timed steps would run a hot, near-lattice system instead."""
     import dataclasses
     from md_engine_b200 import IntegratorVerlet
-    st = _lj_state(sysd, 0.1) if name == "lj" else _water_state(sysd, name == "water_e3b", 25.0)
+    st, _ = _lj_state(sysd, 0.1) if name == "lj" else _water_state(sysd, name == "water_e3b", 25.0)
     IntegratorVerlet(st).run(steps)
     x, v, _ = st.getAtoms()
     return dataclasses.replace(sysd, pos=np.asarray(x, np.float64), vel=np.asarray(v, np.float64))
@@ -136,9 +134,11 @@ def workload(name, seed=20261203, eq_steps=EQ_STEPS):
     from md_engine_b200 import systems
     if name == "lj":
         sysd = equilibrate(name, systems.lj_fcc(ncell=20, seed=seed), eq_steps)
-        return sysd, _lj_state(sysd, 0.5), workload_cfg(name, sysd), 0.005
+        st, fx = _lj_state(sysd, 0.5)
+        return sysd, st, fx, workload_cfg(name, sysd), 0.005
     sysd = equilibrate(name, systems.water_tip4p2005(nside=16, seed=seed), eq_steps)
-    return sysd, _water_state(sysd, name == "water_e3b", 100.0), workload_cfg(name, sysd), 2.0
+    st, fx = _water_state(sysd, name == "water_e3b", 100.0)
+    return sysd, st, fx, workload_cfg(name, sysd), 2.0
 
 
 def timed_temperature(name, sysd, st):
@@ -254,11 +254,40 @@ def profile_traffic(key):
     return None
 
 
-def cpu_baseline(sysd, name, dt_fs, nsample=1):
-    """The oracle's FP64 water step on the host cores (the reference has no CPU
-    force path; its CPU restatement is the baseline).  Bounded sample."""
+def fp64_errors(name, sysd, st, fx):
+    """Error of every reported quantity of the timed state against the FP64
+    oracle on the same positions: per-site forces (the largest error vector
+    and the RMS error, both over the RMS force), potential energy per term
+    and in total, and the total virial (largest component error over the
+    largest component).  The kinetic energy is an FP64 device sum of the FP32
+    velocities (no separate error).  Part of the CPU-baseline leg."""
     from oracle import cpu_step
-    return cpu_step.time_steps(sysd, name, nsample=nsample)
+    st.computeForces(virialMode=1)
+    x, _, fg = st.getAtoms()
+    _, vir = st.virials()
+    eg = np.asarray(st.potentialEnergy(), np.float64)
+    if name == "lj":
+        ref = cpu_step.lj_reference(sysd, x, rcut=2.5, skin=0.3)
+        e_terms = {"pair": (eg[0], ref["energy"]["pair"])}
+    else:
+        ref = cpu_step.water_reference(sysd, x, rcut=9.0, skin=1.0, grid=64, alpha=fx["ewald"].alpha,
+                                       e3b=name == "water_e3b")
+        e_terms = {"pair": (eg[0], ref["energy"]["pair"]), "p3m": (eg[1], ref["energy"]["p3m"])}
+        if name == "water_e3b":
+            e_terms["e3b_two_body"] = (eg[2], ref["energy"]["e3b2"])
+            e_terms["e3b_three_body"] = (eg[3], ref["energy"]["e3b3"])
+    fr = ref["f"]
+    rms = float(np.sqrt(np.mean(np.sum(fr ** 2, 1))))
+    d = np.linalg.norm(fg - fr, axis=1)
+    etot_g = sum(a for a, _ in e_terms.values())
+    etot_r = sum(b for _, b in e_terms.values())
+    vr = ref["virial"]
+    return {"oracle": "FP64 CPU restatement (oracle/), same positions, list, alpha and mesh",
+            "force_max_err_over_rms": float(d.max() / rms), "force_rms_err_over_rms": float(np.sqrt(np.mean(d ** 2)) / rms),
+            "force_rms": rms,
+            "energy_rel": {k: float(abs(a - b) / max(abs(b), 1e-300)) for k, (a, b) in e_terms.items()},
+            "energy_total_rel": float(abs(etot_g - etot_r) / abs(etot_r)),
+            "virial_max_err_over_max": float(np.abs(np.asarray(vir) - vr).max() / np.abs(vr).max())}
 
 
 def run_reference_arm(args, rank, world):
@@ -274,8 +303,10 @@ def run_reference_arm(args, rank, world):
     else:
         sysd = systems.water_tip4p2005(nside=16)
         dt = 2.0
-    steps = max(1, min(args.steps, 3))
-    warm = 1 if args.warmup > 0 else 0
+    # a bounded sample: up to 5 warm-up and 50 timed whole steps (a few
+    # seconds to a minute on the host cores)
+    steps = max(1, min(args.steps, 50))
+    warm = min(args.warmup, 5)
     res = cpu_step.time_steps(sysd, args.workload, nsample=steps, warmup=warm)
     v = res["steps_per_s"]
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "timesteps/s", "n_gpus": world,
@@ -473,7 +504,7 @@ def main():
     lib().mdx_set_device(local)
     dist = init_pg(world, "nccl")
     dev = torch.device("cuda", local)
-    sysd, st, cfg, dt = workload(args.workload, seed=20261203 + rank, eq_steps=args.eq_steps)
+    sysd, st, fx, cfg, dt = workload(args.workload, seed=20261203 + rank, eq_steps=args.eq_steps)
     it = IntegratorVerlet(st)
     # warm-up: prepare, capture graphs, settle clocks (untimed)
     it.run(max(args.warmup, 3))
@@ -495,6 +526,9 @@ def main():
     x, v, _ = st.getAtoms()
     n = len(x)
     e2e_calls = max(1, K // P)
+    # one untimed call first (pinned staging allocation, graph shapes)
+    out = it.runHost(P, positions=x, velocities=v)
+    x, v = out["pos"], out["vel"]
     barrier(dist, dev)
     t0 = time.perf_counter()
     for _ in range(e2e_calls):
@@ -565,14 +599,21 @@ def main():
             except Exception as ex:  # reported, never required
                 line["nve_drift"] = {"value": None, "error": str(ex)}
         if world == 1 and not args.no_cpu_baseline:
+            # the CPU baseline leg: the oracle's FP64 step timed on the host
+            # cores, and the same FP64 evaluation as the judge of the timed
+            # state's forces, energies and virial (outside the timed region)
             try:
                 from oracle import cpu_step
-                res = cpu_step.time_steps(sysd, args.workload, nsample=1, warmup=0)
+                res = cpu_step.time_steps(sysd, args.workload, nsample=10, warmup=2, repeats=3)
                 line["cpu_baseline"] = {"value": res["steps_per_s"], "unit": "timesteps/s", "cores": res["cores"],
                                         "kind": "port", "sample": res["sample"]}
             except Exception as ex:  # the baseline is reported, never required
                 line["cpu_baseline"] = {"value": None, "unit": "timesteps/s", "cores": os.cpu_count(),
                                         "kind": "port", "sample": f"failed: {ex}"}
+            try:
+                line["fp64_oracle_error"] = fp64_errors(args.workload, sysd, st, fx)
+            except Exception as ex:
+                line["fp64_oracle_error"] = {"error": str(ex)}
         print(json.dumps(line))
     if dist is not None:
         barrier(dist, dev)

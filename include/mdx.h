@@ -176,9 +176,11 @@ int mdx_kinetic(mdx_state *st, double *sum_mv2, double *ndf);
  * in the reference.  It allocates nothing: its block partials live in a fixed
  * 64 KiB file-scope device array (held on every GPU that loads the library
  * until exit), so states of more than 2,097,152 atoms are rejected with
- * MDX_ERR_ARG.  The first call on a device looks the array up (set-up, once
- * per device) and should come before any stream capture; all calls share the
- * array, so calls whose kernels overlap on the GPU race. */
+ * MDX_ERR_ARG.  The call runs on the state's own device (made current for
+ * the call; the caller's current device is restored after).  The first call
+ * on a device looks the array up (set-up, once per device) and should come
+ * before any stream capture; all calls share the array, so calls whose
+ * kernels overlap on the GPU race. */
 int mdx_kinetic_noalloc(mdx_state *st, double *sum_mv2);
 /* DataComputerPressure::computeScalar_CPU (src/DataStorageUser/
  * DataComputerPressure.cu:76-92): scalar pressure (sum m v^2 + virial trace)
@@ -193,12 +195,19 @@ int mdx_rigid_settle_positions(mdx_state *st, mdx_fix *rigid);   /* save_prev_va
 int mdx_rigid_save_prev(mdx_state *st, mdx_fix *rigid);
 int mdx_rigid_settle_velocities(mdx_state *st, mdx_fix *rigid);
 int mdx_rigid_distribute_msite(mdx_state *st, mdx_fix *rigid);
+/* validateConstraints (src/Fixes/FixRigid.cu:351-447) on the current
+ * positions and velocities: *n_bad = molecules whose O-H1, O-H2 or H1-H2
+ * length is off by more than 1e-3 (NaN counts as off) or whose relative
+ * velocity along a bond exceeds 1e-3; returns MDX_ERR_NUMERIC when n_bad > 0
+ * (the reference prints instead).  The fused step applies the same length
+ * test to every molecule after SETTLE and reports it as MDX_ERR_NUMERIC. */
+int mdx_rigid_validate(mdx_state *st, mdx_fix *rigid, uint32_t *n_bad);
 int mdx_verlet_first_half(mdx_state *st);   /* nve_v + nve_x (IntegratorVerlet.cu:23-61) */
 int mdx_verlet_second_half(mdx_state *st);  /* postForce_cu (IntegratorVerlet.cu:610-627) */
 
-/* ---- raw device-pointer entry point (EvaluatorWrapper::compute,
- *      src/Evaluators/EvaluatorWrapper.h:10-16 / PairEvaluateIso.h:8-207) --
- * Pair forces over a neighbour list in this library's layout: atom i is in
+/* ---- raw device-pointer entry points (PairEvaluateIso.h:8-207) ----------
+ * mdx_pair_force_raw: the pair kernel over a neighbour list in this
+ * library's own layout (mdx_pair_force_gridgpu below takes GridGPU's): atom i is in
  * warp group g = i / (32/team), slot a = i % (32/team); its k-th entry is at
  * nlist[g*cap*(32/team) + (k/team)*32 + a*team + k%team]; entries are atom
  * indices with the exclusion depth in bits 30-31.  params = {rc2, 24*eps,
@@ -210,6 +219,28 @@ int mdx_pair_force_raw(int n, const float *xs4, float *fs4, const float *qs, con
                        const uint32_t *nlist, int team, int cap, const float *params, int ntypes,
                        const double lo[3], const double hi[3], const float coef[3], int lj_kind, float qrc,
                        float alpha, float qqr_to_eng, float *virials, int accumulate, void *cuda_stream);
+
+/* EvaluatorWrapperImplement::compute (src/Evaluators/EvaluatorWrapper.h:10-16,
+ * 49-109) on GridGPU's list exactly as the reference hands it over
+ * (GridGPU.cu:777-821, cutils_func.h:23-45): neighbor_counts (uint16 per
+ * atom), neighborlist with atom i's k-th entry at
+ *   (NTPB/32)*cum[b] + (cum[b+1]-cum[b])*w + s*NTPA + k%NTPA + 32*(k/NTPA)
+ * where b = i/(NTPB/NTPA), w and s the warp and slot of i within block b
+ * (cum = cumul_sum_max_per_block, NTPB/NTPA = n_thread_per_block/atom);
+ * entries carry the exclusion depth in bits 30-31.  parameters = {rc2,
+ * 24 eps, sig^6} per type pair; lj_kind 0 none / 1 LJ / 2 WCA (the pair
+ * evaluator the reference's template names), q_cutoff <= 0 disables the
+ * Ewald real-space term (alpha and qqr_to_eng are ChargeEvaluatorEwald's
+ * members).  Forces are added to fs4; with virial_mode 1 or 2, 0.5 F (x) dr
+ * per atom is added to virials (6 floats per atom).  warp_size must be 32
+ * and n_per_ring_poly 1.  All pointers device. */
+int mdx_pair_force_gridgpu(int n_atoms, int n_per_ring_poly, const float *xs4, float *fs4,
+                           const uint16_t *neighbor_counts, const uint32_t *neighborlist,
+                           const uint32_t *cumul_sum_max_per_block, int warp_size, const float *parameters,
+                           int num_types, const double lo[3], const double hi[3], float onetwo_str,
+                           float onethree_str, float onefour_str, float *virials, const float *qs, float q_cutoff,
+                           int virial_mode, int n_thread_per_block, int n_thread_per_atom, int lj_kind, float alpha,
+                           float qqr_to_eng, void *cuda_stream);
 
 /* ---- learned E3B three-body surrogate (no reference counterpart; the exact
  *      term is src/Fixes/ThreeBodyE3B.h:255-549, which stays the fallback) --

@@ -87,6 +87,10 @@ SIGNATURES = [
     ("mdx_pair_force_raw", c_int, [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int,
                                    c_void_p, c_int, P(c_dbl), P(c_dbl), P(c_flt), c_int, c_flt, c_flt, c_flt,
                                    c_void_p, c_int, c_void_p]),
+    ("mdx_pair_force_gridgpu", c_int, [c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int,
+                                       c_void_p, c_int, P(c_dbl), P(c_dbl), c_flt, c_flt, c_flt, c_void_p, c_void_p,
+                                       c_flt, c_int, c_int, c_int, c_int, c_flt, c_flt, c_void_p]),
+    ("mdx_rigid_validate", c_int, [c_void_p, c_void_p, P(ctypes.c_uint32)]),
     ("mdx_e3b_surrogate_collect", c_int, [c_void_p, c_void_p]),
     ("mdx_e3b_surrogate_dataset_size", c_int, [c_void_p, P(ctypes.c_int64)]),
     ("mdx_e3b_surrogate_train", c_int, [c_void_p, c_void_p, c_int, c_int, c_flt, ctypes.c_uint64, P(c_dbl), P(c_dbl)]),

@@ -607,6 +607,19 @@ RIGID_HOOK(mdx_rigid_settle_positions, 1)
 RIGID_HOOK(mdx_rigid_distribute_msite, 2)
 RIGID_HOOK(mdx_rigid_settle_velocities, 3)
 
+int mdx_rigid_validate(mdx_state *st, mdx_fix *rigid, uint32_t *n_bad) {
+    ARG_CHECK(st && rigid && n_bad, "null argument");
+    State &s = *st->s;
+    FixRigid *r = rigid_of(st, rigid);
+    ARG_CHECK(r, "not a FixRigid");
+    if (int e = need_prepared(s)) return e;
+    GUARD(if (int e = rigid_validate(s, *r, n_bad)) return e; if (*n_bad) {
+        set_error(MDX_ERR_NUMERIC, "%u rigid molecules off their constraints (side lengths or bond velocities beyond 1e-3)",
+                  *n_bad);
+        return MDX_ERR_NUMERIC;
+    } return 0;)
+}
+
 int mdx_verlet_first_half(mdx_state *st) {
     ARG_CHECK(st, "null state");
     if (int e = need_prepared(*st->s)) return e;
@@ -714,6 +727,38 @@ int mdx_pair_force_raw(int n, const float *xs4, float *fs4, const float *qs, con
     GUARD(return pair_force_raw(n, (const float4 *)xs4, (float4 *)fs4, qs, counts, nlist, team, cap, params, ntypes, b,
                                 coef, lj_kind, qrc, alpha, qqr_to_eng, virials, accumulate != 0,
                                 (cudaStream_t)stream);)
+}
+
+int mdx_pair_force_gridgpu(int n_atoms, int n_per_ring_poly, const float *xs4, float *fs4,
+                           const uint16_t *neighbor_counts, const uint32_t *neighborlist,
+                           const uint32_t *cumul_sum_max_per_block, int warp_size, const float *parameters,
+                           int num_types, const double lo[3], const double hi[3], float onetwo_str,
+                           float onethree_str, float onefour_str, float *virials, const float *qs, float q_cutoff,
+                           int virial_mode, int n_thread_per_block, int n_thread_per_atom, int lj_kind, float alpha,
+                           float qqr_to_eng, void *stream) {
+    ARG_CHECK(n_atoms >= 0 && xs4 && fs4 && neighbor_counts && neighborlist && cumul_sum_max_per_block && lo && hi,
+              "null argument");
+    ARG_CHECK(n_per_ring_poly == 1, "nPerRingPoly must be 1 (path-integral beads are outside this path)");
+    ARG_CHECK(warp_size == 32, "warpSize must be 32");
+    const int t = n_thread_per_atom;
+    ARG_CHECK(t == 1 || t == 2 || t == 4 || t == 8 || t == 16 || t == 32, "nThreadPerAtom must be 1,2,4,8,16 or 32");
+    ARG_CHECK(n_thread_per_block >= 32 && n_thread_per_block % 32 == 0, "nThreadPerBlock must be a multiple of 32");
+    ARG_CHECK(lj_kind == 0 || parameters, "parameters required for LJ/WCA");
+    ARG_CHECK(q_cutoff <= 0.f || qs, "charges required for the Ewald term");
+    ARG_CHECK(virial_mode == 0 || virial_mode == 1 || virial_mode == 2, "virialMode must be 0, 1 or 2");
+    ARG_CHECK(virial_mode == 0 || virials, "virials required for virialMode 1 or 2");
+    Box b;
+    b.lod = make_double3(lo[0], lo[1], lo[2]);
+    b.Ld = make_double3(hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]);
+    b.invLd = make_double3(1.0 / b.Ld.x, 1.0 / b.Ld.y, 1.0 / b.Ld.z);
+    b.lo = make_float3((float)lo[0], (float)lo[1], (float)lo[2]);
+    b.L = make_float3((float)b.Ld.x, (float)b.Ld.y, (float)b.Ld.z);
+    b.invL = make_float3(1.0f / b.L.x, 1.0f / b.L.y, 1.0f / b.L.z);
+    const float coef[3] = {onetwo_str, onethree_str, onefour_str};
+    GUARD(return pair_force_gridgpu(n_atoms, (const float4 *)xs4, (float4 *)fs4, neighbor_counts, neighborlist,
+                                    cumul_sum_max_per_block, n_thread_per_block, t, parameters, num_types, b, coef,
+                                    lj_kind, qs, q_cutoff, alpha, qqr_to_eng, virial_mode ? virials : nullptr,
+                                    (cudaStream_t)stream);)
 }
 
 }  // extern "C"

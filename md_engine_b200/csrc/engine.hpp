@@ -345,6 +345,7 @@ class FixRigid : public Fix {
     RigidConsts rc{};
     DBuf<int4> d_mol_ids, d_mol_idx;
     DBuf<float4> xs0;  // previous constrained O,H1,H2 (stand-alone hook path)
+    DBuf<uint32_t> d_bad;  // validateConstraints hook: molecules off their constraints
     bool foursite = false, threesite = false;
     FixRigid(State *s, std::string h, std::string st);
     int createRigid(int o, int h1, int h2, int m);
@@ -403,8 +404,13 @@ class State {
     DBuf<double> red_partials;
     DBuf<double> red_out;
     DBuf<unsigned int> red_counter;
+    // per-site pair energies and their FP64 sum (energy evaluations outside
+    // the step; sized at upload so that no evaluation allocates)
+    DBuf<float> e_site;
+    DBuf<double> e_sum;
     cudaStream_t stream = nullptr;
     bool own_stream = true;
+    int device = -1;  // the CUDA device the state's buffers and streams live on (set at upload)
     // concurrent branches of the fused step: P3M, E3B, and the list build of
     // a rebuild step
     cudaStream_t side[3] = {nullptr, nullptr, nullptr};
@@ -510,6 +516,10 @@ int pair_force_raw(int n, const float4 *xs, float4 *fs, const float *qs, const u
                    const uint32_t *nlist, int team, int cap, const float *params, int ntypes, const Box &box,
                    const float coef[3], int lj_kind, float qrc, float alpha, float qqr, float *virials,
                    bool accumulate, cudaStream_t stream);
+int pair_force_gridgpu(int n, const float4 *xs, float4 *fs, const uint16_t *counts, const uint32_t *nlist,
+                       const uint32_t *cum, int ntpb, int ntpa, const float *params, int ntypes, const Box &box,
+                       const float coef[3], int lj_kind, const float *qs, float qcut, float alpha, float qqr,
+                       float *virials, cudaStream_t stream);
 // e3b (e3b.cu)
 int e3b_build_list(State &s, FixE3B &f, bool conditional, cudaStream_t st = nullptr);
 int e3b_forces(State &s, FixE3B &f);
@@ -529,10 +539,12 @@ int step_second_half(State &s, bool fused, const float4 *fextra = nullptr, const
 bool has_free_atoms(State &s);
 int rigid_prepare(State &s, FixRigid &r);
 int rigid_hook(State &s, FixRigid &r, int which);
+int rigid_validate(State &s, FixRigid &r, uint32_t *n_bad);
 int kinetic_sum(State &s, double *out);
 int nh_prepare(State &s, FixNoseHoover &nh);
 int zero_forces(State &s);
 int device_sum(State &s, const double *src, int n, double *out_host);
+int float_sum(State &s, const float *src, int n, double *out_host);
 int virial_sum(State &s, double out[6]);
 int remove_com_velocity(State &s);
 int nh_end_of_run(State &s);

@@ -193,6 +193,28 @@ __device__ void settle_vel(const RigidConsts &rc, const Box &box, const float4 x
     v[2] = make_float4((float)vH2.x, (float)vH2.y, (float)vH2.z, v[2].w);
 }
 
+// validateConstraints (FixRigid.cu:351-447): bit 0 set when a side length
+// (O-H1, O-H2, H1-H2) is off its fixed value by more than 1e-3 (a NaN
+// length counts as off); with v, bit 1 set when a relative velocity along a
+// bond, dot(r_ij, v_j - v_i), exceeds 1e-3 (the reference's one-sided test)
+__device__ __forceinline__ uint32_t rigid_violation(const RigidConsts &rc, const Box &box, const float4 x[3],
+                                                    const float4 *v) {
+    const float tol = 1e-3f;
+    const float3 r01 = min_image(box, f3(x[1]) - f3(x[0]));
+    const float3 r02 = min_image(box, f3(x[2]) - f3(x[0]));
+    const float3 r12 = min_image(box, f3(x[2]) - f3(x[1]));
+    const float oh = (float)rc.r_OH, hh = (float)rc.r_HH;
+    uint32_t bad = 0u;
+    if (!(fabsf(sqrtf(dot3(r01, r01)) - oh) <= tol) || !(fabsf(sqrtf(dot3(r02, r02)) - oh) <= tol) ||
+        !(fabsf(sqrtf(dot3(r12, r12)) - hh) <= tol))
+        bad |= 1u;
+    if (v) {
+        const float3 v01 = f3(v[1]) - f3(v[0]), v02 = f3(v[2]) - f3(v[0]), v12 = f3(v[2]) - f3(v[1]);
+        if (dot3(r01, v01) > tol || dot3(r02, v02) > tol || dot3(r12, v12) > tol) bad |= 2u;
+    }
+    return bad;
+}
+
 // setMSite (FixRigid.cu:560-599), FP32 as the reference
 __device__ __forceinline__ float4 msite(const RigidConsts &rc, const Box &box, const float4 x[3], float w) {
     const float3 o = f3(x[0]);
@@ -503,11 +525,9 @@ __global__ void k_second_mol(const MolArgs a0, const MolArgs *__restrict__ tab) 
             for (int k = 0; k < 3; k++) fs[id3[k]] = f[k];
         }
         settle_vel(rc, box, x, v);
-        // validateConstraints (FixRigid.cu:351-447): flag, never print/trap
-        const float3 o = f3(x[0]);
-        const float d1 = sqrtf(dot3(min_image(box, f3(x[1]) - o), min_image(box, f3(x[1]) - o)));
-        const float d2 = sqrtf(dot3(min_image(box, f3(x[2]) - o), min_image(box, f3(x[2]) - o)));
-        if (fabsf(d1 - (float)rc.r_OH) > 1e-3f || fabsf(d2 - (float)rc.r_OH) > 1e-3f) atomicOr(&st->bits, kStatusConstraint);
+        // validateConstraints (FixRigid.cu:351-447), side lengths: flag,
+        // never print or trap
+        if (rigid_violation(rc, box, x, nullptr)) atomicOr(&st->bits, kStatusConstraint);
 #pragma unroll
         for (int k = 0; k < 3; k++) {
             vs[id3[k]] = v[k];
@@ -523,6 +543,18 @@ __global__ void k_second_mol(const MolArgs a0, const MolArgs *__restrict__ tab) 
 }
 
 // ---- stand-alone hooks (one kernel per reference hook) ------------------
+// validateConstraints as its own hook: counts the molecules whose side
+// lengths or bond velocities are off (into *bad), leaves the status word alone
+__global__ void k_validate_hook(int nmol, const int4 *__restrict__ mol_idx, const float4 *__restrict__ xs,
+                                const float4 *__restrict__ vs, RigidConsts rc, Box box, uint32_t *bad) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= nmol) return;
+    const int4 ix = mol_idx[m];
+    const float4 x[3] = {xs[ix.x], xs[ix.y], xs[ix.z]};
+    const float4 v[3] = {vs[ix.x], vs[ix.y], vs[ix.z]};
+    if (rigid_violation(rc, box, x, v)) atomicAdd(bad, 1u);
+}
+
 __global__ void k_save_prev(int nmol, const int4 *__restrict__ mol_idx, const float4 *__restrict__ xs,
                             float4 *__restrict__ xs0) {
     int m = blockIdx.x * blockDim.x + threadIdx.x;
@@ -914,6 +946,22 @@ int rigid_hook(State &s, FixRigid &r, int which) {
     return 0;
 }
 
+// validateConstraints (FixRigid.cu:351-447) on the current positions and
+// velocities: *n_bad = molecules off their constraints
+int rigid_validate(State &s, FixRigid &r, uint32_t *n_bad) {
+    const int nmol = (int)r.mol_ids.size();
+    *n_bad = 0;
+    if (nmol == 0) return 0;
+    if (int e = r.d_bad.alloc(1)) return e;
+    MDX_CUDA_TRY(cudaMemsetAsync(r.d_bad.p, 0, sizeof(uint32_t), s.stream));
+    k_validate_hook<<<(nmol + 127) / 128, 128, 0, s.stream>>>(nmol, r.d_mol_idx.p, s.gpd.xs.p, s.gpd.vs.p, r.rc,
+                                                               s.box, r.d_bad.p);
+    MDX_LAUNCHED();
+    MDX_CUDA_TRY(cudaMemcpyAsync(n_bad, r.d_bad.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s.stream));
+    MDX_CUDA_TRY(cudaStreamSynchronize(s.stream));
+    return 0;
+}
+
 // FixRigid::prepareForRun (FixRigid.cu:1740-1880) with solveInitialConstraints:
 // SETTLE the current configuration onto itself, place M, settle velocities,
 // remove the centre-of-mass velocity
@@ -957,6 +1005,15 @@ int kinetic_sum(State &s, double *out) {
     k_reduce_vec<<<1, 256, 0, s.stream>>>(nb, part.p, 1, 0, o.p);
     MDX_LAUNCHED();
     MDX_CUDA_TRY(cudaMemcpyAsync(out, o.p, sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+    MDX_CUDA_TRY(cudaStreamSynchronize(s.stream));
+    return 0;
+}
+
+// FP64 sum of n floats on the device (one block, fixed order) into *out_host
+int float_sum(State &s, const float *src, int n, double *out_host) {
+    k_reduce_float<<<1, 256, 0, s.stream>>>(n, src, 1, 0, s.e_sum.p);
+    MDX_LAUNCHED();
+    MDX_CUDA_TRY(cudaMemcpyAsync(out_host, s.e_sum.p, sizeof(double), cudaMemcpyDeviceToHost, s.stream));
     MDX_CUDA_TRY(cudaStreamSynchronize(s.stream));
     return 0;
 }

@@ -178,6 +178,38 @@ class IntegratorVerlet {
         g_launches += graph_kernels[std::make_pair(nsteps, with_group ? 1 : 0)];
         return 0;
     }
+    // the (steps, rebuild group) chunk shapes that nturns steps from the
+    // current turn split into, given a window of `chunk` steps (chunk <= 0:
+    // one window); each window is cut at every periodicInterval boundary
+    std::vector<std::pair<int, bool>> chunkShapes(int nturns, int chunk) const {
+        std::vector<std::pair<int, bool>> out;
+        const int P = s->periodicInterval > 0 ? s->periodicInterval : 1;
+        int64_t t = s->turn;
+        int done = 0;
+        while (done < nturns) {
+            int todo = chunk > 0 ? std::min(chunk, nturns - done) : nturns - done;
+            while (todo > 0) {
+                const bool check = (t % P) == 0;
+                int c = check ? P : (int)(P - (t % P));
+                c = std::min(c, todo);
+                out.emplace_back(c, check);
+                t += c;
+                todo -= c;
+                done += c;
+            }
+        }
+        return out;
+    }
+    // capture and instantiate, ahead of time, every graph a run of nturns
+    // steps in windows of `chunk` will launch, so that no capture or
+    // instantiation happens between a window's timing events
+    int precapture(int nturns, int chunk) {
+        for (const auto &sh : chunkShapes(nturns, chunk)) {
+            cudaGraphExec_t ex;
+            if (int e = getGraph(sh.first, sh.second, &ex)) return e;
+        }
+        return 0;
+    }
     // bench support: nturns in chunks of `chunk`, each chunk bracketed by
     // CUDA events on the library stream, L2 flushed (a write larger than L2)
     // before every chunk outside the timed windows; returns summed device ms
@@ -189,6 +221,8 @@ class IntegratorVerlet {
         DBuf<char> flush;
         if (flush_bytes)
             if (int e = flush.alloc(flush_bytes)) return e;
+        // every graph shape of the timed windows exists before the first event
+        if (int e = precapture(nturns, chunk)) return e;
         std::vector<cudaEvent_t> ev;
         const int P = s->periodicInterval > 0 ? s->periodicInterval : 1;
         int done = 0;
@@ -245,6 +279,8 @@ class IntegratorVerlet {
             h_stage_n = 3 * a3;
         }
         if (int e = d_stage.alloc(3 * a3)) return e;
+        // the step graphs of this call exist before any copy is queued
+        if (int e = precapture(nturns, 0)) return e;
         // inputs: a plain copy into pinned memory, one async copy each, the
         // FP32 rounding and the scatter by id on the device
         const double *ins[2] = {pin, vin};

@@ -18,9 +18,11 @@
 //    the last call: each call writes every partial it later reads, so nothing
 //    needs clearing, but calls whose kernels overlap on the GPU (different
 //    streams, no ordering between them) race on the array;
-//  * the first call on a device looks up the array's device address with
-//    cudaGetSymbolAddress (set-up, once per device, with that device current);
-//    make that first call before any stream capture begins.
+//  * the first call for a state on a device looks up the array's device
+//    address with cudaGetSymbolAddress (set-up, once per device), with the
+//    state's own device made current for the call (the caller's current
+//    device is restored afterwards); make that first call before any stream
+//    capture begins.
 #include <mutex>
 
 #include "engine.hpp"
@@ -39,11 +41,10 @@ static __device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxBlocks + 1]
 std::mutex g_noalloc_mu;
 double *g_noalloc_ptr[kMaxDevices] = {nullptr};
 
-// device address of the scratch array on the current device (set-up on the
-// first call per device; the host-side symbol is not a device address)
-int noalloc_scratch(double **out) {
-    int dev = 0;
-    MDX_CUDA_TRY(cudaGetDevice(&dev));
+// device address of the scratch array on device `dev`, which must be the
+// current device (set-up on the first call per device; the host-side symbol
+// is not a device address)
+int noalloc_scratch(int dev, double **out) {
     if (dev < 0 || dev >= kMaxDevices) {
         set_error(MDX_ERR_UNSUPPORTED, "device %d beyond the %d devices this entry point tracks", dev, kMaxDevices);
         return MDX_ERR_UNSUPPORTED;
@@ -97,6 +98,23 @@ __global__ void k_mv2_noalloc_final(int nblocks, double *__restrict__ scratch) {
     }
 }
 
+// the two kernels and the copy-out on the state's stream; `dev` is current
+int kinetic_noalloc_on_device(State &s, int n, int nblocks, int dev, double *sum_mv2) {
+    double *scratch = nullptr;
+    if (int e = noalloc_scratch(dev, &scratch)) return e;
+    if (nblocks > 0) {
+        k_mv2_noalloc<<<nblocks, kNoAllocThreads, 0, s.stream>>>(n, s.gpd.vs.p, scratch);
+        MDX_LAUNCHED();
+    }
+    k_mv2_noalloc_final<<<1, kNoAllocThreads, 0, s.stream>>>(nblocks, scratch);
+    MDX_LAUNCHED();
+    MDX_CUDA_TRY(cudaGetLastError());
+    MDX_CUDA_TRY(cudaMemcpyAsync(sum_mv2, scratch + kNoAllocMaxBlocks, sizeof(double), cudaMemcpyDeviceToHost,
+                                 s.stream));
+    MDX_CUDA_TRY(cudaStreamSynchronize(s.stream));
+    return 0;
+}
+
 }  // namespace
 
 }  // namespace mdx
@@ -120,17 +138,18 @@ extern "C" int mdx_kinetic_noalloc(mdx_state *st, double *sum_mv2) {
                   kNoAllocMaxBlocks * kNoAllocThreads);
         return MDX_ERR_ARG;
     }
-    double *scratch = nullptr;
-    if (int e = noalloc_scratch(&scratch)) return e;
-    if (nblocks > 0) {
-        k_mv2_noalloc<<<nblocks, kNoAllocThreads, 0, s.stream>>>(n, s.gpd.vs.p, scratch);
-        MDX_LAUNCHED();
+    // the state's device is current for the look-up and the launches; the
+    // caller's current device is put back before returning
+    int prev = 0;
+    MDX_CUDA_TRY(cudaGetDevice(&prev));
+    if (s.device >= 0 && s.device != prev) MDX_CUDA_TRY(cudaSetDevice(s.device));
+    const int rc = kinetic_noalloc_on_device(s, n, nblocks, s.device >= 0 ? s.device : prev, sum_mv2);
+    if (s.device >= 0 && s.device != prev) {
+        const cudaError_t back = cudaSetDevice(prev);
+        if (rc == 0 && back != cudaSuccess) {
+            set_error(MDX_ERR_CUDA, "cudaSetDevice(%d): %s", prev, cudaGetErrorString(back));
+            return MDX_ERR_CUDA;
+        }
     }
-    k_mv2_noalloc_final<<<1, kNoAllocThreads, 0, s.stream>>>(nblocks, scratch);
-    MDX_LAUNCHED();
-    MDX_CUDA_TRY(cudaGetLastError());
-    MDX_CUDA_TRY(cudaMemcpyAsync(sum_mv2, scratch + kNoAllocMaxBlocks, sizeof(double), cudaMemcpyDeviceToHost,
-                                 s.stream));
-    MDX_CUDA_TRY(cudaStreamSynchronize(s.stream));
-    return 0;
+    return rc;
 }

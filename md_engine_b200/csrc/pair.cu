@@ -46,6 +46,13 @@ struct PairArgs {
     float *__restrict__ virials;
     float *__restrict__ energy;  // per-atom (energy kernel)
     uint32_t lj_types;           // bit ti: type ti has a pair with eps != 0
+    // GridGPU's own list layout instead of this library's (null: this
+    // library's): per-block padded rows located by cumulSumMaxPerBlock for
+    // ref_ntpb threads per block, counts as uint16 (GridGPU.cu:777-821,
+    // cutils_func.h:23-45)
+    const uint32_t *__restrict__ cum;
+    const uint16_t *__restrict__ counts16;
+    int ref_ntpb;
 };
 
 // erfc(x) for x >= 0 by Abramowitz & Stegun, Handbook of Mathematical
@@ -213,9 +220,20 @@ __global__ void __launch_bounds__(kPairBlock, T >= 32 ? 24 : 1) k_pair(const Pai
         xi = A.xs[i];
         ti = type_of(xi);
         qi = EW ? A.qs[i] : 0.f;
-        cnt = (int)A.counts[i];
-        cnt = cnt < A.cap ? cnt : A.cap;
-        row = A.nlist + (size_t)(i / G) * A.cap * G + a * T + t;
+        if (A.cum) {
+            // GridGPU layout: block b of ref_ntpb threads holds ref_ntpb / T
+            // atoms; its warps' rows start at (ref_ntpb / 32) * cum[b] and are
+            // cum[b+1] - cum[b] entries apart; entry k sits 32 * (k / T) on
+            const int per_block = A.ref_ntpb / T;
+            const int blk = i / per_block, nth = i % per_block;
+            const uint32_t c0 = A.cum[blk], mem = A.cum[blk + 1] - c0;
+            row = A.nlist + (size_t)(A.ref_ntpb / 32) * c0 + (size_t)mem * (nth / G) + (nth % G) * T + t;
+            cnt = (int)A.counts16[i];
+        } else {
+            cnt = (int)A.counts[i];
+            cnt = cnt < A.cap ? cnt : A.cap;
+            row = A.nlist + (size_t)(i / G) * A.cap * G + a * T + t;
+        }
     }
     if (LJ && EW) {
         const bool lj_row = valid && ti < 32 && ((A.lj_types >> ti) & 1u);
@@ -336,6 +354,9 @@ PairArgs make_args(State &s, FixPair &f) {
     }
     A.virials = s.gpd.virials.p;
     A.energy = nullptr;
+    A.cum = nullptr;
+    A.counts16 = nullptr;
+    A.ref_ntpb = 0;
     // types with an LJ partner (eps != 0); every type when unknown
     A.lj_types = 0xffffffffu;
     const int nt = A.ntypes;
@@ -356,22 +377,17 @@ int pair_launch(State &s, FixPair &f, int virialMode, bool accumulate) {
     return launch_any(A, s.grid.team, f.lj_kind, f.chargeFix != nullptr, vir, false, accumulate, s.stream);
 }
 
+// compute_energy_iso (PairEvaluateIso.h:212-358): per-site energies into the
+// state's energy buffer, summed on the device in FP64 in a fixed order
 int pair_energy(State &s, FixPair &f, double *out) {
     PairArgs A = make_args(s, f);
-    DBuf<float> e;
-    if (int r = e.alloc(A.n)) return r;
-    A.energy = e.p;
+    if (s.e_site.n < (size_t)A.n || !s.e_sum.p) {
+        set_error(MDX_ERR_STATE, "energy buffers not sized (prepare the state)");
+        return MDX_ERR_STATE;
+    }
+    A.energy = s.e_site.p;
     if (int r = launch_any(A, s.grid.team, f.lj_kind, f.chargeFix != nullptr, false, true, false, s.stream)) return r;
-    // widen to double for the FP64 reduction
-    DBuf<double> ed;
-    if (int r = ed.alloc(A.n)) return r;
-    std::vector<float> h(A.n);
-    MDX_CUDA_TRY(cudaMemcpyAsync(h.data(), e.p, A.n * sizeof(float), cudaMemcpyDeviceToHost, s.stream));
-    MDX_CUDA_TRY(cudaStreamSynchronize(s.stream));
-    double sum = 0.0;
-    for (int i = 0; i < A.n; i++) sum += (double)h[i];
-    *out = sum;
-    return 0;
+    return float_sum(s, s.e_site.p, A.n, out);
 }
 
 // batched replicas: one launch, blockIdx.y = replica; tables built at prepare
@@ -422,10 +438,52 @@ int pair_force_raw(int n, const float4 *xs, float4 *fs, const float *qs, const u
     A.virials = virials;
     A.energy = nullptr;
     A.lj_types = 0xffffffffu;  // parameters live on the device here: no skipping
+    A.cum = nullptr;
+    A.counts16 = nullptr;
+    A.ref_ntpb = 0;
     bool ew = qrc > 0.f;
     if (lj_kind == 0 && !ew) return 0;
     int r = launch_any(A, team, lj_kind, ew, virials != nullptr, false, accumulate, stream);
     if (r) return r;
+    MDX_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+// EvaluatorWrapperImplement::compute (EvaluatorWrapper.h:49-109) on GridGPU's
+// list as it hands it over: neighborCounts (uint16), neighborlist, the
+// per-block prefix cumulSumMaxPerBlock for nThreadPerBlock threads per block,
+// nThreadPerAtom lanes per atom.  Forces (and, when virials is given,
+// 0.5 F (x) dr per atom) are added, as the reference kernel adds them.
+int pair_force_gridgpu(int n, const float4 *xs, float4 *fs, const uint16_t *counts, const uint32_t *nlist,
+                       const uint32_t *cum, int ntpb, int ntpa, const float *params, int ntypes, const Box &box,
+                       const float coef[3], int lj_kind, const float *qs, float qcut, float alpha, float qqr,
+                       float *virials, cudaStream_t stream) {
+    PairArgs A{};
+    A.n = n;
+    A.xs = xs;
+    A.fs = fs;
+    A.qs = qs;
+    A.counts = nullptr;
+    A.nlist = nlist;
+    A.cap = 1 << 16;  // uint16 counts: never clipped
+    A.params = params;
+    A.ntypes = ntypes;
+    A.box = box;
+    A.coef1 = coef[0];
+    A.coef2 = coef[1];
+    A.coef3 = coef[2];
+    A.qrc2 = qcut > 0.f ? qcut * qcut : 0.f;
+    A.alpha = alpha;
+    A.qqr = qqr;
+    A.virials = virials;
+    A.energy = nullptr;
+    A.lj_types = 0xffffffffu;
+    A.cum = cum;
+    A.counts16 = counts;
+    A.ref_ntpb = ntpb;
+    const bool ew = qcut > 0.f;
+    if (lj_kind == 0 && !ew) return 0;
+    if (int r = launch_any(A, ntpa, lj_kind, ew, virials != nullptr, false, true, stream)) return r;
     MDX_CUDA_TRY(cudaGetLastError());
     return 0;
 }

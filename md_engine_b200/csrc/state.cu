@@ -103,6 +103,7 @@ FixNoseHoover *State::nhFix() {
 // vs.w (INVMASSLESS for massless sites), group tag bits in fs.w
 int State::upload() {
     const int n = (int)atoms.size();
+    if (device < 0) MDX_CUDA_TRY(cudaGetDevice(&device));
     if (!stream) {
         MDX_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         own_stream = true;
@@ -131,6 +132,8 @@ int State::upload() {
     if (int e = d.virials.alloc(6 * (size_t)n)) return e;
     if (int e = red_counter.alloc(1)) return e;
     if (int e = red_out.alloc(4)) return e;
+    if (int e = e_site.alloc(n)) return e;
+    if (int e = e_sum.alloc(1)) return e;
     MDX_CUDA_TRY(cudaMemset(red_counter.p, 0, sizeof(unsigned int)));
     MDX_CUDA_TRY(cudaMemset(d.virials.p, 0, 6 * (size_t)n * sizeof(float)));
     std::vector<float4> xs(n), vs(n), fs(n);

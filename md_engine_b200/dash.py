@@ -444,6 +444,16 @@ class FixRigid(_Fix):
     def distributeMSite(self):
         check(lib().mdx_rigid_distribute_msite(self.state._h, self._h))
 
+    def validateConstraints(self):
+        """FixRigid::validateConstraints: the number of molecules whose side
+        lengths or bond velocities are off by more than 1e-3 (0 = all fine);
+        the C call returns MDX_ERR_NUMERIC when it is not 0"""
+        n = c_u32()
+        rc = lib().mdx_rigid_validate(self.state._h, self._h, ctypes.byref(n))
+        if rc not in (0, 6):
+            check(rc)
+        return n.value
+
 
 class FixNoseHoover(_Fix):
     """FixNoseHoover(state, handle, groupHandle) (src/Fixes/FixNoseHoover.cu:97-130)"""
