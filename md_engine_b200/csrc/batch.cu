@@ -159,7 +159,10 @@ int Batch::prepare() {
         s->nThreadPerAtom = team;
     }
     for (State *s : reps) {
-        if (s->prepared) continue;
+        if (s->prepared && !s->mf.on) continue;
+        // the batched kernels take the per-site form of every replica
+        s->pairForm = 1;
+        s->prepared = false;
         if (int e = s->prepare()) return e;
     }
     MDX_CUDA_TRY(cudaDeviceSynchronize());

@@ -119,7 +119,11 @@ int mdx_state_set_int(mdx_state *st, const char *key, int64_t v) {
     else if (k == "nThreadPerBlock") s.nThreadPerBlock = (int)v;
     else if (k == "gridStencil") s.gridStencil = (int)v;
     else if (k == "gridHomeGroup") s.gridHomeGroup = (int)v;
-    else if (k == "turn") s.turn = v;
+    else if (k == "nThreadPerMolecule") s.nThreadPerMolecule = (int)v;
+    else if (k == "pairForm") {
+        ARG_CHECK(v >= 0 && v <= 2, "pairForm must be 0 (automatic), 1 (per-site) or 2 (molecule)");
+        s.pairForm = (int)v;
+    } else if (k == "turn") s.turn = v;
     else {
         set_error(MDX_ERR_ARG, "unknown int key '%s'", key);
         return MDX_ERR_ARG;
@@ -140,6 +144,9 @@ int mdx_state_get_int(mdx_state *st, const char *key, int64_t *v) {
     else if (k == "cellsPerSide") *v = s.grid.ns.x;
     else if (k == "gridStencil") *v = s.grid.m;
     else if (k == "gridHomeGroup") *v = s.grid.home_group;
+    else if (k == "pairForm") *v = s.prepared ? (s.mf.on ? 2 : 1) : s.pairForm;
+    else if (k == "molListCapacity") *v = s.mf.cap;
+    else if (k == "nThreadPerMolecule") *v = s.prepared && s.mf.on ? s.mf.team : s.nThreadPerMolecule;
     else {
         set_error(MDX_ERR_ARG, "unknown int key '%s'", key);
         return MDX_ERR_ARG;
@@ -472,6 +479,11 @@ int mdx_nlist_get(mdx_state *st, int max_per_atom, int *counts, int *nbr, int *t
     ARG_CHECK(st && counts && nbr && max_per_atom > 0, "null argument");
     State &s = *st->s;
     if (int e = need_prepared(s)) return e;
+    // the molecule form keeps no per-site list: build it now, on the current
+    // positions, into the sort's alternate buffers (the step is untouched)
+    if (s.mf.on) GUARD(if (int e = nlist_build_atoms_view(s)) return e;)
+    MDX_CUDA_TRY(cudaStreamSynchronize(s.stream));
+    if (int e = s.checkStatus()) return e;
     const int n = s.gpd.n;
     GridGPU &g = s.grid;
     const int G = 32 / g.team;
@@ -482,7 +494,9 @@ int mdx_nlist_get(mdx_state *st, int max_per_atom, int *counts, int *nbr, int *t
     if (g.partition) MDX_CUDA_TRY(cudaMemcpy(cint.data(), g.counts_int.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
     else cint = cnt;
     MDX_CUDA_TRY(cudaMemcpy(list.data(), g.nlist.p, list.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-    MDX_CUDA_TRY(cudaMemcpy(ids.data(), s.gpd.ids.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    // list indices refer to the sorted copy of the last per-site build, whose
+    // ids are in ids_alt (equal to ids after a build of the per-site form)
+    MDX_CUDA_TRY(cudaMemcpy(ids.data(), s.gpd.ids_alt.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
     for (int i = 0; i < n; i++) {
         const uint32_t id = ids[i];
         const int c = (int)std::min<uint32_t>(cnt[i], (uint32_t)g.cap);

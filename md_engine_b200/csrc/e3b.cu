@@ -242,6 +242,57 @@ __global__ void k_e3b_list(const E3BArgs a0, const E3BArgs *__restrict__ tab, in
     }
 }
 
+// The molecule form's E3B list, cut from the molecule-pair list of the same
+// rebuild: slot k of molecule m (site 0 at 4k after the sort), every listed
+// slot whose site-0 distance is below the E3B list radius, written as its
+// molecule index (mol_of_slot).  The molecule-pair list holds every site-0
+// pair within its larger radius, so the E3B set is the per-site path's.
+template <int T>
+__global__ void k_e3b_list_mf(const E3BArgs A, const uint32_t *__restrict__ pcounts,
+                              const uint32_t *__restrict__ plist, int pcap, int pteam,
+                              const int *__restrict__ mol_of_slot, const float4 *__restrict__ xs2) {
+    pdl_wait();
+    if (!A.st->rebuild) return;
+    constexpr int G = 32 / T;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int a = lane / T, t = lane % T;
+    const int m = warp * G + a;
+    if (m >= A.nmol) return;
+    const unsigned team_mask = (T == 32) ? 0xffffffffu : (((1u << T) - 1u) << (a * T));
+    const int k = A.mol_idx[m].x >> 2;
+    const float3 po = f3(xs2[4 * k]);
+    int cnt = (int)pcounts[k];
+    cnt = cnt < pcap ? cnt : pcap;
+    const int PG = 32 / pteam;
+    const uint32_t *prow = plist + (size_t)(k / PG) * pcap * PG + (k % PG) * pteam;
+    uint32_t *mrow = A.mlist + (size_t)(m / G) * A.mcap * G + a * T;
+    int mc = 0;
+    for (int k0 = 0; k0 < cnt; k0 += T) {
+        const int e = k0 + t;
+        bool hit = false;
+        int mj = -1;
+        if (e < cnt) {
+            const int j = (int)prow[(size_t)(e / pteam) * 32 + (e % pteam)];
+            const float3 d = min_image(A.box, po - f3(xs2[4 * j]));
+            hit = dot3(d, d) < A.cut2;
+            mj = mol_of_slot[j];
+        }
+        const unsigned b = __ballot_sync(team_mask, hit);
+        if (hit) {
+            const unsigned mine = (T == 32) ? b : (b >> (a * T));
+            const int pos = mc + __popc(mine & ((1u << t) - 1u));
+            if (pos < A.mcap) mrow[(size_t)(pos / T) * 32 + (pos % T)] = (uint32_t)mj;
+        }
+        mc += __popc(b);
+    }
+    if (t == 0) {
+        A.mcounts[m] = (uint32_t)mc;
+        if (mc > A.mcap) atomicOr(&A.st->bits, kStatusMolOverflow);
+        atomicMax(&A.st->max_mol_neighbors, (uint32_t)mc);
+    }
+}
+
 // pass 1: e3bTotals of molecule i (ThreeBodyE3B.h:170-211 summed from i's own
 // full list) and the O-O two-body force (EvaluatorE3B::twoBodyForce, :67-78)
 // STORE: write into a per-step side buffer instead of adding to the forces
@@ -643,6 +694,18 @@ int e3b_build_list(State &s, FixE3B &f, bool conditional, cudaStream_t st) {
     A.xs = s.gpd.xs_alt.p;
     MDX_CUDA_TRY(launch_pdl(k_e3b_list<kMolTeam>, e3b_blocks(nmol), dim3(256), 0, st ? st : s.stream, A,
                             (const E3BArgs *)nullptr, conditional ? 1 : 0));
+    return 0;
+}
+
+// the molecule form: after the sort by molecule, from the molecule-pair list
+int e3b_build_list_mf(State &s, FixE3B &f, cudaStream_t st) {
+    const int nmol = (int)f.mol_ids.size();
+    if (nmol == 0 || !f.prepared) return 0;
+    E3BArgs A = e3b_args(s, f, nullptr);
+    const MolForm &mf = s.mf;
+    MDX_CUDA_TRY(launch_pdl(k_e3b_list_mf<kMolTeam>, e3b_blocks(nmol), dim3(256), 0, st ? st : s.stream, A,
+                            (const uint32_t *)mf.counts.p, (const uint32_t *)mf.list.p, mf.cap, mf.team,
+                            (const int *)mf.perm.p, (const float4 *)s.gpd.xs_alt.p));
     return 0;
 }
 

@@ -184,6 +184,40 @@ struct GridGPU {
     int max_excl = 0;
     bool have_excl = false;
     bool built = false;
+    // host copies of the exclusion lists by id (start, id | depth << 30)
+    std::vector<int> h_excl_start;
+    std::vector<uint32_t> h_excl_ids;
+};
+
+// ---------------------------------------------------------------- MolForm
+// Molecule form of the step for all-rigid four-site water: every atom in a
+// FixRigid molecule, every molecule alike in site types, charges and
+// exclusions, no exclusion between molecules.  The per-atom streams then hold
+// molecule slot k's sites (O, H1, H2, M) at 4k .. 4k+3, slots ordered by the
+// cell of their site 0 at each rebuild, and the pair kernel walks a
+// molecule-pair list (site 0 within cut = pair cutoff + padding + 2 dmax,
+// dmax bounding every site's distance from site 0) evaluating every site
+// pair of a listed molecule pair from one 64-byte gather.  The pair set is
+// unchanged: every site pair within the pair cutoff now is within the list
+// radius of site 0 at the last build while no atom has moved more than half
+// the padding.  The per-site list of the reference stays available (built on
+// demand into the sort's alternate buffers for Grid.getNeighborList).
+struct MolForm {
+    bool on = false;
+    int nmol = 0;
+    int team = 32;      // lanes per molecule in the pair kernel (list layout)
+    int cap = 0;        // entries per molecule row
+    int3 ns{0, 0, 0};   // cells per dimension of the molecule grid
+    int m = 2;          // stencil half width (cells >= cut / m)
+    float cut = 0.f;    // list radius on site 0
+    float far = 0.f;    // pair cutoff + 2 dmax: no site pair interacts beyond it
+    float dmax = 0.f;
+    int type[4] = {0, 0, 0, 0};
+    float q[4] = {0.f, 0.f, 0.f, 0.f};
+    int depth[16] = {0};  // exclusion depth of site pair (a, b) within a molecule
+    DBuf<uint32_t> cell_start, cell_count, cell_fill;
+    DBuf<int> cell_of, perm_tmp, perm;  // by molecule; perm[slot] = FixRigid molecule index
+    DBuf<uint32_t> counts, list;       // molecule-pair list (slots), team layout
 };
 
 // ---------------------------------------------------------------- Fixes
@@ -387,6 +421,11 @@ class State {
     int64_t turn = 0;
     int periodicInterval = 50;
     int nThreadPerAtom = 0, nThreadPerBlock = 256;  // 0 = automatic team size
+    // 0 automatic (molecule form when the system allows it), 1 per-site
+    // (atom) form, 2 molecule form (an error at prepare when not allowed)
+    int pairForm = 0;
+    int nThreadPerMolecule = 0;  // molecule form: lanes per molecule (8, 16, 32; 0 = automatic)
+    MolForm mf;
     // list build tunables, 0 = automatic: cells of >= cut/gridStencil (1..4),
     // home atoms tested at once per warp (2 or 4)
     int gridStencil = 0, gridHomeGroup = 0;
@@ -509,9 +548,12 @@ int nlist_rebuild(State &s, bool force, bool conditional, cudaStream_t bstream =
 int nlist_init(State &s);
 int nlist_exclusions(State &s);
 int nlist_set_interactions(State &s);
+int molform_init(State &s);
+int nlist_build_atoms_view(State &s);
 // pair (pair.cu)
 int pair_launch(State &s, FixPair &f, int virialMode, bool accumulate);
 int pair_energy(State &s, FixPair &f, double *out);
+int pair_mol_launch(State &s, FixPair &f, int virialMode, bool accumulate, float *energy, cudaStream_t st);
 int pair_force_raw(int n, const float4 *xs, float4 *fs, const float *qs, const uint32_t *counts,
                    const uint32_t *nlist, int team, int cap, const float *params, int ntypes, const Box &box,
                    const float coef[3], int lj_kind, float qrc, float alpha, float qqr, float *virials,
@@ -522,6 +564,7 @@ int pair_force_gridgpu(int n, const float4 *xs, float4 *fs, const uint16_t *coun
                        float *virials, cudaStream_t stream);
 // e3b (e3b.cu)
 int e3b_build_list(State &s, FixE3B &f, bool conditional, cudaStream_t st = nullptr);
+int e3b_build_list_mf(State &s, FixE3B &f, cudaStream_t st);
 int e3b_forces(State &s, FixE3B &f);
 int e3b_forces_to(State &s, FixE3B &f, float4 *out, bool side, cudaStream_t stream);
 int e3b_energy(State &s, FixE3B &f, double out[2]);

@@ -134,7 +134,8 @@ class IntegratorVerlet {
     bool build_pending = false;
     int enqueue(int nsteps, bool with_group) {
         if (with_group) {
-            const bool overlap = mode == 0 && s->grid.cap != 0;
+            // (the per-site form's first build sizes its list with a host sync)
+            const bool overlap = mode == 0 && (s->grid.cap != 0 || s->mf.on);
             if (int e = nlist_rebuild(*s, false, true, overlap ? s->side[2] : nullptr)) return e;
             build_pending = overlap;
         }

@@ -69,6 +69,10 @@ struct GridArgs {
     CellGrid g;
     int n, ncell, interval;
     float skin2q;
+    // 1: a list build into the alternate buffers only (the molecule form's
+    // per-site list for Grid.getNeighborList): idToIdx, the primary streams
+    // and the build counter are left alone
+    int view;
 };
 #define MDX_GRID_ARGS \
     pdl_wait();       \
@@ -242,7 +246,7 @@ __global__ void k_gather(const GridArgs a0, const GridArgs *__restrict__ tab) {
     A.qs2[d] = A.qs[s];
     uint32_t id = A.ids[s];
     A.ids2[d] = id;
-    A.idToIdx[id] = d;
+    if (!A.view) A.idToIdx[id] = d;
 }
 
 // the sorted streams back into the primary buffers (the captured graph keeps
@@ -633,8 +637,202 @@ __global__ void k_finish(const GridArgs a0, const GridArgs *__restrict__ tab) {
     for (int c = threadIdx.x; c < A.ncell; c += blockDim.x) A.cell_count[c] = 0u;
     __syncthreads();
     if (threadIdx.x == 0) {
-        st->n_builds += 1;
+        if (!A.view) st->n_builds += 1;
         st->rebuild = 0u;
+    }
+}
+
+// ---- molecule form (all-rigid four-site water) ---------------------------
+// The sort unit is the molecule: its cell is the cell of its site 0, slots
+// are ordered by (cell, molecule index), and slot d's sites land at 4d .. 4d+3
+// of every per-atom stream.
+struct MolGridArgs {
+    float4 *xs, *vs, *fs;
+    float *qs;
+    uint32_t *ids;
+    float4 *xs2, *vs2, *fs2;
+    float *qs2;
+    uint32_t *ids2;
+    float4 *xs_last;
+    int *idToIdx;
+    int4 *mol_idx;      // FixRigid's molecule -> atom indices (rewritten by the sort)
+    int4 *mol_idx_e3b;  // FixE3B's copy of the same molecules (may be null)
+    int *cell_of;
+    uint32_t *cell_count, *cell_start, *cell_fill;
+    int *perm_tmp, *perm;
+    uint32_t *counts, *list;
+    int cap, team;
+    DeviceStatus *st;
+    Box box;
+    CellGrid g;
+    int nmol, ncell, m;
+    float cut2;
+};
+
+__device__ __forceinline__ float4 wrap_pos(const Box &box, float4 p, bool &moved) {
+    // periodicWrap (GridGPU.cu:138-161), per site
+    const float ix = floorf((p.x - box.lo.x) / box.L.x);
+    const float iy = floorf((p.y - box.lo.y) / box.L.y);
+    const float iz = floorf((p.z - box.lo.z) / box.L.z);
+    moved = ix != 0.f || iy != 0.f || iz != 0.f;
+    if (moved) {
+        p.x = p.x - box.L.x * ix;
+        p.y = p.y - box.L.y * iy;
+        p.z = p.z - box.L.z * iz;
+    }
+    return p;
+}
+
+// every site wrapped into the box; the molecule binned by its site 0
+__global__ void k_mf_wrap_bin(const MolGridArgs M) {
+    pdl_wait();
+    if (!M.st->rebuild) return;
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M.nmol) return;
+    const int4 ix = M.mol_idx[m];
+    const int at[4] = {ix.x, ix.y, ix.z, ix.w};
+    float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        bool moved;
+        const float4 p = wrap_pos(M.box, M.xs[at[k]], moved);
+        if (moved) M.xs[at[k]] = p;
+        if (k == 0) p0 = p;
+    }
+    const int c = cell_of_pos(M.g, f3(p0));
+    M.cell_of[m] = c;
+    atomicAdd(M.cell_count + c, 1u);
+}
+
+__global__ void k_mf_scatter(const MolGridArgs M) {
+    pdl_wait();
+    if (!M.st->rebuild) return;
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M.nmol) return;
+    const int c = M.cell_of[m];
+    const uint32_t slot = atomicAdd(M.cell_fill + c, 1u);
+    M.perm_tmp[M.cell_start[c] + slot] = m;
+}
+
+// deterministic order inside each cell: by molecule index; one warp per cell
+__global__ void k_mf_rank(const MolGridArgs M) {
+    pdl_wait();
+    if (!M.st->rebuild) return;
+    const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (c >= M.ncell) return;
+    const uint32_t s = M.cell_start[c], e = M.cell_start[c + 1];
+    for (uint32_t p = s + lane; p < e; p += 32) {
+        const int a = M.perm_tmp[p];
+        uint32_t r = 0;
+        for (uint32_t q = s; q < e; q++) r += M.perm_tmp[q] < a;
+        M.perm[s + r] = a;
+    }
+}
+
+// slot d <- molecule perm[d]: its four sites into 4d .. 4d+3 of the
+// alternate streams, idToIdx and the molecule maps rewritten
+__global__ void k_mf_gather(const MolGridArgs M) {
+    pdl_wait();
+    if (!M.st->rebuild) return;
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= M.nmol) return;
+    const int m = M.perm[d];
+    const int4 ix = M.mol_idx[m];
+    const int at[4] = {ix.x, ix.y, ix.z, ix.w};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int s = at[k], t = 4 * d + k;
+        M.xs2[t] = M.xs[s];
+        M.vs2[t] = M.vs[s];
+        M.fs2[t] = M.fs[s];
+        M.qs2[t] = M.qs[s];
+        const uint32_t id = M.ids[s];
+        M.ids2[t] = id;
+        M.idToIdx[id] = t;
+    }
+    const int4 nx = make_int4(4 * d, 4 * d + 1, 4 * d + 2, 4 * d + 3);
+    M.mol_idx[m] = nx;
+    if (M.mol_idx_e3b) M.mol_idx_e3b[m] = nx;
+}
+
+__global__ void k_mf_copyback(const MolGridArgs M) {
+    pdl_wait();
+    if (!M.st->rebuild) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 4 * M.nmol) return;
+    const float4 p = M.xs2[i];
+    M.xs[i] = p;
+    M.xs_last[i] = p;
+    M.vs[i] = M.vs2[i];
+    M.fs[i] = M.fs2[i];
+    M.qs[i] = M.qs2[i];
+    M.ids[i] = M.ids2[i];
+}
+
+// the molecule-pair list: one warp per slot walks the (2m+1)^2 rows of its
+// stencil (each row one or two contiguous runs of slots: the grid has at
+// least 2m+1 cells per side, so no cell is seen twice) 32 candidates at a
+// time; a candidate is kept when the minimum-image distance of the site-0
+// positions is below the list radius.  Entries are slots, written in
+// candidate order (deterministic) into the team layout: slot k's e-th entry
+// at (k/G) cap G + (e/T) 32 + (k%G) T + e%T, G = 32/T.
+__global__ void __launch_bounds__(128) k_mf_build(const MolGridArgs M) {
+    pdl_wait();
+    if (!M.st->rebuild) return;
+    const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (k >= M.nmol) return;
+    const CellGrid &g = M.g;
+    const float3 p = f3(M.xs2[4 * k]);
+    const int c = cell_of_pos(g, p);
+    const int cz = c % g.ns.z, cy = (c / g.ns.z) % g.ns.y, cx = c / (g.ns.z * g.ns.y);
+    const int mm = M.m, side = 2 * mm + 1;
+    const int T = M.team, G = 32 / T;
+    uint32_t *const row = M.list + (size_t)(k / G) * M.cap * G + (k % G) * T;
+    const uint32_t cap = (uint32_t)M.cap;
+    const uint32_t lt = (1u << lane) - 1u;
+    uint32_t cnt = 0u;
+    for (int r = 0; r < side * side; r++) {
+        int kx = cx - mm + r / side, ky = cy - mm + r % side;
+        kx = kx < 0 ? kx + g.ns.x : (kx >= g.ns.x ? kx - g.ns.x : kx);
+        ky = ky < 0 ? ky + g.ns.y : (ky >= g.ns.y ? ky - g.ns.y : ky);
+        const int rowbase = (kx * g.ns.y + ky) * g.ns.z;
+        const int zlo = cz - mm, zhi = cz + mm;
+        // up to two runs: [zlo, zhi] split where it wraps
+#pragma unroll
+        for (int part = 0; part < 2; part++) {
+            int za, zb;
+            if (zlo < 0) {
+                za = part == 0 ? zlo + g.ns.z : 0;
+                zb = part == 0 ? g.ns.z - 1 : zhi;
+            } else if (zhi >= g.ns.z) {
+                za = part == 0 ? zlo : 0;
+                zb = part == 0 ? g.ns.z - 1 : zhi - g.ns.z;
+            } else {
+                if (part == 1) break;
+                za = zlo;
+                zb = zhi;
+            }
+            const int b = (int)M.cell_start[rowbase + za], e = (int)M.cell_start[rowbase + zb + 1];
+            for (int c0 = b; c0 < e; c0 += 32) {
+                const int j = c0 + lane;
+                bool hit = false;
+                if (j < e && j != k) {
+                    const float3 d = min_image(M.box, f3(M.xs2[4 * j]) - p);
+                    hit = dot3(d, d) < M.cut2;
+                }
+                const uint32_t bal = __ballot_sync(0xffffffffu, hit);
+                const uint32_t pos = cnt + __popc(bal & lt);
+                if (hit && pos < cap) row[(pos / T) * 32u + pos % T] = (uint32_t)j;
+                cnt += __popc(bal);
+            }
+        }
+    }
+    if (lane == 0) {
+        M.counts[k] = cnt;
+        if (cnt > cap) atomicOr(&M.st->bits, kStatusNlistOverflow);
+        atomicMax(&M.st->max_mol_neighbors, cnt);
     }
 }
 
@@ -676,6 +874,65 @@ GridArgs grid_args(State &s) {
     A.ncell = gr.ns.x * gr.ns.y * gr.ns.z;
     A.interval = s.periodicInterval;
     A.skin2q = (float)(s.padding * s.padding) * 0.25f;
+    A.view = 0;
+    return A;
+}
+
+CellGrid mol_grid(const State &s) {
+    CellGrid g;
+    g.lo = s.box.lo;
+    g.ns = s.mf.ns;
+    g.inv_ds = make_float3((float)(s.mf.ns.x / s.box.Ld.x), (float)(s.mf.ns.y / s.box.Ld.y),
+                           (float)(s.mf.ns.z / s.box.Ld.z));
+    return g;
+}
+
+MolGridArgs mol_grid_args(State &s) {
+    MolForm &mf = s.mf;
+    GPUData &d = s.gpd;
+    MolGridArgs M{};
+    M.xs = d.xs.p;
+    M.vs = d.vs.p;
+    M.fs = d.fs.p;
+    M.qs = d.qs.p;
+    M.ids = d.ids.p;
+    M.xs2 = d.xs_alt.p;
+    M.vs2 = d.vs_alt.p;
+    M.fs2 = d.fs_alt.p;
+    M.qs2 = d.qs_alt.p;
+    M.ids2 = d.ids_alt.p;
+    M.xs_last = d.xs_last_build.p;
+    M.idToIdx = d.idToIdx.p;
+    M.mol_idx = s.rigidFix()->d_mol_idx.p;
+    FixE3B *e3 = s.e3bFix();
+    M.mol_idx_e3b = (e3 && e3->side_ok) ? e3->d_mol_idx.p : nullptr;
+    M.cell_of = mf.cell_of.p;
+    M.cell_count = mf.cell_count.p;
+    M.cell_start = mf.cell_start.p;
+    M.cell_fill = mf.cell_fill.p;
+    M.perm_tmp = mf.perm_tmp.p;
+    M.perm = mf.perm.p;
+    M.counts = mf.counts.p;
+    M.list = mf.list.p;
+    M.cap = mf.cap;
+    M.team = mf.team;
+    M.st = s.d_status.p;
+    M.box = s.box;
+    M.g = mol_grid(s);
+    M.nmol = mf.nmol;
+    M.ncell = mf.ns.x * mf.ns.y * mf.ns.z;
+    M.m = mf.m;
+    M.cut2 = mf.cut * mf.cut;
+    return M;
+}
+
+// the scan / finish kernels over the molecule grid's cell arrays
+GridArgs mol_scan_args(State &s) {
+    GridArgs A = grid_args(s);
+    A.cell_count = s.mf.cell_count.p;
+    A.cell_start = s.mf.cell_start.p;
+    A.cell_fill = s.mf.cell_fill.p;
+    A.ncell = s.mf.ns.x * s.mf.ns.y * s.mf.ns.z;
     return A;
 }
 
@@ -778,6 +1035,8 @@ int nlist_exclusions(State &s) {
     for (Fix *f : s.fixes) f->getBonds(bonds);
     GridGPU &gr = s.grid;
     gr.have_excl = !bonds.empty();
+    gr.h_excl_start.assign(s.atoms.size() + 1, 0);
+    gr.h_excl_ids.clear();
     if (!gr.have_excl) return 0;
     const int nid = (int)s.atoms.size();
     std::vector<std::vector<int>> adj(nid);
@@ -829,6 +1088,8 @@ int nlist_exclusions(State &s) {
     if (int e = gr.excl_far.alloc(nid)) return e;
     MDX_CUDA_TRY(cudaMemcpy(gr.excl_win.p, win.data(), nid * sizeof(ulonglong2), cudaMemcpyHostToDevice));
     MDX_CUDA_TRY(cudaMemcpy(gr.excl_far.p, far.data(), nid * sizeof(uint8_t), cudaMemcpyHostToDevice));
+    gr.h_excl_start = start;
+    gr.h_excl_ids = ent;
     if (int e = gr.excl_start.alloc(start.size())) return e;
     if (int e = gr.excl_ids.alloc(ent.size())) return e;
     MDX_CUDA_TRY(cudaMemcpy(gr.excl_start.p, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
@@ -941,7 +1202,10 @@ int nlist_init(State &s) {
 // to that stream after the sort, so the caller can run the step's first half
 // and the P3M chain beside them; it waits on s.ev_join[2] (recorded at the
 // end of bstream) before anything that reads the lists.
+static int nlist_rebuild_mf(State &s, bool force, cudaStream_t bstream);
+
 int nlist_rebuild(State &s, bool force, bool conditional, cudaStream_t bstream) {
+    if (s.mf.on) return nlist_rebuild_mf(s, force, bstream);
     GridGPU &gr = s.grid;
     GPUData &d = s.gpd;
     const int n = d.n;
@@ -990,6 +1254,194 @@ int nlist_rebuild(State &s, bool force, bool conditional, cudaStream_t bstream) 
     MDX_CUDA_TRY(launch_pdl(k_finish, dim3(1), dim3(1024), 0, bs, A, (const GridArgs *)nullptr));
     if (bs != s.stream) MDX_CUDA_TRY(cudaEventRecord(s.ev_join[2], bs));
     gr.built = true;
+    return 0;
+}
+
+// The molecule form's rebuild group: the same skin check, then the sort by
+// molecule, then (on bstream when given, beside the step's first half) the
+// molecule-pair list and the E3B molecule list cut from it.
+static int nlist_rebuild_mf(State &s, bool force, cudaStream_t bstream) {
+    const GridArgs A = grid_args(s);
+    const GridArgs Am = mol_scan_args(s);
+    const MolGridArgs M = mol_grid_args(s);
+    const GridArgs *nt = nullptr;
+    const int nb_atoms = (s.gpd.n + 255) / 256;
+    const int nb_mol = (M.nmol + 255) / 256;
+    MDX_CUDA_TRY(launch_pdl(k_check, dim3(nb_atoms), dim3(256), 0, s.stream, A, nt, force ? 1 : 0));
+    MDX_CUDA_TRY(launch_pdl(k_mf_wrap_bin, dim3(nb_mol), dim3(256), 0, s.stream, M));
+    MDX_CUDA_TRY(launch_pdl(k_scan_cells, dim3(1), dim3(kScanThreads), 0, s.stream, Am, nt));
+    MDX_CUDA_TRY(launch_pdl(k_mf_scatter, dim3(nb_mol), dim3(256), 0, s.stream, M));
+    MDX_CUDA_TRY(launch_pdl(k_mf_rank, dim3((M.ncell * 32 + 255) / 256), dim3(256), 0, s.stream, M));
+    MDX_CUDA_TRY(launch_pdl(k_mf_gather, dim3(nb_mol), dim3(256), 0, s.stream, M));
+    MDX_CUDA_TRY(launch_pdl(k_mf_copyback, dim3((4 * M.nmol + 255) / 256), dim3(256), 0, s.stream, M));
+    cudaStream_t bs = s.stream;
+    if (bstream) {
+        MDX_CUDA_TRY(cudaEventRecord(s.ev_sorted, s.stream));
+        MDX_CUDA_TRY(cudaStreamWaitEvent(bstream, s.ev_sorted, 0));
+        bs = bstream;
+    }
+    MDX_CUDA_TRY(launch_pdl(k_mf_build, dim3((M.nmol * 32 + 127) / 128), dim3(128), 0, bs, M));
+    if (FixE3B *e3 = s.e3bFix()) {
+        if (int e = e3b_build_list_mf(s, *e3, bs)) return e;
+    }
+    MDX_CUDA_TRY(launch_pdl(k_finish, dim3(1), dim3(1024), 0, bs, Am, nt));
+    if (bs != s.stream) MDX_CUDA_TRY(cudaEventRecord(s.ev_join[2], bs));
+    s.grid.built = true;
+    return 0;
+}
+
+// The per-site list (the reference's GridGPU list) of the current positions
+// built into the sort's alternate buffers only: the molecule form's primary
+// streams, idToIdx, molecule maps and skin-check positions are untouched.
+// The list's atom indices refer to that sorted copy (ids_alt holds its ids).
+int nlist_build_atoms_view(State &s) {
+    GridGPU &gr = s.grid;
+    const int n = s.gpd.n;
+    const CellGrid g = make_grid(s);
+    const float cutsq = gr.cut * gr.cut;
+    GridArgs A = grid_args(s);
+    A.view = 1;
+    const int nb = (n + 255) / 256;
+    const int ncell = gr.ns.x * gr.ns.y * gr.ns.z;
+    const GridArgs *nt = nullptr;
+    MDX_CUDA_TRY(launch_pdl(k_check, dim3(nb), dim3(256), 0, s.stream, A, nt, 1));
+    MDX_CUDA_TRY(launch_pdl(k_wrap_bin, dim3(nb), dim3(256), 0, s.stream, A, nt));
+    MDX_CUDA_TRY(launch_pdl(k_scan_cells, dim3(1), dim3(kScanThreads), 0, s.stream, A, nt));
+    MDX_CUDA_TRY(launch_pdl(k_scatter, dim3(nb), dim3(256), 0, s.stream, A, nt));
+    MDX_CUDA_TRY(launch_pdl(k_rank, dim3((ncell * 32 + 255) / 256), dim3(256), 0, s.stream, A, nt));
+    MDX_CUDA_TRY(launch_pdl(k_gather, dim3(nb), dim3(256), 0, s.stream, A, nt));
+    if (gr.cap == 0) {
+        MDX_CUDA_TRY(cudaMemsetAsync(&s.d_status.p->max_neighbors, 0, sizeof(uint32_t), s.stream));
+        launch_count(s, g, cutsq);
+        uint32_t mx = 0;
+        MDX_CUDA_TRY(cudaMemcpyAsync(&mx, &s.d_status.p->max_neighbors, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                     s.stream));
+        MDX_CUDA_TRY(cudaStreamSynchronize(s.stream));
+        int c = (int)(mx * 1.35 + 32);
+        c = (c + gr.team - 1) / gr.team * gr.team;
+        gr.cap = c;
+        size_t groups = (size_t)(n + (32 / gr.team) - 1) / (32 / gr.team);
+        if (int e = gr.nlist.alloc(groups * (size_t)c * (32 / gr.team))) return e;
+    }
+    launch_build(s, g, cutsq, s.stream);
+    MDX_CUDA_TRY(launch_pdl(k_finish, dim3(1), dim3(1024), 0, s.stream, A, nt));
+    return 0;
+}
+
+// Molecule form set-up (see MolForm): decides whether the system allows it
+// and sizes its grid and list.  pairForm 1 keeps the per-site form; 2 makes
+// an unsuitable system an error; 0 takes the molecule form when it can.
+int molform_init(State &s) {
+    MolForm &mf = s.mf;
+    mf.on = false;
+    if (s.pairForm == 1) return 0;
+    auto refuse = [&](const char *why) -> int {
+        if (s.pairForm != 2) return 0;
+        set_error(MDX_ERR_UNSUPPORTED, "pairForm 2 (molecule form) not possible: %s", why);
+        return MDX_ERR_UNSUPPORTED;
+    };
+    FixRigid *r = s.rigidFix();
+    FixPair *pf = s.pairFix();
+    if (!r || !r->foursite) return refuse("needs FixRigid with four-site molecules");
+    if (!pf) return refuse("needs a pair fix");
+    if (has_free_atoms(s)) return refuse("every atom must belong to a rigid molecule");
+    if (FixE3B *e3 = s.e3bFix())
+        if (!e3->side_ok) return refuse("FixE3B's molecules must be FixRigid's, in the same order");
+    const int nmol = (int)r->mol_ids.size();
+    if (nmol == 0) return refuse("no molecules");
+    auto site = [&](const int4 &m, int k) { return k == 0 ? m.x : (k == 1 ? m.y : (k == 2 ? m.z : m.w)); };
+    // every molecule alike: site types and charges (as stored, FP32)
+    const int4 m0 = r->mol_ids[0];
+    for (int k = 0; k < 4; k++) {
+        mf.type[k] = s.atoms[site(m0, k)].type;
+        mf.q[k] = (float)s.atoms[site(m0, k)].q;
+    }
+    for (const int4 &m : r->mol_ids)
+        for (int k = 0; k < 4; k++) {
+            const HostAtom &a = s.atoms[site(m, k)];
+            if (a.type != mf.type[k] || (float)a.q != mf.q[k]) return refuse("molecules differ in site types or charges");
+        }
+    // exclusions only inside a molecule, by the same depth in every molecule
+    const GridGPU &gr = s.grid;
+    std::vector<int> site_of(s.atoms.size(), -1), mol_of(s.atoms.size(), -1);
+    for (int mi = 0; mi < nmol; mi++)
+        for (int k = 0; k < 4; k++) {
+            site_of[site(r->mol_ids[mi], k)] = k;
+            mol_of[site(r->mol_ids[mi], k)] = mi;
+        }
+    for (int k = 0; k < 16; k++) mf.depth[k] = 0;
+    bool first = true;
+    for (int mi = 0; mi < nmol; mi++) {
+        int dep[16] = {0};
+        for (int k = 0; k < 4; k++) {
+            const int id = site(r->mol_ids[mi], k);
+            if (!gr.have_excl) break;
+            for (int e = gr.h_excl_start[id]; e < gr.h_excl_start[id + 1]; e++) {
+                const int o = (int)(gr.h_excl_ids[e] & kExclMask);
+                if (mol_of[o] != mi) return refuse("an exclusion joins two molecules");
+                dep[4 * k + site_of[o]] = (int)(gr.h_excl_ids[e] >> 30);
+            }
+        }
+        if (first) {
+            for (int k = 0; k < 16; k++) mf.depth[k] = dep[k];
+            first = false;
+        } else {
+            for (int k = 0; k < 16; k++)
+                if (dep[k] != mf.depth[k]) return refuse("molecules differ in their exclusions");
+        }
+    }
+    // site 0 to any other site: the rigid geometry (+ a margin for the
+    // FP32 positions SETTLE leaves)
+    const double dmax = std::max(r->rc.r_OH, r->rc.r_OM) + 1e-3;
+    const double pair_cut = (double)s.maxRCut();
+    const double cut = pair_cut + s.padding + 2.0 * dmax;
+    const double Lmin = std::min(s.box.Ld.x, std::min(s.box.Ld.y, s.box.Ld.z));
+    if (2.0 * cut >= Lmin) return refuse("the molecule list radius must stay below half the box");
+    if (2.0 * dmax >= (double)gr.cut) return refuse("a molecule must lie within the neighbour cutoff");
+    // cells >= cut / m with at least 2m + 1 per side; the finest such grid
+    // that keeps a mean of two molecules per cell
+    int m = 3;
+    int3 ns{0, 0, 0};
+    for (;; m--) {
+        if (m == 0) return refuse("box too small for the molecule grid");
+        const double w = cut / m * (1.0 + 1e-5);
+        ns = make_int3((int)(s.box.Ld.x / w), (int)(s.box.Ld.y / w), (int)(s.box.Ld.z / w));
+        if (ns.x < 2 * m + 1 || ns.y < 2 * m + 1 || ns.z < 2 * m + 1) continue;
+        if (m == 1 || (double)nmol >= 2.0 * ns.x * ns.y * ns.z) break;
+    }
+    mf.m = m;
+    mf.ns = ns;
+    mf.nmol = nmol;
+    mf.dmax = (float)dmax;
+    mf.cut = (float)cut;
+    mf.far = (float)(pair_cut + 2.0 * dmax);
+    if (s.nThreadPerMolecule != 0 && s.nThreadPerMolecule != 8 && s.nThreadPerMolecule != 16 &&
+        s.nThreadPerMolecule != 32) {
+        set_error(MDX_ERR_ARG, "nThreadPerMolecule must be 0 (automatic), 8, 16 or 32 (got %d)", s.nThreadPerMolecule);
+        return MDX_ERR_ARG;
+    }
+    mf.team = s.nThreadPerMolecule ? s.nThreadPerMolecule : 16;
+    const double vol = s.box.Ld.x * s.box.Ld.y * s.box.Ld.z;
+    const double nbar = nmol / vol * 4.18879 * cut * cut * cut;
+    mf.cap = ((int)(1.5 * nbar + 64) + mf.team - 1) / mf.team * mf.team;
+    const int ncell = ns.x * ns.y * ns.z;
+    if (int e = mf.cell_start.alloc(ncell + 1)) return e;
+    if (int e = mf.cell_count.alloc(ncell)) return e;
+    if (int e = mf.cell_fill.alloc(ncell)) return e;
+    MDX_CUDA_TRY(cudaMemsetAsync(mf.cell_count.p, 0, ncell * sizeof(uint32_t), s.stream));
+    if (int e = mf.cell_of.alloc(nmol)) return e;
+    if (int e = mf.perm_tmp.alloc(nmol)) return e;
+    if (int e = mf.perm.alloc(nmol)) return e;
+    if (int e = mf.counts.alloc(nmol)) return e;
+    const int G = 32 / mf.team;
+    const size_t groups = (size_t)(nmol + G - 1) / G;
+    if (int e = mf.list.alloc(groups * (size_t)mf.cap * G)) return e;
+    // the sort reads the molecule maps first: after an upload every atom sits
+    // at index == id, so the maps are the molecules' ids
+    MDX_CUDA_TRY(cudaMemcpy(r->d_mol_idx.p, r->mol_ids.data(), nmol * sizeof(int4), cudaMemcpyHostToDevice));
+    if (FixE3B *e3 = s.e3bFix())
+        MDX_CUDA_TRY(cudaMemcpy(e3->d_mol_idx.p, r->mol_ids.data(), nmol * sizeof(int4), cudaMemcpyHostToDevice));
+    mf.on = true;
     return 0;
 }
 

@@ -369,12 +369,330 @@ PairArgs make_args(State &s, FixPair &f) {
     return A;
 }
 
+// ---- molecule form (all-rigid four-site water) ---------------------------
+// One team of T lanes per molecule slot k (sites at 4k .. 4k+3) walks k's
+// molecule-pair list; for each listed slot j the four site positions are one
+// 64-byte gather, and every site pair (a of k, b of j) that can interact
+// (bit 4a+b of the LJ / charge masks: eps(a,b) != 0, q_a q_b != 0) is
+// evaluated as compute_force_iso evaluates a listed pair: minimum image per
+// site pair, LJ/WCA when r^2 < rc^2(a,b), Ewald real space when r^2 < qrc^2.
+// A molecule pair whose site-0 distance is beyond `far` has no site pair
+// within the cutoffs and is skipped.  The molecule's own site pairs (the
+// excluded pairs of the reference's list, multiplier by exclusion depth) are
+// added by the team's first lane.  Forces on the four sites are reduced over
+// the team by shuffles and written by lanes 0..3 (one 64-byte store).
+constexpr int kMolPairBlock = 64;
+
+struct MolPairArgs {
+    int nmol;
+    const float4 *__restrict__ xs;
+    float4 *__restrict__ fs;
+    const uint32_t *__restrict__ counts;
+    const uint32_t *__restrict__ list;
+    int cap;
+    Box box;
+    float far2, qrc2, alpha;
+    uint32_t ljm, qm, selfm;  // bit 4a+b: LJ term, charge term, own-molecule pair
+    // per site pair ab: rc^2, 48 eps sig^12, 24 eps sig^6, sig^6, eps, the
+    // LJ/cut energy shift at rc, qqr q_a q_b, exclusion multiplier (own pairs)
+    float rc2[16], p1[16], p2[16], sig6[16], eps[16], eoff[16], qq[16], mult[16];
+    float *__restrict__ virials;
+    float *__restrict__ energy;  // per site (energy kernel)
+};
+
+template <int T>
+__device__ __forceinline__ float3 team_sum3(float3 v) {
+    return make_float3(team_sum<T>(v.x), team_sum<T>(v.y), team_sum<T>(v.z));
+}
+
+// site pair ab at r2 with multiplier mult (1 between molecules; own pairs
+// carry their exclusion multiplier and the Ewald correction for the excluded
+// part, ChargeEvaluatorEwald.h:11-64): scalar force factor s (F = dr s) and
+// half the pair energy e; returns whether a term was in range
+template <int LJ, bool EW, bool ENERGY, bool OWN>
+__device__ __forceinline__ bool mol_pair_term(const MolPairArgs &A, int ab, float r2, float mult, float &s, float &e) {
+    bool any = false;
+    s = 0.f;
+    e = 0.f;
+    if (LJ && ((A.ljm >> ab) & 1u) && r2 < A.rc2[ab]) {
+        any = true;
+        if (!OWN || mult != 0.f) {
+            const float r2inv = 1.0f / r2;
+            const float r6inv = r2inv * r2inv * r2inv;
+            s += r6inv * r2inv * (A.p1[ab] * r6inv - A.p2[ab]) * (OWN ? mult : 1.0f);
+            if (ENERGY) {
+                const float s6r6 = A.sig6[ab] * r6inv;
+                const float m = OWN ? mult : 1.0f;
+                if (LJ == 1) e += 0.5f * 4.0f * A.eps[ab] * (s6r6 * (s6r6 - 1.0f) - A.eoff[ab]) * m;
+                else e += 0.5f * (4.0f * A.eps[ab] * s6r6 * (s6r6 - 1.0f) + A.eps[ab]) * m;
+            }
+        }
+    }
+    if (EW && ((A.qm >> ab) & 1u) && r2 < A.qrc2) {
+        any = true;
+        const float r2c = r2 < 1e-10f ? 1e-10f : r2;
+        const float rinv = rsqrtf(r2c);
+        const float x = A.alpha * (r2c * rinv);
+        const float expm = __expf(-x * x);
+        const float erfcv = erfc_as(x, expm);
+        const float qq = A.qq[ab];
+        float fsc = qq * (erfcv * rinv + (2.0f * 0.5641895835477563f * A.alpha) * expm);
+        if (OWN && mult < 1.0f) fsc -= (1.0f - mult) * qq * rinv;
+        s += fsc * (rinv * rinv);
+        if (ENERGY) {
+            float eng = qq * rinv * erfcv;
+            if (OWN && mult < 1.0f) eng -= (1.0f - mult) * qq * rinv;
+            e += 0.5f * eng;
+        }
+    }
+    return any;
+}
+
+template <bool VIR>
+__device__ __forceinline__ void add_vir(float (&v)[6], float3 F, float3 dr) {
+    if (VIR) {
+        v[0] += F.x * dr.x;
+        v[1] += F.y * dr.y;
+        v[2] += F.z * dr.z;
+        v[3] += F.x * dr.y;
+        v[4] += F.x * dr.z;
+        v[5] += F.y * dr.z;
+    }
+}
+
+template <int T, int LJ, bool EW, bool VIR, bool ENERGY>
+__global__ void __launch_bounds__(kMolPairBlock) k_pair_mol(const MolPairArgs A, int accumulate) {
+    pdl_wait();
+    constexpr int G = 32 / T;
+    constexpr int U = 2;  // list entries in flight per lane
+    constexpr uint32_t kNone = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int slot = lane / T, t = lane % T;
+    const int k = warp * G + slot;
+    const bool valid = k < A.nmol;
+    float3 xi[4];
+    float3 f[4];
+    float en[4];
+    float v[4][6];
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+        xi[a] = make_float3(0.f, 0.f, 0.f);
+        f[a] = make_float3(0.f, 0.f, 0.f);
+        en[a] = 0.f;
+#pragma unroll
+        for (int c = 0; c < 6; c++) v[a][c] = 0.f;
+    }
+    int cnt = 0;
+    const uint32_t *row = nullptr;
+    if (valid) {
+#pragma unroll
+        for (int a = 0; a < 4; a++) xi[a] = f3(A.xs[4 * k + a]);
+        cnt = (int)A.counts[k];
+        cnt = cnt < A.cap ? cnt : A.cap;
+        row = A.list + (size_t)(k / G) * A.cap * G + slot * T + t;
+    }
+    const uint32_t any_mask = (LJ ? A.ljm : 0u) | (EW ? A.qm : 0u);
+    for (int e0 = t; e0 < cnt; e0 += U * T) {
+        uint32_t ent[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int e = e0 + u * T;
+            ent[u] = e < cnt ? __ldg(row + (size_t)(e / T) * 32) : kNone;
+        }
+        float3 xj[U][4];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int j = ent[u] == kNone ? k : (int)ent[u];
+#pragma unroll
+            for (int b = 0; b < 4; b++) xj[u][b] = f3(__ldg(A.xs + 4 * j + b));
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (ent[u] == kNone) continue;
+            const float3 d00 = min_image(A.box, xi[0] - xj[u][0]);
+            const float r00 = dot3(d00, d00);
+            if (r00 >= A.far2) continue;
+#pragma unroll
+            for (int a = 0; a < 4; a++) {
+#pragma unroll
+                for (int b = 0; b < 4; b++) {
+                    const int ab = 4 * a + b;
+                    if (!((any_mask >> ab) & 1u)) continue;
+                    const float3 dr = ab == 0 ? d00 : min_image(A.box, xi[a] - xj[u][b]);
+                    const float r2 = ab == 0 ? r00 : dot3(dr, dr);
+                    float sc, e;
+                    if (mol_pair_term<LJ, EW, ENERGY, false>(A, ab, r2, 1.0f, sc, e)) {
+                        const float3 F = dr * sc;
+                        f[a] += F;
+                        if (ENERGY) en[a] += e;
+                        add_vir<VIR>(v[a], F, dr);
+                    }
+                }
+            }
+        }
+    }
+    // the molecule's own site pairs, once per molecule
+    if (valid && t == 0 && A.selfm) {
+#pragma unroll
+        for (int a = 0; a < 4; a++) {
+#pragma unroll
+            for (int b = 0; b < 4; b++) {
+                const int ab = 4 * a + b;
+                if (a == b || !((A.selfm >> ab) & 1u)) continue;
+                const float3 dr = min_image(A.box, xi[a] - xi[b]);
+                const float r2 = dot3(dr, dr);
+                float sc, e;
+                if (mol_pair_term<LJ, EW, ENERGY, true>(A, ab, r2, A.mult[ab], sc, e)) {
+                    const float3 F = dr * sc;
+                    f[a] += F;
+                    if (ENERGY) en[a] += e;
+                    add_vir<VIR>(v[a], F, dr);
+                }
+            }
+        }
+    }
+    pdl_trigger();
+    // team sums; lane t < 4 of the team writes site t
+    if (ENERGY) {
+#pragma unroll
+        for (int a = 0; a < 4; a++) en[a] = team_sum<T>(en[a]);
+        if (valid && t < 4) A.energy[4 * k + t] = t == 0 ? en[0] : (t == 1 ? en[1] : (t == 2 ? en[2] : en[3]));
+        return;
+    }
+#pragma unroll
+    for (int a = 0; a < 4; a++) f[a] = team_sum3<T>(f[a]);
+    if (VIR) {
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int c = 0; c < 6; c++) v[a][c] = team_sum<T>(v[a][c]);
+    }
+    if (valid && t < 4) {
+        const float3 fm = t == 0 ? f[0] : (t == 1 ? f[1] : (t == 2 ? f[2] : f[3]));
+        float4 fo = A.fs[4 * k + t];
+        if (accumulate) {
+            fo.x += fm.x;
+            fo.y += fm.y;
+            fo.z += fm.z;
+        } else {
+            fo.x = fm.x;
+            fo.y = fm.y;
+            fo.z = fm.z;
+        }
+        A.fs[4 * k + t] = fo;
+        if (VIR) {
+            float *vv = A.virials + 6 * (size_t)(4 * k + t);
+#pragma unroll
+            for (int c = 0; c < 6; c++) {
+                const float vm = t == 0 ? v[0][c] : (t == 1 ? v[1][c] : (t == 2 ? v[2][c] : v[3][c]));
+                vv[c] += 0.5f * vm;
+            }
+        }
+    }
+}
+
+MolPairArgs make_mol_args(State &s, FixPair &f) {
+    const MolForm &mf = s.mf;
+    MolPairArgs A{};
+    A.nmol = mf.nmol;
+    A.xs = s.gpd.xs.p;
+    A.fs = s.gpd.fs.p;
+    A.counts = mf.counts.p;
+    A.list = mf.list.p;
+    A.cap = mf.cap;
+    A.box = s.box;
+    A.far2 = mf.far * mf.far;
+    A.virials = s.gpd.virials.p;
+    A.energy = nullptr;
+    const int nt = (int)s.species.size();
+    const int nt2 = nt * nt;
+    const bool ew = f.chargeFix != nullptr;
+    A.qrc2 = 0.f;
+    A.alpha = 0.f;
+    if (ew) {
+        const float qrc = (float)f.chargeRCut;
+        A.qrc2 = qrc * qrc;
+        A.alpha = (float)f.chargeFix->alpha;
+    }
+    const float qqr = (float)s.units.qqr_to_eng;
+    const float coef[3] = {s.specialNeighborCoefs[0], s.specialNeighborCoefs[1], s.specialNeighborCoefs[2]};
+    A.ljm = A.qm = A.selfm = 0u;
+    for (int a = 0; a < 4; a++)
+        for (int b = 0; b < 4; b++) {
+            const int ab = 4 * a + b;
+            const int ix = mf.type[a] * nt + mf.type[b];
+            // the same FP32 products as the per-site kernel forms them
+            const float rc2 = f.h_params[ix], eps24 = f.h_params[nt2 + ix], sig6 = f.h_params[2 * nt2 + ix];
+            A.rc2[ab] = rc2;
+            A.p1[ab] = eps24 * 2.f * sig6 * sig6;
+            A.p2[ab] = eps24 * sig6;
+            A.sig6[ab] = sig6;
+            A.eps[ab] = eps24 / 24.0f;
+            const float rc6 = rc2 * rc2 * rc2;
+            const float s6rc6 = sig6 / rc6;
+            A.eoff[ab] = s6rc6 * (s6rc6 - 1.0f);
+            A.qq[ab] = qqr * mf.q[a] * mf.q[b];
+            const int dep = mf.depth[ab];
+            A.mult[ab] = dep == 0 ? 1.0f : coef[dep - 1];
+            if (eps24 != 0.f) A.ljm |= 1u << ab;
+            if (ew && mf.q[a] * mf.q[b] != 0.f) A.qm |= 1u << ab;
+            if (a != b) A.selfm |= 1u << ab;
+        }
+    return A;
+}
+
+template <int T, int LJ, bool EW>
+void mol_launch_t(const MolPairArgs &A, int virialMode, bool energy, bool accumulate, cudaStream_t st) {
+    const int warps = (A.nmol + 32 / T - 1) / (32 / T);
+    const dim3 blocks((warps * 32 + kMolPairBlock - 1) / kMolPairBlock);
+    if (energy) {
+        k_pair_mol<T, LJ, EW, false, true><<<blocks, kMolPairBlock, 0, st>>>(A, 0);
+        MDX_LAUNCHED();
+    } else if (virialMode == 1 || virialMode == 2) {
+        k_pair_mol<T, LJ, EW, true, false><<<blocks, kMolPairBlock, 0, st>>>(A, accumulate ? 1 : 0);
+        MDX_LAUNCHED();
+    } else {
+        launch_pdl(k_pair_mol<T, LJ, EW, false, false>, blocks, dim3(kMolPairBlock), 0, st, A, accumulate ? 1 : 0);
+    }
+}
+
+template <int T>
+void mol_launch_kind(const MolPairArgs &A, int lj, bool ew, int virialMode, bool energy, bool accumulate,
+                     cudaStream_t st) {
+    if (lj == 1 && ew) mol_launch_t<T, 1, true>(A, virialMode, energy, accumulate, st);
+    else if (lj == 1) mol_launch_t<T, 1, false>(A, virialMode, energy, accumulate, st);
+    else if (ew) mol_launch_t<T, 2, true>(A, virialMode, energy, accumulate, st);
+    else mol_launch_t<T, 2, false>(A, virialMode, energy, accumulate, st);
+}
+
 }  // namespace
 
 int pair_launch(State &s, FixPair &f, int virialMode, bool accumulate) {
+    if (s.mf.on) return pair_mol_launch(s, f, virialMode, accumulate, nullptr, s.stream);
     PairArgs A = make_args(s, f);
     bool vir = virialMode == 1 || virialMode == 2;
     return launch_any(A, s.grid.team, f.lj_kind, f.chargeFix != nullptr, vir, false, accumulate, s.stream);
+}
+
+// the molecule form of the pair forces (energy: per-site energies into
+// `energy` instead of forces)
+int pair_mol_launch(State &s, FixPair &f, int virialMode, bool accumulate, float *energy, cudaStream_t st) {
+    MolPairArgs A = make_mol_args(s, f);
+    A.energy = energy;
+    const bool ew = f.chargeFix != nullptr;
+    const bool en = energy != nullptr;
+    if (f.lj_kind != 1 && f.lj_kind != 2) {
+        set_error(MDX_ERR_ARG, "pair kind %d", f.lj_kind);
+        return MDX_ERR_ARG;
+    }
+    switch (s.mf.team) {
+        case 8: mol_launch_kind<8>(A, f.lj_kind, ew, virialMode, en, accumulate, st); break;
+        case 16: mol_launch_kind<16>(A, f.lj_kind, ew, virialMode, en, accumulate, st); break;
+        case 32: mol_launch_kind<32>(A, f.lj_kind, ew, virialMode, en, accumulate, st); break;
+        default: set_error(MDX_ERR_ARG, "lanes per molecule %d not in {8, 16, 32}", s.mf.team); return MDX_ERR_ARG;
+    }
+    return 0;
 }
 
 // compute_energy_iso (PairEvaluateIso.h:212-358): per-site energies into the
@@ -386,7 +704,11 @@ int pair_energy(State &s, FixPair &f, double *out) {
         return MDX_ERR_STATE;
     }
     A.energy = s.e_site.p;
-    if (int r = launch_any(A, s.grid.team, f.lj_kind, f.chargeFix != nullptr, false, true, false, s.stream)) return r;
+    if (s.mf.on) {
+        if (int r = pair_mol_launch(s, f, 0, false, s.e_site.p, s.stream)) return r;
+    } else if (int r = launch_any(A, s.grid.team, f.lj_kind, f.chargeFix != nullptr, false, true, false, s.stream)) {
+        return r;
+    }
     return float_sum(s, s.e_site.p, A.n, out);
 }
 

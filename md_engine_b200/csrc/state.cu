@@ -193,8 +193,12 @@ int State::checkStatus() {
     MDX_CUDA_TRY(cudaStreamSynchronize(stream));
     const uint32_t b = h_status->bits;
     if (b & kStatusNlistOverflow) {
-        set_error(MDX_ERR_OVERFLOW, "neighbour list capacity %d exceeded (max count %u)", grid.cap,
-                  h_status->max_neighbors);
+        if (mf.on)
+            set_error(MDX_ERR_OVERFLOW, "molecule-pair list capacity %d exceeded (max count %u)", mf.cap,
+                      h_status->max_mol_neighbors);
+        else
+            set_error(MDX_ERR_OVERFLOW, "neighbour list capacity %d exceeded (max count %u)", grid.cap,
+                      h_status->max_neighbors);
         return MDX_ERR_OVERFLOW;
     }
     if (b & kStatusMolOverflow) {
@@ -283,6 +287,7 @@ int State::prepare() {
         if (int e = r->prepareForRun()) return e;  // device molecule arrays
     }
     if (int e = nlist_set_interactions(*this)) return e;
+    if (int e = molform_init(*this)) return e;
     // first build (GridGPU::periodicBoundaryConditions(-1, true), Integrator.cu:216)
     if (int e = nlist_rebuild(*this, true, false)) return e;
     if (int e = computeForces(0)) return e;  // forceInitial

@@ -100,7 +100,8 @@ class State:
     """src/State.h:63-146 -- owns the atoms and the device copy."""
 
     _DOUBLE_KEYS = ("rCut", "padding", "dt")
-    _INT_KEYS = ("periodicInterval", "nThreadPerAtom", "nThreadPerBlock", "gridStencil", "gridHomeGroup", "turn")
+    _INT_KEYS = ("periodicInterval", "nThreadPerAtom", "nThreadPerBlock", "gridStencil", "gridHomeGroup", "turn",
+                 "pairForm", "nThreadPerMolecule")
 
     def __init__(self):
         h = c_void_p()
@@ -139,7 +140,7 @@ class State:
             out = c_dbl()
             check(lib().mdx_state_get_double(self._h, k.encode(), ctypes.byref(out)))
             return out.value
-        if k in State._INT_KEYS or k in ("nlistCapacity", "cellsPerSide"):
+        if k in State._INT_KEYS or k in ("nlistCapacity", "cellsPerSide", "molListCapacity"):
             out = c_i64()
             check(lib().mdx_state_get_int(self._h, k.encode(), ctypes.byref(out)))
             return out.value

@@ -127,7 +127,7 @@ def test_pair_force_gridgpu_matches_reference_kernel_lj(oracle, ntpb, ntpa):
     vg = d_v.cpu().numpy().astype(np.float64).sum(0)
     vr = ref["virial"].sum(0)
     assert np.abs(vg - vr).max() < 2e-4 * np.abs(vr).max()
-    if R.available():
+    if R.available() and ntpa >= 2:  # the harness launches the reference's team kernels only
         fr = R.pair_forces(xs4, None, counts, ent, pf, 1, sysd.lo, sysd.L, (0.0, 0.0, 0.5), 1, 0.0, 0.0, 1.0,
                            ntpb=ntpb, ntpa=ntpa)
         rms = np.sqrt(np.mean(np.sum(fr ** 2, 1)))

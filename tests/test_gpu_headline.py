@@ -17,9 +17,10 @@ pytestmark = pytest.mark.gpu
 RCUT, SKIN, GRID = 9.0, 1.0, 64
 
 
-def _state(e3b, steps):
+def _state(e3b, steps, form=0):
     sysd = systems.water_tip4p2005(nside=16, seed=20261203)
     st, fx = systems.build_water_state(sysd, rcut=RCUT, skin=SKIN, grid=GRID, e3b=e3b, T=298.0, tau=25.0)
+    st.pairForm = form
     st.prepare()
     if steps:
         IntegratorVerlet(st).run(steps)
@@ -41,11 +42,14 @@ def _oracle_pair_p3m(O, sysd, x, alpha):
     return pr, frec, erec - alpha / np.sqrt(np.pi) * q2, vir
 
 
-@pytest.mark.parametrize("steps", [0, 300])
-def test_headline_forces_energy_virial_vs_fp64_oracle(oracle, steps):
-    sysd, st, fx = _state(False, steps)
-    # the benchmarked variants: full-warp neighbour team, own 64^3 FFT
-    assert int(st.nThreadPerAtom) == 32
+@pytest.mark.parametrize("steps,form", [(0, 0), (300, 0), (300, 1)])
+def test_headline_forces_energy_virial_vs_fp64_oracle(oracle, steps, form):
+    """form 0: the automatic choice (the molecule form for this all-rigid
+    water, the benchmarked path); form 1: the per-site form (full-warp team)"""
+    sysd, st, fx = _state(False, steps, form)
+    assert int(st.pairForm) == (2 if form == 0 else 1)
+    if form == 1:
+        assert int(st.nThreadPerAtom) == 32
     st.computeForces(virialMode=1)
     x, _, fg = st.getAtoms()
     _, vg = st.virials()
@@ -131,8 +135,10 @@ def test_every_neighbour_team_matches_oracle(oracle, team):
     sysd = water_small(seed=17)
     rc = 6.5
     st, fx = systems.build_water_state(sysd, rcut=rc, skin=1.0, grid=32, alpha=0.35, thermostat=False)
+    st.pairForm = 1  # the per-site form: the team walks the per-site list
     st.nThreadPerAtom = team
     st.prepare()
+    assert int(st.pairForm) == 1
     st.computeForces()
     x, _, fg = st.getAtoms()
     excl = oracle.exclusions_from_bonds(len(x), water_bonds(sysd.molecules))
@@ -146,3 +152,40 @@ def test_every_neighbour_team_matches_oracle(oracle, team):
     ref = ref + oracle.p3m_forces(x, sysd.q, sysd.lo, sysd.L, (32, 32, 32), 0.35)
     rel, rms = force_err(fg, ref)
     assert rel < FORCE_RTOL, f"team {team}: max force error {rel:.3e} of RMS {rms:.3e}"
+
+
+@pytest.mark.parametrize("team", [8, 16, 32])
+def test_molecule_form_teams_match_per_site_form(oracle, team):
+    """The molecule form (molecule-pair list, every site pair of a listed
+    molecule pair) against the per-site form on the same positions, for each
+    lane count per molecule; both against the FP64 oracle; energies and
+    virials too"""
+    from tests.helpers import water_small
+    sysd = water_small(seed=23)
+    rc = 6.5
+    res = {}
+    x0 = None
+    for form in (1, 2):
+        st, fx = systems.build_water_state(sysd, rcut=rc, skin=1.0, grid=32, alpha=0.35, e3b=True,
+                                           thermostat=False)
+        st.pairForm = form
+        st.nThreadPerMolecule = team
+        st.prepare()
+        if x0 is None:
+            x0, _, _ = st.getAtoms()
+        else:
+            st.putAtoms(positions=x0)
+            st.buildNeighborlists(force=True)
+        assert int(st.pairForm) == form
+        st.computeForces(virialMode=1)
+        x, _, f = st.getAtoms()
+        _, vir = st.virials()
+        res[form] = (x, f, vir, st.potentialEnergy())
+    (x1, f1, v1, e1), (x2, f2, v2, e2) = res[1], res[2]
+    d = x2 - x1
+    d -= sysd.L * np.rint(d / sysd.L)
+    assert np.abs(d).max() < 1e-5
+    rel, rms = force_err(f2, f1)
+    assert rel < 2e-5, f"molecule vs per-site form: {rel:.3e} of RMS {rms:.3e}"
+    assert np.abs(v2 - v1).max() < 2e-5 * np.abs(v1).max()
+    assert np.allclose(e2, e1, rtol=1e-5, atol=1e-6)
