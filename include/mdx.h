@@ -158,7 +158,10 @@ int mdx_prepare(mdx_state *st);
 int mdx_nlist_build(mdx_state *st, int force_build);
 /* Grid.getNeighborList (src/GridGPU.cu:1520-1648): per-id neighbour ids,
  * sorted ascending.  counts[id]; nbr[id*max_per_atom + k] (atom ids);
- * tags[id*max_per_atom + k] = exclusion depth (0..3), may be NULL. */
+ * tags[id*max_per_atom + k] = exclusion depth (0..3), may be NULL.  nbr NULL:
+ * the counts alone (to size nbr).  In the molecule form (rigid water, no
+ * per-site list in the step) the per-site list of the current positions is
+ * built by the call itself, beside the step's buffers. */
 int mdx_nlist_get(mdx_state *st, int max_per_atom, int *counts, int *nbr, int *tags);
 /* IntegratorUtil::force(virialMode) (src/Integrators/IntegratorUtil.cpp:15-30):
  * zero forces, run every fix's compute() */

@@ -119,7 +119,6 @@ int mdx_state_set_int(mdx_state *st, const char *key, int64_t v) {
     else if (k == "nThreadPerBlock") s.nThreadPerBlock = (int)v;
     else if (k == "gridStencil") s.gridStencil = (int)v;
     else if (k == "gridHomeGroup") s.gridHomeGroup = (int)v;
-    else if (k == "nThreadPerMolecule") s.nThreadPerMolecule = (int)v;
     else if (k == "pairForm") {
         ARG_CHECK(v >= 0 && v <= 2, "pairForm must be 0 (automatic), 1 (per-site) or 2 (molecule)");
         s.pairForm = (int)v;
@@ -146,7 +145,6 @@ int mdx_state_get_int(mdx_state *st, const char *key, int64_t *v) {
     else if (k == "gridHomeGroup") *v = s.grid.home_group;
     else if (k == "pairForm") *v = s.prepared ? (s.mf.on ? 2 : 1) : s.pairForm;
     else if (k == "molListCapacity") *v = s.mf.cap;
-    else if (k == "nThreadPerMolecule") *v = s.prepared && s.mf.on ? s.mf.team : s.nThreadPerMolecule;
     else {
         set_error(MDX_ERR_ARG, "unknown int key '%s'", key);
         return MDX_ERR_ARG;
@@ -476,7 +474,7 @@ int mdx_nlist_build(mdx_state *st, int force_build) {
 }
 
 int mdx_nlist_get(mdx_state *st, int max_per_atom, int *counts, int *nbr, int *tags) {
-    ARG_CHECK(st && counts && nbr && max_per_atom > 0, "null argument");
+    ARG_CHECK(st && counts && (nbr == nullptr || max_per_atom > 0), "null argument");
     State &s = *st->s;
     if (int e = need_prepared(s)) return e;
     // the molecule form keeps no per-site list: build it now, on the current
@@ -500,6 +498,10 @@ int mdx_nlist_get(mdx_state *st, int max_per_atom, int *counts, int *nbr, int *t
     for (int i = 0; i < n; i++) {
         const uint32_t id = ids[i];
         const int c = (int)std::min<uint32_t>(cnt[i], (uint32_t)g.cap);
+        if (!nbr) {  // counts only (sizing query)
+            counts[id] = (int)cnt[i];
+            continue;
+        }
         if (c > max_per_atom || (int)cnt[i] > g.cap) {
             set_error(MDX_ERR_OVERFLOW, "atom %u has %u neighbours (> %d)", id, cnt[i], std::min(max_per_atom, g.cap));
             return MDX_ERR_OVERFLOW;

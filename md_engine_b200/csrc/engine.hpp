@@ -424,7 +424,6 @@ class State {
     // 0 automatic (molecule form when the system allows it), 1 per-site
     // (atom) form, 2 molecule form (an error at prepare when not allowed)
     int pairForm = 0;
-    int nThreadPerMolecule = 0;  // molecule form: lanes per molecule (8, 16, 32; 0 = automatic)
     MolForm mf;
     // list build tunables, 0 = automatic: cells of >= cut/gridStencil (1..4),
     // home atoms tested at once per warp (2 or 4)

@@ -79,6 +79,7 @@ struct P3MArgs {
     // H1, H2, M of mol_idx[m] (four-site, uncharged O) or O, H1, H2
     const int4 *mol_idx;
     int nmol, four_site;
+    int slots;  // 1: the molecule form's layout, molecule slot m at sites 4m .. 4m+3 (no map read)
 };
 #define MDX_P3M_ARGS const P3MArgs A = tab ? tab[blockIdx.y] : a0
 
@@ -160,7 +161,8 @@ __global__ void k_spread_mol(const P3MArgs A) {
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int m = (lane / 15) * W + w;
     if (lane >= 30 || w >= W || m >= A.nmol) return;
-    spread_plane(A, mol_site(A.mol_idx[m], (lane % 15) / 5, A.four_site), lane % 5);
+    const int4 ix = A.slots ? make_int4(4 * m, 4 * m + 1, 4 * m + 2, 4 * m + 3) : A.mol_idx[m];
+    spread_plane(A, mol_site(ix, (lane % 15) / 5, A.four_site), lane % 5);
 }
 
 // E_d(k) = i k_d G rho on the half spectrum (z halved), batched output
@@ -356,6 +358,7 @@ P3MArgs p3m_args(State &s, FixChargeEwald &f) {
     A.nk = (size_t)f.sz.x * f.sz.y * (f.sz.z / 2 + 1);
     A.ngrid = (size_t)f.sz.x * f.sz.y * f.sz.z;
     A.niv = (float)(-1.0 / (s.box.Ld.x * s.box.Ld.y * s.box.Ld.z));
+    A.slots = 0;
     return A;
 }
 
@@ -673,7 +676,7 @@ __global__ void k_gather_mol(const P3MArgs A, const float4 *__restrict__ e4) {
     int i = 0;
     float q = 0.f;
     if (valid) {
-        ix = A.mol_idx[m];
+        ix = A.slots ? make_int4(4 * m, 4 * m + 1, 4 * m + 2, 4 * m + 3) : A.mol_idx[m];
         i = mol_site(ix, k, A.four_site);
         q = A.qs[i];
     }
@@ -953,6 +956,7 @@ P3MArgs mol_args(State &s, FixChargeEwald &f, const FixRigid &r) {
     A.mol_idx = r.d_mol_idx.p;
     A.nmol = (int)r.mol_ids.size();
     A.four_site = r.mol_ids[0].w >= 0 ? 1 : 0;
+    A.slots = s.mf.on ? 1 : 0;
     return A;
 }
 

@@ -250,7 +250,14 @@ struct MolArgs {
     const float4 *fextra;
     const float4 *frecip;  // P3M reciprocal forces of every site (may be null)
     int nblk;  // blocks of k_second_mol that carry this system's molecules
+    // 1: the molecule form's layout, thread m takes slot m whose sites are
+    // 4m .. 4m+3 (coalesced, no map read); 0: molecule m's sites from mol_idx
+    int slots;
 };
+
+__device__ __forceinline__ int4 mol_sites(const MolArgs &A, int m) {
+    return A.slots ? make_int4(4 * m, 4 * m + 1, 4 * m + 2, 4 * m + 3) : A.mol_idx[m];
+}
 #define MDX_MOL_ARGS \
     pdl_wait();      \
     const MolArgs A = tab ? tab[blockIdx.y] : a0
@@ -304,7 +311,6 @@ __global__ void k_first_mol(const MolArgs a0, const MolArgs *__restrict__ tab) {
     MDX_MOL_ARGS;
     int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= A.nmol) return;
-    const int4 *__restrict__ mol_idx = A.mol_idx;
     float4 *__restrict__ xs = A.xs;
     float4 *__restrict__ vs = A.vs;
     float4 *__restrict__ fs = A.fs;
@@ -313,7 +319,7 @@ __global__ void k_first_mol(const MolArgs a0, const MolArgs *__restrict__ tab) {
     const float dt = A.dt, dtf = A.dtf;
     const NHChain *__restrict__ chain = A.chain;
     DeviceStatus *st = A.st;
-    const int4 ix = mol_idx[m];
+    const int4 ix = mol_sites(A, m);
     const int id3[3] = {ix.x, ix.y, ix.z};
     float4 x0[3], x[3], v[3];
     const float s = NH ? (float)chain[0].scale : 1.0f;
@@ -463,7 +469,6 @@ __global__ void k_second_mol(const MolArgs a0, const MolArgs *__restrict__ tab) 
     if ((int)blockIdx.x >= A.nblk) return;  // the whole block: not counted
     __shared__ double sh[32];
     const int nmol = A.nmol;
-    const int4 *__restrict__ mol_idx = A.mol_idx;
     const float4 *__restrict__ xs = A.xs;
     float4 *__restrict__ vs = A.vs;
     float4 *__restrict__ fs = A.fs;
@@ -476,7 +481,7 @@ __global__ void k_second_mol(const MolArgs a0, const MolArgs *__restrict__ tab) 
     int m = blockIdx.x * blockDim.x + threadIdx.x;
     double mv2 = 0.0;
     if (m < nmol) {
-        const int4 ix = mol_idx[m];
+        const int4 ix = mol_sites(A, m);
         const int id3[3] = {ix.x, ix.y, ix.z};
         float4 x[3], v[3], f[3];
 #pragma unroll
@@ -784,6 +789,7 @@ MolArgs mol_args(State &s, FixRigid &r) {
     A.fextra = nullptr;
     A.frecip = nullptr;
     A.nblk = rigid_blocks(A.nmol);
+    A.slots = 0;
     return A;
 }
 
@@ -859,7 +865,8 @@ int step_first_half(State &s, bool fused) {
         MDX_LAUNCHED();
     }
     if (r) {
-        const MolArgs A = mol_args(s, *r);
+        MolArgs A = mol_args(s, *r);
+        A.slots = s.mf.on ? 1 : 0;
         if (nh)
             MDX_CUDA_TRY(launch_pdl(k_first_mol<true>, dim3(rigid_blocks(A.nmol)), dim3(kMolBlock), 0, s.stream, A,
                                     (const MolArgs *)nullptr));
@@ -913,6 +920,7 @@ int step_second_half(State &s, bool fused, const float4 *fextra, const float4 *f
         A.nparts = nparts;
         A.fextra = fextra;
         A.frecip = frecip;
+        A.slots = s.mf.on ? 1 : 0;
         MDX_CUDA_TRY(launch_pdl(k_second_mol, dim3(mb), dim3(kMolBlock), 0, s.stream, A, (const MolArgs *)nullptr));
     }
     return 0;

@@ -115,7 +115,7 @@ __global__ void k_wrap_bin(const GridArgs a0, const GridArgs *__restrict__ tab) 
         p.x = p.x - box.L.x * ix;
         p.y = p.y - box.L.y * iy;
         p.z = p.z - box.L.z * iz;
-        A.xs[i] = p;
+        if (!A.view) A.xs[i] = p;  // a view build wraps its sorted copy only (k_gather)
     }
     int c = cell_of_pos(A.g, f3(p));
     A.cell_of[i] = c;
@@ -240,7 +240,22 @@ __global__ void k_gather(const GridArgs a0, const GridArgs *__restrict__ tab) {
     int d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= A.n) return;
     int s = A.perm[d];
-    A.xs2[d] = A.xs[s];
+    if (A.view) {
+        // the view build's copy, wrapped as k_wrap_bin wraps in place
+        const Box &box = A.box;
+        float4 p = A.xs[s];
+        const float ix = floorf((p.x - box.lo.x) / box.L.x);
+        const float iy = floorf((p.y - box.lo.y) / box.L.y);
+        const float iz = floorf((p.z - box.lo.z) / box.L.z);
+        if (ix != 0.f || iy != 0.f || iz != 0.f) {
+            p.x = p.x - box.L.x * ix;
+            p.y = p.y - box.L.y * iy;
+            p.z = p.z - box.L.z * iz;
+        }
+        A.xs2[d] = p;
+    } else {
+        A.xs2[d] = A.xs[s];
+    }
     A.vs2[d] = A.vs[s];
     A.fs2[d] = A.fs[s];
     A.qs2[d] = A.qs[s];
@@ -683,7 +698,9 @@ __device__ __forceinline__ float4 wrap_pos(const Box &box, float4 p, bool &moved
     return p;
 }
 
-// every site wrapped into the box; the molecule binned by its site 0
+// site 0 wrapped into the box (periodicWrap's formula), the other sites put
+// at their minimum-image offset from it, so every molecule is stored whole
+// (as SETTLE leaves it after every step); the molecule binned by its site 0
 __global__ void k_mf_wrap_bin(const MolGridArgs M) {
     pdl_wait();
     if (!M.st->rebuild) return;
@@ -691,13 +708,16 @@ __global__ void k_mf_wrap_bin(const MolGridArgs M) {
     if (m >= M.nmol) return;
     const int4 ix = M.mol_idx[m];
     const int at[4] = {ix.x, ix.y, ix.z, ix.w};
-    float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f);
+    bool moved;
+    const float4 r0 = M.xs[at[0]];
+    const float4 p0 = wrap_pos(M.box, r0, moved);
+    if (moved) M.xs[at[0]] = p0;
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-        bool moved;
-        const float4 p = wrap_pos(M.box, M.xs[at[k]], moved);
-        if (moved) M.xs[at[k]] = p;
-        if (k == 0) p0 = p;
+    for (int k = 1; k < 4; k++) {
+        const float4 r = M.xs[at[k]];
+        const float3 d = min_image(M.box, f3(r) - f3(r0));
+        const float4 p = make_float4(p0.x + d.x, p0.y + d.y, p0.z + d.z, r.w);
+        if (p.x != r.x || p.y != r.y || p.z != r.z) M.xs[at[k]] = p;
     }
     const int c = cell_of_pos(M.g, f3(p0));
     M.cell_of[m] = c;
@@ -1397,6 +1417,9 @@ int molform_init(State &s) {
     const double cut = pair_cut + s.padding + 2.0 * dmax;
     const double Lmin = std::min(s.box.Ld.x, std::min(s.box.Ld.y, s.box.Ld.z));
     if (2.0 * cut >= Lmin) return refuse("the molecule list radius must stay below half the box");
+    // a site pair within the pair cutoff lies within pair_cut + 4 dmax under
+    // the site-0 image shift, which must be the unique image within L/2
+    if (2.0 * (pair_cut + 4.0 * dmax) >= Lmin) return refuse("box too small for one image shift per molecule pair");
     if (2.0 * dmax >= (double)gr.cut) return refuse("a molecule must lie within the neighbour cutoff");
     // cells >= cut / m with at least 2m + 1 per side; the finest such grid
     // that keeps a mean of two molecules per cell
@@ -1415,12 +1438,7 @@ int molform_init(State &s) {
     mf.dmax = (float)dmax;
     mf.cut = (float)cut;
     mf.far = (float)(pair_cut + 2.0 * dmax);
-    if (s.nThreadPerMolecule != 0 && s.nThreadPerMolecule != 8 && s.nThreadPerMolecule != 16 &&
-        s.nThreadPerMolecule != 32) {
-        set_error(MDX_ERR_ARG, "nThreadPerMolecule must be 0 (automatic), 8, 16 or 32 (got %d)", s.nThreadPerMolecule);
-        return MDX_ERR_ARG;
-    }
-    mf.team = s.nThreadPerMolecule ? s.nThreadPerMolecule : 16;
+    mf.team = 32;  // one warp per molecule in the pair kernel: each row is contiguous
     const double vol = s.box.Ld.x * s.box.Ld.y * s.box.Ld.z;
     const double nbar = nmol / vol * 4.18879 * cut * cut * cut;
     mf.cap = ((int)(1.5 * nbar + 64) + mf.team - 1) / mf.team * mf.team;

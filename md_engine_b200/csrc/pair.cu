@@ -370,18 +370,25 @@ PairArgs make_args(State &s, FixPair &f) {
 }
 
 // ---- molecule form (all-rigid four-site water) ---------------------------
-// One team of T lanes per molecule slot k (sites at 4k .. 4k+3) walks k's
-// molecule-pair list; for each listed slot j the four site positions are one
-// 64-byte gather, and every site pair (a of k, b of j) that can interact
-// (bit 4a+b of the LJ / charge masks: eps(a,b) != 0, q_a q_b != 0) is
-// evaluated as compute_force_iso evaluates a listed pair: minimum image per
-// site pair, LJ/WCA when r^2 < rc^2(a,b), Ewald real space when r^2 < qrc^2.
-// A molecule pair whose site-0 distance is beyond `far` has no site pair
-// within the cutoffs and is skipped.  The molecule's own site pairs (the
-// excluded pairs of the reference's list, multiplier by exclusion depth) are
-// added by the team's first lane.  Forces on the four sites are reduced over
-// the team by shuffles and written by lanes 0..3 (one 64-byte store).
+// One warp per molecule slot k (sites at 4k .. 4k+3, stored whole) walks k's
+// molecule-pair list in two phases per 32 entries:
+//  * filter: each lane takes one entry j, gathers its site 0 and forms the
+//    minimum-image shift of the site-0 pair; entries whose site-0 distance is
+//    within `far` (beyond it no site pair is within the cutoffs) are
+//    compacted by ballot into a per-warp queue in shared memory;
+//  * evaluate: whenever 32 entries are queued, each lane takes one and
+//    evaluates every site pair (a of k, b of j) that can interact (bit 4a+b
+//    of the LJ / charge masks: eps(a,b) != 0, q_a q_b != 0) as
+//    compute_force_iso evaluates a listed pair -- LJ/WCA when
+//    r^2 < rc^2(a,b), Ewald real space when r^2 < qrc^2 -- with the one
+//    shift of the molecule pair (molecules are whole and a pair within the
+//    cutoff is within L/2 under it, so it is the pair's minimum image) and
+//    the cutoffs applied as masks, not branches: all lanes run one path.
+// The molecule's own site pairs (the excluded pairs of the reference's list,
+// multiplier by exclusion depth) are added by lane 0.  Forces on the four
+// sites are reduced by shuffles and written by lanes 0..3 (one 64-byte store).
 constexpr int kMolPairBlock = 64;
+constexpr int kMolQueue = 64;  // queued entries per warp (two chunks)
 
 struct MolPairArgs {
     int nmol;
@@ -400,52 +407,10 @@ struct MolPairArgs {
     float *__restrict__ energy;  // per site (energy kernel)
 };
 
-template <int T>
-__device__ __forceinline__ float3 team_sum3(float3 v) {
-    return make_float3(team_sum<T>(v.x), team_sum<T>(v.y), team_sum<T>(v.z));
-}
-
-// site pair ab at r2 with multiplier mult (1 between molecules; own pairs
-// carry their exclusion multiplier and the Ewald correction for the excluded
-// part, ChargeEvaluatorEwald.h:11-64): scalar force factor s (F = dr s) and
-// half the pair energy e; returns whether a term was in range
-template <int LJ, bool EW, bool ENERGY, bool OWN>
-__device__ __forceinline__ bool mol_pair_term(const MolPairArgs &A, int ab, float r2, float mult, float &s, float &e) {
-    bool any = false;
-    s = 0.f;
-    e = 0.f;
-    if (LJ && ((A.ljm >> ab) & 1u) && r2 < A.rc2[ab]) {
-        any = true;
-        if (!OWN || mult != 0.f) {
-            const float r2inv = 1.0f / r2;
-            const float r6inv = r2inv * r2inv * r2inv;
-            s += r6inv * r2inv * (A.p1[ab] * r6inv - A.p2[ab]) * (OWN ? mult : 1.0f);
-            if (ENERGY) {
-                const float s6r6 = A.sig6[ab] * r6inv;
-                const float m = OWN ? mult : 1.0f;
-                if (LJ == 1) e += 0.5f * 4.0f * A.eps[ab] * (s6r6 * (s6r6 - 1.0f) - A.eoff[ab]) * m;
-                else e += 0.5f * (4.0f * A.eps[ab] * s6r6 * (s6r6 - 1.0f) + A.eps[ab]) * m;
-            }
-        }
-    }
-    if (EW && ((A.qm >> ab) & 1u) && r2 < A.qrc2) {
-        any = true;
-        const float r2c = r2 < 1e-10f ? 1e-10f : r2;
-        const float rinv = rsqrtf(r2c);
-        const float x = A.alpha * (r2c * rinv);
-        const float expm = __expf(-x * x);
-        const float erfcv = erfc_as(x, expm);
-        const float qq = A.qq[ab];
-        float fsc = qq * (erfcv * rinv + (2.0f * 0.5641895835477563f * A.alpha) * expm);
-        if (OWN && mult < 1.0f) fsc -= (1.0f - mult) * qq * rinv;
-        s += fsc * (rinv * rinv);
-        if (ENERGY) {
-            float eng = qq * rinv * erfcv;
-            if (OWN && mult < 1.0f) eng -= (1.0f - mult) * qq * rinv;
-            e += 0.5f * eng;
-        }
-    }
-    return any;
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
 }
 
 template <bool VIR>
@@ -460,21 +425,86 @@ __device__ __forceinline__ void add_vir(float (&v)[6], float3 F, float3 dr) {
     }
 }
 
-template <int T, int LJ, bool EW, bool VIR, bool ENERGY>
+// site pair ab at r2, multiplier mult (1 between molecules; own pairs carry
+// their exclusion multiplier and the Ewald correction of the excluded part,
+// ChargeEvaluatorEwald.h:11-64): scalar force factor (F = dr s) and half the
+// pair energy, cutoffs applied as masks
+template <int LJ, bool EW, bool ENERGY, bool OWN>
+__device__ __forceinline__ float mol_pair_term(const MolPairArgs &A, int ab, float r2, float mult, float &e) {
+    float s = 0.f;
+    e = 0.f;
+    if (LJ && ((A.ljm >> ab) & 1u)) {
+        const float in = (r2 < A.rc2[ab] && (!OWN || mult != 0.f)) ? (OWN ? mult : 1.0f) : 0.f;
+        const float r2inv = 1.0f / r2;
+        const float r6inv = r2inv * r2inv * r2inv;
+        s += r6inv * r2inv * (A.p1[ab] * r6inv - A.p2[ab]) * in;
+        if (ENERGY) {
+            const float s6r6 = A.sig6[ab] * r6inv;
+            if (LJ == 1) e += 0.5f * 4.0f * A.eps[ab] * (s6r6 * (s6r6 - 1.0f) - A.eoff[ab]) * in;
+            else e += 0.5f * (4.0f * A.eps[ab] * s6r6 * (s6r6 - 1.0f) + A.eps[ab]) * in;
+        }
+    }
+    if (EW && ((A.qm >> ab) & 1u)) {
+        const float r2c = fmaxf(r2, 1e-10f);
+        const float rinv = rsqrtf(r2c);
+        const float x = A.alpha * (r2c * rinv);
+        const float expm = __expf(-x * x);
+        const float erfcv = erfc_as(x, expm);
+        const float qq = A.qq[ab];
+        float fsc = qq * (erfcv * rinv + (2.0f * 0.5641895835477563f * A.alpha) * expm);
+        if (OWN && mult < 1.0f) fsc -= (1.0f - mult) * qq * rinv;
+        const float in = r2 < A.qrc2 ? 1.0f : 0.f;
+        s += fsc * (rinv * rinv) * in;
+        if (ENERGY) {
+            float eng = qq * rinv * erfcv;
+            if (OWN && mult < 1.0f) eng -= (1.0f - mult) * qq * rinv;
+            e += 0.5f * eng * in;
+        }
+    }
+    return s;
+}
+
+// one queued molecule pair: every interacting site pair of slot k (sites
+// xi, the shift already taken off) and slot j
+template <int LJ, bool EW, bool VIR, bool ENERGY>
+__device__ __forceinline__ void mol_pair_eval(const MolPairArgs &A, const float3 (&xi)[4], int j, float3 shift,
+                                              float3 (&f)[4], float (&en)[4], float (&v)[4][6]) {
+    float3 xj[4];
+#pragma unroll
+    for (int b = 0; b < 4; b++) xj[b] = f3(__ldg(A.xs + 4 * j + b));
+    const uint32_t any = (LJ ? A.ljm : 0u) | (EW ? A.qm : 0u);
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+        if (!((any >> (4 * a)) & 15u)) continue;
+        const float3 xa = xi[a] - shift;
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+            const int ab = 4 * a + b;
+            if (!((any >> ab) & 1u)) continue;
+            const float3 dr = xa - xj[b];
+            const float r2 = dot3(dr, dr);
+            float e;
+            const float sc = mol_pair_term<LJ, EW, ENERGY, false>(A, ab, r2, 1.0f, e);
+            const float3 F = dr * sc;
+            f[a] += F;
+            if (ENERGY) en[a] += e;
+            add_vir<VIR>(v[a], F, dr);
+        }
+    }
+}
+
+template <int LJ, bool EW, bool VIR, bool ENERGY>
 __global__ void __launch_bounds__(kMolPairBlock) k_pair_mol(const MolPairArgs A, int accumulate) {
     pdl_wait();
-    constexpr int G = 32 / T;
-    constexpr int U = 2;  // list entries in flight per lane
-    constexpr uint32_t kNone = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int slot = lane / T, t = lane % T;
-    const int k = warp * G + slot;
-    const bool valid = k < A.nmol;
-    float3 xi[4];
-    float3 f[4];
-    float en[4];
-    float v[4][6];
+    __shared__ int q_j[kMolPairBlock / 32][kMolQueue];
+    __shared__ float4 q_s[kMolPairBlock / 32][kMolQueue];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const bool valid = k < A.nmol;  // warp-uniform
+    int *const qj = q_j[wib];
+    float4 *const qs = q_s[wib];
+    float3 xi[4], f[4];
+    float en[4], v[4][6];
 #pragma unroll
     for (int a = 0; a < 4; a++) {
         xi[a] = make_float3(0.f, 0.f, 0.f);
@@ -490,87 +520,84 @@ __global__ void __launch_bounds__(kMolPairBlock) k_pair_mol(const MolPairArgs A,
         for (int a = 0; a < 4; a++) xi[a] = f3(A.xs[4 * k + a]);
         cnt = (int)A.counts[k];
         cnt = cnt < A.cap ? cnt : A.cap;
-        row = A.list + (size_t)(k / G) * A.cap * G + slot * T + t;
+        row = A.list + (size_t)k * A.cap;
     }
-    const uint32_t any_mask = (LJ ? A.ljm : 0u) | (EW ? A.qm : 0u);
-    for (int e0 = t; e0 < cnt; e0 += U * T) {
-        uint32_t ent[U];
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-            const int e = e0 + u * T;
-            ent[u] = e < cnt ? __ldg(row + (size_t)(e / T) * 32) : kNone;
+    const uint32_t lt = (1u << lane) - 1u;
+    int nq = 0;  // queued entries (warp-uniform)
+    for (int base = 0; base < cnt; base += 32) {
+        const int e = base + lane;
+        bool pass = false;
+        int j = 0;
+        float3 sh = make_float3(0.f, 0.f, 0.f);
+        if (e < cnt) {
+            j = (int)__ldg(row + e);
+            const float3 d = xi[0] - f3(__ldg(A.xs + 4 * j));
+            sh = make_float3(A.box.L.x * rintf(d.x * A.box.invL.x), A.box.L.y * rintf(d.y * A.box.invL.y),
+                             A.box.L.z * rintf(d.z * A.box.invL.z));
+            const float3 dm = d - sh;
+            pass = dot3(dm, dm) < A.far2;
         }
-        float3 xj[U][4];
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-            const int j = ent[u] == kNone ? k : (int)ent[u];
-#pragma unroll
-            for (int b = 0; b < 4; b++) xj[u][b] = f3(__ldg(A.xs + 4 * j + b));
+        const uint32_t bal = __ballot_sync(0xffffffffu, pass);
+        if (pass) {
+            const int pos = nq + __popc(bal & lt);
+            qj[pos] = j;
+            qs[pos] = make_float4(sh.x, sh.y, sh.z, 0.f);
         }
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-            if (ent[u] == kNone) continue;
-            const float3 d00 = min_image(A.box, xi[0] - xj[u][0]);
-            const float r00 = dot3(d00, d00);
-            if (r00 >= A.far2) continue;
-#pragma unroll
-            for (int a = 0; a < 4; a++) {
-#pragma unroll
-                for (int b = 0; b < 4; b++) {
-                    const int ab = 4 * a + b;
-                    if (!((any_mask >> ab) & 1u)) continue;
-                    const float3 dr = ab == 0 ? d00 : min_image(A.box, xi[a] - xj[u][b]);
-                    const float r2 = ab == 0 ? r00 : dot3(dr, dr);
-                    float sc, e;
-                    if (mol_pair_term<LJ, EW, ENERGY, false>(A, ab, r2, 1.0f, sc, e)) {
-                        const float3 F = dr * sc;
-                        f[a] += F;
-                        if (ENERGY) en[a] += e;
-                        add_vir<VIR>(v[a], F, dr);
-                    }
-                }
+        nq += __popc(bal);
+        __syncwarp();
+        if (nq >= 32) {
+            const float4 s4 = qs[lane];
+            mol_pair_eval<LJ, EW, VIR, ENERGY>(A, xi, qj[lane], make_float3(s4.x, s4.y, s4.z), f, en, v);
+            __syncwarp();
+            nq -= 32;
+            if (lane < nq) {
+                qj[lane] = qj[32 + lane];
+                qs[lane] = qs[32 + lane];
             }
+            __syncwarp();
         }
+    }
+    if (lane < nq) {
+        const float4 s4 = qs[lane];
+        mol_pair_eval<LJ, EW, VIR, ENERGY>(A, xi, qj[lane], make_float3(s4.x, s4.y, s4.z), f, en, v);
     }
     // the molecule's own site pairs, once per molecule
-    if (valid && t == 0 && A.selfm) {
+    if (valid && lane == 0 && A.selfm) {
 #pragma unroll
         for (int a = 0; a < 4; a++) {
 #pragma unroll
             for (int b = 0; b < 4; b++) {
                 const int ab = 4 * a + b;
                 if (a == b || !((A.selfm >> ab) & 1u)) continue;
-                const float3 dr = min_image(A.box, xi[a] - xi[b]);
+                const float3 dr = xi[a] - xi[b];  // the molecule is whole
                 const float r2 = dot3(dr, dr);
-                float sc, e;
-                if (mol_pair_term<LJ, EW, ENERGY, true>(A, ab, r2, A.mult[ab], sc, e)) {
-                    const float3 F = dr * sc;
-                    f[a] += F;
-                    if (ENERGY) en[a] += e;
-                    add_vir<VIR>(v[a], F, dr);
-                }
+                float e;
+                const float sc = mol_pair_term<LJ, EW, ENERGY, true>(A, ab, r2, A.mult[ab], e);
+                const float3 F = dr * sc;
+                f[a] += F;
+                if (ENERGY) en[a] += e;
+                add_vir<VIR>(v[a], F, dr);
             }
         }
     }
     pdl_trigger();
-    // team sums; lane t < 4 of the team writes site t
     if (ENERGY) {
 #pragma unroll
-        for (int a = 0; a < 4; a++) en[a] = team_sum<T>(en[a]);
-        if (valid && t < 4) A.energy[4 * k + t] = t == 0 ? en[0] : (t == 1 ? en[1] : (t == 2 ? en[2] : en[3]));
+        for (int a = 0; a < 4; a++) en[a] = warp_sum(en[a]);
+        if (valid && lane < 4) A.energy[4 * k + lane] = lane == 0 ? en[0] : (lane == 1 ? en[1] : (lane == 2 ? en[2] : en[3]));
         return;
     }
 #pragma unroll
-    for (int a = 0; a < 4; a++) f[a] = team_sum3<T>(f[a]);
+    for (int a = 0; a < 4; a++) f[a] = make_float3(warp_sum(f[a].x), warp_sum(f[a].y), warp_sum(f[a].z));
     if (VIR) {
 #pragma unroll
         for (int a = 0; a < 4; a++)
 #pragma unroll
-            for (int c = 0; c < 6; c++) v[a][c] = team_sum<T>(v[a][c]);
+            for (int c = 0; c < 6; c++) v[a][c] = warp_sum(v[a][c]);
     }
-    if (valid && t < 4) {
-        const float3 fm = t == 0 ? f[0] : (t == 1 ? f[1] : (t == 2 ? f[2] : f[3]));
-        float4 fo = A.fs[4 * k + t];
+    if (valid && lane < 4) {
+        const float3 fm = lane == 0 ? f[0] : (lane == 1 ? f[1] : (lane == 2 ? f[2] : f[3]));
+        float4 fo = A.fs[4 * k + lane];
         if (accumulate) {
             fo.x += fm.x;
             fo.y += fm.y;
@@ -580,12 +607,12 @@ __global__ void __launch_bounds__(kMolPairBlock) k_pair_mol(const MolPairArgs A,
             fo.y = fm.y;
             fo.z = fm.z;
         }
-        A.fs[4 * k + t] = fo;
+        A.fs[4 * k + lane] = fo;
         if (VIR) {
-            float *vv = A.virials + 6 * (size_t)(4 * k + t);
+            float *vv = A.virials + 6 * (size_t)(4 * k + lane);
 #pragma unroll
             for (int c = 0; c < 6; c++) {
-                const float vm = t == 0 ? v[0][c] : (t == 1 ? v[1][c] : (t == 2 ? v[2][c] : v[3][c]));
+                const float vm = lane == 0 ? v[0][c] : (lane == 1 ? v[1][c] : (lane == 2 ? v[2][c] : v[3][c]));
                 vv[c] += 0.5f * vm;
             }
         }
@@ -642,28 +669,18 @@ MolPairArgs make_mol_args(State &s, FixPair &f) {
     return A;
 }
 
-template <int T, int LJ, bool EW>
+template <int LJ, bool EW>
 void mol_launch_t(const MolPairArgs &A, int virialMode, bool energy, bool accumulate, cudaStream_t st) {
-    const int warps = (A.nmol + 32 / T - 1) / (32 / T);
-    const dim3 blocks((warps * 32 + kMolPairBlock - 1) / kMolPairBlock);
+    const dim3 blocks((A.nmol * 32 + kMolPairBlock - 1) / kMolPairBlock);
     if (energy) {
-        k_pair_mol<T, LJ, EW, false, true><<<blocks, kMolPairBlock, 0, st>>>(A, 0);
+        k_pair_mol<LJ, EW, false, true><<<blocks, kMolPairBlock, 0, st>>>(A, 0);
         MDX_LAUNCHED();
     } else if (virialMode == 1 || virialMode == 2) {
-        k_pair_mol<T, LJ, EW, true, false><<<blocks, kMolPairBlock, 0, st>>>(A, accumulate ? 1 : 0);
+        k_pair_mol<LJ, EW, true, false><<<blocks, kMolPairBlock, 0, st>>>(A, accumulate ? 1 : 0);
         MDX_LAUNCHED();
     } else {
-        launch_pdl(k_pair_mol<T, LJ, EW, false, false>, blocks, dim3(kMolPairBlock), 0, st, A, accumulate ? 1 : 0);
+        launch_pdl(k_pair_mol<LJ, EW, false, false>, blocks, dim3(kMolPairBlock), 0, st, A, accumulate ? 1 : 0);
     }
-}
-
-template <int T>
-void mol_launch_kind(const MolPairArgs &A, int lj, bool ew, int virialMode, bool energy, bool accumulate,
-                     cudaStream_t st) {
-    if (lj == 1 && ew) mol_launch_t<T, 1, true>(A, virialMode, energy, accumulate, st);
-    else if (lj == 1) mol_launch_t<T, 1, false>(A, virialMode, energy, accumulate, st);
-    else if (ew) mol_launch_t<T, 2, true>(A, virialMode, energy, accumulate, st);
-    else mol_launch_t<T, 2, false>(A, virialMode, energy, accumulate, st);
 }
 
 }  // namespace
@@ -686,12 +703,10 @@ int pair_mol_launch(State &s, FixPair &f, int virialMode, bool accumulate, float
         set_error(MDX_ERR_ARG, "pair kind %d", f.lj_kind);
         return MDX_ERR_ARG;
     }
-    switch (s.mf.team) {
-        case 8: mol_launch_kind<8>(A, f.lj_kind, ew, virialMode, en, accumulate, st); break;
-        case 16: mol_launch_kind<16>(A, f.lj_kind, ew, virialMode, en, accumulate, st); break;
-        case 32: mol_launch_kind<32>(A, f.lj_kind, ew, virialMode, en, accumulate, st); break;
-        default: set_error(MDX_ERR_ARG, "lanes per molecule %d not in {8, 16, 32}", s.mf.team); return MDX_ERR_ARG;
-    }
+    if (f.lj_kind == 1 && ew) mol_launch_t<1, true>(A, virialMode, en, accumulate, st);
+    else if (f.lj_kind == 1) mol_launch_t<1, false>(A, virialMode, en, accumulate, st);
+    else if (ew) mol_launch_t<2, true>(A, virialMode, en, accumulate, st);
+    else mol_launch_t<2, false>(A, virialMode, en, accumulate, st);
     return 0;
 }
 

@@ -101,7 +101,7 @@ class State:
 
     _DOUBLE_KEYS = ("rCut", "padding", "dt")
     _INT_KEYS = ("periodicInterval", "nThreadPerAtom", "nThreadPerBlock", "gridStencil", "gridHomeGroup", "turn",
-                 "pairForm", "nThreadPerMolecule")
+                 "pairForm")
 
     def __init__(self):
         h = c_void_p()
@@ -217,9 +217,10 @@ class State:
     def getNeighborList(self, maxPerAtom=None):
         """Grid.getNeighborList: (counts[id], ids[id, k], tags[id, k]) sorted per id."""
         n = self.nAtoms
-        if maxPerAtom is None:
-            maxPerAtom = max(int(self.nlistCapacity), 1)
         c = np.zeros(n, np.int32)
+        if maxPerAtom is None:
+            check(lib().mdx_nlist_get(self._h, 0, c.ctypes.data_as(P(c_int)), None, None))
+            maxPerAtom = max(int(c.max()) if n else 0, 1)
         nb = np.zeros((n, maxPerAtom), np.int32)
         tg = np.zeros((n, maxPerAtom), np.int32)
         check(lib().mdx_nlist_get(self._h, maxPerAtom, c.ctypes.data_as(P(c_int)), nb.ctypes.data_as(P(c_int)),

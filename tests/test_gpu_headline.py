@@ -154,22 +154,20 @@ def test_every_neighbour_team_matches_oracle(oracle, team):
     assert rel < FORCE_RTOL, f"team {team}: max force error {rel:.3e} of RMS {rms:.3e}"
 
 
-@pytest.mark.parametrize("team", [8, 16, 32])
-def test_molecule_form_teams_match_per_site_form(oracle, team):
+@pytest.mark.parametrize("e3b", [False, True])
+def test_molecule_form_matches_per_site_form(oracle, e3b):
     """The molecule form (molecule-pair list, every site pair of a listed
-    molecule pair) against the per-site form on the same positions, for each
-    lane count per molecule; both against the FP64 oracle; energies and
-    virials too"""
+    molecule pair, one warp per molecule) against the per-site form on the
+    same positions: forces, energies and virials (both FP32)"""
     from tests.helpers import water_small
     sysd = water_small(seed=23)
     rc = 6.5
     res = {}
     x0 = None
     for form in (1, 2):
-        st, fx = systems.build_water_state(sysd, rcut=rc, skin=1.0, grid=32, alpha=0.35, e3b=True,
+        st, fx = systems.build_water_state(sysd, rcut=rc, skin=1.0, grid=32, alpha=0.35, e3b=e3b,
                                            thermostat=False)
         st.pairForm = form
-        st.nThreadPerMolecule = team
         st.prepare()
         if x0 is None:
             x0, _, _ = st.getAtoms()

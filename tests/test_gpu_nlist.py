@@ -17,11 +17,17 @@ def _compare(O, st, sysd, rcut, padding, excl=None):
     x_pre, _, _ = st.getAtoms()
     st.buildNeighborlists(force=True)
     x, _, _ = st.getAtoms()
-    # the device wrapped the float32 positions in place: same as the oracle's wrap
+    # the list is built on the wrapped float32 positions: the oracle's wrap of
+    # the positions before and after the rebuild agree (the per-site form
+    # wraps every atom in place; the molecule form keeps molecules whole and
+    # wraps the per-site list's own sorted copy)
     xs4 = np.zeros((len(x_pre), 4), np.float32)
     xs4[:, :3] = np.asarray(x_pre, np.float32)
     O.wrap_f32(xs4, sysd.lo, sysd.L)
-    assert np.array_equal(xs4[:, :3].astype(np.float64), x), "periodic wrap differs"
+    xw = np.zeros((len(x), 4), np.float32)
+    xw[:, :3] = np.asarray(x, np.float32)
+    O.wrap_f32(xw, sysd.lo, sysd.L)
+    assert np.array_equal(xs4[:, :3], xw[:, :3]), "periodic wrap differs"
     cut = neighbor_cut(rcut, padding)
     counts_o, nbr_o = oracle_nlist_for(O, xs4[:, :3], sysd.lo, sysd.L, cut,
                                        ids=np.arange(len(x)), excl=excl)
