@@ -78,6 +78,27 @@ __host__ __device__ inline double3 crossd(double3 a, double3 b) {
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
+// Single-instruction approximations (PTX ISA rsqrt/ex2/rcp .approx.ftz): the
+// hot loops' arguments are normal floats, so flushing denormals changes no
+// result while it drops the range handling of the non-ftz forms.
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float ex2_ftz(float x) {
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float rcp_ftz(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+// exp(-x^2) as 2^(-x^2 log2 e)
+__device__ __forceinline__ float exp_neg_sq(float x) { return ex2_ftz(-(x * x) * 1.4426950408889634f); }
+
 // minimum image (BoundsGPU::minImage, BoundsGPU.h:91-108)
 __device__ inline float3 min_image(const Box &b, float3 v) {
     v.x -= b.L.x * rintf(v.x * b.invL.x);

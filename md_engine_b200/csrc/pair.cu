@@ -61,7 +61,7 @@ struct PairArgs {
 __device__ __forceinline__ float erfc_as(float x, float expmx2) {
     // t only feeds the A&S polynomial (error 1.5e-7): the approximate
     // reciprocal (one SFU op, a few ulp) is plenty
-    const float t = __fdividef(1.0f, fmaf(0.3275911f, x, 1.0f));
+    const float t = rcp_ftz(fmaf(0.3275911f, x, 1.0f));
     float poly = fmaf(t, 1.061405429f, -1.453152027f);
     poly = fmaf(t, poly, 1.421413741f);
     poly = fmaf(t, poly, -0.284496736f);
@@ -111,10 +111,10 @@ __device__ __forceinline__ bool pair_term(const PairArgs &A, const float *sp, in
         if (r2 < A.qrc2 && qi * qj != 0.f) {
             any = true;
             const float r2c = r2 < 1e-10f ? 1e-10f : r2;
-            const float rinv = rsqrtf(r2c);
+            const float rinv = rsqrt_ftz(r2c);
             const float r2inv = rinv * rinv;
             const float x = A.alpha * (r2c * rinv);  // alpha r
-            const float expm = __expf(-x * x);       // exp(-alpha^2 r^2), as the reference's __expf
+            const float expm = exp_neg_sq(x);        // exp(-alpha^2 r^2) (the reference: __expf)
             const float qq = A.qqr * qi * qj;
             const float erfcv = erfc_as(x, expm);
             float fsc = qq * (erfcv * rinv + (2.0f * 0.5641895835477563f * A.alpha) * expm);
@@ -429,13 +429,25 @@ __device__ __forceinline__ void add_vir(float (&v)[6], float3 F, float3 dr) {
 // their exclusion multiplier and the Ewald correction of the excluded part,
 // ChargeEvaluatorEwald.h:11-64): scalar force factor (F = dr s) and half the
 // pair energy, cutoffs applied as masks
-template <int LJ, bool EW, bool ENERGY, bool OWN>
+// TOPO 1: the four-site water pattern known at compile time -- LJ between
+// the sites 0 only, charges on sites 1..3 only (ljm = 0x1, qm = 0xEEE0);
+// TOPO 0: any pattern, from the runtime masks
+template <int TOPO>
+__device__ __forceinline__ bool topo_lj(const MolPairArgs &A, int ab) {
+    return TOPO == 1 ? ab == 0 : ((A.ljm >> ab) & 1u) != 0u;
+}
+template <int TOPO>
+__device__ __forceinline__ bool topo_q(const MolPairArgs &A, int ab) {
+    return TOPO == 1 ? (ab / 4 != 0 && ab % 4 != 0) : ((A.qm >> ab) & 1u) != 0u;
+}
+
+template <int LJ, bool EW, bool ENERGY, bool OWN, int TOPO>
 __device__ __forceinline__ float mol_pair_term(const MolPairArgs &A, int ab, float r2, float mult, float &e) {
     float s = 0.f;
     e = 0.f;
-    if (LJ && ((A.ljm >> ab) & 1u)) {
+    if (LJ && topo_lj<TOPO>(A, ab)) {
         const float in = (r2 < A.rc2[ab] && (!OWN || mult != 0.f)) ? (OWN ? mult : 1.0f) : 0.f;
-        const float r2inv = 1.0f / r2;
+        const float r2inv = rcp_ftz(r2);
         const float r6inv = r2inv * r2inv * r2inv;
         s += r6inv * r2inv * (A.p1[ab] * r6inv - A.p2[ab]) * in;
         if (ENERGY) {
@@ -444,11 +456,11 @@ __device__ __forceinline__ float mol_pair_term(const MolPairArgs &A, int ab, flo
             else e += 0.5f * (4.0f * A.eps[ab] * s6r6 * (s6r6 - 1.0f) + A.eps[ab]) * in;
         }
     }
-    if (EW && ((A.qm >> ab) & 1u)) {
+    if (EW && topo_q<TOPO>(A, ab)) {
         const float r2c = fmaxf(r2, 1e-10f);
-        const float rinv = rsqrtf(r2c);
+        const float rinv = rsqrt_ftz(r2c);
         const float x = A.alpha * (r2c * rinv);
-        const float expm = __expf(-x * x);
+        const float expm = exp_neg_sq(x);
         const float erfcv = erfc_as(x, expm);
         const float qq = A.qq[ab];
         float fsc = qq * (erfcv * rinv + (2.0f * 0.5641895835477563f * A.alpha) * expm);
@@ -466,13 +478,13 @@ __device__ __forceinline__ float mol_pair_term(const MolPairArgs &A, int ab, flo
 
 // one queued molecule pair: every interacting site pair of slot k (sites
 // xi, the shift already taken off) and slot j
-template <int LJ, bool EW, bool VIR, bool ENERGY>
+template <int LJ, bool EW, bool VIR, bool ENERGY, int TOPO>
 __device__ __forceinline__ void mol_pair_eval(const MolPairArgs &A, const float3 (&xi)[4], int j, float3 shift,
                                               float3 (&f)[4], float (&en)[4], float (&v)[4][6]) {
     float3 xj[4];
 #pragma unroll
     for (int b = 0; b < 4; b++) xj[b] = f3(__ldg(A.xs + 4 * j + b));
-    const uint32_t any = (LJ ? A.ljm : 0u) | (EW ? A.qm : 0u);
+    const uint32_t any = TOPO == 1 ? 0xEEE1u : ((LJ ? A.ljm : 0u) | (EW ? A.qm : 0u));
 #pragma unroll
     for (int a = 0; a < 4; a++) {
         if (!((any >> (4 * a)) & 15u)) continue;
@@ -484,7 +496,7 @@ __device__ __forceinline__ void mol_pair_eval(const MolPairArgs &A, const float3
             const float3 dr = xa - xj[b];
             const float r2 = dot3(dr, dr);
             float e;
-            const float sc = mol_pair_term<LJ, EW, ENERGY, false>(A, ab, r2, 1.0f, e);
+            const float sc = mol_pair_term<LJ, EW, ENERGY, false, TOPO>(A, ab, r2, 1.0f, e);
             const float3 F = dr * sc;
             f[a] += F;
             if (ENERGY) en[a] += e;
@@ -493,7 +505,7 @@ __device__ __forceinline__ void mol_pair_eval(const MolPairArgs &A, const float3
     }
 }
 
-template <int LJ, bool EW, bool VIR, bool ENERGY>
+template <int LJ, bool EW, bool VIR, bool ENERGY, int TOPO>
 __global__ void __launch_bounds__(kMolPairBlock) k_pair_mol(const MolPairArgs A, int accumulate) {
     pdl_wait();
     __shared__ int q_j[kMolPairBlock / 32][kMolQueue];
@@ -547,7 +559,7 @@ __global__ void __launch_bounds__(kMolPairBlock) k_pair_mol(const MolPairArgs A,
         __syncwarp();
         if (nq >= 32) {
             const float4 s4 = qs[lane];
-            mol_pair_eval<LJ, EW, VIR, ENERGY>(A, xi, qj[lane], make_float3(s4.x, s4.y, s4.z), f, en, v);
+            mol_pair_eval<LJ, EW, VIR, ENERGY, TOPO>(A, xi, qj[lane], make_float3(s4.x, s4.y, s4.z), f, en, v);
             __syncwarp();
             nq -= 32;
             if (lane < nq) {
@@ -559,7 +571,7 @@ __global__ void __launch_bounds__(kMolPairBlock) k_pair_mol(const MolPairArgs A,
     }
     if (lane < nq) {
         const float4 s4 = qs[lane];
-        mol_pair_eval<LJ, EW, VIR, ENERGY>(A, xi, qj[lane], make_float3(s4.x, s4.y, s4.z), f, en, v);
+        mol_pair_eval<LJ, EW, VIR, ENERGY, TOPO>(A, xi, qj[lane], make_float3(s4.x, s4.y, s4.z), f, en, v);
     }
     // the molecule's own site pairs, once per molecule
     if (valid && lane == 0 && A.selfm) {
@@ -572,7 +584,7 @@ __global__ void __launch_bounds__(kMolPairBlock) k_pair_mol(const MolPairArgs A,
                 const float3 dr = xi[a] - xi[b];  // the molecule is whole
                 const float r2 = dot3(dr, dr);
                 float e;
-                const float sc = mol_pair_term<LJ, EW, ENERGY, true>(A, ab, r2, A.mult[ab], e);
+                const float sc = mol_pair_term<LJ, EW, ENERGY, true, 0>(A, ab, r2, A.mult[ab], e);
                 const float3 F = dr * sc;
                 f[a] += F;
                 if (ENERGY) en[a] += e;
@@ -669,17 +681,18 @@ MolPairArgs make_mol_args(State &s, FixPair &f) {
     return A;
 }
 
-template <int LJ, bool EW>
+template <int LJ, bool EW, int TOPO>
 void mol_launch_t(const MolPairArgs &A, int virialMode, bool energy, bool accumulate, cudaStream_t st) {
     const dim3 blocks((A.nmol * 32 + kMolPairBlock - 1) / kMolPairBlock);
     if (energy) {
-        k_pair_mol<LJ, EW, false, true><<<blocks, kMolPairBlock, 0, st>>>(A, 0);
+        k_pair_mol<LJ, EW, false, true, TOPO><<<blocks, kMolPairBlock, 0, st>>>(A, 0);
         MDX_LAUNCHED();
     } else if (virialMode == 1 || virialMode == 2) {
-        k_pair_mol<LJ, EW, true, false><<<blocks, kMolPairBlock, 0, st>>>(A, accumulate ? 1 : 0);
+        k_pair_mol<LJ, EW, true, false, TOPO><<<blocks, kMolPairBlock, 0, st>>>(A, accumulate ? 1 : 0);
         MDX_LAUNCHED();
     } else {
-        launch_pdl(k_pair_mol<LJ, EW, false, false>, blocks, dim3(kMolPairBlock), 0, st, A, accumulate ? 1 : 0);
+        launch_pdl(k_pair_mol<LJ, EW, false, false, TOPO>, blocks, dim3(kMolPairBlock), 0, st, A,
+                   accumulate ? 1 : 0);
     }
 }
 
@@ -703,10 +716,15 @@ int pair_mol_launch(State &s, FixPair &f, int virialMode, bool accumulate, float
         set_error(MDX_ERR_ARG, "pair kind %d", f.lj_kind);
         return MDX_ERR_ARG;
     }
-    if (f.lj_kind == 1 && ew) mol_launch_t<1, true>(A, virialMode, en, accumulate, st);
-    else if (f.lj_kind == 1) mol_launch_t<1, false>(A, virialMode, en, accumulate, st);
-    else if (ew) mol_launch_t<2, true>(A, virialMode, en, accumulate, st);
-    else mol_launch_t<2, false>(A, virialMode, en, accumulate, st);
+    // the four-site water pattern (LJ on sites 0, charges on 1..3) as
+    // compile-time masks; any other pattern from the runtime masks
+    const bool water4 = ew && A.ljm == 0x1u && A.qm == 0xEEE0u;
+    if (f.lj_kind == 1 && water4) mol_launch_t<1, true, 1>(A, virialMode, en, accumulate, st);
+    else if (f.lj_kind == 1 && ew) mol_launch_t<1, true, 0>(A, virialMode, en, accumulate, st);
+    else if (f.lj_kind == 1) mol_launch_t<1, false, 0>(A, virialMode, en, accumulate, st);
+    else if (water4) mol_launch_t<2, true, 1>(A, virialMode, en, accumulate, st);
+    else if (ew) mol_launch_t<2, true, 0>(A, virialMode, en, accumulate, st);
+    else mol_launch_t<2, false, 0>(A, virialMode, en, accumulate, st);
     return 0;
 }
 
