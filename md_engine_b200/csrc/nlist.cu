@@ -751,31 +751,26 @@ __global__ void k_mf_rank(const MolGridArgs M) {
 }
 
 // slot d <- molecule perm[d]: its four sites into 4d .. 4d+3 of the
-// alternate streams, idToIdx and the molecule maps rewritten
+// alternate streams and idToIdx rewritten; one thread per site
 __global__ void k_mf_gather(const MolGridArgs M) {
     pdl_wait();
     if (!M.st->rebuild) return;
-    const int d = blockIdx.x * blockDim.x + threadIdx.x;
-    if (d >= M.nmol) return;
-    const int m = M.perm[d];
-    const int4 ix = M.mol_idx[m];
-    const int at[4] = {ix.x, ix.y, ix.z, ix.w};
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const int s = at[k], t = 4 * d + k;
-        M.xs2[t] = M.xs[s];
-        M.vs2[t] = M.vs[s];
-        M.fs2[t] = M.fs[s];
-        M.qs2[t] = M.qs[s];
-        const uint32_t id = M.ids[s];
-        M.ids2[t] = id;
-        M.idToIdx[id] = t;
-    }
-    const int4 nx = make_int4(4 * d, 4 * d + 1, 4 * d + 2, 4 * d + 3);
-    M.mol_idx[m] = nx;
-    if (M.mol_idx_e3b) M.mol_idx_e3b[m] = nx;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 4 * M.nmol) return;
+    const int d = t >> 2, site = t & 3;
+    const int4 ix = M.mol_idx[M.perm[d]];
+    const int s = site == 0 ? ix.x : (site == 1 ? ix.y : (site == 2 ? ix.z : ix.w));
+    M.xs2[t] = M.xs[s];
+    M.vs2[t] = M.vs[s];
+    M.fs2[t] = M.fs[s];
+    M.qs2[t] = M.qs[s];
+    const uint32_t id = M.ids[s];
+    M.ids2[t] = id;
+    M.idToIdx[id] = t;
 }
 
+// the sorted streams back into the primary buffers, the positions of this
+// build for the skin check, and the molecule maps (molecule perm[d] at slot d)
 __global__ void k_mf_copyback(const MolGridArgs M) {
     pdl_wait();
     if (!M.st->rebuild) return;
@@ -788,71 +783,105 @@ __global__ void k_mf_copyback(const MolGridArgs M) {
     M.fs[i] = M.fs2[i];
     M.qs[i] = M.qs2[i];
     M.ids[i] = M.ids2[i];
+    if ((i & 3) == 0) {
+        const int d = i >> 2;
+        const int4 nx = make_int4(i, i + 1, i + 2, i + 3);
+        M.mol_idx[M.perm[d]] = nx;
+        if (M.mol_idx_e3b) M.mol_idx_e3b[M.perm[d]] = nx;
+    }
 }
 
-// the molecule-pair list: one warp per slot walks the (2m+1)^2 rows of its
-// stencil (each row one or two contiguous runs of slots: the grid has at
-// least 2m+1 cells per side, so no cell is seen twice) 32 candidates at a
-// time; a candidate is kept when the minimum-image distance of the site-0
-// positions is below the list radius.  Entries are slots, written in
-// candidate order (deterministic) into the team layout: slot k's e-th entry
-// at (k/G) cap G + (e/T) 32 + (k%G) T + e%T, G = 32/T.
-__global__ void __launch_bounds__(128) k_mf_build(const MolGridArgs M) {
+// the molecule-pair list: one block per slot, one thread per row of its
+// (2m+1)^2-row stencil (each row one or two contiguous runs of slots: the
+// grid has at least 2m+1 cells per side, so no cell is seen twice).  A
+// candidate is kept when the minimum-image distance of the site-0 positions
+// is below the list radius.  Two passes over the row: count, a block scan of
+// the row counts, then the writes -- rows in stencil order, candidates in slot
+// order (deterministic) -- into the team layout: slot k's e-th entry at
+// (k/G) cap G + (e/T) 32 + (k%G) T + e%T, G = 32/T.  Every row's cell-start
+// loads and candidate loads are in flight at once instead of one row after
+// another.
+constexpr int kMfBuildThreads = 64;  // >= 49 rows (m <= 3)
+
+__device__ __forceinline__ void mf_row_runs(const MolGridArgs &M, int r, int cx, int cy, int cz, int (&b)[2],
+                                            int (&e)[2]) {
+    const CellGrid &g = M.g;
+    const int mm = M.m, side = 2 * mm + 1;
+    int kx = cx - mm + r / side, ky = cy - mm + r % side;
+    kx = kx < 0 ? kx + g.ns.x : (kx >= g.ns.x ? kx - g.ns.x : kx);
+    ky = ky < 0 ? ky + g.ns.y : (ky >= g.ns.y ? ky - g.ns.y : ky);
+    const int rowbase = (kx * g.ns.y + ky) * g.ns.z;
+    const int zlo = cz - mm, zhi = cz + mm;
+    int za[2], zb[2], nr;
+    if (zlo < 0) {
+        za[0] = zlo + g.ns.z; zb[0] = g.ns.z - 1; za[1] = 0; zb[1] = zhi; nr = 2;
+    } else if (zhi >= g.ns.z) {
+        za[0] = zlo; zb[0] = g.ns.z - 1; za[1] = 0; zb[1] = zhi - g.ns.z; nr = 2;
+    } else {
+        za[0] = zlo; zb[0] = zhi; za[1] = 0; zb[1] = -1; nr = 1;
+    }
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        b[q] = 0;
+        e[q] = 0;
+        if (q < nr) {
+            b[q] = (int)M.cell_start[rowbase + za[q]];
+            e[q] = (int)M.cell_start[rowbase + zb[q] + 1];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kMfBuildThreads) k_mf_build(const MolGridArgs M) {
     pdl_wait();
     if (!M.st->rebuild) return;
-    const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (k >= M.nmol) return;
-    const CellGrid &g = M.g;
+    const int k = blockIdx.x;
+    if (k >= M.nmol) return;  // block-uniform
+    __shared__ uint32_t sh_cnt[kMfBuildThreads];
+    const int r = threadIdx.x;
+    const int side = 2 * M.m + 1;
+    const bool has_row = r < side * side;
     const float3 p = f3(M.xs2[4 * k]);
-    const int c = cell_of_pos(g, p);
-    const int cz = c % g.ns.z, cy = (c / g.ns.z) % g.ns.y, cx = c / (g.ns.z * g.ns.y);
-    const int mm = M.m, side = 2 * mm + 1;
+    const int c = cell_of_pos(M.g, p);
+    const int cz = c % M.g.ns.z, cy = (c / M.g.ns.z) % M.g.ns.y, cx = c / (M.g.ns.z * M.g.ns.y);
+    int b[2] = {0, 0}, e[2] = {0, 0};
+    if (has_row) mf_row_runs(M, r, cx, cy, cz, b, e);
+    // pass 1: this row's hits
+    uint32_t n = 0;
+#pragma unroll
+    for (int q = 0; q < 2; q++)
+        for (int j = b[q]; j < e[q]; j++) {
+            if (j == k) continue;
+            const float3 d = min_image(M.box, f3(M.xs2[4 * j]) - p);
+            n += dot3(d, d) < M.cut2 ? 1u : 0u;
+        }
+    // exclusive scan of the row counts over the block (rows in order)
+    sh_cnt[r] = n;
+    __syncthreads();
+    uint32_t off = 0, tot = 0;
+    for (int q = 0; q < kMfBuildThreads; q++) {
+        const uint32_t v = sh_cnt[q];
+        off += q < r ? v : 0u;
+        tot += v;
+    }
+    // pass 2: the writes
     const int T = M.team, G = 32 / T;
     uint32_t *const row = M.list + (size_t)(k / G) * M.cap * G + (k % G) * T;
     const uint32_t cap = (uint32_t)M.cap;
-    const uint32_t lt = (1u << lane) - 1u;
-    uint32_t cnt = 0u;
-    for (int r = 0; r < side * side; r++) {
-        int kx = cx - mm + r / side, ky = cy - mm + r % side;
-        kx = kx < 0 ? kx + g.ns.x : (kx >= g.ns.x ? kx - g.ns.x : kx);
-        ky = ky < 0 ? ky + g.ns.y : (ky >= g.ns.y ? ky - g.ns.y : ky);
-        const int rowbase = (kx * g.ns.y + ky) * g.ns.z;
-        const int zlo = cz - mm, zhi = cz + mm;
-        // up to two runs: [zlo, zhi] split where it wraps
+    uint32_t pos = off;
 #pragma unroll
-        for (int part = 0; part < 2; part++) {
-            int za, zb;
-            if (zlo < 0) {
-                za = part == 0 ? zlo + g.ns.z : 0;
-                zb = part == 0 ? g.ns.z - 1 : zhi;
-            } else if (zhi >= g.ns.z) {
-                za = part == 0 ? zlo : 0;
-                zb = part == 0 ? g.ns.z - 1 : zhi - g.ns.z;
-            } else {
-                if (part == 1) break;
-                za = zlo;
-                zb = zhi;
-            }
-            const int b = (int)M.cell_start[rowbase + za], e = (int)M.cell_start[rowbase + zb + 1];
-            for (int c0 = b; c0 < e; c0 += 32) {
-                const int j = c0 + lane;
-                bool hit = false;
-                if (j < e && j != k) {
-                    const float3 d = min_image(M.box, f3(M.xs2[4 * j]) - p);
-                    hit = dot3(d, d) < M.cut2;
-                }
-                const uint32_t bal = __ballot_sync(0xffffffffu, hit);
-                const uint32_t pos = cnt + __popc(bal & lt);
-                if (hit && pos < cap) row[(pos / T) * 32u + pos % T] = (uint32_t)j;
-                cnt += __popc(bal);
+    for (int q = 0; q < 2; q++)
+        for (int j = b[q]; j < e[q]; j++) {
+            if (j == k) continue;
+            const float3 d = min_image(M.box, f3(M.xs2[4 * j]) - p);
+            if (dot3(d, d) < M.cut2) {
+                if (pos < cap) row[(pos / T) * 32u + pos % T] = (uint32_t)j;
+                pos++;
             }
         }
-    }
-    if (lane == 0) {
-        M.counts[k] = cnt;
-        if (cnt > cap) atomicOr(&M.st->bits, kStatusNlistOverflow);
-        atomicMax(&M.st->max_mol_neighbors, cnt);
+    if (r == 0) {
+        M.counts[k] = tot;
+        if (tot > cap) atomicOr(&M.st->bits, kStatusNlistOverflow);
+        atomicMax(&M.st->max_mol_neighbors, tot);
     }
 }
 
@@ -1292,7 +1321,7 @@ static int nlist_rebuild_mf(State &s, bool force, cudaStream_t bstream) {
     MDX_CUDA_TRY(launch_pdl(k_scan_cells, dim3(1), dim3(kScanThreads), 0, s.stream, Am, nt));
     MDX_CUDA_TRY(launch_pdl(k_mf_scatter, dim3(nb_mol), dim3(256), 0, s.stream, M));
     MDX_CUDA_TRY(launch_pdl(k_mf_rank, dim3((M.ncell * 32 + 255) / 256), dim3(256), 0, s.stream, M));
-    MDX_CUDA_TRY(launch_pdl(k_mf_gather, dim3(nb_mol), dim3(256), 0, s.stream, M));
+    MDX_CUDA_TRY(launch_pdl(k_mf_gather, dim3((4 * M.nmol + 255) / 256), dim3(256), 0, s.stream, M));
     MDX_CUDA_TRY(launch_pdl(k_mf_copyback, dim3((4 * M.nmol + 255) / 256), dim3(256), 0, s.stream, M));
     cudaStream_t bs = s.stream;
     if (bstream) {
@@ -1300,7 +1329,7 @@ static int nlist_rebuild_mf(State &s, bool force, cudaStream_t bstream) {
         MDX_CUDA_TRY(cudaStreamWaitEvent(bstream, s.ev_sorted, 0));
         bs = bstream;
     }
-    MDX_CUDA_TRY(launch_pdl(k_mf_build, dim3((M.nmol * 32 + 127) / 128), dim3(128), 0, bs, M));
+    MDX_CUDA_TRY(launch_pdl(k_mf_build, dim3(M.nmol), dim3(kMfBuildThreads), 0, bs, M));
     if (FixE3B *e3 = s.e3bFix()) {
         if (int e = e3b_build_list_mf(s, *e3, bs)) return e;
     }
