@@ -44,17 +44,21 @@ __device__ __forceinline__ float e3b_dsw(const E3BParams &p, float r) {
     return 6.0f * (p.rf - r) * (p.rs - r) * p.rfminusrs_cubed_inv;
 }
 // threeBodyPairEnergy(r) and threeBodyForce(dr, r) (EvaluatorE3B.h:117-141)
+// (square root, exponential and divisions in the single-instruction forms
+// the reference's --use_fast_math build gives them, CMakeLists.txt:53)
 __device__ __forceinline__ void e3b_ef(const E3BParams &p, float3 dr, float &e, float3 &f) {
-    const float r = sqrtf(dot3(dr, dr));
-    const float es = expf(-p.k3 * r);
+    const float r2 = dot3(dr, dr);
+    const float rinv = rsqrt_ftz(r2);
+    const float r = r2 * rinv;
+    const float es = ex2_ftz(-p.k3 * r * 1.4426950408889634f);
     const float sw = e3b_sw(p, r);
     e = sw * es;
     f = make_float3(0.f, 0.f, 0.f);
     if (r <= p.rf) {
-        float s = p.k3 * es / r;
+        float s = p.k3 * es * rinv;
         if (r > p.rs) {
             s *= sw;
-            s -= (es * e3b_dsw(p, r) / r);
+            s -= es * e3b_dsw(p, r) * rinv;
         }
         f = dr * s;
     }
@@ -165,7 +169,14 @@ struct E3BArgs {
     float4 *totals;
     double *e_out;    // energy passes
     int twobody;      // 0: the totals pass leaves out the O-O two-body force
+    // 1: the molecule form -- molecule index = slot, sites at 4m .. 4m+3
+    // (mol_idx holds that identity map; the hot passes skip reading it)
+    int slots;
 };
+
+__device__ __forceinline__ int4 e3b_sites(const E3BArgs &A, const int4 *__restrict__ mol_idx, int m) {
+    return A.slots ? make_int4(4 * m, 4 * m + 1, 4 * m + 2, 4 * m + 3) : __ldg(mol_idx + m);
+}
 #define MDX_E3B_ARGS \
     pdl_wait();      \
     const E3BArgs A = tab ? tab[blockIdx.y] : a0
@@ -243,10 +254,10 @@ __global__ void k_e3b_list(const E3BArgs a0, const E3BArgs *__restrict__ tab, in
 }
 
 // The molecule form's E3B list, cut from the molecule-pair list of the same
-// rebuild: slot k of molecule m (site 0 at 4k after the sort), every listed
-// slot whose site-0 distance is below the E3B list radius, written as its
-// molecule index (mol_of_slot).  The molecule-pair list holds every site-0
-// pair within its larger radius, so the E3B set is the per-site path's.
+// rebuild: in that form the E3B molecule index is the slot (sites 4k ..
+// 4k+3), so row k holds every listed slot whose site-0 distance is below the
+// E3B list radius.  The molecule-pair list holds every site-0 pair within its
+// larger radius, so the E3B set is the per-site path's.
 template <int T>
 __global__ void k_e3b_list_mf(const E3BArgs A, const uint32_t *__restrict__ pcounts,
                               const uint32_t *__restrict__ plist, int pcap, int pteam,
@@ -260,7 +271,7 @@ __global__ void k_e3b_list_mf(const E3BArgs A, const uint32_t *__restrict__ pcou
     const int m = warp * G + a;
     if (m >= A.nmol) return;
     const unsigned team_mask = (T == 32) ? 0xffffffffu : (((1u << T) - 1u) << (a * T));
-    const int k = A.mol_idx[m].x >> 2;
+    const int k = m;
     const float3 po = f3(xs2[4 * k]);
     int cnt = (int)pcounts[k];
     cnt = cnt < pcap ? cnt : pcap;
@@ -276,7 +287,7 @@ __global__ void k_e3b_list_mf(const E3BArgs A, const uint32_t *__restrict__ pcou
             const int j = (int)prow[(size_t)(e / pteam) * 32 + (e % pteam)];
             const float3 d = min_image(A.box, po - f3(xs2[4 * j]));
             hit = dot3(d, d) < A.cut2;
-            mj = mol_of_slot[j];
+            mj = j;
         }
         const unsigned b = __ballot_sync(team_mask, hit);
         if (hit) {
@@ -320,7 +331,7 @@ __global__ void k_e3b_totals(const E3BArgs a0, const E3BArgs *__restrict__ tab) 
     float fx = 0.f, fy = 0.f, fz = 0.f, tx = 0.f, ty = 0.f, tz = 0.f, e2 = 0.f;
     int4 ix = make_int4(0, 0, 0, 0);
     if (valid) {
-        ix = mol_idx[m];
+        ix = e3b_sites(A, mol_idx, m);
         const MolPos mi = load_mol(xs, ix);
         int cnt = (int)mcounts[m];
         cnt = cnt < mcap ? cnt : mcap;
@@ -336,7 +347,7 @@ __global__ void k_e3b_totals(const E3BArgs a0, const E3BArgs *__restrict__ tab) 
                 const int k = k0 + u * T;
                 has[u] = k < cnt;
                 const int mj = has[u] ? (int)row[(size_t)(k / T) * 32] : m;
-                jxs[u] = __ldg(mol_idx + mj);
+                jxs[u] = e3b_sites(A, mol_idx, mj);
             }
 #pragma unroll
             for (int u = 0; u < 2; u++) ojs[u] = f3(__ldg(xs + jxs[u].x));
@@ -348,9 +359,10 @@ __global__ void k_e3b_totals(const E3BArgs a0, const E3BArgs *__restrict__ tab) 
             const float3 dr = min_image(box, mi.a - oj);
             const float r2 = dot3(dr, dr);
             if (r2 >= p.list_cut2) continue;
-            const float r = sqrtf(r2);
-            const float ex = expf(-p.k2 * r);
-            const float s = p.k2 * p.E2 * ex / r;
+            const float rinv = rsqrt_ftz(r2);
+            const float r = r2 * rinv;
+            const float ex = ex2_ftz(-p.k2 * r * 1.4426950408889634f);
+            const float s = p.k2 * p.E2 * ex * rinv;
             fx += dr.x * s;
             fy += dr.y * s;
             fz += dr.z * s;
@@ -428,7 +440,7 @@ __global__ void k_e3b_forces(const E3BArgs a0, const E3BArgs *__restrict__ tab) 
     float e3 = 0.f;
     int4 ix = make_int4(0, 0, 0, 0);
     if (valid) {
-        ix = mol_idx[m];
+        ix = e3b_sites(A, mol_idx, m);
         const MolPos mi = load_mol(xs, ix);
         const float4 Ti = totals[m];
         int cnt = (int)mcounts[m];
@@ -443,7 +455,7 @@ __global__ void k_e3b_forces(const E3BArgs a0, const E3BArgs *__restrict__ tab) 
             for (int u = 0; u < 2; u++) {
                 const int k = k0 + u * T;
                 mjs[u] = k < cnt ? (int)row[(size_t)(k / T) * 32] : -1;
-                jxs[u] = __ldg(mol_idx + (mjs[u] < 0 ? m : mjs[u]));
+                jxs[u] = e3b_sites(A, mol_idx, mjs[u] < 0 ? m : mjs[u]);
             }
 #pragma unroll
             for (int u = 0; u < 2; u++) ojs[u] = f3(__ldg(xs + jxs[u].x));
@@ -457,7 +469,7 @@ __global__ void k_e3b_forces(const E3BArgs a0, const E3BArgs *__restrict__ tab) 
             const float3 dr = min_image(box, mi.a - mjp.a);
             const float r2 = dot3(dr, dr);
             if (r2 >= p.list_cut2) continue;
-            if (sqrtf(r2) > p.rmax) continue;
+            if (r2 > p.rmax * p.rmax) continue;
             mjp.b = f3(__ldg(xs + jx.y));
             mjp.c = f3(__ldg(xs + jx.z));
             const float4 Tj = __ldg(totals + mj);
@@ -676,6 +688,7 @@ static E3BArgs e3b_args(State &s, FixE3B &f, float4 *out) {
     A.totals = f.totals.p;
     A.e_out = nullptr;
     A.twobody = 1;
+    A.slots = s.mf.on ? 1 : 0;
     return A;
 }
 

@@ -953,8 +953,8 @@ MolGridArgs mol_grid_args(State &s) {
     M.xs_last = d.xs_last_build.p;
     M.idToIdx = d.idToIdx.p;
     M.mol_idx = s.rigidFix()->d_mol_idx.p;
-    FixE3B *e3 = s.e3bFix();
-    M.mol_idx_e3b = (e3 && e3->side_ok) ? e3->d_mol_idx.p : nullptr;
+    // (FixE3B's map is the identity slot map in this form, never rewritten)
+    M.mol_idx_e3b = nullptr;
     M.cell_of = mf.cell_of.p;
     M.cell_count = mf.cell_count.p;
     M.cell_start = mf.cell_start.p;
@@ -1486,8 +1486,13 @@ int molform_init(State &s) {
     // the sort reads the molecule maps first: after an upload every atom sits
     // at index == id, so the maps are the molecules' ids
     MDX_CUDA_TRY(cudaMemcpy(r->d_mol_idx.p, r->mol_ids.data(), nmol * sizeof(int4), cudaMemcpyHostToDevice));
-    if (FixE3B *e3 = s.e3bFix())
-        MDX_CUDA_TRY(cudaMemcpy(e3->d_mol_idx.p, r->mol_ids.data(), nmol * sizeof(int4), cudaMemcpyHostToDevice));
+    // E3B works by slot in this form (its molecules are FixRigid's): its map
+    // is the identity slot map, slot k at sites 4k .. 4k+3
+    if (FixE3B *e3 = s.e3bFix()) {
+        std::vector<int4> ident(nmol);
+        for (int k = 0; k < nmol; k++) ident[k] = make_int4(4 * k, 4 * k + 1, 4 * k + 2, 4 * k + 3);
+        MDX_CUDA_TRY(cudaMemcpy(e3->d_mol_idx.p, ident.data(), nmol * sizeof(int4), cudaMemcpyHostToDevice));
+    }
     mf.on = true;
     return 0;
 }

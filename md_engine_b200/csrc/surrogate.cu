@@ -24,6 +24,8 @@
 #include <random>
 #include <vector>
 
+#include <cstring>
+
 #include "engine.hpp"
 
 namespace mdx {
@@ -967,15 +969,31 @@ int mdx_e3b_surrogate_features(mdx_state *st, mdx_fix *fix, float *raw, float *f
     k_features<<<feat_blocks(nmol), 256, 0, s.stream>>>(A);
     MDX_LAUNCHED();
     MDX_CUDA_TRY(cudaStreamSynchronize(s.stream));
-    if (raw) MDX_CUDA_TRY(cudaMemcpy(raw, u.raw.p, (size_t)nmol * S::kIn * sizeof(float), cudaMemcpyDeviceToHost));
+    // rows come per E3B molecule index; in the molecule form that index is the
+    // slot, mapped back here to the fix's molecule order (FixRigid's maps)
+    std::vector<int> row_of(nmol);
+    for (int m = 0; m < nmol; m++) row_of[m] = m;
+    if (s.mf.on) {
+        std::vector<int4> mi(nmol);
+        MDX_CUDA_TRY(cudaMemcpy(mi.data(), s.rigidFix()->d_mol_idx.p, nmol * sizeof(int4), cudaMemcpyDeviceToHost));
+        for (int m = 0; m < nmol; m++) row_of[m] = mi[m].x >> 2;
+    }
+    if (raw) {
+        std::vector<float> h((size_t)nmol * S::kIn);
+        MDX_CUDA_TRY(cudaMemcpy(h.data(), u.raw.p, h.size() * sizeof(float), cudaMemcpyDeviceToHost));
+        for (int m = 0; m < nmol; m++)
+            std::memcpy(raw + (size_t)m * S::kIn, h.data() + (size_t)row_of[m] * S::kIn, S::kIn * sizeof(float));
+    }
     if (frames) {
         std::vector<float4> h(3 * (size_t)nmol);
         MDX_CUDA_TRY(cudaMemcpy(h.data(), u.frame.p, h.size() * sizeof(float4), cudaMemcpyDeviceToHost));
-        for (size_t k = 0; k < h.size(); k++) {
-            frames[3 * k] = h[k].x;
-            frames[3 * k + 1] = h[k].y;
-            frames[3 * k + 2] = h[k].z;
-        }
+        for (int m = 0; m < nmol; m++)
+            for (int c = 0; c < 3; c++) {
+                const float4 v = h[3 * (size_t)row_of[m] + c];
+                frames[9 * (size_t)m + 3 * c] = v.x;
+                frames[9 * (size_t)m + 3 * c + 1] = v.y;
+                frames[9 * (size_t)m + 3 * c + 2] = v.z;
+            }
     }
     return 0;
 }
