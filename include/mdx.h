@@ -94,8 +94,27 @@ int mdx_state_synchronize(mdx_state *st);
 int mdx_fix_lj_cut_create(mdx_state *st, const char *handle, const char *mixing, mdx_fix **out);
 /* FixWCA(state, handle, mixingRules) (src/Fixes/FixWCA.cu) */
 int mdx_fix_wca_create(mdx_state *st, const char *handle, const char *mixing, mdx_fix **out);
+/* FixLJCutFS(state, handle, mixingRules) (src/Fixes/FixLJCutFS.cu:12-26):
+ * force-shifted LJ (PairEvaluatorLJFS.h:15-57), parameters eps, sig, rCut */
+int mdx_fix_lj_cut_fs_create(mdx_state *st, const char *handle, const char *mixing, mdx_fix **out);
+/* FixLJCHARMM(state, handle, mixingRules) (src/Fixes/FixLJCHARMM.cu:15-32):
+ * LJ with separate 1-4 parameters (PairEvaluatorCHARMM.h:7-44), parameters
+ * eps, sig, eps14, sig14, rCut; a pair whose exclusion multiplier equals the
+ * 1-4 coefficient takes eps14/sig14 */
+int mdx_fix_lj_charmm_create(mdx_state *st, const char *handle, const char *mixing, mdx_fix **out);
+/* FixTICG(state, handle, mixingRules) (src/Fixes/FixTICG.cu:11-22): soft
+ * sphere overlap (PairEvaluatorTICG.h:9-52), parameters C and rCut, set for
+ * every pair of species (no mixing) */
+int mdx_fix_ticg_create(mdx_state *st, const char *handle, const char *mixing, mdx_fix **out);
+/* FixChargePairDSF(state, handle, group) + setParameters(alpha, r_cut)
+ * (src/Fixes/FixChargePairDSF.cu): damped shifted force charges
+ * (ChargeEvaluatorDSF.h:13-47), evaluated inside the pair fix's kernel;
+ * defaults alpha 0.25, r_cut 9.0.  One charge fix (Ewald or DSF) per state. */
+int mdx_fix_charge_pair_dsf_create(mdx_state *st, const char *handle, const char *group, mdx_fix **out);
+int mdx_fix_charge_pair_dsf_set_parameters(mdx_fix *fix, double alpha, double r_cut);
 /* FixPair::setParameter(param, handleA, handleB, val) (src/Fixes/FixPair.cpp:143-168);
- * param is "eps", "sig" or "rCut" */
+ * param is one of the fix's handles: "eps", "sig", "rCut" (LJ/cut, WCA,
+ * LJCutFS), + "eps14", "sig14" (LJCHARMM), "C", "rCut" (TICG) */
 int mdx_fix_pair_set_parameter(mdx_fix *fix, const char *param, const char *handle_a, const char *handle_b,
                                double value);
 /* FixChargeEwald(state, handle, group) (src/Fixes/FixChargeEwald.cu:828-839) */

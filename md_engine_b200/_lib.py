@@ -50,6 +50,11 @@ SIGNATURES = [
     ("mdx_state_synchronize", c_int, [c_void_p]),
     ("mdx_fix_lj_cut_create", c_int, [c_void_p, c_char_p, c_char_p, P(c_void_p)]),
     ("mdx_fix_wca_create", c_int, [c_void_p, c_char_p, c_char_p, P(c_void_p)]),
+    ("mdx_fix_lj_cut_fs_create", c_int, [c_void_p, c_char_p, c_char_p, P(c_void_p)]),
+    ("mdx_fix_lj_charmm_create", c_int, [c_void_p, c_char_p, c_char_p, P(c_void_p)]),
+    ("mdx_fix_ticg_create", c_int, [c_void_p, c_char_p, c_char_p, P(c_void_p)]),
+    ("mdx_fix_charge_pair_dsf_create", c_int, [c_void_p, c_char_p, c_char_p, P(c_void_p)]),
+    ("mdx_fix_charge_pair_dsf_set_parameters", c_int, [c_void_p, c_dbl, c_dbl]),
     ("mdx_fix_pair_set_parameter", c_int, [c_void_p, c_char_p, c_char_p, c_char_p, c_dbl]),
     ("mdx_fix_charge_ewald_create", c_int, [c_void_p, c_char_p, c_char_p, P(c_void_p)]),
     ("mdx_fix_charge_ewald_set_parameters", c_int, [c_void_p, c_int, c_int, c_int, c_dbl, c_int]),

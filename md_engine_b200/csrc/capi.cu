@@ -267,8 +267,9 @@ int mdx_state_activate_fix(mdx_state *st, mdx_fix *fix) {
     State &s = *st->s;
     ARG_CHECK(fix->owner == st, "fix belongs to another state");
     if (std::find(s.fixes.begin(), s.fixes.end(), fix->f) != s.fixes.end()) return 0;
+    auto charge = [](FixKind k) { return k == FixKind::ChargeEwald || k == FixKind::ChargeDSF; };
     for (Fix *f : s.fixes)
-        if (f->kind == fix->f->kind) {
+        if (f->kind == fix->f->kind || (charge(f->kind) && charge(fix->f->kind))) {
             set_error(MDX_ERR_UNSUPPORTED, "only one fix of kind '%s' is supported per state", fix->f->type.c_str());
             return MDX_ERR_UNSUPPORTED;
         }
@@ -344,6 +345,38 @@ int mdx_fix_wca_create(mdx_state *st, const char *handle, const char *mixing, md
     std::string mix = mixing ? mixing : "geometric";
     ARG_CHECK(mix == "geometric" || mix == "arithmetic", "mixing must be 'geometric' or 'arithmetic'");
     return new_fix(st, new FixPair(st->s, handle, 2, mix), out);
+}
+
+static int new_pair_fix(mdx_state *st, const char *handle, const char *mixing, int kind, mdx_fix **out) {
+    ARG_CHECK(st && handle && out, "null argument");
+    std::string mix = mixing ? mixing : "geometric";
+    ARG_CHECK(mix == "geometric" || mix == "arithmetic", "mixing must be 'geometric' or 'arithmetic'");
+    return new_fix(st, new FixPair(st->s, handle, kind, mix), out);
+}
+
+int mdx_fix_lj_cut_fs_create(mdx_state *st, const char *handle, const char *mixing, mdx_fix **out) {
+    return new_pair_fix(st, handle, mixing, 3, out);
+}
+
+int mdx_fix_lj_charmm_create(mdx_state *st, const char *handle, const char *mixing, mdx_fix **out) {
+    return new_pair_fix(st, handle, mixing, 4, out);
+}
+
+int mdx_fix_ticg_create(mdx_state *st, const char *handle, const char *mixing, mdx_fix **out) {
+    return new_pair_fix(st, handle, mixing, 5, out);
+}
+
+int mdx_fix_charge_pair_dsf_create(mdx_state *st, const char *handle, const char *group, mdx_fix **out) {
+    ARG_CHECK(st && handle && out, "null argument");
+    return new_fix(st, new FixChargePairDSF(st->s, handle, group ? group : "all"), out);
+}
+
+int mdx_fix_charge_pair_dsf_set_parameters(mdx_fix *fix, double alpha, double r_cut) {
+    ARG_CHECK(fix && fix->f->kind == FixKind::ChargeDSF, "not a FixChargePairDSF");
+    ARG_CHECK(alpha >= 0.0 && r_cut > 0.0, "alpha must be >= 0 and r_cut > 0");
+    fix->f->state->prepared = false;
+    static_cast<FixChargePairDSF *>(fix->f)->setParameters(alpha, r_cut);
+    return 0;
 }
 
 int mdx_fix_pair_set_parameter(mdx_fix *fix, const char *param, const char *ha, const char *hb, double value) {

@@ -221,7 +221,7 @@ struct MolForm {
 };
 
 // ---------------------------------------------------------------- Fixes
-enum class FixKind { Pair, ChargeEwald, E3B, Rigid, NoseHoover };
+enum class FixKind { Pair, ChargeEwald, ChargeDSF, E3B, Rigid, NoseHoover };
 
 class Fix {
    public:
@@ -247,19 +247,29 @@ class Fix {
 };
 
 class FixChargeEwald;
+class FixChargePairDSF;
 class FixRigid;
 
-// FixPair / FixLJCut / FixWCA (src/Fixes/FixPair.cpp, FixLJCut.cu, FixWCA.cu)
+// FixPair and its pair styles (src/Fixes/FixPair.cpp): 1 FixLJCut
+// (FixLJCut.cu), 2 FixWCA (FixWCA.cu), 3 FixLJCutFS (FixLJCutFS.cu),
+// 4 FixLJCHARMM (FixLJCHARMM.cu), 5 FixTICG (FixTICG.cu)
 class FixPair : public Fix {
    public:
-    int lj_kind;  // 1 LJ/cut, 2 WCA
+    int lj_kind;
     std::string mixing;
     // unprocessed per-type tables; NaN = unset (DEFAULT_FILL)
     std::map<std::string, std::vector<double>> params;
-    DBuf<float> d_params;  // rc2, eps24, sig6 (3*T*T)
+    // processed tables in the reference's paramOrder, nparam() x T x T:
+    // {rCut^2, 24 eps, sig^6} (LJ/cut, WCA), + F(rCut) (LJCutFS),
+    // + 24 eps14, sig14^6 (LJCHARMM), {rCut^2, C} (TICG)
+    DBuf<float> d_params;
     std::vector<float> h_params;
-    FixChargeEwald *chargeFix = nullptr;  // offloaded real-space Ewald (State.cpp:648-660)
+    FixChargeEwald *chargeFix = nullptr;     // offloaded real-space Ewald (State.cpp:648-660)
+    FixChargePairDSF *dsfFix = nullptr;      // offloaded damped shifted force charges
     double chargeRCut = 0;
+    int nparam() const { return lj_kind == 3 ? 4 : (lj_kind == 4 ? 5 : (lj_kind == 5 ? 2 : 3)); }
+    // whether the pair evaluator can give a non-zero force for types (a, b)
+    bool pairActive(int a, int b) const;
     FixPair(State *s, std::string h, int kind, std::string mix);
     int setParameter(const std::string &param, int a, int b, double v);
     int prepareForRun() override;
@@ -305,6 +315,18 @@ class FixChargeEwald : public Fix {
     int spread_mol(cudaStream_t st, const FixRigid &r);
     int gather_mol_to(float4 *out, cudaStream_t st, const FixRigid &r);
     DBuf<float4> f_recip;                         // per-step reciprocal forces (fused step)
+};
+
+// FixChargePairDSF (src/Fixes/FixChargePairDSF.cu): damped shifted force
+// charges (Fennell & Gezelter, J. Chem. Phys. 124, 234104 (2006)), a pair
+// term offloaded into the pair fix's kernel
+class FixChargePairDSF : public Fix {
+   public:
+    double alpha = 0.25, r_cut = 9.0, A = 0, shift = 0;
+    FixChargePairDSF(State *s, std::string h, std::string g);
+    void setParameters(double alpha_, double r_cut_);
+    int prepareForRun() override;
+    std::vector<double> getRCuts() override { return {r_cut}; }
 };
 
 struct E3BParams {  // EvaluatorE3B (EvaluatorE3B.h:9-65), FixE3B.cu:515-593
@@ -468,6 +490,7 @@ class State {
     int checkStatus();
     FixPair *pairFix();
     FixChargeEwald *ewaldFix();
+    FixChargePairDSF *dsfFix();
     FixE3B *e3bFix();
     FixRigid *rigidFix();
     FixNoseHoover *nhFix();

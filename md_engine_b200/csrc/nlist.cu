@@ -1147,25 +1147,27 @@ int nlist_exclusions(State &s) {
 }
 
 // Which listed pairs can interact: bit tj of ljmask[ti] is set when the pair
-// fix's eps(ti, tj) != 0; with an Ewald fix, pairs with q_i q_j != 0 also
-// interact.  Everything else contributes exactly zero force, energy and
-// virial in compute_force_iso (PairEvaluatorLJ.h:17-30 scales by eps,
-// ChargeEvaluatorEwald.h:11-40 by q_i q_j) and is kept at the back of the row.
+// fix's evaluator can give (ti, tj) a force (eps != 0; eps14 != 0 for
+// LJCHARMM; C != 0 for TICG); with a charge fix (Ewald or DSF), pairs with
+// q_i q_j != 0 also interact.  Everything else contributes exactly zero
+// force, energy and virial in compute_force_iso (the pair evaluators scale by
+// eps or C, the charge evaluators by q_i q_j) and is kept at the back of the
+// row.
 int nlist_set_interactions(State &s) {
     GridGPU &gr = s.grid;
     FixPair *pf = s.pairFix();
     const int nt = (int)s.species.size();
     gr.partition = false;
     gr.part_q = false;
-    if (!pf || nt > 32 || pf->h_params.size() != (size_t)3 * nt * nt) return 0;
+    if (!pf || nt > 32 || pf->h_params.size() != (size_t)pf->nparam() * nt * nt) return 0;
     std::vector<uint32_t> mask(nt, 0u);
     for (int a = 0; a < nt; a++)
         for (int b = 0; b < nt; b++)
-            if (pf->h_params[nt * nt + a * nt + b] != 0.f) mask[a] |= 1u << b;
+            if (pf->pairActive(a, b)) mask[a] |= 1u << b;
     if (int e = gr.ljmask.alloc(nt)) return e;
     MDX_CUDA_TRY(cudaMemcpy(gr.ljmask.p, mask.data(), nt * sizeof(uint32_t), cudaMemcpyHostToDevice));
     gr.partition = true;
-    gr.part_q = pf->chargeFix != nullptr;
+    gr.part_q = pf->chargeFix != nullptr || pf->dsfFix != nullptr;
     return 0;
 }
 
@@ -1393,6 +1395,8 @@ int molform_init(State &s) {
     FixPair *pf = s.pairFix();
     if (!r || !r->foursite) return refuse("needs FixRigid with four-site molecules");
     if (!pf) return refuse("needs a pair fix");
+    if (pf->lj_kind != 1 && pf->lj_kind != 2) return refuse("the molecule form evaluates LJ/cut or WCA");
+    if (s.dsfFix()) return refuse("the molecule form evaluates Ewald real-space charges");
     if (has_free_atoms(s)) return refuse("every atom must belong to a rigid molecule");
     if (FixE3B *e3 = s.e3bFix())
         if (!e3->side_ok) return refuse("FixE3B's molecules must be FixRigid's, in the same order");

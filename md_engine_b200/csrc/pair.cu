@@ -10,324 +10,48 @@
 // paramsCoalesced order).  The team's partial forces (and the optional
 // per-atom virial, x0.5 as helpers.h:34-41 / PairEvaluateIso.h:180-195) are
 // reduced with register shuffles, not shared memory.
+#include <cmath>
 #include <cstdio>
 
-#include "engine.hpp"
+#include "pair_kernel.cuh"
 
 namespace mdx {
 
 namespace {
 
-// threads per block of the pair kernel: small blocks retire and refill SM
-// slots finely, beside the P3M chain on another stream (measured against 256:
-// water step +1.8 %, LJ +2.4 %)
-constexpr int kPairBlock = 64;
+using pk::PairArgs;
+using pk::kPairBlock;
 
+// LJ/cut and WCA with Ewald or no charges (the other pair and charge
+// evaluators: pair_styles.cu)
 template <int T>
-__device__ __forceinline__ float team_sum(float v) {
-#pragma unroll
-    for (int o = T / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-struct PairArgs {
-    int n;
-    const float4 *__restrict__ xs;
-    float4 *__restrict__ fs;
-    const float *__restrict__ qs;
-    const uint32_t *__restrict__ counts;
-    const uint32_t *__restrict__ nlist;
-    int cap;
-    const float *__restrict__ params;
-    int ntypes;
-    Box box;
-    float coef1, coef2, coef3;
-    float qrc2, alpha, qqr;
-    float *__restrict__ virials;
-    float *__restrict__ energy;  // per-atom (energy kernel)
-    uint32_t lj_types;           // bit ti: type ti has a pair with eps != 0
-    // GridGPU's own list layout instead of this library's (null: this
-    // library's): per-block padded rows located by cumulSumMaxPerBlock for
-    // ref_ntpb threads per block, counts as uint16 (GridGPU.cu:777-821,
-    // cutils_func.h:23-45)
-    const uint32_t *__restrict__ cum;
-    const uint16_t *__restrict__ counts16;
-    int ref_ntpb;
-};
-
-// erfc(x) for x >= 0 by Abramowitz & Stegun, Handbook of Mathematical
-// Functions, eq. 7.1.26 (|error| <= 1.5e-7): erfc(x) = t P5(t) exp(-x^2) with
-// t = 1 / (1 + p x).  exp(-x^2) is passed in: the Ewald force needs it anyway.
-__device__ __forceinline__ float erfc_as(float x, float expmx2) {
-    // t only feeds the A&S polynomial (error 1.5e-7): the approximate
-    // reciprocal (one SFU op, a few ulp) is plenty
-    const float t = rcp_ftz(fmaf(0.3275911f, x, 1.0f));
-    float poly = fmaf(t, 1.061405429f, -1.453152027f);
-    poly = fmaf(t, poly, 1.421413741f);
-    poly = fmaf(t, poly, -0.284496736f);
-    poly = fmaf(t, poly, 0.254829592f);
-    return t * poly * expmx2;
-}
-
-// one neighbour: returns the scalar force factor (F = dr * s) and energy
-template <int LJ, bool EW, bool ENERGY>
-__device__ __forceinline__ bool pair_term(const PairArgs &A, const float *sp, int nt2, int ti, float qi, float4 xj,
-                                          float qj, float3 dr, float r2, float mult, float &s, float &e) {
-    bool any = false;
-    s = 0.f;
-    e = 0.f;
-    if (LJ) {
-        const int tj = type_of(xj);
-        const int ix = ti * A.ntypes + tj;
-        const float rc2 = sp[ix];
-        if (r2 < rc2) {
-            any = true;
-            const float eps24 = sp[nt2 + ix];
-            // eps = 0 (e.g. TIP4P/2005 H and M sites) contributes exactly zero
-            if (mult != 0.f && eps24 != 0.f) {
-                const float sig6 = sp[2 * nt2 + ix];
-                const float p1 = eps24 * 2.f * sig6 * sig6;
-                const float p2 = eps24 * sig6;
-                const float r2inv = 1.0f / r2;
-                const float r6inv = r2inv * r2inv * r2inv;
-                s += r6inv * r2inv * (p1 * r6inv - p2) * mult;
-                if (ENERGY) {
-                    const float eps = eps24 / 24.0f;
-                    const float s6r6 = sig6 * r6inv;
-                    if (LJ == 1) {
-                        const float rc6 = rc2 * rc2 * rc2;
-                        const float s6rc6 = sig6 / rc6;
-                        const float off = s6rc6 * (s6rc6 - 1.0f);
-                        e += 0.5f * 4.0f * eps * (s6r6 * (s6r6 - 1.0f) - off) * mult;
-                    } else {
-                        e += 0.5f * (4.0f * eps * s6r6 * (s6r6 - 1.0f) + eps) * mult;
-                    }
-                }
-            }
-        }
-    }
-    if (EW) {
-        // q_i q_j = 0 (e.g. the TIP4P/2005 oxygen) contributes exactly zero
-        if (r2 < A.qrc2 && qi * qj != 0.f) {
-            any = true;
-            const float r2c = r2 < 1e-10f ? 1e-10f : r2;
-            const float rinv = rsqrt_ftz(r2c);
-            const float r2inv = rinv * rinv;
-            const float x = A.alpha * (r2c * rinv);  // alpha r
-            const float expm = exp_neg_sq(x);        // exp(-alpha^2 r^2) (the reference: __expf)
-            const float qq = A.qqr * qi * qj;
-            const float erfcv = erfc_as(x, expm);
-            float fsc = qq * (erfcv * rinv + (2.0f * 0.5641895835477563f * A.alpha) * expm);
-            if (mult < 1.0f) fsc -= (1.0f - mult) * qq * rinv;
-            s += fsc * r2inv;
-            if (ENERGY) {
-                float eng = qq * rinv * erfcv;
-                if (mult < 1.0f) eng -= (1.0f - mult) * qq * rinv;
-                e += 0.5f * eng;
-            }
-        }
-    }
-    return any;
-}
-
-// one lane's share of atom i's row: U entries per trip -- all list loads,
-// then all position and charge gathers, then the arithmetic, so U memory
-// chains are in flight per lane instead of one dependent list->position chain
-template <int T, int LJ, bool EW, bool VIR, bool ENERGY>
-__device__ __forceinline__ void pair_row(const PairArgs &A, const float *sp, int nt2, int i, int ti, float qi,
-                                         float4 xi, const uint32_t *row, int cnt, int t, float &fx, float &fy,
-                                         float &fz, float &en, float (&v)[6]) {
-    // entries per lane per trip: a full-warp team (long water rows) keeps
-    // three in flight within its 40-register cap (measured at 24 blocks per
-    // SM: U = 3 vs 2, pair 35.1 -> 33.4 us; U = 4 at the old 256-thread
-    // shape cost registers and resident warps beside the P3M chain)
-    constexpr int U = T >= 32 ? 3 : 4;
-    constexpr uint32_t kNone = 0xffffffffu;
-    for (int k0 = t; k0 < cnt; k0 += U * T) {
-        uint32_t ent[U];
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-            const int k = k0 + u * T;
-            ent[u] = k < cnt ? __ldg(row + (size_t)(k / T) * 32) : kNone;
-        }
-        float4 xj[U];
-        float qj[U];
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-            const int j = ent[u] == kNone ? i : (int)(ent[u] & kExclMask);
-            xj[u] = __ldg(A.xs + j);
-            qj[u] = EW ? __ldg(A.qs + j) : 0.f;
-        }
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-            if (ent[u] == kNone) continue;
-            const uint32_t tag = ent[u] >> 30;
-            float mult = 1.0f;
-            if (tag) mult = tag == 1u ? A.coef1 : (tag == 2u ? A.coef2 : A.coef3);
-            const float3 dr = min_image(A.box, make_float3(xi.x - xj[u].x, xi.y - xj[u].y, xi.z - xj[u].z));
-            const float r2 = dot3(dr, dr);
-            float s, eng;
-            if (pair_term<LJ, EW, ENERGY>(A, sp, nt2, ti, qi, xj[u], qj[u], dr, r2, mult, s, eng)) {
-                const float Fx = dr.x * s, Fy = dr.y * s, Fz = dr.z * s;
-                fx += Fx;
-                fy += Fy;
-                fz += Fz;
-                if (ENERGY) en += eng;
-                if (VIR) {
-                    v[0] += Fx * dr.x;
-                    v[1] += Fy * dr.y;
-                    v[2] += Fz * dr.z;
-                    v[3] += Fx * dr.y;
-                    v[4] += Fx * dr.z;
-                    v[5] += Fy * dr.z;
-                }
-            }
-        }
-    }
-}
-
-// tab: one argument record per replica (batched launch, blockIdx.y = replica)
-// or null (single system, a0).  With both LJ and Ewald terms, a warp whose
-// atoms have no LJ partner type (water H, M) runs the row without the LJ
-// term, and one whose atoms are all uncharged (water O) without the Ewald
-// term: both contribute exactly zero there, and the choice is warp-uniform.
-// The full-warp team (long water rows) is latency bound on the x_j gathers:
-// capped at 40 registers it keeps 24 blocks (48 warps) per SM (measured:
-// pair 36.9 -> 35.1 us, water step +0 to +3 %); other teams are left alone
-template <int T, int LJ, bool EW, bool VIR, bool ENERGY>
-__global__ void __launch_bounds__(kPairBlock, T >= 32 ? 24 : 1) k_pair(const PairArgs a0, const PairArgs *__restrict__ tab, int accumulate) {
-    pdl_wait();
-    const PairArgs A = tab ? tab[blockIdx.y] : a0;
-    extern __shared__ float sp[];
-    const int nt2 = A.ntypes * A.ntypes;
-    if (LJ) {
-        for (int k = threadIdx.x; k < 3 * nt2; k += blockDim.x) sp[k] = A.params[k];
-        __syncthreads();
-    }
-    constexpr int G = 32 / T;
-    const int lane = threadIdx.x & 31;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int a = lane / T, t = lane % T;
-    const int i = warp * G + a;
-    const bool valid = i < A.n;
-    float fx = 0.f, fy = 0.f, fz = 0.f, en = 0.f;
-    float v[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
-    int ti = 0, cnt = 0;
-    float qi = 0.f;
-    const uint32_t *row = nullptr;
-    if (valid) {
-        xi = A.xs[i];
-        ti = type_of(xi);
-        qi = EW ? A.qs[i] : 0.f;
-        if (A.cum) {
-            // GridGPU layout: block b of ref_ntpb threads holds ref_ntpb / T
-            // atoms; its warps' rows start at (ref_ntpb / 32) * cum[b] and are
-            // cum[b+1] - cum[b] entries apart; entry k sits 32 * (k / T) on
-            const int per_block = A.ref_ntpb / T;
-            const int blk = i / per_block, nth = i % per_block;
-            const uint32_t c0 = A.cum[blk], mem = A.cum[blk + 1] - c0;
-            row = A.nlist + (size_t)(A.ref_ntpb / 32) * c0 + (size_t)mem * (nth / G) + (nth % G) * T + t;
-            cnt = (int)A.counts16[i];
-        } else {
-            cnt = (int)A.counts[i];
-            cnt = cnt < A.cap ? cnt : A.cap;
-            row = A.nlist + (size_t)(i / G) * A.cap * G + a * T + t;
-        }
-    }
-    if (LJ && EW) {
-        const bool lj_row = valid && ti < 32 && ((A.lj_types >> ti) & 1u);
-        const bool q_row = valid && qi != 0.f;
-        if (!__any_sync(0xffffffffu, lj_row)) {
-            if (valid) pair_row<T, 0, true, VIR, ENERGY>(A, sp, nt2, i, ti, qi, xi, row, cnt, t, fx, fy, fz, en, v);
-        } else if (!__any_sync(0xffffffffu, q_row)) {
-            if (valid) pair_row<T, LJ, false, VIR, ENERGY>(A, sp, nt2, i, ti, qi, xi, row, cnt, t, fx, fy, fz, en, v);
-        } else if (valid) {
-            pair_row<T, LJ, EW, VIR, ENERGY>(A, sp, nt2, i, ti, qi, xi, row, cnt, t, fx, fy, fz, en, v);
-        }
-    } else if (valid) {
-        pair_row<T, LJ, EW, VIR, ENERGY>(A, sp, nt2, i, ti, qi, xi, row, cnt, t, fx, fy, fz, en, v);
-    }
-    // late trigger (row loop done): the next kernel's blocks take SM slots
-    // as this grid drains; its griddepcontrol.wait still waits for the stores
-    pdl_trigger();
-    // invalid lanes carry zeros; whole warp takes part in the shuffles
-    if (ENERGY) {
-        en = team_sum<T>(en);
-        if (valid && t == 0) A.energy[i] = en;
-        return;
-    }
-    fx = team_sum<T>(fx);
-    fy = team_sum<T>(fy);
-    fz = team_sum<T>(fz);
-    if (VIR) {
-#pragma unroll
-        for (int c = 0; c < 6; c++) v[c] = team_sum<T>(v[c]);
-    }
-    if (valid && t == 0) {
-        float4 f = A.fs[i];
-        if (accumulate) {
-            f.x += fx;
-            f.y += fy;
-            f.z += fz;
-        } else {
-            f.x = fx;
-            f.y = fy;
-            f.z = fz;
-        }
-        A.fs[i] = f;
-        if (VIR) {
-            float *vv = A.virials + 6 * (size_t)i;
-#pragma unroll
-            for (int c = 0; c < 6; c++) vv[c] += 0.5f * v[c];
-        }
-    }
-}
-
-// nrep > 1: tab holds nrep records, A is the largest replica (grid sizing)
-template <int T, int LJ, bool EW>
-void launch_t(const PairArgs &A, const PairArgs *tab, int nrep, bool vir, bool energy, bool accumulate,
-              cudaStream_t st) {
-    const int G = 32 / T;
-    const int warps = (A.n + G - 1) / G;
-    const dim3 blocks((warps * 32 + kPairBlock - 1) / kPairBlock, nrep);
-    const size_t smem = LJ ? 3 * A.ntypes * A.ntypes * sizeof(float) : 0;
-    if (energy) {
-        k_pair<T, LJ, EW, false, true><<<blocks, kPairBlock, smem, st>>>(A, tab, 0);
-        MDX_LAUNCHED();
-    } else if (vir) {
-        k_pair<T, LJ, EW, true, false><<<blocks, kPairBlock, smem, st>>>(A, tab, accumulate ? 1 : 0);
-        MDX_LAUNCHED();
-    } else {
-        launch_pdl(k_pair<T, LJ, EW, false, false>, blocks, dim3(kPairBlock), smem, st, A, tab, accumulate ? 1 : 0);
-    }
-}
-
-template <int T>
-int launch_kind(const PairArgs &A, const PairArgs *tab, int nrep, int lj, bool ew, bool vir, bool energy, bool acc,
+int launch_kind(const PairArgs &A, const PairArgs *tab, int nrep, int lj, int ck, bool vir, bool energy, bool acc,
                 cudaStream_t st) {
-    if (lj == 0 && ew) launch_t<T, 0, true>(A, tab, nrep, vir, energy, acc, st);
-    else if (lj == 1 && ew) launch_t<T, 1, true>(A, tab, nrep, vir, energy, acc, st);
-    else if (lj == 1) launch_t<T, 1, false>(A, tab, nrep, vir, energy, acc, st);
-    else if (lj == 2 && ew) launch_t<T, 2, true>(A, tab, nrep, vir, energy, acc, st);
-    else if (lj == 2) launch_t<T, 2, false>(A, tab, nrep, vir, energy, acc, st);
-    else return MDX_ERR_ARG;
+    if (lj == 0 && ck == 1) pk::launch_t<T, 0, 1>(A, tab, nrep, vir, energy, acc, st);
+    else if (lj == 1 && ck == 1) pk::launch_t<T, 1, 1>(A, tab, nrep, vir, energy, acc, st);
+    else if (lj == 1 && ck == 0) pk::launch_t<T, 1, 0>(A, tab, nrep, vir, energy, acc, st);
+    else if (lj == 2 && ck == 1) pk::launch_t<T, 2, 1>(A, tab, nrep, vir, energy, acc, st);
+    else if (lj == 2 && ck == 0) pk::launch_t<T, 2, 0>(A, tab, nrep, vir, energy, acc, st);
+    else return pk::pair_launch_styles(A, tab, nrep, T, lj, ck, vir, energy, acc, st);
     return 0;
 }
 
-int launch_any(const PairArgs &A, int team, int lj, bool ew, bool vir, bool energy, bool acc, cudaStream_t st,
+int launch_any(const PairArgs &A, int team, int lj, int ck, bool vir, bool energy, bool acc, cudaStream_t st,
                const PairArgs *tab = nullptr, int nrep = 1) {
     switch (team) {
-        case 1: return launch_kind<1>(A, tab, nrep, lj, ew, vir, energy, acc, st);
-        case 2: return launch_kind<2>(A, tab, nrep, lj, ew, vir, energy, acc, st);
-        case 4: return launch_kind<4>(A, tab, nrep, lj, ew, vir, energy, acc, st);
-        case 8: return launch_kind<8>(A, tab, nrep, lj, ew, vir, energy, acc, st);
-        case 16: return launch_kind<16>(A, tab, nrep, lj, ew, vir, energy, acc, st);
-        case 32: return launch_kind<32>(A, tab, nrep, lj, ew, vir, energy, acc, st);
+        case 1: return launch_kind<1>(A, tab, nrep, lj, ck, vir, energy, acc, st);
+        case 2: return launch_kind<2>(A, tab, nrep, lj, ck, vir, energy, acc, st);
+        case 4: return launch_kind<4>(A, tab, nrep, lj, ck, vir, energy, acc, st);
+        case 8: return launch_kind<8>(A, tab, nrep, lj, ck, vir, energy, acc, st);
+        case 16: return launch_kind<16>(A, tab, nrep, lj, ck, vir, energy, acc, st);
+        case 32: return launch_kind<32>(A, tab, nrep, lj, ck, vir, energy, acc, st);
     }
     set_error(MDX_ERR_ARG, "team size %d not in {1,2,4,8,16,32}", team);
     return MDX_ERR_ARG;
 }
+
+// the charge evaluator the pair fix carries: 0 none, 1 Ewald, 2 DSF
+int charge_kind(const FixPair &f) { return f.chargeFix ? 1 : (f.dsfFix ? 2 : 0); }
 
 PairArgs make_args(State &s, FixPair &f) {
     PairArgs A;
@@ -339,6 +63,7 @@ PairArgs make_args(State &s, FixPair &f) {
     A.nlist = s.grid.nlist.p;
     A.cap = s.grid.cap;
     A.params = f.d_params.p;
+    A.np = f.nparam();
     A.ntypes = (int)s.species.size();
     A.box = s.box;
     A.coef1 = s.specialNeighborCoefs[0];
@@ -347,24 +72,35 @@ PairArgs make_args(State &s, FixPair &f) {
     A.qrc2 = 0.f;
     A.alpha = 0.f;
     A.qqr = (float)s.units.qqr_to_eng;
+    A.dsf_A = A.dsf_shift = A.dsf_ecut = A.dsf_rc = 0.f;
     if (f.chargeFix) {
         float qrc = (float)f.chargeRCut;
         A.qrc2 = qrc * qrc;
         A.alpha = (float)f.chargeFix->alpha;
+    } else if (f.dsfFix) {
+        // FixChargePairDSF's evaluator (generateEvaluator, FixChargePairDSF.cu)
+        const FixChargePairDSF &d = *f.dsfFix;
+        const float qrc = (float)d.r_cut;
+        A.qrc2 = qrc * qrc;
+        A.alpha = (float)d.alpha;
+        A.dsf_A = (float)d.A;
+        A.dsf_shift = (float)d.shift;
+        A.dsf_ecut = (float)(std::erfc(d.alpha * d.r_cut) / d.r_cut);
+        A.dsf_rc = qrc;
     }
     A.virials = s.gpd.virials.p;
     A.energy = nullptr;
     A.cum = nullptr;
     A.counts16 = nullptr;
     A.ref_ntpb = 0;
-    // types with an LJ partner (eps != 0); every type when unknown
+    // types with a pair partner the pair evaluator does not zero
     A.lj_types = 0xffffffffu;
     const int nt = A.ntypes;
-    if (nt <= 32 && f.h_params.size() == (size_t)3 * nt * nt) {
+    if (nt <= 32 && f.h_params.size() == (size_t)f.nparam() * nt * nt) {
         A.lj_types = 0u;
         for (int x = 0; x < nt; x++)
             for (int y = 0; y < nt; y++)
-                if (f.h_params[(size_t)nt * nt + x * nt + y] != 0.f) A.lj_types |= 1u << x;
+                if (f.pairActive(x, y)) A.lj_types |= 1u << x;
     }
     return A;
 }
@@ -461,7 +197,7 @@ __device__ __forceinline__ float mol_pair_term(const MolPairArgs &A, int ab, flo
         const float rinv = rsqrt_ftz(r2c);
         const float x = A.alpha * (r2c * rinv);
         const float expm = exp_neg_sq(x);
-        const float erfcv = erfc_as(x, expm);
+        const float erfcv = pk::erfc_as(x, expm);
         const float qq = A.qq[ab];
         float fsc = qq * (erfcv * rinv + (2.0f * 0.5641895835477563f * A.alpha) * expm);
         if (OWN && mult < 1.0f) fsc -= (1.0f - mult) * qq * rinv;
@@ -702,7 +438,7 @@ int pair_launch(State &s, FixPair &f, int virialMode, bool accumulate) {
     if (s.mf.on) return pair_mol_launch(s, f, virialMode, accumulate, nullptr, s.stream);
     PairArgs A = make_args(s, f);
     bool vir = virialMode == 1 || virialMode == 2;
-    return launch_any(A, s.grid.team, f.lj_kind, f.chargeFix != nullptr, vir, false, accumulate, s.stream);
+    return launch_any(A, s.grid.team, f.lj_kind, charge_kind(f), vir, false, accumulate, s.stream);
 }
 
 // the molecule form of the pair forces (energy: per-site energies into
@@ -739,7 +475,7 @@ int pair_energy(State &s, FixPair &f, double *out) {
     A.energy = s.e_site.p;
     if (s.mf.on) {
         if (int r = pair_mol_launch(s, f, 0, false, s.e_site.p, s.stream)) return r;
-    } else if (int r = launch_any(A, s.grid.team, f.lj_kind, f.chargeFix != nullptr, false, true, false, s.stream)) {
+    } else if (int r = launch_any(A, s.grid.team, f.lj_kind, charge_kind(f), false, true, false, s.stream)) {
         return r;
     }
     return float_sum(s, s.e_site.p, A.n, out);
@@ -765,7 +501,7 @@ int batch_pair_launch(Batch &b, cudaStream_t stream) {
     State &big = *b.reps[b.pair_big];
     FixPair &f = *big.pairFix();
     const PairArgs A = make_args(big, f);
-    return launch_any(A, big.grid.team, f.lj_kind, f.chargeFix != nullptr, false, false, true, stream,
+    return launch_any(A, big.grid.team, f.lj_kind, charge_kind(f), false, false, true, stream,
                       reinterpret_cast<const PairArgs *>(b.tab_pair.p), R);
 }
 
@@ -787,6 +523,7 @@ int pair_force_raw(int n, const float4 *xs, float4 *fs, const float *qs, const u
     A.coef1 = coef[0];
     A.coef2 = coef[1];
     A.coef3 = coef[2];
+    A.dsf_A = A.dsf_shift = A.dsf_ecut = A.dsf_rc = 0.f;
     A.qrc2 = qrc > 0.f ? qrc * qrc : 0.f;
     A.alpha = alpha;
     A.qqr = qqr;
@@ -798,7 +535,8 @@ int pair_force_raw(int n, const float4 *xs, float4 *fs, const float *qs, const u
     A.ref_ntpb = 0;
     bool ew = qrc > 0.f;
     if (lj_kind == 0 && !ew) return 0;
-    int r = launch_any(A, team, lj_kind, ew, virials != nullptr, false, accumulate, stream);
+    A.np = 3;
+    int r = launch_any(A, team, lj_kind, ew ? 1 : 0, virials != nullptr, false, accumulate, stream);
     if (r) return r;
     MDX_CUDA_TRY(cudaGetLastError());
     return 0;
@@ -827,6 +565,7 @@ int pair_force_gridgpu(int n, const float4 *xs, float4 *fs, const uint16_t *coun
     A.coef1 = coef[0];
     A.coef2 = coef[1];
     A.coef3 = coef[2];
+    A.dsf_A = A.dsf_shift = A.dsf_ecut = A.dsf_rc = 0.f;
     A.qrc2 = qcut > 0.f ? qcut * qcut : 0.f;
     A.alpha = alpha;
     A.qqr = qqr;
@@ -838,7 +577,8 @@ int pair_force_gridgpu(int n, const float4 *xs, float4 *fs, const uint16_t *coun
     A.ref_ntpb = ntpb;
     const bool ew = qcut > 0.f;
     if (lj_kind == 0 && !ew) return 0;
-    if (int r = launch_any(A, ntpa, lj_kind, ew, virials != nullptr, false, true, stream)) return r;
+    A.np = 3;
+    if (int r = launch_any(A, ntpa, lj_kind, ew ? 1 : 0, virials != nullptr, false, true, stream)) return r;
     MDX_CUDA_TRY(cudaGetLastError());
     return 0;
 }

@@ -83,6 +83,11 @@ FixChargeEwald *State::ewaldFix() {
         if (f->kind == FixKind::ChargeEwald) return static_cast<FixChargeEwald *>(f);
     return nullptr;
 }
+FixChargePairDSF *State::dsfFix() {
+    for (Fix *f : fixes)
+        if (f->kind == FixKind::ChargeDSF) return static_cast<FixChargePairDSF *>(f);
+    return nullptr;
+}
 FixE3B *State::e3bFix() {
     for (Fix *f : fixes)
         if (f->kind == FixKind::E3B) return static_cast<FixE3B *>(f);
@@ -250,13 +255,20 @@ int State::prepare() {
     requiresCharges = false;
     FixPair *pf = pairFix();
     FixChargeEwald *ew = ewaldFix();
+    FixChargePairDSF *dsf = dsfFix();
+    if (ew && dsf) {
+        set_error(MDX_ERR_UNSUPPORTED, "one charge fix per state: FixChargeEwald or FixChargePairDSF");
+        return MDX_ERR_UNSUPPORTED;
+    }
     if (ew) {
         requiresCharges = true;
         if (ew->r_cut < 0) ew->r_cut = rCut;
     }
+    if (dsf) requiresCharges = true;
     if (pf) {
         pf->chargeFix = ew;
-        pf->chargeRCut = ew ? ew->r_cut : 0.0;
+        pf->dsfFix = dsf;
+        pf->chargeRCut = ew ? ew->r_cut : (dsf ? dsf->r_cut : 0.0);
         if (ew) ew->offloaded = true;
     }
     // reset NDF (Atom ndf 3, FixRigid::assignNDF sets 2 / 0)
@@ -309,12 +321,64 @@ int State::prepare() {
 }
 
 // ---------------------------------------------------------------- FixPair
+static const char *pair_type_name(int kind) {
+    switch (kind) {
+        case 1: return "LJCut";
+        case 2: return "WCA";
+        case 3: return "LJCutFS";
+        case 4: return "LJCHARMM";
+        default: return "TICG";
+    }
+}
+
 FixPair::FixPair(State *s, std::string h, int kind, std::string mix)
-    : Fix(s, h, "all", kind == 1 ? "LJCut" : "WCA", FixKind::Pair), lj_kind(kind), mixing(mix) {
+    : Fix(s, h, "all", pair_type_name(kind), FixKind::Pair), lj_kind(kind), mixing(mix) {
     orderPreference = -1;  // FixPair.h:34
-    params["eps"] = {};
-    params["sig"] = {};
+    // the parameter handles each style's constructor initializes
+    if (kind == 5) {
+        params["C"] = {};
+    } else {
+        params["eps"] = {};
+        params["sig"] = {};
+    }
+    if (kind == 4) {
+        params["eps14"] = {};
+        params["sig14"] = {};
+    }
     params["rCut"] = {};
+}
+
+bool FixPair::pairActive(int a, int b) const {
+    const int nt = (int)state->species.size();
+    const size_t nt2 = (size_t)nt * nt, k = (size_t)a * nt + b;
+    if (h_params.size() != (size_t)nparam() * nt2) return true;
+    if (h_params[nt2 + k] != 0.f) return true;  // 24 eps, or C (TICG)
+    return lj_kind == 4 && h_params[3 * nt2 + k] != 0.f;  // 24 eps14
+}
+
+// ---------------------------------------------------------------- FixChargePairDSF
+FixChargePairDSF::FixChargePairDSF(State *s, std::string h, std::string g)
+    : Fix(s, h, g, "ChargePairDSF", FixKind::ChargeDSF) {
+    requiresCharges = true;
+    setParameters(0.25, 9.0);  // the constructor's defaults (FixChargePairDSF.cu)
+}
+
+// FixChargePairDSF::setParameters: A = 2 alpha / sqrt(pi),
+// shift = erfc(alpha rc) / rc^2 + A exp(-alpha^2 rc^2) / rc
+void FixChargePairDSF::setParameters(double alpha_, double r_cut_) {
+    alpha = alpha_;
+    r_cut = r_cut_;
+    A = 2.0 / std::sqrt(M_PI) * alpha;
+    shift = std::erfc(alpha * r_cut) / (r_cut * r_cut) + A * std::exp(-alpha * alpha * r_cut * r_cut) / r_cut;
+}
+
+int FixChargePairDSF::prepareForRun() {
+    if (!state->pairFix()) {
+        set_error(MDX_ERR_UNSUPPORTED, "FixChargePairDSF is evaluated inside a pair fix's kernel: add a pair fix");
+        return MDX_ERR_UNSUPPORTED;
+    }
+    prepared = true;
+    return 0;
 }
 
 void FixPair::ensureSize() {
@@ -346,12 +410,18 @@ int FixPair::setParameter(const std::string &param, int a, int b, double v) {
     return 0;
 }
 
-// prepareParameters (FixPair.cpp:13-33) with FixLJCut's lambdas
-// (FixLJCut.cu:83-122) or FixWCA's (FixWCA.cu:60-106)
+// prepareParameters (FixPair.cpp:13-63) with each style's lambdas: FixLJCut
+// (FixLJCut.cu:83-122), FixWCA (FixWCA.cu:60-106), FixLJCutFS
+// (FixLJCutFS.cu:84-130), FixLJCHARMM (FixLJCHARMM.cu:113-180), FixTICG
+// (FixTICG.cu:68-83).  Off-diagonal entries left unset are mixed from the
+// diagonal ones (eps geometric, sig geometric or arithmetic, rCut the larger
+// one, the diagonal rCut defaulting to state.rCut); TICG mixes nothing
+// (check_populate: every entry must be set).
 int FixPair::prepareForRun() {
     State &s = *state;
     ensureSize();
     const int nt = (int)s.species.size();
+    const size_t nt2 = (size_t)nt * nt;
     auto fill = [&](std::vector<double> v, bool geo, bool fillDiag, double diag) {
         if (fillDiag)
             for (int i = 0; i < nt; i++)
@@ -364,32 +434,83 @@ int FixPair::prepareForRun() {
                 }
         return v;
     };
-    std::vector<double> eps = fill(params["eps"], true, false, 0);
-    std::vector<double> sig = fill(params["sig"], mixing != "arithmetic", false, 0);
-    std::vector<double> rc;
-    if (lj_kind == 1) {
+    auto fill_rcut = [&]() {
         // fillRCut = fmax(a, b), diagonal default state->rCut
-        rc = params["rCut"];
+        std::vector<double> rc = params["rCut"];
         for (int i = 0; i < nt; i++)
             if (std::isnan(rc[i * nt + i])) rc[i * nt + i] = (float)s.rCut;
         for (int i = 0; i < nt; i++)
             for (int j = 0; j < nt; j++)
                 if (std::isnan(rc[i * nt + j])) rc[i * nt + j] = std::fmax((float)rc[i * nt + i], (float)rc[j * nt + j]);
-    } else {
-        rc.resize(nt * nt);
-        for (int k = 0; k < nt * nt; k++) rc[k] = (float)sig[k] * (float)std::pow(2.0, 1.0 / 6.0);
-    }
-    for (int k = 0; k < nt * nt; k++)
-        if (std::isnan(eps[k]) || std::isnan(sig[k])) {
-            set_error(MDX_ERR_STATE, "pair parameters eps/sig not set for every species");
-            return MDX_ERR_STATE;
+        return rc;
+    };
+    auto all_set = [&](const std::vector<double> &v, const char *what) {
+        for (size_t k = 0; k < nt2; k++)
+            if (std::isnan(v[k])) {
+                set_error(MDX_ERR_STATE, "pair parameter %s not set for every pair of species", what);
+                return false;
+            }
+        return true;
+    };
+    h_params.assign((size_t)nparam() * nt2, 0.f);
+    if (lj_kind == 5) {
+        // TICG: {rCut^2, C}, no mixing
+        const std::vector<double> &C = params["C"], &rc = params["rCut"];
+        if (!all_set(C, "C") || !all_set(rc, "rCut")) return MDX_ERR_STATE;
+        for (size_t k = 0; k < nt2; k++) {
+            const float r = (float)rc[k];
+            h_params[k] = r * r;
+            h_params[nt2 + k] = (float)C[k];
         }
-    h_params.assign(3 * nt * nt, 0.f);
-    for (int k = 0; k < nt * nt; k++) {
-        const float r = (float)rc[k];
-        h_params[k] = r * r;                                  // processRCut
-        h_params[nt * nt + k] = 24.0f * (float)eps[k];        // processEps
-        h_params[2 * nt * nt + k] = (float)std::pow((float)sig[k], 6);  // processSig
+    } else {
+        const double c14 = s.specialNeighborCoefs[2];
+        if (lj_kind == 4) {
+            // an unset 1-4 diagonal entry is the ordinary one times the 1-4
+            // coefficient, for eps14 and for sig14 (FixLJCHARMM.cu:147-155)
+            for (const char *h : {"eps14", "sig14"}) {
+                std::vector<double> &v14 = params[h];
+                const std::vector<double> &v = params[h[0] == 'e' ? "eps" : "sig"];
+                for (int i = 0; i < nt; i++)
+                    if (std::isnan(v14[i * nt + i])) v14[i * nt + i] = (float)v[i * nt + i] * (float)c14;
+            }
+        }
+        std::vector<double> eps = fill(params["eps"], true, false, 0);
+        std::vector<double> sig = fill(params["sig"], mixing != "arithmetic", false, 0);
+        if (!all_set(eps, "eps") || !all_set(sig, "sig")) return MDX_ERR_STATE;
+        std::vector<double> rc;
+        if (lj_kind == 2) {
+            rc.resize(nt2);
+            for (size_t k = 0; k < nt2; k++) rc[k] = (float)sig[k] * (float)std::pow(2.0, 1.0 / 6.0);
+        } else {
+            rc = fill_rcut();
+        }
+        for (size_t k = 0; k < nt2; k++) {
+            const float r = (float)rc[k];
+            h_params[k] = r * r;                                    // processRCut
+            h_params[nt2 + k] = 24.0f * (float)eps[k];              // processEps
+            h_params[2 * nt2 + k] = (float)std::pow((float)sig[k], 6);  // processSig
+        }
+        if (lj_kind == 3) {
+            // F(rCut): the unshifted LJ force magnitude at the pair's cutoff,
+            // from its processed parameters (the table EvaluatorLJFS::force
+            // reads as params[3]; see EvaluatorLJFS::forcePy, PairEvaluatorLJFS.cu)
+            for (size_t k = 0; k < nt2; k++) {
+                const float rc2 = h_params[k], eps24 = h_params[nt2 + k], sig6 = h_params[2 * nt2 + k];
+                const float p1 = eps24 * 2.0f * sig6 * sig6, p2 = eps24 * sig6;
+                const float r2inv = 1.0f / rc2, rinv = std::sqrt(r2inv);
+                const float r6inv = r2inv * r2inv * r2inv;
+                h_params[3 * nt2 + k] = r6inv * rinv * (p1 * r6inv - p2);
+            }
+        }
+        if (lj_kind == 4) {
+            std::vector<double> eps14 = fill(params["eps14"], true, false, 0);
+            std::vector<double> sig14 = fill(params["sig14"], mixing != "arithmetic", false, 0);
+            if (!all_set(eps14, "eps14") || !all_set(sig14, "sig14")) return MDX_ERR_STATE;
+            for (size_t k = 0; k < nt2; k++) {
+                h_params[3 * nt2 + k] = 24.0f * (float)eps14[k];
+                h_params[4 * nt2 + k] = (float)std::pow((float)sig14[k], 6);
+            }
+        }
     }
     if (int e = d_params.alloc(h_params.size())) return e;
     MDX_CUDA_TRY(cudaMemcpy(d_params.p, h_params.data(), h_params.size() * sizeof(float), cudaMemcpyHostToDevice));
@@ -410,6 +531,7 @@ std::vector<double> FixPair::getRCuts() {
         }
         return {m};
     }
+    (void)nt;
     ensureSize();
     for (double v : params["rCut"])
         if (!std::isnan(v)) m = std::max(m, v);

@@ -310,6 +310,52 @@ class FixWCA(FixPair):
         self.handle = handle
 
 
+def _pair_fix(obj, create, state, handle, mixingRules):
+    h = c_void_p()
+    check(create(state._h, handle.encode(), mixingRules.encode(), ctypes.byref(h)))
+    obj._h = h
+    obj.state = state
+    obj.handle = handle
+
+
+class FixLJCutFS(FixPair):
+    """FixLJCutFS(state, handle, mixingRules='geometric') (src/Fixes/FixLJCutFS.cu:12-26):
+    force-shifted Lennard-Jones; parameters eps, sig, rCut"""
+
+    def __init__(self, state, handle, mixingRules="geometric"):
+        _pair_fix(self, lib().mdx_fix_lj_cut_fs_create, state, handle, mixingRules)
+
+
+class FixLJCHARMM(FixPair):
+    """FixLJCHARMM(state, handle, mixingRules='geometric') (src/Fixes/FixLJCHARMM.cu:15-32):
+    LJ with 1-4 parameters; parameters eps, sig, eps14, sig14, rCut"""
+
+    def __init__(self, state, handle, mixingRules="geometric"):
+        _pair_fix(self, lib().mdx_fix_lj_charmm_create, state, handle, mixingRules)
+
+
+class FixTICG(FixPair):
+    """FixTICG(state, handle, mixingRules='geometric') (src/Fixes/FixTICG.cu:11-22):
+    soft-sphere overlap; parameters C and rCut for every pair of species"""
+
+    def __init__(self, state, handle, mixingRules="geometric"):
+        _pair_fix(self, lib().mdx_fix_ticg_create, state, handle, mixingRules)
+
+
+class FixChargePairDSF(_Fix):
+    """FixChargePairDSF(state, handle, groupHandle) (src/Fixes/FixChargePairDSF.cu):
+    damped shifted force charges, evaluated inside the pair fix's kernel"""
+
+    def __init__(self, state, handle, groupHandle="all"):
+        h = c_void_p()
+        check(lib().mdx_fix_charge_pair_dsf_create(state._h, handle.encode(), groupHandle.encode(), ctypes.byref(h)))
+        self._h = h
+        self.state = state
+
+    def setParameters(self, alpha, r_cut):
+        check(lib().mdx_fix_charge_pair_dsf_set_parameters(self._h, float(alpha), float(r_cut)))
+
+
 class FixChargeEwald(_Fix):
     """FixChargeEwald(state, handle, groupHandle) (src/Fixes/FixChargeEwald.cu:828-839)"""
 

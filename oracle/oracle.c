@@ -288,6 +288,119 @@ void orc_pair_forces(int n, const double *x, const int *type, const double *q,
 }
 
 /* ---------------------------------------------------------------------------
+ * The other pair styles of compute_force_iso, FP64, on a list as above.
+ *   params: np x ntypes x ntypes processed tables in the reference's
+ *     paramOrder; lj_kind 1 LJ/cut {rc2, 24eps, sig6} (PairEvaluatorLJ.h:17-60),
+ *     3 force-shifted LJ {rc2, 24eps, sig6, F(rc)} (PairEvaluatorLJFS.h:15-57),
+ *     4 CHARMM {rc2, 24eps, sig6, 24eps14, sig14^6} (PairEvaluatorCHARMM.h:7-44,
+ *     a pair whose multiplier equals coef[3] takes the 1-4 parameters),
+ *     5 TICG {rc2, C} (PairEvaluatorTICG.h:9-52), 0 none.
+ *   ck: 0 no charges, 1 Ewald real space (ChargeEvaluatorEwald.h:11-64),
+ *     2 damped shifted force (ChargeEvaluatorDSF.h:13-47) with
+ *     dsf = {2 alpha/sqrt(pi), shift, erfc(alpha rc)/rc, rc}.
+ * Outputs as orc_pair_forces.
+ * ------------------------------------------------------------------------- */
+void orc_pair_forces_styles(int n, const double *x, const int *type, const double *q, int ntypes,
+                            const double *params, int np, int lj_kind, int ck, double qrc, double alpha,
+                            double qqr_to_eng, const double *dsf, const double L[3], const int *counts,
+                            const uint32_t *nbr, int maxn, const double coef[4], double *f, double *virial,
+                            double *energy) {
+    const double qrc2 = qrc * qrc;
+    const double two_over_sqrtpi = 2.0 * 0.5641895835477563;
+    const int nt2 = ntypes * ntypes;
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int i = 0; i < n; i++) {
+        double fx = 0, fy = 0, fz = 0, e = 0;
+        double v[6] = {0, 0, 0, 0, 0, 0};
+        for (int k = 0; k < counts[i]; k++) {
+            uint32_t raw = nbr[(size_t)i * maxn + k];
+            int j = (int)(raw & ORC_EXCL_MASK);
+            double mult = coef[raw >> 30];
+            double dr[3];
+            for (int d = 0; d < 3; d++) {
+                double t = x[3 * i + d] - x[3 * j + d];
+                dr[d] = t - L[d] * rint(t / L[d]);
+            }
+            double r2 = dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2];
+            double fs = 0.0;
+            int any = 0;
+            int tp = type[i] * ntypes + type[j];
+            (void)np;
+            if (lj_kind && r2 < params[tp]) {
+                const double rc2 = params[tp];
+                any = 1;
+                if (mult != 0.0) {
+                    if (lj_kind == 5) {
+                        const double C = params[nt2 + tp];
+                        if (r2 != 0.0) fs += -C * 1.5 / sqrt(rc2 * r2) * (r2 / rc2 - 1.0) * mult;
+                        const double xr = sqrt(r2 / rc2);
+                        e += 0.5 * C * (0.5 * (xr - 1.0) * (xr - 1.0) * (xr + 2.0)) * mult;
+                    } else {
+                        double eps24 = params[nt2 + tp], sig6 = params[2 * nt2 + tp];
+                        if (lj_kind == 4 && mult == coef[3]) {
+                            eps24 = params[3 * nt2 + tp];
+                            sig6 = params[4 * nt2 + tp];
+                        }
+                        const double p1 = eps24 * 2.0 * sig6 * sig6, p2 = eps24 * sig6;
+                        const double r2inv = 1.0 / r2, r6inv = r2inv * r2inv * r2inv;
+                        double s = r6inv * r2inv * (p1 * r6inv - p2);
+                        if (lj_kind == 3) s -= params[3 * nt2 + tp] / sqrt(r2);
+                        fs += s * mult;
+                        const double eps = eps24 / 24.0, s6r6 = sig6 * r6inv;
+                        const double rc6 = rc2 * rc2 * rc2, s6rc6 = sig6 / rc6;
+                        double u = 4.0 * eps * (s6r6 * (s6r6 - 1.0) - s6rc6 * (s6rc6 - 1.0));
+                        /* U(r) - U(rc) + F(rc) (r - rc): the force-consistent form the
+                           reference documents (PairEvaluatorLJFS.h:41-44); its code adds
+                           F(rc) (rc - r) */
+                        if (lj_kind == 3) u += params[3 * nt2 + tp] * (sqrt(r2) - sqrt(rc2));
+                        e += 0.5 * u * mult;
+                    }
+                }
+            }
+            if (ck == 1 && r2 < qrc2) {
+                any = 1;
+                double rr2 = r2 < 1e-10 ? 1e-10 : r2;
+                double r2inv = 1.0 / rr2, rinv = sqrt(r2inv), len = sqrt(rr2);
+                double qq = qqr_to_eng * q[i] * q[j];
+                double s = qq * (erfc(alpha * len) * rinv + two_over_sqrtpi * alpha * exp(-alpha * alpha * rr2));
+                if (mult < 1.0) s -= (1.0 - mult) * qq * rinv;
+                fs += s * r2inv;
+                double eng = qq * rinv * erfc(alpha * len);
+                if (mult < 1.0) eng -= (1.0 - mult) * qq * rinv;
+                e += 0.5 * eng;
+            }
+            if (ck == 2 && r2 < qrc2) {
+                any = 1;
+                double r2inv = 1.0 / r2, rinv = sqrt(r2inv), len = sqrt(r2);
+                double qq = qqr_to_eng * q[i] * q[j];
+                fs += qq * (erfc(alpha * len) * r2inv + dsf[0] * exp(-alpha * alpha * r2) * rinv - dsf[1]) * rinv * mult;
+                e += 0.5 * qq * (erfc(alpha * len) * rinv - dsf[2] + dsf[1] * (len - dsf[3])) * mult;
+            }
+            if (any) {
+                double F[3] = {dr[0] * fs, dr[1] * fs, dr[2] * fs};
+                fx += F[0];
+                fy += F[1];
+                fz += F[2];
+                v[0] += F[0] * dr[0];
+                v[1] += F[1] * dr[1];
+                v[2] += F[2] * dr[2];
+                v[3] += F[0] * dr[1];
+                v[4] += F[0] * dr[2];
+                v[5] += F[1] * dr[2];
+            }
+        }
+        if (f) {
+            f[3 * i] = fx;
+            f[3 * i + 1] = fy;
+            f[3 * i + 2] = fz;
+        }
+        if (virial)
+            for (int c = 0; c < 6; c++) virial[6 * i + c] = 0.5 * v[c];
+        if (energy) energy[i] = e;
+    }
+}
+
+/* ---------------------------------------------------------------------------
  * E3B (EvaluatorE3B.h, ThreeBodyE3B.h).  Molecules are (O, H1, H2, M) atom
  * indices into x.  All O-O pairs with r < r2b_cut (the reference's molecule
  * list radius rf + 1 A) get the two-body term; pairs with r <= rmax3 get the

@@ -58,6 +58,7 @@ def lib():
         L.orc_nlist_brute.argtypes = [I, P, P, F, P, P, I]
         L.orc_nlist_brute.restype = I
         L.orc_pair_forces.argtypes = [I, P, P, P, I, P, P, P, I, D, D, D, P, P, P, I, P, P, P, P]
+        L.orc_pair_forces_styles.argtypes = [I, P, P, P, I, P, I, I, I, D, D, D, P, P, P, P, I, P, P, P, P]
         L.orc_e3b.argtypes = [I, P, P, P, P, P, P, P]
         L.orc_e3b.restype = I
         L.orc_lj_force_single.argtypes = [D, D, D, P, P]
@@ -243,6 +244,98 @@ def lj_params(ntypes, sig, eps, rcut, mixing="geometric", wca=False):
     else:
         rc = np.full((ntypes, ntypes), float(rcut))
     return dict(rc2=rc * rc, eps24=24.0 * E, sig6=S ** 6)
+
+
+def style_params(kind, ntypes, eps=None, sig=None, rcut=None, rcut_pairs=None, eps14=None, sig14=None, C=None,
+                 mixing="geometric", coef14=0.5):
+    """The processed parameter tables (np x ntypes x ntypes, FP64, the
+    reference's paramOrder) of a pair style: 1 LJ/cut, 3 force-shifted LJ,
+    4 CHARMM, 5 TICG -- prepareForRun of FixLJCut.cu:83-122,
+    FixLJCutFS.cu:84-130 (F(rc) as EvaluatorLJFS::forcePy forms it,
+    PairEvaluatorLJFS.cu), FixLJCHARMM.cu:113-180 (unset 1-4 diagonal
+    entries are the ordinary ones times the 1-4 coefficient), FixTICG.cu:68-83
+    (no mixing).  Dicts {(a, b): value} for the explicitly set pairs; rcut is
+    state.rCut, rcut_pairs the per-pair rCut overrides."""
+    def table(d, mix, diag_default=None):
+        T = np.full((ntypes, ntypes), np.nan)
+        for (a, b), val in (d or {}).items():
+            T[a, b] = T[b, a] = val
+        if diag_default is not None:
+            for a in range(ntypes):
+                if np.isnan(T[a, a]):
+                    T[a, a] = diag_default(a)
+        for a in range(ntypes):
+            for b in range(ntypes):
+                if np.isnan(T[a, b]):
+                    if mix == "max":
+                        T[a, b] = max(T[a, a], T[b, b])
+                    elif mix == "arithmetic":
+                        T[a, b] = (T[a, a] + T[b, b]) / 2.0
+                    else:
+                        T[a, b] = math.sqrt(T[a, a] * T[b, b])
+        return T
+    if kind == 5:
+        Ct = table(C, None)
+        R = table(rcut_pairs, None)
+        return np.stack([R * R, Ct])
+    E = table(eps, "geometric")
+    S = table(sig, "arithmetic" if mixing == "arithmetic" else "geometric")
+    R = table(rcut_pairs, "max", lambda a: float(rcut))
+    rc2, e24, s6 = R * R, 24.0 * E, S ** 6
+    out = [rc2, e24, s6]
+    if kind == 3:
+        p1, p2 = e24 * 2.0 * s6 * s6, e24 * s6
+        r2inv = 1.0 / rc2
+        out.append(r2inv ** 3 * np.sqrt(r2inv) * (p1 * r2inv ** 3 - p2))
+    if kind == 4:
+        E0 = {(a, a): E[a, a] * coef14 for a in range(ntypes)}
+        S0 = {(a, a): S[a, a] * coef14 for a in range(ntypes)}
+        E0.update(eps14 or {})
+        S0.update(sig14 or {})
+        E14 = table(E0, "geometric")
+        S14 = table(S0, "arithmetic" if mixing == "arithmetic" else "geometric")
+        out += [24.0 * E14, S14 ** 6]
+    return np.stack(out)
+
+
+def dsf_constants(alpha, rc):
+    """FixChargePairDSF::setParameters: (2 alpha/sqrt(pi), shift,
+    erfc(alpha rc)/rc, rc), shift = erfc(alpha rc)/rc^2 + A exp(-alpha^2 rc^2)/rc"""
+    A = 2.0 / math.sqrt(math.pi) * alpha
+    shift = math.erfc(alpha * rc) / (rc * rc) + A * math.exp(-alpha * alpha * rc * rc) / rc
+    return np.array([A, shift, math.erfc(alpha * rc) / rc, rc], np.float64)
+
+
+def pair_forces_styles(x, types, q, table, L, counts, nbr, coef=(1.0, 0.0, 0.0, 0.5), lj_kind=1, ck=0, qrc=0.0,
+                       alpha=0.0, qqr_to_eng=1.0, dsf=None, want=("f",)):
+    """FP64 compute_force_iso with any of the pair styles (table from
+    style_params; lj_kind 0 none, 1, 3, 4, 5) and charge evaluators (ck 0
+    none, 1 Ewald, 2 DSF with dsf from dsf_constants)."""
+    x = np.ascontiguousarray(x, np.float64)
+    n = len(x)
+    tb = np.ascontiguousarray(table, np.float64)
+    npar, nt = tb.shape[0], tb.shape[1]
+    t = np.ascontiguousarray(types, np.int32)
+    qq = np.ascontiguousarray(q if q is not None else np.zeros(n), np.float64)
+    Ld = np.asarray(L, np.float64)
+    c = np.ascontiguousarray(counts, np.int32)
+    nb = np.ascontiguousarray(nbr, np.uint32)
+    cf = np.asarray(coef, np.float64)
+    ds = np.ascontiguousarray(dsf if dsf is not None else np.zeros(4), np.float64)
+    f = np.zeros((n, 3)) if "f" in want else None
+    v = np.zeros((n, 6)) if "virial" in want else None
+    e = np.zeros(n) if "energy" in want else None
+    lib().orc_pair_forces_styles(n, _p(x), _p(t), _p(qq), nt, _p(tb), npar, int(lj_kind), int(ck), float(qrc),
+                                 float(alpha), float(qqr_to_eng), _p(ds), _p(Ld), _p(c), _p(nb), nb.shape[1], _p(cf),
+                                 _p(f), _p(v), _p(e))
+    out = {}
+    if f is not None:
+        out["f"] = f
+    if v is not None:
+        out["virial"] = v
+    if e is not None:
+        out["energy"] = e
+    return out
 
 
 # --------------------------------------------------------------------------

@@ -19,16 +19,21 @@
 #include <cstring>
 #include <vector>
 
+#include "ChargeEvaluatorDSF.h"
 #include "ChargeEvaluatorEwald.h"
 #include "ChargeEvaluatorNone.h"
 #include "PairEvaluateIso.h"
+#include "PairEvaluatorCHARMM.h"
 #include "PairEvaluatorLJ.h"
+#include "PairEvaluatorLJFS.h"
+#include "PairEvaluatorTICG.h"
 #include "PairEvaluatorWCA.h"
 #include "ThreeBodyE3B.h"
 
-// declared (not defined) by PairEvaluatorLJ.h; its definition lives in a file
-// that needs Boost.Python
+// declared (not defined) by PairEvaluatorLJ.h / PairEvaluatorLJFS.h; their
+// definitions live in files that need Boost.Python
 EvaluatorLJ::EvaluatorLJ() {}
+EvaluatorLJFS::EvaluatorLJFS() {}
 
 namespace {
 
@@ -147,6 +152,60 @@ int ref_pair_forces(int n, const float *xs4, const float *qs, const int *counts,
     return e == cudaSuccess ? 0 : (int)e;
 }
 
+// compute_force_iso with the other pair evaluators and charge evaluators:
+// lj_kind 0 none, 3 EvaluatorLJFS (4 parameters per pair, the table its
+// force() reads), 4 EvaluatorCHARMM (5 parameters, mult14 = c14), 5
+// EvaluatorTICG (2 parameters); ck 0 none, 1 ChargeEvaluatorEwald, 2
+// ChargeEvaluatorDSF (alpha, A, shift, qqr, rc as generateEvaluator builds
+// them).  params: np x ntypes^2.
+int ref_pair_styles(int n, const float *xs4, const float *qs, const int *counts, const uint32_t *nbr, int maxn,
+                    const float *params, int np, int ntypes, const float lo[3], const float L[3], float c12,
+                    float c13, float c14, int lj_kind, int ck, float qcut, float alpha, float qqr, float dsf_A,
+                    float dsf_shift, int ntpb, int ntpa, float *fs4_out) {
+    RefLayout lay = make_layout(n, counts, nbr, maxn, ntpb, ntpa);
+    std::vector<float4> hx(n), hf(n, make_float4(0.f, 0.f, 0.f, 0.f));
+    std::memcpy(hx.data(), xs4, n * sizeof(float4));
+    std::vector<float> hq(qs, qs + n), hp(params, params + (size_t)np * ntypes * ntypes);
+    if (hp.empty()) hp.push_back(0.f);
+    float4 *dx = dev(hx), *df = dev(hf);
+    float *dq = dev(hq), *dp = dev(hp);
+    uint16_t *dc = dev(lay.counts);
+    uint32_t *dl = dev(lay.list), *dcum = dev(lay.cum);
+    BoundsGPU b(make_float3(lo[0], lo[1], lo[2]), make_float3(L[0], L[1], L[2]), make_float3(1.f, 1.f, 1.f));
+    const int blocks = NBLOCKTEAM(n, ntpb, ntpa);
+    const size_t smem = (size_t)std::max(np, 1) * ntypes * ntypes * sizeof(float) + ntpb * sizeof(float3);
+    ChargeEvaluatorEwald ew(alpha, qqr);
+    ChargeEvaluatorDSF dsf(alpha, dsf_A, dsf_shift, qqr, qcut);
+    ChargeEvaluatorNone none;
+    if (ntpa < 2) return -2;
+    const float q2 = qcut * qcut;
+#define MDX_REF_LAUNCH(EV, NP, CE, HASQ, ev_, ce_)                                                              \
+    compute_force_iso<EV, true, NP, false, CE, HASQ, 1><<<blocks, ntpb, smem>>>(                                \
+        n, 1, dx, df, dc, dl, dcum, 32, dp, ntypes, b, c12, c13, c14, nullptr, dq, HASQ ? q2 : 0.f, ntpa, ev_, \
+        ce_)
+    auto launch = [&]() {
+        if (lj_kind == 3 && ck == 0) MDX_REF_LAUNCH(EvaluatorLJFS, 4, ChargeEvaluatorNone, false, EvaluatorLJFS(), none);
+        else if (lj_kind == 3 && ck == 1) MDX_REF_LAUNCH(EvaluatorLJFS, 4, ChargeEvaluatorEwald, true, EvaluatorLJFS(), ew);
+        else if (lj_kind == 3 && ck == 2) MDX_REF_LAUNCH(EvaluatorLJFS, 4, ChargeEvaluatorDSF, true, EvaluatorLJFS(), dsf);
+        else if (lj_kind == 4 && ck == 0) MDX_REF_LAUNCH(EvaluatorCHARMM, 5, ChargeEvaluatorNone, false, EvaluatorCHARMM(c14), none);
+        else if (lj_kind == 4 && ck == 1) MDX_REF_LAUNCH(EvaluatorCHARMM, 5, ChargeEvaluatorEwald, true, EvaluatorCHARMM(c14), ew);
+        else if (lj_kind == 4 && ck == 2) MDX_REF_LAUNCH(EvaluatorCHARMM, 5, ChargeEvaluatorDSF, true, EvaluatorCHARMM(c14), dsf);
+        else if (lj_kind == 5 && ck == 0) MDX_REF_LAUNCH(EvaluatorTICG, 2, ChargeEvaluatorNone, false, EvaluatorTICG(), none);
+        else if (lj_kind == 1 && ck == 2) MDX_REF_LAUNCH(EvaluatorLJ, 3, ChargeEvaluatorDSF, true, EvaluatorLJ(), dsf);
+    };
+#undef MDX_REF_LAUNCH
+    const bool known = (lj_kind == 3 || lj_kind == 4) ? (ck >= 0 && ck <= 2)
+                                                      : ((lj_kind == 5 && ck == 0) || (lj_kind == 1 && ck == 2));
+    if (!known) return -1;
+    launch();
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(hf.data(), df, n * sizeof(float4), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) time_launches(launch);
+    std::memcpy(fs4_out, hf.data(), n * sizeof(float4));
+    cudaFree(dx); cudaFree(df); cudaFree(dq); cudaFree(dp); cudaFree(dc); cudaFree(dl); cudaFree(dcum);
+    return e == cudaSuccess ? 0 : (int)e;
+}
+
 // compute_E3B_force_twobody + compute_E3B_force_threebody (FixE3B::compute,
 // FixE3B.cu:85-347) with the molecule list given (molecule indices), atoms
 // in the given order, E3B3 or E3B2 parameters as FixE3B::createEvaluator.
@@ -203,6 +262,26 @@ void ref_lj_force_host(float sigma, float eps, float rcut, const float dr[3], fl
     out[0] = f.x;
     out[1] = f.y;
     out[2] = f.z;
+}
+
+// the reference's host-callable force-shifted LJ functor (PairEvaluatorLJFS.h
+// :15-57) on the parameters EvaluatorLJFS::forcePy / energyPy form for one
+// pair (PairEvaluatorLJFS.cu): {rc^2, 24 eps, sig^6, F(rc)}; out = force
+// (3), energy at |dr|
+void ref_ljfs_host(float sigma, float eps, float rcut, const float dr[3], float out[4]) {
+    EvaluatorLJFS lj;
+    const float sig2 = sigma * sigma, sig6 = sig2 * sig2 * sig2;
+    const float eps24 = eps * 24.0f, rc2 = rcut * rcut;
+    const float rc_inv2 = 1.0f / rc2, rc_inv = 1.0f / rcut, rc_inv6 = rc_inv2 * rc_inv2 * rc_inv2;
+    const float fcut = eps24 * rc_inv * rc_inv6 * ((2.0f * sig6 * sig6 * rc_inv6) - sig6);
+    float params[4] = {rc2, eps24, sig6, fcut};
+    float3 d = make_float3(dr[0], dr[1], dr[2]);
+    const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+    float3 f = lj.force(d, params, r2, 1.0f);
+    out[0] = f.x;
+    out[1] = f.y;
+    out[2] = f.z;
+    out[3] = lj.energy(params, r2, 1.0f);
 }
 
 // EvaluatorE3B host/device scalar functions (EvaluatorE3B.h:91-141)

@@ -34,6 +34,9 @@ def lib():
         _L.ref_last_ms.restype = F
         _L.ref_lj_force_host.argtypes = [F, F, F, V, V]
         _L.ref_e3b_single_host.argtypes = [F, V]
+        _L.ref_ljfs_host.argtypes = [F, F, F, V, V]
+        _L.ref_pair_styles.argtypes = [I, V, V, V, V, I, V, I, I, V, V, F, F, F, I, I, F, F, F, F, F, I, I, V]
+        _L.ref_pair_styles.restype = I
     return _L
 
 
@@ -57,6 +60,35 @@ def pair_forces(xs4, q, counts, nbr, params_flat, ntypes, lo, L, coef, lj_kind, 
     if rc != 0:
         raise RuntimeError(f"reference pair kernel failed: {rc}")
     return out[:, :3].astype(np.float64)
+
+
+def pair_styles(xs4, q, counts, nbr, table, ntypes, lo, L, coef, lj_kind, ck, qcut=0.0, alpha=0.0, qqr=1.0,
+                dsf_A=0.0, dsf_shift=0.0, ntpb=256, ntpa=8):
+    """the reference's compute_force_iso with EvaluatorLJFS (lj_kind 3),
+    EvaluatorCHARMM (4), EvaluatorTICG (5) or EvaluatorLJ (1, with DSF) and
+    ChargeEvaluatorNone / Ewald / DSF (ck 0 / 1 / 2); table: np x nt x nt"""
+    xs4 = np.ascontiguousarray(xs4, np.float32)
+    n = len(xs4)
+    q = np.ascontiguousarray(q if q is not None else np.zeros(n), np.float32)
+    counts = np.ascontiguousarray(counts, np.int32)
+    nbr = np.ascontiguousarray(nbr, np.uint32)
+    tb = np.ascontiguousarray(table, np.float32)
+    lo = np.ascontiguousarray(lo, np.float32)
+    L = np.ascontiguousarray(L, np.float32)
+    out = np.zeros((n, 4), np.float32)
+    rc = lib().ref_pair_styles(n, _p(xs4), _p(q), _p(counts), _p(nbr), nbr.shape[1], _p(tb), tb.shape[0], ntypes,
+                               _p(lo), _p(L), coef[0], coef[1], coef[2], lj_kind, ck, qcut, alpha, qqr, dsf_A,
+                               dsf_shift, ntpb, ntpa, _p(out))
+    if rc != 0:
+        raise RuntimeError(f"reference pair kernel failed: {rc}")
+    return out[:, :3].astype(np.float64)
+
+
+def ljfs_host(sigma, eps, rcut, dr):
+    d = np.ascontiguousarray(dr, np.float32)
+    o = np.zeros(4, np.float32)
+    lib().ref_ljfs_host(sigma, eps, rcut, _p(d), _p(o))
+    return o
 
 
 def e3b_forces(xs4, mol, mcounts, mnbr, lo, L, style3=True, ntpb=256, ntpa=8):

@@ -308,3 +308,75 @@ def test_e3b_and_p3m_virials_are_volume_derivatives(oracle):
 
     d = (rec(h) - rec(-h)) / (2 * h)
     assert abs(vir[:3].sum() + d) < 1e-6 * abs(d)
+
+
+def _two_atom_style(oracle, kind, table, dr, coef=(1.0, 0.0, 0.0, 0.5), ck=0, q=None, qrc=0.0, alpha=0.0,
+                    dsf=None):
+    """force on atom 0 and the pair energy of a two-atom system (atom 1 at the
+    origin, atom 0 at dr) by the oracle's pair styles; the per-atom energy
+    of atom 0 is half of it (the reference half-counts each ordered pair)"""
+    x = np.array([dr, [0.0, 0.0, 0.0]], np.float64)
+    counts = np.array([1, 1], np.int32)
+    nbr = np.array([[1], [0]], np.uint32)
+    out = oracle.pair_forces_styles(x, [0, 0], q, table, [50.0, 50.0, 50.0], counts, nbr, coef=coef, lj_kind=kind,
+                                    ck=ck, qrc=qrc, alpha=alpha, dsf=dsf, want=("f", "energy"))
+    return out["f"][0], out["energy"].sum()
+
+
+def test_ljfs_vs_committed_reference_functor_vectors(oracle):
+    """the force-shifted LJ (FixLJCutFS) of the oracle against the reference's
+    EvaluatorLJFS::force / energy on the parameters its forcePy forms, from
+    the committed golden vectors; force and energy vanish at the cutoff"""
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "ref_functors.json")) as f:
+        g = json.load(f)
+    assert len(g["ljfs"]) > 20
+    for v in g["ljfs"]:
+        tb = oracle.style_params(3, 1, eps={(0, 0): v["eps"]}, sig={(0, 0): v["sigma"]}, rcut=v["rcut"])
+        dr = np.array(v["dr"], np.float64)
+        fo, eo = _two_atom_style(oracle, 3, tb, dr)
+        assert np.max(np.abs(np.array(v["force"]) - fo)) <= 2e-5 * max(1.0, np.abs(fo).max())
+        # the functor adds F(rc) (rc - r) / 2 to the half-counted energy; the
+        # oracle the force-consistent F(rc) (r - rc) / 2 its comment documents
+        fcut, r = tb[3, 0, 0], np.linalg.norm(dr)
+        assert abs(v["energy"] + fcut * (r - v["rcut"]) - 0.5 * eo) <= 2e-5 * max(1.0, abs(eo))
+    tb = oracle.style_params(3, 1, eps={(0, 0): 0.8}, sig={(0, 0): 1.1}, rcut=2.5)
+    f, e = _two_atom_style(oracle, 3, tb, np.array([2.5 - 1e-9, 0.0, 0.0]))
+    assert abs(f[0]) < 1e-7 and abs(e) < 1e-9
+
+
+def test_pair_style_forces_are_energy_gradients(oracle):
+    """every pair style and charge term of the oracle: the force equals minus
+    the gradient of its energy (central differences), away from the cutoff"""
+    cases = [
+        (1, oracle.style_params(1, 1, eps={(0, 0): 0.9}, sig={(0, 0): 1.0}, rcut=2.5), 0, 1.0),
+        (3, oracle.style_params(3, 1, eps={(0, 0): 0.9}, sig={(0, 0): 1.0}, rcut=2.5), 0, 1.0),
+        (4, oracle.style_params(4, 1, eps={(0, 0): 0.9}, sig={(0, 0): 1.0}, rcut=2.5,
+                                eps14={(0, 0): 0.4}, sig14={(0, 0): 0.8}), 0, 1.0),
+        (4, oracle.style_params(4, 1, eps={(0, 0): 0.9}, sig={(0, 0): 1.0}, rcut=2.5,
+                                eps14={(0, 0): 0.4}, sig14={(0, 0): 0.8}), 0, 0.5),
+        (5, oracle.style_params(5, 1, C={(0, 0): 3.0}, rcut_pairs={(0, 0): 2.0}), 0, 1.0),
+        (0, np.zeros((3, 1, 1)), 2, 1.0),
+    ]
+    dsf = oracle.dsf_constants(0.25, 9.0)
+    for kind, tb, ck, mult in cases:
+        coef = (1.0, 0.5, 0.0, 0.5)
+        q = np.array([0.7, -0.4])
+        dr = np.array([1.05, 0.31, -0.22]) * (4.0 if ck else 1.0)
+        tag_coef = (1.0, 0.0, 0.0, mult) if mult != 1.0 else coef
+        f, _ = _two_atom_style(oracle, kind, tb, dr, coef=tag_coef if mult == 1.0 else (mult, 0.0, 0.0, mult),
+                               ck=ck, q=q, qrc=9.0, alpha=0.25, dsf=dsf)
+        h = 1e-6
+        g = np.zeros(3)
+        for d in range(3):
+            e1 = np.array(dr)
+            e2 = np.array(dr)
+            e1[d] += h
+            e2[d] -= h
+            c = tag_coef if mult == 1.0 else (mult, 0.0, 0.0, mult)
+            g[d] = -(_two_atom_style(oracle, kind, tb, e1, coef=c, ck=ck, q=q, qrc=9.0, alpha=0.25, dsf=dsf)[1] -
+                     _two_atom_style(oracle, kind, tb, e2, coef=c, ck=ck, q=q, qrc=9.0, alpha=0.25, dsf=dsf)[1]) / (2 * h)
+        # the pair energy is counted once per atom (half each): d/dx of the sum
+        # is the force on atom 0
+        assert np.allclose(f, g, rtol=1e-5, atol=1e-8), (kind, ck, mult, f, g)
