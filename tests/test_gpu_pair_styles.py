@@ -56,7 +56,9 @@ def _check(oracle, st, sysd, types, table, kind, ck=0, q=None, qrc=0.0, alpha=0.
     assert rms > 0.1
     assert rel < FORCE_RTOL, f"max force error {rel:.3e} of RMS {rms:.3e}"
     e_ref = float(ref["energy"].sum())
-    assert abs(eg - e_ref) < 1e-5 * abs(e_ref) + 1e-4, (eg, e_ref)
+    # the per-site energies cancel in the sum (DSF charges): scale the FP32
+    # tolerance by their magnitudes
+    assert abs(eg - e_ref) < 1e-5 * float(np.abs(ref["energy"]).sum()) + 1e-4, (eg, e_ref)
     vr = ref["virial"].sum(0)
     assert np.abs(vg - vr).max() < 2e-4 * np.abs(vr).max()
     R = pytest.importorskip("oracle.refkernels")
