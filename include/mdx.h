@@ -117,6 +117,10 @@ int mdx_fix_charge_pair_dsf_set_parameters(mdx_fix *fix, double alpha, double r_
  * LJCutFS), + "eps14", "sig14" (LJCHARMM), "C", "rCut" (TICG) */
 int mdx_fix_pair_set_parameter(mdx_fix *fix, const char *param, const char *handle_a, const char *handle_b,
                                double value);
+/* FixPair::getParameter(param, handleA, handleB) (FixPair.cpp:173-200): the
+ * raw value set (or read from a restart); -1000 (DEFAULT_FILL) when unset */
+int mdx_fix_pair_get_parameter(mdx_fix *fix, const char *param, const char *handle_a, const char *handle_b,
+                               double *value);
 /* FixChargeEwald(state, handle, group) (src/Fixes/FixChargeEwald.cu:828-839) */
 int mdx_fix_charge_ewald_create(mdx_state *st, const char *handle, const char *group, mdx_fix **out);
 /* FixChargeEwald::setParameters(sz, rcut, order) (src/Fixes/FixChargeEwald.cu:969-1021);
@@ -322,6 +326,58 @@ int mdx_batch_run_timed(mdx_batch *b, int num_turns, int chunk, size_t flush_byt
  * it before the production run: the timing runs start from the initial state. */
 int mdx_batch_autotune(mdx_batch *b, int steps, const int *teams, int nteams, int *best_team, double *best_ms);
 int mdx_batch_destroy(mdx_batch *b);
+
+/* ---- configuration IO (src/WriteConfig.cpp, src/ReadConfig.cpp) ---------- */
+typedef struct mdx_writer mdx_writer;
+/* WriteConfig(state, fn, handle, format, writeEvery, groupHandle,
+ * unwrapMolecules) (WriteConfig.cpp:389-416, Python signature at
+ * WriteConfig.cpp:442-453).  format "base64" (writeXMLfileBase64,
+ * WriteConfig.cpp:91-162), "xyz" (writeXYZFile, :206-251), "lammpstrj"
+ * (writeLAMMPSTRJFile, :165-203), anything else the plain "xml" form
+ * (writeXMLfile, :253-343, with the fixes' restart chunks).  fn gets the
+ * format's suffix; a '*' in fn is replaced by the turn and makes every write
+ * its own file, else writes append to one file opened (and emptied) here.
+ * group_handle NULL = "all". */
+int mdx_write_config_create(mdx_state *st, const char *fn, const char *handle, const char *format, int write_every,
+                            const char *group_handle, int unwrap_molecules, mdx_writer **out);
+/* WriteConfig attributes (WriteConfig.cpp:446-451): "writeEvery",
+ * "unwrapMolecules", "writingVelocities", "writingForces" (xyz columns) */
+int mdx_write_config_set(mdx_writer *w, const char *key, int64_t value);
+/* WriteConfig::writePy (WriteConfig.cpp:433-439) for turn < 0 (the state's
+ * turn; xyz in real units guesses atomic numbers from the masses first), else
+ * WriteConfig::write(turn) (:427-432) */
+int mdx_write_config_write(mdx_writer *w, int64_t turn);
+/* WriteConfig::finish (closes the single-file XML's <data>) and release */
+int mdx_write_config_destroy(mdx_writer *w);
+/* State::activateWriteConfig / deactivateWriteConfig (State.cpp:475-480): an
+ * active writer fires inside mdx_integrator_run after the step of every turn
+ * that is a multiple of its writeEvery (Integrator::asyncOperations,
+ * Integrator.cu:77-113) */
+int mdx_state_activate_write_config(mdx_state *st, mdx_writer *w);
+int mdx_state_deactivate_write_config(mdx_state *st, mdx_writer *w);
+/* Integrator::writeOutput (Integrator.cu:265-269): every active writer now */
+int mdx_write_output(mdx_state *st);
+/* ReadConfig::loadFile (ReadConfig.cpp:319-332) */
+int mdx_read_config_load(mdx_state *st, const char *fn);
+/* ReadConfig::next (op 0), prev (op 1), moveBy(by) (op 2)
+ * (ReadConfig.cpp:259-315): *found = 0 when there is no such configuration;
+ * else the state's atoms, species, bounds, turn, rCut, padding, dt, groups and
+ * molecules are replaced by the configuration's (ReadConfig::read,
+ * ReadConfig.cpp:176-257), and fixes created afterwards read their restart
+ * chunk from it (FixPair::readFromRestart, FixPair.cpp:211-240;
+ * FixRigid::readFromRestart, FixRigid.cu:1458-1514).  Atom ids must be
+ * 0..numAtoms-1 (this library's ids are indices). */
+int mdx_read_config_move(mdx_state *st, int op, int by, int *found);
+/* State::createGroup(handle, ids) (State.cpp:878-889): the next free tag bit */
+int mdx_state_create_group(mdx_state *st, const char *handle, int n, const int *ids);
+int mdx_state_group_tag(mdx_state *st, const char *handle, uint32_t *bit);
+/* State::createMolecule(ids) (State.cpp createMoleculePy): written to
+ * <molecules> and unwrapped by writers with unwrapMolecules */
+int mdx_state_create_molecule(mdx_state *st, int n, const int *ids);
+/* the state's bounds and species as a read configuration left them */
+int mdx_state_get_bounds(mdx_state *st, double lo[3], double hi[3]);
+/* species k (handle copied into handle[0..cap)); k < 0 only sets *count */
+int mdx_state_get_species(mdx_state *st, int k, char *handle, int cap, double *mass, int *atomic_num, int *count);
 
 #ifdef __cplusplus
 }

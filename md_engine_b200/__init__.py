@@ -5,5 +5,5 @@ velocity-Verlet / Nose-Hoover update, as hand-written sm_100a CUDA behind the
 C ABI of include/mdx.h (libmdx.so)."""
 from .dash import (Bounds, FixChargeEwald, FixChargePairDSF, FixE3B, FixLJCHARMM, FixLJCut,  # noqa: F401
                    FixLJCutFS, FixNoseHoover, FixRigid, FixTICG, FixWCA, BatchReplicas, IntegratorVerlet, State,
-                   Vector, kernel_launches)
+                   Vector, WriteConfig, kernel_launches)
 from ._lib import LIB_PATH, MdxError, lib  # noqa: F401

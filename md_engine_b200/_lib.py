@@ -56,6 +56,7 @@ SIGNATURES = [
     ("mdx_fix_charge_pair_dsf_create", c_int, [c_void_p, c_char_p, c_char_p, P(c_void_p)]),
     ("mdx_fix_charge_pair_dsf_set_parameters", c_int, [c_void_p, c_dbl, c_dbl]),
     ("mdx_fix_pair_set_parameter", c_int, [c_void_p, c_char_p, c_char_p, c_char_p, c_dbl]),
+    ("mdx_fix_pair_get_parameter", c_int, [c_void_p, c_char_p, c_char_p, c_char_p, P(c_dbl)]),
     ("mdx_fix_charge_ewald_create", c_int, [c_void_p, c_char_p, c_char_p, P(c_void_p)]),
     ("mdx_fix_charge_ewald_set_parameters", c_int, [c_void_p, c_int, c_int, c_int, c_dbl, c_int]),
     ("mdx_fix_charge_ewald_set_alpha", c_int, [c_void_p, c_dbl]),
@@ -114,6 +115,21 @@ SIGNATURES = [
     ("mdx_batch_run_timed", c_int, [c_void_p, c_int, c_int, ctypes.c_size_t, P(c_dbl)]),
     ("mdx_batch_autotune", c_int, [c_void_p, c_int, P(c_int), c_int, P(c_int), P(c_dbl)]),
     ("mdx_batch_destroy", c_int, [c_void_p]),
+    ("mdx_write_config_create", c_int, [c_void_p, c_char_p, c_char_p, c_char_p, c_int, c_char_p, c_int,
+                                        P(c_void_p)]),
+    ("mdx_write_config_set", c_int, [c_void_p, c_char_p, c_i64]),
+    ("mdx_write_config_write", c_int, [c_void_p, c_i64]),
+    ("mdx_write_config_destroy", c_int, [c_void_p]),
+    ("mdx_state_activate_write_config", c_int, [c_void_p, c_void_p]),
+    ("mdx_state_deactivate_write_config", c_int, [c_void_p, c_void_p]),
+    ("mdx_write_output", c_int, [c_void_p]),
+    ("mdx_read_config_load", c_int, [c_void_p, c_char_p]),
+    ("mdx_read_config_move", c_int, [c_void_p, c_int, c_int, P(c_int)]),
+    ("mdx_state_create_group", c_int, [c_void_p, c_char_p, c_int, P(c_int)]),
+    ("mdx_state_group_tag", c_int, [c_void_p, c_char_p, P(c_u32)]),
+    ("mdx_state_create_molecule", c_int, [c_void_p, c_int, P(c_int)]),
+    ("mdx_state_get_bounds", c_int, [c_void_p, P(c_dbl), P(c_dbl)]),
+    ("mdx_state_get_species", c_int, [c_void_p, c_int, c_char_p, c_int, P(c_dbl), P(c_int), P(c_int)]),
 ]
 
 

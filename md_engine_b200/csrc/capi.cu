@@ -53,6 +53,7 @@ int mdx_state_create(mdx_state **out) {
 int mdx_state_destroy(mdx_state *st) {
     if (!st) return 0;
     if (st->s->stream) cudaStreamSynchronize(st->s->stream);
+    config_state_detach(*st->s);
     delete st->s;
     delete st;
     return 0;
@@ -328,7 +329,14 @@ int mdx_state_synchronize(mdx_state *st) {
 }
 
 // ---- fixes ---------------------------------------------------------------
+// every fix constructor of the reference ends with readFromRestart(): the
+// fix takes its parameters / molecules from the configuration the state's
+// reader is on, when that configuration holds a fix of its type and handle
 static int new_fix(mdx_state *st, Fix *f, mdx_fix **out) {
+    if (int e = config_fix_restart(*st->s, *f)) {
+        delete f;
+        return e;
+    }
     *out = new mdx_fix{f, st};
     return 0;
 }
@@ -390,6 +398,27 @@ int mdx_fix_pair_set_parameter(mdx_fix *fix, const char *param, const char *ha, 
     }
     s.prepared = false;
     return static_cast<FixPair *>(fix->f)->setParameter(param, a, b, value);
+}
+
+int mdx_fix_pair_get_parameter(mdx_fix *fix, const char *param, const char *ha, const char *hb, double *value) {
+    ARG_CHECK(fix && param && ha && hb && value, "null argument");
+    ARG_CHECK(fix->f->kind == FixKind::Pair, "not a pair fix");
+    FixPair &p = *static_cast<FixPair *>(fix->f);
+    State &s = *p.state;
+    int a = s.typeFromHandle(ha), b = s.typeFromHandle(hb);
+    if (a < 0 || b < 0) {
+        set_error(MDX_ERR_ARG, "unknown species handle '%s' or '%s'", ha, hb);
+        return MDX_ERR_ARG;
+    }
+    auto it = p.params.find(param);
+    if (it == p.params.end()) {
+        set_error(MDX_ERR_ARG, "unknown pair parameter '%s'", param);
+        return MDX_ERR_ARG;
+    }
+    p.ensureSize();
+    const double v = it->second[(size_t)a * s.species.size() + b];
+    *value = std::isnan(v) ? -1000.0 : v;  // unset entries read as DEFAULT_FILL
+    return 0;
 }
 
 int mdx_fix_charge_ewald_create(mdx_state *st, const char *handle, const char *group, mdx_fix **out) {

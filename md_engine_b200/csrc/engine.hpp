@@ -135,6 +135,19 @@ struct HostAtom {
 };
 
 class State;
+class Fix;
+// configuration IO (WriteConfig.cpp, ReadConfig.cpp): host-only, in config_io.cu
+struct ConfigWriter;
+struct ConfigReader;
+// the smallest turn >= t at which an active writer fires, or -1
+int64_t config_next_write(const State &s, int64_t t);
+// writes every active writer due at `turn` (state's host copy current)
+int config_write_due(State &s, int64_t turn);
+// a new fix's readFromRestart: parameters / molecules from the configuration
+// the state's reader is on (no-op without one)
+int config_fix_restart(State &s, Fix &f);
+// the state is going away: its writers stop writing, its reader is freed
+void config_state_detach(State &s);
 
 // ---------------------------------------------------------------- GPUData
 // Per-atom device streams (src/GPUData.h:18-28): xs (type bits in .w),
@@ -478,6 +491,14 @@ class State {
     bool uploaded = false;   // device copy is authoritative
     bool prepared = false;
     bool requiresCharges = false;
+    // host-side bookkeeping of the reference's State used by configuration
+    // IO: group tags (bit 0 = "all", State.cpp:31), molecules
+    // (State::createMolecule), active writers, the configuration reader
+    int periodic[3] = {1, 1, 1};
+    std::map<std::string, uint32_t> groupTags{{"all", 1u}};
+    std::vector<std::vector<int>> molecules;
+    std::vector<ConfigWriter *> writers;
+    ConfigReader *reader = nullptr;
     State();
     ~State();
     int typeFromHandle(const std::string &h) const;

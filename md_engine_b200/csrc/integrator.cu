@@ -346,6 +346,11 @@ class IntegratorVerlet {
             const bool check = (t % P) == 0;
             int chunk = check ? P : (int)(P - (t % P));
             if (chunk > nturns - done) chunk = nturns - done;
+            // configuration writers (Integrator::asyncOperations,
+            // Integrator.cu:77-113): a writer due at turn T writes after that
+            // turn's step, so the chunk ends there
+            const int64_t wt = config_next_write(*s, t);
+            if (wt >= 0 && wt - t + 1 < chunk) chunk = (int)(wt - t + 1);
             if (mode == 0) {
                 if (int e = launchGraph(chunk, check)) return e;
             } else {
@@ -353,6 +358,10 @@ class IntegratorVerlet {
             }
             s->turn += chunk;
             done += chunk;
+            if (wt >= 0 && s->turn == wt + 1) {
+                if (int e = s->checkStatus()) return e;
+                if (int e = config_write_due(*s, wt)) return e;
+            }
         }
         MDX_CUDA_TRY(cudaEventRecord(e1, s->stream));
         if (nturns > 0)

@@ -324,7 +324,7 @@ int State::prepare() {
 static const char *pair_type_name(int kind) {
     switch (kind) {
         case 1: return "LJCut";
-        case 2: return "WCA";
+        case 2: return "LJCutWCA";
         case 3: return "LJCutFS";
         case 4: return "LJCHARMM";
         default: return "TICG";

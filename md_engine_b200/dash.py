@@ -76,12 +76,24 @@ class _AtomParams:
         self.handles = []
         self.masses = []
 
-    def addSpecies(self, handle, mass, atomicNum=0):
+    def addSpecies(self, handle, mass, atomicNum=-1):
         t = c_int()
         check(lib().mdx_state_add_species(self._st._h, handle.encode(), float(mass), int(atomicNum), ctypes.byref(t)))
         self.handles.append(handle)
         self.masses.append(float(mass))
         return t.value
+
+    def _refresh(self):
+        """the species the library holds (after a configuration was read)"""
+        n = c_int()
+        check(lib().mdx_state_get_species(self._st._h, -1, None, 0, None, None, ctypes.byref(n)))
+        self.handles, self.masses = [], []
+        buf = ctypes.create_string_buffer(256)
+        for k in range(n.value):
+            m = c_dbl()
+            check(lib().mdx_state_get_species(self._st._h, k, buf, 256, ctypes.byref(m), None, None))
+            self.handles.append(buf.value.decode())
+            self.masses.append(m.value)
 
     def typeFromHandle(self, handle):
         return self.handles.index(handle)
@@ -94,6 +106,37 @@ class _AtomParams:
 def _darr(a, n=None):
     a = np.ascontiguousarray(a, dtype=np.float64)
     return a, a.ctypes.data_as(P(c_dbl))
+
+
+class _ReadConfig:
+    """state.readConfig (src/ReadConfig.cpp): loadFile(fn), then next(),
+    prev() or moveBy(n) load a configuration of the file into the state and
+    return whether there was one; fixes created afterwards read their restart
+    data from that configuration."""
+
+    def __init__(self, st):
+        self._st = st
+        self.fileOpen = False
+
+    def loadFile(self, fn):
+        check(lib().mdx_read_config_load(self._st._h, str(fn).encode()))
+        self.fileOpen = True
+
+    def _move(self, op, by=0):
+        found = c_int()
+        check(lib().mdx_read_config_move(self._st._h, op, int(by), ctypes.byref(found)))
+        if found.value:
+            self._st._after_read()
+        return bool(found.value)
+
+    def next(self):
+        return self._move(0)
+
+    def prev(self):
+        return self._move(1)
+
+    def moveBy(self, by):
+        return self._move(2, by)
 
 
 class State:
@@ -113,6 +156,8 @@ class State:
         object.__setattr__(self, "_fixes", [])
         object.__setattr__(self, "_units", UNITS_LJ)
         object.__setattr__(self, "_charges", [])
+        object.__setattr__(self, "readConfig", _ReadConfig(self))
+        object.__setattr__(self, "writeConfigs", [])
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -147,6 +192,40 @@ class State:
         if k == "bounds":
             return object.__getattribute__(self, "_bounds")
         raise AttributeError(k)
+
+    def _after_read(self):
+        self.atomParams._refresh()
+        lo = (ctypes.c_double * 3)()
+        hi = (ctypes.c_double * 3)()
+        check(lib().mdx_state_get_bounds(self._h, lo, hi))
+        object.__setattr__(self, "_bounds", Bounds(self, lo=Vector(*lo), hi=Vector(*hi)))
+
+    # -- configuration IO, groups, molecules --------------------------------
+    def activateWriteConfig(self, wc):
+        check(lib().mdx_state_activate_write_config(self._h, wc._h))
+        if wc not in self.writeConfigs:
+            self.writeConfigs.append(wc)
+        return True
+
+    def deactivateWriteConfig(self, wc):
+        check(lib().mdx_state_deactivate_write_config(self._h, wc._h))
+        if wc in self.writeConfigs:
+            self.writeConfigs.remove(wc)
+        return True
+
+    def createGroup(self, handle, atoms=()):
+        ids = np.ascontiguousarray(list(atoms), np.int32)
+        check(lib().mdx_state_create_group(self._h, handle.encode(), len(ids), ids.ctypes.data_as(P(c_int))))
+        return True
+
+    def groupTagFromHandle(self, handle):
+        b = c_u32()
+        check(lib().mdx_state_group_tag(self._h, handle.encode(), ctypes.byref(b)))
+        return b.value
+
+    def createMolecule(self, ids):
+        ids = np.ascontiguousarray(list(ids), np.int32)
+        check(lib().mdx_state_create_molecule(self._h, len(ids), ids.ctypes.data_as(P(c_int))))
 
     def setSpecialNeighborCoefs(self, onetwo, onethree, onefour):
         check(lib().mdx_state_set_special_neighbor_coefs(self._h, onetwo, onethree, onefour))
@@ -286,6 +365,12 @@ class _Fix:
 class FixPair(_Fix):
     def setParameter(self, param, handleA, handleB, val):
         check(lib().mdx_fix_pair_set_parameter(self._h, param.encode(), handleA.encode(), handleB.encode(), float(val)))
+
+    def getParameter(self, param, handleA, handleB):
+        out = c_dbl()
+        check(lib().mdx_fix_pair_get_parameter(self._h, param.encode(), handleA.encode(), handleB.encode(),
+                                               ctypes.byref(out)))
+        return out.value
 
 
 class FixLJCut(FixPair):
@@ -516,6 +601,58 @@ class FixNoseHoover(_Fix):
         check(lib().mdx_fix_nose_hoover_set_temperature(self._h, float(temperature), float(timeConstant)))
 
 
+class WriteConfig:
+    """WriteConfig(state, fn, handle, format, writeEvery, groupHandle='all',
+    unwrapMolecules=False) (src/WriteConfig.cpp:389-453): format 'base64',
+    'xml', 'xyz' or 'lammpstrj'; a '*' in fn writes one file per turn.  Fires
+    during runs once activated with state.activateWriteConfig; write() writes
+    the current configuration now."""
+
+    _KEYS = ("writeEvery", "unwrapMolecules", "writingVelocities", "writingForces")
+
+    def __init__(self, state, fn, handle, format, writeEvery, groupHandle="all", unwrapMolecules=False):
+        h = c_void_p()
+        check(lib().mdx_write_config_create(state._h, str(fn).encode(), handle.encode(), format.encode(),
+                                            int(writeEvery), groupHandle.encode(), int(bool(unwrapMolecules)),
+                                            ctypes.byref(h)))
+        object.__setattr__(self, "_h", h)
+        object.__setattr__(self, "state", state)
+        object.__setattr__(self, "handle", handle)
+        object.__setattr__(self, "format", format)
+        object.__setattr__(self, "_vals", {"writeEvery": int(writeEvery), "unwrapMolecules": bool(unwrapMolecules),
+                                           "writingVelocities": False, "writingForces": False})
+
+    def __setattr__(self, k, v):
+        if k in self._KEYS:
+            check(lib().mdx_write_config_set(self._h, k.encode(), int(v)))
+            self._vals[k] = type(self._vals[k])(v)
+        else:
+            object.__setattr__(self, k, v)
+
+    def __getattr__(self, k):
+        if k in WriteConfig._KEYS:
+            return object.__getattribute__(self, "_vals")[k]
+        raise AttributeError(k)
+
+    def write(self):
+        check(lib().mdx_write_config_write(self._h, -1))
+
+    def finish(self):
+        """close the file (the single-file XML's </data>); the writer is spent"""
+        h = object.__getattribute__(self, "_h")
+        if h is not None and h.value:
+            if self in self.state.writeConfigs:
+                self.state.writeConfigs.remove(self)
+            lib().mdx_write_config_destroy(h)
+            object.__setattr__(self, "_h", c_void_p())
+
+    def __del__(self):
+        try:
+            self.finish()
+        except Exception:
+            pass
+
+
 class IntegratorVerlet:
     """IntegratorVerlet(state).run(numTurns) (src/Integrators/IntegratorVerlet.cu:649-770)."""
 
@@ -532,6 +669,10 @@ class IntegratorVerlet:
                 lib().mdx_integrator_destroy(h)
             except Exception:
                 pass
+
+    def writeOutput(self):
+        """Integrator::writeOutput: every active writer writes now"""
+        check(lib().mdx_write_output(self.state._h))
 
     def setMode(self, mode):
         """0: fused, CUDA-graph captured (default); 1: one kernel per reference hook."""
