@@ -57,7 +57,11 @@ int mdx_state_set_bounds(mdx_state *st, const double lo[3], const double hi[3]);
  * "nThreadPerBlock", "turn" (int).  Tunables of this library's list build
  * (0 = automatic, the default): "gridStencil" (cells of at least
  * (rCut + padding) / gridStencil, 1..4), "gridHomeGroup" (2 or 4 home atoms
- * tested at once per warp).  Read-only: "nlistCapacity", "cellsPerSide". */
+ * tested at once per warp).  "pairForm": 0 automatic (the molecule form for
+ * all-rigid four-site water), 1 per-site list, 2 molecule form.
+ * "pairBlocksPerSM": molecule form, cap on the pair kernel's grid in blocks
+ * per SM (0 = automatic, -1 = uncapped: one warp per molecule).  Read-only:
+ * "nlistCapacity", "cellsPerSide", "molListCapacity". */
 int mdx_state_set_double(mdx_state *st, const char *key, double value);
 int mdx_state_get_double(mdx_state *st, const char *key, double *value);
 int mdx_state_set_int(mdx_state *st, const char *key, int64_t value);
@@ -170,7 +174,9 @@ int mdx_integrator_run_timed(mdx_integrator *it, int num_turns, int chunk, size_
 /* Benchmark support (no reference counterpart): average device time of one
  * launch of a hot-path stage over `iters` launches, L2 flushed between them.
  * stage 0 pair forces, 1 P3M reciprocal (spread+FFT+field+gather), 2 E3B,
- * 3 neighbour-list rebuild (forced), 4 fused first half, 5 fused second half */
+ * 3 neighbour-list rebuild (forced), 4 fused first half, 5 fused second half;
+ * the fused step's P3M chain as it runs there: 6 spread, 7 solve (FFT, field,
+ * inverse FFT), 8 gather, 9 all three */
 int mdx_time_stage(mdx_state *st, int stage, int iters, size_t flush_bytes, double *avg_ms);
 
 /* ---- stage-level hot path ------------------------------------------------ */

@@ -120,7 +120,10 @@ int mdx_state_set_int(mdx_state *st, const char *key, int64_t v) {
     else if (k == "nThreadPerBlock") s.nThreadPerBlock = (int)v;
     else if (k == "gridStencil") s.gridStencil = (int)v;
     else if (k == "gridHomeGroup") s.gridHomeGroup = (int)v;
-    else if (k == "pairForm") {
+    else if (k == "pairBlocksPerSM") {
+        ARG_CHECK(v >= -1 && v <= 32, "pairBlocksPerSM must be -1 (uncapped), 0 (automatic) or 1..32");
+        s.pairBlocksPerSM = (int)v;
+    } else if (k == "pairForm") {
         ARG_CHECK(v >= 0 && v <= 2, "pairForm must be 0 (automatic), 1 (per-site) or 2 (molecule)");
         s.pairForm = (int)v;
     } else if (k == "turn") s.turn = v;
@@ -146,6 +149,7 @@ int mdx_state_get_int(mdx_state *st, const char *key, int64_t *v) {
     else if (k == "gridHomeGroup") *v = s.grid.home_group;
     else if (k == "pairForm") *v = s.prepared ? (s.mf.on ? 2 : 1) : s.pairForm;
     else if (k == "molListCapacity") *v = s.mf.cap;
+    else if (k == "pairBlocksPerSM") *v = s.pairBlocksPerSM;
     else {
         set_error(MDX_ERR_ARG, "unknown int key '%s'", key);
         return MDX_ERR_ARG;
@@ -769,6 +773,25 @@ int mdx_time_stage(mdx_state *st, int stage, int iters, size_t flush_bytes, doub
             case 3: e = nlist_rebuild(s, true, false); break;
             case 4: e = step_first_half(s, true); break;
             case 5: e = step_second_half(s, true); break;
+            case 6:
+            case 7:
+            case 8:
+            case 9: {
+                // the fused step's P3M chain as it runs there (by molecule
+                // for all-rigid water, gather into the per-step buffer):
+                // 6 spread, 7 solve (the FFT chain), 8 gather, 9 all three
+                FixChargeEwald *w = s.ewaldFix();
+                ARG_CHECK(w, "no FixChargeEwald");
+                FixRigid *r = s.rigidFix();
+                const bool side = r && !has_free_atoms(s);
+                const bool mol = side && w->mol_form_ok(*r);
+                if (stage == 6 || stage == 9) e = mol ? w->spread_mol(s.stream, *r) : w->spread(s.stream);
+                if (!e && (stage == 7 || stage == 9)) e = w->solve(s.stream);
+                if (!e && (stage == 8 || stage == 9))
+                    e = side ? (mol ? w->gather_mol_to(w->f_recip.p, s.stream, *r) : w->gather_to(w->f_recip.p, s.stream))
+                             : w->gather(true, s.stream);
+                break;
+            }
             default: ARG_CHECK(false, "unknown stage");
         }
         if (e) return e;

@@ -38,6 +38,8 @@ constexpr int kE3BTeam = 16;
 // kept as a node priority by graphs instantiated with
 // cudaGraphInstantiateFlagUseNodePriority
 int high_priority();
+// SMs of the current device (cached per device)
+int num_sms();
 template <typename... KArgs, typename... Args>
 inline cudaError_t launch_pdl_prio(bool high, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
                                    cudaStream_t st, Args... args) {
@@ -459,6 +461,11 @@ class State {
     // 0 automatic (molecule form when the system allows it), 1 per-site
     // (atom) form, 2 molecule form (an error at prepare when not allowed)
     int pairForm = 0;
+    // molecule form: cap on the pair kernel's grid in blocks per SM (0
+    // automatic, -1 uncapped: one warp per molecule); a capped grid strides
+    // over the molecules and leaves every SM room for the P3M chain running
+    // beside it
+    int pairBlocksPerSM = 0;
     MolForm mf;
     // list build tunables, 0 = automatic: cells of >= cut/gridStencil (1..4),
     // home atoms tested at once per warp (2 or 4)

@@ -212,14 +212,20 @@ __device__ __forceinline__ float mol_pair_term(const MolPairArgs &A, int ab, flo
     return s;
 }
 
+// asynchronous 16-byte global -> shared copies (cp.async, cached in L1): a
+// batch of neighbour molecules is staged while the warp scans the next chunk
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 // one queued molecule pair: every interacting site pair of slot k (sites
-// xi, the shift already taken off) and slot j
+// xi, the shift already taken off) and the neighbour's sites xj
 template <int LJ, bool EW, bool VIR, bool ENERGY, int TOPO>
-__device__ __forceinline__ void mol_pair_eval(const MolPairArgs &A, const float3 (&xi)[4], int j, float3 shift,
-                                              float3 (&f)[4], float (&en)[4], float (&v)[4][6]) {
-    float3 xj[4];
-#pragma unroll
-    for (int b = 0; b < 4; b++) xj[b] = f3(__ldg(A.xs + 4 * j + b));
+__device__ __forceinline__ void mol_pair_eval_x(const MolPairArgs &A, const float3 (&xi)[4], const float3 (&xj)[4],
+                                                float3 shift, float3 (&f)[4], float (&en)[4], float (&v)[4][6]) {
     const uint32_t any = TOPO == 1 ? 0xEEE1u : ((LJ ? A.ljm : 0u) | (EW ? A.qm : 0u));
 #pragma unroll
     for (int a = 0; a < 4; a++) {
@@ -242,129 +248,178 @@ __device__ __forceinline__ void mol_pair_eval(const MolPairArgs &A, const float3
 }
 
 template <int LJ, bool EW, bool VIR, bool ENERGY, int TOPO>
-__global__ void __launch_bounds__(kMolPairBlock) k_pair_mol(const MolPairArgs A, int accumulate) {
+__device__ __forceinline__ void mol_pair_eval(const MolPairArgs &A, const float3 (&xi)[4], int j, float3 shift,
+                                              float3 (&f)[4], float (&en)[4], float (&v)[4][6]) {
+    float3 xj[4];
+#pragma unroll
+    for (int b = 0; b < 4; b++) xj[b] = f3(__ldg(A.xs + 4 * j + b));
+    mol_pair_eval_x<LJ, EW, VIR, ENERGY, TOPO>(A, xi, xj, shift, f, en, v);
+}
+
+// one warp per molecule slot; the grid strides over the slots, so a grid
+// capped below the device's capacity leaves room on every SM for the P3M
+// chain's blocks that run beside it.  The row is scanned in 32-entry chunks
+// (ids loaded two chunks ahead, first sites one chunk ahead); the entries
+// within the far cutoff queue up in shared memory, and each full batch of
+// 32 has its four sites staged into shared memory by cp.async while the
+// warp scans the next chunk, then is evaluated one entry per lane.
+template <int LJ, bool EW, bool VIR, bool ENERGY, int TOPO>
+__global__ void __launch_bounds__(kMolPairBlock, 14) k_pair_mol(const MolPairArgs A, int accumulate) {
     pdl_wait();
     __shared__ int q_j[kMolPairBlock / 32][kMolQueue];
     __shared__ float4 q_s[kMolPairBlock / 32][kMolQueue];
+    __shared__ float4 s_b[kMolPairBlock / 32][4][32];  // staged batch: site b of entry lane
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const bool valid = k < A.nmol;  // warp-uniform
     int *const qj = q_j[wib];
     float4 *const qs = q_s[wib];
-    float3 xi[4], f[4];
-    float en[4], v[4][6];
-#pragma unroll
-    for (int a = 0; a < 4; a++) {
-        xi[a] = make_float3(0.f, 0.f, 0.f);
-        f[a] = make_float3(0.f, 0.f, 0.f);
-        en[a] = 0.f;
-#pragma unroll
-        for (int c = 0; c < 6; c++) v[a][c] = 0.f;
-    }
-    int cnt = 0;
-    const uint32_t *row = nullptr;
-    if (valid) {
-#pragma unroll
-        for (int a = 0; a < 4; a++) xi[a] = f3(A.xs[4 * k + a]);
-        cnt = (int)A.counts[k];
-        cnt = cnt < A.cap ? cnt : A.cap;
-        row = A.list + (size_t)k * A.cap;
-    }
+    float4(*const sb)[32] = s_b[wib];
     const uint32_t lt = (1u << lane) - 1u;
-    int nq = 0;  // queued entries (warp-uniform)
-    for (int base = 0; base < cnt; base += 32) {
-        const int e = base + lane;
-        bool pass = false;
-        int j = 0;
-        float3 sh = make_float3(0.f, 0.f, 0.f);
-        if (e < cnt) {
-            j = (int)__ldg(row + e);
-            const float3 d = xi[0] - f3(__ldg(A.xs + 4 * j));
-            sh = make_float3(A.box.L.x * rintf(d.x * A.box.invL.x), A.box.L.y * rintf(d.y * A.box.invL.y),
-                             A.box.L.z * rintf(d.z * A.box.invL.z));
-            const float3 dm = d - sh;
-            pass = dot3(dm, dm) < A.far2;
-        }
-        const uint32_t bal = __ballot_sync(0xffffffffu, pass);
-        if (pass) {
-            const int pos = nq + __popc(bal & lt);
-            qj[pos] = j;
-            qs[pos] = make_float4(sh.x, sh.y, sh.z, 0.f);
-        }
-        nq += __popc(bal);
-        __syncwarp();
-        if (nq >= 32) {
-            const float4 s4 = qs[lane];
-            mol_pair_eval<LJ, EW, VIR, ENERGY, TOPO>(A, xi, qj[lane], make_float3(s4.x, s4.y, s4.z), f, en, v);
-            __syncwarp();
-            nq -= 32;
-            if (lane < nq) {
-                qj[lane] = qj[32 + lane];
-                qs[lane] = qs[32 + lane];
-            }
-            __syncwarp();
-        }
-    }
-    if (lane < nq) {
-        const float4 s4 = qs[lane];
-        mol_pair_eval<LJ, EW, VIR, ENERGY, TOPO>(A, xi, qj[lane], make_float3(s4.x, s4.y, s4.z), f, en, v);
-    }
-    // the molecule's own site pairs, once per molecule
-    if (valid && lane == 0 && A.selfm) {
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < A.nmol; k += nwarps) {  // warp-uniform
+        float3 xi[4], f[4];
+        float en[4], v[4][6];
 #pragma unroll
         for (int a = 0; a < 4; a++) {
+            f[a] = make_float3(0.f, 0.f, 0.f);
+            en[a] = 0.f;
 #pragma unroll
-            for (int b = 0; b < 4; b++) {
-                const int ab = 4 * a + b;
-                if (a == b || !((A.selfm >> ab) & 1u)) continue;
-                const float3 dr = xi[a] - xi[b];  // the molecule is whole
-                const float r2 = dot3(dr, dr);
-                float e;
-                const float sc = mol_pair_term<LJ, EW, ENERGY, true, 0>(A, ab, r2, A.mult[ab], e);
-                const float3 F = dr * sc;
-                f[a] += F;
-                if (ENERGY) en[a] += e;
-                add_vir<VIR>(v[a], F, dr);
+            for (int c = 0; c < 6; c++) v[a][c] = 0.f;
+        }
+#pragma unroll
+        for (int a = 0; a < 4; a++) xi[a] = f3(A.xs[4 * k + a]);
+        int cnt = (int)A.counts[k];
+        cnt = cnt < A.cap ? cnt : A.cap;
+        const uint32_t *row = A.list + (size_t)k * A.cap;
+        int nq = 0;           // queued entries (warp-uniform)
+        bool staged = false;  // a batch of 32 queued entries is being copied into sb (warp-uniform)
+        float3 bshift = make_float3(0.f, 0.f, 0.f);
+        int j_cur = lane < cnt ? (int)__ldg(row + lane) : 0;
+        int j_nxt = 32 + lane < cnt ? (int)__ldg(row + 32 + lane) : 0;
+        float4 x_cur = lane < cnt ? __ldg(A.xs + 4 * j_cur) : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int base = 0; base < cnt; base += 32) {
+            float4 x_nxt = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (base + 32 + lane < cnt) x_nxt = __ldg(A.xs + 4 * j_nxt);
+            const int j_nn = base + 64 + lane < cnt ? (int)__ldg(row + base + 64 + lane) : 0;
+            const int e = base + lane;
+            bool pass = false;
+            const int j = j_cur;
+            float3 sh = make_float3(0.f, 0.f, 0.f);
+            if (e < cnt) {
+                const float3 d = xi[0] - f3(x_cur);
+                sh = make_float3(A.box.L.x * rintf(d.x * A.box.invL.x), A.box.L.y * rintf(d.y * A.box.invL.y),
+                                 A.box.L.z * rintf(d.z * A.box.invL.z));
+                const float3 dm = d - sh;
+                pass = dot3(dm, dm) < A.far2;
+            }
+            j_cur = j_nxt;
+            j_nxt = j_nn;
+            x_cur = x_nxt;
+            const uint32_t bal = __ballot_sync(0xffffffffu, pass);
+            if (pass) {
+                const int pos = nq + __popc(bal & lt);
+                qj[pos] = j;
+                qs[pos] = make_float4(sh.x, sh.y, sh.z, 0.f);
+            }
+            nq += __popc(bal);
+            __syncwarp();
+            // the batch staged one chunk ago: its copies had the scan above to land
+            if (staged) {
+                cp_async_wait_all();
+                __syncwarp();
+                float3 xj[4];
+#pragma unroll
+                for (int b = 0; b < 4; b++) xj[b] = f3(sb[b][lane]);
+                mol_pair_eval_x<LJ, EW, VIR, ENERGY, TOPO>(A, xi, xj, bshift, f, en, v);
+                staged = false;
+                __syncwarp();
+            }
+            if (nq >= 32) {
+                const float4 s4 = qs[lane];
+                bshift = make_float3(s4.x, s4.y, s4.z);
+                const float4 *src = A.xs + 4 * qj[lane];
+#pragma unroll
+                for (int b = 0; b < 4; b++) cp_async16(&sb[b][lane], src + b);
+                cp_async_commit();
+                staged = true;
+                __syncwarp();
+                nq -= 32;
+                if (lane < nq) {
+                    qj[lane] = qj[32 + lane];
+                    qs[lane] = qs[32 + lane];
+                }
+                __syncwarp();
+            }
+        }
+        if (staged) {
+            cp_async_wait_all();
+            __syncwarp();
+            float3 xj[4];
+#pragma unroll
+            for (int b = 0; b < 4; b++) xj[b] = f3(sb[b][lane]);
+            mol_pair_eval_x<LJ, EW, VIR, ENERGY, TOPO>(A, xi, xj, bshift, f, en, v);
+        }
+        if (lane < nq) {
+            const float4 s4 = qs[lane];
+            mol_pair_eval<LJ, EW, VIR, ENERGY, TOPO>(A, xi, qj[lane], make_float3(s4.x, s4.y, s4.z), f, en, v);
+        }
+        __syncwarp();  // the queue and the batch are reused by the warp's next slot
+        // the molecule's own site pairs, once per molecule
+        if (lane == 0 && A.selfm) {
+#pragma unroll
+            for (int a = 0; a < 4; a++) {
+#pragma unroll
+                for (int b = 0; b < 4; b++) {
+                    const int ab = 4 * a + b;
+                    if (a == b || !((A.selfm >> ab) & 1u)) continue;
+                    const float3 dr = xi[a] - xi[b];  // the molecule is whole
+                    const float r2 = dot3(dr, dr);
+                    float e;
+                    const float sc = mol_pair_term<LJ, EW, ENERGY, true, 0>(A, ab, r2, A.mult[ab], e);
+                    const float3 F = dr * sc;
+                    f[a] += F;
+                    if (ENERGY) en[a] += e;
+                    add_vir<VIR>(v[a], F, dr);
+                }
+            }
+        }
+        if (ENERGY) {
+#pragma unroll
+            for (int a = 0; a < 4; a++) en[a] = warp_sum(en[a]);
+            if (lane < 4) A.energy[4 * k + lane] = lane == 0 ? en[0] : (lane == 1 ? en[1] : (lane == 2 ? en[2] : en[3]));
+            continue;
+        }
+#pragma unroll
+        for (int a = 0; a < 4; a++) f[a] = make_float3(warp_sum(f[a].x), warp_sum(f[a].y), warp_sum(f[a].z));
+        if (VIR) {
+#pragma unroll
+            for (int a = 0; a < 4; a++)
+#pragma unroll
+                for (int c = 0; c < 6; c++) v[a][c] = warp_sum(v[a][c]);
+        }
+        if (lane < 4) {
+            const float3 fm = lane == 0 ? f[0] : (lane == 1 ? f[1] : (lane == 2 ? f[2] : f[3]));
+            float4 fo = A.fs[4 * k + lane];
+            if (accumulate) {
+                fo.x += fm.x;
+                fo.y += fm.y;
+                fo.z += fm.z;
+            } else {
+                fo.x = fm.x;
+                fo.y = fm.y;
+                fo.z = fm.z;
+            }
+            A.fs[4 * k + lane] = fo;
+            if (VIR) {
+                float *vv = A.virials + 6 * (size_t)(4 * k + lane);
+#pragma unroll
+                for (int c = 0; c < 6; c++) {
+                    const float vm = lane == 0 ? v[0][c] : (lane == 1 ? v[1][c] : (lane == 2 ? v[2][c] : v[3][c]));
+                    vv[c] += 0.5f * vm;
+                }
             }
         }
     }
     pdl_trigger();
-    if (ENERGY) {
-#pragma unroll
-        for (int a = 0; a < 4; a++) en[a] = warp_sum(en[a]);
-        if (valid && lane < 4) A.energy[4 * k + lane] = lane == 0 ? en[0] : (lane == 1 ? en[1] : (lane == 2 ? en[2] : en[3]));
-        return;
-    }
-#pragma unroll
-    for (int a = 0; a < 4; a++) f[a] = make_float3(warp_sum(f[a].x), warp_sum(f[a].y), warp_sum(f[a].z));
-    if (VIR) {
-#pragma unroll
-        for (int a = 0; a < 4; a++)
-#pragma unroll
-            for (int c = 0; c < 6; c++) v[a][c] = warp_sum(v[a][c]);
-    }
-    if (valid && lane < 4) {
-        const float3 fm = lane == 0 ? f[0] : (lane == 1 ? f[1] : (lane == 2 ? f[2] : f[3]));
-        float4 fo = A.fs[4 * k + lane];
-        if (accumulate) {
-            fo.x += fm.x;
-            fo.y += fm.y;
-            fo.z += fm.z;
-        } else {
-            fo.x = fm.x;
-            fo.y = fm.y;
-            fo.z = fm.z;
-        }
-        A.fs[4 * k + lane] = fo;
-        if (VIR) {
-            float *vv = A.virials + 6 * (size_t)(4 * k + lane);
-#pragma unroll
-            for (int c = 0; c < 6; c++) {
-                const float vm = lane == 0 ? v[0][c] : (lane == 1 ? v[1][c] : (lane == 2 ? v[2][c] : v[3][c]));
-                vv[c] += 0.5f * vm;
-            }
-        }
-    }
 }
 
 MolPairArgs make_mol_args(State &s, FixPair &f) {
@@ -418,8 +473,11 @@ MolPairArgs make_mol_args(State &s, FixPair &f) {
 }
 
 template <int LJ, bool EW, int TOPO>
-void mol_launch_t(const MolPairArgs &A, int virialMode, bool energy, bool accumulate, cudaStream_t st) {
-    const dim3 blocks((A.nmol * 32 + kMolPairBlock - 1) / kMolPairBlock);
+void mol_launch_t(const MolPairArgs &A, int virialMode, bool energy, bool accumulate, int max_blocks,
+                  cudaStream_t st) {
+    int nb = (A.nmol * 32 + kMolPairBlock - 1) / kMolPairBlock;
+    if (max_blocks > 0 && nb > max_blocks) nb = max_blocks;
+    const dim3 blocks(nb > 0 ? nb : 1);
     if (energy) {
         k_pair_mol<LJ, EW, false, true, TOPO><<<blocks, kMolPairBlock, 0, st>>>(A, 0);
         MDX_LAUNCHED();
@@ -455,12 +513,24 @@ int pair_mol_launch(State &s, FixPair &f, int virialMode, bool accumulate, float
     // the four-site water pattern (LJ on sites 0, charges on 1..3) as
     // compile-time masks; any other pattern from the runtime masks
     const bool water4 = ew && A.ljm == 0x1u && A.qm == 0xEEE0u;
-    if (f.lj_kind == 1 && water4) mol_launch_t<1, true, 1>(A, virialMode, en, accumulate, st);
-    else if (f.lj_kind == 1 && ew) mol_launch_t<1, true, 0>(A, virialMode, en, accumulate, st);
-    else if (f.lj_kind == 1) mol_launch_t<1, false, 0>(A, virialMode, en, accumulate, st);
-    else if (water4) mol_launch_t<2, true, 1>(A, virialMode, en, accumulate, st);
-    else if (ew) mol_launch_t<2, true, 0>(A, virialMode, en, accumulate, st);
-    else mol_launch_t<2, false, 0>(A, virialMode, en, accumulate, st);
+    // blocks per SM of the grid.  Automatic: a pair block holds its SM for
+    // most of the kernel (one molecule per warp, one wave), so with every SM
+    // full the P3M chain beside it (all-rigid water) waits for the pair
+    // kernel at each of its launches; a grid capped below the SMs' capacity
+    // keeps room for it (measured on B200, 4,096 molecules: 10 blocks per SM
+    // without E3B, 7 with the E3B kernel as a third branch).  Else uncapped.
+    int bps = s.pairBlocksPerSM;
+    if (bps == 0) {
+        const bool p3m_beside = ew && s.rigidFix() && !has_free_atoms(s);
+        bps = p3m_beside ? (s.e3bFix() ? 7 : 10) : -1;
+    }
+    const int mb = bps > 0 ? bps * num_sms() : 0;
+    if (f.lj_kind == 1 && water4) mol_launch_t<1, true, 1>(A, virialMode, en, accumulate, mb, st);
+    else if (f.lj_kind == 1 && ew) mol_launch_t<1, true, 0>(A, virialMode, en, accumulate, mb, st);
+    else if (f.lj_kind == 1) mol_launch_t<1, false, 0>(A, virialMode, en, accumulate, mb, st);
+    else if (water4) mol_launch_t<2, true, 1>(A, virialMode, en, accumulate, mb, st);
+    else if (ew) mol_launch_t<2, true, 0>(A, virialMode, en, accumulate, mb, st);
+    else mol_launch_t<2, false, 0>(A, virialMode, en, accumulate, mb, st);
     return 0;
 }
 

@@ -35,6 +35,18 @@ void set_error(int code, const char *fmt, ...) {
 const char *last_error() { return g_err; }
 
 // ---------------------------------------------------------------- State
+int num_sms() {
+    static int cache[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    if (!cache[dev]) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) return 148;
+        cache[dev] = n;
+    }
+    return cache[dev];
+}
+
 State::State() {
     units.setLJ();
 }

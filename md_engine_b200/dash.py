@@ -144,7 +144,7 @@ class State:
 
     _DOUBLE_KEYS = ("rCut", "padding", "dt")
     _INT_KEYS = ("periodicInterval", "nThreadPerAtom", "nThreadPerBlock", "gridStencil", "gridHomeGroup", "turn",
-                 "pairForm")
+                 "pairForm", "pairBlocksPerSM")
 
     def __init__(self):
         h = c_void_p()
@@ -346,7 +346,8 @@ class State:
     def synchronize(self):
         check(lib().mdx_state_synchronize(self._h))
 
-    STAGES = {"pair": 0, "p3m": 1, "e3b": 2, "nlist": 3, "first_half": 4, "second_half": 5}
+    STAGES = {"pair": 0, "p3m": 1, "e3b": 2, "nlist": 3, "first_half": 4, "second_half": 5, "p3m_spread": 6,
+              "p3m_solve": 7, "p3m_gather": 8, "p3m_step": 9}
 
     def timeStage(self, stage, iters=20, flushBytes=0):
         """average device ms of one launch of a hot-path stage"""
