@@ -169,6 +169,10 @@ struct E3BArgs {
     float4 *totals;
     double *e_out;    // energy passes
     int twobody;      // 0: the totals pass leaves out the O-O two-body force
+    // the forces pass's own list, written by the totals pass each step: the
+    // partners mj > m within rmax (each unordered pair once), in mlist's
+    // team layout with mcap entries per molecule (null: walk the full list)
+    uint32_t *ccounts, *clist;
     // 1: the molecule form -- molecule index = slot, sites at 4m .. 4m+3
     // (mol_idx holds that identity map; the hot passes skip reading it)
     int slots;
@@ -330,34 +334,53 @@ __global__ void k_e3b_totals(const E3BArgs a0, const E3BArgs *__restrict__ tab) 
     const bool valid = m < nmol;
     float fx = 0.f, fy = 0.f, fz = 0.f, tx = 0.f, ty = 0.f, tz = 0.f, e2 = 0.f;
     int4 ix = make_int4(0, 0, 0, 0);
+    uint32_t *const clist = A.clist;
+    // the team's lanes (the teams of a warp walk rows of different lengths)
+    const unsigned team_mask = (T == 32 ? 0xffffffffu : ((1u << T) - 1u)) << (a * T);
+    int nc = 0;  // the forces pass's partners found (team-uniform)
     if (valid) {
         ix = e3b_sites(A, mol_idx, m);
         const MolPos mi = load_mol(xs, ix);
         int cnt = (int)mcounts[m];
         cnt = cnt < mcap ? cnt : mcap;
         const uint32_t *row = mlist + (size_t)(m / G) * mcap * G + a * T + t;
+        uint32_t *crow = clist ? clist + (size_t)(m / G) * mcap * G + a * T : nullptr;
         // two entries per lane per trip: both list -> molecule -> O chains are
-        // in flight before either pair is evaluated
-        for (int k0 = t; k0 < cnt; k0 += 2 * T) {
+        // in flight before either pair is evaluated.  Every lane of the team
+        // makes the same trips (the partner ballot below takes the team)
+        for (int k00 = 0; k00 < cnt; k00 += 2 * T) {
+            const int k0 = k00 + t;
             int4 jxs[2];
             float3 ojs[2];
             bool has[2];
+            int mjs[2];
 #pragma unroll
             for (int u = 0; u < 2; u++) {
                 const int k = k0 + u * T;
                 has[u] = k < cnt;
-                const int mj = has[u] ? (int)row[(size_t)(k / T) * 32] : m;
-                jxs[u] = e3b_sites(A, mol_idx, mj);
+                mjs[u] = has[u] ? (int)row[(size_t)(k / T) * 32] : m;
+                jxs[u] = e3b_sites(A, mol_idx, mjs[u]);
             }
 #pragma unroll
             for (int u = 0; u < 2; u++) ojs[u] = f3(__ldg(xs + jxs[u].x));
 #pragma unroll
             for (int u = 0; u < 2; u++) {
-            if (!has[u]) continue;
             const int4 jx = jxs[u];
             const float3 oj = ojs[u];
             const float3 dr = min_image(box, mi.a - oj);
             const float r2 = dot3(dr, dr);
+            if (!ENERGY && clist) {
+                // the forces pass's partners: the same tests it makes
+                const int mj = mjs[u];
+                const bool keep = has[u] && r2 < p.list_cut2 && !(r2 > p.rmax * p.rmax) && m < mj;
+                const unsigned tm = __ballot_sync(team_mask, keep) >> (a * T);
+                if (keep) {
+                    const int pos = nc + __popc(tm & ((1u << t) - 1u));
+                    crow[(size_t)(pos / T) * 32 + pos % T] = (uint32_t)mj;
+                }
+                nc += __popc(tm);
+            }
+            if (!has[u]) continue;
             if (r2 >= p.list_cut2) continue;
             const float rinv = rsqrt_ftz(r2);
             const float r = r2 * rinv;
@@ -399,6 +422,7 @@ __global__ void k_e3b_totals(const E3BArgs a0, const E3BArgs *__restrict__ tab) 
     tz = tsum<T>(tz);
     if (!A.twobody) fx = fy = fz = 0.f;
     if (valid && t == 0) {
+        if (clist) A.ccounts[m] = (uint32_t)nc;
         totals[m] = make_float4(tx, ty, tz, 0.f);
         if (STORE) {
             // the forces pass adds into these with atomics
@@ -443,9 +467,12 @@ __global__ void k_e3b_forces(const E3BArgs a0, const E3BArgs *__restrict__ tab) 
         ix = e3b_sites(A, mol_idx, m);
         const MolPos mi = load_mol(xs, ix);
         const float4 Ti = totals[m];
-        int cnt = (int)mcounts[m];
+        // forces: the partners the totals pass kept (mj > m within rmax);
+        // the energy walks the full list (both orders, half each)
+        const bool compact = !ENERGY && A.clist;
+        int cnt = compact ? (int)A.ccounts[m] : (int)mcounts[m];
         cnt = cnt < mcap ? cnt : mcap;
-        const uint32_t *row = mlist + (size_t)(m / G) * mcap * G + a * T + t;
+        const uint32_t *row = (compact ? A.clist : mlist) + (size_t)(m / G) * mcap * G + a * T + t;
         // two entries per lane per trip, as the totals pass
         for (int k0 = t; k0 < cnt; k0 += 2 * T) {
             int mjs[2];
@@ -658,6 +685,9 @@ int FixE3B::prepareForRun() {
     mcap = ((int)(2.0 * est + 32) + mteam - 1) / mteam * mteam;
     const size_t groups = (size_t)(nmol + 32 / mteam - 1) / (32 / mteam);
     if (int e = mlist.alloc(groups * mcap * (32 / mteam))) return e;
+    // the forces pass's list: a subset of each full row, so the same capacity
+    if (int e = ccounts.alloc(nmol)) return e;
+    if (int e = clist.alloc(groups * mcap * (32 / mteam))) return e;
     prepared = true;
     return 0;
 }
@@ -688,6 +718,8 @@ static E3BArgs e3b_args(State &s, FixE3B &f, float4 *out) {
     A.totals = f.totals.p;
     A.e_out = nullptr;
     A.twobody = 1;
+    A.ccounts = f.ccounts.p;
+    A.clist = f.clist.p;
     A.slots = s.mf.on ? 1 : 0;
     return A;
 }

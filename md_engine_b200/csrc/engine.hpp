@@ -390,6 +390,7 @@ class FixE3B : public Fix {
     DBuf<int4> d_mol_ids, d_mol_idx;
     DBuf<int> d_mol_of_atom;  // by atom index, -1 if none (rebuilt with the list)
     DBuf<uint32_t> mcounts, mlist;  // molecule neighbour list (full, team layout)
+    DBuf<uint32_t> ccounts, clist;  // per step: the forces pass's partners (mj > m within rmax)
     DBuf<float4> totals;
     DBuf<float4> f_side;  // per-step E3B forces when run beside the pair kernel
     bool side_ok = false; // molecules identical to FixRigid's, in the same order

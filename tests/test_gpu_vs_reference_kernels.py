@@ -99,6 +99,7 @@ def test_kernel_times_vs_reference_water4096(oracle):
     parity is checked by the tests above)."""
     sysd = systems.water_tip4p2005(nside=16)
     st, fx = systems.build_water_state(sysd, rcut=9.0, skin=1.0, grid=64, e3b=True, thermostat=False)
+    st.pairBlocksPerSM = -1  # the pair kernel alone: the whole GPU (no room kept for the P3M chain)
     st.prepare()
     st.computeForces()
     x, _, _ = st.getAtoms()
