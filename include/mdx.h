@@ -333,6 +333,30 @@ int mdx_batch_run_timed(mdx_batch *b, int num_turns, int chunk, size_t flush_byt
 int mdx_batch_autotune(mdx_batch *b, int steps, const int *teams, int nteams, int *best_team, double *best_ms);
 int mdx_batch_destroy(mdx_batch *b);
 
+/* ---- pressure control (src/Fixes/FixPressureBerendsen.cu) ----------------- */
+/* FixPressureBerendsen(state, handle, pressure, period, applyEvery)
+ * (FixPressureBerendsen.cu:8-12, Python signature :62-67): every applyEvery
+ * turns, after the step, the scalar pressure P sets the dilation
+ * (1 - dt/period (pressure - P)/bulkModulus)^(1/3), clamped to
+ * 1 +- maxDilation (stepFinal, :26-51); the box scales about its centre,
+ * free atoms with it and rigid molecules by their centres of mass
+ * (Mod::scaleSystem, Mod.cu:301-330).  The P3M splitting and Green function
+ * follow the box (FixChargeEwald::handleBoundsChange, FixChargeEwald.cu:
+ * 1200-1229) and the neighbour list is rebuilt.  A state with an active
+ * barostat runs through mdx_integrator_run only (its steps are launched one
+ * by one rather than replayed from captured graphs). */
+int mdx_fix_pressure_berendsen_create(mdx_state *st, const char *handle, double pressure, double period,
+                                      int apply_every, mdx_fix **out);
+/* keys "maxDilation" (setParameters, :57-59), "bulkModulus" (default 10),
+ * "pressure", "period" */
+int mdx_fix_pressure_berendsen_set(mdx_fix *fix, const char *key, double value);
+/* the keys above and, read-only, "lastPressure", "lastDilation",
+ * "applications" (the pressure and dilation of the last application) */
+int mdx_fix_pressure_berendsen_get(mdx_fix *fix, const char *key, double *value);
+/* Mod::scaleSystem(state, (s, s, s)) with everything that follows a box
+ * change, on a prepared state */
+int mdx_state_scale_system(mdx_state *st, double scale);
+
 /* ---- configuration IO (src/WriteConfig.cpp, src/ReadConfig.cpp) ---------- */
 typedef struct mdx_writer mdx_writer;
 /* WriteConfig(state, fn, handle, format, writeEvery, groupHandle,

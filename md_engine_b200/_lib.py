@@ -115,6 +115,10 @@ SIGNATURES = [
     ("mdx_batch_run_timed", c_int, [c_void_p, c_int, c_int, ctypes.c_size_t, P(c_dbl)]),
     ("mdx_batch_autotune", c_int, [c_void_p, c_int, P(c_int), c_int, P(c_int), P(c_dbl)]),
     ("mdx_batch_destroy", c_int, [c_void_p]),
+    ("mdx_fix_pressure_berendsen_create", c_int, [c_void_p, c_char_p, c_dbl, c_dbl, c_int, P(c_void_p)]),
+    ("mdx_fix_pressure_berendsen_set", c_int, [c_void_p, c_char_p, c_dbl]),
+    ("mdx_fix_pressure_berendsen_get", c_int, [c_void_p, c_char_p, P(c_dbl)]),
+    ("mdx_state_scale_system", c_int, [c_void_p, c_dbl]),
     ("mdx_write_config_create", c_int, [c_void_p, c_char_p, c_char_p, c_char_p, c_int, c_char_p, c_int,
                                         P(c_void_p)]),
     ("mdx_write_config_set", c_int, [c_void_p, c_char_p, c_i64]),

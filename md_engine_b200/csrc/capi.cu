@@ -637,18 +637,7 @@ int mdx_pressure(mdx_state *st, double *pressure, double virial6[6]) {
     ARG_CHECK(st && pressure, "null argument");
     State &s = *st->s;
     if (int e = need_prepared(s)) return e;
-    GUARD(const int n = s.gpd.n; DBuf<float4> keep; if (int e = keep.alloc(n)) return e;
-          MDX_CUDA_TRY(cudaMemcpyAsync(keep.p, s.gpd.fs.p, (size_t)n * sizeof(float4), cudaMemcpyDeviceToDevice,
-                                       s.stream));
-          if (int e = s.computeForces(1)) return e; double v6[6];
-          if (int e = virial_sum(s, v6)) return e; double mv2 = 0.0; if (int e = kinetic_sum(s, &mv2)) return e;
-          MDX_CUDA_TRY(cudaMemcpyAsync(s.gpd.fs.p, keep.p, (size_t)n * sizeof(float4), cudaMemcpyDeviceToDevice,
-                                       s.stream));
-          MDX_CUDA_TRY(cudaStreamSynchronize(s.stream)); if (int e = s.checkStatus()) return e;
-          const double V = s.box.Ld.x * s.box.Ld.y * s.box.Ld.z;
-          *pressure = (mv2 * s.units.mvv_to_eng + v6[0] + v6[1] + v6[2]) / (3.0 * V) * s.units.nktv_to_press;
-          if (virial6) for (int c = 0; c < 6; c++) virial6[c] = v6[c];
-          return 0;)
+    GUARD(return pressure_now(s, pressure, virial6);)
 }
 
 int mdx_get_virials(mdx_state *st, double *per_atom, double sum6[6]) {

@@ -236,7 +236,7 @@ struct MolForm {
 };
 
 // ---------------------------------------------------------------- Fixes
-enum class FixKind { Pair, ChargeEwald, ChargeDSF, E3B, Rigid, NoseHoover };
+enum class FixKind { Pair, ChargeEwald, ChargeDSF, E3B, Rigid, NoseHoover, Barostat };
 
 class Fix {
    public:
@@ -321,6 +321,8 @@ class FixChargeEwald : public Fix {
     int compute(int virialMode) override;
     std::vector<double> getRCuts() override { return {r_cut}; }
     double findAlpha();
+    int computeGreen(cudaStream_t st);  // the influence function for the current box
+    int boxChanged();                   // alpha and the Green function after a box change
     int spread(cudaStream_t st);   // zero + spread
     int solve(cudaStream_t st);    // FFT, E-field, inverse FFTs
     int gather(bool accumulate, cudaStream_t st);
@@ -426,6 +428,37 @@ class FixRigid : public Fix {
     int setConsts();
 };
 
+// FixPressureBerendsen (src/Fixes/FixPressureBerendsen.cu): every
+// applyEvery turns, after the step, the scalar pressure P (DataComputerPressure)
+// sets the box dilation (1 - dt / period (P0 - P) / bulkModulus)^(1/3),
+// clamped to 1 +- maxDilation; atoms and molecules are scaled about the box
+// centre (Mod::scaleSystem)
+class FixPressureBerendsen : public Fix {
+   public:
+    double pressure, period;
+    int applyEvery;
+    double bulkModulus = 10.0;  // FixPressureBerendsen.cu:12 (as LAMMPS)
+    double maxDilation = 1e-5;
+    double lastPressure = 0.0, lastDilation = 1.0;
+    int64_t applications = 0;
+    FixPressureBerendsen(State *s, std::string h, double p, double per, int every)
+        : Fix(s, h, "all", "Berendsen", FixKind::Barostat), pressure(p), period(per), applyEvery(every) {}
+};
+// scalar pressure (DataComputerPressure, FP64) from a virial-mode force
+// evaluation at the current positions (the forces are kept); virial6 may be null
+int pressure_now(State &s, double *pressure, double virial6[6]);
+// Mod::scaleSystem on the device positions about the box centre
+int scale_positions(State &s, double sc);
+// the box scaled by sc about its centre, with everything that follows it:
+// positions, the P3M splitting and Green function, the cell grids, a forced
+// list rebuild
+int box_rescale(State &s, double sc);
+int nlist_box_changed(State &s);
+// FixPressureBerendsen::stepFinal
+int barostat_apply(State &s, FixPressureBerendsen &b);
+// the smallest turn >= t at which the state's barostat fires, or -1
+int64_t barostat_next(State &s, int64_t t);
+
 constexpr int kNHChain = 10;  // chain links (FixNoseHoover's default chainLength)
 struct NHChain {  // FixNoseHoover chain state (FixNoseHoover.h), FP64
     double vel[10], force[10], mass[10];
@@ -507,6 +540,9 @@ class State {
     std::vector<std::vector<int>> molecules;
     std::vector<ConfigWriter *> writers;
     ConfigReader *reader = nullptr;
+    // bumped at every box change (a barostat): captured step graphs hold the
+    // box by value and are rebuilt when it moves
+    uint64_t box_gen = 0;
     State();
     ~State();
     int typeFromHandle(const std::string &h) const;
@@ -523,6 +559,7 @@ class State {
     FixE3B *e3bFix();
     FixRigid *rigidFix();
     FixNoseHoover *nhFix();
+    FixPressureBerendsen *barostatFix();
     double maxRCut();
 };
 

@@ -315,7 +315,7 @@ __global__ void k_add_field_virial(float *__restrict__ vir, const double *__rest
     if (c < 6) vir[c] += (float)(scale * sum6[c]);
 }
 
-double sinc(double x) {
+__host__ __device__ double sinc(double x) {
     if (x < 0.1 && x > -0.1) {
         double x2 = x * x;
         return 1.0 - x2 * 0.16666666667 + x2 * x2 * 0.008333333333333333 - x2 * x2 * x2 * 0.00019841269841269841;
@@ -783,41 +783,8 @@ int FixChargeEwald::prepareForRun() {
     }
     cufftSetStream(plan_r2c, s.stream);
     cufftSetStream(plan_c2r, s.stream);
-    // Green function on the half spectrum (Green_function_cu, FP64 here)
-    std::vector<float> G(nk);
-    const double L[3] = {s.box.Ld.x, s.box.Ld.y, s.box.Ld.z};
-    const double h[3] = {L[0] / sz.x, L[1] / sz.y, L[2] / sz.z};
-    const int lim = (int)(alpha * std::pow(h[0] * h[1] * h[2], 1.0 / 3.0) / 3.14159 * std::sqrt(-std::log(10E-7))) + 1;
-    const double f4a = 0.25 / alpha / alpha;
-    const double tp = 6.28318530717958647693;
-    const int nzh = sz.z / 2 + 1;
-    for (int ix = 0; ix < sz.x; ix++) {
-        double kx = tp * (ix > sz.x / 2 ? ix - sz.x : ix) / L[0];
-        for (int iy = 0; iy < sz.y; iy++) {
-            double ky = tp * (iy > sz.y / 2 ? iy - sz.y : iy) / L[1];
-            for (int iz = 0; iz < nzh; iz++) {
-                double kz = tp * iz / L[2];
-                double k2 = kx * kx + ky * ky + kz * kz;
-                double val = 0.0;
-                if (k2 != 0.0) {
-                    double s1 = 0.0, s2 = 0.0;
-                    for (int mx = -lim; mx <= lim; mx++)
-                        for (int my = -lim; my <= lim; my++)
-                            for (int mz = -lim; mz <= lim; mz++) {
-                                double px = kx + tp * mx / h[0], py = ky + tp * my / h[1], pz = kz + tp * mz / h[2];
-                                double pp = px * px + py * py + pz * pz;
-                                double W = sinc(px * h[0] * 0.5) * sinc(py * h[1] * 0.5) * sinc(pz * h[2] * 0.5);
-                                double W2 = std::pow(W, order * 2);
-                                s1 += 12.56637061435917295385 * std::exp(-pp * f4a) * (kx * px + ky * py + kz * pz) / pp * W2;
-                                s2 += W2;
-                            }
-                    val = s1 / (s2 * s2) / k2;
-                }
-                G[((size_t)ix * sz.y + iy) * nzh + iz] = (float)val;
-            }
-        }
-    }
-    MDX_CUDA_TRY(cudaMemcpy(green.p, G.data(), nk * sizeof(float), cudaMemcpyHostToDevice));
+    // Green function on the half spectrum (Green_function_cu), on the device
+    if (int e = computeGreen(s.stream)) return e;
     // own FFT for cubic 32^3 / 64^3 meshes (cuFFT for every other size)
     if (int e = f_recip.alloc(std::max(s.gpd.n, 1))) return e;
     own_fft = sz.x == sz.y && sz.y == sz.z && (sz.x == 32 || sz.x == 64);
@@ -873,6 +840,67 @@ int own_fft_setup() {
     return 0;
 }
 }  // namespace
+
+namespace {
+// the optimal influence function of order-5 P3M on the half spectrum
+// (Green_function_cu, FixChargeEwald.cu:218-294), one thread per k, FP64:
+// sum over the aliasing images m within +-lim of the charge assignment
+// function's transform W^(2 order) and the reference force R(k_m)
+__global__ void k_green(int3 sz, double3 L, double alpha, int lim, float *__restrict__ green) {
+    const int nzh = sz.z / 2 + 1;
+    const size_t nk = (size_t)sz.x * sz.y * nzh;
+    const size_t id = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= nk) return;
+    const int iz = (int)(id % nzh);
+    const int iy = (int)((id / nzh) % sz.y);
+    const int ix = (int)(id / ((size_t)nzh * sz.y));
+    const double tp = 6.28318530717958647693;
+    const double h0 = L.x / sz.x, h1 = L.y / sz.y, h2 = L.z / sz.z;
+    const double kx = tp * (ix > sz.x / 2 ? ix - sz.x : ix) / L.x;
+    const double ky = tp * (iy > sz.y / 2 ? iy - sz.y : iy) / L.y;
+    const double kz = tp * iz / L.z;
+    const double k2 = kx * kx + ky * ky + kz * kz;
+    const double f4a = 0.25 / alpha / alpha;
+    double val = 0.0;
+    if (k2 != 0.0) {
+        double s1 = 0.0, s2 = 0.0;
+        for (int mx = -lim; mx <= lim; mx++)
+            for (int my = -lim; my <= lim; my++)
+                for (int mz = -lim; mz <= lim; mz++) {
+                    const double px = kx + tp * mx / h0, py = ky + tp * my / h1, pz = kz + tp * mz / h2;
+                    const double pp = px * px + py * py + pz * pz;
+                    const double W = sinc(px * h0 * 0.5) * sinc(py * h1 * 0.5) * sinc(pz * h2 * 0.5);
+                    const double W2 = W * W, W4 = W2 * W2, W8 = W4 * W4;
+                    const double W10 = W8 * W2;  // W^(2 order), order 5
+                    s1 += 12.56637061435917295385 * exp(-pp * f4a) * (kx * px + ky * py + kz * pz) / pp * W10;
+                    s2 += W10;
+                }
+        val = s1 / (s2 * s2) / k2;
+    }
+    green[id] = (float)val;
+}
+}  // namespace
+
+int FixChargeEwald::computeGreen(cudaStream_t st) {
+    State &s = *state;
+    const double L[3] = {s.box.Ld.x, s.box.Ld.y, s.box.Ld.z};
+    const double h[3] = {L[0] / sz.x, L[1] / sz.y, L[2] / sz.z};
+    const int lim = (int)(alpha * std::pow(h[0] * h[1] * h[2], 1.0 / 3.0) / 3.14159 * std::sqrt(-std::log(10E-7))) + 1;
+    const size_t nk = (size_t)sz.x * sz.y * (sz.z / 2 + 1);
+    k_green<<<(unsigned)((nk + 255) / 256), 256, 0, st>>>(sz, make_double3(L[0], L[1], L[2]), alpha, lim, green.p);
+    MDX_LAUNCHED();
+    MDX_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+// FixChargeEwald::handleBoundsChange (FixChargeEwald.cu:1200-1229): the
+// splitting parameter for the new box (unless set by hand) and the Green
+// function
+int FixChargeEwald::boxChanged() {
+    if (!prepared) return 0;
+    alpha = alpha_user > 0 ? alpha_user : findAlpha();
+    return computeGreen(state->stream);
+}
 
 int FixChargeEwald::spread(cudaStream_t st) {
     State &s = *state;

@@ -1125,6 +1125,76 @@ static int batch_sizing(Batch &b, MolArgs *out) {
     return 0;
 }
 
+namespace {
+// Mod::scaleSystem (Mod.cu:201-240) for the atoms outside rigid molecules:
+// x -> c + (x - c) s about the box centre c
+__global__ void k_scale_free(int n, float4 *__restrict__ xs, const uint32_t *__restrict__ ids,
+                             const uint8_t *__restrict__ rigid_by_id, double3 c, double s) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (rigid_by_id && rigid_by_id[ids[i]]) return;
+    float4 x = xs[i];
+    x.x = (float)(c.x + ((double)x.x - c.x) * s);
+    x.y = (float)(c.y + ((double)x.y - c.y) * s);
+    x.z = (float)(c.z + ((double)x.z - c.z) * s);
+    xs[i] = x;
+}
+
+// FixRigid::scaleRigidBodies (rigid_scaleSystem_cu, FixRigid.cu:164-242):
+// the centre of mass of O, H1, H2 (the hydrogens at the oxygen's image)
+// moves to c + (com - c) s and every site of the molecule moves with it, so
+// the rigid geometry (and the M site) is kept
+__global__ void k_scale_mol(const MolArgs A, double3 c, double s) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= A.nmol) return;
+    const int4 ix = mol_sites(A, m);
+    const Box &b = A.box;
+    const float4 o = A.xs[ix.x], h1 = A.xs[ix.y], h2 = A.xs[ix.z];
+    auto mi = [&](double d, double L, double iL) { return d - L * rint(d * iL); };
+    const double3 d1 = make_double3(mi((double)h1.x - o.x, b.Ld.x, b.invLd.x), mi((double)h1.y - o.y, b.Ld.y, b.invLd.y),
+                                    mi((double)h1.z - o.z, b.Ld.z, b.invLd.z));
+    const double3 d2 = make_double3(mi((double)h2.x - o.x, b.Ld.x, b.invLd.x), mi((double)h2.y - o.y, b.Ld.y, b.invLd.y),
+                                    mi((double)h2.z - o.z, b.Ld.z, b.invLd.z));
+    const double wH = A.rc.wH;
+    const double3 com = make_double3(o.x + (d1.x + d2.x) * wH, o.y + (d1.y + d2.y) * wH, o.z + (d1.z + d2.z) * wH);
+    const double3 sh = make_double3((c.x + (com.x - c.x) * s) - com.x, (c.y + (com.y - c.y) * s) - com.y,
+                                    (c.z + (com.z - c.z) * s) - com.z);
+    const int id4[4] = {ix.x, ix.y, ix.z, ix.w};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        if (id4[k] < 0) continue;
+        float4 x = A.xs[id4[k]];
+        x.x = (float)((double)x.x + sh.x);
+        x.y = (float)((double)x.y + sh.y);
+        x.z = (float)((double)x.z + sh.z);
+        A.xs[id4[k]] = x;
+    }
+}
+}  // namespace
+
+// Mod::scaleSystem (Mod.cu:301-330) on the device positions, about the
+// centre of the current box (which the caller then scales): free atoms
+// scaled, rigid molecules moved with their centres of mass
+int scale_positions(State &s, double sc) {
+    const double3 c = make_double3(s.box.lod.x + 0.5 * s.box.Ld.x, s.box.lod.y + 0.5 * s.box.Ld.y,
+                                   s.box.lod.z + 0.5 * s.box.Ld.z);
+    FixRigid *r = s.rigidFix();
+    const int n = s.gpd.n;
+    if (has_free_atoms(s)) {
+        k_scale_free<<<(n + 255) / 256, 256, 0, s.stream>>>(n, s.gpd.xs.p, s.gpd.ids.p, r ? rigid_flags(s) : nullptr,
+                                                           c, sc);
+        MDX_LAUNCHED();
+    }
+    if (r && !r->mol_ids.empty()) {
+        MolArgs A = mol_args(s, *r);
+        A.slots = s.mf.on ? 1 : 0;
+        k_scale_mol<<<(A.nmol + 255) / 256, 256, 0, s.stream>>>(A, c, sc);
+        MDX_LAUNCHED();
+    }
+    MDX_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
 int batch_rigid_maps(Batch &b) {
     MolArgs A;
     if (int e = batch_sizing(b, &A)) return e;

@@ -145,7 +145,12 @@ class IntegratorVerlet {
         build_pending = false;
         return 0;
     }
+    uint64_t graph_box_gen = 0;
     int getGraph(int nsteps, bool with_group, cudaGraphExec_t *out) {
+        if (graph_box_gen != s->box_gen) {
+            clearGraphs();
+            graph_box_gen = s->box_gen;
+        }
         auto key = std::make_pair(nsteps, with_group ? 1 : 0);
         auto it = graphs.find(key);
         if (it != graphs.end()) {
@@ -215,6 +220,10 @@ class IntegratorVerlet {
     // CUDA events on the library stream, L2 flushed (a write larger than L2)
     // before every chunk outside the timed windows; returns summed device ms
     int runTimed(int nturns, int chunk, size_t flush_bytes, double *ms_total) {
+        if (s->barostatFix()) {
+            set_error(MDX_ERR_UNSUPPORTED, "a barostat changes the box between steps: use mdx_integrator_run");
+            return MDX_ERR_UNSUPPORTED;
+        }
         if (!s->prepared) {
             clearGraphs();
             if (int e = s->prepare()) return e;
@@ -268,6 +277,10 @@ class IntegratorVerlet {
     size_t h_stage_n = 0;
     DBuf<double> d_stage;
     int runHost(int nturns, const double *pin, const double *vin, double *pout, double *vout, double *fout) {
+        if (s->barostatFix()) {
+            set_error(MDX_ERR_UNSUPPORTED, "a barostat changes the box between steps: use mdx_integrator_run");
+            return MDX_ERR_UNSUPPORTED;
+        }
         if (!s->prepared) {
             clearGraphs();
             if (int e = s->prepare()) return e;
@@ -347,17 +360,27 @@ class IntegratorVerlet {
             int chunk = check ? P : (int)(P - (t % P));
             if (chunk > nturns - done) chunk = nturns - done;
             // configuration writers (Integrator::asyncOperations,
-            // Integrator.cu:77-113): a writer due at turn T writes after that
-            // turn's step, so the chunk ends there
+            // Integrator.cu:77-113) and the barostat (its stepFinal): due at
+            // turn T, they act after that turn's step, so the chunk ends there
             const int64_t wt = config_next_write(*s, t);
             if (wt >= 0 && wt - t + 1 < chunk) chunk = (int)(wt - t + 1);
-            if (mode == 0) {
+            FixPressureBerendsen *baro = s->barostatFix();
+            const int64_t bt = barostat_next(*s, t);
+            if (bt >= 0 && bt - t + 1 < chunk) chunk = (int)(bt - t + 1);
+            // with a barostat the box moves every few steps: launched step by
+            // step (captured graphs hold the box by value)
+            if (mode == 0 && !baro) {
                 if (int e = launchGraph(chunk, check)) return e;
             } else {
                 if (int e = enqueue(chunk, check)) return e;
             }
             s->turn += chunk;
             done += chunk;
+            if (bt >= 0 && s->turn == bt + 1) {
+                MDX_CUDA_TRY(cudaStreamSynchronize(s->stream));
+                if (int e = s->checkStatus()) return e;
+                if (int e = barostat_apply(*s, *baro)) return e;
+            }
             if (wt >= 0 && s->turn == wt + 1) {
                 if (int e = s->checkStatus()) return e;
                 if (int e = config_write_due(*s, wt)) return e;

@@ -1501,6 +1501,55 @@ int molform_init(State &s) {
     return 0;
 }
 
+// the box changed size (a barostat): the cell grids keep their stencil
+// widths m and take as many cells per side as the new box holds at that
+// width (cells never narrower than the list radius / m); the caller forces a
+// rebuild.  The minimum-image and stencil conditions of nlist_init and
+// molform_init are checked again.
+int nlist_box_changed(State &s) {
+    GridGPU &gr = s.grid;
+    const double Lmin = std::min(s.box.Ld.x, std::min(s.box.Ld.y, s.box.Ld.z));
+    if (2.0 * (double)gr.cut >= Lmin) {
+        set_error(MDX_ERR_UNSUPPORTED, "the box shrank below twice the neighbour cutoff %g", (double)gr.cut);
+        return MDX_ERR_UNSUPPORTED;
+    }
+    {
+        const double w = (double)gr.cut / gr.m * (1.0 + 1e-5);
+        const int3 ns = make_int3((int)(s.box.Ld.x / w), (int)(s.box.Ld.y / w), (int)(s.box.Ld.z / w));
+        const int need = std::max(3, 2 * gr.m);
+        if (ns.x < need || ns.y < need || ns.z < need) {
+            set_error(MDX_ERR_UNSUPPORTED, "the box shrank below the neighbour grid's %d cells per side", need);
+            return MDX_ERR_UNSUPPORTED;
+        }
+        const int ncell = ns.x * ns.y * ns.z;
+        if (int e = gr.cell_start.alloc(ncell + 1)) return e;
+        if (int e = gr.cell_count.alloc(ncell)) return e;
+        if (int e = gr.cell_fill.alloc(ncell)) return e;
+        MDX_CUDA_TRY(cudaMemsetAsync(gr.cell_count.p, 0, ncell * sizeof(uint32_t), s.stream));
+        gr.ns = ns;
+    }
+    if (s.mf.on) {
+        MolForm &mf = s.mf;
+        if (2.0 * (double)mf.cut >= Lmin) {
+            set_error(MDX_ERR_UNSUPPORTED, "the box shrank below twice the molecule list radius %g", (double)mf.cut);
+            return MDX_ERR_UNSUPPORTED;
+        }
+        const double w = (double)mf.cut / mf.m * (1.0 + 1e-5);
+        const int3 ns = make_int3((int)(s.box.Ld.x / w), (int)(s.box.Ld.y / w), (int)(s.box.Ld.z / w));
+        if (ns.x < 2 * mf.m + 1 || ns.y < 2 * mf.m + 1 || ns.z < 2 * mf.m + 1) {
+            set_error(MDX_ERR_UNSUPPORTED, "the box shrank below the molecule grid's %d cells per side", 2 * mf.m + 1);
+            return MDX_ERR_UNSUPPORTED;
+        }
+        const int ncell = ns.x * ns.y * ns.z;
+        if (int e = mf.cell_start.alloc(ncell + 1)) return e;
+        if (int e = mf.cell_count.alloc(ncell)) return e;
+        if (int e = mf.cell_fill.alloc(ncell)) return e;
+        MDX_CUDA_TRY(cudaMemsetAsync(mf.cell_count.p, 0, ncell * sizeof(uint32_t), s.stream));
+        mf.ns = ns;
+    }
+    return 0;
+}
+
 // batched replicas: the same group, one launch per kernel for all replicas
 // (blockIdx.y = replica); every kernel returns at once for a replica whose
 // skin check did not fire.  Tables are built at prepare, before any capture.

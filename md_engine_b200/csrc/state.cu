@@ -110,6 +110,11 @@ FixRigid *State::rigidFix() {
         if (f->kind == FixKind::Rigid) return static_cast<FixRigid *>(f);
     return nullptr;
 }
+FixPressureBerendsen *State::barostatFix() {
+    for (Fix *f : fixes)
+        if (f->kind == FixKind::Barostat) return static_cast<FixPressureBerendsen *>(f);
+    return nullptr;
+}
 FixNoseHoover *State::nhFix() {
     for (Fix *f : fixes)
         if (f->kind == FixKind::NoseHoover) return static_cast<FixNoseHoover *>(f);

@@ -190,7 +190,13 @@ class State:
             check(lib().mdx_state_get_int(self._h, k.encode(), ctypes.byref(out)))
             return out.value
         if k == "bounds":
-            return object.__getattribute__(self, "_bounds")
+            # the library's box (a barostat or a read configuration moves it)
+            if object.__getattribute__(self, "_bounds") is None:
+                return None
+            lo = (ctypes.c_double * 3)()
+            hi = (ctypes.c_double * 3)()
+            check(lib().mdx_state_get_bounds(self._h, lo, hi))
+            return Bounds(self, lo=Vector(*lo), hi=Vector(*hi))
         raise AttributeError(k)
 
     def _after_read(self):
@@ -222,6 +228,15 @@ class State:
         b = c_u32()
         check(lib().mdx_state_group_tag(self._h, handle.encode(), ctypes.byref(b)))
         return b.value
+
+    def scaleSystem(self, scale):
+        """Mod::scaleSystem: the box and the positions scaled by `scale`
+        about the box centre (rigid molecules by their centres of mass)"""
+        check(lib().mdx_state_scale_system(self._h, float(scale)))
+        lo = (ctypes.c_double * 3)()
+        hi = (ctypes.c_double * 3)()
+        check(lib().mdx_state_get_bounds(self._h, lo, hi))
+        object.__setattr__(self, "_bounds", Bounds(self, lo=Vector(*lo), hi=Vector(*hi)))
 
     def createMolecule(self, ids):
         ids = np.ascontiguousarray(list(ids), np.int32)
@@ -587,6 +602,45 @@ class FixRigid(_Fix):
         if rc not in (0, 6):
             check(rc)
         return n.value
+
+
+class FixPressureBerendsen(_Fix):
+    """FixPressureBerendsen(state, handle, pressure, period, applyEvery)
+    (src/Fixes/FixPressureBerendsen.cu): Berendsen box rescaling every
+    applyEvery turns toward `pressure` (state units) with time constant
+    `period`."""
+
+    _KEYS = ("maxDilation", "bulkModulus", "pressure", "period")
+
+    def __init__(self, state, handle, pressure, period, applyEvery):
+        h = c_void_p()
+        check(lib().mdx_fix_pressure_berendsen_create(state._h, handle.encode(), float(pressure), float(period),
+                                                      int(applyEvery), ctypes.byref(h)))
+        object.__setattr__(self, "_h", h)
+        object.__setattr__(self, "handle", handle)
+        object.__setattr__(self, "applyEvery", int(applyEvery))
+
+    def setParameters(self, maxDilation=-1):
+        if maxDilation > 0:
+            check(lib().mdx_fix_pressure_berendsen_set(self._h, b"maxDilation", float(maxDilation)))
+
+    def _get(self, k):
+        out = c_dbl()
+        check(lib().mdx_fix_pressure_berendsen_get(self._h, k.encode(), ctypes.byref(out)))
+        return out.value
+
+    def __setattr__(self, k, v):
+        if k in FixPressureBerendsen._KEYS:
+            check(lib().mdx_fix_pressure_berendsen_set(self._h, k.encode(), float(v)))
+        else:
+            object.__setattr__(self, k, v)
+
+    def __getattr__(self, k):
+        if k in FixPressureBerendsen._KEYS or k in ("lastPressure", "lastDilation"):
+            return self._get(k)
+        if k == "applications":
+            return int(self._get(k))
+        raise AttributeError(k)
 
 
 class FixNoseHoover(_Fix):
