@@ -593,7 +593,12 @@ class Batch {
         DBuf<float> rho, e_r;
         DBuf<float2> rho_k, e_k;
         cufftHandle r2c = 0, c2r = 0;
+        // cubic 32^3 / 64^3 meshes: this library's FFT kernels over the
+        // class's replicas (a table of their field pointers), no cuFFT
+        bool own = false;
+        DBuf<char> tab;
     };
+    bool p3m_own = false;  // every class on the own FFT: the gather reads the float4 fields
     std::vector<std::unique_ptr<FFTClass>> fft;
     std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
     std::map<std::pair<int, int>, uint64_t> graph_kernels;

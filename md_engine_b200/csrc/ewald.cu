@@ -80,6 +80,7 @@ struct P3MArgs {
     const int4 *mol_idx;
     int nmol, four_site;
     int slots;  // 1: the molecule form's layout, molecule slot m at sites 4m .. 4m+3 (no map read)
+    const float4 *e4;  // the own FFT's interleaved field (batched gather), or null
 };
 #define MDX_P3M_ARGS const P3MArgs A = tab ? tab[blockIdx.y] : a0
 
@@ -359,6 +360,7 @@ P3MArgs p3m_args(State &s, FixChargeEwald &f) {
     A.ngrid = (size_t)f.sz.x * f.sz.y * f.sz.z;
     A.niv = (float)(-1.0 / (s.box.Ld.x * s.box.Ld.y * s.box.Ld.z));
     A.slots = 0;
+    A.e4 = f.own_fft ? f.e4.p : nullptr;
     return A;
 }
 
@@ -447,11 +449,12 @@ __device__ __forceinline__ int fft_out_index(int k1, int lane) { return k1 + R *
 constexpr int kFftPlaneWarps = 16;
 
 template <int R>
-__global__ void __launch_bounds__(kFftPlaneWarps * 32) k_fft_zy(const FFTArgs A) {
+__global__ void __launch_bounds__(kFftPlaneWarps * 32) k_fft_zy(const FFTArgs a0, const FFTArgs *__restrict__ tab) {
     extern __shared__ float2 plane[];  // [n][n/2+1]
     constexpr int N = 32 * R, NH = N / 2 + 1;
     constexpr int nw = kFftPlaneWarps, UNR = R <= 2 ? 4 : 1;
     pdl_wait();
+    const FFTArgs A = tab ? tab[blockIdx.y] : a0;  // batched replicas: blockIdx.y
     const int x = blockIdx.x;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const LaneTw T = lane_twiddles<R>(lane, A.tw);
@@ -484,9 +487,10 @@ __global__ void __launch_bounds__(kFftPlaneWarps * 32) k_fft_zy(const FFTArgs A)
 }
 
 template <int R>
-__global__ void __launch_bounds__(256) k_fft_xe(const FFTArgs A) {
+__global__ void __launch_bounds__(256) k_fft_xe(const FFTArgs a0, const FFTArgs *__restrict__ tab) {
     constexpr int N = 32 * R, NH = N / 2 + 1;
     pdl_wait();
+    const FFTArgs A = tab ? tab[blockIdx.y] : a0;
     __shared__ float2 sline[8][N];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int line_id = blockIdx.x * (blockDim.x >> 5) + w;  // at most 8 warps per block (sline)
@@ -534,11 +538,12 @@ __global__ void __launch_bounds__(256) k_fft_xe(const FFTArgs A) {
 // one block per (x plane, field component): inverse along y for every kz,
 // then the real inverse along z; component d of the float4 field is written
 template <int R>
-__global__ void __launch_bounds__(kFftPlaneWarps * 32) k_ifft_yz(const FFTArgs A) {
+__global__ void __launch_bounds__(kFftPlaneWarps * 32) k_ifft_yz(const FFTArgs a0, const FFTArgs *__restrict__ tab) {
     extern __shared__ float2 plane[];  // [n][n/2+1]
     constexpr int N = 32 * R, NH = N / 2 + 1;
     constexpr int nw = kFftPlaneWarps, UNR = R <= 2 ? 4 : 1;
     pdl_wait();
+    const FFTArgs A = tab ? tab[blockIdx.z] : a0;  // batched replicas: blockIdx.z
     const int x = blockIdx.x, d = blockIdx.y;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const LaneTw T = lane_twiddles<R>(lane, A.tw);
@@ -631,8 +636,7 @@ __device__ __forceinline__ float3 group5_sum(float3 e, int base) {
 }
 
 template <bool ACC>
-__global__ void k_gather4(const P3MArgs A, const float4 *__restrict__ e4) {
-    pdl_wait();
+__device__ __forceinline__ void gather4_body(const P3MArgs &A, const float4 *__restrict__ e4) {
     const int lane = threadIdx.x & 31;
     const int t = lane % 5, base = lane - t;
     const int i = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 6 + lane / 5;
@@ -658,6 +662,20 @@ __global__ void k_gather4(const P3MArgs A, const float4 *__restrict__ e4) {
         f.z = s * sm.z;
     }
     fs[i] = f;
+}
+
+template <bool ACC>
+__global__ void k_gather4(const P3MArgs A, const float4 *__restrict__ e4) {
+    pdl_wait();
+    gather4_body<ACC>(A, e4);
+}
+
+// batched replicas (blockIdx.y = replica), each with its own field
+template <bool ACC>
+__global__ void k_gather4_tab(const P3MArgs a0, const P3MArgs *__restrict__ tab) {
+    MDX_P3M_ARGS;
+    if ((blockIdx.x * blockDim.x >> 5) * 6 >= (unsigned)A.n) return;  // past this replica's atoms
+    gather4_body<ACC>(A, A.e4);
 }
 
 // the molecule form of the gather into a per-step buffer (STORE): the
@@ -824,9 +842,10 @@ int own_solve(State &s, FixChargeEwald &f, cudaStream_t st) {
     const FFTArgs A = fft_args(s, f);
     // 512-thread plane blocks (measured +0.8 % per water step against 1024
     // beside the pair kernel; 256 was slower)
-    MDX_CUDA_TRY(launch_pdl_prio(true, k_fft_zy<R>, dim3(N), dim3(kFftPlaneWarps * 32), (size_t)N * NH * sizeof(float2), st, A));
-    MDX_CUDA_TRY(launch_pdl_prio(true, k_fft_xe<R>, dim3((N * NH + 7) / 8), dim3(256), 0, st, A));
-    MDX_CUDA_TRY(launch_pdl_prio(true, k_ifft_yz<R>, dim3(N, 3), dim3(kFftPlaneWarps * 32), (size_t)N * NH * sizeof(float2), st, A));
+    const FFTArgs *nt = nullptr;
+    MDX_CUDA_TRY(launch_pdl_prio(true, k_fft_zy<R>, dim3(N), dim3(kFftPlaneWarps * 32), (size_t)N * NH * sizeof(float2), st, A, nt));
+    MDX_CUDA_TRY(launch_pdl_prio(true, k_fft_xe<R>, dim3((N * NH + 7) / 8), dim3(256), 0, st, A, nt));
+    MDX_CUDA_TRY(launch_pdl_prio(true, k_ifft_yz<R>, dim3(N, 3), dim3(kFftPlaneWarps * 32), (size_t)N * NH * sizeof(float2), st, A, nt));
     return 0;
 }
 
@@ -1095,15 +1114,27 @@ int batch_p3m_prepare(Batch &b) {
             f->e_k.view(c.e_k.p + j * 3 * nk, 3 * nk);
             f->e_r.view(c.e_r.p + j * 3 * ng, 3 * ng);
         }
-        int dims[3] = {c.sz.x, c.sz.y, c.sz.z};
-        if (cufftPlanMany(&c.r2c, 3, dims, nullptr, 1, (int)ng, nullptr, 1, (int)nk, CUFFT_R2C, K) != CUFFT_SUCCESS ||
-            cufftPlanMany(&c.c2r, 3, dims, nullptr, 1, (int)nk, nullptr, 1, (int)ng, CUFFT_C2R, 3 * K) !=
-                CUFFT_SUCCESS) {
-            set_error(MDX_ERR_CUDA, "batched cufftPlanMany failed");
-            return MDX_ERR_CUDA;
+        c.own = true;
+        for (int j = 0; j < K; j++) c.own = c.own && b.reps[c.reps[j]]->ewaldFix()->own_fft;
+        if (c.own) {
+            std::vector<FFTArgs> ft(K);
+            for (int j = 0; j < K; j++) ft[j] = fft_args(*b.reps[c.reps[j]], *b.reps[c.reps[j]]->ewaldFix());
+            if (int e = c.tab.alloc(K * sizeof(FFTArgs))) return e;
+            MDX_CUDA_TRY(cudaMemcpy(c.tab.p, ft.data(), K * sizeof(FFTArgs), cudaMemcpyHostToDevice));
+        } else {
+            int dims[3] = {c.sz.x, c.sz.y, c.sz.z};
+            if (cufftPlanMany(&c.r2c, 3, dims, nullptr, 1, (int)ng, nullptr, 1, (int)nk, CUFFT_R2C, K) !=
+                    CUFFT_SUCCESS ||
+                cufftPlanMany(&c.c2r, 3, dims, nullptr, 1, (int)nk, nullptr, 1, (int)ng, CUFFT_C2R, 3 * K) !=
+                    CUFFT_SUCCESS) {
+                set_error(MDX_ERR_CUDA, "batched cufftPlanMany failed");
+                return MDX_ERR_CUDA;
+            }
         }
         b.max_nk = std::max(b.max_nk, nk);
     }
+    b.p3m_own = true;
+    for (auto &cp : b.fft) b.p3m_own = b.p3m_own && cp->own;
     std::vector<P3MArgs> h(R);
     for (int r = 0; r < R; r++) h[r] = p3m_args(*b.reps[r], *b.reps[r]->ewaldFix());
     if (int e = b.tab_p3m.alloc(R * sizeof(P3MArgs))) return e;
@@ -1120,6 +1151,29 @@ int batch_p3m_spread_solve(Batch &b, cudaStream_t st) {
     for (auto &c : b.fft) MDX_CUDA_TRY(cudaMemsetAsync(c->rho.p, 0, c->rho.n * sizeof(float), st));
     k_spread5<<<dim3((A.n + 47) / 48, R), 256, 0, st>>>(A, tab);
     MDX_LAUNCHED();
+    if (b.p3m_own) {
+        // each mesh class: R2C + E(k) + 3 C2R as the single system's three
+        // FFT kernels, one launch each over the class's replicas
+        for (auto &c : b.fft) {
+            const unsigned K = (unsigned)c->reps.size();
+            const FFTArgs a0 = fft_args(*b.reps[c->reps[0]], *b.reps[c->reps[0]]->ewaldFix());
+            const FFTArgs *ft = reinterpret_cast<const FFTArgs *>(c->tab.p);
+            const int N = c->sz.x, NH = N / 2 + 1;
+            const size_t smem = (size_t)N * NH * sizeof(float2);
+            if (N == 64) {
+                k_fft_zy<2><<<dim3(N, K), kFftPlaneWarps * 32, smem, st>>>(a0, ft);
+                k_fft_xe<2><<<dim3((N * NH + 7) / 8, K), 256, 0, st>>>(a0, ft);
+                k_ifft_yz<2><<<dim3(N, 3, K), kFftPlaneWarps * 32, smem, st>>>(a0, ft);
+            } else {
+                k_fft_zy<1><<<dim3(N, K), kFftPlaneWarps * 32, smem, st>>>(a0, ft);
+                k_fft_xe<1><<<dim3((N * NH + 7) / 8, K), 256, 0, st>>>(a0, ft);
+                k_ifft_yz<1><<<dim3(N, 3, K), kFftPlaneWarps * 32, smem, st>>>(a0, ft);
+            }
+            g_launches += 3;
+        }
+        MDX_CUDA_TRY(cudaGetLastError());
+        return 0;
+    }
     for (auto &c : b.fft) {
         cufftSetStream(c->r2c, st);
         if (cufftExecR2C(c->r2c, c->rho.p, (cufftComplex *)c->rho_k.p) != CUFFT_SUCCESS) {
@@ -1143,6 +1197,11 @@ int batch_p3m_gather(Batch &b, cudaStream_t st) {
     const P3MArgs *tab = reinterpret_cast<const P3MArgs *>(b.tab_p3m.p);
     P3MArgs A = p3m_args(*b.reps[0], *b.reps[0]->ewaldFix());
     A.n = b.max_n;
+    if (b.p3m_own) {
+        k_gather4_tab<true><<<dim3((A.n + 47) / 48, (unsigned)b.reps.size()), 256, 0, st>>>(A, tab);
+        MDX_LAUNCHED();
+        return 0;
+    }
     k_gather<true><<<dim3((A.n + 127) / 128, (unsigned)b.reps.size()), 128, 0, st>>>(A, tab);
     MDX_LAUNCHED();
     return 0;
