@@ -61,7 +61,8 @@ int mdx_state_set_bounds(mdx_state *st, const double lo[3], const double hi[3]);
  * all-rigid four-site water), 1 per-site list, 2 molecule form.
  * "pairBlocksPerSM": molecule form, cap on the pair kernel's grid in blocks
  * per SM (0 = automatic, -1 = uncapped: one warp per molecule).  Read-only:
- * "nlistCapacity", "cellsPerSide", "molListCapacity". */
+ * "nlistCapacity", "cellsPerSide", "molListCapacity", "molListEntries" (the
+ * molecule-pair list's entries, summed over its rows). */
 int mdx_state_set_double(mdx_state *st, const char *key, double value);
 int mdx_state_get_double(mdx_state *st, const char *key, double *value);
 int mdx_state_set_int(mdx_state *st, const char *key, int64_t value);

@@ -150,6 +150,18 @@ int mdx_state_get_int(mdx_state *st, const char *key, int64_t *v) {
     else if (k == "pairForm") *v = s.prepared ? (s.mf.on ? 2 : 1) : s.pairForm;
     else if (k == "molListCapacity") *v = s.mf.cap;
     else if (k == "pairBlocksPerSM") *v = s.pairBlocksPerSM;
+    else if (k == "molListEntries") {
+        // molecule form: entries of the molecule-pair list (sum of the row counts)
+        *v = 0;
+        if (s.mf.on && s.mf.counts.p) {
+            std::vector<uint32_t> c(s.mf.nmol);
+            MDX_CUDA_TRY(cudaStreamSynchronize(s.stream));
+            MDX_CUDA_TRY(cudaMemcpy(c.data(), s.mf.counts.p, c.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+            int64_t t = 0;
+            for (uint32_t x : c) t += std::min<int64_t>(x, s.mf.cap);
+            *v = t;
+        }
+    }
     else {
         set_error(MDX_ERR_ARG, "unknown int key '%s'", key);
         return MDX_ERR_ARG;

@@ -185,7 +185,7 @@ class State:
             out = c_dbl()
             check(lib().mdx_state_get_double(self._h, k.encode(), ctypes.byref(out)))
             return out.value
-        if k in State._INT_KEYS or k in ("nlistCapacity", "cellsPerSide", "molListCapacity"):
+        if k in State._INT_KEYS or k in ("nlistCapacity", "cellsPerSide", "molListCapacity", "molListEntries"):
             out = c_i64()
             check(lib().mdx_state_get_int(self._h, k.encode(), ctypes.byref(out)))
             return out.value
