@@ -147,6 +147,17 @@ int mdx_fix_rigid_create_rigid(mdx_fix *fix, int id_o, int id_h1, int id_h2, int
  * (src/Fixes/FixNoseHoover.cu:97-130, 221-226) */
 int mdx_fix_nose_hoover_create(mdx_state *st, const char *handle, const char *group, mdx_fix **out);
 int mdx_fix_nose_hoover_set_temperature(mdx_fix *fix, double temperature, double time_constant);
+/* FixNoseHoover::setPressure("ISO", pressure, timeConstant)
+ * (FixNoseHoover.cu:193-202): the fix also barostats, with the MTK
+ * propagator of stepInit / postNVE_V / stepFinal (FixNoseHoover.cu:413-605,
+ * 628-1032) run on the host in FP64 around device kernels, the box scaled
+ * about its centre every step.  Systems without FixRigid ("ANISO" and rigid
+ * bodies: MDX_ERR_UNSUPPORTED).  A barostatting state runs through
+ * mdx_integrator_run only. */
+int mdx_fix_nose_hoover_set_pressure(mdx_fix *fix, const char *mode, double pressure, double time_constant);
+/* "lastPressure" (the instantaneous pressure of the last stepFinal),
+ * "pressVel", "pressMass" (the isotropic barostat's velocity and mass) */
+int mdx_fix_nose_hoover_get(mdx_fix *fix, const char *key, double *value);
 int mdx_fix_destroy(mdx_fix *fix);
 
 /* ---- integrator (src/Integrators/IntegratorVerlet.cu:649-770) ----------- */

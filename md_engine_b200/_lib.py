@@ -67,6 +67,8 @@ SIGNATURES = [
     ("mdx_fix_rigid_create_rigid", c_int, [c_void_p, c_int, c_int, c_int, c_int]),
     ("mdx_fix_nose_hoover_create", c_int, [c_void_p, c_char_p, c_char_p, P(c_void_p)]),
     ("mdx_fix_nose_hoover_set_temperature", c_int, [c_void_p, c_dbl, c_dbl]),
+    ("mdx_fix_nose_hoover_set_pressure", c_int, [c_void_p, c_char_p, c_dbl, c_dbl]),
+    ("mdx_fix_nose_hoover_get", c_int, [c_void_p, c_char_p, P(c_dbl)]),
     ("mdx_fix_destroy", c_int, [c_void_p]),
     ("mdx_integrator_verlet_create", c_int, [c_void_p, P(c_void_p)]),
     ("mdx_integrator_run", c_int, [c_void_p, c_int, P(c_dbl)]),

@@ -518,6 +518,28 @@ int mdx_fix_nose_hoover_set_temperature(mdx_fix *fix, double T, double tau) {
     return static_cast<FixNoseHoover *>(fix->f)->setTemperature(T, tau);
 }
 
+int mdx_fix_nose_hoover_set_pressure(mdx_fix *fix, const char *mode, double pressure, double time_constant) {
+    ARG_CHECK(fix && mode, "null argument");
+    ARG_CHECK(fix->f->kind == FixKind::NoseHoover, "not a FixNoseHoover");
+    fix->f->state->prepared = false;
+    return static_cast<FixNoseHoover *>(fix->f)->setPressure(mode, pressure, time_constant);
+}
+
+int mdx_fix_nose_hoover_get(mdx_fix *fix, const char *key, double *value) {
+    ARG_CHECK(fix && key && value, "null argument");
+    ARG_CHECK(fix->f->kind == FixKind::NoseHoover, "not a FixNoseHoover");
+    const FixNoseHoover &nh = *static_cast<FixNoseHoover *>(fix->f);
+    const std::string k = key;
+    if (k == "lastPressure") *value = nh.lastPressure;
+    else if (k == "pressVel") *value = nh.pressVel[0];
+    else if (k == "pressMass") *value = nh.pressMass[0];
+    else {
+        set_error(MDX_ERR_ARG, "unknown FixNoseHoover key '%s'", key);
+        return MDX_ERR_ARG;
+    }
+    return 0;
+}
+
 int mdx_fix_destroy(mdx_fix *fix) {
     if (!fix) return 0;
     State &s = *fix->f->state;

@@ -479,10 +479,27 @@ class FixNoseHoover : public Fix {
     DBuf<double> partials;
     DBuf<unsigned int> counter;
     bool chain_on_device = false;
+    // barostatting (setPressure("ISO", P, timeConstant), FixNoseHoover.cu:
+    // 153-219): the MTK propagator of FixNoseHoover.cu:413-604 on the host in
+    // FP64, as the reference runs it, with the box change, velocity scalings
+    // and reductions on the device
+    bool barostatting = false;
+    double pressure = 0, ptau = 0;
+    double pressVel[3] = {0, 0, 0}, pressMass[3] = {0, 0, 0};
+    double pThermVel[kNHChain] = {}, pThermForce[kNHChain] = {}, pThermMass[kNHChain] = {};
+    double pendingScale = 1.0;    // thermostat factors not yet applied to the velocities
+    double lastPressure = 0.0;    // the instantaneous pressure of the last stepFinal
     FixNoseHoover(State *s, std::string h, std::string g);
     int setTemperature(double T_, double tau_);
+    int setPressure(const std::string &mode, double P, double tau_);
     int prepareFinal();
 };
+// an NPT run with FixNoseHoover's barostat: initialisation (prepareFinal,
+// FixNoseHoover.cu:240-404) and one step in the reference's hook order
+double nh_integrate(NHChain &c, bool stepInit);  // thermostatIntegrate on a chain (FP64)
+int mtk_prepare(State &s, FixNoseHoover &nh);
+int mtk_step(State &s, FixNoseHoover &nh);
+int mtk_finish(State &s, FixNoseHoover &nh);
 
 // ---------------------------------------------------------------- State
 class State {

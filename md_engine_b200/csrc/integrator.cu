@@ -220,7 +220,7 @@ class IntegratorVerlet {
     // CUDA events on the library stream, L2 flushed (a write larger than L2)
     // before every chunk outside the timed windows; returns summed device ms
     int runTimed(int nturns, int chunk, size_t flush_bytes, double *ms_total) {
-        if (s->barostatFix()) {
+        if (s->barostatFix() || (s->nhFix() && s->nhFix()->barostatting)) {
             set_error(MDX_ERR_UNSUPPORTED, "a barostat changes the box between steps: use mdx_integrator_run");
             return MDX_ERR_UNSUPPORTED;
         }
@@ -277,7 +277,7 @@ class IntegratorVerlet {
     size_t h_stage_n = 0;
     DBuf<double> d_stage;
     int runHost(int nturns, const double *pin, const double *vin, double *pout, double *vout, double *fout) {
-        if (s->barostatFix()) {
+        if (s->barostatFix() || (s->nhFix() && s->nhFix()->barostatting)) {
             set_error(MDX_ERR_UNSUPPORTED, "a barostat changes the box between steps: use mdx_integrator_run");
             return MDX_ERR_UNSUPPORTED;
         }
@@ -339,6 +339,37 @@ class IntegratorVerlet {
         return 0;
     }
 
+    // an NPT run with FixNoseHoover's barostat (the MTK propagator): host
+    // steps in the reference's hook order, the box moving every step
+    int runMtk(FixNoseHoover &nh, int nturns, double *ptsps) {
+        if (int e = mtk_prepare(*s, nh)) return e;
+        cudaEvent_t e0, e1;
+        MDX_CUDA_TRY(cudaEventCreate(&e0));
+        MDX_CUDA_TRY(cudaEventCreate(&e1));
+        MDX_CUDA_TRY(cudaEventRecord(e0, s->stream));
+        for (int k = 0; k < nturns; k++) {
+            if (int e = mtk_step(*s, nh)) return e;
+            const int64_t t = s->turn;
+            s->turn += 1;
+            MDX_CUDA_TRY(cudaMemcpyAsync(&s->d_status.p->turn, &s->turn, sizeof(int64_t), cudaMemcpyHostToDevice,
+                                         s->stream));
+            if (config_next_write(*s, t) == t) {
+                if (int e = s->checkStatus()) return e;
+                if (int e = config_write_due(*s, t)) return e;
+            }
+        }
+        MDX_CUDA_TRY(cudaEventRecord(e1, s->stream));
+        MDX_CUDA_TRY(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        MDX_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (int e = s->checkStatus()) return e;
+        if (int e = mtk_finish(*s, nh)) return e;
+        if (ptsps) *ptsps = ms > 0 ? (double)s->atoms.size() * nturns / (ms * 1e-3) : 0.0;
+        return s->download();
+    }
+
     int run(int nturns, double *ptsps) {
         if (nturns < 0) {
             set_error(MDX_ERR_ARG, "numTurns must be >= 0");
@@ -348,6 +379,8 @@ class IntegratorVerlet {
             clearGraphs();
             if (int e = s->prepare()) return e;
         }
+        if (FixNoseHoover *nh = s->nhFix())
+            if (nh->barostatting) return runMtk(*nh, nturns, ptsps);
         const int P = s->periodicInterval > 0 ? s->periodicInterval : 1;
         cudaEvent_t e0, e1;
         MDX_CUDA_TRY(cudaEventCreate(&e0));

@@ -1506,6 +1506,18 @@ int molform_init(State &s) {
 // width (cells never narrower than the list radius / m); the caller forces a
 // rebuild.  The minimum-image and stencil conditions of nlist_init and
 // molform_init are checked again.
+// a box that grew without bound (a barostat run away) ends the run with an
+// error instead of an overflowing grid
+static int grid_cells_fit(int3 ns) {
+    const long long n = (long long)ns.x * ns.y * ns.z;
+    if (n > (1LL << 27)) {
+        set_error(MDX_ERR_UNSUPPORTED, "the box grew to %d x %d x %d neighbour cells (more than 2^27)", ns.x, ns.y,
+                  ns.z);
+        return MDX_ERR_UNSUPPORTED;
+    }
+    return 0;
+}
+
 int nlist_box_changed(State &s) {
     GridGPU &gr = s.grid;
     const double Lmin = std::min(s.box.Ld.x, std::min(s.box.Ld.y, s.box.Ld.z));
@@ -1521,6 +1533,7 @@ int nlist_box_changed(State &s) {
             set_error(MDX_ERR_UNSUPPORTED, "the box shrank below the neighbour grid's %d cells per side", need);
             return MDX_ERR_UNSUPPORTED;
         }
+        if (int e = grid_cells_fit(ns)) return e;
         const int ncell = ns.x * ns.y * ns.z;
         if (int e = gr.cell_start.alloc(ncell + 1)) return e;
         if (int e = gr.cell_count.alloc(ncell)) return e;
@@ -1540,6 +1553,7 @@ int nlist_box_changed(State &s) {
             set_error(MDX_ERR_UNSUPPORTED, "the box shrank below the molecule grid's %d cells per side", 2 * mf.m + 1);
             return MDX_ERR_UNSUPPORTED;
         }
+        if (int e = grid_cells_fit(ns)) return e;
         const int ncell = ns.x * ns.y * ns.z;
         if (int e = mf.cell_start.alloc(ncell + 1)) return e;
         if (int e = mf.cell_count.alloc(ncell)) return e;

@@ -695,6 +695,22 @@ int FixNoseHoover::setTemperature(double T_, double tau_) {
     return 0;
 }
 
+int FixNoseHoover::setPressure(const std::string &mode, double P, double tau_) {
+    if (mode != "ISO") {
+        set_error(MDX_ERR_UNSUPPORTED, "FixNoseHoover::setPressure: mode '%s' (this library implements ISO)",
+                  mode.c_str());
+        return MDX_ERR_UNSUPPORTED;
+    }
+    if (tau_ <= 0) {
+        set_error(MDX_ERR_ARG, "pressure time constant must be positive");
+        return MDX_ERR_ARG;
+    }
+    barostatting = true;
+    pressure = P;
+    ptau = tau_;
+    return 0;
+}
+
 int FixNoseHoover::prepareFinal() { return nh_prepare(*state, *this); }
 
 }  // namespace mdx

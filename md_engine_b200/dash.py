@@ -655,6 +655,24 @@ class FixNoseHoover(_Fix):
     def setTemperature(self, temperature, timeConstant):
         check(lib().mdx_fix_nose_hoover_set_temperature(self._h, float(temperature), float(timeConstant)))
 
+    def setPressure(self, pressMode, pressure, timeConstant):
+        """FixNoseHoover::setPressure (FixNoseHoover.cu:193-202); pressMode "ISO" """
+        check(lib().mdx_fix_nose_hoover_set_pressure(self._h, pressMode.encode(), float(pressure),
+                                                     float(timeConstant)))
+
+    def _get(self, k):
+        out = c_dbl()
+        check(lib().mdx_fix_nose_hoover_get(self._h, k.encode(), ctypes.byref(out)))
+        return out.value
+
+    @property
+    def lastPressure(self):
+        return self._get("lastPressure")
+
+    @property
+    def pressVel(self):
+        return self._get("pressVel")
+
 
 class WriteConfig:
     """WriteConfig(state, fn, handle, format, writeEvery, groupHandle='all',

@@ -173,3 +173,61 @@ def test_berendsen_water_runs_in_the_molecule_form(oracle):
     sysd1 = systems.System(**{**sysd.__dict__, "lo": lo1, "L": hi1 - lo1})
     rel, rms = _water_forces_vs_oracle(oracle, st, sysd1, lo1, hi1 - lo1)
     assert rel < FORCE_RTOL, f"{rel:.3e} of RMS {rms:.3e}"
+
+
+def test_mtk_npt_lj_follows_the_fp64_oracle():
+    """FixNoseHoover.setPressure("ISO", P, tau): 30 NPT steps of an LJ fluid
+    against the FP64 restatement of the reference's MTK propagator
+    (oracle/mtk.py) from the same start: box, positions, barostat velocity
+    and pressure"""
+    from oracle.mtk import MTKLJ
+    sysd = systems.lj_fcc(ncell=6, rho=0.8, jitter=0.05, seed=21, T=1.5)
+    st, fx = systems.build_lj_state(sysd, rcut=2.5, skin=0.3, T=1.5, tau=0.5)
+    nh = fx[1]
+    nh.setPressure("ISO", 2.5, 0.5)
+    ref = MTKLJ(sysd, T=1.5, tau=0.5, P=2.5, ptau=0.5)
+    it = IntegratorVerlet(st)
+    for chunk in range(3):
+        it.run(10)
+        if chunk:
+            ref.restart()  # each run restarts the barostat at rest
+        for _ in range(10):
+            ref.step()
+        ref.v *= ref.pending  # run end: the pending thermostat scale applied
+        ref.pending = 1.0
+        lo, hi = _box(st)
+        np.testing.assert_allclose(hi - lo, ref.L, rtol=2e-6)
+        assert nh.pressVel == pytest.approx(ref.pvel[0], rel=2e-3, abs=1e-6)
+        assert nh.lastPressure == pytest.approx(ref.last_pressure, rel=2e-4)
+        x, v, _ = st.getAtoms()
+        d = _min_image(x - ref.x, ref.L)
+        assert np.abs(d).max() < 5e-4, np.abs(d).max()
+        assert np.abs(v - ref.v).max() < 5e-3 * np.abs(ref.v).max()
+    assert st.status()[0] == 0
+
+
+def test_mtk_npt_lj_reaches_the_set_pressure():
+    """an LJ fluid started on a lattice at T = 1.5, rho = 0.7 (pressure -3.7)
+    under the MTK barostat at P = 1: the box first shrinks, the mean pressure
+    over the last stretch is the set point, and the density is the one the
+    FP64 oracle's own 1,500-step run of the same propagator reaches on 864
+    atoms (0.58)"""
+    sysd = systems.lj_fcc(ncell=10, rho=0.7, jitter=0.05, seed=23, T=1.5)
+    st, fx = systems.build_lj_state(sysd, rcut=2.5, skin=0.3, T=1.5, tau=0.5)
+    nh = fx[1]
+    nh.setPressure("ISO", 1.0, 0.5)
+    lo0, hi0 = _box(st)
+    it = IntegratorVerlet(st)
+    it.run(100)
+    lo1, hi1 = _box(st)
+    assert np.prod(hi1 - lo1) < np.prod(hi0 - lo0)
+    it.run(1400)
+    ps, rho = [], []
+    for _ in range(40):
+        it.run(25)
+        ps.append(nh.lastPressure)
+        lo, hi = _box(st)
+        rho.append(len(sysd.pos) / np.prod(hi - lo))
+    assert abs(np.mean(ps) - 1.0) < 0.25, np.mean(ps)
+    assert abs(np.mean(rho) - 0.58) < 0.03, np.mean(rho)
+    assert st.status()[0] == 0
