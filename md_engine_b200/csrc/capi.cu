@@ -761,6 +761,15 @@ int mdx_verlet_second_half(mdx_state *st) {
     return 0;
 }
 
+// holds the stream for a fixed number of SM clock cycles (bounded: reads
+// nothing, waits on nothing) so that the host enqueues every timed launch
+// before the first one runs: the events then time the device alone, not the
+// host's launch rate
+static __global__ void k_hold(long long cycles) {
+    const long long t0 = clock64();
+    while (clock64() - t0 < cycles) __nanosleep(2000);
+}
+
 int mdx_time_stage(mdx_state *st, int stage, int iters, size_t flush_bytes, double *avg_ms) {
     ARG_CHECK(st && avg_ms && iters > 0, "bad argument");
     State &s = *st->s;
@@ -770,6 +779,9 @@ int mdx_time_stage(mdx_state *st, int stage, int iters, size_t flush_bytes, doub
         if (int e = flush.alloc(flush_bytes)) return e;
     std::vector<cudaEvent_t> ev(2 * iters);
     for (auto &e : ev) MDX_CUDA_TRY(cudaEventCreate(&e));
+    // ~40 us of host enqueue per iteration covered (at 2 GHz), 2 ms at least
+    k_hold<<<1, 1, 0, s.stream>>>(std::max(4000000LL, 80000LL * iters));
+    MDX_LAUNCHED();
     for (int k = 0; k < iters; k++) {
         if (flush_bytes) MDX_CUDA_TRY(cudaMemsetAsync(flush.p, k & 0xff, flush_bytes, s.stream));
         MDX_CUDA_TRY(cudaEventRecord(ev[2 * k], s.stream));
@@ -790,7 +802,10 @@ int mdx_time_stage(mdx_state *st, int stage, int iters, size_t flush_bytes, doub
             case 2: {
                 FixE3B *f = s.e3bFix();
                 ARG_CHECK(f, "no FixE3B");
-                e = e3b_forces(s, *f);
+                // the kernels as the fused step launches them: into the
+                // per-step E3B buffer (16-byte atomics), PDL-chained
+                if (f->side_ok && f->f_side.p) e = e3b_forces_to(s, *f, f->f_side.p, true, s.stream);
+                else e = e3b_forces(s, *f);
                 break;
             }
             case 3: e = nlist_rebuild(s, true, false); break;

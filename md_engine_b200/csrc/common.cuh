@@ -99,11 +99,21 @@ __device__ __forceinline__ float rcp_ftz(float x) {
 // exp(-x^2) as 2^(-x^2 log2 e)
 __device__ __forceinline__ float exp_neg_sq(float x) { return ex2_ftz(-(x * x) * 1.4426950408889634f); }
 
-// minimum image (BoundsGPU::minImage, BoundsGPU.h:91-108)
+// nearest integer of |x| < 2^22 as rintf gives it (ties to even), by two
+// round-to-nearest additions of 1.5 * 2^23: the sum's unit in the last place
+// is 1, so the addition itself rounds x to an integer.  Two FP32 adds on the
+// FMA pipe in place of a rounding instruction; __fadd_rn keeps the compiler
+// from folding the pair.
+__device__ __forceinline__ float rint_small(float x) {
+    return __fadd_rn(__fadd_rn(x, 12582912.0f), -12582912.0f);
+}
+
+// minimum image (BoundsGPU::minImage, BoundsGPU.h:91-108); the scaled
+// separations are a few box lengths at most
 __device__ inline float3 min_image(const Box &b, float3 v) {
-    v.x -= b.L.x * rintf(v.x * b.invL.x);
-    v.y -= b.L.y * rintf(v.y * b.invL.y);
-    v.z -= b.L.z * rintf(v.z * b.invL.z);
+    v.x -= b.L.x * rint_small(v.x * b.invL.x);
+    v.y -= b.L.y * rint_small(v.y * b.invL.y);
+    v.z -= b.L.z * rint_small(v.z * b.invL.z);
     return v;
 }
 __device__ inline double3 min_image(const Box &b, double3 v) {

@@ -89,6 +89,18 @@ __device__ __forceinline__ void pair_geom(const E3BParams &p, const Box &box, co
     e3b_ef(p, min_image(box, m1.c - m2.a), g.es[3], g.fv[3]);
 }
 
+// the same with whole molecules (the molecule form: a molecule's sites are
+// made whole at every rebuild and move together): each O-H separation is an
+// intramolecular vector plus the O-O image d12 = x(O1) - x(O2), no further
+// minimum images.  h1b/h1c, h2b/h2c: the H - O vectors of molecules 1 and 2
+__device__ __forceinline__ void pair_geom_whole(const E3BParams &p, float3 d12, float3 h1b, float3 h1c, float3 h2b,
+                                                float3 h2c, PairGeom &g) {
+    e3b_ef(p, h2b - d12, g.es[0], g.fv[0]);
+    e3b_ef(p, h2c - d12, g.es[1], g.fv[1]);
+    e3b_ef(p, h1b + d12, g.es[2], g.fv[2]);
+    e3b_ef(p, h1c + d12, g.es[3], g.fv[3]);
+}
+
 // EvaluatorE3B::threeBodyPairForce (EvaluatorE3B.h:145-249): the forces on
 // both molecules' atoms of one unordered pair (molecule 1 = lower index)
 __device__ __forceinline__ void pair_force_both(const E3BParams &p, const PairGeom &g, float4 T1, float4 T2,
@@ -312,6 +324,13 @@ __global__ void k_e3b_list_mf(const E3BArgs A, const uint32_t *__restrict__ pcou
 // full list) and the O-O two-body force (EvaluatorE3B::twoBodyForce, :67-78)
 // STORE: write into a per-step side buffer instead of adding to the forces
 // (lets E3B run concurrently with the pair kernel; the second half merges it)
+// list entries per lane per trip of the totals pass: all of them in flight
+// (list -> sites) before the first is evaluated
+#ifndef MDX_E3B_TOT_U
+#define MDX_E3B_TOT_U 2
+#endif
+constexpr int kTotU = MDX_E3B_TOT_U;
+
 template <int T, bool ENERGY, bool STORE = false>
 __global__ void k_e3b_totals(const E3BArgs a0, const E3BArgs *__restrict__ tab) {
     MDX_E3B_ARGS;
@@ -341,6 +360,7 @@ __global__ void k_e3b_totals(const E3BArgs a0, const E3BArgs *__restrict__ tab) 
     if (valid) {
         ix = e3b_sites(A, mol_idx, m);
         const MolPos mi = load_mol(xs, ix);
+        const float3 hb = mi.b - mi.a, hc = mi.c - mi.a;  // whole molecules (A.slots)
         int cnt = (int)mcounts[m];
         cnt = cnt < mcap ? cnt : mcap;
         const uint32_t *row = mlist + (size_t)(m / G) * mcap * G + a * T + t;
@@ -348,25 +368,26 @@ __global__ void k_e3b_totals(const E3BArgs a0, const E3BArgs *__restrict__ tab) 
         // two entries per lane per trip: both list -> molecule -> O chains are
         // in flight before either pair is evaluated.  Every lane of the team
         // makes the same trips (the partner ballot below takes the team)
-        for (int k00 = 0; k00 < cnt; k00 += 2 * T) {
+        for (int k00 = 0; k00 < cnt; k00 += kTotU * T) {
             const int k0 = k00 + t;
-            int4 jxs[2];
-            float3 ojs[2];
-            bool has[2];
-            int mjs[2];
+            int4 jxs[kTotU];
+            MolPos mps[kTotU];
+            bool has[kTotU];
+            int mjs[kTotU];
 #pragma unroll
-            for (int u = 0; u < 2; u++) {
+            for (int u = 0; u < kTotU; u++) {
                 const int k = k0 + u * T;
                 has[u] = k < cnt;
                 mjs[u] = has[u] ? (int)row[(size_t)(k / T) * 32] : m;
                 jxs[u] = e3b_sites(A, mol_idx, mjs[u]);
             }
+            // the partner's three sites in one round of loads (L2-resident;
+            // the hydrogens are used only within rmax)
 #pragma unroll
-            for (int u = 0; u < 2; u++) ojs[u] = f3(__ldg(xs + jxs[u].x));
+            for (int u = 0; u < kTotU; u++) mps[u] = load_mol(xs, jxs[u]);
 #pragma unroll
-            for (int u = 0; u < 2; u++) {
-            const int4 jx = jxs[u];
-            const float3 oj = ojs[u];
+            for (int u = 0; u < kTotU; u++) {
+            const float3 oj = mps[u].a;
             const float3 dr = min_image(box, mi.a - oj);
             const float r2 = dot3(dr, dr);
             if (!ENERGY && clist) {
@@ -391,20 +412,13 @@ __global__ void k_e3b_totals(const E3BArgs a0, const E3BArgs *__restrict__ tab) 
             fz += dr.z * s;
             if (ENERGY) e2 += 0.5f * p.E2 * ex;
             if (r <= p.rmax) {
-                MolPos mj_;
-                mj_.a = oj;
-                mj_.b = f3(__ldg(xs + jx.y));
-                mj_.c = f3(__ldg(xs + jx.z));
-                float e;
-                float3 f;
-                e3b_ef(p, min_image(box, mj_.b - mi.a), e, f);
-                tx += e;
-                e3b_ef(p, min_image(box, mj_.c - mi.a), e, f);
-                tx += e;
-                e3b_ef(p, min_image(box, mi.b - mj_.a), e, f);
-                ty += e;
-                e3b_ef(p, min_image(box, mi.c - mj_.a), e, f);
-                tz += e;
+                const MolPos &mj_ = mps[u];
+                PairGeom g;
+                if (A.slots) pair_geom_whole(p, dr, hb, hc, mj_.b - oj, mj_.c - oj, g);
+                else pair_geom(p, box, mi, mj_, g);
+                tx += g.es[0] + g.es[1];
+                ty += g.es[2];
+                tz += g.es[3];
             }
             }
         }
@@ -477,29 +491,31 @@ __global__ void k_e3b_forces(const E3BArgs a0, const E3BArgs *__restrict__ tab) 
         for (int k0 = t; k0 < cnt; k0 += 2 * T) {
             int mjs[2];
             int4 jxs[2];
-            float3 ojs[2];
+            MolPos mps[2];
+            float4 Tjs[2];
 #pragma unroll
             for (int u = 0; u < 2; u++) {
                 const int k = k0 + u * T;
                 mjs[u] = k < cnt ? (int)row[(size_t)(k / T) * 32] : -1;
                 jxs[u] = e3b_sites(A, mol_idx, mjs[u] < 0 ? m : mjs[u]);
             }
+            // sites and totals of both partners in one round of loads
 #pragma unroll
-            for (int u = 0; u < 2; u++) ojs[u] = f3(__ldg(xs + jxs[u].x));
+            for (int u = 0; u < 2; u++) {
+                mps[u] = load_mol(xs, jxs[u]);
+                Tjs[u] = __ldg(totals + (mjs[u] < 0 ? m : mjs[u]));
+            }
 #pragma unroll
             for (int u = 0; u < 2; u++) {
             if (mjs[u] < 0) continue;
             const int mj = mjs[u];
             const int4 jx = jxs[u];
-            MolPos mjp;
-            mjp.a = ojs[u];
+            const MolPos &mjp = mps[u];
             const float3 dr = min_image(box, mi.a - mjp.a);
             const float r2 = dot3(dr, dr);
             if (r2 >= p.list_cut2) continue;
             if (r2 > p.rmax * p.rmax) continue;
-            mjp.b = f3(__ldg(xs + jx.y));
-            mjp.c = f3(__ldg(xs + jx.z));
-            const float4 Tj = __ldg(totals + mj);
+            const float4 Tj = Tjs[u];
             const bool first = m < mj;
             PairGeom g;
             if (ENERGY) {
@@ -512,7 +528,8 @@ __global__ void k_e3b_forces(const E3BArgs a0, const E3BArgs *__restrict__ tab) 
             // (molecule 1, as the reference's i < j); the partner's share is
             // scattered with vector atomics
             if (!first) continue;
-            pair_geom(p, box, mi, mjp, g);
+            if (A.slots) pair_geom_whole(p, dr, mi.b - mi.a, mi.c - mi.a, mjp.b - mjp.a, mjp.c - mjp.a, g);
+            else pair_geom(p, box, mi, mjp, g);
             float3 a1, b1, c1, a2, b2, c2;
             pair_force_both(p, g, Ti, Tj, a1, b1, c1, a2, b2, c2);
             fa += a1;

@@ -306,8 +306,9 @@ __global__ void __launch_bounds__(kMolPairBlock, 14) k_pair_mol(const MolPairArg
             float3 sh = make_float3(0.f, 0.f, 0.f);
             if (e < cnt) {
                 const float3 d = xi[0] - f3(x_cur);
-                sh = make_float3(A.box.L.x * rintf(d.x * A.box.invL.x), A.box.L.y * rintf(d.y * A.box.invL.y),
-                                 A.box.L.z * rintf(d.z * A.box.invL.z));
+                sh = make_float3(A.box.L.x * rint_small(d.x * A.box.invL.x),
+                                 A.box.L.y * rint_small(d.y * A.box.invL.y),
+                                 A.box.L.z * rint_small(d.z * A.box.invL.z));
                 const float3 dm = d - sh;
                 pass = dot3(dm, dm) < A.far2;
             }

@@ -85,6 +85,14 @@ RefLayout make_layout(int n, const int *counts, const uint32_t *nbr, int maxn, i
 int g_iters = 0;
 float g_ms = 0.f;
 
+// holds the stream for a fixed number of SM cycles (bounded, waits on
+// nothing) so that every timed launch is enqueued before the first runs and
+// the events time the device, not the host's launch rate
+__global__ void k_hold(long long cycles) {
+    const long long t0 = clock64();
+    while (clock64() - t0 < cycles) __nanosleep(2000);
+}
+
 template <class F>
 void time_launches(F &&launch) {
     g_ms = 0.f;
@@ -93,6 +101,7 @@ void time_launches(F &&launch) {
     cudaEventCreate(&a);
     cudaEventCreate(&b);
     launch();  // warm
+    k_hold<<<1, 1>>>(g_iters * 80000LL > 4000000LL ? g_iters * 80000LL : 4000000LL);
     cudaEventRecord(a);
     for (int k = 0; k < g_iters; k++) launch();
     cudaEventRecord(b);
