@@ -1,22 +1,39 @@
-# Compiles the reference's own header kernels (from the reference sources in
-# place) plus oracle/ref_harness.cu into oracle/_ref/librefkernels.so.
-# Test infrastructure only; run where the reference is mounted, the .so
-# travels to the GPU box.  Flags follow the reference's CMakeLists.txt:53.
+# Compiles the reference's own kernels (from the reference sources in place)
+# plus oracle/ref_harness.cu and oracle/ref_grid_harness.cu into
+# oracle/_ref/librefkernels.so.  Test infrastructure only; run where the
+# reference is mounted, the .so travels to the GPU box.  Flags follow the
+# reference's CMakeLists.txt:53.
 # The reference source tree: $(MDX_REFERENCE_SRC) when set, else the default
 # below; the target is skipped (with a note) when the tree is absent.
 REF ?= $(or $(MDX_REFERENCE_SRC),/root/reference/src)
 NVCC ?= /usr/local/cuda/bin/nvcc
+CUDA_INC ?= $(dir $(NVCC))../targets/x86_64-linux/include
 INC = -I ref_shim -I $(REF) -I $(REF)/Evaluators -I $(REF)/GPUArrays -I $(REF)/Fixes -I $(REF)/DataStorageUser
 FLAGS = -gencode arch=compute_100a,code=sm_100a -std=c++14 -Xcompiler -fPIC --use_fast_math --prec-div=true \
         --prec-sqrt=true -O3 -w
+# GridGPU.cu includes State.h, Fix.h, Bond.h and Mod.h with quotes from its
+# own directory; the split include path (-I-) stops that directory from being
+# searched first, so that the stand-ins in ref_shim_grid/ are found instead.
+# Quote includes of CUDA's own headers and of nvcc's temporary files then
+# need their directories before the split.
+GRID_TMP = _ref/tmp
+GRID_INC = -I ref_shim_grid -I $(CUDA_INC)/crt -I $(CUDA_INC) -I $(GRID_TMP) -I- -I ref_shim_grid -I $(REF) \
+           -I $(REF)/Evaluators -I $(REF)/GPUArrays -I $(REF)/Fixes -I $(REF)/DataStorageUser -I $(REF)/BondedForcers
 
 ifeq ($(wildcard $(REF)/Evaluators/PairEvaluateIso.h),)
 _ref/librefkernels.so:
 	@echo "reference sources not found under $(REF): oracle/_ref not built"
 else
-_ref/librefkernels.so: ref_harness.cu
+_ref/librefkernels.so: _ref/ref_harness.o _ref/ref_grid_harness.o
+	$(NVCC) -gencode arch=compute_100a,code=sm_100a -shared -o $@ $^
+
+_ref/ref_harness.o: ref_harness.cu
 	@mkdir -p _ref
-	$(NVCC) $(FLAGS) $(INC) -shared -o $@ ref_harness.cu
+	$(NVCC) $(FLAGS) $(INC) -c -o $@ ref_harness.cu
+
+_ref/ref_grid_harness.o: ref_grid_harness.cu $(wildcard ref_shim_grid/*.h ref_shim_grid/boost/*.hpp)
+	@mkdir -p _ref $(GRID_TMP)
+	TMPDIR=$(abspath $(GRID_TMP)) $(NVCC) $(FLAGS) $(GRID_INC) -c -o $@ ref_grid_harness.cu
 endif
 
 clean:

@@ -37,6 +37,10 @@ def lib():
         _L.ref_ljfs_host.argtypes = [F, F, F, V, V]
         _L.ref_pair_styles.argtypes = [I, V, V, V, V, I, V, I, I, V, V, F, F, F, I, I, F, F, F, F, F, I, I, V]
         _L.ref_pair_styles.restype = I
+        _L.ref_grid_skin_flag.argtypes = [I, V, V, V, V, F]
+        _L.ref_grid_skin_flag.restype = I
+        _L.ref_grid_build.argtypes = [I, V, V, V, V, F, I, I, I, V, V, V]
+        _L.ref_grid_build.restype = I
     return _L
 
 
@@ -128,3 +132,38 @@ def timed(fn, iters, *a, **kw):
         return out, float(lib().ref_last_ms())
     finally:
         lib().ref_set_timing(0)
+
+
+def grid_skin_flag(xa, xb, lo, L, padding):
+    """the reference's setBuildFlag on positions xa (current) and xb (last
+    build): 1 if some atom moved more than padding / 2"""
+    a = np.zeros((len(xa), 4), np.float32)
+    a[:, :3] = xa
+    b = np.zeros((len(xb), 4), np.float32)
+    b[:, :3] = xb
+    lo = np.ascontiguousarray(lo, np.float32)
+    L = np.ascontiguousarray(L, np.float32)
+    r = lib().ref_grid_skin_flag(len(a), _p(a), _p(b), _p(lo), _p(L), float(padding))
+    if r < 0:
+        raise RuntimeError(f"reference setBuildFlag failed: {r}")
+    return r
+
+
+def grid_build(x, lo, L, neigh_cut, min_dim=None, ntpb=256, ntpa=1, maxn=512):
+    """a forced build of the reference's GridGPU kernels on positions x (ids
+    0..n-1): per id its neighbour count, its neighbours' ids (list order) and
+    the wrapped position the list was built on"""
+    n = len(x)
+    xs4 = np.zeros((n, 4), np.float32)
+    xs4[:, :3] = x
+    lo = np.ascontiguousarray(lo, np.float32)
+    L = np.ascontiguousarray(L, np.float32)
+    md = np.ascontiguousarray(min_dim if min_dim is not None else np.full(3, neigh_cut), np.float32)
+    counts = np.zeros(n, np.int32)
+    nbr = np.zeros((n, maxn), np.uint32)
+    wrapped = np.zeros((n, 4), np.float32)
+    r = lib().ref_grid_build(n, _p(xs4), _p(lo), _p(L), _p(md), float(neigh_cut), ntpb, ntpa, maxn, _p(counts),
+                             _p(nbr), _p(wrapped))
+    if r != 0:
+        raise RuntimeError(f"reference GridGPU build failed: {r}")
+    return counts, nbr, wrapped[:, :3]

@@ -11,6 +11,7 @@ import numpy as np
 import pytest
 
 from md_engine_b200 import MdxError, systems
+from oracle import refkernels as R
 from tests.helpers import FORCE_RTOL, force_err, oracle_water_params, water_small
 
 pytestmark = pytest.mark.gpu
@@ -33,8 +34,13 @@ def test_skin_check_rebuilds_only_past_half_the_skin(oracle):
     c1, n1, _ = st.getNeighborList()
     assert b1 == b0
     assert np.array_equal(c0, c1) and np.array_equal(n0, n1)
+    if R.available():
+        # the reference's own setBuildFlag makes the same decision
+        assert R.grid_skin_flag(x, x0, sysd.lo, sysd.L, skin) == 0
     # just over skin/2: rebuilt on the new positions, the oracle's pair set
     x[7, 0] = x0[7, 0] + 0.501 * skin
+    if R.available():
+        assert R.grid_skin_flag(x, x0, sysd.lo, sysd.L, skin) == 1
     st.putAtoms(positions=x)
     st.buildNeighborlists(force=False)
     _, _, b2 = st.status()

@@ -1,12 +1,14 @@
 """The B200 kernels against the REFERENCE's own kernels compiled from its
-source for sm_100a (oracle/ref.mk: compute_force_iso, compute_E3B_force_*),
-run on the same GPU with the same inputs.  Both are FP32, so the tolerance is
-tight.  Skipped where oracle/_ref was not built (reference sources absent)."""
+source for sm_100a (oracle/ref.mk: compute_force_iso, compute_E3B_force_*,
+and GridGPU.cu's grid kernels from periodicWrap to assignNeighbors), run on
+the same GPU with the same inputs.  Both are FP32, so the tolerance is tight
+and the neighbour sets are compared bit for bit.  Skipped where oracle/_ref
+was not built (reference sources absent)."""
 import numpy as np
 import pytest
 
 from md_engine_b200 import systems
-from tests.helpers import water_bonds, water_small
+from tests.helpers import neighbor_cut, water_bonds, water_small
 
 pytestmark = pytest.mark.gpu
 
@@ -24,6 +26,39 @@ def _xs4(x, types):
     xs4[:, :3] = x
     xs4[:, 3] = np.asarray(types, np.int32).view(np.float32)
     return xs4
+
+
+@pytest.mark.parametrize("case,ntpa", [("lj", 1), ("lj", 8), ("water", 1), ("water_mf", 4)])
+def test_neighbor_list_matches_reference_gridgpu(oracle, case, ntpa):
+    """this library's list against a forced build of the reference's own
+    GridGPU kernels (GridGPU.cu:138-161 wrap, 190-293 bin and sort, 326-734
+    count and assign) on the same positions: the same wrapped positions, the
+    same per-atom counts and the same neighbour set of every atom (ids; the
+    reference is built without exclusions, so the intramolecular pairs this
+    library tags are compared as plain pairs)"""
+    if case == "lj":
+        sysd = systems.lj_fcc(ncell=12, seed=5, jitter=0.05)
+        st, _ = systems.build_lj_state(sysd, rcut=2.5, skin=0.3)
+        rcut, pad = 2.5, 0.3
+    else:
+        sysd = systems.water_tip4p2005(nside=12)
+        st, _ = systems.build_water_state(sysd, rcut=9.0, skin=1.0, grid=32)
+        st.pairForm = 2 if case == "water_mf" else 1
+        rcut, pad = 9.0, 1.0
+    st.prepare()
+    x_pre, _, _ = st.getAtoms()
+    st.buildNeighborlists(force=True)
+    counts_g, nbr_g, _ = st.getNeighborList()
+    cut = neighbor_cut(rcut, pad)
+    rc, rn, rw = R.grid_build(np.asarray(x_pre, np.float32), sysd.lo, sysd.L, cut, ntpa=ntpa, maxn=1024)
+    xs4 = np.zeros((len(x_pre), 4), np.float32)
+    xs4[:, :3] = np.asarray(x_pre, np.float32)
+    oracle.wrap_f32(xs4, sysd.lo, sysd.L)
+    assert np.array_equal(rw, xs4[:, :3]), "periodicWrap differs from the oracle's wrap"
+    assert np.array_equal(counts_g, rc), f"{int((counts_g != rc).sum())} atoms with other neighbour counts"
+    mism = [i for i in range(len(rc))
+            if not np.array_equal(np.sort(nbr_g[i, :rc[i]].astype(np.int64)), np.sort(rn[i, :rc[i]].astype(np.int64)))]
+    assert not mism, f"{len(mism)} atoms with other neighbour sets (first {mism[:5]})"
 
 
 def test_pair_kernel_matches_reference_kernel_lj(oracle):
