@@ -1,5 +1,6 @@
 # Compiles the reference's own kernels (from the reference sources in place)
-# plus oracle/ref_harness.cu and oracle/ref_grid_harness.cu into
+# plus oracle/ref_harness.cu, oracle/ref_grid_harness.cu and
+# oracle/ref_rigid_harness.cu into
 # oracle/_ref/librefkernels.so.  Test infrastructure only; run where the
 # reference is mounted, the .so travels to the GPU box.  Flags follow the
 # reference's CMakeLists.txt:53.
@@ -11,20 +12,23 @@ CUDA_INC ?= $(dir $(NVCC))../targets/x86_64-linux/include
 INC = -I ref_shim -I $(REF) -I $(REF)/Evaluators -I $(REF)/GPUArrays -I $(REF)/Fixes -I $(REF)/DataStorageUser
 FLAGS = -gencode arch=compute_100a,code=sm_100a -std=c++14 -Xcompiler -fPIC --use_fast_math --prec-div=true \
         --prec-sqrt=true -O3 -w
-# GridGPU.cu includes State.h, Fix.h, Bond.h and Mod.h with quotes from its
-# own directory; the split include path (-I-) stops that directory from being
-# searched first, so that the stand-ins in ref_shim_grid/ are found instead.
-# Quote includes of CUDA's own headers and of nvcc's temporary files then
-# need their directories before the split.
+# GridGPU.cu and FixRigid.cu include State.h, Fix.h, Bond.h, ... with quotes
+# from their own directories; the split include path (-I-) stops those
+# directories from being searched first, so that the stand-ins in
+# ref_shim_grid/ and ref_shim_rigid/ are found instead.  Quote includes of
+# CUDA's own headers and of nvcc's temporary files then need their
+# directories before the split.
 GRID_TMP = _ref/tmp
-GRID_INC = -I ref_shim_grid -I $(CUDA_INC)/crt -I $(CUDA_INC) -I $(GRID_TMP) -I- -I ref_shim_grid -I $(REF) \
-           -I $(REF)/Evaluators -I $(REF)/GPUArrays -I $(REF)/Fixes -I $(REF)/DataStorageUser -I $(REF)/BondedForcers
+REF_DIRS = -I $(REF) -I $(REF)/Evaluators -I $(REF)/GPUArrays -I $(REF)/Fixes -I $(REF)/DataStorageUser \
+           -I $(REF)/BondedForcers
+GRID_INC = -I ref_shim_grid -I $(CUDA_INC)/crt -I $(CUDA_INC) -I $(GRID_TMP) -I- -I ref_shim_grid $(REF_DIRS)
+RIGID_INC = -I ref_shim_rigid -I $(CUDA_INC)/crt -I $(CUDA_INC) -I $(GRID_TMP) -I- -I ref_shim_rigid $(REF_DIRS)
 
 ifeq ($(wildcard $(REF)/Evaluators/PairEvaluateIso.h),)
 _ref/librefkernels.so:
 	@echo "reference sources not found under $(REF): oracle/_ref not built"
 else
-_ref/librefkernels.so: _ref/ref_harness.o _ref/ref_grid_harness.o
+_ref/librefkernels.so: _ref/ref_harness.o _ref/ref_grid_harness.o _ref/ref_rigid_harness.o
 	$(NVCC) -gencode arch=compute_100a,code=sm_100a -shared -o $@ $^
 
 _ref/ref_harness.o: ref_harness.cu
@@ -34,6 +38,10 @@ _ref/ref_harness.o: ref_harness.cu
 _ref/ref_grid_harness.o: ref_grid_harness.cu $(wildcard ref_shim_grid/*.h ref_shim_grid/boost/*.hpp)
 	@mkdir -p _ref $(GRID_TMP)
 	TMPDIR=$(abspath $(GRID_TMP)) $(NVCC) $(FLAGS) $(GRID_INC) -c -o $@ ref_grid_harness.cu
+
+_ref/ref_rigid_harness.o: ref_rigid_harness.cu $(wildcard ref_shim_rigid/*.h ref_shim_rigid/boost/*.hpp)
+	@mkdir -p _ref $(GRID_TMP)
+	TMPDIR=$(abspath $(GRID_TMP)) $(NVCC) $(FLAGS) $(RIGID_INC) -c -o $@ ref_rigid_harness.cu
 endif
 
 clean:

@@ -41,6 +41,9 @@ def lib():
         _L.ref_grid_skin_flag.restype = I
         _L.ref_grid_build.argtypes = [I, V, V, V, V, F, I, I, I, V, V, V]
         _L.ref_grid_build.restype = I
+        D = ctypes.c_double
+        _L.ref_settle.argtypes = [I, V, V, V, V, V, V, D, D, I]
+        _L.ref_settle.restype = I
     return _L
 
 
@@ -167,3 +170,26 @@ def grid_build(x, lo, L, neigh_cut, min_dim=None, ntpb=256, ntpa=1, maxn=512):
     if r != 0:
         raise RuntimeError(f"reference GridGPU build failed: {r}")
     return counts, nbr, wrapped[:, :3]
+
+
+def settle(x0, x, v, masses, lo, L, dt, ftm_to_v, mode):
+    """the reference's SETTLE on rigid TIP4P/2005 molecules laid out O, H1,
+    H2, M per molecule (n = 4 * nmol sites): mode 1 settles the positions x
+    (from the constrained x0 of the step's start) and velocities v, then
+    places M (settlePositions + setMSite); mode 2 settles the velocities v at
+    the positions x (settleVelocities).  Returns (x, v) as float64."""
+    n = len(x)
+    def four(a, w=None):
+        o = np.zeros((n, 4), np.float32)
+        o[:, :3] = a
+        if w is not None:
+            o[:, 3] = w
+        return o
+    X0, X, Vv = four(x0), four(x), four(v)
+    ms = np.ascontiguousarray(masses, np.float64)
+    lo = np.ascontiguousarray(lo, np.float32)
+    L = np.ascontiguousarray(L, np.float32)
+    r = lib().ref_settle(n // 4, _p(X0), _p(X), _p(Vv), _p(ms), _p(lo), _p(L), float(dt), float(ftm_to_v), mode)
+    if r != 0:
+        raise RuntimeError(f"reference SETTLE failed: {r}")
+    return X[:, :3].astype(np.float64), Vv[:, :3].astype(np.float64)

@@ -168,3 +168,52 @@ def test_kernel_times_vs_reference_water4096(oracle):
     print(f"\npair: reference {best[0] * 1e3:.1f} us (NTPB {best[1]}, NTPA {best[2]}), this library {ours * 1e3:.1f} us")
     print(f"E3B: reference {best3[0] * 1e3:.1f} us (NTPB {best3[1]}, NTPA {best3[2]}), this library {ours3 * 1e3:.1f} us")
     assert best is not None and best3 is not None and ours > 0 and ours3 > 0
+
+
+def _min_image(d, L):
+    return d - L * np.rint(d / L)
+
+
+def test_settle_matches_reference_kernels(oracle):
+    """one velocity-Verlet step of rigid TIP4P/2005 water (thermostat off,
+    molecule form): the positions after this library's first half against
+    the reference's settlePositions + setMSite (FixRigid.cu:561-602,
+    850-1132), and the velocities after its second half against the
+    reference's settleVelocities (:658-848), each run on the same step's
+    inputs (the kick and drift restated in FP32 as nve_v / nve_x,
+    IntegratorVerlet.cu:23-61; the rigid-water constants from the
+    reference's own FixRigid::populateRigidData)"""
+    from md_engine_b200 import IntegratorVerlet
+    sysd = water_small(seed=41)
+    st, _ = systems.build_water_state(sysd, rcut=6.5, skin=1.0, grid=32, alpha=0.35, thermostat=False)
+    st.prepare()
+    assert int(st.pairForm) == 2
+    x0, v0, f0 = st.getAtoms()
+    IntegratorVerlet(st).run(1)
+    x1, v2, f1 = st.getAtoms()
+    mol = np.asarray(sysd.molecules)
+    assert np.array_equal(mol.ravel(), np.arange(4 * len(mol))), "sites laid out O, H1, H2, M per molecule"
+    # the step's second half folds M's force onto O and H (distributeMSite);
+    # the first half after prepare kicks O and H with their own forces only,
+    # as the reference's first step after prepareForRun does
+    assert np.abs(f1[mol[:, 3]]).max() == 0, "M forces folded onto O, H"
+    m = np.asarray(sysd.mass, np.float64)
+    invm = np.where(m > 0, 1.0 / np.where(m > 0, m, 1.0), 0.0).astype(np.float32)
+    masses = (m[mol[0, 0]], m[mol[0, 1]], m[mol[0, 3]])
+    dt = float(st.dt)
+    ftm = oracle.REAL_UNITS["ftm_to_v"]
+    dtf = np.float32(0.5 * dt * np.float32(ftm))
+    L = np.asarray(sysd.L)
+    # first half: kick, drift, SETTLE, M
+    vk = (np.asarray(v0, np.float32) + dtf * invm[:, None] * np.asarray(f0, np.float32)).astype(np.float32)
+    xu = (np.asarray(x0, np.float32) + np.float32(dt) * vk).astype(np.float32)
+    x1r, v1r = R.settle(x0, xu, vk, masses, sysd.lo, L, dt, ftm, 1)
+    dx = np.abs(_min_image(np.asarray(x1) - x1r, L)).max()
+    assert dx < 2e-5, f"positions after SETTLE differ by {dx:.2e} A"
+    # second half: kick with the step's forces, SETTLE the velocities
+    vk2 = (v1r.astype(np.float32) + dtf * invm[:, None] * np.asarray(f1, np.float32)).astype(np.float32)
+    _, v2r = R.settle(x1r, x1r, vk2, masses, sysd.lo, L, dt, ftm, 2)
+    sites = mol[:, :3].ravel()
+    vrms = np.sqrt(np.mean(np.sum(v2r[sites] ** 2, 1)))
+    dv = np.abs(np.asarray(v2)[sites] - v2r[sites]).max()
+    assert dv < 1e-3 * vrms, f"velocities after SETTLE differ by {dv / vrms:.2e} of their RMS"
