@@ -19,20 +19,23 @@ namespace mdx {
 // ---------------------------------------------------------------- NH chain
 // exp(x) for the chain's arguments, -dt/8 .. -dt/2 times a thermostat
 // velocity (|x| well below 1/64 for any stable run): the Taylor polynomial of
-// degree 8 by Horner's rule (truncation below 1e-22 relative, under FP64
-// rounding), a short dependent chain on the device's serial tail; larger
-// arguments use exp().  Host and device run the same code.
+// degree 8 (truncation below 1e-22 relative, under FP64 rounding) evaluated
+// by Estrin's scheme -- pairs of terms, then x^2, x^4, x^8 -- a dependent
+// depth of four multiply-adds on the device's serial tail instead of
+// Horner's nine; larger arguments use exp().  Host and device run the same
+// code.
 __host__ __device__ inline double nh_exp(double x) {
     if (fabs(x) >= 0.015625) return exp(x);
-    double p = 1.0 / 40320.0;
-    p = fma(p, x, 1.0 / 5040.0);
-    p = fma(p, x, 1.0 / 720.0);
-    p = fma(p, x, 1.0 / 120.0);
-    p = fma(p, x, 1.0 / 24.0);
-    p = fma(p, x, 1.0 / 6.0);
-    p = fma(p, x, 0.5);
-    p = fma(p, x, 1.0);
-    return fma(p, x, 1.0);
+    const double x2 = x * x;
+    const double x4 = x2 * x2;
+    const double b0 = 1.0 + x;
+    const double b1 = fma(x, 1.0 / 6.0, 0.5);
+    const double b2 = fma(x, 1.0 / 120.0, 1.0 / 24.0);
+    const double b3 = fma(x, 1.0 / 5040.0, 1.0 / 720.0);
+    const double c0 = fma(x2, b1, b0);
+    const double c1 = fma(x2, b3, b2);
+    const double d0 = fma(x4, c1, c0);
+    return fma(x4 * x4, 1.0 / 40320.0, d0);
 }
 
 // thermostatIntegrate (FixNoseHoover.cu:795-866), nTimesteps = n_ys = 1, for
@@ -322,6 +325,13 @@ __global__ void k_first_mol(const MolArgs a0, const MolArgs *__restrict__ tab) {
     const int4 ix = mol_sites(A, m);
     const int id3[3] = {ix.x, ix.y, ix.z};
     float4 x0[3], x[3], v[3];
+    // the M site's words read with the rest, not after the SETTLE
+    float vmw = 0.f, fmw = 0.f, xmw = 0.f;
+    if (rc.foursite) {
+        vmw = vs[ix.w].w;
+        fmw = fs[ix.w].w;
+        xmw = xs[ix.w].w;
+    }
     const float s = NH ? (float)chain[0].scale : 1.0f;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
@@ -344,11 +354,9 @@ __global__ void k_first_mol(const MolArgs a0, const MolArgs *__restrict__ tab) {
         vs[id3[k]] = v[k];
     }
     if (rc.foursite) {
-        const float4 vm = vs[ix.w];
-        const float4 fm = fs[ix.w];
-        vs[ix.w] = make_float4(0.f, 0.f, 0.f, vm.w);
-        fs[ix.w] = make_float4(0.f, 0.f, 0.f, fm.w);
-        xs[ix.w] = msite(rc, box, x, xs[ix.w].w);
+        vs[ix.w] = make_float4(0.f, 0.f, 0.f, vmw);
+        fs[ix.w] = make_float4(0.f, 0.f, 0.f, fmw);
+        xs[ix.w] = msite(rc, box, x, xmw);
     }
     // late trigger: the dependent's blocks become resident during this
     // grid's tail; their griddepcontrol.wait still waits for all of it
@@ -400,6 +408,25 @@ __device__ void finish_step(double *partials, int nparts, unsigned int *counter,
     __syncthreads();
     if (!last) return;
     __threadfence();
+    // thread 0 reads the chain into registers (a copy of the struct would
+    // sit in local memory on this serial path) while the partials are read
+    NHRegs c;
+    double mvv = 0.0;
+    if (threadIdx.x == 0 && nh) {
+        const NHChain &g = chain[0];
+#pragma unroll
+        for (int k = 0; k < kNHChain; k++) {
+            c.vel[k] = __ldcg(&g.vel[k]);
+            c.force[k] = __ldcg(&g.force[k]);
+            c.mass[k] = __ldcg(&g.mass[k]);
+            c.inv_mass[k] = __ldcg(&g.inv_mass[k]);
+        }
+        c.ndf = __ldcg(&g.ndf);
+        c.kB = __ldcg(&g.kB);
+        c.T = __ldcg(&g.T);
+        c.dt = __ldcg(&g.dt);
+        mvv = __ldcg(&g.mvv_to_eng);
+    }
     // every thread of the last block sums a fixed strided share of the
     // partials (L2 reads), then a fixed-order block reduction: deterministic
     __shared__ double red[32];
@@ -411,22 +438,8 @@ __device__ void finish_step(double *partials, int nparts, unsigned int *counter,
         *counter = 0u;
         if (ke_out) *ke_out = tot;
         if (nh) {
-            // the chain in registers (a copy of the struct would sit in local
-            // memory on this serial path); constants stay in chain[0/1]
-            NHRegs c;
-            const NHChain &g = chain[0];
-#pragma unroll
-            for (int k = 0; k < kNHChain; k++) {
-                c.vel[k] = g.vel[k];
-                c.force[k] = g.force[k];
-                c.mass[k] = g.mass[k];
-                c.inv_mass[k] = g.inv_mass[k];
-            }
-            c.ndf = g.ndf;
-            c.kB = g.kB;
-            c.T = g.T;
-            c.dt = g.dt;
-            c.ke = tot * g.mvv_to_eng;
+            // constants stay in chain[0/1]
+            c.ke = tot * mvv;
             const double last_ke = c.ke;
             const double sf1 = nh_integrate_n<kNHChain>(c, false);  // stepFinal
             store_chain(chain[1], c, last_ke, sf1);
