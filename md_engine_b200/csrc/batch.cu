@@ -66,8 +66,12 @@ void Batch::reset() {
         if (c->c2r) cufftDestroy(c->c2r);
     }
     fft.clear();
-    for (DBuf<char> *t : {&tab_pair, &tab_grid, &tab_build, &tab_p3m, &tab_e3b, &tab_first, &tab_second}) t->release();
+    for (DBuf<char> *t : {&tab_pair, &tab_grid, &tab_grid_ps, &tab_build, &tab_p3m, &tab_e3b, &tab_first,
+                          &tab_second, &tab_molgrid, &tab_molscan, &tab_pairmol})
+        t->release();
     max_n = max_mol = max_cell = 0;
+    ps.clear();
+    mfi.clear();
     max_nk = 0;
     prepared = false;
 }
@@ -158,22 +162,33 @@ int Batch::prepare() {
         }
         s->nThreadPerAtom = team;
     }
-    for (State *s : reps) {
-        if (s->prepared && !s->mf.on) continue;
-        // the batched kernels take the per-site form of every replica
-        s->pairForm = 1;
-        s->prepared = false;
-        if (int e = s->prepare()) return e;
-    }
+    // each replica in its own form: the molecule form where its box holds
+    // the molecule list's minimum image (pairForm 0 or 2), else the per-site
+    // form; a phase whose kernels differ by form launches once per form
+    for (State *s : reps)
+        if (!s->prepared)
+            if (int e = s->prepare()) return e;
     MDX_CUDA_TRY(cudaDeviceSynchronize());
     max_n = max_mol = max_cell = 0;
-    for (State *s : reps) {
+    ps.clear();
+    mfi.clear();
+    max_n_ps = max_cell_ps = max_mol_mf = 0;
+    for (int r = 0; r < (int)reps.size(); r++) {
+        State *s = reps[r];
         max_n = std::max(max_n, s->gpd.n);
         max_mol = std::max(max_mol, (int)s->rigidFix()->mol_ids.size());
         max_cell = std::max(max_cell, s->grid.ns.x * s->grid.ns.y * s->grid.ns.z);
-        if (s->grid.team != team) {
-            set_error(MDX_ERR_STATE, "replica built with team %d, batch uses %d", s->grid.team, team);
-            return MDX_ERR_STATE;
+        if (s->mf.on) {
+            mfi.push_back(r);
+            max_mol_mf = std::max(max_mol_mf, (int)s->rigidFix()->mol_ids.size());
+        } else {
+            ps.push_back(r);
+            max_n_ps = std::max(max_n_ps, s->gpd.n);
+            max_cell_ps = std::max(max_cell_ps, s->grid.ns.x * s->grid.ns.y * s->grid.ns.z);
+            if (s->grid.team != team) {
+                set_error(MDX_ERR_STATE, "replica built with team %d, batch uses %d", s->grid.team, team);
+                return MDX_ERR_STATE;
+            }
         }
     }
     periodicInterval = s0.periodicInterval > 0 ? s0.periodicInterval : 1;

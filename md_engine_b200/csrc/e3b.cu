@@ -188,6 +188,11 @@ struct E3BArgs {
     // 1: the molecule form -- molecule index = slot, sites at 4m .. 4m+3
     // (mol_idx holds that identity map; the hot passes skip reading it)
     int slots;
+    // the molecule form's list source: the molecule-pair list of the same
+    // rebuild (counts, entries in its team layout) and the sorted positions
+    const uint32_t *mf_counts, *mf_list;
+    int mf_cap, mf_team;
+    const float4 *mf_xs2;
 };
 
 __device__ __forceinline__ int4 e3b_sites(const E3BArgs &A, const int4 *__restrict__ mol_idx, int m) {
@@ -202,6 +207,7 @@ __device__ __forceinline__ int4 e3b_sites(const E3BArgs &A, const int4 *__restri
 template <int T>
 __global__ void k_e3b_list(const E3BArgs a0, const E3BArgs *__restrict__ tab, int conditional) {
     MDX_E3B_ARGS;
+    if (A.slots) return;  // a molecule-form replica: its list comes from k_e3b_list_mf
     DeviceStatus *st = A.st;
     const int nmol = A.nmol;
     const int4 *__restrict__ mol_ids = A.mol_ids;
@@ -275,11 +281,13 @@ __global__ void k_e3b_list(const E3BArgs a0, const E3BArgs *__restrict__ tab, in
 // E3B list radius.  The molecule-pair list holds every site-0 pair within its
 // larger radius, so the E3B set is the per-site path's.
 template <int T>
-__global__ void k_e3b_list_mf(const E3BArgs A, const uint32_t *__restrict__ pcounts,
-                              const uint32_t *__restrict__ plist, int pcap, int pteam,
-                              const int *__restrict__ mol_of_slot, const float4 *__restrict__ xs2) {
-    pdl_wait();
-    if (!A.st->rebuild) return;
+__global__ void k_e3b_list_mf(const E3BArgs a0, const E3BArgs *__restrict__ tab) {
+    MDX_E3B_ARGS;
+    if (!A.slots || !A.st->rebuild) return;
+    const uint32_t *__restrict__ pcounts = A.mf_counts;
+    const uint32_t *__restrict__ plist = A.mf_list;
+    const int pcap = A.mf_cap, pteam = A.mf_team;
+    const float4 *__restrict__ xs2 = A.mf_xs2;
     constexpr int G = 32 / T;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -738,6 +746,13 @@ static E3BArgs e3b_args(State &s, FixE3B &f, float4 *out) {
     A.ccounts = f.ccounts.p;
     A.clist = f.clist.p;
     A.slots = s.mf.on ? 1 : 0;
+    if (s.mf.on) {
+        A.mf_counts = s.mf.counts.p;
+        A.mf_list = s.mf.list.p;
+        A.mf_cap = s.mf.cap;
+        A.mf_team = s.mf.team;
+        A.mf_xs2 = s.gpd.xs_alt.p;
+    }
     return A;
 }
 
@@ -763,11 +778,9 @@ int e3b_build_list(State &s, FixE3B &f, bool conditional, cudaStream_t st) {
 int e3b_build_list_mf(State &s, FixE3B &f, cudaStream_t st) {
     const int nmol = (int)f.mol_ids.size();
     if (nmol == 0 || !f.prepared) return 0;
-    E3BArgs A = e3b_args(s, f, nullptr);
-    const MolForm &mf = s.mf;
+    const E3BArgs A = e3b_args(s, f, nullptr);
     MDX_CUDA_TRY(launch_pdl(k_e3b_list_mf<kMolTeam>, e3b_blocks(nmol), dim3(256), 0, st ? st : s.stream, A,
-                            (const uint32_t *)mf.counts.p, (const uint32_t *)mf.list.p, mf.cap, mf.team,
-                            (const int *)mf.perm.p, (const float4 *)s.gpd.xs_alt.p));
+                            (const E3BArgs *)nullptr));
     return 0;
 }
 
@@ -882,9 +895,17 @@ static int batch_e3b_sizing(Batch &b, E3BArgs *out) {
 int batch_e3b_list(Batch &b) {
     E3BArgs A;
     if (int e = batch_e3b_sizing(b, &A)) return e;
-    k_e3b_list<kMolTeam><<<e3b_blocks(b.max_mol, (unsigned)b.reps.size()), 256, 0, b.stream>>>(
-        A, reinterpret_cast<const E3BArgs *>(b.tab_e3b.p), 1);
-    MDX_LAUNCHED();
+    const E3BArgs *tab = reinterpret_cast<const E3BArgs *>(b.tab_e3b.p);
+    const dim3 grid = e3b_blocks(b.max_mol, (unsigned)b.reps.size());
+    // each kernel returns at once for the replicas of the other form
+    if (!b.ps.empty()) {
+        k_e3b_list<kMolTeam><<<grid, 256, 0, b.stream>>>(A, tab, 1);
+        MDX_LAUNCHED();
+    }
+    if (!b.mfi.empty()) {  // from each replica's molecule-pair list
+        k_e3b_list_mf<kMolTeam><<<grid, 256, 0, b.stream>>>(A, tab);
+        MDX_LAUNCHED();
+    }
     return 0;
 }
 

@@ -598,6 +598,14 @@ class Batch {
     int64_t turn = 0;
     // argument tables (device), one record per replica, built at prepare
     DBuf<char> tab_pair, tab_grid, tab_build, tab_p3m, tab_e3b, tab_first, tab_second;
+    // replicas by form: ps (per-site list) and mfi (molecule form); the pair
+    // kernel and the rebuild group launch once per form over that form's
+    // replicas (tab_grid: every replica, for the skin check; tab_grid_ps,
+    // tab_build, tab_pair: the per-site ones; tab_molgrid, tab_molscan,
+    // tab_pairmol: the molecule-form ones, in the order of ps / mfi)
+    std::vector<int> ps, mfi;
+    DBuf<char> tab_grid_ps, tab_molgrid, tab_molscan, tab_pairmol;
+    int max_n_ps = 0, max_cell_ps = 0, max_mol_mf = 0, max_mcell = 0;
     int pair_big = 0;
     int max_n = 0, max_mol = 0, max_cell = 0;
     size_t max_nk = 0;

@@ -268,7 +268,8 @@ __device__ __forceinline__ int4 mol_sites(const MolArgs &A, int m) {
 // rebuild-group kernel: molecule -> current atom indices (idToIdx after sort)
 __global__ void k_rigid_maps(const MolArgs a0, const MolArgs *__restrict__ tab, int conditional) {
     MDX_MOL_ARGS;
-    if (conditional && !A.st->rebuild) return;
+    // a molecule-form replica's sort rewrites its map itself
+    if (A.slots || (conditional && !A.st->rebuild)) return;
     int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= A.nmol) return;
     const int *__restrict__ idToIdx = A.idToIdx;
@@ -1114,6 +1115,7 @@ int batch_mol_tables(Batch &b) {
         State &s = *b.reps[r];
         FixRigid *fr = s.rigidFix();
         h1[r] = mol_args(s, *fr);
+        h1[r].slots = s.mf.on ? 1 : 0;
         h2[r] = h1[r];
         FixE3B *e3 = s.e3bFix();
         h2[r].fextra = (e3 && e3->side_ok) ? e3->f_side.p : nullptr;

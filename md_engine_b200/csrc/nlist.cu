@@ -684,6 +684,12 @@ struct MolGridArgs {
     float cut2;
 };
 
+// one system (m0) or, for batched replicas, tab[blockIdx.y] (m0 then only
+// sizes the grid; blocks past a smaller replica's work return at once)
+#define MDX_MG_ARGS \
+    pdl_wait();     \
+    const MolGridArgs M = tab ? tab[blockIdx.y] : m0
+
 __device__ __forceinline__ float4 wrap_pos(const Box &box, float4 p, bool &moved) {
     // periodicWrap (GridGPU.cu:138-161), per site
     const float ix = floorf((p.x - box.lo.x) / box.L.x);
@@ -701,8 +707,8 @@ __device__ __forceinline__ float4 wrap_pos(const Box &box, float4 p, bool &moved
 // site 0 wrapped into the box (periodicWrap's formula), the other sites put
 // at their minimum-image offset from it, so every molecule is stored whole
 // (as SETTLE leaves it after every step); the molecule binned by its site 0
-__global__ void k_mf_wrap_bin(const MolGridArgs M) {
-    pdl_wait();
+__global__ void k_mf_wrap_bin(const MolGridArgs m0, const MolGridArgs *__restrict__ tab) {
+    MDX_MG_ARGS;
     if (!M.st->rebuild) return;
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M.nmol) return;
@@ -724,8 +730,8 @@ __global__ void k_mf_wrap_bin(const MolGridArgs M) {
     atomicAdd(M.cell_count + c, 1u);
 }
 
-__global__ void k_mf_scatter(const MolGridArgs M) {
-    pdl_wait();
+__global__ void k_mf_scatter(const MolGridArgs m0, const MolGridArgs *__restrict__ tab) {
+    MDX_MG_ARGS;
     if (!M.st->rebuild) return;
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M.nmol) return;
@@ -735,8 +741,8 @@ __global__ void k_mf_scatter(const MolGridArgs M) {
 }
 
 // deterministic order inside each cell: by molecule index; one warp per cell
-__global__ void k_mf_rank(const MolGridArgs M) {
-    pdl_wait();
+__global__ void k_mf_rank(const MolGridArgs m0, const MolGridArgs *__restrict__ tab) {
+    MDX_MG_ARGS;
     if (!M.st->rebuild) return;
     const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -752,8 +758,8 @@ __global__ void k_mf_rank(const MolGridArgs M) {
 
 // slot d <- molecule perm[d]: its four sites into 4d .. 4d+3 of the
 // alternate streams and idToIdx rewritten; one thread per site
-__global__ void k_mf_gather(const MolGridArgs M) {
-    pdl_wait();
+__global__ void k_mf_gather(const MolGridArgs m0, const MolGridArgs *__restrict__ tab) {
+    MDX_MG_ARGS;
     if (!M.st->rebuild) return;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 4 * M.nmol) return;
@@ -771,8 +777,8 @@ __global__ void k_mf_gather(const MolGridArgs M) {
 
 // the sorted streams back into the primary buffers, the positions of this
 // build for the skin check, and the molecule maps (molecule perm[d] at slot d)
-__global__ void k_mf_copyback(const MolGridArgs M) {
-    pdl_wait();
+__global__ void k_mf_copyback(const MolGridArgs m0, const MolGridArgs *__restrict__ tab) {
+    MDX_MG_ARGS;
     if (!M.st->rebuild) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= 4 * M.nmol) return;
@@ -831,8 +837,9 @@ __device__ __forceinline__ void mf_row_runs(const MolGridArgs &M, int r, int cx,
     }
 }
 
-__global__ void __launch_bounds__(kMfBuildThreads) k_mf_build(const MolGridArgs M) {
-    pdl_wait();
+__global__ void __launch_bounds__(kMfBuildThreads) k_mf_build(const MolGridArgs m0,
+                                                               const MolGridArgs *__restrict__ tab) {
+    MDX_MG_ARGS;
     if (!M.st->rebuild) return;
     const int k = blockIdx.x;
     if (k >= M.nmol) return;  // block-uniform
@@ -1316,22 +1323,23 @@ static int nlist_rebuild_mf(State &s, bool force, cudaStream_t bstream) {
     const GridArgs Am = mol_scan_args(s);
     const MolGridArgs M = mol_grid_args(s);
     const GridArgs *nt = nullptr;
+    const MolGridArgs *mnt = nullptr;
     const int nb_atoms = (s.gpd.n + 255) / 256;
     const int nb_mol = (M.nmol + 255) / 256;
     MDX_CUDA_TRY(launch_pdl(k_check, dim3(nb_atoms), dim3(256), 0, s.stream, A, nt, force ? 1 : 0));
-    MDX_CUDA_TRY(launch_pdl(k_mf_wrap_bin, dim3(nb_mol), dim3(256), 0, s.stream, M));
+    MDX_CUDA_TRY(launch_pdl(k_mf_wrap_bin, dim3(nb_mol), dim3(256), 0, s.stream, M, mnt));
     MDX_CUDA_TRY(launch_pdl(k_scan_cells, dim3(1), dim3(kScanThreads), 0, s.stream, Am, nt));
-    MDX_CUDA_TRY(launch_pdl(k_mf_scatter, dim3(nb_mol), dim3(256), 0, s.stream, M));
-    MDX_CUDA_TRY(launch_pdl(k_mf_rank, dim3((M.ncell * 32 + 255) / 256), dim3(256), 0, s.stream, M));
-    MDX_CUDA_TRY(launch_pdl(k_mf_gather, dim3((4 * M.nmol + 255) / 256), dim3(256), 0, s.stream, M));
-    MDX_CUDA_TRY(launch_pdl(k_mf_copyback, dim3((4 * M.nmol + 255) / 256), dim3(256), 0, s.stream, M));
+    MDX_CUDA_TRY(launch_pdl(k_mf_scatter, dim3(nb_mol), dim3(256), 0, s.stream, M, mnt));
+    MDX_CUDA_TRY(launch_pdl(k_mf_rank, dim3((M.ncell * 32 + 255) / 256), dim3(256), 0, s.stream, M, mnt));
+    MDX_CUDA_TRY(launch_pdl(k_mf_gather, dim3((4 * M.nmol + 255) / 256), dim3(256), 0, s.stream, M, mnt));
+    MDX_CUDA_TRY(launch_pdl(k_mf_copyback, dim3((4 * M.nmol + 255) / 256), dim3(256), 0, s.stream, M, mnt));
     cudaStream_t bs = s.stream;
     if (bstream) {
         MDX_CUDA_TRY(cudaEventRecord(s.ev_sorted, s.stream));
         MDX_CUDA_TRY(cudaStreamWaitEvent(bstream, s.ev_sorted, 0));
         bs = bstream;
     }
-    MDX_CUDA_TRY(launch_pdl(k_mf_build, dim3(M.nmol), dim3(kMfBuildThreads), 0, bs, M));
+    MDX_CUDA_TRY(launch_pdl(k_mf_build, dim3(M.nmol), dim3(kMfBuildThreads), 0, bs, M, mnt));
     if (FixE3B *e3 = s.e3bFix()) {
         if (int e = e3b_build_list_mf(s, *e3, bs)) return e;
     }
@@ -1565,30 +1573,102 @@ int nlist_box_changed(State &s) {
 }
 
 // batched replicas: the same group, one launch per kernel for all replicas
-// (blockIdx.y = replica); every kernel returns at once for a replica whose
-// skin check did not fire.  Tables are built at prepare, before any capture.
+// of a form (blockIdx.y = replica of that form); every kernel returns at once
+// for a replica whose skin check did not fire.  Tables are built at prepare,
+// before any capture.
 int batch_nlist_tables(Batch &b) {
     const int R = (int)b.reps.size();
     std::vector<GridArgs> hg(R);
-    std::vector<BuildArgs> hb(R);
-    for (int r = 0; r < R; r++) {
-        State &s = *b.reps[r];
-        hg[r] = grid_args(s);
-        hb[r] = build_args(s, make_grid(s), s.grid.cut * s.grid.cut);
-        // one list-build kernel serves the batch: its exclusion and
-        // front/back split forms are compile-time, so they must agree
-        if ((hb[r].use_excl != 0) != (hb[0].use_excl != 0) ||
-            (hb[r].ljmask != nullptr) != (hb[0].ljmask != nullptr)) {
-            set_error(MDX_ERR_UNSUPPORTED,
-                      "batched replicas must agree on exclusions and on the interacting-pair split (replica %d)", r);
-            return MDX_ERR_UNSUPPORTED;
-        }
-    }
+    for (int r = 0; r < R; r++) hg[r] = grid_args(*b.reps[r]);
     if (int e = b.tab_grid.alloc(R * sizeof(GridArgs))) return e;
-    if (int e = b.tab_build.alloc(R * sizeof(BuildArgs))) return e;
     MDX_CUDA_TRY(cudaMemcpy(b.tab_grid.p, hg.data(), R * sizeof(GridArgs), cudaMemcpyHostToDevice));
-    MDX_CUDA_TRY(cudaMemcpy(b.tab_build.p, hb.data(), R * sizeof(BuildArgs), cudaMemcpyHostToDevice));
+    const int P = (int)b.ps.size();
+    if (P) {
+        std::vector<GridArgs> hp(P);
+        std::vector<BuildArgs> hb(P);
+        for (int q = 0; q < P; q++) {
+            State &s = *b.reps[b.ps[q]];
+            hp[q] = hg[b.ps[q]];
+            hb[q] = build_args(s, make_grid(s), s.grid.cut * s.grid.cut);
+            // one list-build kernel serves the batch: its exclusion and
+            // front/back split forms are compile-time, so they must agree
+            if ((hb[q].use_excl != 0) != (hb[0].use_excl != 0) ||
+                (hb[q].ljmask != nullptr) != (hb[0].ljmask != nullptr)) {
+                set_error(MDX_ERR_UNSUPPORTED,
+                          "batched replicas must agree on exclusions and on the interacting-pair split (replica %d)",
+                          b.ps[q]);
+                return MDX_ERR_UNSUPPORTED;
+            }
+        }
+        if (int e = b.tab_grid_ps.alloc(P * sizeof(GridArgs))) return e;
+        if (int e = b.tab_build.alloc(P * sizeof(BuildArgs))) return e;
+        MDX_CUDA_TRY(cudaMemcpy(b.tab_grid_ps.p, hp.data(), P * sizeof(GridArgs), cudaMemcpyHostToDevice));
+        MDX_CUDA_TRY(cudaMemcpy(b.tab_build.p, hb.data(), P * sizeof(BuildArgs), cudaMemcpyHostToDevice));
+    }
+    const int Q = (int)b.mfi.size();
+    if (Q) {
+        std::vector<MolGridArgs> hm(Q);
+        std::vector<GridArgs> hs(Q);
+        b.max_mcell = 0;
+        for (int q = 0; q < Q; q++) {
+            State &s = *b.reps[b.mfi[q]];
+            hm[q] = mol_grid_args(s);
+            hs[q] = mol_scan_args(s);
+            b.max_mcell = std::max(b.max_mcell, hs[q].ncell);
+        }
+        if (int e = b.tab_molgrid.alloc(Q * sizeof(MolGridArgs))) return e;
+        if (int e = b.tab_molscan.alloc(Q * sizeof(GridArgs))) return e;
+        MDX_CUDA_TRY(cudaMemcpy(b.tab_molgrid.p, hm.data(), Q * sizeof(MolGridArgs), cudaMemcpyHostToDevice));
+        MDX_CUDA_TRY(cudaMemcpy(b.tab_molscan.p, hs.data(), Q * sizeof(GridArgs), cudaMemcpyHostToDevice));
+    }
     return 0;
+}
+
+// the per-site replicas' sort and list build (nlist_rebuild's kernels)
+static void batch_rebuild_sites(Batch &b, cudaStream_t st) {
+    const int P = (int)b.ps.size();
+    const GridArgs *tg = reinterpret_cast<const GridArgs *>(b.tab_grid_ps.p);
+    const BuildArgs *tb = reinterpret_cast<const BuildArgs *>(b.tab_build.p);
+    State &s0 = *b.reps[b.ps[0]];
+    GridArgs A = grid_args(s0);  // sizing only: the kernels read tab
+    A.n = b.max_n_ps;
+    A.ncell = b.max_cell_ps;
+    BuildArgs B = build_args(s0, make_grid(s0), s0.grid.cut * s0.grid.cut);
+    B.ncell = b.max_cell_ps;
+    const dim3 nb((b.max_n_ps + 255) / 256, P);
+    k_wrap_bin<<<nb, 256, 0, st>>>(A, tg);
+    k_scan_cells<<<dim3(1, P), kScanThreads, 0, st>>>(A, tg);
+    k_scatter<<<nb, 256, 0, st>>>(A, tg);
+    k_rank<<<dim3((b.max_cell_ps * 32 + 255) / 256, P), 256, 0, st>>>(A, tg);
+    k_gather<<<nb, 256, 0, st>>>(A, tg);
+    k_copyback<<<nb, 256, 0, st>>>(A, tg);
+    int hg = 2;
+    for (int r : b.ps) hg = std::max(hg, b.reps[r]->grid.home_group);
+    launch_build_any<false>(s0.grid.team, hg, build_grid(b.max_cell_ps, P), st, B, tb);
+    g_launches += 6;
+}
+
+// the molecule-form replicas' sort by molecule and molecule-pair list
+// (nlist_rebuild_mf's kernels)
+static void batch_rebuild_mols(Batch &b, cudaStream_t st) {
+    const int Q = (int)b.mfi.size();
+    const GridArgs *ts = reinterpret_cast<const GridArgs *>(b.tab_molscan.p);
+    const MolGridArgs *tm = reinterpret_cast<const MolGridArgs *>(b.tab_molgrid.p);
+    State &s0 = *b.reps[b.mfi[0]];
+    GridArgs Am = mol_scan_args(s0);  // sizing only: the kernels read the tables
+    Am.ncell = b.max_mcell;
+    MolGridArgs M = mol_grid_args(s0);
+    M.nmol = b.max_mol_mf;
+    M.ncell = b.max_mcell;
+    const int nb_mol = (b.max_mol_mf + 255) / 256, nb_site = (4 * b.max_mol_mf + 255) / 256;
+    k_mf_wrap_bin<<<dim3(nb_mol, Q), 256, 0, st>>>(M, tm);
+    k_scan_cells<<<dim3(1, Q), kScanThreads, 0, st>>>(Am, ts);
+    k_mf_scatter<<<dim3(nb_mol, Q), 256, 0, st>>>(M, tm);
+    k_mf_rank<<<dim3((b.max_mcell * 32 + 255) / 256, Q), 256, 0, st>>>(M, tm);
+    k_mf_gather<<<dim3(nb_site, Q), 256, 0, st>>>(M, tm);
+    k_mf_copyback<<<dim3(nb_site, Q), 256, 0, st>>>(M, tm);
+    k_mf_build<<<dim3(b.max_mol_mf, Q), kMfBuildThreads, 0, st>>>(M, tm);
+    g_launches += 7;
 }
 
 int batch_nlist_rebuild(Batch &b) {
@@ -1598,31 +1678,32 @@ int batch_nlist_rebuild(Batch &b) {
         return MDX_ERR_STATE;
     }
     const GridArgs *tg = reinterpret_cast<const GridArgs *>(b.tab_grid.p);
-    const BuildArgs *tb = reinterpret_cast<const BuildArgs *>(b.tab_build.p);
     State &s0 = *b.reps[0];
-    GridArgs A = grid_args(s0);  // sizing only: the kernels read tab
+    GridArgs A = grid_args(s0);  // sizing only
     A.n = b.max_n;
-    A.ncell = b.max_cell;
-    BuildArgs B = build_args(s0, make_grid(s0), s0.grid.cut * s0.grid.cut);
-    B.ncell = b.max_cell;
-    const dim3 nb((b.max_n + 255) / 256, R);
     cudaStream_t st = b.stream;
-    k_check<<<nb, 256, 0, st>>>(A, tg, 0);
-    k_wrap_bin<<<nb, 256, 0, st>>>(A, tg);
-    k_scan_cells<<<dim3(1, R), kScanThreads, 0, st>>>(A, tg);
-    k_scatter<<<nb, 256, 0, st>>>(A, tg);
-    k_rank<<<dim3((b.max_cell * 32 + 255) / 256, R), 256, 0, st>>>(A, tg);
-    k_gather<<<nb, 256, 0, st>>>(A, tg);
-    k_copyback<<<nb, 256, 0, st>>>(A, tg);
-    int hg = 2;
-    for (State *r : b.reps) hg = std::max(hg, r->grid.home_group);
-    launch_build_any<false>(s0.grid.team, hg, build_grid(b.max_cell, R), st, B, tb);
-    g_launches += 7;
-    if (int e = batch_rigid_maps(b)) return e;
+    k_check<<<dim3((b.max_n + 255) / 256, R), 256, 0, st>>>(A, tg, 0);
+    MDX_LAUNCHED();
+    if (!b.ps.empty()) batch_rebuild_sites(b, st);
+    if (!b.mfi.empty()) batch_rebuild_mols(b, st);
+    // the per-site replicas' molecule maps (the molecule form's copyback
+    // rewrote its own)
+    if (!b.ps.empty())
+        if (int e = batch_rigid_maps(b)) return e;
     if (s0.e3bFix())
         if (int e = batch_e3b_list(b)) return e;
-    k_finish<<<dim3(1, R), 1024, 0, st>>>(A, tg);
-    MDX_LAUNCHED();
+    if (!b.ps.empty()) {
+        GridArgs Ap = A;
+        Ap.n = b.max_n_ps;
+        k_finish<<<dim3(1, (unsigned)b.ps.size()), 1024, 0, st>>>(Ap, reinterpret_cast<const GridArgs *>(b.tab_grid_ps.p));
+        MDX_LAUNCHED();
+    }
+    if (!b.mfi.empty()) {
+        GridArgs Am = mol_scan_args(*b.reps[b.mfi[0]]);
+        Am.ncell = b.max_mcell;
+        k_finish<<<dim3(1, (unsigned)b.mfi.size()), 1024, 0, st>>>(Am, reinterpret_cast<const GridArgs *>(b.tab_molscan.p));
+        MDX_LAUNCHED();
+    }
     MDX_CUDA_TRY(cudaGetLastError());
     return 0;
 }

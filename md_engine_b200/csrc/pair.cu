@@ -263,9 +263,13 @@ __device__ __forceinline__ void mol_pair_eval(const MolPairArgs &A, const float3
 // within the far cutoff queue up in shared memory, and each full batch of
 // 32 has its four sites staged into shared memory by cp.async while the
 // warp scans the next chunk, then is evaluated one entry per lane.
-template <int LJ, bool EW, bool VIR, bool ENERGY, int TOPO>
-__global__ void __launch_bounds__(kMolPairBlock, 14) k_pair_mol(const MolPairArgs A, int accumulate) {
+// BATCH: batched replicas, the arguments of replica blockIdx.y from tab
+// (a0 unused); otherwise a0
+template <int LJ, bool EW, bool VIR, bool ENERGY, int TOPO, bool BATCH = false>
+__global__ void __launch_bounds__(kMolPairBlock, 14) k_pair_mol(const MolPairArgs a0,
+                                                                const MolPairArgs *__restrict__ tab, int accumulate) {
     pdl_wait();
+    const MolPairArgs &A = BATCH ? tab[blockIdx.y] : a0;
     __shared__ int q_j[kMolPairBlock / 32][kMolQueue];
     __shared__ float4 q_s[kMolPairBlock / 32][kMolQueue];
     __shared__ float4 s_b[kMolPairBlock / 32][4][32];  // staged batch: site b of entry lane
@@ -479,14 +483,15 @@ void mol_launch_t(const MolPairArgs &A, int virialMode, bool energy, bool accumu
     int nb = (A.nmol * 32 + kMolPairBlock - 1) / kMolPairBlock;
     if (max_blocks > 0 && nb > max_blocks) nb = max_blocks;
     const dim3 blocks(nb > 0 ? nb : 1);
+    const MolPairArgs *nt = nullptr;
     if (energy) {
-        k_pair_mol<LJ, EW, false, true, TOPO><<<blocks, kMolPairBlock, 0, st>>>(A, 0);
+        k_pair_mol<LJ, EW, false, true, TOPO><<<blocks, kMolPairBlock, 0, st>>>(A, nt, 0);
         MDX_LAUNCHED();
     } else if (virialMode == 1 || virialMode == 2) {
-        k_pair_mol<LJ, EW, true, false, TOPO><<<blocks, kMolPairBlock, 0, st>>>(A, accumulate ? 1 : 0);
+        k_pair_mol<LJ, EW, true, false, TOPO><<<blocks, kMolPairBlock, 0, st>>>(A, nt, accumulate ? 1 : 0);
         MDX_LAUNCHED();
     } else {
-        launch_pdl(k_pair_mol<LJ, EW, false, false, TOPO>, blocks, dim3(kMolPairBlock), 0, st, A,
+        launch_pdl(k_pair_mol<LJ, EW, false, false, TOPO>, blocks, dim3(kMolPairBlock), 0, st, A, nt,
                    accumulate ? 1 : 0);
     }
 }
@@ -552,28 +557,88 @@ int pair_energy(State &s, FixPair &f, double *out) {
     return float_sum(s, s.e_site.p, A.n, out);
 }
 
-// batched replicas: one launch, blockIdx.y = replica; tables built at prepare
+// batched replicas: one launch per form, blockIdx.y = replica of that form;
+// tables built at prepare
 int batch_pair_tables(Batch &b) {
-    const int R = (int)b.reps.size();
-    std::vector<PairArgs> h(R);
-    for (int r = 0; r < R; r++) h[r] = make_args(*b.reps[r], *b.reps[r]->pairFix());
-    if (int e = b.tab_pair.alloc(R * sizeof(PairArgs))) return e;
-    MDX_CUDA_TRY(cudaMemcpy(b.tab_pair.p, h.data(), R * sizeof(PairArgs), cudaMemcpyHostToDevice));
-    b.pair_big = b.biggest_rep();
+    const int P = (int)b.ps.size(), Q = (int)b.mfi.size();
+    if (P) {
+        std::vector<PairArgs> h(P);
+        b.pair_big = b.ps[0];
+        for (int q = 0; q < P; q++) {
+            State &s = *b.reps[b.ps[q]];
+            h[q] = make_args(s, *s.pairFix());
+            if (s.gpd.n > b.reps[b.pair_big]->gpd.n) b.pair_big = b.ps[q];
+        }
+        if (int e = b.tab_pair.alloc(P * sizeof(PairArgs))) return e;
+        MDX_CUDA_TRY(cudaMemcpy(b.tab_pair.p, h.data(), P * sizeof(PairArgs), cudaMemcpyHostToDevice));
+    }
+    if (Q) {
+        // one kernel instance serves these replicas: their force fields
+        // must give the same compile-time pattern
+        std::vector<MolPairArgs> hm(Q);
+        const FixPair &f0 = *b.reps[b.mfi[0]]->pairFix();
+        for (int q = 0; q < Q; q++) {
+            State &s = *b.reps[b.mfi[q]];
+            const FixPair &f = *s.pairFix();
+            hm[q] = make_mol_args(s, *s.pairFix());
+            hm[q].energy = nullptr;
+            if (hm[q].ljm != hm[0].ljm || hm[q].qm != hm[0].qm || f.lj_kind != f0.lj_kind ||
+                (f.chargeFix != nullptr) != (f0.chargeFix != nullptr)) {
+                set_error(MDX_ERR_UNSUPPORTED, "batched replicas must share one pair style and site pattern (replica %d)",
+                          b.mfi[q]);
+                return MDX_ERR_UNSUPPORTED;
+            }
+        }
+        if (int e = b.tab_pairmol.alloc(Q * sizeof(MolPairArgs))) return e;
+        MDX_CUDA_TRY(cudaMemcpy(b.tab_pairmol.p, hm.data(), Q * sizeof(MolPairArgs), cudaMemcpyHostToDevice));
+    }
+    return 0;
+}
+
+// the molecule-form replicas: one warp per molecule slot, the grid (slots
+// of the largest of them, replicas) with blocks past a smaller replica's
+// slots idle
+template <int LJ, bool EW, int TOPO>
+static void batch_mol_launch_t(const MolPairArgs &A, const MolPairArgs *tab, int Q, cudaStream_t st) {
+    const int nb = (A.nmol * 32 + kMolPairBlock - 1) / kMolPairBlock;
+    k_pair_mol<LJ, EW, false, false, TOPO, true><<<dim3(nb > 0 ? nb : 1, Q), kMolPairBlock, 0, st>>>(A, tab, 0);
+    MDX_LAUNCHED();
+}
+
+static int batch_pair_mol_launch(Batch &b, cudaStream_t stream) {
+    const int Q = (int)b.mfi.size();
+    State &s0 = *b.reps[b.mfi[0]];
+    FixPair &f = *s0.pairFix();
+    MolPairArgs A = make_mol_args(s0, f);  // sizing and pattern only: the kernel reads tab
+    A.nmol = b.max_mol_mf;
+    const MolPairArgs *tab = reinterpret_cast<const MolPairArgs *>(b.tab_pairmol.p);
+    const bool ew = f.chargeFix != nullptr;
+    const bool water4 = ew && A.ljm == 0x1u && A.qm == 0xEEE0u;
+    if (f.lj_kind == 1 && water4) batch_mol_launch_t<1, true, 1>(A, tab, Q, stream);
+    else if (f.lj_kind == 1 && ew) batch_mol_launch_t<1, true, 0>(A, tab, Q, stream);
+    else if (f.lj_kind == 1) batch_mol_launch_t<1, false, 0>(A, tab, Q, stream);
+    else if (water4) batch_mol_launch_t<2, true, 1>(A, tab, Q, stream);
+    else if (ew) batch_mol_launch_t<2, true, 0>(A, tab, Q, stream);
+    else batch_mol_launch_t<2, false, 0>(A, tab, Q, stream);
     return 0;
 }
 
 int batch_pair_launch(Batch &b, cudaStream_t stream) {
-    const int R = (int)b.reps.size();
-    if (!b.tab_pair.p) {
+    if ((!b.ps.empty() && !b.tab_pair.p) || (!b.mfi.empty() && !b.tab_pairmol.p)) {
         set_error(MDX_ERR_STATE, "batch tables not built (prepare the batch)");
         return MDX_ERR_STATE;
     }
-    State &big = *b.reps[b.pair_big];
-    FixPair &f = *big.pairFix();
-    const PairArgs A = make_args(big, f);
-    return launch_any(A, big.grid.team, f.lj_kind, charge_kind(f), false, false, true, stream,
-                      reinterpret_cast<const PairArgs *>(b.tab_pair.p), R);
+    if (!b.ps.empty()) {
+        State &big = *b.reps[b.pair_big];
+        FixPair &f = *big.pairFix();
+        const PairArgs A = make_args(big, f);
+        if (int e = launch_any(A, big.grid.team, f.lj_kind, charge_kind(f), false, false, true, stream,
+                               reinterpret_cast<const PairArgs *>(b.tab_pair.p), (int)b.ps.size()))
+            return e;
+    }
+    if (!b.mfi.empty())
+        if (int e = batch_pair_mol_launch(b, stream)) return e;
+    return 0;
 }
 
 int pair_force_raw(int n, const float4 *xs, float4 *fs, const float *qs, const uint32_t *counts,

@@ -22,10 +22,20 @@ def _replica(nmol, T, seed, e3b=False):
     return st, fixes
 
 
-def _trajectories(spec, nsteps, e3b=False):
+def _trajectories(spec, nsteps, e3b=False, form=0):
     batch_states = [_replica(m, T, seed, e3b)[0] for m, T, seed in spec]
+    if form:
+        for st in batch_states:
+            st.pairForm = form
     b = BatchReplicas(batch_states)
     b.prepare()
+    forms = [int(st.pairForm) for st in batch_states]
+    if form == 1:
+        assert forms == [1] * len(spec)
+    else:
+        # each replica in its own form: the molecule form where its box holds
+        # the molecule list's minimum image, the per-site form below that
+        assert 1 in forms and 2 in forms, forms
     b.run(nsteps)
     xb = [st.getAtoms()[0] for st in batch_states]
     singles = []
@@ -36,15 +46,19 @@ def _trajectories(spec, nsteps, e3b=False):
     return xb, singles, batch_states
 
 
+@pytest.mark.parametrize("form", [0, 1])
 @pytest.mark.parametrize("e3b", [False, True])
-def test_batch_matches_single_runs(e3b):
-    spec = [(256, 265.0, 11), (311, 300.0, 12), (420, 350.0, 13)]
-    xb, xs, states = _trajectories(spec, 25, e3b=e3b)
+def test_batch_matches_single_runs(e3b, form):
+    # form 0: a mixed batch (the 256-molecule box too small for the molecule
+    # form, the others in it); form 1: every replica per-site
+    spec = [(256, 265.0, 11), (520, 300.0, 12), (700, 350.0, 13)] if form == 0 else \
+        [(256, 265.0, 11), (311, 300.0, 12), (420, 350.0, 13)]
+    xb, xs, states = _trajectories(spec, 25, e3b=e3b, form=form)
     for (m, T, seed), a, b in zip(spec, xb, xs):
         assert a.shape == (4 * m, 3)
-        # positions compared by minimum image (the batch keeps the per-site
-        # form, the single run the molecule form: they store periodic images
-        # of some sites differently between rebuilds)
+        # positions compared by minimum image (in the per-site form the
+        # batch stores periodic images of some sites differently from the
+        # single run's molecule form between rebuilds)
         L = systems.water_tip4p2005(nmol=m, T=T, seed=seed).L
         d = a - b
         d -= L * np.rint(d / L)
