@@ -67,7 +67,7 @@ void Batch::reset() {
     }
     fft.clear();
     for (DBuf<char> *t : {&tab_pair, &tab_grid, &tab_grid_ps, &tab_build, &tab_p3m, &tab_e3b, &tab_first,
-                          &tab_second, &tab_molgrid, &tab_molscan, &tab_pairmol})
+                          &tab_second, &tab_molgrid, &tab_molscan, &tab_pairmol, &tab_p3m_mol})
         t->release();
     max_n = max_mol = max_cell = 0;
     ps.clear();
@@ -225,6 +225,8 @@ int Batch::step() {
     MDX_CUDA_TRY(cudaEventRecord(ev_fork, stream));
     MDX_CUDA_TRY(cudaStreamWaitEvent(side[0], ev_fork, 0));
     if (int e = batch_p3m_spread_solve(*this, side[0])) return e;
+    if (p3m_mol)  // the gather on the P3M branch, beside the pair kernel
+        if (int e = batch_p3m_gather(*this, side[0])) return e;
     MDX_CUDA_TRY(cudaEventRecord(ev_join[0], side[0]));
     if (e3b) {
         MDX_CUDA_TRY(cudaStreamWaitEvent(side[1], ev_fork, 0));
@@ -233,7 +235,8 @@ int Batch::step() {
     }
     if (int e = batch_pair_launch(*this, stream)) return e;
     MDX_CUDA_TRY(cudaStreamWaitEvent(stream, ev_join[0], 0));
-    if (int e = batch_p3m_gather(*this, stream)) return e;
+    if (!p3m_mol)
+        if (int e = batch_p3m_gather(*this, stream)) return e;
     if (e3b) MDX_CUDA_TRY(cudaStreamWaitEvent(stream, ev_join[1], 0));
     return batch_second_half(*this, e3b);
 }

@@ -624,6 +624,11 @@ class Batch {
         DBuf<char> tab;
     };
     bool p3m_own = false;  // every class on the own FFT: the gather reads the float4 fields
+    // and every replica's molecules fit the molecule form of spread and
+    // gather: spread and gather by molecule, the gather on the P3M branch
+    // into each replica's per-step reciprocal buffer
+    bool p3m_mol = false;
+    DBuf<char> tab_p3m_mol;
     std::vector<std::unique_ptr<FFTClass>> fft;
     std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
     std::map<std::pair<int, int>, uint64_t> graph_kernels;

@@ -155,8 +155,9 @@ __device__ __forceinline__ int mol_site(int4 ix, int k, int four_site) {
 // the molecule form: lanes 15 j .. 15 j + 14 of a warp take the three
 // charged sites (five planes each) of one molecule, two molecules per warp,
 // the two W = nmol/2 apart; no lane is spent on an uncharged oxygen
-__global__ void k_spread_mol(const P3MArgs A) {
+__global__ void k_spread_mol(const P3MArgs a0, const P3MArgs *__restrict__ tab) {
     pdl_wait();
+    MDX_P3M_ARGS;
     const int lane = threadIdx.x & 31;
     const int W = (A.nmol + 1) / 2;
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -681,8 +682,10 @@ __global__ void k_gather4_tab(const P3MArgs a0, const P3MArgs *__restrict__ tab)
 // the molecule form of the gather into a per-step buffer (STORE): the
 // mapping of k_spread_mol, each charged site's force stored, the uncharged
 // oxygen of a four-site molecule stored as zero
-__global__ void k_gather_mol(const P3MArgs A, const float4 *__restrict__ e4) {
+__global__ void k_gather_mol(const P3MArgs a0, const P3MArgs *__restrict__ tab, const float4 *__restrict__ e4_one) {
     pdl_wait();
+    MDX_P3M_ARGS;
+    const float4 *__restrict__ e4 = tab ? A.e4 : e4_one;  // batched: each replica's own field
     const int lane = threadIdx.x & 31;
     const int t = lane % 5, base = lane - t;
     const int W = (A.nmol + 1) / 2;
@@ -1015,7 +1018,8 @@ int FixChargeEwald::spread_mol(cudaStream_t st, const FixRigid &r) {
     const int warps = (A.nmol + 1) / 2;
     // two-warp blocks: they slot in beside the pair kernel's (measured +1 % per
     // water step against 256-thread blocks)
-    MDX_CUDA_TRY(launch_pdl_prio(true, k_spread_mol, dim3((warps + 1) / 2), dim3(64), 0, st, A));
+    MDX_CUDA_TRY(launch_pdl_prio(true, k_spread_mol, dim3((warps + 1) / 2), dim3(64), 0, st, A,
+                                 (const P3MArgs *)nullptr));
     return 0;
 }
 
@@ -1025,7 +1029,7 @@ int FixChargeEwald::gather_mol_to(float4 *out, cudaStream_t st, const FixRigid &
     A.fs = out;
     const int warps = (A.nmol + 1) / 2;
     MDX_CUDA_TRY(launch_pdl_prio(true, k_gather_mol, dim3((warps + 1) / 2), dim3(64), 0, st, A,
-                                 (const float4 *)e4.p));
+                                 (const P3MArgs *)nullptr, (const float4 *)e4.p));
     return 0;
 }
 
@@ -1139,6 +1143,20 @@ int batch_p3m_prepare(Batch &b) {
     for (int r = 0; r < R; r++) h[r] = p3m_args(*b.reps[r], *b.reps[r]->ewaldFix());
     if (int e = b.tab_p3m.alloc(R * sizeof(P3MArgs))) return e;
     MDX_CUDA_TRY(cudaMemcpy(b.tab_p3m.p, h.data(), R * sizeof(P3MArgs), cudaMemcpyHostToDevice));
+    // the molecule form of spread and gather, as the single system's fused
+    // step: the charged sites of each molecule only, the reciprocal forces
+    // stored into each replica's per-step buffer by the P3M branch itself
+    b.p3m_mol = b.p3m_own;
+    for (State *s : b.reps) b.p3m_mol = b.p3m_mol && s->ewaldFix()->mol_form_ok(*s->rigidFix());
+    if (b.p3m_mol) {
+        for (int r = 0; r < R; r++) {
+            State &s = *b.reps[r];
+            h[r] = mol_args(s, *s.ewaldFix(), *s.rigidFix());
+            h[r].fs = s.ewaldFix()->f_recip.p;
+        }
+        if (int e = b.tab_p3m_mol.alloc(R * sizeof(P3MArgs))) return e;
+        MDX_CUDA_TRY(cudaMemcpy(b.tab_p3m_mol.p, h.data(), R * sizeof(P3MArgs), cudaMemcpyHostToDevice));
+    }
     return 0;
 }
 
@@ -1149,7 +1167,12 @@ int batch_p3m_spread_solve(Batch &b, cudaStream_t st) {
     A.n = b.max_n;
     A.nk = b.max_nk;
     for (auto &c : b.fft) MDX_CUDA_TRY(cudaMemsetAsync(c->rho.p, 0, c->rho.n * sizeof(float), st));
-    k_spread5<<<dim3((A.n + 47) / 48, R), 256, 0, st>>>(A, tab);
+    if (b.p3m_mol) {
+        const int warps = (b.max_mol + 1) / 2;
+        k_spread_mol<<<dim3((warps + 1) / 2, R), 64, 0, st>>>(A, reinterpret_cast<const P3MArgs *>(b.tab_p3m_mol.p));
+    } else {
+        k_spread5<<<dim3((A.n + 47) / 48, R), 256, 0, st>>>(A, tab);
+    }
     MDX_LAUNCHED();
     if (b.p3m_own) {
         // each mesh class: R2C + E(k) + 3 C2R as the single system's three
@@ -1197,6 +1220,13 @@ int batch_p3m_gather(Batch &b, cudaStream_t st) {
     const P3MArgs *tab = reinterpret_cast<const P3MArgs *>(b.tab_p3m.p);
     P3MArgs A = p3m_args(*b.reps[0], *b.reps[0]->ewaldFix());
     A.n = b.max_n;
+    if (b.p3m_mol) {  // into each replica's per-step buffer (the second half adds it)
+        const int warps = (b.max_mol + 1) / 2;
+        k_gather_mol<<<dim3((warps + 1) / 2, (unsigned)b.reps.size()), 64, 0, st>>>(
+            A, reinterpret_cast<const P3MArgs *>(b.tab_p3m_mol.p), (const float4 *)nullptr);
+        MDX_LAUNCHED();
+        return 0;
+    }
     if (b.p3m_own) {
         k_gather4_tab<true><<<dim3((A.n + 47) / 48, (unsigned)b.reps.size()), 256, 0, st>>>(A, tab);
         MDX_LAUNCHED();

@@ -1116,6 +1116,8 @@ int batch_mol_tables(Batch &b) {
         FixRigid *fr = s.rigidFix();
         h1[r] = mol_args(s, *fr);
         h1[r].slots = s.mf.on ? 1 : 0;
+        // the P3M branch's per-step reciprocal forces (molecule-form gather)
+        h1[r].frecip = b.p3m_mol ? s.ewaldFix()->f_recip.p : nullptr;
         h2[r] = h1[r];
         FixE3B *e3 = s.e3bFix();
         h2[r].fextra = (e3 && e3->side_ok) ? e3->f_side.p : nullptr;
