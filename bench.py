@@ -508,6 +508,10 @@ def main():
     it = IntegratorVerlet(st)
     # warm-up: prepare, capture graphs, settle clocks (untimed)
     it.run(max(args.warmup, 3))
+    # the run-start tuning of the molecule form's pair grid (Integrator::tune's
+    # role); a no-op for the per-site form.  Untimed, state untouched.
+    tuned_cap, tuned_ms = it.autotune()
+    it.run(3)
     K = args.steps
     P = 10
     barrier(dist, dev)
@@ -586,7 +590,9 @@ def main():
                     f"relaxed {args.eq_steps} untimed steps at the target temperature)",
             "config": dict(cfg, l2="flushed between timed 10-step chunks (256 MiB write)",
                            start=f"equilibrated: {args.eq_steps} steps, tight Nose-Hoover, before warm-up",
-                           parallelism="replicas only" if world > 1 else "single system"),
+                           parallelism="replicas only" if world > 1 else "single system",
+                           pair_grid_autotuned={"blocks_per_sm": tuned_cap, "ms_per_force_phase": tuned_ms}
+                           if tuned_cap else "per-site form: no grid shape tuned"),
             "ns_per_day": ns_day,
             "temperature_end_of_timed_region": t_end,
             "e2e": {"value": e2e, "unit": "timesteps/s",

@@ -183,6 +183,17 @@ int mdx_integrator_run_host(mdx_integrator *it, int num_turns, const double *pos
  * events on the library stream and preceded, outside the timed window, by a
  * flush_bytes device write that evicts L2.  *device_ms = summed chunk time. */
 int mdx_integrator_run_timed(mdx_integrator *it, int num_turns, int chunk, size_t flush_bytes, double *device_ms);
+/* Integrator::tune (src/Integrators/Integrator.cu:272-376), which times the
+ * force kernels for each NTPB x NTPA at the start of a run and keeps the
+ * fastest: here the shape is the molecule-form pair grid's blocks per SM
+ * (caps: candidates, -1 = uncapped, 0 = the built-in default), timed on the
+ * force phase of the fused step (the pair kernel beside the P3M chain and
+ * E3B), `reps` phases per timing; the fastest is kept as the state's
+ * pairBlocksPerSM and returned with its ms per phase.  Positions and
+ * velocities are untouched.  Systems without that shape: *best_cap = 0,
+ * *best_ms = 0, nothing timed. */
+int mdx_integrator_autotune(mdx_integrator *it, int reps, const int *caps, int ncaps, int *best_cap,
+                            double *best_ms);
 /* Benchmark support (no reference counterpart): average device time of one
  * launch of a hot-path stage over `iters` launches, L2 flushed between them.
  * stage 0 pair forces, 1 P3M reciprocal (spread+FFT+field+gather), 2 E3B,

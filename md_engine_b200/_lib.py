@@ -76,6 +76,7 @@ SIGNATURES = [
     ("mdx_integrator_destroy", c_int, [c_void_p]),
     ("mdx_integrator_run_host", c_int, [c_void_p, c_int, P(c_dbl), P(c_dbl), P(c_dbl), P(c_dbl), P(c_dbl)]),
     ("mdx_integrator_run_timed", c_int, [c_void_p, c_int, c_int, ctypes.c_size_t, P(c_dbl)]),
+    ("mdx_integrator_autotune", c_int, [c_void_p, c_int, P(c_int), c_int, P(c_int), P(c_dbl)]),
     ("mdx_time_stage", c_int, [c_void_p, c_int, c_int, ctypes.c_size_t, P(c_dbl)]),
     ("mdx_prepare", c_int, [c_void_p]),
     ("mdx_nlist_build", c_int, [c_void_p, c_int]),

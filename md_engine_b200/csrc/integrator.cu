@@ -121,6 +121,107 @@ class IntegratorVerlet {
         if (e3side) MDX_CUDA_TRY(cudaStreamWaitEvent(s->stream, s->ev_join[1], 0));
         return step_second_half(*s, true, e3side ? e3->f_side.p : nullptr, recip_side ? ew->f_recip.p : nullptr);
     }
+    // the force phase of the fused step alone (fork, the pair kernel beside
+    // the P3M chain and E3B, join): what the pair grid's cap trades off
+    int forcePhase() {
+        FixPair *pf = s->pairFix();
+        FixChargeEwald *ew = s->ewaldFix();
+        FixE3B *e3 = s->e3bFix();
+        FixRigid &r = *s->rigidFix();
+        MDX_CUDA_TRY(cudaEventRecord(s->ev_fork, s->stream));
+        MDX_CUDA_TRY(cudaStreamWaitEvent(s->side[0], s->ev_fork, 0));
+        if (int e = ew->spread_mol(s->side[0], r)) return e;
+        if (int e = ew->solve(s->side[0])) return e;
+        if (int e = ew->gather_mol_to(ew->f_recip.p, s->side[0], r)) return e;
+        MDX_CUDA_TRY(cudaEventRecord(s->ev_join[0], s->side[0]));
+        if (e3) {
+            MDX_CUDA_TRY(cudaStreamWaitEvent(s->side[1], s->ev_fork, 0));
+            if (int e = e3b_forces_to(*s, *e3, e3->f_side.p, true, s->side[1])) return e;
+            MDX_CUDA_TRY(cudaEventRecord(s->ev_join[1], s->side[1]));
+        }
+        if (int e = pair_launch(*s, *pf, 0, false)) return e;
+        MDX_CUDA_TRY(cudaStreamWaitEvent(s->stream, s->ev_join[0], 0));
+        if (e3) MDX_CUDA_TRY(cudaStreamWaitEvent(s->stream, s->ev_join[1], 0));
+        return 0;
+    }
+
+    // Integrator::tune (Integrator.cu:272-376) times the force kernels for
+    // each NTPB x NTPA at the start of a run and keeps the fastest.  Here, for
+    // the molecule form of all-rigid water with P3M (and E3B) beside the pair
+    // kernel, the tuned shape is the pair grid's blocks per SM: each
+    // candidate's force phase is captured as a graph of `reps` repetitions
+    // and timed by CUDA events (median of three launches); the fastest is
+    // kept in State::pairBlocksPerSM (-1: uncapped).  Positions and
+    // velocities are not touched, the force array is saved and put back.
+    // Other systems have no such shape: best = 0, nothing is timed.
+    int autotunePairGrid(int reps, const int *caps, int ncaps, int *best, double *best_ms) {
+        *best = 0;
+        *best_ms = 0.0;
+        if (!s->prepared) {
+            clearGraphs();
+            if (int e = s->prepare()) return e;
+        }
+        FixChargeEwald *ew = s->ewaldFix();
+        FixE3B *e3 = s->e3bFix();
+        const bool ok = s->pairFix() && ew && s->mf.on && s->rigidFix() && !has_free_atoms(*s) &&
+                        ew->mol_form_ok(*s->rigidFix()) && (!e3 || e3->side_ok) &&
+                        !(e3 && e3->sur && e3->sur->enabled);
+        if (!ok || reps <= 0 || ncaps <= 0) return 0;
+        const int n = s->gpd.n;
+        DBuf<float4> fsave;
+        if (int e = fsave.alloc(n)) return e;
+        MDX_CUDA_TRY(cudaMemcpyAsync(fsave.p, s->gpd.fs.p, n * sizeof(float4), cudaMemcpyDeviceToDevice, s->stream));
+        const int keep = s->pairBlocksPerSM;
+        cudaEvent_t a, b;
+        MDX_CUDA_TRY(cudaEventCreate(&a));
+        MDX_CUDA_TRY(cudaEventCreate(&b));
+        double best_t = 0.0;
+        int best_c = keep;
+        for (int k = 0; k < ncaps; k++) {
+            s->pairBlocksPerSM = caps[k];
+            cudaGraph_t g;
+            MDX_CUDA_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+            const uint64_t before = g_launches;
+            int e = 0;
+            for (int r = 0; r < reps && !e; r++) e = forcePhase();
+            g_launches = before;
+            cudaError_t ce = cudaStreamEndCapture(s->stream, &g);
+            if (e) return e;
+            if (ce != cudaSuccess) {
+                set_error(MDX_ERR_CUDA, "autotune capture failed: %s", cudaGetErrorString(ce));
+                return MDX_ERR_CUDA;
+            }
+            cudaGraphExec_t ex;
+            MDX_CUDA_TRY(cudaGraphInstantiate(&ex, g, cudaGraphInstantiateFlagUseNodePriority));
+            cudaGraphDestroy(g);
+            MDX_CUDA_TRY(cudaGraphLaunch(ex, s->stream));  // warm
+            float t[3];
+            for (int q = 0; q < 3; q++) {
+                MDX_CUDA_TRY(cudaEventRecord(a, s->stream));
+                MDX_CUDA_TRY(cudaGraphLaunch(ex, s->stream));
+                MDX_CUDA_TRY(cudaEventRecord(b, s->stream));
+                MDX_CUDA_TRY(cudaEventSynchronize(b));
+                MDX_CUDA_TRY(cudaEventElapsedTime(&t[q], a, b));
+            }
+            cudaGraphExecDestroy(ex);
+            std::sort(t, t + 3);
+            const double ms = (double)t[1] / reps;
+            if (k == 0 || ms < best_t) {
+                best_t = ms;
+                best_c = caps[k];
+            }
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        MDX_CUDA_TRY(cudaMemcpyAsync(s->gpd.fs.p, fsave.p, n * sizeof(float4), cudaMemcpyDeviceToDevice, s->stream));
+        MDX_CUDA_TRY(cudaStreamSynchronize(s->stream));
+        s->pairBlocksPerSM = best_c;
+        clearGraphs();  // the step graphs take the chosen shape
+        *best = best_c;
+        *best_ms = best_t;
+        return s->checkStatus();
+    }
+
     int stepBody() {
         if (mode == 0) return stepFused();
         if (int e = step_first_half(*s, false)) return e;
@@ -467,6 +568,25 @@ int mdx_integrator_run(mdx_integrator *it, int num_turns, double *ptsps_out) {
         return it->it->run(num_turns, ptsps_out);
     } catch (...) {
         set_error(MDX_ERR_STATE, "exception in run");
+        return MDX_ERR_STATE;
+    }
+}
+
+int mdx_integrator_autotune(mdx_integrator *it, int reps, const int *caps, int ncaps, int *best_cap,
+                            double *best_ms) {
+    if (!it || !caps || !best_cap || !best_ms || reps <= 0 || ncaps <= 0) {
+        set_error(MDX_ERR_ARG, "bad argument");
+        return MDX_ERR_ARG;
+    }
+    for (int k = 0; k < ncaps; k++)
+        if (caps[k] < -1 || caps[k] > 32) {
+            set_error(MDX_ERR_ARG, "pair grid caps are -1 (uncapped) or 0..32 blocks per SM (got %d)", caps[k]);
+            return MDX_ERR_ARG;
+        }
+    try {
+        return it->it->autotunePairGrid(reps, caps, ncaps, best_cap, best_ms);
+    } catch (...) {
+        set_error(MDX_ERR_STATE, "exception in autotune");
         return MDX_ERR_STATE;
     }
 }

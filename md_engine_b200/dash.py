@@ -780,6 +780,16 @@ class IntegratorVerlet:
         check(lib().mdx_integrator_run_timed(self._h, int(numTurns), int(chunk), int(flushBytes), ctypes.byref(out)))
         return out.value
 
+    def autotune(self, reps=10, caps=(6, 8, 10, 12, 14, -1)):
+        """Integrator::tune's role (Integrator.cu:272-376) for the molecule
+        form of all-rigid water: the pair grid's blocks per SM timed against
+        the P3M chain and E3B beside it; the fastest is kept on the state.
+        (best cap, ms per force phase); (0, 0.0) where there is no such shape."""
+        arr = (c_int * len(caps))(*caps)
+        best, ms = c_int(), c_dbl()
+        check(lib().mdx_integrator_autotune(self._h, int(reps), arr, len(caps), ctypes.byref(best), ctypes.byref(ms)))
+        return best.value, ms.value
+
     # stage-level halves
     def firstHalf(self):
         check(lib().mdx_verlet_first_half(self.state._h))

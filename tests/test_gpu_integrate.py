@@ -229,3 +229,36 @@ def test_water_nve_energy_conservation():
 def _total_energy_real(st):
     mv2, _ = st.kinetic()
     return 0.5 * mv2 * systems.MVV_TO_ENG_REAL + float(np.sum(st.potentialEnergy()))
+
+
+def test_autotune_keeps_the_state_and_the_trajectory():
+    """IntegratorVerlet.autotune (Integrator::tune's role): the molecule
+    form's pair grid cap is timed on the force phase alone; positions,
+    velocities and forces are left as they were, the chosen cap is kept on
+    the state, and the run that follows equals a run with that cap set by
+    hand (to the float-atomic order of the P3M spread)"""
+    from md_engine_b200 import IntegratorVerlet
+    sysd = systems.water_tip4p2005(nside=10, seed=5)
+    a, _ = systems.build_water_state(sysd, rcut=9.0, skin=1.0, grid=32)
+    b, _ = systems.build_water_state(sysd, rcut=9.0, skin=1.0, grid=32)
+    ia, ib = IntegratorVerlet(a), IntegratorVerlet(b)
+    ia.run(5)
+    ib.run(5)
+    x0, v0, f0 = a.getAtoms()
+    cap, ms = ia.autotune(reps=4, caps=(4, 10, -1))
+    assert cap in (4, 10, -1) and ms > 0
+    assert int(a.pairBlocksPerSM) == cap
+    x1, v1, f1 = a.getAtoms()
+    assert np.array_equal(x0, x1) and np.array_equal(v0, v1) and np.array_equal(f0, f1)
+    b.pairBlocksPerSM = cap
+    ia.run(20)
+    ib.run(20)
+    xa, _, _ = a.getAtoms()
+    xb, _, _ = b.getAtoms()
+    d = xa - xb
+    d -= sysd.L * np.rint(d / sysd.L)
+    assert np.abs(d).max() < 1e-4
+    # the per-site form has no such shape
+    lj = systems.lj_fcc(ncell=6, seed=3)
+    st, _ = systems.build_lj_state(lj, rcut=2.5, skin=0.3)
+    assert IntegratorVerlet(st).autotune(reps=2) == (0, 0.0)
