@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--train-iters", type=int, default=4000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-nve", action="store_true", help="skip the NVE energy-drift measurement")
+    ap.add_argument("--batch-eq-steps", type=int, default=BATCH_EQ_STEPS,
+                    help="batched: untimed relaxation of the replicas' seeded starts (0: the lattice starts)")
     ap.add_argument("--eq-steps", type=int, default=EQ_STEPS,
                     help="untimed relaxation steps of the seeded start before the warm-up")
     return ap.parse_args()
@@ -322,23 +324,49 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line))
 
 
-def batched_states(nrep, seed, e3b=True, subset=None):
+BATCH_EQ_STEPS = 2000  # untimed relaxation of the replicas' seeded starts
+
+
+def _replica_state(sysd, T, e3b, tau):
+    from md_engine_b200 import systems
+    st, _ = systems.build_water_state(sysd, rcut=9.0, skin=0.8, dt=2.0, interval=10,
+                                      grid=systems.p3m_mesh_for(sysd.L[0]), e3b=e3b, T=float(T), tau=tau)
+    st.nThreadPerAtom = 8
+    return st
+
+
+def batched_systems(nrep, seed, e3b=True, subset=None, eq_steps=BATCH_EQ_STEPS):
     """the batched-replica workload: nrep TIP4P/2005(+E3B3) boxes, molecule
     counts log-uniform in [256, 2048], T uniform in [260, 360] K, rc 9 A,
-    skin 0.8 A, P3M mesh 32^3 or 64^3 by box size; subset: build only these
-    replica indices (each replica is seeded by its index, whoever builds it)"""
-    from md_engine_b200 import systems
+    skin 0.8 A, P3M mesh 32^3 or 64^3 by box size; subset: only these replica
+    indices (each replica is seeded by its index, whoever builds it).  As the
+    single-system workloads, every seeded lattice start is relaxed first
+    (eq_steps batched steps with a tight Nose-Hoover coupling, tau 25 fs, at
+    the replica's temperature), so that the timed steps run liquid water at
+    the replicas' temperatures rather than a lattice melting.  Returns
+    [(system, T, molecules)]."""
+    import dataclasses
+    from md_engine_b200 import BatchReplicas, systems
     sizes, temps = systems.water_replica_sizes(nrep, seed=seed)
+    raw = [(systems.water_tip4p2005(nmol=int(m), T=float(T), seed=seed + 1000 + r), float(T), int(m))
+           for r, (m, T) in enumerate(zip(sizes, temps)) if subset is None or r in subset]
+    if eq_steps <= 0:
+        return raw
+    states = [_replica_state(sysd, T, e3b, 25.0) for sysd, T, _ in raw]
+    b = BatchReplicas(states)
+    b.prepare()
+    b.run(eq_steps)
     out = []
-    for r, (m, T) in enumerate(zip(sizes, temps)):
-        if subset is not None and r not in subset:
-            continue
-        sysd = systems.water_tip4p2005(nmol=int(m), T=float(T), seed=seed + 1000 + r)
-        st, _ = systems.build_water_state(sysd, rcut=9.0, skin=0.8, dt=2.0, interval=10,
-                                          grid=systems.p3m_mesh_for(sysd.L[0]), e3b=e3b, T=float(T), tau=100.0)
-        st.nThreadPerAtom = 8
-        out.append((st, int(m)))
+    for (sysd, T, m), st in zip(raw, states):
+        x, v, _ = st.getAtoms()
+        out.append((dataclasses.replace(sysd, pos=np.asarray(x, np.float64), vel=np.asarray(v, np.float64)), T, m))
+    del b
     return out
+
+
+def batched_states(systems_, e3b=True):
+    """the timed replicas: states (tau 100 fs) from batched_systems' output"""
+    return [(_replica_state(sysd, T, e3b, 100.0), m) for sysd, T, m in systems_]
 
 
 def side_line(args, world, value, unit, K, ms_max, cfg, extra, clk, launches):
@@ -367,7 +395,8 @@ def run_batched(args, rank, world, local):
     total = args.replicas * world
     sizes, _ = systems.water_replica_sizes(total, seed=seed)
     mine = shard_by_sites([4 * int(m) for m in sizes], world)[rank]
-    reps = batched_states(total, seed, subset=set(mine))
+    eq = batched_systems(total, seed, subset=set(mine), eq_steps=args.batch_eq_steps)
+    reps = batched_states(eq)
     states = [s for s, _ in reps]
     mols = sum(m for _, m in reps)
     b = BatchReplicas(states)
@@ -393,7 +422,7 @@ def run_batched(args, rank, world, local):
     # the plain path: every replica alone (fresh copies), same step count
     seq_ms = 0.0
     Ks = min(K, 50)
-    for st, _ in batched_states(total, seed, subset=set(mine)):
+    for st, _ in batched_states(eq):
         it = IntegratorVerlet(st)
         it.run(3)
         seq_ms += it.runTimed(Ks, 10, 0)
@@ -401,6 +430,8 @@ def run_batched(args, rank, world, local):
     if rank == 0:
         cfg = {"workload": f"{total} TIP4P/2005+E3B3 replicas ({args.replicas} per GPU), sizes log-uniform "
                            "256-2048 molecules, T 260-360 K, rc 9 A, skin 0.8 A, P3M 32^3/64^3",
+               "start": (f"equilibrated: {args.batch_eq_steps} batched steps, tight Nose-Hoover, before warm-up"
+                         if args.batch_eq_steps > 0 else "seeded lattice starts"),
                "replicas": total, "replicas_rank0": R, "molecules_rank0": mols, "autotuned_team": team,
                "l2": "flushed between timed 10-step chunks (256 MiB write)",
                "parallelism": f"replicas dealt to {world} GPUs by site count" if world > 1 else "one batch"}
