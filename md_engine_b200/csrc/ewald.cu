@@ -444,6 +444,42 @@ __device__ __forceinline__ void warp_fft(float2 (&v)[R], int lane, const LaneTw 
 template <int R>
 __device__ __forceinline__ int fft_out_index(int k1, int lane) { return k1 + R * brev5(lane); }
 
+// Inverse transform of a line held the way warp_fft leaves its output (lane
+// l holds Y[k1 + R bitrev5(l)] in v[k1]): radix-2 decimation in time across
+// the lanes (stages h = 1 .. 16, twiddle W_2h^(lane mod h) conjugated, on
+// the bit-reversed positions), then for R = 2 the in-lane step y[l] = z0 +
+// W_N^-l z1, y[l + 32] = z0 - W_N^-l z1.  Lane l then holds y[32 r + l] in
+// v[r]: natural order, no permutation through shared memory.  Unnormalised.
+template <int R>
+__device__ __forceinline__ void warp_ifft_dit(float2 (&v)[R], int lane, const LaneTw &T) {
+#pragma unroll
+    for (int k1 = 0; k1 < R; k1++) {
+#pragma unroll
+        for (int s = 4; s >= 0; s--) {
+            const int h = 16 >> s;
+            const float px = __shfl_xor_sync(0xffffffffu, v[k1].x, h);
+            const float py = __shfl_xor_sync(0xffffffffu, v[k1].y, h);
+            float2 w = T.st[s];
+            w.y = -w.y;
+            if ((lane & h) == 0) {
+                const float2 t = cmul(make_float2(px, py), w);
+                v[k1] = make_float2(v[k1].x + t.x, v[k1].y + t.y);
+            } else {
+                const float2 t = cmul(v[k1], w);
+                v[k1] = make_float2(px - t.x, py - t.y);
+            }
+        }
+    }
+    if (R == 2) {
+        float2 w = T.wn;
+        w.y = -w.y;
+        const float2 z0 = v[0];
+        const float2 t = cmul(v[R - 1], w);
+        v[0] = make_float2(z0.x + t.x, z0.y + t.y);
+        v[R - 1] = make_float2(z0.x - t.x, z0.y - t.y);
+    }
+}
+
 // plane kernels: kFftPlaneWarps warps per block, fixed at compile time so a
 // warp's line loop has a constant trip count and, for the small meshes,
 // unrolls (the lines' loads are in flight together)
@@ -492,9 +528,8 @@ __global__ void __launch_bounds__(256) k_fft_xe(const FFTArgs a0, const FFTArgs 
     constexpr int N = 32 * R, NH = N / 2 + 1;
     pdl_wait();
     const FFTArgs A = tab ? tab[blockIdx.y] : a0;
-    __shared__ float2 sline[8][N];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int line_id = blockIdx.x * (blockDim.x >> 5) + w;  // at most 8 warps per block (sline)
+    const int line_id = blockIdx.x * (blockDim.x >> 5) + w;
     if (line_id >= N * NH) return;  // warp-uniform; no block barrier below
     const LaneTw T = lane_twiddles<R>(lane, A.tw);
     const int ky = line_id / NH, kz = line_id % NH;
@@ -520,19 +555,17 @@ __global__ void __launch_bounds__(256) k_fft_xe(const FFTArgs a0, const FFTArgs 
         e[1][k1] = make_float2(-gy * q.y, gy * q.x);
         e[2][k1] = make_float2(-gz * q.y, gz * q.x);
     }
+    // the inverse x transforms take the forward's bit-reversed layout as it
+    // stands and leave natural order
 #pragma unroll
     for (int d = 0; d < 3; d++) {
-#pragma unroll
-        for (int k1 = 0; k1 < R; k1++) sline[w][fft_out_index<R>(k1, lane)] = e[d][k1];
-        __syncwarp();
         float2 u[R];
 #pragma unroll
-        for (int r = 0; r < R; r++) u[r] = sline[w][32 * r + lane];
-        __syncwarp();
-        warp_fft<R, true>(u, lane, T);
+        for (int k1 = 0; k1 < R; k1++) u[k1] = e[d][k1];
+        warp_ifft_dit<R>(u, lane, T);
         float2 *out = A.mid2 + (size_t)d * N * stride;
 #pragma unroll
-        for (int k1 = 0; k1 < R; k1++) out[fft_out_index<R>(k1, lane) * stride + base] = u[k1];
+        for (int r = 0; r < R; r++) out[(32 * r + lane) * stride + base] = u[r];
     }
 }
 
@@ -564,10 +597,13 @@ __global__ void __launch_bounds__(kFftPlaneWarps * 32) k_ifft_yz(const FFTArgs a
 #pragma unroll UNR
     for (int y = w; y < N; y += nw) {
         const float2 *row = plane + y * NH;
+        // the Hermitian half spectrum read in the bit-reversed order the
+        // decimation-in-time inverse takes; the line comes out in natural
+        // order (consecutive lanes, consecutive points)
         float2 v[R];
 #pragma unroll
-        for (int r = 0; r < R; r++) {
-            const int n = 32 * r + lane;
+        for (int k1 = 0; k1 < R; k1++) {
+            const int n = fft_out_index<R>(k1, lane);
             float2 X;
             if (n == 0 || n == N / 2) {
                 X = make_float2(row[n].x, 0.f);
@@ -577,12 +613,12 @@ __global__ void __launch_bounds__(kFftPlaneWarps * 32) k_ifft_yz(const FFTArgs a
                 const float2 c = row[N - n];
                 X = make_float2(c.x, -c.y);
             }
-            v[r] = X;
+            v[k1] = X;
         }
-        warp_fft<R, true>(v, lane, T);
+        warp_ifft_dit<R>(v, lane, T);
         const size_t base = ((size_t)x * N + y) * N;
 #pragma unroll
-        for (int k1 = 0; k1 < R; k1++) e[4 * (base + fft_out_index<R>(k1, lane))] = v[k1].x;
+        for (int r = 0; r < R; r++) e[4 * (base + 32 * r + lane)] = v[r].x;
     }
 }
 
