@@ -380,7 +380,7 @@ P3MArgs p3m_args(State &s, FixChargeEwald &f) {
 struct FFTArgs {
     int n;                   // points per side (32 or 64)
     const float *rho;        // [n][n][n]
-    float2 *mid1;            // [n][n][n/2+1]: after the z and y passes
+    float2 *mid1;            // [n][n/2+1][n] (x, kz, ky): after the z and y passes
     float2 *mid2;            // [3][n][n][n/2+1]: E_d after the inverse x pass
     float4 *e4;              // [n][n][n]
     const float *green;      // [n][n][n/2+1]
@@ -518,7 +518,7 @@ __global__ void __launch_bounds__(kFftPlaneWarps * 32) k_fft_zy(const FFTArgs a0
 #pragma unroll
         for (int k1 = 0; k1 < R; k1++) {
             const int ky = fft_out_index<R>(k1, lane);
-            A.mid1[((size_t)x * N + ky) * NH + kz] = v[k1];
+            A.mid1[((size_t)x * NH + kz) * N + ky] = v[k1];  // a column's 64 ky in one 512-byte row
         }
     }
 }
@@ -537,7 +537,7 @@ __global__ void __launch_bounds__(256) k_fft_xe(const FFTArgs a0, const FFTArgs 
     const size_t base = (size_t)ky * NH + kz;
     float2 v[R];
 #pragma unroll
-    for (int r = 0; r < R; r++) v[r] = A.mid1[(32 * r + lane) * stride + base];
+    for (int r = 0; r < R; r++) v[r] = A.mid1[(32 * r + lane) * stride + (size_t)kz * N + ky];
     warp_fft<R, false>(v, lane, T);
     const float kyv = A.tpl.y * (float)(ky > N / 2 ? ky - N : ky);
     const float kzv = A.tpl.z * (float)kz;
