@@ -381,7 +381,7 @@ struct FFTArgs {
     int n;                   // points per side (32 or 64)
     const float *rho;        // [n][n][n]
     float2 *mid1;            // [n][n/2+1][n] (x, kz, ky): after the z and y passes
-    float2 *mid2;            // [3][n][n][n/2+1]: E_d after the inverse x pass
+    float2 *mid2;            // [3][n][n/2+1][n] (d, x, kz, ky): E_d after the inverse x pass
     float4 *e4;              // [n][n][n]
     const float *green;      // [n][n][n/2+1]
     const float2 *tw;        // W_32^k (32) then W_64^k (64), forward sign
@@ -565,7 +565,7 @@ __global__ void __launch_bounds__(256) k_fft_xe(const FFTArgs a0, const FFTArgs 
         warp_ifft_dit<R>(u, lane, T);
         float2 *out = A.mid2 + (size_t)d * N * stride;
 #pragma unroll
-        for (int r = 0; r < R; r++) out[(32 * r + lane) * stride + base] = u[r];
+        for (int r = 0; r < R; r++) out[(32 * r + lane) * stride + (size_t)kz * N + ky] = u[r];
     }
 }
 
@@ -587,7 +587,7 @@ __global__ void __launch_bounds__(kFftPlaneWarps * 32) k_ifft_yz(const FFTArgs a
     for (int kz = w; kz < NH; kz += nw) {
         float2 v[R];
 #pragma unroll
-        for (int r = 0; r < R; r++) v[r] = src0[(size_t)(32 * r + lane) * NH + kz];
+        for (int r = 0; r < R; r++) v[r] = src0[(size_t)kz * N + 32 * r + lane];  // one contiguous ky row
         warp_fft<R, true>(v, lane, T);
 #pragma unroll
         for (int k1 = 0; k1 < R; k1++) plane[fft_out_index<R>(k1, lane) * NH + kz] = v[k1];
