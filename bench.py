@@ -652,8 +652,9 @@ def main():
                 line["nve_drift"] = {"value": None, "error": str(ex)}
         if world == 1 and not args.no_cpu_baseline:
             # the CPU baseline leg: the oracle's FP64 step timed on the host
-            # cores, and the same FP64 evaluation as the judge of the timed
-            # state's forces, energies and virial (outside the timed region)
+            # cores, and the same FP64 evaluation as the reference values of
+            # the timed state's forces, energies and virial (outside the
+            # timed region)
             try:
                 from oracle import cpu_step
                 res = cpu_step.time_steps(sysd, args.workload, nsample=10, warmup=2, repeats=3)
