@@ -10,7 +10,14 @@ barostatVelocityIntegrate :868-943, scaleVelocitiesBarostat :945-1015,
 rescaleVolume :1017-1032; Mod::scaleSystem about the box centre, Mod.cu:
 201-240), LJ units (boltz = mvv_to_eng = nktv_to_press = ftm_to_v = 1).
 Forces, virials and the cell list are the oracle's (oracle.py), on a list
-rebuilt every step (the box moves every step)."""
+rebuilt every step (the box moves every step).
+
+Parity unpinned: the reference holds no test, golden vector or fixture for
+its barostat, and FixNoseHoover.cu (with DataComputerPressure and
+DataComputerTemperature behind it) is not compiled here, so this
+restatement is checked only against the library's own MTK step (and, for
+the physics, by an LJ fluid reaching its set pressure at the density this
+propagator gives)."""
 from __future__ import annotations
 
 import math
