@@ -12,12 +12,18 @@ rescaleVolume :1017-1032; Mod::scaleSystem about the box centre, Mod.cu:
 Forces, virials and the cell list are the oracle's (oracle.py), on a list
 rebuilt every step (the box moves every step).
 
-Parity unpinned: the reference holds no test, golden vector or fixture for
-its barostat, and FixNoseHoover.cu (with DataComputerPressure and
-DataComputerTemperature behind it) is not compiled here, so this
-restatement is checked only against the library's own MTK step (and, for
-the physics, by an LJ fluid reaching its set pressure at the density this
-propagator gives)."""
+Parity: the barostat propagators (masses, thermal masses, the barostat
+chain, the cell-velocity kick) are pinned against the reference's own
+FixNoseHoover.cu compiled from source on the CPU (oracle/ref_nh_harness.cu
+-> oracle/_ref/librefnh.so; fixture tests/golden/ref_barostat.json): with
+barostat_velocity(ref_float=True) and a float time step this restatement
+reproduces the reference bit for bit; in FP64 (the library's precision) it
+differs only by the reference's float rounding of the pressure, the cell
+kick, the volume and the time step.  The step's hook order, the particle
+scaling factors and the volume rescale remain a restatement checked against
+the library's MTK step (their kernels and the pressure computer are not run
+by the harness), and, for the physics, by an LJ fluid reaching its set
+pressure at the density this propagator gives."""
 from __future__ import annotations
 
 import math
@@ -77,18 +83,21 @@ class MTKLJ:
     def barostat_masses(self):
         kt = self.T
         for i in range(3):
-            self.pmass[i] = (self.ndf + 3.0) * kt / self.pfreq ** 2
+            self.pmass[i] = (self.ndf + 3.0) * kt / (self.pfreq * self.pfreq)
 
     def barostat_thermal_masses(self):
         kt = self.T
         self.ptm[0] = 3.0 * 4.0 * kt / (2.0 * self.pfreq)
         for i in range(1, self.pc):
-            self.ptm[i] = kt / self.pfreq ** 2
+            self.ptm[i] = kt / (self.pfreq * self.pfreq)
         for i in range(1, self.pc):
-            self.ptf[i] = (self.ptm[i - 1] * self.ptv[i - 1] ** 2 - kt) / self.ptm[i]
+            self.ptf[i] = (self.ptm[i - 1] * self.ptv[i - 1] * self.ptv[i - 1] - kt) / self.ptm[i]
 
     def ke_barostat(self):
-        return sum(self.pmass[i] * self.pvel[i] ** 2 for i in range(3))
+        ke = 0.0
+        for i in range(3):
+            ke += self.pmass[i] * self.pvel[i] * self.pvel[i]
+        return ke
 
     def barostat_thermostat(self, step_init):
         kt, n = self.T, self.pc
@@ -112,15 +121,28 @@ class MTKLJ:
         for k in range(1, n - 1):
             pf = math.exp(-t8 * v[k + 1])
             v[k] *= pf
-            F[k] = (M[k - 1] * v[k - 1] ** 2 - kt) / M[k]
+            F[k] = (M[k - 1] * v[k - 1] * v[k - 1] - kt) / M[k]
             v[k] += t4 * F[k]
             v[k] *= pf
-        F[n - 1] = (M[n - 2] * v[n - 2] ** 2 - kt) / M[n - 1]
+        F[n - 1] = (M[n - 2] * v[n - 2] * v[n - 2] - kt) / M[n - 1]
         v[n - 1] += t4 * F[n - 1]
 
-    def barostat_velocity(self, ke, p):
+    def barostat_velocity(self, ke, p, ref_float=False):
+        """the cell-velocity kick in FP64; with ref_float, in the reference's
+        own precision: its pressure tensor and the kick G are Virials of
+        floats (Virial.h:10), the volume the float product of the float box
+        lengths (BoundsGPU.h:110-112), the time step a float (State.h:117)"""
         tcur = ke / self.ndf
         alpha = tcur * self.ndf / (self.n * 3.0)
+        if ref_float:
+            f32 = np.float32
+            V = float(f32(f32(self.L[0]) * f32(self.L[1])) * f32(self.L[2]))
+            pf, dt = float(f32(p)), f32(self.dt)
+            for i in range(3):
+                G = f32(alpha / self.pmass[i])
+                G = f32(float(G) + (pf - self.P) * V / self.pmass[i])
+                self.pvel[i] += float(G * dt) * 0.5
+            return
         for i in range(3):
             G = alpha / self.pmass[i] + (p - self.P) * self.volume() / self.pmass[i]
             self.pvel[i] += G * self.dt * 0.5

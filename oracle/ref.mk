@@ -1,7 +1,9 @@
 # Compiles the reference's own kernels (from the reference sources in place)
 # plus oracle/ref_harness.cu, oracle/ref_grid_harness.cu and
 # oracle/ref_rigid_harness.cu into
-# oracle/_ref/librefkernels.so.  Test infrastructure only; run where the
+# oracle/_ref/librefkernels.so, and the reference's host-side MTK barostat
+# propagator (FixNoseHoover.cu) with oracle/ref_nh_harness.cu into
+# oracle/_ref/librefnh.so, which needs no GPU.  Test infrastructure only; run where the
 # reference is mounted, the .so travels to the GPU box.  Flags follow the
 # reference's CMakeLists.txt:53.
 # The reference source tree: $(MDX_REFERENCE_SRC) when set, else the default
@@ -23,9 +25,12 @@ REF_DIRS = -I $(REF) -I $(REF)/Evaluators -I $(REF)/GPUArrays -I $(REF)/Fixes -I
            -I $(REF)/BondedForcers
 GRID_INC = -I ref_shim_grid -I $(CUDA_INC)/crt -I $(CUDA_INC) -I $(GRID_TMP) -I- -I ref_shim_grid $(REF_DIRS)
 RIGID_INC = -I ref_shim_rigid -I $(CUDA_INC)/crt -I $(CUDA_INC) -I $(GRID_TMP) -I- -I ref_shim_rigid $(REF_DIRS)
+NH_INC = -I ref_shim_nh -I $(CUDA_INC)/crt -I $(CUDA_INC) -I $(GRID_TMP) -I- -I ref_shim_nh $(REF_DIRS)
+
+all: _ref/librefkernels.so _ref/librefnh.so
 
 ifeq ($(wildcard $(REF)/Evaluators/PairEvaluateIso.h),)
-_ref/librefkernels.so:
+_ref/librefkernels.so _ref/librefnh.so:
 	@echo "reference sources not found under $(REF): oracle/_ref not built"
 else
 _ref/librefkernels.so: _ref/ref_harness.o _ref/ref_grid_harness.o _ref/ref_rigid_harness.o
@@ -42,9 +47,16 @@ _ref/ref_grid_harness.o: ref_grid_harness.cu $(wildcard ref_shim_grid/*.h ref_sh
 _ref/ref_rigid_harness.o: ref_rigid_harness.cu $(wildcard ref_shim_rigid/*.h ref_shim_rigid/boost/*.hpp)
 	@mkdir -p _ref $(GRID_TMP)
 	TMPDIR=$(abspath $(GRID_TMP)) $(NVCC) $(FLAGS) $(RIGID_INC) -c -o $@ ref_rigid_harness.cu
+
+_ref/librefnh.so: _ref/ref_nh_harness.o
+	$(NVCC) -gencode arch=compute_100a,code=sm_100a -shared -o $@ $^
+
+_ref/ref_nh_harness.o: ref_nh_harness.cu $(wildcard ref_shim_nh/*.h ref_shim_nh/boost/*.hpp ref_shim_nh/boost/python/*)
+	@mkdir -p _ref $(GRID_TMP)
+	TMPDIR=$(abspath $(GRID_TMP)) $(NVCC) $(FLAGS) $(NH_INC) -c -o $@ ref_nh_harness.cu
 endif
 
 clean:
 	rm -rf _ref
 
-.PHONY: clean
+.PHONY: all clean

@@ -1,0 +1,23 @@
+// Test infrastructure only (oracle/ref_nh_harness.cu).
+// Stand-in for the reference's DataComputerPressure: the fields
+// FixNoseHoover.cu reads, set by the harness
+#pragma once
+#include <cstdint>
+#include <string>
+#include "Virial.h"
+class State;
+namespace MD_ENGINE {
+class DataComputerPressure {
+public:
+    double tempScalar = 0.0, pressureScalar = 0.0;
+    Virial tempTensor, pressureTensor;
+    int64_t tempNDF = 0;
+    bool usingExternalTemperature = false;
+    DataComputerPressure(State *, std::string) {}
+    void prepareForRun() {}
+    void computeScalar_GPU(bool, uint32_t) {}
+    void computeScalar_CPU() {}
+    void computeTensor_GPU(bool, uint32_t) {}
+    void computeTensor_CPU() {}
+};
+}  // namespace MD_ENGINE

@@ -1,0 +1,19 @@
+// Test infrastructure only (oracle/ref_nh_harness.cu).
+// Stand-in for the reference's Interpolator: a constant set point (the
+// harness drives FixNoseHoover's propagator at fixed temperature/pressure)
+#pragma once
+#include <cstdint>
+#include <vector>
+#include <boost/python.hpp>
+class Interpolator {
+public:
+    double constVal = 0.0, currentVal = 0.0;
+    int64_t turnBeginRun = 0, turnFinishRun = 0;
+    Interpolator() {}
+    explicit Interpolator(double v) : constVal(v), currentVal(v) {}
+    explicit Interpolator(boost::python::object) {}
+    Interpolator(boost::python::list, boost::python::list) {}
+    void computeCurrentVal(int64_t) { currentVal = constVal; }
+    double getCurrentVal() { return constVal; }
+    void finishRun() {}
+};

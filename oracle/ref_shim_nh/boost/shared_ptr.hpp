@@ -1,0 +1,7 @@
+// Test infrastructure only (oracle/ref_rigid_harness.cu, oracle/ref_nh_harness.cu).
+// Stand-in for <boost/shared_ptr.hpp>
+#pragma once
+#include <memory>
+namespace boost {
+using std::shared_ptr;
+}

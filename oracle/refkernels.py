@@ -193,3 +193,36 @@ def settle(x0, x, v, masses, lo, L, dt, ftm_to_v, mode):
     if r != 0:
         raise RuntimeError(f"reference SETTLE failed: {r}")
     return X[:, :3].astype(np.float64), Vv[:, :3].astype(np.float64)
+
+
+NH_PATH = os.path.join(_HERE, "_ref", "librefnh.so")
+_NH = None
+
+
+def nh_available():
+    return os.path.exists(NH_PATH)
+
+
+def nh_barostat(op, step_init, par, pvel, pmass, ptv, ptf, ptm):
+    """one call of the reference's host-side isotropic MTK propagator
+    (FixNoseHoover.cu compiled from source into oracle/_ref/librefnh.so; no
+    GPU needed): op 0 updateBarostatMasses, 1 updateBarostatThermalMasses,
+    2 barostatThermostatIntegrate, 3 barostatVelocityIntegrate.  par = (natoms,
+    ndf, T, P, pfreq, dt, boltz, nktv_to_press, p_inst, t_inst, Lx, Ly, Lz).
+    Returns the updated (pvel, pmass, ptv, ptf, ptm) as new float64 arrays."""
+    global _NH
+    if _NH is None:
+        _NH = ctypes.CDLL(NH_PATH)
+        V = ctypes.c_void_p
+        I = ctypes.c_int
+        _NH.ref_nh_barostat.argtypes = [I, I, V, I, V, V, V, V, V]
+        _NH.ref_nh_barostat.restype = I
+    par = np.ascontiguousarray(par, np.float64)
+    assert par.shape == (13,)
+    out = [np.array(a, np.float64, copy=True) for a in (pvel, pmass, ptv, ptf, ptm)]
+    chain = len(out[2])
+    assert len(out[0]) == len(out[1]) == 3 and len(out[3]) == len(out[4]) == chain
+    r = _NH.ref_nh_barostat(int(op), int(bool(step_init)), _p(par), chain, *(_p(a) for a in out))
+    if r != 0:
+        raise RuntimeError(f"reference barostat propagator failed: {r}")
+    return tuple(out)

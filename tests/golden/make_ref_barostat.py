@@ -1,0 +1,83 @@
+"""Generate tests/golden/ref_barostat.json from the reference's own isotropic
+MTK barostat propagator (FixNoseHoover.cu: updateBarostatMasses :628-667,
+updateBarostatThermalMasses :669-700, barostatThermostatIntegrate :702-793,
+barostatVelocityIntegrate :868-943), compiled from the reference source by
+oracle/ref.mk into oracle/_ref/librefnh.so (host code; no GPU needed).
+
+Each case drives the barostat variables through the calls one NPT step
+makes, in the order of the step's hooks (stepInit: masses, thermal masses,
+the barostat chain at the old set point, the first cell-velocity kick;
+postNVE_V: the second kick; stepFinal: masses, thermal masses, the chain),
+with a seeded kinetic energy and pressure for every kick standing in for
+the particles.  The fixture holds the inputs, every call's output for the
+first steps and the state after the last.
+
+Run in a checkout where the reference source is present:
+    make -f oracle/ref.mk && python tests/golden/make_ref_barostat.py"""
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle import refkernels as R  # noqa: E402
+
+# (name, natoms, ndf, T, P, pfreq, dt, L, chain, steps, recorded steps)
+CASES = [
+    # box lengths and time step exactly representable in float: the
+    # reference's float cell volume and float time step equal the FP64 ones
+    ("lj500_chain10", 500, 1497, 1.2, 0.8, 1.0, float(np.float32(0.005)), (8.5, 8.5, 8.5), 10, 25, 3),
+    ("lj256_chain4", 256, 765, 0.9, 1.5, 2.0, 0.00390625, (7.0, 7.25, 6.5), 4, 25, 3),
+    # general box lengths and dt = 0.005 (the reference rounds both to float)
+    ("lj864_general", 864, 2589, 1.1, 0.6, 1.0, 0.005, (10.1, 9.7, 10.3), 10, 25, 0),
+]
+
+
+def calls_of_step(ke1, p1, ke2, p2):
+    return [(0, 1, None), (1, 1, None), (2, 1, None), (3, 0, (ke1, p1)), (3, 0, (ke2, p2)),
+            (0, 0, None), (1, 0, None), (2, 0, None)]
+
+
+def run(case):
+    name, natoms, ndf, T, P, pfreq, dt, L, chain, steps, rec = case
+    rng = np.random.default_rng(20261204 + natoms)
+    kicks = []
+    for _ in range(steps):
+        ke = ndf * T * (1.0 + 0.15 * rng.standard_normal(2))
+        p = P + 0.6 * rng.standard_normal(2)
+        kicks.append([float(ke[0]), float(p[0]), float(ke[1]), float(p[1])])
+    st = (np.zeros(3), np.zeros(3), np.zeros(chain), np.zeros(chain), np.zeros(chain))
+
+    def call(st, op, si, kp):
+        ke, p = kp if kp is not None else (0.0, 0.0)
+        par = [natoms, ndf, T, P, pfreq, dt, 1.0, 1.0, p, ke / ndf, L[0], L[1], L[2]]
+        return R.nh_barostat(op, si, par, *st)
+
+    # the prepare-time masses (FixNoseHoover::prepareFinal)
+    st = call(st, 0, 0, None)
+    st = call(st, 1, 0, None)
+    records = []
+    for s, (ke1, p1, ke2, p2) in enumerate(kicks):
+        for op, si, kp in calls_of_step(ke1, p1, ke2, p2):
+            st = call(st, op, si, kp)
+            if s < rec:
+                records.append({"step": s, "op": op, "step_init": si, "out": [a.tolist() for a in st]})
+    return {"name": name, "natoms": natoms, "ndf": ndf, "T": T, "P": P, "pfreq": pfreq, "dt": dt, "L": list(L),
+            "chain": chain, "kicks": kicks, "records": records, "final": [a.tolist() for a in st]}
+
+
+def main():
+    if not R.nh_available():
+        raise SystemExit("oracle/_ref/librefnh.so is not built")
+    out = {"source": "FixNoseHoover.cu barostat propagators, compiled from the reference source",
+           "cases": [run(c) for c in CASES]}
+    with open(os.path.join(HERE, "ref_barostat.json"), "w") as f:
+        json.dump(out, f, indent=0)
+        f.write("\n")
+
+
+if __name__ == "__main__":
+    main()

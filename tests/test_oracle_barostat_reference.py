@@ -1,0 +1,128 @@
+"""The oracle's MTK barostat propagator (oracle/mtk.py) against the
+reference's own (FixNoseHoover.cu: updateBarostatMasses :628-667,
+updateBarostatThermalMasses :669-700, barostatThermostatIntegrate :702-793,
+barostatVelocityIntegrate :868-943), on CPU.
+
+tests/golden/ref_barostat.json holds the reference's outputs
+(tests/golden/make_ref_barostat.py, from FixNoseHoover.cu compiled from
+source); where oracle/_ref/librefnh.so is built the reference also runs
+live.  In its own precision (float pressure, cell kick, volume and time
+step) the oracle reproduces the reference call for call, bit for bit with
+this image's libm (the test allows 1e-14 for another libm's exp); in FP64,
+the precision the library's propagator computes in, it stays within the
+float rounding of those four quantities (relative 1e-6 on the barostat
+variables after 25 steps)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import refkernels as R
+from oracle.mtk import MTKLJ
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FIX = json.load(open(os.path.join(HERE, "golden", "ref_barostat.json")))
+
+
+def calls_of_step(k):
+    ke1, p1, ke2, p2 = k
+    return [(0, 1, None), (1, 1, None), (2, 1, None), (3, 0, (ke1, p1)), (3, 0, (ke2, p2)),
+            (0, 0, None), (1, 0, None), (2, 0, None)]
+
+
+def bare(c, ref_float):
+    m = MTKLJ.__new__(MTKLJ)
+    m.T, m.P, m.pfreq = c["T"], c["P"], c["pfreq"]
+    m.n, m.ndf, m.pc = c["natoms"], c["ndf"], c["chain"]
+    # the reference's time step is a float
+    m.dt = float(np.float32(c["dt"])) if ref_float else c["dt"]
+    m.L = np.asarray(c["L"], np.float64)
+    m.pvel, m.pmass = [0.0] * 3, [0.0] * 3
+    m.ptv, m.ptf, m.ptm = [0.0] * m.pc, [0.0] * m.pc, [0.0] * m.pc
+    return m
+
+
+def apply(m, op, si, kp, ref_float):
+    if op == 0:
+        m.barostat_masses()
+    elif op == 1:
+        m.barostat_thermal_masses()
+    elif op == 2:
+        m.barostat_thermostat(bool(si))
+    else:
+        m.barostat_velocity(kp[0], kp[1], ref_float=ref_float)
+
+
+def state(m):
+    return [np.asarray(a, np.float64) for a in (m.pvel, m.pmass, m.ptv, m.ptf, m.ptm)]
+
+
+def close(got, want, rtol, atol, what):
+    for name, g, w in zip(("pvel", "pmass", "ptv", "ptf", "ptm"), got, want):
+        np.testing.assert_allclose(g, np.asarray(w), rtol=rtol, atol=atol, err_msg=f"{what}: {name}")
+
+
+def replay(c, ref_float, rtol, atol):
+    m = bare(c, ref_float)
+    m.barostat_masses()
+    m.barostat_thermal_masses()
+    recs = iter(c["records"])
+    for s, k in enumerate(c["kicks"]):
+        for op, si, kp in calls_of_step(k):
+            apply(m, op, si, kp, ref_float)
+            r = next(recs, None) if s < len(c["records"]) // 8 else None
+            if r is not None:
+                assert (r["step"], r["op"], r["step_init"]) == (s, op, si)
+                close(state(m), r["out"], rtol, atol, f"{c['name']} step {s} op {op}")
+    close(state(m), c["final"], rtol, atol, f"{c['name']} after {len(c['kicks'])} steps")
+
+
+@pytest.mark.parametrize("c", FIX["cases"], ids=lambda c: c["name"])
+def test_oracle_in_reference_precision_matches_reference(c):
+    replay(c, True, 1e-14, 0.0)
+
+
+@pytest.mark.parametrize("c", FIX["cases"], ids=lambda c: c["name"])
+def test_oracle_fp64_within_reference_float_rounding(c):
+    replay(c, False, 1e-6, 1e-9)
+
+
+def test_reference_precision_differs_from_fp64_where_float_rounds():
+    """a planted difference, on the CPU: the general box (float volume and
+    float dt differ from FP64) moves the FP64 replay off the reference's
+    values by more than the in-precision tolerance, so that tolerance is not
+    vacuous"""
+    c = next(c for c in FIX["cases"] if c["name"] == "lj864_general")
+    with pytest.raises(AssertionError):
+        replay(c, False, 1e-13, 1e-15)
+
+
+@pytest.mark.skipif(not R.nh_available(), reason="oracle/_ref/librefnh.so not built")
+@pytest.mark.parametrize("c", FIX["cases"], ids=lambda c: c["name"])
+def test_live_reference_reproduces_fixture(c):
+    """the reference propagator compiled here gives the committed values"""
+    z = c["chain"]
+    st = (np.zeros(3), np.zeros(3), np.zeros(z), np.zeros(z), np.zeros(z))
+
+    def call(st, op, si, kp):
+        ke, p = kp if kp is not None else (0.0, 0.0)
+        par = [c["natoms"], c["ndf"], c["T"], c["P"], c["pfreq"], c["dt"], 1.0, 1.0, p, ke / c["ndf"]] + c["L"]
+        return R.nh_barostat(op, si, par, *st)
+
+    st = call(st, 0, 0, None)
+    st = call(st, 1, 0, None)
+    for k in c["kicks"]:
+        for op, si, kp in calls_of_step(k):
+            st = call(st, op, si, kp)
+    close(st, c["final"], 0.0, 0.0, c["name"])
+
+
+@pytest.mark.skipif(not R.nh_available(), reason="oracle/_ref/librefnh.so not built")
+def test_live_reference_rejects_bad_calls():
+    z = np.zeros(10)
+    par = [100, 297, 1.0, 1.0, 1.0, 0.005, 1.0, 1.0, 1.0, 1.0, 5.0, 5.0, 5.0]
+    with pytest.raises(RuntimeError):
+        R.nh_barostat(7, 0, par, np.zeros(3), np.zeros(3), z, z, z)
+    with pytest.raises(RuntimeError):
+        R.nh_barostat(0, 0, par, np.zeros(3), np.zeros(3), z[:1], z[:1], z[:1])
