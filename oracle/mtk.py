@@ -15,7 +15,7 @@ rebuilt every step (the box moves every step).
 Parity: the barostat propagators (masses, thermal masses, the barostat
 chain, the cell-velocity kick) are pinned against the reference's own
 FixNoseHoover.cu compiled from source on the CPU (oracle/ref_nh_harness.cu
--> oracle/_ref/librefnh.so; fixture tests/golden/ref_barostat.json): with
+-> oracle/_ref/librefbarostat.so; fixture tests/golden/ref_barostat.json): with
 barostat_velocity(ref_float=True) and a float time step this restatement
 reproduces the reference bit for bit; in FP64 (the library's precision) it
 differs only by the reference's float rounding of the pressure, the cell

@@ -1,9 +1,10 @@
 # Compiles the reference's own kernels (from the reference sources in place)
 # plus oracle/ref_harness.cu, oracle/ref_grid_harness.cu and
 # oracle/ref_rigid_harness.cu into
-# oracle/_ref/librefkernels.so, and the reference's host-side MTK barostat
-# propagator (FixNoseHoover.cu) with oracle/ref_nh_harness.cu into
-# oracle/_ref/librefnh.so, which needs no GPU.  Test infrastructure only; run where the
+# oracle/_ref/librefkernels.so, and the reference's host-side barostat code
+# (FixNoseHoover.cu's MTK propagator, FixPressureBerendsen.cu's step) with
+# oracle/ref_nh_harness.cu and oracle/ref_berendsen_harness.cu into
+# oracle/_ref/librefbarostat.so, which needs no GPU.  Test infrastructure only; run where the
 # reference is mounted, the .so travels to the GPU box.  Flags follow the
 # reference's CMakeLists.txt:53.
 # The reference source tree: $(MDX_REFERENCE_SRC) when set, else the default
@@ -27,10 +28,10 @@ GRID_INC = -I ref_shim_grid -I $(CUDA_INC)/crt -I $(CUDA_INC) -I $(GRID_TMP) -I-
 RIGID_INC = -I ref_shim_rigid -I $(CUDA_INC)/crt -I $(CUDA_INC) -I $(GRID_TMP) -I- -I ref_shim_rigid $(REF_DIRS)
 NH_INC = -I ref_shim_nh -I $(CUDA_INC)/crt -I $(CUDA_INC) -I $(GRID_TMP) -I- -I ref_shim_nh $(REF_DIRS)
 
-all: _ref/librefkernels.so _ref/librefnh.so
+all: _ref/librefkernels.so _ref/librefbarostat.so
 
 ifeq ($(wildcard $(REF)/Evaluators/PairEvaluateIso.h),)
-_ref/librefkernels.so _ref/librefnh.so:
+_ref/librefkernels.so _ref/librefbarostat.so:
 	@echo "reference sources not found under $(REF): oracle/_ref not built"
 else
 _ref/librefkernels.so: _ref/ref_harness.o _ref/ref_grid_harness.o _ref/ref_rigid_harness.o
@@ -48,12 +49,16 @@ _ref/ref_rigid_harness.o: ref_rigid_harness.cu $(wildcard ref_shim_rigid/*.h ref
 	@mkdir -p _ref $(GRID_TMP)
 	TMPDIR=$(abspath $(GRID_TMP)) $(NVCC) $(FLAGS) $(RIGID_INC) -c -o $@ ref_rigid_harness.cu
 
-_ref/librefnh.so: _ref/ref_nh_harness.o
+_ref/librefbarostat.so: _ref/ref_nh_harness.o _ref/ref_berendsen_harness.o
 	$(NVCC) -gencode arch=compute_100a,code=sm_100a -shared -o $@ $^
 
 _ref/ref_nh_harness.o: ref_nh_harness.cu $(wildcard ref_shim_nh/*.h ref_shim_nh/boost/*.hpp ref_shim_nh/boost/python/*)
 	@mkdir -p _ref $(GRID_TMP)
 	TMPDIR=$(abspath $(GRID_TMP)) $(NVCC) $(FLAGS) $(NH_INC) -c -o $@ ref_nh_harness.cu
+
+_ref/ref_berendsen_harness.o: ref_berendsen_harness.cu $(wildcard ref_shim_nh/*.h ref_shim_nh/boost/*.hpp ref_shim_nh/boost/python/*)
+	@mkdir -p _ref $(GRID_TMP)
+	TMPDIR=$(abspath $(GRID_TMP)) $(NVCC) $(FLAGS) $(NH_INC) -c -o $@ ref_berendsen_harness.cu
 endif
 
 clean:

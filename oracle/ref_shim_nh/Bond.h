@@ -1,4 +1,4 @@
-// Test infrastructure only (oracle/ref_rigid_harness.cu, oracle/ref_nh_harness.cu).
+// Test infrastructure only (oracle/ref_nh_harness.cu, oracle/ref_berendsen_harness.cu).
 // Stand-in for the reference's Bond.h: the bond record the Fix stand-in names
 #pragma once
 #include <array>

@@ -1,6 +1,6 @@
-// Test infrastructure only (oracle/ref_nh_harness.cu).
+// Test infrastructure only (oracle/ref_nh_harness.cu, oracle/ref_berendsen_harness.cu).
 // Stand-in for the reference's DataComputerPressure: the fields
-// FixNoseHoover.cu reads, set by the harness
+// the barostats read, set by the harnesses
 #pragma once
 #include <cstdint>
 #include <string>

@@ -1,4 +1,4 @@
-// Test infrastructure only (oracle/ref_nh_harness.cu).
+// Test infrastructure only (oracle/ref_nh_harness.cu, oracle/ref_berendsen_harness.cu).
 // Stand-in for the reference's DataComputerTemperature: the fields
 // FixNoseHoover.cu reads, set by the harness (the GPU reductions are not
 // part of what the harness runs)

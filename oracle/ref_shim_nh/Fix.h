@@ -1,5 +1,5 @@
-// Test infrastructure only (oracle/ref_nh_harness.cu).
-// Stand-in for the reference's Fix.h: the base-class members FixNoseHoover.cu uses
+// Test infrastructure only (oracle/ref_nh_harness.cu, oracle/ref_berendsen_harness.cu).
+// Stand-in for the reference's Fix.h: the base-class members the barostats use
 #pragma once
 #include <cstdint>
 #include <string>
@@ -15,7 +15,8 @@ public:
     std::string handle, groupHandle, type;
     uint32_t groupTag = 1;
     bool prepared = false;
-    bool requiresPostNVE_V = false, requiresForces = false, isThermostat = false, requiresVirials = false;
+    bool requiresPostNVE_V = false, requiresForces = false, isThermostat = false, requiresVirials = false,
+         requiresPerAtomVirials = false;
     int virialMode = 0;
     template <class... A>
     Fix(boost::shared_ptr<State> s, std::string h, std::string g, std::string t, A...)

@@ -1,4 +1,4 @@
-// Test infrastructure only (oracle/ref_nh_harness.cu).
+// Test infrastructure only (oracle/ref_nh_harness.cu, oracle/ref_berendsen_harness.cu).
 // Stand-in for the reference's GPUArrayGlobal: a sized host array with no
 // device storage, so that FixNoseHoover's constructor (which sizes a
 // two-element kinetic-energy array) runs on a machine without a GPU.  The

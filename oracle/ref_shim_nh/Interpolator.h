@@ -1,6 +1,6 @@
-// Test infrastructure only (oracle/ref_nh_harness.cu).
+// Test infrastructure only (oracle/ref_nh_harness.cu, oracle/ref_berendsen_harness.cu).
 // Stand-in for the reference's Interpolator: a constant set point (the
-// harness drives FixNoseHoover's propagator at fixed temperature/pressure)
+// harnesses drive the barostats at a fixed temperature and pressure)
 #pragma once
 #include <cstdint>
 #include <vector>
@@ -9,6 +9,7 @@ class Interpolator {
 public:
     double constVal = 0.0, currentVal = 0.0;
     int64_t turnBeginRun = 0, turnFinishRun = 0;
+    bool finished = false;
     Interpolator() {}
     explicit Interpolator(double v) : constVal(v), currentVal(v) {}
     explicit Interpolator(boost::python::object) {}

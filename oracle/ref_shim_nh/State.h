@@ -1,5 +1,5 @@
-// Test infrastructure only (oracle/ref_nh_harness.cu).
-// Stand-in for the reference's State.h: the members FixNoseHoover.cu reads,
+// Test infrastructure only (oracle/ref_nh_harness.cu, oracle/ref_berendsen_harness.cu).
+// Stand-in for the reference's State.h: the members the barostats read,
 // with the reference's types (the time step and the unit factors are real,
 // State.h:117, Units.h:8-13)
 #pragma once
@@ -26,4 +26,5 @@ public:
     GPUData gpd;
     int64_t turn = 0, runInit = 0, runningFor = 0;
     real dt = 0.0;
+    void findRigidBodies() {}
 };

@@ -1,5 +1,5 @@
-// Test infrastructure only (oracle/ref_rigid_harness.cu, oracle/ref_nh_harness.cu).
-// Stand-in for <boost/python.hpp>: the names FixNoseHoover.cu mentions, doing nothing
+// Test infrastructure only (oracle/ref_nh_harness.cu, oracle/ref_berendsen_harness.cu).
+// Stand-in for <boost/python.hpp>: the names the barostat sources mention, doing nothing
 #pragma once
 #include <string>
 namespace boost {

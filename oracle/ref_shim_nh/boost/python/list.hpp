@@ -1,3 +1,3 @@
-// Test infrastructure only (oracle/ref_rigid_harness.cu, oracle/ref_nh_harness.cu).
+// Test infrastructure only (oracle/ref_nh_harness.cu, oracle/ref_berendsen_harness.cu).
 #pragma once
 #include <boost/python.hpp>

@@ -1,4 +1,4 @@
-// Test infrastructure only (oracle/ref_rigid_harness.cu, oracle/ref_nh_harness.cu).
+// Test infrastructure only (oracle/ref_nh_harness.cu, oracle/ref_berendsen_harness.cu).
 // Stand-in for <boost/shared_ptr.hpp>
 #pragma once
 #include <memory>

@@ -195,34 +195,55 @@ def settle(x0, x, v, masses, lo, L, dt, ftm_to_v, mode):
     return X[:, :3].astype(np.float64), Vv[:, :3].astype(np.float64)
 
 
-NH_PATH = os.path.join(_HERE, "_ref", "librefnh.so")
+BAROSTAT_PATH = os.path.join(_HERE, "_ref", "librefbarostat.so")
 _NH = None
 
 
-def nh_available():
-    return os.path.exists(NH_PATH)
+def barostat_available():
+    return os.path.exists(BAROSTAT_PATH)
+
+
+def _barostat_lib():
+    global _NH
+    if _NH is None:
+        _NH = ctypes.CDLL(BAROSTAT_PATH)
+        V = ctypes.c_void_p
+        I = ctypes.c_int
+        D = ctypes.c_double
+        _NH.ref_nh_barostat.argtypes = [I, I, V, I, V, V, V, V, V]
+        _NH.ref_nh_barostat.restype = I
+        _NH.ref_berendsen_dilation.argtypes = [D, D, D, D, D, D, V]
+        _NH.ref_berendsen_dilation.restype = I
+    return _NH
 
 
 def nh_barostat(op, step_init, par, pvel, pmass, ptv, ptf, ptm):
     """one call of the reference's host-side isotropic MTK propagator
-    (FixNoseHoover.cu compiled from source into oracle/_ref/librefnh.so; no
-    GPU needed): op 0 updateBarostatMasses, 1 updateBarostatThermalMasses,
+    (FixNoseHoover.cu compiled from source into oracle/_ref/librefbarostat.so;
+    no GPU needed): op 0 updateBarostatMasses, 1 updateBarostatThermalMasses,
     2 barostatThermostatIntegrate, 3 barostatVelocityIntegrate.  par = (natoms,
     ndf, T, P, pfreq, dt, boltz, nktv_to_press, p_inst, t_inst, Lx, Ly, Lz).
     Returns the updated (pvel, pmass, ptv, ptf, ptm) as new float64 arrays."""
-    global _NH
-    if _NH is None:
-        _NH = ctypes.CDLL(NH_PATH)
-        V = ctypes.c_void_p
-        I = ctypes.c_int
-        _NH.ref_nh_barostat.argtypes = [I, I, V, I, V, V, V, V, V]
-        _NH.ref_nh_barostat.restype = I
     par = np.ascontiguousarray(par, np.float64)
     assert par.shape == (13,)
     out = [np.array(a, np.float64, copy=True) for a in (pvel, pmass, ptv, ptf, ptm)]
     chain = len(out[2])
     assert len(out[0]) == len(out[1]) == 3 and len(out[3]) == len(out[4]) == chain
-    r = _NH.ref_nh_barostat(int(op), int(bool(step_init)), _p(par), chain, *(_p(a) for a in out))
+    r = _barostat_lib().ref_nh_barostat(int(op), int(bool(step_init)), _p(par), chain, *(_p(a) for a in out))
     if r != 0:
         raise RuntimeError(f"reference barostat propagator failed: {r}")
     return tuple(out)
+
+
+def berendsen_dilation(target, pressure, period, dt, bulk=-1.0, max_dil=-1.0):
+    """the box scale factors of one reference FixPressureBerendsen step
+    (stepFinal, FixPressureBerendsen.cu:26-46, compiled from source into
+    oracle/_ref/librefbarostat.so; no GPU needed) at the instantaneous
+    pressure `pressure`; bulk / max_dil < 0 keep the fix's defaults.
+    Returns the three float32 factors."""
+    out = np.zeros(3, np.float32)
+    r = _barostat_lib().ref_berendsen_dilation(float(target), float(pressure), float(period), float(dt),
+                                               float(bulk), float(max_dil), _p(out))
+    if r != 0:
+        raise RuntimeError(f"reference Berendsen step failed: {r}")
+    return out

@@ -1,8 +1,10 @@
 """Generate tests/golden/ref_barostat.json from the reference's own isotropic
 MTK barostat propagator (FixNoseHoover.cu: updateBarostatMasses :628-667,
 updateBarostatThermalMasses :669-700, barostatThermostatIntegrate :702-793,
-barostatVelocityIntegrate :868-943), compiled from the reference source by
-oracle/ref.mk into oracle/_ref/librefnh.so (host code; no GPU needed).
+barostatVelocityIntegrate :868-943) and Berendsen step
+(FixPressureBerendsen::stepFinal, FixPressureBerendsen.cu:26-46), compiled
+from the reference source by oracle/ref.mk into oracle/_ref/librefbarostat.so
+(host code; no GPU needed).
 
 Each case drives the barostat variables through the calls one NPT step
 makes, in the order of the step's hooks (stepInit: masses, thermal masses,
@@ -69,11 +71,27 @@ def run(case):
             "chain": chain, "kicks": kicks, "records": records, "final": [a.tolist() for a in st]}
 
 
+def berendsen_cases():
+    """a grid over the pressure offset (inside the clamp, at both clamps,
+    and a negative cube-root base), the period, dt, the bulk modulus and
+    maxDilation (-1: the fix's defaults)"""
+    out = []
+    for target, bulk, max_dil in ((1.0, -1.0, -1.0), (1.0, 20.0, 1e-3), (0.5, 5.0, 2e-2), (3.0, 100.0, 1e-1)):
+        for off in (0.0, 1e-4, -1e-4, 0.01, -0.01, 0.3, -0.3, 2.0, -2.0, 40.0, -40.0, 5e3, -5e3):
+            for period, dt in ((0.5, 0.005), (2.0, 0.002), (1.0, 0.00390625)):
+                p = target - off
+                d = R.berendsen_dilation(target, p, period, dt, bulk, max_dil)
+                out.append({"target": target, "pressure": p, "period": period, "dt": dt, "bulk": bulk,
+                            "max_dil": max_dil, "dilation": [float(x) for x in d]})
+    return out
+
+
 def main():
-    if not R.nh_available():
-        raise SystemExit("oracle/_ref/librefnh.so is not built")
-    out = {"source": "FixNoseHoover.cu barostat propagators, compiled from the reference source",
-           "cases": [run(c) for c in CASES]}
+    if not R.barostat_available():
+        raise SystemExit("oracle/_ref/librefbarostat.so is not built")
+    out = {"source": "FixNoseHoover.cu barostat propagators and FixPressureBerendsen.cu's step, "
+                     "compiled from the reference source",
+           "cases": [run(c) for c in CASES], "berendsen": berendsen_cases()}
     with open(os.path.join(HERE, "ref_barostat.json"), "w") as f:
         json.dump(out, f, indent=0)
         f.write("\n")

@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 from md_engine_b200 import FixNoseHoover, FixPressureBerendsen, IntegratorVerlet, systems
+from oracle import berendsen
 from tests.helpers import FORCE_RTOL, force_err, oracle_lj_params, oracle_water_params, water_bonds, water_small
 
 pytestmark = pytest.mark.gpu
@@ -115,8 +116,9 @@ def test_berendsen_dilation_follows_the_reference_formula():
     IntegratorVerlet(st).run(1)  # the barostat fires after the step of turn 0
     assert baro.applications == 1
     p, dil = baro.lastPressure, baro.lastDilation
-    want = (1.0 - 0.005 / 0.5 * (p0 + 3.0 - p) / 20.0) ** (1.0 / 3.0)
-    assert dil == pytest.approx(min(max(want, 1 - 1e-3), 1 + 1e-3), rel=1e-15, abs=1e-15)
+    # the oracle's FP64 dilation (pinned against the reference's stepFinal)
+    want = berendsen.dilation(p0 + 3.0, p, 0.5, 0.005, bulk=20.0, max_dil=1e-3)
+    assert dil == pytest.approx(want, rel=1e-15, abs=1e-15)
     assert dil < 1.0  # a target above the pressure compresses
     lo1, hi1 = _box(st)
     np.testing.assert_allclose(hi1 - lo1, (hi0 - lo0) * dil, rtol=1e-14)

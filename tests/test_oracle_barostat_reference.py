@@ -1,23 +1,30 @@
-"""The oracle's MTK barostat propagator (oracle/mtk.py) against the
-reference's own (FixNoseHoover.cu: updateBarostatMasses :628-667,
-updateBarostatThermalMasses :669-700, barostatThermostatIntegrate :702-793,
-barostatVelocityIntegrate :868-943), on CPU.
+"""The oracle's barostats against the reference's own, on CPU: the MTK
+propagator (oracle/mtk.py vs FixNoseHoover.cu: updateBarostatMasses
+:628-667, updateBarostatThermalMasses :669-700, barostatThermostatIntegrate
+:702-793, barostatVelocityIntegrate :868-943) and the Berendsen dilation
+(oracle/berendsen.py vs FixPressureBerendsen::stepFinal,
+FixPressureBerendsen.cu:26-46).
 
 tests/golden/ref_barostat.json holds the reference's outputs
 (tests/golden/make_ref_barostat.py, from FixNoseHoover.cu compiled from
-source); where oracle/_ref/librefnh.so is built the reference also runs
+source); where oracle/_ref/librefbarostat.so is built the reference also runs
 live.  In its own precision (float pressure, cell kick, volume and time
 step) the oracle reproduces the reference call for call, bit for bit with
 this image's libm (the test allows 1e-14 for another libm's exp); in FP64,
 the precision the library's propagator computes in, it stays within the
 float rounding of those four quantities (relative 1e-6 on the barostat
-variables after 25 steps)."""
+variables after 25 steps).  The Berendsen dilation matches the reference's
+bit for bit in its precision (a float time step and a float factor) and to
+float rounding in FP64, except where the cube root's base is negative: the
+reference passes NaN to the box rescale there, the library (and the FP64
+oracle) takes the lower clamp."""
 import json
 import os
 
 import numpy as np
 import pytest
 
+from oracle import berendsen as B
 from oracle import refkernels as R
 from oracle.mtk import MTKLJ
 
@@ -98,7 +105,7 @@ def test_reference_precision_differs_from_fp64_where_float_rounds():
         replay(c, False, 1e-13, 1e-15)
 
 
-@pytest.mark.skipif(not R.nh_available(), reason="oracle/_ref/librefnh.so not built")
+@pytest.mark.skipif(not R.barostat_available(), reason="oracle/_ref/librefbarostat.so not built")
 @pytest.mark.parametrize("c", FIX["cases"], ids=lambda c: c["name"])
 def test_live_reference_reproduces_fixture(c):
     """the reference propagator compiled here gives the committed values"""
@@ -118,7 +125,7 @@ def test_live_reference_reproduces_fixture(c):
     close(st, c["final"], 0.0, 0.0, c["name"])
 
 
-@pytest.mark.skipif(not R.nh_available(), reason="oracle/_ref/librefnh.so not built")
+@pytest.mark.skipif(not R.barostat_available(), reason="oracle/_ref/librefbarostat.so not built")
 def test_live_reference_rejects_bad_calls():
     z = np.zeros(10)
     par = [100, 297, 1.0, 1.0, 1.0, 0.005, 1.0, 1.0, 1.0, 1.0, 5.0, 5.0, 5.0]
@@ -126,3 +133,42 @@ def test_live_reference_rejects_bad_calls():
         R.nh_barostat(7, 0, par, np.zeros(3), np.zeros(3), z, z, z)
     with pytest.raises(RuntimeError):
         R.nh_barostat(0, 0, par, np.zeros(3), np.zeros(3), z[:1], z[:1], z[:1])
+
+
+def _bargs(c):
+    kw = {}
+    if c["bulk"] >= 0:
+        kw["bulk"] = c["bulk"]
+    if c["max_dil"] >= 0:
+        kw["max_dil"] = c["max_dil"]
+    return (c["target"], c["pressure"], c["period"], c["dt"]), kw
+
+
+def test_berendsen_in_reference_precision_matches_reference():
+    got = [B.dilation(*a, ref_float=True, **kw) for a, kw in map(_bargs, FIX["berendsen"])]
+    want = [c["dilation"][0] for c in FIX["berendsen"]]
+    assert all(c["dilation"][0] == c["dilation"][1] == c["dilation"][2] or np.isnan(c["dilation"]).all()
+               for c in FIX["berendsen"])
+    np.testing.assert_array_equal(np.array(got), np.array(want))
+    # the grid reaches both clamps, the inside and the NaN of a negative base
+    w = np.array(want)
+    assert np.isnan(w).sum() >= 4 and (w[~np.isnan(w)] < 1.0).any() and (w[~np.isnan(w)] > 1.0).any()
+
+
+def test_berendsen_fp64_matches_reference_but_for_the_negative_base():
+    for c in FIX["berendsen"]:
+        a, kw = _bargs(c)
+        d = B.dilation(*a, **kw)
+        want = c["dilation"][0]
+        if np.isnan(want):
+            # the reference's NaN box; the library compresses at the limit
+            assert d == 1.0 - kw.get("max_dil", 1e-5), c
+        else:
+            assert d == pytest.approx(want, rel=1.2e-7, abs=0.0), c
+
+
+@pytest.mark.skipif(not R.barostat_available(), reason="oracle/_ref/librefbarostat.so not built")
+def test_live_reference_berendsen_reproduces_fixture():
+    for c in FIX["berendsen"]:
+        d = R.berendsen_dilation(c["target"], c["pressure"], c["period"], c["dt"], c["bulk"], c["max_dil"])
+        np.testing.assert_array_equal(d.astype(np.float64), np.array(c["dilation"]))
