@@ -727,8 +727,23 @@ def msite_distribute(fO, fH1, fH2, fM, vO, vH1, vH2, invmO, invmH, gamma, dtf):
 # Nose-Hoover chain (FixNoseHoover.cu), host FP64 exactly as the reference
 # --------------------------------------------------------------------------
 class NoseHooverChain:
-    def __init__(self, T, tau, ndf, boltz, dt, chain=10):
-        self.T, self.freq, self.ndf, self.kB, self.dt = T, 1.0 / tau, ndf, boltz, dt
+    """FixNoseHoover's particle chain (FixNoseHoover.cu:221-290, 795-866,
+    1034-1041) in FP64, the library's precision.  ref_float: in the
+    reference's own precision instead -- its frequency and kinetic energy
+    are floats (`real frequency`, `real ke_current`, FixNoseHoover.h), as
+    are its time step (State.h:117) and Boltzmann constant (Units.h:8), and
+    M v^2 is taken as (M v) v.  Pinned against the reference's own chain
+    compiled from source on the CPU (oracle/ref_nh_harness.cu): bit for bit
+    with ref_float, to 1e-5 in FP64 over 40 steps."""
+
+    def __init__(self, T, tau, ndf, boltz, dt, chain=10, ref_float=False):
+        self.rf = ref_float
+        if ref_float:
+            f32 = np.float32
+            self.freq, boltz, dt = float(f32(1.0 / tau)), float(f32(boltz)), float(f32(dt))
+        else:
+            self.freq = 1.0 / tau
+        self.T, self.ndf, self.kB, self.dt = T, ndf, boltz, dt
         self.n = chain
         self.vel = [0.0] * chain
         self.force = [0.0] * chain
@@ -736,18 +751,27 @@ class NoseHooverChain:
         self.ke = 0.0
         self.scale = 1.0
 
+    def _freq2(self):
+        if self.rf:
+            return float(np.float32(self.freq) * np.float32(self.freq))
+        return self.freq ** 2
+
+    def _mv2(self, m, v):
+        return m * v * v if self.rf else m * v ** 2
+
     def update_masses(self):
-        self.mass[0] = self.ndf * self.kB * self.T / (self.freq ** 2)
+        f2 = self._freq2()
+        self.mass[0] = self.ndf * self.kB * self.T / f2
         for i in range(1, self.n):
-            self.mass[i] = self.kB * self.T / (self.freq ** 2)
+            self.mass[i] = self.kB * self.T / f2
 
     def prepare(self, ke):
         """prepareFinal (FixNoseHoover.cu:240-290): ke = sum m v^2 * mvv_to_eng."""
-        self.ke = ke
+        self.ke = float(np.float32(ke)) if self.rf else ke
         self.update_masses()
-        self.force[0] = (ke - self.ndf * self.kB * self.T) / self.mass[0]
+        self.force[0] = (self.ke - self.ndf * self.kB * self.T) / self.mass[0]
         for k in range(1, self.n):
-            self.force[k] = (self.mass[k - 1] * self.vel[k - 1] ** 2 - self.kB * self.T) / self.mass[k]
+            self.force[k] = (self._mv2(self.mass[k - 1], self.vel[k - 1]) - self.kB * self.T) / self.mass[k]
 
     def integrate(self, step_init):
         """thermostatIntegrate (FixNoseHoover.cu:795-866); returns the
@@ -770,7 +794,10 @@ class NoseHooverChain:
         v[0] += t4 * F[0]
         v[0] *= pf
         sf = math.exp(-t2 * v[0])
-        self.ke *= sf * sf
+        if self.rf:
+            self.ke = float(np.float32(self.ke * (sf * sf)))
+        else:
+            self.ke *= sf * sf
         v[0] *= pf
         F[0] = (self.ke - nkt) / Q[0]
         v[0] += t4 * F[0]
@@ -778,10 +805,10 @@ class NoseHooverChain:
         for k in range(1, n - 1):
             pf = math.exp(-t8 * v[k + 1])
             v[k] *= pf
-            F[k] = (Q[k - 1] * v[k - 1] ** 2 - self.kB * self.T) / Q[k]
+            F[k] = (self._mv2(Q[k - 1], v[k - 1]) - self.kB * self.T) / Q[k]
             v[k] += t4 * F[k]
             v[k] *= pf
-        F[n - 1] = (Q[n - 2] * v[n - 2] ** 2 - self.kB * self.T) / Q[n - 1]
+        F[n - 1] = (self._mv2(Q[n - 2], v[n - 2]) - self.kB * self.T) / Q[n - 1]
         v[n - 1] += t4 * F[n - 1]
         return sf
 

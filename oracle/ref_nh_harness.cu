@@ -1,5 +1,5 @@
-// Harness around the REFERENCE's own MTK barostat propagator -- TEST
-// INFRASTRUCTURE ONLY.
+// Harness around the REFERENCE's own Nose-Hoover propagators (the MTK
+// barostat's and the particles' chain) -- TEST INFRASTRUCTURE ONLY.
 //
 // oracle/ref.mk compiles the reference's src/Fixes/FixNoseHoover.cu where it
 // lies, with the reference's nvcc flags, against the stand-in headers of
@@ -7,16 +7,17 @@
 // pressure computers, the device arrays and the Boost.Python names
 // FixNoseHoover.cu mentions; the split include path makes them shadow the
 // reference's own).  The stand-in device arrays hold no device storage, so
-// nothing here needs a GPU: the harness calls only the four host-side
-// propagators of the isotropic barostat,
+// nothing here needs a GPU: the harness calls only host-side code -- the
+// four propagators of the isotropic barostat,
 //   updateBarostatMasses          (FixNoseHoover.cu:628-667)
 //   updateBarostatThermalMasses   (FixNoseHoover.cu:669-700)
 //   barostatThermostatIntegrate   (FixNoseHoover.cu:702-793)
 //   barostatVelocityIntegrate     (FixNoseHoover.cu:868-943)
-// on a FixNoseHoover whose members it sets (private members are opened to
-// this file only for that), and none of the fix's kernel launches.  The only
-// code written here is the C entry point that copies the barostat state in
-// and out.
+// and, for the particles' chain of a thermostat-only fix, prepareFinal,
+// updateThermalMasses and thermostatIntegrate -- on a FixNoseHoover whose
+// members it sets (private members are opened to this file only for that),
+// and none of the fix's kernel launches.  The only code written here is the
+// C entry points that copy the barostat and chain state in and out.
 #define private public
 #include "FixNoseHoover.cu"
 #undef private
@@ -49,7 +50,7 @@ int ref_nh_barostat(int op, int step_init, const double *par, int chain, double 
     FixNoseHoover fix(st, "nh", "all");
     fix.pressMode = PRESSMODE::ISO;
     fix.barostatting = true;
-    fix.boltz = par[6];
+    fix.boltz = st->units.boltz;  // as prepareFinal sets it (:259), from the float units
     fix.ndf = (size_t)par[1];
     fix.setPointTemperature = fix.oldSetPointTemperature = par[2];
     fix.setPointPressure = fix.oldSetPointPressure = par[3];
@@ -87,6 +88,61 @@ int ref_nh_barostat(int op, int step_init, const double *par, int chain, double 
         ptf[i] = fix.pressThermForce[i];
         ptm[i] = fix.pressThermMass[i];
     }
+    return 0;
+}
+
+// One call on the particles' Nose-Hoover chain of a thermostat-only fix
+// (setTemperature(T, tau), FixNoseHoover.cu:221-225):
+//   op 0 prepareFinal (:240-290, thermostatting only) with the kinetic
+//        energy *ke (sum m v^2) -> masses, forces, ke
+//   op 1 updateThermalMasses (:1034-1041)                -> tmass
+//   op 2 thermostatIntegrate(step_init) (:795-866) on *ke -> tvel, tforce,
+//        ke, scale (the accumulated velocity factor, *scale in, out)
+// par: natoms, ndf, T, tau, dt, boltz.  tvel, tforce, tmass: `chain` each
+// (in and out).  The fix keeps the kinetic energy and the scale as floats,
+// so *ke and *scale come back float-rounded.  Returns 0, or -1 for an
+// unknown op or a chain shorter than 2.
+int ref_nh_chain(int op, int step_init, const double *par, int chain, double *tvel, double *tforce, double *tmass,
+                 double *ke, double *scale) {
+    if (op < 0 || op > 2 || chain < 2) return -1;
+    auto st = boost::shared_ptr<State>(new State());
+    const int natoms = (int)par[0];
+    st->dt = par[4];
+    st->units.boltz = par[5];
+    st->boundsGPU = BoundsGPU(make_real3(0, 0, 0), make_real3(10, 10, 10), make_real3(1, 1, 1));
+    st->atoms.assign(natoms, Atom(Vector(0, 0, 0), 0, 0, 1.0, 0.0, nullptr));
+
+    FixNoseHoover fix(st, "nh", "all");
+    fix.setTemperature(par[2], par[3]);
+    fix.chainLength = (size_t)chain;
+    fix.thermVel.assign(tvel, tvel + chain);
+    fix.thermForce.assign(tforce, tforce + chain);
+    fix.thermMass.assign(tmass, tmass + chain);
+    fix.boltz = st->units.boltz;  // as prepareFinal sets it (:259), from the float units
+    fix.ndf = (size_t)par[1];
+    fix.setPointTemperature = fix.oldSetPointTemperature = par[2];
+    fix.ke_current = (real)*ke;
+    fix.scale = make_real3((real)*scale, (real)*scale, (real)*scale);
+
+    if (op == 0) {
+        // calculateKineticEnergy reads these from the temperature computer
+        fix.tempComputer.ndf = (int64_t)par[1];
+        fix.tempComputer.totalKEScalar = *ke;
+        fix.tempComputer.tempScalar = *ke / (par[1] * par[5]);
+        fix.prepareFinal();
+    } else if (op == 1) {
+        fix.updateThermalMasses();
+    } else {
+        fix.thermostatIntegrate(step_init != 0);
+    }
+
+    for (int i = 0; i < chain; i++) {
+        tvel[i] = fix.thermVel[i];
+        tforce[i] = fix.thermForce[i];
+        tmass[i] = fix.thermMass[i];
+    }
+    *ke = fix.ke_current;
+    *scale = fix.scale.x;
     return 0;
 }
 

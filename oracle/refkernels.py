@@ -214,6 +214,8 @@ def _barostat_lib():
         _NH.ref_nh_barostat.restype = I
         _NH.ref_berendsen_dilation.argtypes = [D, D, D, D, D, D, V]
         _NH.ref_berendsen_dilation.restype = I
+        _NH.ref_nh_chain.argtypes = [I, I, V, I, V, V, V, V, V]
+        _NH.ref_nh_chain.restype = I
     return _NH
 
 
@@ -247,3 +249,23 @@ def berendsen_dilation(target, pressure, period, dt, bulk=-1.0, max_dil=-1.0):
     if r != 0:
         raise RuntimeError(f"reference Berendsen step failed: {r}")
     return out
+
+
+def nh_chain(op, step_init, par, tvel, tforce, tmass, ke, scale):
+    """one call on the reference's particle Nose-Hoover chain of a
+    thermostat-only FixNoseHoover (compiled from source into
+    oracle/_ref/librefbarostat.so; no GPU needed): op 0 prepareFinal, 1
+    updateThermalMasses, 2 thermostatIntegrate.  par = (natoms, ndf, T, tau,
+    dt, boltz).  Returns the updated (tvel, tforce, tmass) as new float64
+    arrays and the kinetic energy and velocity scale (float-rounded, as the
+    fix holds them)."""
+    par = np.ascontiguousarray(par, np.float64)
+    assert par.shape == (6,)
+    out = [np.array(a, np.float64, copy=True) for a in (tvel, tforce, tmass)]
+    assert len(out[0]) == len(out[1]) == len(out[2])
+    kes = np.array([ke, scale], np.float64)
+    r = _barostat_lib().ref_nh_chain(int(op), int(bool(step_init)), _p(par), len(out[0]), *(_p(a) for a in out),
+                                     _p(kes[0:]), _p(kes[1:]))
+    if r != 0:
+        raise RuntimeError(f"reference Nose-Hoover chain failed: {r}")
+    return out[0], out[1], out[2], float(kes[0]), float(kes[1])

@@ -1,7 +1,9 @@
 """Generate tests/golden/ref_barostat.json from the reference's own isotropic
 MTK barostat propagator (FixNoseHoover.cu: updateBarostatMasses :628-667,
 updateBarostatThermalMasses :669-700, barostatThermostatIntegrate :702-793,
-barostatVelocityIntegrate :868-943) and Berendsen step
+barostatVelocityIntegrate :868-943), particle Nose-Hoover chain
+(prepareFinal :240-290, thermostatIntegrate :795-866, updateThermalMasses
+:1034-1041) and Berendsen step
 (FixPressureBerendsen::stepFinal, FixPressureBerendsen.cu:26-46), compiled
 from the reference source by oracle/ref.mk into oracle/_ref/librefbarostat.so
 (host code; no GPU needed).
@@ -86,12 +88,49 @@ def berendsen_cases():
     return out
 
 
+# (name, natoms, ndf, T, tau, dt, boltz, chain, steps, recorded steps)
+CHAIN_CASES = [
+    ("lj500_chain10", 500, 1497, 1.2, 0.5, 0.005, 1.0, 10, 40, 3),
+    ("lj256_chain3", 256, 765, 0.9, 0.1, 0.002, 1.0, 3, 40, 3),
+    # rigid TIP4P/2005 in real units (6 per molecule less the centre of mass)
+    ("water4096_real", 16384, 24573, 298.0, 100.0, 1.0, 0.0019872067, 10, 40, 0),
+]
+
+
+def run_chain(case):
+    """the thermostat-only fix's calls over `steps` steps: prepareFinal on a
+    seeded kinetic energy; then per step stepInit's thermostatIntegrate(true)
+    (its scale applied and reset by rescale) and stepFinal's
+    thermostatIntegrate(false) on the step's seeded kinetic energy"""
+    name, natoms, ndf, T, tau, dt, boltz, chain, steps, rec = case
+    rng = np.random.default_rng(20261205 + natoms)
+    kes = [float(ndf * boltz * T * (1.0 + 0.2 * x)) for x in rng.standard_normal(steps + 1)]
+    par = [natoms, ndf, T, tau, dt, boltz]
+    z = np.zeros(chain)
+    v, f, m, ke, sc = R.nh_chain(0, 0, par, z, z, z, kes[0], 1.0)
+    records = [{"step": -1, "op": 0, "step_init": 0, "out": [v.tolist(), f.tolist(), m.tolist(), ke, sc]}]
+    for s_ in range(steps):
+        v, f, m, ke, sc = R.nh_chain(2, 1, par, v, f, m, ke, sc)
+        if s_ < rec:
+            records.append({"step": s_, "op": 2, "step_init": 1, "out": [v.tolist(), f.tolist(), m.tolist(), ke, sc]})
+        sc = 1.0  # rescale() applies the scale and resets it
+        v, f, m, ke, sc = R.nh_chain(2, 0, par, v, f, m, kes[s_ + 1], sc)
+        if s_ < rec:
+            records.append({"step": s_, "op": 2, "step_init": 0, "out": [v.tolist(), f.tolist(), m.tolist(), ke, sc]})
+    # updateThermalMasses on the final state
+    v, f, m2, ke, sc = R.nh_chain(1, 0, par, v, f, np.zeros(chain), ke, sc)
+    return {"name": name, "natoms": natoms, "ndf": ndf, "T": T, "tau": tau, "dt": dt, "boltz": boltz,
+            "chain": chain, "kes": kes, "records": records, "final": [v.tolist(), f.tolist(), m.tolist(), ke, sc],
+            "masses": m2.tolist()}
+
+
 def main():
     if not R.barostat_available():
         raise SystemExit("oracle/_ref/librefbarostat.so is not built")
-    out = {"source": "FixNoseHoover.cu barostat propagators and FixPressureBerendsen.cu's step, "
+    out = {"source": "FixNoseHoover.cu barostat propagators and particle chain, FixPressureBerendsen.cu's step, "
                      "compiled from the reference source",
-           "cases": [run(c) for c in CASES], "berendsen": berendsen_cases()}
+           "cases": [run(c) for c in CASES], "chain": [run_chain(c) for c in CHAIN_CASES],
+           "berendsen": berendsen_cases()}
     with open(os.path.join(HERE, "ref_barostat.json"), "w") as f:
         json.dump(out, f, indent=0)
         f.write("\n")

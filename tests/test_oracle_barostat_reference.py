@@ -1,9 +1,11 @@
-"""The oracle's barostats against the reference's own, on CPU: the MTK
-propagator (oracle/mtk.py vs FixNoseHoover.cu: updateBarostatMasses
-:628-667, updateBarostatThermalMasses :669-700, barostatThermostatIntegrate
-:702-793, barostatVelocityIntegrate :868-943) and the Berendsen dilation
-(oracle/berendsen.py vs FixPressureBerendsen::stepFinal,
-FixPressureBerendsen.cu:26-46).
+"""The oracle's thermostat and barostats against the reference's own, on
+CPU: the MTK propagator (oracle/mtk.py vs FixNoseHoover.cu:
+updateBarostatMasses :628-667, updateBarostatThermalMasses :669-700,
+barostatThermostatIntegrate :702-793, barostatVelocityIntegrate :868-943),
+the particles' Nose-Hoover chain (oracle.NoseHooverChain vs prepareFinal
+:240-290, thermostatIntegrate :795-866, updateThermalMasses :1034-1041) and
+the Berendsen dilation (oracle/berendsen.py vs
+FixPressureBerendsen::stepFinal, FixPressureBerendsen.cu:26-46).
 
 tests/golden/ref_barostat.json holds the reference's outputs
 (tests/golden/make_ref_barostat.py, from FixNoseHoover.cu compiled from
@@ -13,7 +15,11 @@ step) the oracle reproduces the reference call for call, bit for bit with
 this image's libm (the test allows 1e-14 for another libm's exp); in FP64,
 the precision the library's propagator computes in, it stays within the
 float rounding of those four quantities (relative 1e-6 on the barostat
-variables after 25 steps).  The Berendsen dilation matches the reference's
+variables after 25 steps).  The chain likewise: bit for bit in the
+reference's precision (float frequency, kinetic energy, velocity scale, time
+step and Boltzmann constant), within 1e-5 in FP64 over 40 steps (1e-7 in LJ
+units; the float Boltzmann constant of real units moves the chain's
+(ke - N k T) by up to 3e-6).  The Berendsen dilation matches the reference's
 bit for bit in its precision (a float time step and a float factor) and to
 float rounding in FP64, except where the cube root's base is negative: the
 reference passes NaN to the box rescale there, the library (and the FP64
@@ -172,3 +178,73 @@ def test_live_reference_berendsen_reproduces_fixture():
     for c in FIX["berendsen"]:
         d = R.berendsen_dilation(c["target"], c["pressure"], c["period"], c["dt"], c["bulk"], c["max_dil"])
         np.testing.assert_array_equal(d.astype(np.float64), np.array(c["dilation"]))
+
+
+def _acc(scale, sf, ref_float):
+    # the fix's velocity scale is a float3 that `scale *= scaleFactor`
+    # multiplies by the float-converted factor
+    if ref_float:
+        return float(np.float32(scale) * np.float32(sf))
+    return scale * sf
+
+
+def chain_replay(c, ref_float, rtol, atol_frac):
+    """the thermostat-only fix's calls (prepareFinal; per step stepInit's
+    thermostatIntegrate(true) on the scale stepFinal left, that scale applied
+    and reset, then stepFinal's thermostatIntegrate(false) on the step's
+    kinetic energy) through the
+    oracle's chain, checked against the reference's outputs; atol_frac
+    scales each array's absolute tolerance by its largest value"""
+    from oracle import oracle as O
+    nh = O.NoseHooverChain(c["T"], c["tau"], c["ndf"], c["boltz"], c["dt"], c["chain"], ref_float=ref_float)
+    kes = c["kes"]
+
+    def check(scale, want, what):
+        got = (nh.vel, nh.force, nh.mass, [nh.ke], [scale])
+        for name, g, w in zip(("vel", "force", "mass", "ke", "scale"), got, want):
+            w = np.atleast_1d(np.asarray(w, np.float64))
+            np.testing.assert_allclose(np.asarray(g, np.float64), w, rtol=rtol,
+                                       atol=atol_frac * float(np.abs(w).max()), err_msg=f"{c['name']} {what}: {name}")
+
+    nh.prepare(kes[0])
+    recs = list(c["records"])
+    check(1.0, recs[0]["out"], "prepare")
+    nrec = (len(recs) - 1) // 2
+    scale = 1.0
+    for s in range(len(kes) - 1):
+        # stepInit multiplies the scale stepFinal left, then rescale()
+        # applies it and resets it to 1
+        scale = _acc(scale, nh.integrate(True), ref_float)
+        if s < nrec:
+            check(scale, recs[1 + 2 * s]["out"], f"step {s} init")
+        nh.ke = float(np.float32(kes[s + 1])) if ref_float else kes[s + 1]
+        scale = _acc(1.0, nh.integrate(False), ref_float)
+        if s < nrec:
+            check(scale, recs[2 + 2 * s]["out"], f"step {s} final")
+    check(scale, c["final"], "final")
+    nh.update_masses()
+    np.testing.assert_allclose(nh.mass, c["masses"], rtol=rtol, err_msg=f"{c['name']}: updateThermalMasses")
+
+
+@pytest.mark.parametrize("c", FIX["chain"], ids=lambda c: c["name"])
+def test_chain_in_reference_precision_matches_reference(c):
+    chain_replay(c, True, 1e-14, 0.0)
+
+
+@pytest.mark.parametrize("c", FIX["chain"], ids=lambda c: c["name"])
+def test_chain_fp64_within_reference_float_rounding(c):
+    chain_replay(c, False, 1e-5, 1e-5)
+
+
+@pytest.mark.skipif(not R.barostat_available(), reason="oracle/_ref/librefbarostat.so not built")
+@pytest.mark.parametrize("c", FIX["chain"], ids=lambda c: c["name"])
+def test_live_reference_chain_reproduces_fixture(c):
+    par = [c["natoms"], c["ndf"], c["T"], c["tau"], c["dt"], c["boltz"]]
+    z = np.zeros(c["chain"])
+    v, f, m, ke, sc = R.nh_chain(0, 0, par, z, z, z, c["kes"][0], 1.0)
+    for s in range(len(c["kes"]) - 1):
+        v, f, m, ke, sc = R.nh_chain(2, 1, par, v, f, m, ke, sc)
+        v, f, m, ke, sc = R.nh_chain(2, 0, par, v, f, m, c["kes"][s + 1], 1.0)
+    got = (v, f, m, [ke], [sc])
+    for g, w in zip(got, c["final"]):
+        np.testing.assert_array_equal(np.asarray(g, np.float64), np.atleast_1d(np.asarray(w, np.float64)))
