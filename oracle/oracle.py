@@ -389,23 +389,41 @@ _AMP = [
 ]
 
 
-def p3m_alpha(q, natoms, L, sz, rcut, order=5, qqr_to_eng=REAL_UNITS["qqr_to_eng"]):
-    """FixChargeEwald::find_optimal_parameters (FixChargeEwald.cu:848-967):
-    secant solve of DeltaF_k(alpha) = DeltaF_real(alpha)."""
-    Q2 = qqr_to_eng * float(np.sum(np.asarray(q, np.float64) ** 2))
-    L = np.asarray(L, np.float64)
-    h = L / np.asarray(sz, np.float64)
+def p3m_alpha(q, natoms, L, sz, rcut, order=5, qqr_to_eng=REAL_UNITS["qqr_to_eng"], ref_float=False, q2=None):
+    """FixChargeEwald::find_optimal_parameters (FixChargeEwald.cu:918-967):
+    secant solve of DeltaF_k(alpha) = DeltaF_real(alpha) (:865-883), in FP64
+    (the library's precision).  ref_float: in the reference's own precision
+    -- its box sides, mesh spacings, cutoff, total squared charge and alpha
+    are floats (real3 L, h; real r_cut, total_Q2, alpha; FixChargeEwald.h),
+    so L.x * L.x and the product under DeltaF_real's square root are float
+    arithmetic.  q2: the total squared charge times qqr_to_eng, in place of
+    the charges q."""
+    Q2 = qqr_to_eng * float(np.sum(np.asarray(q, np.float64) ** 2)) if q2 is None else float(q2)
     amp = _AMP[order - 1]
+    if ref_float:
+        f32 = np.float32
+        Lf = np.asarray(L, np.float32)
+        hf = Lf / np.asarray(sz, np.float32)
+        rcf, Q2f = f32(rcut), f32(Q2)
+        L, h, rcut, Q2 = Lf.astype(np.float64), hf.astype(np.float64), float(rcf), float(Q2f)
+        invL2 = 1.0 / (Lf * Lf).astype(np.float64)
+        vol = f32(f32(f32(f32(natoms) * rcf) * Lf[0]) * Lf[1]) * Lf[2]
+        pre_r = float(f32(f32(2) * Q2f) / np.sqrt(f32(vol)))
+    else:
+        L = np.asarray(L, np.float64)
+        h = L / np.asarray(sz, np.float64)
+        invL2 = 1.0 / (L * L)
+        pre_r = 2 * Q2 / math.sqrt(natoms * rcut * L[0] * L[1] * L[2])
 
     def dk(a):
         s = np.zeros(3)
         for m in range(order):
             s += amp[m] * (h * a) ** (2 * m)
-        return Q2 / 3.0 * float(np.sum(1.0 / (L * L) * (a * h) ** order *
+        return Q2 / 3.0 * float(np.sum(invL2 * (a * h) ** order *
                                        np.sqrt(a * L / natoms * math.sqrt(2.0 * math.pi) * s)))
 
     def dr(a):
-        return 2 * Q2 / math.sqrt(natoms * rcut * L[0] * L[1] * L[2]) * math.exp(-a * a * rcut * rcut)
+        return pre_r * math.exp(-a * a * rcut * rcut)
 
     xa, xb = 0.0, 4.79853 / rcut
     ya, yb = dk(xa) - dr(xa), dk(xb) - dr(xb)
@@ -416,7 +434,7 @@ def p3m_alpha(q, natoms, L, sz, rcut, order=5, qqr_to_eng=REAL_UNITS["qqr_to_eng
         xb = xa - ya * kinv
         yb = dk(xb) - dr(xb)
         it += 1
-    return xb
+    return float(np.float32(xb)) if ref_float else xb
 
 
 def _W5(i, x):

@@ -269,3 +269,35 @@ def nh_chain(op, step_init, par, tvel, tforce, tmass, ke, scale):
     if r != 0:
         raise RuntimeError(f"reference Nose-Hoover chain failed: {r}")
     return out[0], out[1], out[2], float(kes[0]), float(kes[1])
+
+
+EWALD_PATH = os.path.join(_HERE, "_ref", "librefewald.so")
+_EW = None
+
+
+def ewald_available():
+    return os.path.exists(EWALD_PATH)
+
+
+def ewald_alpha(natoms, L, sz, rcut, order, q2):
+    """the reference's FixChargeEwald::find_optimal_parameters
+    (FixChargeEwald.cu:918-967, compiled from source into
+    oracle/_ref/librefewald.so; host code, run where a GPU is) for natoms
+    atoms in a box of sides L, mesh sz, cutoff rcut, interpolation order
+    `order`, total squared charge q2 (times qqr_to_eng).  Returns (alpha, the
+    RMS error estimate); alpha is the float the fix keeps."""
+    global _EW
+    if _EW is None:
+        _EW = ctypes.CDLL(EWALD_PATH)
+        V = ctypes.c_void_p
+        I = ctypes.c_int
+        D = ctypes.c_double
+        _EW.ref_ewald_alpha.argtypes = [I, V, V, D, I, D, V, V]
+        _EW.ref_ewald_alpha.restype = I
+    Ld = np.ascontiguousarray(L, np.float64)
+    szi = np.ascontiguousarray(sz, np.int32)
+    out = np.zeros(2, np.float64)
+    r = _EW.ref_ewald_alpha(int(natoms), _p(Ld), _p(szi), float(rcut), int(order), float(q2), _p(out[0:]), _p(out[1:]))
+    if r != 0:
+        raise RuntimeError(f"reference Ewald parameter solve failed: {r}")
+    return float(out[0]), float(out[1])
