@@ -279,13 +279,7 @@ def ewald_available():
     return os.path.exists(EWALD_PATH)
 
 
-def ewald_alpha(natoms, L, sz, rcut, order, q2):
-    """the reference's FixChargeEwald::find_optimal_parameters
-    (FixChargeEwald.cu:918-967, compiled from source into
-    oracle/_ref/librefewald.so; host code, run where a GPU is) for natoms
-    atoms in a box of sides L, mesh sz, cutoff rcut, interpolation order
-    `order`, total squared charge q2 (times qqr_to_eng).  Returns (alpha, the
-    RMS error estimate); alpha is the float the fix keeps."""
+def _ewald_lib():
     global _EW
     if _EW is None:
         _EW = ctypes.CDLL(EWALD_PATH)
@@ -294,10 +288,37 @@ def ewald_alpha(natoms, L, sz, rcut, order, q2):
         D = ctypes.c_double
         _EW.ref_ewald_alpha.argtypes = [I, V, V, D, I, D, V, V]
         _EW.ref_ewald_alpha.restype = I
+        _EW.ref_ewald_green.argtypes = [V, V, D, I, V]
+        _EW.ref_ewald_green.restype = I
+    return _EW
+
+
+def ewald_alpha(natoms, L, sz, rcut, order, q2):
+    """the reference's FixChargeEwald::find_optimal_parameters
+    (FixChargeEwald.cu:918-967, compiled from source into
+    oracle/_ref/librefewald.so; host code, run where a GPU is) for natoms
+    atoms in a box of sides L, mesh sz, cutoff rcut, interpolation order
+    `order`, total squared charge q2 (times qqr_to_eng).  Returns (alpha, the
+    RMS error estimate); alpha is the float the fix keeps."""
     Ld = np.ascontiguousarray(L, np.float64)
     szi = np.ascontiguousarray(sz, np.int32)
     out = np.zeros(2, np.float64)
-    r = _EW.ref_ewald_alpha(int(natoms), _p(Ld), _p(szi), float(rcut), int(order), float(q2), _p(out[0:]), _p(out[1:]))
+    r = _ewald_lib().ref_ewald_alpha(int(natoms), _p(Ld), _p(szi), float(rcut), int(order), float(q2), _p(out[0:]),
+                                     _p(out[1:]))
     if r != 0:
         raise RuntimeError(f"reference Ewald parameter solve failed: {r}")
     return float(out[0]), float(out[1])
+
+
+def ewald_green(L, sz, alpha, order):
+    """the reference's influence function (Green_function_cu,
+    FixChargeEwald.cu:314-366, launched by calc_Green_function on the GPU)
+    for a box of sides L, mesh sz, splitting parameter alpha and
+    interpolation order `order`: float32 array of shape sz."""
+    Ld = np.ascontiguousarray(L, np.float64)
+    szi = np.ascontiguousarray(sz, np.int32)
+    out = np.zeros(tuple(int(x) for x in sz), np.float32)
+    r = _ewald_lib().ref_ewald_green(_p(Ld), _p(szi), float(alpha), int(order), _p(out))
+    if r != 0:
+        raise RuntimeError(f"reference Green function failed: {r}")
+    return out
